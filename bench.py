@@ -1,0 +1,333 @@
+"""Benchmark of the libcfd2lcs_b200 hot path (one JSON line on rank 0).
+
+Metric: grid-pt*RK-steps/s -- the reference's own integration counter
+(integrations_fwd + integrations_bkwd, src/lp_motion_m.f90:120-121: particles x subcycles)
+divided by the device time of the updates -- plus the FTLE-field time of an h boundary.
+
+A step is one cfd2lcs_update of the workload (every diagnostic advances through all of
+its CFL subcycles).  Default workload: the 3-D ABC flow on 256^3 (A=sqrt3, B=sqrt2, C=1),
+dt = 0.05, forward and backward FTLE with T = 10, h = 1, RK3, cubic B-spline, plain FP64.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload abc256|dg512] [--precision fp64|mixed]
+
+With --gpus N > 1 (under torchrun) each rank runs an independent replica of the workload
+(the single-field path has no halo exchange): weak scaling, no data-path collective.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "grid-pt·RK-steps/s + FTLE-field ms, mixed vs FP64 plain at stated FTLE error"
+UNIT = "grid-pt·RK-steps/s"
+
+# algorithmic HBM bytes per grid point per subcycle of the SL kernel: read u_n, u_np1 and
+# the previous flow map (3 components each), write the new flow map
+def sl_bytes_per_point(itemsize: int) -> int:
+    return 4 * 3 * itemsize
+
+
+WORKLOADS = {
+    "abc256": dict(kind="abc", n=256, dt=0.05, T=10.0, h=1.0, integrator=3, interpolator=3, dirs=(0, 1), t0=0.95,
+                   desc="ABC flow 256^3 periodic, dt=0.05, FTLE fwd+bkwd T=10 h=1, RK3, cubic B-spline"),
+    "dg512": dict(kind="dg", n=512, dt=0.1, T=15.0, h=1.5, integrator=2, interpolator=1, dirs=(1,), t0=1.4,
+                  desc="double gyre 512x256x1, dt=0.1, FTLE bkwd T=15 h=1.5, RK2, linear"),
+}
+
+
+def make_grid(w, n=None):
+    from libcfd2lcs_b200 import workloads as W
+    if w["kind"] == "abc":
+        g = W.abc_grid(n or w["n"])
+        vel = W.abc_velocity(g)
+        return g, (lambda t: vel), True
+    g = W.double_gyre_grid(n or w["n"], (n or w["n"]) // 2)
+    return g, (lambda t: W.double_gyre_velocity(g, t)), False
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx.append(float(f[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_sample(w, steps: int, threads: int | None = None):
+    """The oracle (CPU restatement of the reference path) on a bounded sample of the
+    workload: the same flow, options, dt, T and h on a coarser grid, one update per step."""
+    from oracle.oracle import Oracle
+    o = Oracle("dp")
+    o.reset()
+    if threads:
+        o.set_threads(threads)
+    nsample = 48 if w["kind"] == "abc" else 128
+    g, vel, steady = make_grid(w, nsample)
+    o.init(g.n, g.x, g.y, g.z, g.flag)
+    for d in w["dirs"]:
+        o.diagnostic_init(d, 0, w["T"], w["h"], f"d{d}")
+    o.set_option("INTEGRATOR", w["integrator"])
+    o.set_option("INTERPOLATOR", w["interpolator"])
+    t = w["t0"]
+    u, v, wv = vel(t)
+    o.update(u, v, wv, t)  # first call: no advection
+    before = o.counter("integrations_fwd") + o.counter("integrations_bkwd")
+    t_start = time.perf_counter()
+    for s in range(steps):
+        t = w["t0"] + (s + 1) * w["dt"]
+        u, v, wv = vel(t)
+        o.update(u, v, wv, t)
+    el = time.perf_counter() - t_start
+    work = o.counter("integrations_fwd") + o.counter("integrations_bkwd") - before
+    assert o.error() == 0, o.error_msg()
+    sample = (f"oracle on {g.n[0]}x{g.n[1]}x{g.n[2]} ({w['desc'].split(',')[0]} coarsened), same dt/T/h/integrator/"
+              f"interpolator, {steps} update(s), {work} grid-pt*RK-steps in {el:.2f} s")
+    return work / el, o.threads(), sample, el
+
+
+def run_reference(args, w):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    steps = max(1, min(args.steps, 3))
+    rate, threads, sample, el = cpu_sample(w, steps)
+    line = {"metric": METRIC, "value": rate, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus, "steps": steps,
+            "warmup": 0, "ms_per_step": 1000.0 * el / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": {"workload": w["desc"], "sample": "coarsened grid, see cpu_baseline"},
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, w):
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    import libcfd2lcs_b200 as L
+    api = L.Cfd2lcs("dp")
+    api.reset()
+    if args.precision == "mixed":
+        api.set_option("MIXED_PRECISION", 1)
+    g, vel, steady = make_grid(w, args.n)
+    api.init(g.n, g.x, g.y, g.z, g.flag)
+    handles = [api.diagnostic_init(d, 0, w["T"], w["h"], f"d{d}") for d in w["dirs"]]
+    api.set_option("INTEGRATOR", w["integrator"])
+    api.set_option("INTERPOLATOR", w["interpolator"])
+    err, msg = api.error()
+    if err:
+        raise RuntimeError(msg)
+    N = int(np.prod(g.n))
+    dev = torch.device("cuda", local)
+    total = args.warmup + args.steps
+
+    def dev_fields(t):
+        u, v, wv = vel(t)
+        return [torch.from_numpy(np.ascontiguousarray(a.ravel(order="F"))).to(dev) for a in (u, v, wv)]
+
+    fields = [dev_fields(w["t0"])] if steady else [dev_fields(w["t0"] + s * w["dt"]) for s in range(total + 1)]
+
+    def step(s):
+        f = fields[0] if steady else fields[s]
+        api.update_device(f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr(), w["t0"] + s * w["dt"])
+
+    step(0)  # first call (no advection)
+    for s in range(1, args.warmup + 1):
+        step(s)
+    err, msg = api.error()
+    if err:
+        raise RuntimeError(msg)
+    frame_ph = api.phase_times_ms()
+    frame_cnt = api.counters()
+    # --- timed region (inputs resident in HBM) ---
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    c0, p0, k0 = api.counters(), api.phase_times_ms(), api.kernel_times()
+    with ClockSampler(local) as clk:
+        for s in range(args.warmup + 1, total + 1):
+            step(s)
+        torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    c1, p1, k1 = api.counters(), api.phase_times_ms(), api.kernel_times()
+    err, msg = api.error()
+    if err:
+        raise RuntimeError(msg)
+    work = (c1["integrations_fwd"] + c1["integrations_bkwd"]) - (c0["integrations_fwd"] + c0["integrations_bkwd"])
+    ms = p1["update_total"] - p0["update_total"]
+    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(ms_t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * work / (ms_max / 1000.0)
+    launches = c1["kernel_launches"] - c0["kernel_launches"]
+    # FTLE-field time: snapshot + composition + FTLE of the frames seen so far
+    frames = c1["ftle_frames"]
+    ftle_ms = (p1["snapshot"] + p1["compose"] + p1["ftle"]) / frames if frames else None
+    # --- end to end: host arrays through cfd2lcs_update_c, FTLE read back each step ---
+    pin = []
+    for s in range(args.steps):
+        t = w["t0"] + (total + 1 + s) * w["dt"]
+        u, v, wv = vel(t)
+        arrs = []
+        for a in (u, v, wv):
+            tt = torch.empty(N, dtype=torch.float64, pin_memory=True)
+            tt.numpy()[:] = a.ravel(order="F")
+            arrs.append(tt)
+        pin.append((t, arrs))
+        if steady:
+            break
+    out = torch.empty(N, dtype=torch.float64, pin_memory=True)
+    nint = np.ascontiguousarray(g.n, dtype=np.int32)
+    ce0 = api.counters()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    t_e0 = time.perf_counter()
+    for s in range(args.steps):
+        tt, arrs = pin[0] if steady else pin[s]
+        tt = w["t0"] + (total + 1 + s) * w["dt"]
+        api.lib.cfd2lcs_update_c(api._p(nint), arrs[0].data_ptr(), arrs[1].data_ptr(), arrs[2].data_ptr(), api.R(tt))
+        for h in handles:
+            api.lib.cfd2lcs_get_ftle_c(int(h), out.data_ptr())
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t_e0
+    et = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(et, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.barrier()
+    ce1 = api.counters()
+    err, msg = api.error()
+    if err:
+        raise RuntimeError(msg)
+    e2e_work = (ce1["integrations_fwd"] + ce1["integrations_bkwd"]) - (ce0["integrations_fwd"] + ce0["integrations_bkwd"])
+    e2e = {"value": world * e2e_work / float(et.item()), "unit": UNIT, "h2d_bytes_per_step": 3 * N * 8,
+           "d2h_bytes_per_step": len(handles) * N * 8}
+    # --- roofline of the dominant kernel (backward SL subcycle) ---
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs")
+    nsl = k1["sl_launches"] - k0["sl_launches"]
+    roof = None
+    if nsl > 0 and hbm:
+        avg_s = (k1["sl_ms"] - k0["sl_ms"]) / nsl / 1000.0
+        achieved = N * sl_bytes_per_point(8) / avg_s / 1e9
+        roof = {"kernel": "k_sl_subcycle", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)", "avg_launch_ms": avg_s * 1000.0,
+                "algorithmic_bytes_per_launch": N * sl_bytes_per_point(8), "traffic": None}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
+            "config": {"workload": w["desc"], "grid": list(g.n), "precision": args.precision, "l2": "inputs larger than L2 (126 MB)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "ftle_field_ms": ftle_ms, "ftle_frames_seen": frames,
+            "slots_composed_per_frame": (c1["slots_composed"] / frames if frames else None),
+            "nsub_per_update": {"fwd": c1["nsub_fwd"], "bkwd": c1["nsub_bkwd"]},
+            "gpu_launches": launches, "e2e": e2e, "roofline": roof}
+    if rank == 0:
+        line["clocks"] = clk.summary()
+        if world == 1 and not args.no_cpu:
+            rate, threads, sample, _ = cpu_sample(w, 1)
+            line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+        print(json.dumps(line), flush=True)
+    api.finalize()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="abc256", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--n", type=int, default=None, help="override the grid size (smaller smoke runs)")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, w)
+    else:
+        run_b200(args, w)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,71 @@
+/*
+ * cfd2lcs_b200.h -- extensions of libcfd2lcs_b200 beyond the reference interface.
+ * Include after cfd2lcs_inc_dp.h or cfd2lcs_inc_sp.h (lcsdata_t comes from there).
+ *
+ * The reference library has no return codes: an error latches a global flag and every
+ * later call returns at once (src/cfd2lcs.f90:684-706).  These entry points keep that
+ * convention and add ways to read the latch and the results (the reference only writes
+ * them to files).
+ */
+#ifndef CFD2LCS_B200_H
+#define CFD2LCS_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Releases all host and device state (the reference's cfd2lcs_finalize,
+ * src/cfd2lcs.f90:388-434, has no _c wrapper in src/cfd2lcs_c.c).  The error latch is
+ * kept, as in the reference. */
+void cfd2lcs_finalize_c(void);
+
+/* Returns the error latch (0: no error) and copies the first error message into msg
+ * (at most len bytes, NUL terminated).  Replaces reading CFD2LCS_ERROR, data_m.f90:380. */
+int cfd2lcs_get_error_c(char *msg, size_t len);
+
+/* Clears the error latch and all state, as a fresh process would start. */
+void cfd2lcs_reset_c(void);
+
+/* Copies the latest FTLE field of a diagnostic (n[0]*n[1]*n[2] values, i fastest) to host
+ * memory.  The reference writes the same field to cfd2lcs_output/ (write_lcs,
+ * src/io_nohdf5_m.f90:47-137).  Returns 0, or 1 for an unknown handle / no field yet. */
+int cfd2lcs_get_ftle_c(int lcs_handle, lcsdata_t *ftle);
+
+/* Copies the composed flow map (displacement form) of the latest FTLE frame: three
+ * consecutive arrays (x, y, z components) of n[0]*n[1]*n[2] values each. */
+int cfd2lcs_get_flowmap_c(int lcs_handle, lcsdata_t *fm);
+
+/* cfd2lcs_update_c with u, v, w already resident in device memory (n[0]*n[1]*n[2] values
+ * each, i fastest, same precision as lcsdata_t); no host copies. */
+void cfd2lcs_update_device_c(int n[3], const lcsdata_t *d_u, const lcsdata_t *d_v, const lcsdata_t *d_w, lcsdata_t time);
+
+/* Device pointer of a diagnostic's latest FTLE field (n[0]*n[1]*n[2] doubles in the dp
+ * build, floats in the sp build), valid until the next update or finalize. */
+const lcsdata_t *cfd2lcs_ftle_device_ptr_c(int lcs_handle);
+
+/* Work counters, as cfd2lcs_info prints them (src/cfd2lcs.f90:754-803):
+ * counters[0] forward particle integrations (grid-pt x subcycles), cumulative
+ * counters[1] backward particle integrations, cumulative
+ * counters[2] subcycles of the last forward update, counters[3] of the last backward update
+ * counters[4] FTLE frames computed, counters[5] updates
+ * counters[6] kernel launches issued, counters[7] sub-flow maps composed */
+void cfd2lcs_get_counters_c(long long counters[8]);
+
+/* Device time (ms, CUDA events on the library's stream), cumulative:
+ * t[0] ingest + padding (+ spline fit of the new velocity), t[1] backward advect,
+ * t[2] forward advect, t[3] ring snapshot, t[4] composition, t[5] FTLE,
+ * t[6] whole updates (first to last event of each update, host waits included). */
+void cfd2lcs_get_phase_times_c(double t[7]);
+
+/* Device time of the hot kernels alone (CUDA events around each launch), cumulative:
+ * t[0] backward semi-Lagrangian subcycle kernels, t[1] forward particle kernels (ms);
+ * n[0], n[1] the number of launches timed. */
+void cfd2lcs_get_kernel_times_c(double t[2], long long n[2]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,218 @@
+"""libcfd2lcs_b200 -- B200-native (sm_100a) FTLE hot path of libcfd2lcs behind its C ABI.
+
+The product is the shared library ``libcfd2lcs_b200_{dp,sp}.so`` (C / Fortran entry points
+of the reference, see include/cfd2lcs_inc_dp.h).  This module is the Python mirror of that
+interface, for tests, benchmarks and Python drivers: the same call names, argument meaning
+and error behaviour as the reference's cfd2lcs_* entry points (src/cfd2lcs_c.c:67-142).
+
+There is no CPU fallback: every call goes through the CUDA library, which latches an error
+(like the reference's CFD2LCS_ERROR) when no GPU is available.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import workloads  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# constants of cfd2lcs_inc_double.h:27-65
+LCS_INTERNAL, LCS_INFLOW, LCS_OUTFLOW, LCS_WALL, LCS_SLIP, LCS_2D, LCS_MASK = range(7)
+FTLE_FWD, FTLE_BKWD, LP_TRACER = 0, 1, 2
+EULER, TRAPEZOIDAL, RK2, RK3, RK4 = 0, 1, 2, 3, 4
+NEAREST_NBR, LINEAR, QUADRATIC, CUBIC, TSE, TSE_LIMIT = 0, 1, 2, 3, 5, 6
+LCS_FALSE, LCS_TRUE = 0, 1
+LCS_NAMELEN = 128
+
+EXPORTED_SYMBOLS = [
+    # reference C interface (src/cfd2lcs_c.c)
+    "cfd2lcs_init_c", "cfd2lcs_diagnostic_init_c", "cfd2lcs_update_c", "cfd2lcs_diagnostic_destroy_c",
+    "cfd2lcs_set_option_c", "cfd2lcs_set_param_c",
+    # reference Fortran interface (src/cfd2lcs.f90), gfortran mangling
+    "cfd2lcs_init_", "cfd2lcs_diagnostic_init_", "cfd2lcs_update_", "cfd2lcs_diagnostic_destroy_",
+    "cfd2lcs_set_option_", "cfd2lcs_set_param_", "cfd2lcs_finalize_",
+    # extensions (include/cfd2lcs_b200.h)
+    "cfd2lcs_finalize_c", "cfd2lcs_get_error_c", "cfd2lcs_reset_c", "cfd2lcs_get_ftle_c", "cfd2lcs_get_flowmap_c",
+    "cfd2lcs_update_device_c", "cfd2lcs_ftle_device_ptr_c", "cfd2lcs_get_counters_c", "cfd2lcs_get_phase_times_c",
+    "cfd2lcs_get_kernel_times_c",
+]
+
+
+def library_path(precision: str = "dp") -> str:
+    return os.path.join(HERE, f"libcfd2lcs_b200_{precision}.so")
+
+
+def build(precisions=("dp", "sp"), force=False):
+    from .build import build as _b
+    return _b(precisions, force=force)
+
+
+_LIBS = {}
+
+
+def load(precision: str = "dp") -> C.CDLL:
+    """Loads the in-tree CUDA library; raises if it has not been built (no fallback)."""
+    if precision in _LIBS:
+        return _LIBS[precision]
+    path = library_path(precision)
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m libcfd2lcs_b200.build` (no CPU fallback exists)")
+    lib = C.CDLL(path)
+    R = C.c_double if precision == "dp" else C.c_float
+    P = C.c_void_p
+    lib.cfd2lcs_init_c.argtypes = [C.c_ssize_t, P, P, P, P, P, P]
+    lib.cfd2lcs_init_c.restype = None
+    lib.cfd2lcs_diagnostic_init_c.argtypes = [C.c_int, C.c_int, R, R, C.c_char_p]
+    lib.cfd2lcs_diagnostic_init_c.restype = C.c_int
+    lib.cfd2lcs_update_c.argtypes = [P, P, P, P, R]
+    lib.cfd2lcs_update_c.restype = None
+    lib.cfd2lcs_update_device_c.argtypes = [P, P, P, P, R]
+    lib.cfd2lcs_update_device_c.restype = None
+    lib.cfd2lcs_diagnostic_destroy_c.argtypes = [C.c_int]
+    lib.cfd2lcs_set_option_c.argtypes = [C.c_char_p, C.c_int]
+    lib.cfd2lcs_set_param_c.argtypes = [C.c_char_p, R]
+    lib.cfd2lcs_finalize_c.restype = None
+    lib.cfd2lcs_reset_c.restype = None
+    lib.cfd2lcs_get_error_c.argtypes = [C.c_char_p, C.c_size_t]
+    lib.cfd2lcs_get_error_c.restype = C.c_int
+    lib.cfd2lcs_get_ftle_c.argtypes = [C.c_int, P]
+    lib.cfd2lcs_get_ftle_c.restype = C.c_int
+    lib.cfd2lcs_get_flowmap_c.argtypes = [C.c_int, P]
+    lib.cfd2lcs_get_flowmap_c.restype = C.c_int
+    lib.cfd2lcs_ftle_device_ptr_c.argtypes = [C.c_int]
+    lib.cfd2lcs_ftle_device_ptr_c.restype = C.c_void_p
+    lib.cfd2lcs_get_counters_c.argtypes = [P]
+    lib.cfd2lcs_get_phase_times_c.argtypes = [P]
+    lib.cfd2lcs_get_kernel_times_c.argtypes = [P, P]
+    lib.cfd2lcs_b200_grid_tables.argtypes = [P, P, P, P, P, P, P, P, P, P, C.c_char_p, C.c_size_t]
+    lib.cfd2lcs_b200_grid_tables.restype = C.c_int
+    _LIBS[precision] = lib
+    return lib
+
+
+class Cfd2lcs:
+    """The reference's entry points on one library instance (process-global state, like the
+    Fortran module globals).  Arrays are numpy arrays of shape (ni, nj, nk); they are
+    passed in Fortran (i-fastest) order."""
+
+    def __init__(self, precision: str = "dp"):
+        self.precision = precision
+        self.lib = load(precision)
+        self.dtype = np.float64 if precision == "dp" else np.float32
+        self.R = C.c_double if precision == "dp" else C.c_float
+        self.n = None
+
+    @staticmethod
+    def _p(a):
+        return a.ctypes.data_as(C.c_void_p)
+
+    def _r(self, a):
+        return np.asfortranarray(a, dtype=self.dtype).ravel(order="F")
+
+    # reference API ---------------------------------------------------------------------
+    def init(self, n, x, y, z, flag, offset=(0, 0, 0), comm: int = 0):
+        n = np.ascontiguousarray(n, dtype=np.int32)
+        off = np.ascontiguousarray(offset, dtype=np.int32)
+        x, y, z = self._r(x), self._r(y), self._r(z)
+        f = np.asfortranarray(flag, dtype=np.int32).ravel(order="F")
+        self.lib.cfd2lcs_init_c(comm, self._p(n), self._p(off), self._p(x), self._p(y), self._p(z), self._p(f))
+        self.n = tuple(int(v) for v in n)
+
+    def diagnostic_init(self, lcs_type, resolution, T, h, label="lcs") -> int:
+        return self.lib.cfd2lcs_diagnostic_init_c(int(lcs_type), int(resolution), self.R(T), self.R(h), label.encode())
+
+    def update(self, u, v, w, time):
+        n = np.ascontiguousarray(self.n if self.n else (0, 0, 0), dtype=np.int32)
+        u, v, w = self._r(u), self._r(v), self._r(w)
+        self.lib.cfd2lcs_update_c(self._p(n), self._p(u), self._p(v), self._p(w), self.R(time))
+
+    def update_device(self, d_u: int, d_v: int, d_w: int, time):
+        """u, v, w already in device memory (raw device pointers, e.g. tensor.data_ptr())."""
+        n = np.ascontiguousarray(self.n, dtype=np.int32)
+        self.lib.cfd2lcs_update_device_c(self._p(n), C.c_void_p(d_u), C.c_void_p(d_v), C.c_void_p(d_w), self.R(time))
+
+    def diagnostic_destroy(self, handle):
+        self.lib.cfd2lcs_diagnostic_destroy_c(int(handle))
+
+    def set_option(self, name: str, val: int):
+        self.lib.cfd2lcs_set_option_c(name.encode(), int(val))
+
+    def set_param(self, name: str, val: float):
+        self.lib.cfd2lcs_set_param_c(name.encode(), self.R(val))
+
+    def finalize(self):
+        self.lib.cfd2lcs_finalize_c()
+
+    # extensions ------------------------------------------------------------------------
+    def reset(self):
+        self.lib.cfd2lcs_reset_c()
+        self.n = None
+
+    def error(self):
+        buf = C.create_string_buffer(512)
+        e = self.lib.cfd2lcs_get_error_c(buf, 512)
+        return e, buf.value.decode()
+
+    def ftle(self, handle):
+        out = np.zeros(int(np.prod(self.n)), dtype=self.dtype)
+        if self.lib.cfd2lcs_get_ftle_c(int(handle), self._p(out)) != 0:
+            raise RuntimeError("no FTLE field for this handle yet")
+        return out.reshape(self.n, order="F")
+
+    def flowmap(self, handle):
+        out = np.zeros(3 * int(np.prod(self.n)), dtype=self.dtype)
+        if self.lib.cfd2lcs_get_flowmap_c(int(handle), self._p(out)) != 0:
+            raise RuntimeError("no flow map for this handle yet")
+        N = int(np.prod(self.n))
+        return np.stack([out[c * N:(c + 1) * N].reshape(self.n, order="F") for c in range(3)])
+
+    def ftle_device_ptr(self, handle) -> int:
+        return int(self.lib.cfd2lcs_ftle_device_ptr_c(int(handle)) or 0)
+
+    def counters(self) -> dict:
+        a = np.zeros(8, dtype=np.int64)
+        self.lib.cfd2lcs_get_counters_c(self._p(a))
+        keys = ["integrations_fwd", "integrations_bkwd", "nsub_fwd", "nsub_bkwd", "ftle_frames", "updates", "kernel_launches",
+                "slots_composed"]
+        return {k: int(v) for k, v in zip(keys, a)}
+
+    def phase_times_ms(self) -> dict:
+        a = np.zeros(7, dtype=np.float64)
+        self.lib.cfd2lcs_get_phase_times_c(self._p(a))
+        keys = ["ingest", "bkwd_advect", "fwd_advect", "snapshot", "compose", "ftle", "update_total"]
+        return {k: float(v) for k, v in zip(keys, a)}
+
+    def kernel_times(self) -> dict:
+        t = np.zeros(2, dtype=np.float64)
+        n = np.zeros(2, dtype=np.int64)
+        self.lib.cfd2lcs_get_kernel_times_c(self._p(t), self._p(n))
+        return dict(sl_ms=float(t[0]), fwd_ms=float(t[1]), sl_launches=int(n[0]), fwd_launches=int(n[1]))
+
+    def grid_tables(self, n, x, y, z, flag):
+        """Host-only grid set-up (no GPU needed): padded coordinates, flags, normals and
+        inverse half spans, shapes (3, ni+2, nj+2, nk+2) etc."""
+        n = np.ascontiguousarray(n, dtype=np.int32)
+        x, y, z = self._r(x), self._r(y), self._r(z)
+        f = np.asfortranarray(flag, dtype=np.int32).ravel(order="F")
+        nt = int(np.prod(np.asarray(n) + 2))
+        xyz = np.zeros(3 * nt, dtype=self.dtype)
+        fl = np.zeros(nt, dtype=np.int32)
+        nrm = np.zeros(3 * nt, dtype=self.dtype)
+        inv = np.zeros(3 * nt, dtype=self.dtype)
+        per = np.zeros(3, dtype=np.int32)
+        msg = C.create_string_buffer(512)
+        rc = self.lib.cfd2lcs_b200_grid_tables(self._p(n), self._p(x), self._p(y), self._p(z), self._p(f), self._p(xyz), self._p(fl),
+                                               self._p(nrm), self._p(inv), self._p(per), msg, 512)
+        if rc != 0:
+            raise ValueError(msg.value.decode())
+        shp = tuple(int(v) + 2 for v in n[::-1])
+        return dict(
+            xyz=xyz.reshape((3,) + shp).transpose(0, 3, 2, 1),
+            flag=fl.reshape(shp).transpose(2, 1, 0),
+            bcnorm=nrm.reshape((3,) + shp).transpose(0, 3, 2, 1),
+            inv_delta=inv.reshape((3,) + shp).transpose(0, 3, 2, 1),
+            periodic=per.astype(bool),
+        )

@@ -1,0 +1,344 @@
+// Point-wise advection pieces shared by the backward semi-Lagrangian kernel, the forward
+// particle kernel and the composition kernel: interpolation stencils (NEAREST, LINEAR,
+// B-spline), the five Runge-Kutta integrators with the reference's stage placement,
+// boundary conditions on particles and the node search.
+#pragma once
+
+#include "device_common.cuh"
+#include "spline.cuh"
+
+namespace cfd2lcs {
+
+// ---------------------------------------------------------------------------------------
+// Trilinear stencil around a node, interp_s2u_r1 LINEAR (src/lp_tracking_m.f90:342-474):
+// per axis the bracket is [no, no+1] when x > line(no), else [no-1, no]; t is clamped to
+// [0,1]; the eight weights are formed as mt*mt*mt ... in the reference's order.
+// ---------------------------------------------------------------------------------------
+template <typename T>
+struct LinStencil {
+  int p0;         // padded index of the lower corner
+  int s[3];       // padded stride of the upper corner along each axis (0 if clamped onto p0)
+  T w[8];
+};
+
+template <typename T>
+__device__ __forceinline__ void lin_stencil(const DevGrid<T> &g, const T x[3], const int no[3], LinStencil<T> &st) {
+  int i0[3];
+  T t[3], mt[3];
+  const int str[3] = {1, g.P.sx, g.P.sxy};
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const T *L = g.li[a];
+    const int n0 = no[a];
+    int lo, hi;
+    if (x[a] > __ldg(L + n0)) {
+      lo = n0;
+      hi = n0 + 1;
+    } else {
+      lo = n0 - 1;
+      hi = n0;
+    }
+    // the reference leaves a bracket outside the padded array undefined; keep it inside
+    lo = min(max(lo, 0), g.P.n[a] + 1);
+    hi = min(max(hi, 0), g.P.n[a] + 1);
+    const T x0 = __ldg(L + lo), x1 = __ldg(L + hi);
+    t[a] = clamp01((x[a] - x0) / (x1 - x0));
+    mt[a] = T(1) - t[a];
+    i0[a] = lo;
+    st.s[a] = (hi - lo) * str[a];
+  }
+  st.p0 = pidx(g.P.sx, g.P.sxy, i0[0], i0[1], i0[2]);
+  st.w[0] = mt[0] * mt[1] * mt[2];
+  st.w[1] = t[0] * mt[1] * mt[2];
+  st.w[2] = mt[0] * t[1] * mt[2];
+  st.w[3] = t[0] * t[1] * mt[2];
+  st.w[4] = mt[0] * mt[1] * t[2];
+  st.w[5] = t[0] * mt[1] * t[2];
+  st.w[6] = mt[0] * t[1] * t[2];
+  st.w[7] = t[0] * t[1] * t[2];
+}
+
+template <typename T>
+__device__ __forceinline__ T lin_apply(const LinStencil<T> &st, const T *__restrict__ f) {
+  const int p = st.p0;
+  const T f0 = __ldg(f + p), f1 = __ldg(f + p + st.s[0]), f2 = __ldg(f + p + st.s[1]), f3 = __ldg(f + p + st.s[0] + st.s[1]);
+  const T f4 = __ldg(f + p + st.s[2]), f5 = __ldg(f + p + st.s[0] + st.s[2]), f6 = __ldg(f + p + st.s[1] + st.s[2]),
+          f7 = __ldg(f + p + st.s[0] + st.s[1] + st.s[2]);
+  return st.w[0] * f0 + st.w[1] * f1 + st.w[2] * f2 + st.w[3] * f3 + st.w[4] * f4 + st.w[5] * f5 + st.w[6] * f6 + st.w[7] * f7;
+}
+
+// time-blended field u = (1-ct) u_n + ct u_np1 sampled at the corners, then trilinear
+template <typename T>
+__device__ __forceinline__ T lin_apply_blend(const LinStencil<T> &st, const T *__restrict__ a, const T *__restrict__ b, T omc,
+                                             T ct) {
+  const int p = st.p0;
+  const int q[8] = {p, p + st.s[0], p + st.s[1], p + st.s[0] + st.s[1], p + st.s[2], p + st.s[0] + st.s[2], p + st.s[1] + st.s[2],
+                    p + st.s[0] + st.s[1] + st.s[2]};
+  T acc = T(0);
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    const T v = omc * __ldg(a + q[c]) + ct * __ldg(b + q[c]);
+    acc = c == 0 ? st.w[0] * v : acc + st.w[c] * v;
+  }
+  return acc;
+}
+
+// ---------------------------------------------------------------------------------------
+// Velocity sampler for one stage: NEAREST, LINEAR or B-spline, blended in time.
+// ---------------------------------------------------------------------------------------
+template <typename T>
+struct VelFields {
+  const T *un[3];
+  const T *unp1[3];
+  const T *cn[3];    // spline coefficients of u_n (INTERP_SPLINE)
+  const T *cnp1[3];  // spline coefficients of u_np1
+};
+
+template <typename T, int INTERP>
+__device__ __forceinline__ void sample_velocity(const DevGrid<T> &g, const SplineAxes<T> &sa, const VelFields<T> &V, const T x[3],
+                                                const int no[3], T ct, T out[3]) {
+  const T omc = T(1) - ct;
+  if (INTERP == INTERP_NEAREST) {
+    const int p = pidx(g.P.sx, g.P.sxy, no[0], no[1], no[2]);
+#pragma unroll
+    for (int c = 0; c < 3; c++) out[c] = omc * __ldg(V.un[c] + p) + ct * __ldg(V.unp1[c] + p);
+  } else if (INTERP == INTERP_LINEAR) {
+    LinStencil<T> st;
+    lin_stencil(g, x, no, st);
+#pragma unroll
+    for (int c = 0; c < 3; c++) out[c] = lin_apply_blend(st, V.un[c], V.unp1[c], omc, ct);
+  } else {
+    SplineStencil<T> st;
+    if (!spline_stencil(g, sa, x, st)) {
+      out[0] = out[1] = out[2] = T(0);
+      return;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) out[c] = omc * spline_apply(g, sa, st, V.cn[c]) + ct * spline_apply(g, sa, st, V.cnp1[c]);
+  }
+}
+
+template <typename T, int INTERP>
+__device__ __forceinline__ void sample_field(const DevGrid<T> &g, const SplineAxes<T> &sa, const T *const f[3], const T x[3],
+                                             const int no[3], T out[3]) {
+  if (INTERP == INTERP_NEAREST) {
+    const int p = pidx(g.P.sx, g.P.sxy, no[0], no[1], no[2]);
+#pragma unroll
+    for (int c = 0; c < 3; c++) out[c] = __ldg(f[c] + p);
+  } else if (INTERP == INTERP_LINEAR) {
+    LinStencil<T> st;
+    lin_stencil(g, x, no, st);
+#pragma unroll
+    for (int c = 0; c < 3; c++) out[c] = lin_apply(st, f[c]);
+  } else {
+    SplineStencil<T> st;
+    if (!spline_stencil(g, sa, x, st)) {
+      out[0] = out[1] = out[2] = T(0);
+      return;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) out[c] = spline_apply(g, sa, st, f[c]);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// One integration step, integrate_lp (src/lp_motion_m.f90:129-360).  ct[] holds the stage
+// time fractions the host computed for this subcycle (clamped, see stage_times()).
+//   EULER       : ct[0]                    TRAPEZOIDAL: ct[0] = midpoint, velocity at xn
+//   RK2         : ct[0] at t, ct[1] at t+dt/2
+//   RK3         : ct[0] at t, ct[1] at t+dt/2, ct[2] at t+dt; stage 3 at xn + 2 k2
+//   RK4         : ct[0] at t, ct[1] = ct[2] at t+dt/2, ct[3] at t+dt
+// ---------------------------------------------------------------------------------------
+struct StageTimes {
+  double ct[4];
+};
+
+template <typename T, int INTEG, int INTERP>
+__device__ __forceinline__ void integrate(const DevGrid<T> &g, const SplineAxes<T> &sa, const VelFields<T> &V, const StageTimes &S,
+                                          T dt, const T xn[3], const int no[3], T x[3]) {
+  const T HALF = T(1) / T(2), THIRD = T(1) / T(3), TWOTHIRD = T(2) / T(3), SIXTH = T(1) / T(6), TWO = T(2);
+  T u[3];
+  if (INTEG == EULER_ || INTEG == TRAPEZOIDAL_) {
+    sample_velocity<T, INTERP>(g, sa, V, xn, no, T(S.ct[0]), u);
+#pragma unroll
+    for (int c = 0; c < 3; c++) x[c] = xn[c] + dt * u[c];
+  } else if (INTEG == RK2_) {
+    sample_velocity<T, INTERP>(g, sa, V, xn, no, T(S.ct[0]), u);
+    T xh[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) xh[c] = xn[c] + HALF * dt * u[c];
+    sample_velocity<T, INTERP>(g, sa, V, xh, no, T(S.ct[1]), u);
+#pragma unroll
+    for (int c = 0; c < 3; c++) x[c] = xn[c] + dt * u[c];
+  } else if (INTEG == RK3_) {
+    T k[3], xs[3], acc[3];
+    sample_velocity<T, INTERP>(g, sa, V, xn, no, T(S.ct[0]), u);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k[c] = dt * u[c];
+      acc[c] = xn[c] + SIXTH * k[c];
+      xs[c] = xn[c] + HALF * k[c];
+    }
+    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[1]), u);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k[c] = dt * u[c];
+      xs[c] = xn[c] + TWO * k[c];
+      acc[c] = acc[c] + TWOTHIRD * k[c];
+    }
+    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[2]), u);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k[c] = dt * u[c];
+      x[c] = acc[c] + SIXTH * k[c];
+    }
+  } else {  // RK4
+    T k[3], xs[3], acc[3];
+    sample_velocity<T, INTERP>(g, sa, V, xn, no, T(S.ct[0]), u);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k[c] = dt * u[c];
+      acc[c] = xn[c] + SIXTH * k[c];
+      xs[c] = xn[c] + HALF * k[c];
+    }
+    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[1]), u);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k[c] = dt * u[c];
+      acc[c] = acc[c] + THIRD * k[c];
+      xs[c] = xn[c] + HALF * k[c];
+    }
+    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[2]), u);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k[c] = dt * u[c];
+      acc[c] = acc[c] + THIRD * k[c];
+      xs[c] = xn[c] + k[c];
+    }
+    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[3]), u);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k[c] = dt * u[c];
+      x[c] = acc[c] + SIXTH * k[c];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Particle boundary conditions.
+// project_lp2plane (src/lp_m.f90:418-538) on a rectilinear 2-D grid: the plane normal is
+// the singleton axis, so only that coordinate moves, x_a - (x_a - x_a(node)).
+// set_lp_bc (src/lp_tracking_m.f90:185-277): the node is clamped to the interior; MASK
+// nodes (and SLIP/WALL nodes on the boundary) project the particle back along bcnorm if
+// it moved outward; INFLOW/OUTFLOW boundary nodes stick it to the node.
+// Returns true when the particle sticks.
+// ---------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void project_plane(const DevGrid<T> &g, int no[3], T x[3]) {
+  const int a = g.P.single_axis;
+  if (a < 0) return;
+  no[a] = 1;
+  const T plane = __ldg(g.lt[a] + 1);
+  T d = x[a] - plane;
+  const T dist = d < T(0) ? -d : d;
+  const T nrm = d < T(0) ? T(-1) : T(1);
+  x[a] = x[a] - dist * nrm;
+}
+
+template <typename T, bool HAS_FLAGS>
+__device__ __forceinline__ bool particle_bc(const DevGrid<T> &g, int no[3], T x[3], int *err) {
+#pragma unroll
+  for (int a = 0; a < 3; a++) no[a] = min(max(no[a], 1), g.P.n[a]);
+  if (!HAS_FLAGS) return false;
+  const int p = pidx(g.P.sx, g.P.sxy, no[0], no[1], no[2]);
+  const int f = g.flag[p];
+  if (f == LCS_INTERNAL || f == LCS_2D) return false;
+  const bool interior = no[0] > 1 && no[1] > 1 && no[2] > 1 && no[0] < g.P.n[0] && no[1] < g.P.n[1] && no[2] < g.P.n[2];
+  if (f == LCS_MASK || f == LCS_SLIP || f == LCS_WALL) {
+    if (f != LCS_MASK && interior) return false;
+    T nx = __ldg(g.nrm[0] + p), ny = __ldg(g.nrm[1] + p), nz = __ldg(g.nrm[2] + p);
+    const T gx = __ldg(g.lt[0] + no[0]), gy = __ldg(g.lt[1] + no[1]), gz = __ldg(g.lt[2] + no[2]);
+    const T dist = (x[0] - gx) * nx + (x[1] - gy) * ny + (x[2] - gz) * nz;
+    if (dist > T(0)) {
+      x[0] = x[0] - nx * dist;
+      x[1] = x[1] - ny * dist;
+      x[2] = x[2] - nz * dist;
+    }
+    return false;
+  }
+  if (f == LCS_INFLOW || f == LCS_OUTFLOW) {
+    if (interior) return false;
+    x[0] = __ldg(g.lt[0] + no[0]);
+    x[1] = __ldg(g.lt[1] + no[1]);
+    x[2] = __ldg(g.lt[2] + no[2]);
+    return true;
+  }
+  atomicOr(err, ERR_UNKNOWN_FLAG);
+  return false;
+}
+
+// ---------------------------------------------------------------------------------------
+// Node search, track_lp2node (src/lp_tracking_m.f90:16-183): one pass looks at the 27
+// neighbours (fewer on a 2-D grid) in NBR_OFFSET order (src/data_m.f90:124-152) and moves
+// to one that is closer than 0.99 of the best so far.
+// ---------------------------------------------------------------------------------------
+__constant__ int8_t c_nbr[27][3] = {
+    {0, 0, 0},   {-1, 0, 0},  {0, -1, 0}, {0, 0, -1}, {1, 0, 0},  {0, 1, 0},  {0, 0, 1},   {-1, -1, -1}, {0, -1, -1},
+    {1, -1, -1}, {-1, 0, -1}, {1, 0, -1}, {-1, 1, -1}, {0, 1, -1}, {1, 1, -1}, {-1, -1, 0}, {1, -1, 0},  {-1, 1, 0},
+    {1, 1, 0},   {-1, -1, 1}, {0, -1, 1}, {1, -1, 1},  {-1, 0, 1}, {1, 0, 1},  {-1, 1, 1},  {0, 1, 1},   {1, 1, 1}};
+
+template <typename T>
+__device__ __forceinline__ bool track_pass(const DevGrid<T> &g, const T x[3], int no[3]) {
+  T best = T(0);
+  bool have = false;
+  int off[3] = {0, 0, 0};
+  const int sa = g.P.single_axis;
+  for (int nb = 0; nb < 27; nb++) {
+    const int o0 = c_nbr[nb][0], o1 = c_nbr[nb][1], o2 = c_nbr[nb][2];
+    if ((sa == 0 && o0 != 0) || (sa == 1 && o1 != 0) || (sa == 2 && o2 != 0)) continue;
+    const int i = min(max(no[0] + o0, 0), g.P.n[0] + 1);
+    const int j = min(max(no[1] + o1, 0), g.P.n[1] + 1);
+    const int k = min(max(no[2] + o2, 0), g.P.n[2] + 1);
+    const T ex = node_coord(g, 0, i, j, k) - x[0];
+    const T ey = node_coord(g, 1, i, j, k) - x[1];
+    const T ez = node_coord(g, 2, i, j, k) - x[2];
+    const T r = ex * ex + ey * ey + ez * ez;
+    // rsq < 0.99*rsq_min with rsq_min starting at huge()
+    if (!have || r < T(0.99) * best) {
+      best = r;
+      have = true;
+      off[0] = o0;
+      off[1] = o1;
+      off[2] = o2;
+    }
+  }
+  no[0] += off[0];
+  no[1] += off[1];
+  no[2] += off[2];
+  return off[0] != 0 || off[1] != 0 || off[2] != 0;
+}
+
+// exchange_lpdata on one rank (src/comms_m.f90:872-1189): a particle whose node left the
+// interior through a periodic direction is shifted by that direction's periodic shift and
+// its node indices are wrapped.
+template <typename T>
+__device__ __forceinline__ void wrap_particle(const DevGrid<T> &g, T x[3], int no[3]) {
+  int d[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) d[a] = no[a] < 1 ? -1 : (no[a] > g.P.n[a] ? 1 : 0);
+  if (d[0] == 0 && d[1] == 0 && d[2] == 0) return;
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+    if (d[a] != 0 && !g.P.per[a]) return;
+  const T *s = g.P.ps[(d[2] + 1) * 9 + (d[1] + 1) * 3 + (d[0] + 1)];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    x[a] = x[a] + s[a];
+    int v = no[a];
+    if (v > g.P.n[a]) v -= g.P.n[a];
+    if (v < 1) v += g.P.n[a];
+    no[a] = v;
+  }
+}
+
+}  // namespace cfd2lcs

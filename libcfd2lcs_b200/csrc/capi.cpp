@@ -1,0 +1,306 @@
+// C ABI of libcfd2lcs_b200: the reference's C entry points (src/cfd2lcs_c.c:67-142), the
+// gfortran-mangled Fortran entry points (src/cfd2lcs.f90:2-682, external subroutines
+// cfd2lcs_*_ with by-reference arguments and hidden character lengths), and the
+// extensions declared in include/cfd2lcs_b200.h.
+//
+// Error convention as in the reference (src/cfd2lcs.f90:684-706): no return codes; the
+// first error latches a flag, is reported once on stdout, and every later call returns
+// immediately.
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "engine.h"
+
+using cfd2lcs::Counters;
+using cfd2lcs::EngineBase;
+using cfd2lcs::Options;
+
+#define CFD2LCS_EXPORT extern "C" __attribute__((visibility("default")))
+
+namespace {
+
+enum { LCS_FALSE = 0, LCS_TRUE = 1 };
+enum { NEAREST_NBR = 0, LINEAR = 1, QUADRATIC = 2, CUBIC = 3, TSE = 5, TSE_LIMIT = 6 };
+enum { EULER = 0, TRAPEZOIDAL = 1, RK2 = 2, RK3 = 3, RK4 = 4 };
+
+struct Library {
+  int error = 0;
+  std::string msg;
+  Options opt;
+  std::unique_ptr<EngineBase> eng;
+  bool inited = false;
+  Counters zero;
+};
+
+Library &L() {
+  static Library lib;
+  return lib;
+}
+
+bool quiet() {
+  const char *q = std::getenv("CFD2LCS_B200_QUIET");
+  return q && q[0] && q[0] != '0';
+}
+
+void latch(const std::string &m) {
+  Library &lib = L();
+  if (!lib.error) {
+    lib.msg = m;
+    if (!quiet()) std::printf("ERROR (libcfd2lcs_b200): %s\nFATAL CFD2LCS_ERROR DETECTED, WILL NOT PERFORM LCS COMPUTATIONS\n", m.c_str());
+  }
+  lib.error = 1;
+}
+
+// Fortran character argument: trailing blanks are insignificant (trim()).  The reference's
+// C shim passes the length as int while gfortran >= 8 reads size_t; only the low 32 bits
+// are used and the string is also bounded by a NUL.
+std::string fstr(const char *s, size_t len) {
+  size_t n = (size_t)(uint32_t)len;
+  n = strnlen(s, n);
+  while (n > 0 && s[n - 1] == ' ') n--;
+  return std::string(s, n);
+}
+
+void do_init(const int *n, const int *offset, const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, const int *flag) {
+  (void)offset;  // one rank: offsets are normalised to 0 (src/sgrid_m.f90:90-93)
+  Library &lib = L();
+  if (lib.error) return;
+  lib.eng.reset();
+  lib.inited = false;
+  lib.eng = cfd2lcs::make_engine(&lib.opt);
+  std::string msg;
+  if (!lib.eng->init(n, x, y, z, flag, msg)) {
+    lib.eng.reset();
+    latch(msg);
+    return;
+  }
+  lib.inited = true;
+}
+
+int do_diagnostic_init(int type, int resolution, lcsdata_t T, lcsdata_t h, const char *label) {
+  Library &lib = L();
+  if (lib.error) return -1;
+  if (!lib.inited) {
+    latch("cfd2lcs_diagnostic_init called before cfd2lcs_init");
+    return -1;
+  }
+  std::string msg;
+  const int id = lib.eng->diagnostic_init(type, resolution, T, h, label, msg);
+  if (id < 0) latch(msg);
+  return id;
+}
+
+void do_update(const int *n, const lcsdata_t *u, const lcsdata_t *v, const lcsdata_t *w, lcsdata_t time, bool dev) {
+  Library &lib = L();
+  if (lib.error) return;
+  if (!lib.inited) {
+    latch("update: received velocity array of incorrect dimension (cfd2lcs_init was not called)");
+    return;
+  }
+  std::string msg;
+  if (!lib.eng->update(n, u, v, w, time, dev, msg)) latch(msg);
+}
+
+// cfd2lcs_set_option, src/cfd2lcs.f90:436-622
+void do_set_option(const std::string &opt, int val) {
+  Library &lib = L();
+  if (lib.error) return;
+  const bool tf = (val == LCS_TRUE || val == LCS_FALSE);
+  bool ok = true;
+  if (opt == "SYNCTIMER" || opt == "DEBUG" || opt == "WRITE_FLOWMAP" || opt == "WRITE_VELOCITY" || opt == "WRITE_BCFLAG") {
+    ok = tf;  // timing / verbosity / output switches: accepted, no effect on the results
+  } else if (opt == "VELOCITY_INVARIANTS") {
+    ok = tf;
+    if (ok) lib.opt.velocity_invariants = val;
+  } else if (opt == "INCOMPRESSIBLE") {
+    ok = tf;
+    if (ok) lib.opt.incompressible = val;
+  } else if (opt == "AUX_GRID") {
+    ok = tf;
+    if (ok && val == LCS_TRUE) {
+      latch("AUX_GRID = TRUE (auxiliary-grid Cauchy-Green gradient) is not supported by this library");
+      return;
+    }
+    if (ok) lib.opt.aux_grid = val;
+  } else if (opt == "UPDATE_FREQ") {
+    ok = true;
+  } else if (opt == "INTERPOLATOR") {
+    ok = val == NEAREST_NBR || val == LINEAR || val == QUADRATIC || val == CUBIC || val == TSE || val == TSE_LIMIT;
+    lib.opt.interpolator = val;  // assigned even for a bad value, as the reference does (:584)
+  } else if (opt == "INTEGRATOR") {
+    ok = val >= EULER && val <= RK4;
+    lib.opt.integrator = val;
+  } else if (opt == "MIXED_PRECISION") {  // extension: select the FP32-compensated form
+    ok = tf;
+    if (ok && lib.inited) {
+      latch("MIXED_PRECISION must be set before cfd2lcs_init");
+      return;
+    }
+    if (ok) lib.opt.mixed_precision = val;
+  } else {
+    ok = false;
+  }
+  if (!ok) latch("ERROR, bad libcfd2lcs option/val combination: " + opt + "," + std::to_string(val));
+}
+
+// cfd2lcs_set_param, src/cfd2lcs.f90:624-682
+void do_set_param(const std::string &p, lcsdata_t val) {
+  Library &lib = L();
+  if (lib.error) return;
+  if (p == "CFL") lib.opt.cfl = (double)val;
+  else if (p == "TRACER_INJECT_X" || p == "TRACER_INJECT_Y" || p == "TRACER_INJECT_Z" || p == "TRACER_INJECT_RADIUS") {
+  } else latch("ERROR, unknown libcfd2lcs parameter: " + p);
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------------- C interface
+CFD2LCS_EXPORT void cfd2lcs_init_c(intptr_t usercomm, int n[3], int offset[3], lcsdata_t *x, lcsdata_t *y, lcsdata_t *z, int *flag) {
+  (void)usercomm;  // MPI_Comm by value (int or pointer, depending on the MPI); one rank
+  do_init(n, offset, x, y, z, flag);
+}
+
+CFD2LCS_EXPORT int cfd2lcs_diagnostic_init_c(int lcs_type, int resolution, lcsdata_t t, lcsdata_t h, char label[]) {
+  return do_diagnostic_init(lcs_type, resolution, t, h, label);
+}
+
+CFD2LCS_EXPORT void cfd2lcs_update_c(int n[3], lcsdata_t *u, lcsdata_t *v, lcsdata_t *w, lcsdata_t time) {
+  do_update(n, u, v, w, time, false);
+}
+
+CFD2LCS_EXPORT void cfd2lcs_diagnostic_destroy_c(int lcs_handle) {
+  (void)lcs_handle;  // a no-op in the reference (src/cfd2lcs.f90:360-386)
+}
+
+CFD2LCS_EXPORT void cfd2lcs_set_option_c(char option[], int val) { do_set_option(fstr(option, std::strlen(option)), val); }
+
+CFD2LCS_EXPORT void cfd2lcs_set_param_c(char param[], lcsdata_t val) { do_set_param(fstr(param, std::strlen(param)), val); }
+
+// ----------------------------------------------------------------------- Fortran interface
+CFD2LCS_EXPORT void cfd2lcs_init_(int *cfdcomm, int *n, int *offset, lcsdata_t *x, lcsdata_t *y, lcsdata_t *z, int *flag) {
+  (void)cfdcomm;
+  do_init(n, offset, x, y, z, flag);
+}
+
+CFD2LCS_EXPORT void cfd2lcs_diagnostic_init_(int *lcs_handle, int *lcs_type, int *resolution, lcsdata_t *T, lcsdata_t *h, char *label,
+                                             size_t label_len) {
+  const std::string lab = fstr(label, label_len);
+  const int id = do_diagnostic_init(*lcs_type, *resolution, *T, *h, lab.c_str());
+  if (lcs_handle) *lcs_handle = id;
+}
+
+CFD2LCS_EXPORT void cfd2lcs_update_(int *n, lcsdata_t *ux, lcsdata_t *uy, lcsdata_t *uz, lcsdata_t *time) {
+  do_update(n, ux, uy, uz, *time, false);
+}
+
+CFD2LCS_EXPORT void cfd2lcs_diagnostic_destroy_(int *lcs_handle) { (void)lcs_handle; }
+
+CFD2LCS_EXPORT void cfd2lcs_set_option_(char *option, int *val, size_t len) { do_set_option(fstr(option, len), *val); }
+
+CFD2LCS_EXPORT void cfd2lcs_set_param_(char *param, lcsdata_t *val, size_t len) { do_set_param(fstr(param, len), *val); }
+
+CFD2LCS_EXPORT void cfd2lcs_finalize_(void) {
+  Library &lib = L();
+  if (lib.error) return;
+  lib.eng.reset();
+  lib.inited = false;
+}
+
+// ----------------------------------------------------------------------- extensions
+CFD2LCS_EXPORT void cfd2lcs_finalize_c(void) { cfd2lcs_finalize_(); }
+
+CFD2LCS_EXPORT int cfd2lcs_get_error_c(char *msg, size_t len) {
+  Library &lib = L();
+  if (!lib.error && lib.eng) {
+    std::string m;
+    if (!lib.eng->sync_errors(m)) latch(m);
+  }
+  if (msg && len > 0) {
+    std::strncpy(msg, lib.msg.c_str(), len - 1);
+    msg[len - 1] = 0;
+  }
+  return lib.error;
+}
+
+CFD2LCS_EXPORT void cfd2lcs_reset_c(void) {
+  Library &lib = L();
+  lib.eng.reset();
+  lib.inited = false;
+  lib.error = 0;
+  lib.msg.clear();
+  lib.opt = Options();
+}
+
+CFD2LCS_EXPORT int cfd2lcs_get_ftle_c(int lcs_handle, lcsdata_t *ftle) {
+  Library &lib = L();
+  if (!lib.eng) return 1;
+  std::string m;
+  return lib.eng->get_ftle(lcs_handle, ftle, m) ? 0 : 1;
+}
+
+CFD2LCS_EXPORT int cfd2lcs_get_flowmap_c(int lcs_handle, lcsdata_t *fm) {
+  Library &lib = L();
+  if (!lib.eng) return 1;
+  std::string m;
+  return lib.eng->get_flowmap(lcs_handle, fm, m) ? 0 : 1;
+}
+
+CFD2LCS_EXPORT void cfd2lcs_update_device_c(int n[3], const lcsdata_t *d_u, const lcsdata_t *d_v, const lcsdata_t *d_w, lcsdata_t time) {
+  do_update(n, d_u, d_v, d_w, time, true);
+}
+
+CFD2LCS_EXPORT const lcsdata_t *cfd2lcs_ftle_device_ptr_c(int lcs_handle) {
+  Library &lib = L();
+  return lib.eng ? lib.eng->ftle_device_ptr(lcs_handle) : nullptr;
+}
+
+CFD2LCS_EXPORT void cfd2lcs_get_counters_c(long long c[8]) {
+  Library &lib = L();
+  const Counters &k = lib.eng ? lib.eng->counters() : lib.zero;
+  c[0] = k.integrations_fwd;
+  c[1] = k.integrations_bkwd;
+  c[2] = k.nsub_fwd;
+  c[3] = k.nsub_bkwd;
+  c[4] = k.ftle_frames;
+  c[5] = k.updates;
+  c[6] = k.kernel_launches;
+  c[7] = k.slots_composed;
+}
+
+CFD2LCS_EXPORT void cfd2lcs_get_phase_times_c(double t[7]) {
+  Library &lib = L();
+  const Counters &k = lib.eng ? lib.eng->counters() : lib.zero;
+  for (int q = 0; q < 7; q++) t[q] = k.phase_ms[q];
+}
+
+// Event-timed hot kernels: t[0] backward SL subcycle kernels (ms, cumulative),
+// t[1] forward particle kernels; n[0], n[1] their launch counts.
+CFD2LCS_EXPORT void cfd2lcs_get_kernel_times_c(double t[2], long long n[2]) {
+  Library &lib = L();
+  const Counters &k = lib.eng ? lib.eng->counters() : lib.zero;
+  t[0] = k.sl_kernel_ms;
+  t[1] = k.fwd_kernel_ms;
+  n[0] = k.sl_kernel_launches;
+  n[1] = k.fwd_kernel_launches;
+}
+
+// Host-only grid set-up (no device work): the padded coordinates, flags, boundary normals
+// and inverse half spans the library derives at init.  Used to check the host logic on
+// machines without a GPU.  Returns 0 on success.
+CFD2LCS_EXPORT int cfd2lcs_b200_grid_tables(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, const int *flag,
+                                            lcsdata_t *xyz_pad, int *flag_pad, lcsdata_t *nrm_pad, lcsdata_t *inv_delta, int *per,
+                                            char *msg, size_t len) {
+  Options o;
+  std::unique_ptr<EngineBase> e = cfd2lcs::make_engine(&o);
+  std::string m;
+  const bool ok = e->host_grid_tables(n, x, y, z, flag, xyz_pad, flag_pad, nrm_pad, inv_delta, per, m);
+  if (msg && len > 0) {
+    std::strncpy(msg, m.c_str(), len - 1);
+    msg[len - 1] = 0;
+  }
+  return ok ? 0 : 1;
+}

@@ -1,0 +1,783 @@
+// Host orchestration of the device path: init (grid tables to HBM), diagnostic init,
+// and the per-update sequence of cfd2lcs_update (src/cfd2lcs.f90:55-250).
+#include "engine.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+
+#include "grid.h"
+#include "kernels.cuh"
+#include "spline_host.h"
+
+namespace cfd2lcs {
+
+namespace {
+
+enum { FTLE_FWD = 0, FTLE_BKWD = 1, LP_TRACER = 2 };
+enum { NEAREST_NBR = 0, LINEAR = 1, QUADRATIC = 2, CUBIC = 3, TSE = 5, TSE_LIMIT = 6 };
+
+#define CK(call)                                                                                 \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess) {                                                                     \
+      msg = std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " + #call;               \
+      return false;                                                                              \
+    }                                                                                            \
+  } while (0)
+
+// Fortran NINT
+inline long fnint(double v) { return v >= 0 ? (long)std::floor(v + 0.5) : -(long)std::floor(-v + 0.5); }
+
+// Device allocations released together with the engine.
+class DevArena {
+ public:
+  ~DevArena() { release(); }
+  void release() {
+    for (void *p : ptrs_) cudaFree(p);
+    ptrs_.clear();
+  }
+  template <typename X>
+  X *alloc(size_t n, std::string &msg) {
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, n * sizeof(X) > 0 ? n * sizeof(X) : 1);
+    if (e != cudaSuccess) {
+      msg = std::string("device allocation failed: ") + cudaGetErrorString(e);
+      return nullptr;
+    }
+    ptrs_.push_back(p);
+    return static_cast<X *>(p);
+  }
+
+ private:
+  std::vector<void *> ptrs_;
+};
+
+template <typename T>
+struct SplineSet {
+  int deg = 0;
+  SplineAxes<T> axes{};
+};
+
+template <typename T>
+struct Diag {
+  int handle = 0, type = 0;
+  lcsdata_t T_ = 0, h = 0, dt_factor = 1;
+  int nslot = 0;
+  // backward: working flow map (double buffered, padded)
+  T *fm[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  int cur = 0;
+  T *fmcoef[3] = {nullptr, nullptr, nullptr};
+  // forward: particles
+  Particles<T> P{};
+  // ring of sub-flow maps (padded) and their spline coefficients
+  std::vector<T *> slot;      // 3 per slot
+  std::vector<T *> slotcoef;  // 3 per slot (allocated on first spline use)
+  std::vector<int> written, coef_deg;
+  T **slot_list_dev = nullptr;  // pointers of the slots used by one composition
+  std::vector<T *> slot_list_host;
+  T *composed[3] = {nullptr, nullptr, nullptr};  // interior, last FTLE frame
+  lcsdata_t *ftle = nullptr;                      // interior
+  bool have_frame = false;
+};
+
+}  // namespace
+
+template <typename T>
+class Engine : public EngineBase {
+ public:
+  explicit Engine(const Options *opt) : opt_(opt) {}
+  ~Engine() override {
+    if (stream_) cudaStreamSynchronize(stream_);
+    arena_.release();
+    for (auto &e : ev_) cudaEventDestroy(e);
+    for (auto &e : kev_) cudaEventDestroy(e);
+    if (red_host_) cudaFreeHost(red_host_);
+    if (stream_) cudaStreamDestroy(stream_);
+  }
+
+  bool host_grid_tables(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, const int *flag, lcsdata_t *xyz,
+                        int *flag_pad, lcsdata_t *nrm, lcsdata_t *invd, int *per, std::string &msg) override {
+    HostGrid<lcsdata_t> g;
+    if (!g.build(n, x, y, z, flag)) {
+      msg = g.error;
+      return false;
+    }
+    const long nt = g.ntot();
+    for (int k = 0; k <= n[2] + 1; k++)
+      for (int j = 0; j <= n[1] + 1; j++)
+        for (int i = 0; i <= n[0] + 1; i++) {
+          const long p = g.pidx(i, j, k);
+          for (int c = 0; c < 3; c++) {
+            if (xyz) xyz[c * nt + p] = g.coord(c, i, j, k);
+            if (nrm) nrm[c * nt + p] = g.bcnorm.empty() ? lcsdata_t(0) : g.bcnorm[(size_t)c * nt + p];
+          }
+          if (flag_pad) flag_pad[p] = g.flag.empty() ? 0 : g.flag[p];
+          if (invd) {
+            const bool inside = i >= 1 && j >= 1 && k >= 1 && i <= n[0] && j <= n[1] && k <= n[2];
+            const int idx[3] = {i, j, k};
+            for (int a = 0; a < 3; a++) {
+              lcsdata_t v = 0;
+              if (inside) {
+                const int b = (a + 1) % 3, c = (a + 2) % 3;
+                const int cb = (idx[b] - 1 == 0 ? 1 : 0) | (idx[b] + 1 == n[b] + 1 ? 2 : 0);
+                const int cc = (idx[c] - 1 == 0 ? 1 : 0) | (idx[c] + 1 == n[c] + 1 ? 2 : 0);
+                v = g.invd[a][((size_t)idx[a] * 4 + cb) * 4 + cc];
+              }
+              invd[a * nt + p] = v;
+            }
+          }
+        }
+    if (per)
+      for (int a = 0; a < 3; a++) per[a] = g.P.per[a];
+    return true;
+  }
+
+  bool init(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, const int *flag, std::string &msg) override {
+    if (!hg_.build(n, x, y, z, flag)) {
+      msg = hg_.error;
+      return false;
+    }
+    CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    for (int e = 0; e < 10; e++) {
+      cudaEvent_t ev;
+      CK(cudaEventCreate(&ev));
+      ev_.push_back(ev);
+    }
+    CK(cudaMallocHost(&red_host_, sizeof(DevReduce)));
+    for (int a = 0; a < 3; a++) n_[a] = n[a];
+    N_ = (long)n[0] * n[1] * n[2];
+    ntot_ = hg_.ntot();
+    // grid tables
+    GridParams<T> P;
+    const GridParams<lcsdata_t> &H = hg_.P;
+    for (int a = 0; a < 3; a++) {
+      P.n[a] = H.n[a];
+      P.per[a] = H.per[a];
+      for (int s = 0; s < 2; s++)
+        for (int e = 0; e < 2; e++) P.gx[a][s][e] = (T)H.gx[a][s][e];
+    }
+    P.sx = H.sx;
+    P.sxy = H.sxy;
+    P.single_axis = H.single_axis;
+    P.zquirk = H.zquirk;
+    for (int q = 0; q < 6; q++) P.bb[q] = (T)H.bb[q];
+    for (int d = 0; d < 27; d++)
+      for (int c = 0; c < 3; c++) P.ps[d][c] = (T)H.ps[d][c];
+    P.has_flags = H.has_flags;
+    P.maxtrack = H.maxtrack;
+    dg_.P = P;
+    for (int a = 0; a < 3; a++) {
+      if (!(dg_.lt[a] = upload(hg_.lt[a], msg))) return false;
+      if (!(dg_.li[a] = upload(hg_.li[a], msg))) return false;
+      if (!(dg_.invd[a] = upload(hg_.invd[a], msg))) return false;
+    }
+    dg_.flag = nullptr;
+    for (int a = 0; a < 3; a++) dg_.nrm[a] = nullptr;
+    if (H.has_flags) {
+      int8_t *f = arena_.alloc<int8_t>(hg_.flag.size(), msg);
+      if (!f) return false;
+      CK(cudaMemcpy(f, hg_.flag.data(), hg_.flag.size(), cudaMemcpyHostToDevice));
+      dg_.flag = f;
+      if (!hg_.bcnorm.empty()) {
+        for (int a = 0; a < 3; a++) {
+          std::vector<lcsdata_t> comp(hg_.bcnorm.begin() + (size_t)a * ntot_, hg_.bcnorm.begin() + (size_t)(a + 1) * ntot_);
+          if (!(dg_.nrm[a] = upload(comp, msg))) return false;
+        }
+      } else {
+        // flags without normals (e.g. only INFLOW/OUTFLOW or 2-D): a zero field keeps the
+        // kernels free of null checks
+        std::vector<lcsdata_t> zero(ntot_, lcsdata_t(0));
+        T *z0 = upload(zero, msg);
+        if (!z0) return false;
+        for (int a = 0; a < 3; a++) dg_.nrm[a] = z0;
+      }
+    }
+    // velocity levels (zero-initialised, as init_sr1 does, src/structured_m.f90:73-96)
+    for (int l = 0; l < 2; l++)
+      for (int c = 0; c < 3; c++) {
+        if (!(u_[l][c] = arena_.alloc<T>(ntot_, msg))) return false;
+        CK(cudaMemsetAsync(u_[l][c], 0, ntot_ * sizeof(T), stream_));
+      }
+    if (!(stage_ = arena_.alloc<lcsdata_t>((size_t)3 * N_, msg))) return false;
+    if (!(red_ = arena_.alloc<DevReduce>(1, msg))) return false;
+    CK(cudaMemsetAsync(red_, 0, sizeof(DevReduce), stream_));
+    CK(cudaStreamSynchronize(stream_));
+    first_call_ = true;
+    return true;
+  }
+
+  int diagnostic_init(int type, int resolution, lcsdata_t Tint, lcsdata_t h, const char *label, std::string &msg) override {
+    (void)label;
+    if (resolution != 0) {
+      msg = "diagnostic_init: resolution /= 0 (a refined lcs grid, new_sgrid_from_sgrid) is not supported";
+      return -1;
+    }
+    if (type == LP_TRACER) {
+      msg = "diagnostic_init: LP_TRACER is not supported by this library";
+      return -1;
+    }
+    if (type != FTLE_FWD && type != FTLE_BKWD) {
+      msg = "ERROR, bad specification for lcs_type. Options are: FTLE_FWD, FTLE_BKWD, LP_TRACER";
+      return -1;
+    }
+    if (!(h > lcsdata_t(0)) || !(Tint > lcsdata_t(0))) {
+      msg = "diagnostic_init: T and h must be positive";
+      return -1;
+    }
+    Diag<T> d;
+    d.handle = (int)diags_.size() + 1;
+    d.type = type;
+    d.T_ = Tint;
+    d.h = h;
+    d.dt_factor = type == FTLE_BKWD ? lcsdata_t(1) / lcsdata_t(std::max(1 + resolution, 1)) : lcsdata_t(1);
+    d.nslot = (int)std::max(1L, fnint((double)(Tint / h)));
+    if (type == FTLE_BKWD) {
+      for (int b = 0; b < 2; b++)
+        for (int c = 0; c < 3; c++) {
+          if (!(d.fm[b][c] = arena_.alloc<T>(ntot_, msg))) return -1;
+          if (cudaMemsetAsync(d.fm[b][c], 0, ntot_ * sizeof(T), stream_) != cudaSuccess) return fail(msg, "memset");
+        }
+    } else {
+      for (int c = 0; c < 3; c++) {
+        if (!(d.P.x[c] = arena_.alloc<T>(N_, msg))) return -1;
+        if (!(d.P.dx[c] = arena_.alloc<T>(N_, msg))) return -1;
+        if (!(d.P.no[c] = arena_.alloc<int>(N_, msg))) return -1;
+      }
+      launch_reset(d);
+    }
+    d.slot.assign((size_t)3 * d.nslot, nullptr);
+    d.slotcoef.assign((size_t)3 * d.nslot, nullptr);
+    d.written.assign(d.nslot, 0);
+    d.coef_deg.assign(d.nslot, 0);
+    for (int s = 0; s < 3 * d.nslot; s++)
+      if (!(d.slot[s] = arena_.alloc<T>(ntot_, msg))) return -1;
+    if (!(d.slot_list_dev = arena_.alloc<T *>((size_t)3 * d.nslot, msg))) return -1;
+    d.slot_list_host.assign((size_t)3 * d.nslot, nullptr);
+    for (int c = 0; c < 3; c++)
+      if (!(d.composed[c] = arena_.alloc<T>(N_, msg))) return -1;
+    if (!(d.ftle = arena_.alloc<lcsdata_t>(N_, msg))) return -1;
+    if (cudaStreamSynchronize(stream_) != cudaSuccess) return fail(msg, "sync");
+    diags_.push_back(d);
+    return d.handle;
+  }
+
+  bool update(const int n[3], const lcsdata_t *u, const lcsdata_t *v, const lcsdata_t *w, lcsdata_t time, bool device_ptrs,
+              std::string &msg) override {
+    if (n[0] != n_[0] || n[1] != n_[1] || n[2] != n_[2]) {
+      msg = "update: received velocity array of incorrect dimension";
+      return false;
+    }
+    if (first_call_) {
+      t_n_ = time;
+      t_np1_ = time;
+      first_call_ = false;
+    } else {
+      t_n_ = t_np1_;
+      t_np1_ = time;
+    }
+    cur_ ^= 1;  // u_n = u_np1 (buffer swap); u_np1 is rewritten below
+    const int interp = opt_->interpolator;
+    if (interp == TSE || interp == TSE_LIMIT) {
+      msg = "update: TSE / TSE_LIMIT interpolation (non-rectilinear grids) is not supported";
+      return false;
+    }
+    if (interp != NEAREST_NBR && interp != LINEAR && interp != QUADRATIC && interp != CUBIC) {
+      msg = "ERROR: Unrecognized interpolator";
+      return false;
+    }
+    // --- K0 ingest --------------------------------------------------------------------
+    CK(cudaEventRecord(ev_[8], stream_));
+    CK(cudaEventRecord(ev_[0], stream_));
+    const lcsdata_t *su = u, *sv = v, *sw = w;
+    if (!device_ptrs) {
+      CK(cudaMemcpyAsync(stage_, u, N_ * sizeof(lcsdata_t), cudaMemcpyHostToDevice, stream_));
+      CK(cudaMemcpyAsync(stage_ + N_, v, N_ * sizeof(lcsdata_t), cudaMemcpyHostToDevice, stream_));
+      CK(cudaMemcpyAsync(stage_ + 2 * N_, w, N_ * sizeof(lcsdata_t), cudaMemcpyHostToDevice, stream_));
+      su = stage_;
+      sv = stage_ + N_;
+      sw = stage_ + 2 * N_;
+    }
+    DevReduce init{};
+    init.cmax = 0ull;
+    double big = std::numeric_limits<double>::max();
+    std::memcpy(&init.cmin, &big, sizeof(double));
+    init.err = red_err_;
+    *red_host_ = init;
+    CK(cudaMemcpyAsync(red_, red_host_, sizeof(DevReduce), cudaMemcpyHostToDevice, stream_));
+    {
+      const dim3 blk(32, 8, 1), grd((n_[0] + 31) / 32, (n_[1] + 7) / 8, n_[2]);
+      T *const *U = u_[cur_];
+      counters_.kernel_launches++;
+      if (dg_.P.has_flags)
+        k_ingest<T, lcsdata_t, true><<<grd, blk, 0, stream_>>>(dg_, su, sv, sw, U[0], U[1], U[2], red_);
+      else
+        k_ingest<T, lcsdata_t, false><<<grd, blk, 0, stream_>>>(dg_, su, sv, sw, U[0], U[1], U[2], red_);
+      CK(cudaGetLastError());
+    }
+    const bool spline = interp == QUADRATIC || interp == CUBIC;
+    const int deg = interp == QUADRATIC ? 2 : 3;
+    if (spline) {
+      if (!ensure_spline(deg, msg)) return false;
+      for (int l = 0; l < 2; l++)
+        if (!ucoef_[l][0])
+          for (int c = 0; c < 3; c++)
+            if (!(ucoef_[l][c] = arena_.alloc<T>(ntot_, msg))) return false;
+      if (ucoef_deg_[cur_ ^ 1] != deg) {  // coefficients of u_n missing (first spline use)
+        if (!fit(u_[cur_ ^ 1], ucoef_[cur_ ^ 1], msg)) return false;
+        ucoef_deg_[cur_ ^ 1] = deg;
+      }
+      if (!fit(u_[cur_], ucoef_[cur_], msg)) return false;
+      ucoef_deg_[cur_] = deg;
+    } else {
+      ucoef_deg_[cur_] = 0;
+    }
+    CK(cudaMemcpyAsync(red_host_, red_, sizeof(DevReduce), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaEventRecord(ev_[1], stream_));
+    CK(cudaStreamSynchronize(stream_));
+    red_err_ = red_host_->err;
+    if (red_err_) return err_msg(msg);
+    double cmax, cmin;
+    std::memcpy(&cmax, &red_host_->cmax, sizeof(double));
+    std::memcpy(&cmin, &red_host_->cmin, sizeof(double));
+    const lcsdata_t dt_f = t_np1_ - t_n_;
+    const lcsdata_t this_cfl = dt_f >= lcsdata_t(0) ? (lcsdata_t)cmax * dt_f : (lcsdata_t)cmin * dt_f;
+    counters_.updates++;
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
+    counters_.phase_ms[0] += ms;
+
+    VelFields<T> V;
+    for (int c = 0; c < 3; c++) {
+      V.un[c] = u_[cur_ ^ 1][c];
+      V.unp1[c] = u_[cur_][c];
+      V.cn[c] = spline ? ucoef_[cur_ ^ 1][c] : nullptr;
+      V.cnp1[c] = spline ? ucoef_[cur_][c] : nullptr;
+    }
+    const int iv = interp == NEAREST_NBR ? INTERP_NEAREST : (interp == LINEAR ? INTERP_LINEAR : INTERP_SPLINE);
+    const SplineAxes<T> sa = spline ? splines_[deg].axes : SplineAxes<T>{};
+
+    // --- per particle set: K1 (backward) / K6 (forward) --------------------------------
+    for (auto &d : diags_) {
+      const lcsdata_t q = this_cfl / (lcsdata_t(opt_->cfl) * d.dt_factor);
+      long nsub = (long)std::ceil((double)q);
+      if (!(q == q)) {
+        msg = "set_dt: non-finite CFL number";
+        return false;
+      }
+      if (nsub < 1) nsub = 1;
+      lcsdata_t dt = dt_f / (lcsdata_t)nsub;
+      if (d.type == FTLE_BKWD) dt = lcsdata_t(-1) * dt;
+      if (std::fabs((double)dt) > 0) {
+        if (d.type == FTLE_FWD) counters_.integrations_fwd += (long long)N_ * nsub;
+        else counters_.integrations_bkwd += (long long)N_ * nsub;
+      }
+      if (d.type == FTLE_FWD) counters_.nsub_fwd = nsub;
+      else counters_.nsub_bkwd = nsub;
+      CK(cudaEventRecord(ev_[2], stream_));
+      lcsdata_t lp_time = d.type == FTLE_BKWD ? t_np1_ : t_n_;
+      while ((long)kev_.size() < 2 * nsub) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        kev_.push_back(e);
+      }
+      for (long sc = 0; sc < nsub; sc++) {
+        StageTimes S = stage_times(lp_time, dt);
+        if (d.type == FTLE_BKWD) {
+          FieldPtrs<T> fo;
+          FieldPtrsW<T> fn;
+          for (int c = 0; c < 3; c++) {
+            fo.f[c] = d.fm[d.cur][c];
+            fn.f[c] = d.fm[d.cur ^ 1][c];
+          }
+          if (spline) {
+            if (!d.fmcoef[0])
+              for (int c = 0; c < 3; c++)
+                if (!(d.fmcoef[c] = arena_.alloc<T>(ntot_, msg))) return false;
+            if (!fit(d.fm[d.cur], d.fmcoef, msg)) return false;
+            for (int c = 0; c < 3; c++) fo.f[c] = d.fmcoef[c];
+          }
+          CK(cudaEventRecord(kev_[2 * sc], stream_));
+          if (!launch_sl(iv, sa, V, fo, fn, S, (T)dt, msg)) return false;
+          CK(cudaEventRecord(kev_[2 * sc + 1], stream_));
+          d.cur ^= 1;
+        } else {
+          CK(cudaEventRecord(kev_[2 * sc], stream_));
+          if (!launch_fwd(iv, sa, V, d.P, S, (T)dt, msg)) return false;
+          CK(cudaEventRecord(kev_[2 * sc + 1], stream_));
+        }
+        lp_time = lp_time + dt;
+      }
+      CK(cudaEventRecord(ev_[3], stream_));
+      CK(cudaEventSynchronize(ev_[3]));
+      CK(cudaEventElapsedTime(&ms, ev_[2], ev_[3]));
+      counters_.phase_ms[d.type == FTLE_BKWD ? 1 : 2] += ms;
+      for (long sc = 0; sc < nsub; sc++) {
+        float km = 0;
+        CK(cudaEventElapsedTime(&km, kev_[2 * sc], kev_[2 * sc + 1]));
+        if (d.type == FTLE_BKWD) {
+          counters_.sl_kernel_ms += km;
+          counters_.sl_kernel_launches++;
+        } else {
+          counters_.fwd_kernel_ms += km;
+          counters_.fwd_kernel_launches++;
+        }
+      }
+    }
+
+    // --- h boundaries: K7 snapshot, K4 composition, K5 FTLE, reset ----------------------
+    for (auto &d : diags_) {
+      if ((long)(t_np1_ / d.h) == (long)(t_n_ / d.h)) continue;
+      CK(cudaEventRecord(ev_[4], stream_));
+      const long step0 = fnint((double)(lcsdata_t)std::fmod((double)t_np1_, (double)d.T_) / (double)d.h);
+      // the reference writes slot nint(mod(t,T)/h); slot nint(T/h) and negative slots go to
+      // files reconstruct never reads back
+      const long wslot = fnint((double)((lcsdata_t)std::fmod((double)t_np1_, (double)d.T_) / d.h));
+      (void)step0;
+      if (wslot >= 0 && wslot < d.nslot) {
+        if (!launch_snapshot(d, (int)wslot, msg)) return false;
+        d.written[wslot] = 1;
+        d.coef_deg[wslot] = 0;
+      }
+      CK(cudaEventRecord(ev_[5], stream_));
+      // composition order (reconstruct_flowmap, src/flowmap_m.f90:202-268)
+      const int nstep = d.nslot;
+      long step = wslot;
+      const int inc = d.type == FTLE_FWD ? 1 : -1;
+      if (d.type == FTLE_FWD) step += inc;
+      int m = 0;
+      for (int i = 0; i < nstep; i++) {
+        if (step >= nstep) step = 0;
+        if (step < 0) step = nstep - 1;
+        if (d.written[step]) {
+          if (spline) {
+            if (!d.slotcoef[3 * step])
+              for (int c = 0; c < 3; c++)
+                if (!(d.slotcoef[3 * step + c] = arena_.alloc<T>(ntot_, msg))) return false;
+            if (d.coef_deg[step] != deg) {
+              if (!fit(&d.slot[3 * step], &d.slotcoef[3 * step], msg)) return false;
+              d.coef_deg[step] = deg;
+            }
+            for (int c = 0; c < 3; c++) d.slot_list_host[3 * m + c] = d.slotcoef[3 * step + c];
+          } else {
+            for (int c = 0; c < 3; c++) d.slot_list_host[3 * m + c] = d.slot[3 * step + c];
+          }
+          m++;
+        }
+        step += inc;
+      }
+      CK(cudaMemcpyAsync(d.slot_list_dev, d.slot_list_host.data(), sizeof(T *) * 3 * std::max(m, 1), cudaMemcpyHostToDevice,
+                         stream_));
+      if (!launch_compose(iv, sa, d, m, msg)) return false;
+      CK(cudaEventRecord(ev_[6], stream_));
+      if (!launch_ftle(d, msg)) return false;
+      CK(cudaEventRecord(ev_[7], stream_));
+      // reset_lp: particles back to the grid, flow map to zero (src/cfd2lcs.f90:208-209)
+      if (d.type == FTLE_BKWD) {
+        for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(d.fm[d.cur][c], 0, ntot_ * sizeof(T), stream_));
+      } else {
+        launch_reset(d);
+      }
+      CK(cudaStreamSynchronize(stream_));
+      // the working map of the next interval starts from zero; the memcpy of the slot
+      // pointer list above must complete before the host buffer is reused
+      CK(cudaEventElapsedTime(&ms, ev_[4], ev_[5]));
+      counters_.phase_ms[3] += ms;
+      CK(cudaEventElapsedTime(&ms, ev_[5], ev_[6]));
+      counters_.phase_ms[4] += ms;
+      CK(cudaEventElapsedTime(&ms, ev_[6], ev_[7]));
+      counters_.phase_ms[5] += ms;
+      d.have_frame = true;
+      counters_.ftle_frames++;
+    }
+    CK(cudaEventRecord(ev_[9], stream_));
+    CK(cudaEventSynchronize(ev_[9]));
+    CK(cudaEventElapsedTime(&ms, ev_[8], ev_[9]));
+    counters_.phase_ms[6] += ms;
+    return sync_errors(msg);
+  }
+
+  bool sync_errors(std::string &msg) override {
+    if (!stream_) return true;
+    CK(cudaStreamSynchronize(stream_));
+    int err = 0;
+    CK(cudaMemcpy(&err, &red_->err, sizeof(int), cudaMemcpyDeviceToHost));
+    red_err_ |= err;
+    if (red_err_) return err_msg(msg);
+    return true;
+  }
+
+  bool get_ftle(int handle, lcsdata_t *out, std::string &msg) override {
+    Diag<T> *d = find(handle);
+    if (!d || !d->have_frame) {
+      msg = "get_ftle: unknown handle or no FTLE frame yet";
+      return false;
+    }
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpy(out, d->ftle, N_ * sizeof(lcsdata_t), cudaMemcpyDeviceToHost));
+    return true;
+  }
+
+  bool get_flowmap(int handle, lcsdata_t *out, std::string &msg) override {
+    Diag<T> *d = find(handle);
+    if (!d || !d->have_frame) {
+      msg = "get_flowmap: unknown handle or no FTLE frame yet";
+      return false;
+    }
+    CK(cudaStreamSynchronize(stream_));
+    std::vector<T> tmp(N_);
+    for (int c = 0; c < 3; c++) {
+      CK(cudaMemcpy(tmp.data(), d->composed[c], N_ * sizeof(T), cudaMemcpyDeviceToHost));
+      for (long q = 0; q < N_; q++) out[c * N_ + q] = (lcsdata_t)tmp[q];
+    }
+    return true;
+  }
+
+  const lcsdata_t *ftle_device_ptr(int handle) override {
+    Diag<T> *d = find(handle);
+    return d ? d->ftle : nullptr;
+  }
+
+  const Counters &counters() const override { return counters_; }
+
+ private:
+  int fail(std::string &msg, const char *what) {
+    msg = std::string("CUDA error in ") + what;
+    return -1;
+  }
+
+  bool err_msg(std::string &msg) {
+    if (red_err_ & ERR_NONFINITE_VELOCITY) msg = "update: non-finite velocity (CFL number is not finite)";
+    else if (red_err_ & ERR_TRACKING) msg = "ERROR: cannot locate all particles (node search did not converge)";
+    else if (red_err_ & ERR_UNKNOWN_FLAG) msg = "ERROR: Unknown bcflag";
+    else msg = "device error";
+    return false;
+  }
+
+  template <typename V>
+  T *upload(const std::vector<V> &h, std::string &msg) {
+    std::vector<T> tmp(h.size());
+    for (size_t q = 0; q < h.size(); q++) tmp[q] = (T)h[q];
+    T *d = arena_.alloc<T>(tmp.size(), msg);
+    if (!d) return nullptr;
+    if (cudaMemcpy(d, tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) {
+      msg = "upload failed";
+      return nullptr;
+    }
+    return d;
+  }
+
+  Diag<T> *find(int handle) {
+    for (auto &d : diags_)
+      if (d.handle == handle) return &d;
+    return nullptr;
+  }
+
+  // stage time fractions of integrate_lp (src/lp_motion_m.f90:165-327) in the interface
+  // precision, as the reference computes them
+  StageTimes stage_times(lcsdata_t t, lcsdata_t dt) const {
+    const lcsdata_t t0 = t_n_, t1 = t_np1_;
+    const lcsdata_t HALF = lcsdata_t(1) / lcsdata_t(2);
+    auto ct = [&](lcsdata_t tt) -> double {
+      if (t1 == t0) return 0.0;  // first update: 0/0, the displacement is zero for any ct
+      lcsdata_t v = (tt - t0) / (t1 - t0);
+      v = std::max(std::min(v, lcsdata_t(1)), lcsdata_t(0));
+      return (double)v;
+    };
+    StageTimes S{};
+    switch (opt_->integrator) {
+      case 0: S.ct[0] = ct(t); break;
+      case 1: S.ct[0] = ct(t + HALF * dt); break;
+      case 2: S.ct[0] = ct(t); S.ct[1] = ct(t + HALF * dt); break;
+      case 3: S.ct[0] = ct(t); S.ct[1] = ct(t + HALF * dt); S.ct[2] = ct(t + dt); break;
+      default: S.ct[0] = ct(t); S.ct[1] = ct(t + HALF * dt); S.ct[2] = S.ct[1]; S.ct[3] = ct(t + dt); break;
+    }
+    return S;
+  }
+
+  bool ensure_spline(int deg, std::string &msg) {
+    if (splines_[deg].deg == deg) return true;
+    SplineSet<T> s;
+    s.deg = deg;
+    for (int a = 0; a < 3; a++) {
+      SplineAxisHost<lcsdata_t> A;
+      const int npts = n_[a] + 2;
+      const int k = std::max(std::min(deg + 1, npts - 1), 2);
+      if (!A.build(hg_.li[a], k)) {
+        msg = "bspline: singular collocation system or bad abscissae";
+        return false;
+      }
+      SplineAxis<T> &D = s.axes.ax[a];
+      D.n = A.n;
+      D.k = A.k;
+      if (!(D.t = upload(A.t, msg))) return false;
+      if (!(D.rinv = upload(A.rinv, msg))) return false;
+      if (!(D.lu = upload(A.lu, msg))) return false;
+    }
+    splines_[deg] = s;
+    return true;
+  }
+
+  // coefficients of the padded fields src (3 components) into dst (db3ink, x then y then z)
+  bool fit(T *const src[3], T *const dst[3], std::string &msg) {
+    const SplineAxes<T> &S = splines_[opt_->interpolator == QUADRATIC ? 2 : 3].axes;
+    const int sx = dg_.P.sx, sxy = dg_.P.sxy, nz = n_[2] + 2, ny = n_[1] + 2;
+    for (int c = 0; c < 3; c++) {
+      if (src[c] != dst[c]) CK(cudaMemcpyAsync(dst[c], src[c], ntot_ * sizeof(T), cudaMemcpyDeviceToDevice, stream_));
+      counters_.kernel_launches += 3;
+      {
+        const int lines = ny * nz, wpb = 4;
+        const size_t smem = (size_t)wpb * sx * sizeof(T);
+        k_fit_axis_x<T><<<(lines + wpb - 1) / wpb, 32 * wpb, smem, stream_>>>(S.ax[0], dst[c], lines);
+      }
+      {
+        const dim3 blk(128, 1), grd((sx + 127) / 128, nz);
+        k_fit_axis_yz<T><<<grd, blk, 0, stream_>>>(S.ax[1], dst[c], sx, nz, (long)sx, (long)sxy);
+      }
+      {
+        const dim3 blk(128, 1), grd((sxy + 127) / 128, 1);
+        k_fit_axis_yz<T><<<grd, blk, 0, stream_>>>(S.ax[2], dst[c], sxy, 1, (long)sxy, 0L);
+      }
+      CK(cudaGetLastError());
+    }
+    return true;
+  }
+
+  dim3 node_grid() const { return dim3((n_[0] + 31) / 32, (n_[1] + 7) / 8, n_[2]); }
+
+  template <int INTERP, bool F>
+  void sl_integ(const SplineAxes<T> &sa, const VelFields<T> &V, FieldPtrs<T> fo, FieldPtrsW<T> fn, StageTimes S, T dt) {
+    const dim3 blk(32, 8, 1), grd = node_grid();
+    int *err = &red_->err;
+    counters_.kernel_launches++;
+    switch (opt_->integrator) {
+      case 0: k_sl_subcycle<T, EULER_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
+      case 1: k_sl_subcycle<T, TRAPEZOIDAL_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
+      case 2: k_sl_subcycle<T, RK2_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
+      case 3: k_sl_subcycle<T, RK3_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
+      default: k_sl_subcycle<T, RK4_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
+    }
+  }
+
+  bool launch_sl(int iv, const SplineAxes<T> &sa, const VelFields<T> &V, FieldPtrs<T> fo, FieldPtrsW<T> fn, StageTimes S, T dt,
+                 std::string &msg) {
+    const bool F = dg_.P.has_flags != 0;
+    if (iv == INTERP_NEAREST) F ? sl_integ<INTERP_NEAREST, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_NEAREST, false>(sa, V, fo, fn, S, dt);
+    else if (iv == INTERP_LINEAR) F ? sl_integ<INTERP_LINEAR, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_LINEAR, false>(sa, V, fo, fn, S, dt);
+    else F ? sl_integ<INTERP_SPLINE, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_SPLINE, false>(sa, V, fo, fn, S, dt);
+    CK(cudaGetLastError());
+    return true;
+  }
+
+  template <int INTERP, bool F>
+  void fwd_integ(const SplineAxes<T> &sa, const VelFields<T> &V, Particles<T> P, StageTimes S, T dt) {
+    const int blk = 256, grd = (int)((N_ + blk - 1) / blk);
+    int *err = &red_->err;
+    const int np = (int)N_;
+    counters_.kernel_launches++;
+    switch (opt_->integrator) {
+      case 0: k_fwd_subcycle<T, EULER_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, P, S, dt, np, err); break;
+      case 1: k_fwd_subcycle<T, TRAPEZOIDAL_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, P, S, dt, np, err); break;
+      case 2: k_fwd_subcycle<T, RK2_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, P, S, dt, np, err); break;
+      case 3: k_fwd_subcycle<T, RK3_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, P, S, dt, np, err); break;
+      default: k_fwd_subcycle<T, RK4_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, P, S, dt, np, err); break;
+    }
+  }
+
+  bool launch_fwd(int iv, const SplineAxes<T> &sa, const VelFields<T> &V, Particles<T> P, StageTimes S, T dt, std::string &msg) {
+    const bool F = dg_.P.has_flags != 0;
+    if (iv == INTERP_NEAREST) F ? fwd_integ<INTERP_NEAREST, true>(sa, V, P, S, dt) : fwd_integ<INTERP_NEAREST, false>(sa, V, P, S, dt);
+    else if (iv == INTERP_LINEAR) F ? fwd_integ<INTERP_LINEAR, true>(sa, V, P, S, dt) : fwd_integ<INTERP_LINEAR, false>(sa, V, P, S, dt);
+    else F ? fwd_integ<INTERP_SPLINE, true>(sa, V, P, S, dt) : fwd_integ<INTERP_SPLINE, false>(sa, V, P, S, dt);
+    CK(cudaGetLastError());
+    return true;
+  }
+
+  bool launch_snapshot(Diag<T> &d, int s, std::string &msg) {
+    const dim3 blk(32, 8, 1), grd = node_grid();
+    FieldPtrs<T> src{};
+    FieldPtrsW<T> dst{};
+    for (int c = 0; c < 3; c++) {
+      dst.f[c] = d.slot[3 * s + c];
+      src.f[c] = d.type == FTLE_BKWD ? d.fm[d.cur][c] : nullptr;
+    }
+    int *err = &red_->err;
+    const bool F = dg_.P.has_flags != 0;
+    counters_.kernel_launches++;
+    if (d.type == FTLE_BKWD) {
+      if (F) k_snapshot<T, true, false><<<grd, blk, 0, stream_>>>(dg_, src, d.P, dst, err);
+      else k_snapshot<T, false, false><<<grd, blk, 0, stream_>>>(dg_, src, d.P, dst, err);
+    } else {
+      if (F) k_snapshot<T, true, true><<<grd, blk, 0, stream_>>>(dg_, src, d.P, dst, err);
+      else k_snapshot<T, false, true><<<grd, blk, 0, stream_>>>(dg_, src, d.P, dst, err);
+    }
+    CK(cudaGetLastError());
+    return true;
+  }
+
+  bool launch_compose(int iv, const SplineAxes<T> &sa, Diag<T> &d, int m, std::string &msg) {
+    const dim3 blk(32, 8, 1), grd = node_grid();
+    FieldPtrsW<T> out{};
+    for (int c = 0; c < 3; c++) out.f[c] = d.composed[c];
+    int *err = &red_->err;
+    const bool F = dg_.P.has_flags != 0;
+    const T *const *sl = d.slot_list_dev;
+    counters_.kernel_launches++;
+    counters_.slots_composed += m;
+#define COMPOSE(I, FL) k_compose<T, I, FL><<<grd, blk, 0, stream_>>>(dg_, sa, sl, m, out, err)
+    if (iv == INTERP_NEAREST) { if (F) COMPOSE(INTERP_NEAREST, true); else COMPOSE(INTERP_NEAREST, false); }
+    else if (iv == INTERP_LINEAR) { if (F) COMPOSE(INTERP_LINEAR, true); else COMPOSE(INTERP_LINEAR, false); }
+    else { if (F) COMPOSE(INTERP_SPLINE, true); else COMPOSE(INTERP_SPLINE, false); }
+#undef COMPOSE
+    CK(cudaGetLastError());
+    return true;
+  }
+
+  bool launch_ftle(Diag<T> &d, std::string &msg) {
+    const dim3 blk(32, 8, 1), grd = node_grid();
+    FieldPtrs<T> f{};
+    for (int c = 0; c < 3; c++) f.f[c] = d.composed[c];
+    counters_.kernel_launches++;
+    if (dg_.P.has_flags)
+      k_ftle<T, lcsdata_t, true><<<grd, blk, 0, stream_>>>(dg_, f, d.ftle, d.T_, opt_->incompressible);
+    else
+      k_ftle<T, lcsdata_t, false><<<grd, blk, 0, stream_>>>(dg_, f, d.ftle, d.T_, opt_->incompressible);
+    CK(cudaGetLastError());
+    return true;
+  }
+
+  void launch_reset(Diag<T> &d) {
+    const dim3 blk(32, 8, 1), grd = node_grid();
+    counters_.kernel_launches++;
+    k_reset_particles<T><<<grd, blk, 0, stream_>>>(dg_, d.P);
+  }
+
+  const Options *opt_;
+  HostGrid<lcsdata_t> hg_;
+  DevGrid<T> dg_{};
+  DevArena arena_;
+  cudaStream_t stream_ = nullptr;
+  std::vector<cudaEvent_t> ev_, kev_;
+  int n_[3] = {0, 0, 0};
+  long N_ = 0, ntot_ = 0;
+  T *u_[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  T *ucoef_[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  int ucoef_deg_[2] = {0, 0};
+  int cur_ = 0;
+  lcsdata_t *stage_ = nullptr;
+  DevReduce *red_ = nullptr, *red_host_ = nullptr;
+  int red_err_ = 0;
+  SplineSet<T> splines_[4];
+  std::vector<Diag<T>> diags_;
+  lcsdata_t t_n_ = 0, t_np1_ = 0;
+  bool first_call_ = true;
+  Counters counters_;
+};
+
+std::unique_ptr<EngineBase> make_engine(const Options *opt) {
+  if (opt->mixed_precision) return std::unique_ptr<EngineBase>(new Engine<float>(opt));
+  return std::unique_ptr<EngineBase>(new Engine<lcsdata_t>(opt));
+}
+
+}  // namespace cfd2lcs

@@ -1,0 +1,63 @@
+// Host orchestration of libcfd2lcs_b200: owns the device state of one library instance
+// (the reference keeps the same state in Fortran module globals, src/data_m.f90:313-387)
+// and runs the per-update sequence of cfd2lcs_update (src/cfd2lcs.f90:55-250) as kernel
+// launches on one CUDA stream.
+#pragma once
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#ifdef CFD2LCS_SP
+typedef float lcsdata_t;
+#else
+typedef double lcsdata_t;
+#endif
+
+namespace cfd2lcs {
+
+// User options (src/data_m.f90:19-92) plus the precision form of this library.
+struct Options {
+  int integrator = 2;     // RK2
+  int interpolator = 1;   // LINEAR
+  int incompressible = 0;
+  int aux_grid = 0;
+  int velocity_invariants = 0;
+  double cfl = 0.5;
+  int mixed_precision = 0;  // extension: FP32 advection/composition, FP64 Cauchy-Green + eigen
+};
+
+struct Counters {
+  long long integrations_fwd = 0, integrations_bkwd = 0;
+  long long nsub_fwd = 0, nsub_bkwd = 0;
+  long long ftle_frames = 0, updates = 0;
+  long long kernel_launches = 0, slots_composed = 0;
+  // event-timed hot kernels: backward SL subcycle and forward particle subcycle
+  double sl_kernel_ms = 0, fwd_kernel_ms = 0;
+  long long sl_kernel_launches = 0, fwd_kernel_launches = 0;
+  // ingest, bkwd advect, fwd advect, snapshot, compose, ftle, whole update (event span)
+  double phase_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+};
+
+class EngineBase {
+ public:
+  virtual ~EngineBase() {}
+  // false + msg on failure (the caller latches the error)
+  virtual bool init(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, const int *flag, std::string &msg) = 0;
+  virtual int diagnostic_init(int type, int resolution, lcsdata_t T, lcsdata_t h, const char *label, std::string &msg) = 0;
+  virtual bool update(const int n[3], const lcsdata_t *u, const lcsdata_t *v, const lcsdata_t *w, lcsdata_t time, bool device_ptrs,
+                      std::string &msg) = 0;
+  virtual bool get_ftle(int handle, lcsdata_t *out, std::string &msg) = 0;
+  virtual bool get_flowmap(int handle, lcsdata_t *out, std::string &msg) = 0;
+  virtual const lcsdata_t *ftle_device_ptr(int handle) = 0;
+  virtual bool sync_errors(std::string &msg) = 0;
+  virtual const Counters &counters() const = 0;
+  virtual bool host_grid_tables(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, const int *flag,
+                                lcsdata_t *xyz_pad, int *flag_pad, lcsdata_t *nrm_pad, lcsdata_t *inv_delta, int *per,
+                                std::string &msg) = 0;
+};
+
+// Creates the engine for the current options (plain precision of lcsdata_t, or mixed).
+std::unique_ptr<EngineBase> make_engine(const Options *opt);
+
+}  // namespace cfd2lcs

@@ -1,0 +1,1845 @@
+/*
+ * cfd2lcs_oracle.c -- TEST INFRASTRUCTURE ONLY (the parity checker).
+ *
+ * A CPU restatement of libcfd2lcs's FTLE hot path as it behaves on ONE MPI rank:
+ * grid ingest, ghost/boundary padding, CFL subcycling, the backward semi-Lagrangian
+ * flow-map update, the forward particle update, the in-memory sub-flow-map ring,
+ * the composition (reconstruct) and the FTLE.  Every routine names the reference
+ * file:line it restates (paths relative to the libcfd2lcs source tree).
+ *
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference arm
+ * may load this library.  The shipped library (libcfd2lcs_b200) never links it.
+ *
+ * PARITY UNPINNED: the reference ships no tests, no golden vectors and no fixtures,
+ * and it cannot be compiled here (it needs gfortran, MPI and LAPACK, none of which are
+ * installed).  This restatement is therefore checked against analytic known answers
+ * (translation, rigid rotation, polynomial reproduction of the spline) rather than
+ * against outputs of the reference itself.
+ *
+ * Build: oracle/Makefile -> liboracle_dp.so (real = double, the reference's "dp"
+ * build) and liboracle_sp.so (real = float, the "sp" build).  Compiled without FMA
+ * contraction, as gfortran -O3 compiles the reference for baseline x86-64.
+ *
+ * Deliberate single-rank simplifications (all identities when nprocs == 1):
+ *   - every MPI collective is the identity; exchange_sdata reduces to the SELF copies
+ *     of src/comms_m.f90:814-822; exchange_lp_alltoall / exchange_lpmap keep particle
+ *     order (pack order == unpack order for one rank);
+ *   - the cfd2lcs_tmp/ sub-flow-map files become an in-memory ring (a fresh, empty
+ *     temp directory is assumed at init);
+ *   - no output files are written (write_lcs is out of scope).
+ */
+#include <math.h>
+#include <float.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <stdint.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#ifdef ORACLE_SP
+typedef float real;
+#define R_TINY FLT_MIN
+#define R_HUGE FLT_MAX
+#else
+typedef double real;
+#define R_TINY DBL_MIN
+#define R_HUGE DBL_MAX
+#endif
+
+/* cfd2lcs_inc_double.h:27-65 */
+enum { LCS_INTERNAL = 0, LCS_INFLOW = 1, LCS_OUTFLOW = 2, LCS_WALL = 3, LCS_SLIP = 4, LCS_2D = 5, LCS_MASK = 6 };
+enum { FTLE_FWD = 0, FTLE_BKWD = 1, LP_TRACER = 2 };
+enum { EULER = 0, TRAPEZOIDAL = 1, RK2 = 2, RK3 = 3, RK4 = 4 };
+enum { NEAREST_NBR = 0, LINEAR = 1, QUADRATIC = 2, CUBIC = 3, TSE = 5, TSE_LIMIT = 6 };
+enum { LCS_FALSE = 0, LCS_TRUE = 1 };
+/* data_m.f90:110-121 */
+enum { LP_IB = -1, LP_UNKNOWN = -2, LP_RECYCLE = -3, LP_STICK = -4 };
+enum { FWD = 1, BKWD = -1 };
+enum { NO_COMM = 0, SELF_COMM = 1 };
+
+/* Neighbour offsets, data_m.f90:124-152 (order matters for tracking ties). */
+static const int NBR[27][3] = {
+    {0, 0, 0},   {-1, 0, 0},  {0, -1, 0}, {0, 0, -1}, {1, 0, 0},  {0, 1, 0},  {0, 0, 1},
+    {-1, -1, -1}, {0, -1, -1}, {1, -1, -1}, {-1, 0, -1}, {1, 0, -1}, {-1, 1, -1}, {0, 1, -1},
+    {1, 1, -1},  {-1, -1, 0}, {1, -1, 0},  {-1, 1, 0}, {1, 1, 0},  {-1, -1, 1}, {0, -1, 1},
+    {1, -1, 1},  {-1, 0, 1},  {1, 0, 1},   {-1, 1, 1}, {0, 1, 1},  {1, 1, 1}};
+
+#define MAXLCS 64
+#define MAXMSG 512
+
+/* ------------------------------------------------------------------------------------
+ * Ghost-padded structured storage: Fortran bounds (0:n+1) in each direction, i fastest
+ * (structured_m.f90:73-96; NGHOST_CFD = 1, data_m.f90:106).
+ * ------------------------------------------------------------------------------------ */
+typedef struct {
+    int ni, nj, nk;
+    long sx, sy, ntot;
+} dims_t;
+
+static inline long PX(const dims_t *d, int i, int j, int k) { return (long)i + d->sx * (long)j + d->sy * (long)k; }
+
+typedef struct {
+    real *c[3];
+} sr1_t;
+
+typedef struct {
+    /* dimensions (one rank: local == global, offsets 0) */
+    dims_t d;
+    int gn[3];
+    int per[3];
+    int rectilinear;
+    sr1_t grid;
+    int *bcflag;
+    sr1_t bcnorm;
+    real ps[3][3][3][3]; /* periodic_shift(i,j,k,c) stored [k+1][j+1][i+1][c] */
+    real bb[6];
+    int scomm_flag[3][3][3]; /* max-connectivity SELF/NO comm flag per direction */
+} sgrid_t;
+
+typedef struct {
+    int np;
+    int direction;
+    int recursive_tracking;
+    real dt_factor;
+    real *xp[3], *up[3], *dx[3];
+    int *no[3], *no_scfd[3];
+    int *flag;
+    sr1_t fm;
+} lp_t;
+
+typedef struct {
+    int id;
+    int diagnostic;
+    real T, h;
+    lp_t lp;
+    real *ftle; /* padded sr0 */
+    sr1_t fm_out; /* composed flow map of the last FTLE frame (written by write_lcs) */
+    int nslot;
+    real **slot[3]; /* slot[c][s] -> interior values of stored sub-flow map */
+    int *written;
+} lcs_t;
+
+static struct {
+    int error;
+    char msg[MAXMSG];
+    /* options (data_m.f90:19-92) */
+    int integrator, interpolator, incompressible, aux_grid, velocity_invariants;
+    real cfl_max;
+    /* state */
+    int inited;
+    sgrid_t g;
+    sr1_t u_n, u_np1, delta;
+    real t_n, t_np1;
+    int first_call;
+    int nlcs;
+    lcs_t *lcs[MAXLCS];
+    long long integrations_fwd, integrations_bkwd;
+    int last_nsub_fwd, last_nsub_bkwd;
+    long long ftle_frames;
+} S = {0, "", RK2, LINEAR, 0, 0, 0, (real)0.5, 0};
+
+static void latch(const char *m) {
+    if (!S.error) snprintf(S.msg, MAXMSG, "%s", m);
+    S.error = 1;
+}
+
+static real *zalloc(long n) {
+    real *p = (real *)calloc((size_t)(n > 0 ? n : 1), sizeof(real));
+    if (!p) {
+        latch("oracle: out of host memory");
+    }
+    return p;
+}
+
+static void sr1_alloc(sr1_t *a, const dims_t *d) {
+    for (int c = 0; c < 3; c++) a->c[c] = zalloc(d->ntot);
+}
+static void sr1_free(sr1_t *a) {
+    for (int c = 0; c < 3; c++) {
+        free(a->c[c]);
+        a->c[c] = NULL;
+    }
+}
+
+static inline int imin(int a, int b) { return a < b ? a : b; }
+static inline int imax(int a, int b) { return a > b ? a : b; }
+static inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+static inline real rmax(real a, real b) { return a > b ? a : b; }
+static inline real rmin(real a, real b) { return a < b ? a : b; }
+
+/* Fortran NINT: round half away from zero. */
+static inline int fnint(real v) { return (int)(v >= 0 ? floor((double)v + 0.5) : -floor(-(double)v + 0.5)); }
+
+/* ------------------------------------------------------------------------------------
+ * exchange_sdata on one rank (comms_m.f90:679-869 with the SELF copy at :814-822).
+ * For every direction d (26 for max connectivity, 6 for face) whose neighbour is SELF
+ * (all non-zero components periodic, comms_m.f90:241-279), the interior slab next to
+ * face d is copied to the ghost slab on the opposite side.  Coordinates carry the
+ * periodic shift of d, with the z component read at (i,k,k) as comms_m.f90:750 does.
+ * ------------------------------------------------------------------------------------ */
+static int comm_self(const sgrid_t *g, int di, int dj, int dk) {
+    if (di && !g->per[0]) return 0;
+    if (dj && !g->per[1]) return 0;
+    if (dk && !g->per[2]) return 0;
+    return 1;
+}
+
+static void exchange_self(const sgrid_t *g, real *const *f, int ncomp, int max_conn, int translate) {
+    const dims_t *d = &g->d;
+    int n[3] = {d->ni, d->nj, d->nk};
+    int ncomm = max_conn ? 27 : 7;
+    for (int ic = 1; ic < ncomm; ic++) {
+        int dd[3] = {NBR[ic][0], NBR[ic][1], NBR[ic][2]};
+        if (!comm_self(g, dd[0], dd[1], dd[2])) continue;
+        int lo[3], hi[3];
+        for (int a = 0; a < 3; a++) {
+            /* pack_list (comms_m.f90:357-415): d=-1 -> [1,ng], 0 -> [1,n], 1 -> [n-ng+1,n] */
+            if (dd[a] == -1) { lo[a] = 1; hi[a] = 1; }
+            else if (dd[a] == 0) { lo[a] = 1; hi[a] = n[a]; }
+            else { lo[a] = n[a]; hi[a] = n[a]; }
+        }
+        real sh[3] = {0, 0, 0};
+        if (translate) {
+            sh[0] = g->ps[dd[2] + 1][dd[1] + 1][dd[0] + 1][0];
+            sh[1] = g->ps[dd[2] + 1][dd[1] + 1][dd[0] + 1][1];
+            sh[2] = g->ps[dd[2] + 1][dd[2] + 1][dd[0] + 1][2]; /* (i,k,k): comms_m.f90:750 */
+        }
+        for (int k = lo[2]; k <= hi[2]; k++)
+            for (int j = lo[1]; j <= hi[1]; j++)
+                for (int i = lo[0]; i <= hi[0]; i++) {
+                    /* ghost on the opposite side: q = p - d*n */
+                    int qi = i - dd[0] * n[0], qj = j - dd[1] * n[1], qk = k - dd[2] * n[2];
+                    long src = PX(d, i, j, k), dst = PX(d, qi, qj, qk);
+                    for (int c = 0; c < ncomp; c++) f[c][dst] = f[c][src] + sh[c];
+                }
+    }
+}
+
+/* ------------------------------------------------------------------------------------
+ * init_sgrid (sgrid_m.f90:16-444), one rank.
+ * ------------------------------------------------------------------------------------ */
+static void cross_unit(const real v1[3], const real v2[3], real out[3]) {
+    /* geometry_m.f90:12-31 (unitvector = .true.) */
+    out[0] = v1[1] * v2[2] - v1[2] * v2[1];
+    out[1] = v1[2] * v2[0] - v1[0] * v2[2];
+    out[2] = v1[0] * v2[1] - v1[1] * v2[0];
+    real m = sqrt(out[0] * out[0] + out[1] * out[1] + out[2] * out[2]);
+    if (m > 0) {
+        out[0] /= m; out[1] /= m; out[2] /= m;
+    }
+}
+
+static void check_rectilinear(sgrid_t *g) {
+    /* sgrid_m.f90:868-949 (including the z loop's 1:k with k = nk+1 left over) */
+    const dims_t *d = &g->d;
+    int ni = d->ni, nj = d->nj, nk = d->nk;
+    const real TOL = (real)1e-4;
+    real mx[3], mn[3];
+    for (int c = 0; c < 3; c++) { mx[c] = -R_HUGE; mn[c] = R_HUGE; }
+    for (long p = 0; p < d->ntot; p++)
+        for (int c = 0; c < 3; c++) {
+            mx[c] = rmax(mx[c], g->grid.c[c][p]);
+            mn[c] = rmin(mn[c], g->grid.c[c][p]);
+        }
+    real big = rmax(rmax(mx[0] - mn[0], mx[1] - mn[1]), mx[2] - mn[2]);
+    int ortho[3] = {1, 1, 1};
+    /* x lines */
+    for (int k = 1; k <= nk && ortho[0]; k++)
+        for (int j = 1; j <= nj && ortho[0]; j++) {
+            real a[3] = {-R_HUGE, -R_HUGE, -R_HUGE}, b[3] = {R_HUGE, R_HUGE, R_HUGE};
+            for (int i = 1; i <= ni; i++)
+                for (int c = 0; c < 3; c++) {
+                    real v = g->grid.c[c][PX(d, i, j, k)];
+                    a[c] = rmax(a[c], v); b[c] = rmin(b[c], v);
+                }
+            if (fabs(a[1] - b[1]) / big > TOL || fabs(a[2] - b[2]) / big > TOL) ortho[0] = 0;
+        }
+    for (int k = 1; k <= nk && ortho[1]; k++)
+        for (int i = 1; i <= ni && ortho[1]; i++) {
+            real a[3] = {-R_HUGE, -R_HUGE, -R_HUGE}, b[3] = {R_HUGE, R_HUGE, R_HUGE};
+            for (int j = 1; j <= nj; j++)
+                for (int c = 0; c < 3; c++) {
+                    real v = g->grid.c[c][PX(d, i, j, k)];
+                    a[c] = rmax(a[c], v); b[c] = rmin(b[c], v);
+                }
+            if (fabs(a[0] - b[0]) / big > TOL || fabs(a[2] - b[2]) / big > TOL) ortho[1] = 0;
+        }
+    for (int j = 1; j <= nj && ortho[2]; j++)
+        for (int i = 1; i <= ni && ortho[2]; i++) {
+            real a[3] = {-R_HUGE, -R_HUGE, -R_HUGE}, b[3] = {R_HUGE, R_HUGE, R_HUGE};
+            for (int k = 1; k <= nk + 1; k++)
+                for (int c = 0; c < 3; c++) {
+                    real v = g->grid.c[c][PX(d, i, j, k)];
+                    a[c] = rmax(a[c], v); b[c] = rmin(b[c], v);
+                }
+            if (fabs(a[0] - b[0]) / big > TOL || fabs(a[1] - b[1]) / big > TOL) ortho[2] = 0;
+        }
+    g->rectilinear = ortho[0] && ortho[1] && ortho[2];
+}
+
+static void compute_bcnorm(sgrid_t *g) {
+    /* sgrid_m.f90:385-419 with compute_lsgw(full_conn) gradient_m.f90:114-217 and
+     * grad_sr0_ls gradient_m.f90:297-335 */
+    const dims_t *d = &g->d;
+    real *bc = zalloc(d->ntot);
+    for (int k = 0; k <= d->nk + 1; k++)
+        for (int j = 0; j <= d->nj + 1; j++)
+            for (int i = 0; i <= d->ni + 1; i++) {
+                long p = PX(d, i, j, k);
+                int f = g->bcflag[p];
+                bc[p] = (f == LCS_2D) ? (real)LCS_INTERNAL : (real)imin(f, 1);
+            }
+    exchange_self(g, &bc, 1, 1, 0);
+    sr1_alloc(&g->bcnorm, d);
+    const real *X = g->grid.c[0], *Y = g->grid.c[1], *Z = g->grid.c[2];
+    for (int k = 1; k <= d->nk; k++)
+        for (int j = 1; j <= d->nj; j++)
+            for (int i = 1; i <= d->ni; i++) {
+                long p = PX(d, i, j, k);
+                real sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
+                for (int nb = 1; nb < 27; nb++) {
+                    long q = PX(d, i + NBR[nb][0], j + NBR[nb][1], k + NBR[nb][2]);
+                    real dx0 = X[q] - X[p], dx1 = Y[q] - Y[p], dx2 = Z[q] - Z[p];
+                    real idw = (real)1 / (dx0 * dx0 + dx1 * dx1 + dx2 * dx2);
+                    sxx = sxx + idw * dx0 * dx0;
+                    syy = syy + idw * dx1 * dx1;
+                    szz = szz + idw * dx2 * dx2;
+                    sxy = sxy + idw * dx0 * dx1;
+                    sxz = sxz + idw * dx0 * dx2;
+                    syz = syz + idw * dx1 * dx2;
+                }
+                real sden = (real)2 * sxy * sxz * syz + sxx * syy * szz - sxx * syz * syz - syy * sxz * sxz - szz * sxy * sxy;
+                real gx = 0, gy = 0, gz = 0;
+                for (int nb = 1; nb < 27; nb++) {
+                    long q = PX(d, i + NBR[nb][0], j + NBR[nb][1], k + NBR[nb][2]);
+                    real dx0 = X[q] - X[p], dx1 = Y[q] - Y[p], dx2 = Z[q] - Z[p];
+                    real idw = (real)1 / (dx0 * dx0 + dx1 * dx1 + dx2 * dx2);
+                    real wx = idw * ((syy * szz - syz * syz) * dx0 + (sxz * syz - sxy * szz) * dx1 + (sxy * syz - sxz * syy) * dx2) / sden;
+                    real wy = idw * ((sxz * syz - sxy * szz) * dx0 + (sxx * szz - sxz * sxz) * dx1 + (sxy * sxz - syz * sxx) * dx2) / sden;
+                    real wz = idw * ((sxy * syz - sxz * syy) * dx0 + (sxy * sxz - syz * sxx) * dx1 + (sxx * syy - sxy * sxy) * dx2) / sden;
+                    real df = bc[q] - bc[p];
+                    gx = gx + df * wx;
+                    gy = gy + df * wy;
+                    gz = gz + df * wz;
+                }
+                real mag = gx * gx + gy * gy + gz * gz;
+                if (mag <= 0) {
+                    gx = gy = gz = 0;
+                } else {
+                    gx = gx / sqrt(mag); gy = gy / sqrt(mag); gz = gz / sqrt(mag);
+                }
+                g->bcnorm.c[0][p] = gx; g->bcnorm.c[1][p] = gy; g->bcnorm.c[2][p] = gz;
+            }
+    free(bc);
+}
+
+static int init_sgrid(sgrid_t *g, const int n[3], const real *x, const real *y, const real *z, const int *flag) {
+    dims_t *d = &g->d;
+    d->ni = n[0]; d->nj = n[1]; d->nk = n[2];
+    if (d->ni < 1 || d->nj < 1 || d->nk < 1) {
+        latch("init: ng > ni, nj or nk");
+        return 1;
+    }
+    d->sx = d->ni + 2;
+    d->sy = d->sx * (long)(d->nj + 2);
+    d->ntot = d->sy * (long)(d->nk + 2);
+    int ni = d->ni, nj = d->nj, nk = d->nk;
+    for (int a = 0; a < 3; a++) g->gn[a] = n[a];
+    /* periodicity from flags, sgrid_m.f90:107-136 */
+    int pl[6] = {0, 0, 0, 0, 0, 0};
+    for (int k = 0; k < nk; k++)
+        for (int j = 0; j < nj; j++)
+            for (int i = 0; i < ni; i++) {
+                int f = flag[i + (long)ni * (j + (long)nj * k)];
+                if (f != LCS_INTERNAL) continue;
+                if (i == 0) pl[0] = 1;
+                if (j == 0) pl[1] = 1;
+                if (k == 0) pl[2] = 1;
+                if (i == ni - 1) pl[3] = 1;
+                if (j == nj - 1) pl[4] = 1;
+                if (k == nk - 1) pl[5] = 1;
+            }
+    for (int a = 0; a < 3; a++)
+        if (pl[a] != pl[a + 3]) {
+            latch("init: periodicity does not appear to match; check flag values passed to cfd2lcs_init");
+            return 1;
+        }
+    for (int a = 0; a < 3; a++) g->per[a] = pl[a] && g->gn[a] != 1;
+
+    sr1_alloc(&g->grid, d);
+    g->bcflag = (int *)calloc((size_t)d->ntot, sizeof(int));
+    /* interior, sgrid_m.f90:169-178 */
+    for (int k = 1; k <= nk; k++)
+        for (int j = 1; j <= nj; j++)
+            for (int i = 1; i <= ni; i++) {
+                long s = (i - 1) + (long)ni * ((j - 1) + (long)nj * (k - 1));
+                long p = PX(d, i, j, k);
+                g->grid.c[0][p] = x[s]; g->grid.c[1][p] = y[s]; g->grid.c[2][p] = z[s];
+                g->bcflag[p] = flag[s];
+            }
+    /* fake (mirrored) ghost coordinates and ghost flags, sgrid_m.f90:182-214 */
+    for (int k = 0; k <= nk + 1; k++)
+        for (int j = 0; j <= nj + 1; j++)
+            for (int i = 0; i <= ni + 1; i++) {
+                int ib = clampi(i, 1, ni), jb = clampi(j, 1, nj), kb = clampi(k, 1, nk);
+                if (i == ib && j == jb && k == kb) continue;
+                int iib = clampi(ib + (ib - i), 1, ni), jib = clampi(jb + (jb - j), 1, nj), kib = clampi(kb + (kb - k), 1, nk);
+                long pb = PX(d, ib, jb, kb), pib = PX(d, iib, jib, kib), p = PX(d, i, j, k);
+                for (int c = 0; c < 3; c++) {
+                    real delta = g->grid.c[c][pb] - g->grid.c[c][pib];
+                    g->grid.c[c][p] = g->grid.c[c][pb] + delta;
+                }
+                g->bcflag[p] = g->bcflag[pb];
+            }
+    /* singleton directions, sgrid_m.f90:217-255 */
+    if (g->gn[0] == 1)
+        for (int k = 0; k <= nk + 1; k++)
+            for (int j = 0; j <= nj + 1; j++) {
+                int f1 = g->bcflag[PX(d, 1, j, k)];
+                int v = (f1 == LCS_INTERNAL) ? LCS_2D : f1;
+                g->bcflag[PX(d, 0, j, k)] = v;
+                for (int i = 2; i <= ni + 1; i++) g->bcflag[PX(d, i, j, k)] = v;
+            }
+    if (g->gn[1] == 1)
+        for (int k = 0; k <= nk + 1; k++)
+            for (int i = 0; i <= ni + 1; i++) {
+                int f1 = g->bcflag[PX(d, i, 1, k)];
+                int v = (f1 == LCS_INTERNAL) ? LCS_2D : f1;
+                g->bcflag[PX(d, i, 0, k)] = v;
+                for (int j = 2; j <= nj + 1; j++) g->bcflag[PX(d, i, j, k)] = v;
+            }
+    if (g->gn[2] == 1)
+        for (int j = 0; j <= nj + 1; j++)
+            for (int i = 0; i <= ni + 1; i++) {
+                int f1 = g->bcflag[PX(d, i, j, 1)];
+                int v = (f1 == LCS_INTERNAL) ? LCS_2D : f1;
+                g->bcflag[PX(d, i, j, 0)] = v;
+                for (int k = 2; k <= nk + 1; k++) g->bcflag[PX(d, i, j, k)] = v;
+            }
+    /* SELF/NO comm flags (comms_m.f90:241-279) */
+    for (int dk = -1; dk <= 1; dk++)
+        for (int dj = -1; dj <= 1; dj++)
+            for (int di = -1; di <= 1; di++) g->scomm_flag[dk + 1][dj + 1][di + 1] = comm_self(g, di, dj, dk) ? SELF_COMM : NO_COMM;
+    /* periodic shifts: exchange with zero shift, difference to the fakes, exchange again
+     * (sgrid_m.f90:257-297) */
+    sr1_t fake;
+    sr1_alloc(&fake, d);
+    for (int c = 0; c < 3; c++) memcpy(fake.c[c], g->grid.c[c], sizeof(real) * (size_t)d->ntot);
+    memset(g->ps, 0, sizeof(g->ps));
+    exchange_self(g, g->grid.c, 3, 1, 1);
+    for (int c = 0; c < 3; c++)
+        for (long p = 0; p < d->ntot; p++) fake.c[c][p] = g->grid.c[c][p] - fake.c[c][p];
+    for (int kk = -1; kk <= 1; kk++)
+        for (int jj = -1; jj <= 1; jj++)
+            for (int ii = -1; ii <= 1; ii++) {
+                int gi = ii == -1 ? 0 : (ii == 0 ? 1 : ni + 1);
+                int gj = jj == -1 ? 0 : (jj == 0 ? 1 : nj + 1);
+                int gk = kk == -1 ? 0 : (kk == 0 ? 1 : nk + 1);
+                for (int c = 0; c < 3; c++) g->ps[kk + 1][jj + 1][ii + 1][c] = fake.c[c][PX(d, gi, gj, gk)];
+            }
+    exchange_self(g, g->grid.c, 3, 1, 1);
+    sr1_free(&fake);
+    /* 2-D extrusion of the singleton direction, sgrid_m.f90:304-359 */
+    {
+        real sc[3];
+        for (int c = 0; c < 3; c++) {
+            real a = -R_HUGE, b = R_HUGE;
+            for (int k = 1; k <= nk; k++)
+                for (int j = 1; j <= nj; j++)
+                    for (int i = 1; i <= ni; i++) {
+                        real v = g->grid.c[c][PX(d, i, j, k)];
+                        a = rmax(a, v); b = rmin(b, v);
+                    }
+            sc[c] = a - b;
+        }
+        real scaling = rmax(rmax(sc[0], sc[1]), sc[2]) / (real)imax(imax(ni, nj), nk);
+        const real *X = g->grid.c[0], *Y = g->grid.c[1], *Z = g->grid.c[2];
+        real *Xw = g->grid.c[0], *Yw = g->grid.c[1], *Zw = g->grid.c[2];
+        (void)X; (void)Y; (void)Z;
+        for (int k = 0; k <= nk + 1; k++)
+            for (int j = 0; j <= nj + 1; j++)
+                for (int i = 0; i <= ni + 1; i++) {
+                    int im1 = imax(i - 1, 0), ip1 = imin(i + 1, ni + 1);
+                    int jm1 = imax(j - 1, 0), jp1 = imin(j + 1, nj + 1);
+                    int km1 = imax(k - 1, 0), kp1 = imin(k + 1, nk + 1);
+                    real dl[3] = {0, 0, 0}, v1[3], v2[3], cu[3];
+                    if (g->gn[0] == 1 && i != 1) {
+                        for (int c = 0; c < 3; c++) {
+                            v1[c] = g->grid.c[c][PX(d, 1, jp1, 1)] - g->grid.c[c][PX(d, 1, jm1, 1)];
+                            v2[c] = g->grid.c[c][PX(d, 1, 1, kp1)] - g->grid.c[c][PX(d, 1, 1, km1)];
+                        }
+                        cross_unit(v1, v2, cu);
+                        for (int c = 0; c < 3; c++) dl[c] = (real)(i - 1) * cu[c];
+                    }
+                    if (g->gn[1] == 1 && j != 1) {
+                        for (int c = 0; c < 3; c++) {
+                            v1[c] = g->grid.c[c][PX(d, ip1, 1, 1)] - g->grid.c[c][PX(d, im1, 1, 1)];
+                            v2[c] = g->grid.c[c][PX(d, 1, 1, kp1)] - g->grid.c[c][PX(d, 1, 1, km1)];
+                        }
+                        cross_unit(v1, v2, cu);
+                        for (int c = 0; c < 3; c++) dl[c] = (real)(j - 1) * cu[c];
+                    }
+                    if (g->gn[2] == 1 && k != 1) {
+                        for (int c = 0; c < 3; c++) {
+                            v1[c] = g->grid.c[c][PX(d, ip1, 1, 1)] - g->grid.c[c][PX(d, im1, 1, 1)];
+                            v2[c] = g->grid.c[c][PX(d, 1, jp1, 1)] - g->grid.c[c][PX(d, 1, jm1, 1)];
+                        }
+                        cross_unit(v1, v2, cu);
+                        for (int c = 0; c < 3; c++) dl[c] = (real)(k - 1) * cu[c];
+                    }
+                    long p = PX(d, i, j, k);
+                    Xw[p] = Xw[p] + dl[0] * scaling;
+                    Yw[p] = Yw[p] + dl[1] * scaling;
+                    Zw[p] = Zw[p] + dl[2] * scaling;
+                }
+    }
+    /* bounding box including ghosts, sgrid_m.f90:362-372 */
+    for (int c = 0; c < 3; c++) {
+        real a = R_HUGE, b = -R_HUGE;
+        for (long p = 0; p < d->ntot; p++) {
+            a = rmin(a, g->grid.c[c][p]);
+            b = rmax(b, g->grid.c[c][p]);
+        }
+        g->bb[c] = a;
+        g->bb[c + 3] = b;
+    }
+    check_rectilinear(g);
+    compute_bcnorm(g);
+    return 0;
+}
+
+/* compute_delta_xyz, sgrid_m.f90:951-1014: 1/(half span of the 3x3x3 neighbourhood) */
+static void compute_delta(const sgrid_t *g, sr1_t *delta) {
+    const dims_t *d = &g->d;
+    sr1_alloc(delta, d);
+    for (int k = 1; k <= d->nk; k++)
+        for (int j = 1; j <= d->nj; j++)
+            for (int i = 1; i <= d->ni; i++) {
+                for (int c = 0; c < 3; c++) {
+                    real a = -R_HUGE, b = R_HUGE;
+                    for (int kk = k - 1; kk <= k + 1; kk++)
+                        for (int jj = j - 1; jj <= j + 1; jj++)
+                            for (int ii = i - 1; ii <= i + 1; ii++) {
+                                real v = g->grid.c[c][PX(d, ii, jj, kk)];
+                                a = rmax(a, v); b = rmin(b, v);
+                            }
+                    real dl = (real)0.5 * fabs(a - b);
+                    delta->c[c][PX(d, i, j, k)] = dl > 0 ? (real)1 / dl : (real)0;
+                }
+            }
+}
+
+/* ------------------------------------------------------------------------------------
+ * Boundary conditions on padded fields.
+ * ------------------------------------------------------------------------------------ */
+/* set_velocity_bc, sgrid_m.f90:810-866 */
+static void set_velocity_bc(const sgrid_t *g, sr1_t *v) {
+    const dims_t *d = &g->d;
+    for (int k = 0; k <= d->nk + 1; k++)
+        for (int j = 0; j <= d->nj + 1; j++)
+            for (int i = 0; i <= d->ni + 1; i++) {
+                long p = PX(d, i, j, k);
+                int f = g->bcflag[p];
+                int inside = i >= 1 && j >= 1 && k >= 1 && i <= d->ni && j <= d->nj && k <= d->nk;
+                switch (f) {
+                case LCS_INTERNAL: break;
+                case LCS_MASK:
+                    for (int c = 0; c < 3; c++) v->c[c][p] = 0;
+                    break;
+                case LCS_WALL:
+                    if (inside) break;
+                    for (int c = 0; c < 3; c++) v->c[c][p] = 0;
+                    break;
+                case LCS_SLIP: case LCS_INFLOW: case LCS_OUTFLOW: case LCS_2D: {
+                    if (inside) break;
+                    long b = PX(d, clampi(i, 1, d->ni), clampi(j, 1, d->nj), clampi(k, 1, d->nk));
+                    for (int c = 0; c < 3; c++) v->c[c][p] = v->c[c][b];
+                    break;
+                }
+                default: latch("set_velocity_bc: unknown bcflag");
+                }
+            }
+}
+
+/* set_flowmap_bc, flowmap_m.f90:325-392 */
+static void set_flowmap_bc(const sgrid_t *g, sr1_t *fm) {
+    const dims_t *d = &g->d;
+    for (int k = 1; k <= d->nk; k++)
+        for (int j = 1; j <= d->nj; j++)
+            for (int i = 1; i <= d->ni; i++) {
+                long p = PX(d, i, j, k);
+                int f = g->bcflag[p];
+                if (f == LCS_MASK || f == LCS_INFLOW || f == LCS_OUTFLOW)
+                    for (int c = 0; c < 3; c++) fm->c[c][p] = 0;
+            }
+    for (int k = 0; k <= d->nk + 1; k++)
+        for (int j = 0; j <= d->nj + 1; j++)
+            for (int i = 0; i <= d->ni + 1; i++) {
+                if (i >= 1 && j >= 1 && k >= 1 && i <= d->ni && j <= d->nj && k <= d->nk) continue;
+                long p = PX(d, i, j, k);
+                switch (g->bcflag[p]) {
+                case LCS_INTERNAL: break;
+                case LCS_WALL: case LCS_MASK: case LCS_INFLOW: case LCS_OUTFLOW:
+                    for (int c = 0; c < 3; c++) fm->c[c][p] = 0;
+                    break;
+                case LCS_SLIP: case LCS_2D: {
+                    long b = PX(d, clampi(i, 1, d->ni), clampi(j, 1, d->nj), clampi(k, 1, d->nk));
+                    for (int c = 0; c < 3; c++) fm->c[c][p] = fm->c[c][b];
+                    break;
+                }
+                default: latch("set_flowmap_bc: unknown bcflag");
+                }
+            }
+}
+
+static void pad_flowmap(const sgrid_t *g, sr1_t *fm) {
+    /* exchange_sdata(scomm_max_r1, fm) + set_flowmap_bc (flowmap_m.f90:90-91) */
+    exchange_self(g, fm->c, 3, 1, 0);
+    set_flowmap_bc(g, fm);
+}
+
+/* ------------------------------------------------------------------------------------
+ * Lagrangian particle sets (lp_m.f90).
+ * ------------------------------------------------------------------------------------ */
+static void lp_alloc(lp_t *lp, int np) {
+    lp->np = np;
+    for (int c = 0; c < 3; c++) {
+        lp->xp[c] = zalloc(np); lp->up[c] = zalloc(np); lp->dx[c] = zalloc(np);
+        lp->no[c] = (int *)calloc((size_t)np, sizeof(int));
+        lp->no_scfd[c] = (int *)calloc((size_t)np, sizeof(int));
+    }
+    lp->flag = (int *)calloc((size_t)np, sizeof(int));
+}
+
+/* reset_lp, lp_m.f90:228-294 (init_lp :13-114 is the same with fresh storage) */
+static void reset_lp(const sgrid_t *g, lp_t *lp, int zero_fm) {
+    const dims_t *d = &g->d;
+    int ip = 0;
+    for (int k = 1; k <= d->nk; k++)
+        for (int j = 1; j <= d->nj; j++)
+            for (int i = 1; i <= d->ni; i++, ip++) {
+                long p = PX(d, i, j, k);
+                for (int c = 0; c < 3; c++) {
+                    lp->xp[c][ip] = g->grid.c[c][p];
+                    lp->up[c][ip] = 0;
+                    lp->dx[c][ip] = 0;
+                }
+                lp->no[0][ip] = i; lp->no[1][ip] = j; lp->no[2][ip] = k;
+                /* educated guess, lp_m.f90:276-278: nint(real(i*ni)/real(ni)) == i */
+                lp->no_scfd[0][ip] = clampi(fnint((real)((float)(i * d->ni) / (float)d->ni)), 1, d->ni);
+                lp->no_scfd[1][ip] = clampi(fnint((real)((float)(j * d->nj) / (float)d->nj)), 1, d->nj);
+                lp->no_scfd[2][ip] = clampi(fnint((real)((float)(k * d->nk) / (float)d->nk)), 1, d->nk);
+                lp->flag[ip] = LP_UNKNOWN;
+            }
+    lp->recursive_tracking = 1;
+    if (zero_fm)
+        for (int c = 0; c < 3; c++) memset(lp->fm.c[c], 0, sizeof(real) * (size_t)d->ntot);
+}
+
+/* project_lp2plane, lp_m.f90:418-538, for a rectilinear grid (its plane normal is the
+ * singleton axis).  Returns immediately on 3-D grids (:433). */
+static void project_lp2plane(const sgrid_t *g, lp_t *lp, int *const *no) {
+    const dims_t *d = &g->d;
+    if (g->gn[0] > 1 && g->gn[1] > 1 && g->gn[2] > 1) return;
+    int ax = g->gn[2] == 1 ? 2 : (g->gn[1] == 1 ? 1 : 0);
+    /* the last matching block wins in the reference; it also forces no%ax = 1 for both node sets */
+    for (int ip = 0; ip < lp->np; ip++) {
+        lp->no[ax][ip] = 1;
+        lp->no_scfd[ax][ip] = 1;
+    }
+#pragma omp parallel for schedule(static)
+    for (int ip = 0; ip < lp->np; ip++) {
+        int i = clampi(no[0][ip], 1, d->ni), j = clampi(no[1][ip], 1, d->nj), k = clampi(no[2][ip], 1, d->nk);
+        long p = PX(d, i, j, k);
+        /* normal = v1 x v2 from central differences of the grid around the node */
+        real v1[3], v2[3], nrm[3];
+        int ip1 = i + 1, im1 = i - 1, jp1 = j + 1, jm1 = j - 1, kp1 = k + 1, km1 = k - 1;
+        for (int c = 0; c < 3; c++) {
+            if (ax == 0) {
+                v1[c] = g->grid.c[c][PX(d, i, jp1, k)] - g->grid.c[c][PX(d, i, jm1, k)];
+                v2[c] = g->grid.c[c][PX(d, i, j, kp1)] - g->grid.c[c][PX(d, i, j, km1)];
+            } else if (ax == 1) {
+                v1[c] = g->grid.c[c][PX(d, ip1, j, k)] - g->grid.c[c][PX(d, im1, j, k)];
+                v2[c] = g->grid.c[c][PX(d, i, j, kp1)] - g->grid.c[c][PX(d, i, j, km1)];
+            } else {
+                v1[c] = g->grid.c[c][PX(d, ip1, j, k)] - g->grid.c[c][PX(d, im1, j, k)];
+                v2[c] = g->grid.c[c][PX(d, i, jp1, k)] - g->grid.c[c][PX(d, i, jm1, k)];
+            }
+        }
+        nrm[0] = v1[1] * v2[2] - v1[2] * v2[1];
+        nrm[1] = v1[2] * v2[0] - v1[0] * v2[2];
+        nrm[2] = v1[0] * v2[1] - v1[1] * v2[0];
+        real mag = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+        for (int c = 0; c < 3; c++) nrm[c] = nrm[c] / mag;
+        real dd[3];
+        for (int c = 0; c < 3; c++) dd[c] = lp->xp[c][ip] - g->grid.c[c][p];
+        real dist = dd[0] * nrm[0] + dd[1] * nrm[1] + dd[2] * nrm[2];
+        if (dist < 0) {
+            dist = -dist;
+            for (int c = 0; c < 3; c++) nrm[c] = -nrm[c];
+        }
+        for (int c = 0; c < 3; c++) lp->xp[c][ip] = lp->xp[c][ip] - dist * nrm[c];
+    }
+}
+
+/* set_lp_bc, lp_tracking_m.f90:185-277 */
+static void set_lp_bc(const sgrid_t *g, lp_t *lp, int *const *no) {
+    const dims_t *d = &g->d;
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (int ip = 0; ip < lp->np; ip++) {
+        int i = clampi(no[0][ip], 1, d->ni), j = clampi(no[1][ip], 1, d->nj), k = clampi(no[2][ip], 1, d->nk);
+        no[0][ip] = i; no[1][ip] = j; no[2][ip] = k;
+        lp->flag[ip] = LP_IB;
+        long p = PX(d, i, j, k);
+        int f = g->bcflag[p];
+        int interior = i > 1 && j > 1 && k > 1 && i < d->ni && j < d->nj && k < d->nk;
+        switch (f) {
+        case LCS_INTERNAL: case LCS_2D: break;
+        case LCS_MASK: case LCS_SLIP: case LCS_WALL: {
+            if (f != LCS_MASK && interior) break;
+            /* dot_product accumulates left to right */
+            real dist = (lp->xp[0][ip] - g->grid.c[0][p]) * g->bcnorm.c[0][p] + (lp->xp[1][ip] - g->grid.c[1][p]) * g->bcnorm.c[1][p] +
+                   (lp->xp[2][ip] - g->grid.c[2][p]) * g->bcnorm.c[2][p];
+            if (dist > 0)
+                for (int c = 0; c < 3; c++) lp->xp[c][ip] = lp->xp[c][ip] - g->bcnorm.c[c][p] * dist;
+            break;
+        }
+        case LCS_INFLOW: case LCS_OUTFLOW:
+            if (interior) break;
+            lp->flag[ip] = LP_STICK;
+            for (int c = 0; c < 3; c++) lp->xp[c][ip] = g->grid.c[c][p];
+            break;
+        default: bad = 1;
+        }
+    }
+    if (bad) latch("set_lp_bc: unknown bcflag");
+}
+
+/* ------------------------------------------------------------------------------------
+ * Tensor-product B-spline interpolation, restated from the algorithms used by the
+ * vendored bspline-fortran (src/bspline/bspline_sub_module.f90): knots dbknot :1737-1785,
+ * collocation + banded LU without pivoting dbintk/dbnfac/dbnslv :1896-2259 (basis values
+ * by the Cox-de Boor recurrence of dbspvn :2288-2370), three transposing passes x,y,z
+ * (db3ink :451-533), and evaluation by de Boor's recurrence (dbvalu :2397-2533) after the
+ * interval search of dintrv (:2558-2634) with db3val's range rules (:574-656).
+ * Arrays here are 0-based; knot t[m] is the reference's t(m+1).
+ * ------------------------------------------------------------------------------------ */
+static void bsp_knots(const real *x, int n, int k, real *t) {
+    real rnot = x[n - 1] + (real)0.1 * (x[n - 1] - x[n - 2]);
+    for (int j = 0; j < k; j++) {
+        t[j] = x[0];
+        t[n + j] = rnot;
+    }
+    if (k % 2 == 1) {
+        int off = (k - 1) / 2 - k;
+        for (int j = k + 1; j <= n; j++) t[j - 1] = (real)0.5 * (x[off + j - 1] + x[off + j]);
+    } else {
+        int off = k / 2 - k;
+        for (int j = k + 1; j <= n; j++) t[j - 1] = x[off + j - 1];
+    }
+}
+
+/* values of the k B-splines of order k that are non-zero on [t(left), t(left+1)) at xv;
+ * left is 1-based as in the reference. */
+static void bsp_basis(const real *t, int k, int left, real xv, real *b) {
+    real dr[8], dl[8];
+    b[0] = 1;
+    for (int j = 1; j < k; j++) {
+        dr[j] = t[left + j - 1] - xv;      /* t(left+j) - x */
+        dl[j] = xv - t[left - j];          /* x - t(left+1-j) */
+        real prev = 0;
+        for (int l = 1; l <= j; l++) {
+            real vm = b[l - 1] / (dr[l] + dl[j + 1 - l]);
+            b[l - 1] = vm * dr[l] + prev;
+            prev = vm * dl[j + 1 - l];
+        }
+        b[j] = prev;
+    }
+}
+
+typedef struct {
+    int n, k;
+    real *t;   /* n + k knots */
+    real *w;   /* band LU, (2k-1) x n column-major, middle row k-1 (0-based) */
+    int ok;
+} bsp_axis_t;
+
+static void bsp_axis_setup(bsp_axis_t *a, const real *x, int n, int k) {
+    a->n = n; a->k = k;
+    a->t = zalloc(n + k);
+    int nr = 2 * k - 1;
+    a->w = zalloc((long)nr * n);
+    a->ok = 1;
+    bsp_knots(x, n, k, a->t);
+    int left = k;
+    for (int i = 1; i <= n; i++) {
+        real xi = x[i - 1];
+        int lim = imin(i + k, n + 1);
+        left = imax(left, i);
+        if (xi < a->t[left - 1]) { a->ok = 0; return; }
+        int found = 0;
+        while (1) {
+            if (xi < a->t[left]) { found = 1; break; }
+            left = left + 1;
+            if (left >= lim) break;
+        }
+        if (!found) {
+            left = left - 1;
+            if (xi > a->t[left]) { a->ok = 0; return; }
+        }
+        real b[8];
+        bsp_basis(a->t, k, left, xi, b);
+        for (int j = 1; j <= k; j++) {
+            int col = left - k + j;                /* 1-based column */
+            int row = k + i - col;                 /* 1-based band row */
+            a->w[(row - 1) + (long)nr * (col - 1)] = b[j - 1];
+        }
+    }
+    /* dbnfac with nbandl = nbandu = k-1 */
+    int mid = k; /* 1-based */
+    int nb = k - 1;
+    for (int i = 1; i <= n - 1; i++) {
+        real piv = a->w[(mid - 1) + (long)nr * (i - 1)];
+        if (piv == 0) { a->ok = 0; return; }
+        int jmax = imin(nb, n - i);
+        for (int j = 1; j <= jmax; j++) a->w[(mid + j - 1) + (long)nr * (i - 1)] = a->w[(mid + j - 1) + (long)nr * (i - 1)] / piv;
+        int kmax = imin(nb, n - i);
+        for (int kk = 1; kk <= kmax; kk++) {
+            int ipk = i + kk, midmk = mid - kk;
+            real fac = a->w[(midmk - 1) + (long)nr * (ipk - 1)];
+            for (int j = 1; j <= jmax; j++)
+                a->w[(midmk + j - 1) + (long)nr * (ipk - 1)] =
+                    a->w[(midmk + j - 1) + (long)nr * (ipk - 1)] - a->w[(mid + j - 1) + (long)nr * (i - 1)] * fac;
+        }
+    }
+    if (a->w[(mid - 1) + (long)nr * (n - 1)] == 0) a->ok = 0;
+}
+
+static void bsp_axis_free(bsp_axis_t *a) {
+    free(a->t); free(a->w);
+    a->t = a->w = NULL;
+}
+
+/* dbnslv: solve in place, b strided by `st` */
+static void bsp_axis_solve(const bsp_axis_t *a, real *b, long st) {
+    int n = a->n, k = a->k, nr = 2 * k - 1, mid = k, nb = k - 1;
+    const real *w = a->w;
+#define B(i) b[(long)((i)-1) * st]
+#define W(r, c) w[((r)-1) + (long)nr * ((c)-1)]
+    if (n != 1) {
+        for (int i = 1; i <= n - 1; i++) {
+            int jmax = imin(nb, n - i);
+            for (int j = 1; j <= jmax; j++) B(i + j) = B(i + j) - B(i) * W(mid + j, i);
+        }
+        int i = n;
+        while (1) {
+            B(i) = B(i) / W(mid, i);
+            int jmax = imin(nb, i - 1);
+            for (int j = 1; j <= jmax; j++) B(i - j) = B(i - j) - B(i) * W(mid - j, i);
+            i = i - 1;
+            if (i <= 1) break;
+        }
+    }
+    B(1) = B(1) / W(mid, 1);
+#undef B
+#undef W
+}
+
+typedef struct {
+    bsp_axis_t ax[3];
+    long nx, ny, nz;
+    real *coef; /* x fastest */
+} bsp3_t;
+
+static void bsp3_setup(bsp3_t *s, const real *xg, const real *yg, const real *zg, int nx, int ny, int nz, int kx, int ky, int kz) {
+    s->nx = nx; s->ny = ny; s->nz = nz;
+    bsp_axis_setup(&s->ax[0], xg, nx, kx);
+    bsp_axis_setup(&s->ax[1], yg, ny, ky);
+    bsp_axis_setup(&s->ax[2], zg, nz, kz);
+    s->coef = zalloc((long)nx * ny * nz);
+}
+
+static void bsp3_free(bsp3_t *s) {
+    for (int a = 0; a < 3; a++) bsp_axis_free(&s->ax[a]);
+    free(s->coef);
+    s->coef = NULL;
+}
+
+/* fit: db3ink with iflag = 0 (knots by dbknot).  Order of the three passes: x, y, z. */
+static void bsp3_fit(bsp3_t *s, const real *f) {
+    long nx = s->nx, ny = s->ny, nz = s->nz;
+    memcpy(s->coef, f, sizeof(real) * (size_t)(nx * ny * nz));
+    if (!s->ax[0].ok || !s->ax[1].ok || !s->ax[2].ok) {
+        latch("bspline: singular collocation system");
+        return;
+    }
+#pragma omp parallel for schedule(static)
+    for (long l = 0; l < ny * nz; l++) bsp_axis_solve(&s->ax[0], s->coef + l * nx, 1);
+#pragma omp parallel for schedule(static)
+    for (long l = 0; l < nx * nz; l++) {
+        long i = l % nx, kk = l / nx;
+        bsp_axis_solve(&s->ax[1], s->coef + i + kk * nx * ny, nx);
+    }
+#pragma omp parallel for schedule(static)
+    for (long l = 0; l < nx * ny; l++) bsp_axis_solve(&s->ax[2], s->coef + l, nx * ny);
+}
+
+/* dintrv: largest ileft (1-based) with xt(ileft) <= x; mflag -1 below, 1 at/above the end */
+static int bsp_intrv(const real *xt, int lxt, real x, int *mflag) {
+    if (x < xt[0]) { *mflag = -1; return 1; }
+    if (x >= xt[lxt - 1]) { *mflag = 1; return lxt; }
+    int lo = 1, hi = lxt; /* xt(lo) <= x < xt(hi) */
+    while (hi - lo > 1) {
+        int mid = (lo + hi) / 2;
+        if (x >= xt[mid - 1]) lo = mid; else hi = mid;
+    }
+    *mflag = 0;
+    return lo;
+}
+
+/* dbvalu with ideriv = 0; t points at the knot vector (0-based), a at n coefficients with
+ * stride st.  Returns 0 and *bad = 1 where the reference returns an error. */
+static real bsp_value(const real *t, const real *a, long st, int n, int k, real x, int *bad) {
+    int mflag;
+    int i = bsp_intrv(t, n + 1, x, &mflag);
+    if (x < t[k - 1]) { *bad = 1; return 0; }
+    if (mflag != 0) {
+        if (x > t[i - 1]) { *bad = 1; return 0; }
+        while (1) {
+            if (i == k) { *bad = 1; return 0; }
+            i = i - 1;
+            if (x != t[i - 1]) break;
+        }
+    }
+    real c[8], tr[8], tl[8];
+    for (int j = 1; j <= k; j++) c[j - 1] = a[(long)(i - k + j - 1) * st];
+    for (int j = 1; j <= k; j++) {
+        tr[j] = t[i + j - 1] - x;       /* t(i+j) - x */
+        tl[j] = x - t[i + 1 - j - 1];   /* x - t(i+1-j) */
+    }
+    for (int j = 1; j <= k - 1; j++) {
+        int kmj = k - j, ilo = kmj;
+        for (int jj = 1; jj <= kmj; jj++) {
+            c[jj - 1] = (c[jj] * tl[ilo] + c[jj - 1] * tr[jj]) / (tl[ilo] + tr[jj]);
+            ilo = ilo - 1;
+        }
+    }
+    return c[0];
+}
+
+/* db3val: 0 outside [t(1), t(n+k)], 0 on any interval-search failure */
+static real bsp3_eval(const bsp3_t *s, real x, real y, real z) {
+    const bsp_axis_t *X = &s->ax[0], *Y = &s->ax[1], *Z = &s->ax[2];
+    if (x < X->t[0] || x > X->t[X->n + X->k - 1]) return 0;
+    if (y < Y->t[0] || y > Y->t[Y->n + Y->k - 1]) return 0;
+    if (z < Z->t[0] || z > Z->t[Z->n + Z->k - 1]) return 0;
+    int mf;
+    int ly = bsp_intrv(Y->t, Y->n + Y->k, y, &mf);
+    if (mf != 0) return 0;
+    int lz = bsp_intrv(Z->t, Z->n + Z->k, z, &mf);
+    if (mf != 0) return 0;
+    real t1[8][8], t2[8];
+    int bad = 0;
+    long nx = s->nx, nxy = s->nx * s->ny;
+    for (int kk = 1; kk <= Z->k; kk++) {
+        int cz = lz - Z->k + kk;
+        for (int jj = 1; jj <= Y->k; jj++) {
+            int cy = ly - Y->k + jj;
+            t1[kk - 1][jj - 1] = bsp_value(X->t, s->coef + (long)(cy - 1) * nx + (long)(cz - 1) * nxy, 1, X->n, X->k, x, &bad);
+            if (bad) return 0;
+        }
+    }
+    int ky0 = ly - Y->k + 1;
+    for (int kk = 1; kk <= Z->k; kk++) {
+        t2[kk - 1] = bsp_value(Y->t + (ky0 - 1), t1[kk - 1], 1, Y->k, Y->k, y, &bad);
+        if (bad) return 0;
+    }
+    int kz0 = lz - Z->k + 1;
+    return bsp_value(Z->t + (kz0 - 1), t2, 1, Z->k, Z->k, z, &bad);
+}
+
+/* ------------------------------------------------------------------------------------
+ * interp_s2u_r1, lp_tracking_m.f90:279-662 (NEAREST_NBR, LINEAR, QUADRATIC, CUBIC;
+ * TSE / TSE_LIMIT are used by the reference only for non-rectilinear grids, which this
+ * restatement rejects at init).
+ * ------------------------------------------------------------------------------------ */
+static void coord_lines(const sgrid_t *g, real **xg, real **yg, real **zg) {
+    const dims_t *d = &g->d;
+    *xg = zalloc(d->ni + 2); *yg = zalloc(d->nj + 2); *zg = zalloc(d->nk + 2);
+    for (int i = 0; i <= d->ni + 1; i++) (*xg)[i] = g->grid.c[0][PX(d, i, 1, 1)];
+    for (int j = 0; j <= d->nj + 1; j++) (*yg)[j] = g->grid.c[1][PX(d, 1, j, 1)];
+    for (int k = 0; k <= d->nk + 1; k++) (*zg)[k] = g->grid.c[2][PX(d, 1, 1, k)];
+    /* 2-D: fake unit spacing, lp_tracking_m.f90:367-378 */
+    if (g->gn[0] == 1) { (*xg)[0] = (*xg)[1] - (real)1.0; (*xg)[2] = (*xg)[1] + (real)1.0; }
+    if (g->gn[1] == 1) { (*yg)[0] = (*yg)[1] - (real)1.0; (*yg)[2] = (*yg)[1] + (real)1.0; }
+    if (g->gn[2] == 1) { (*zg)[0] = (*zg)[1] - (real)1.0; (*zg)[2] = (*zg)[1] + (real)1.0; }
+}
+
+static void interp_r1(const sgrid_t *g, int method, int np, real *const *xp, int *const *no, const sr1_t *f, real *const *out) {
+    const dims_t *d = &g->d;
+    switch (method) {
+    case NEAREST_NBR:
+#pragma omp parallel for schedule(static)
+        for (int ip = 0; ip < np; ip++) {
+            long p = PX(d, no[0][ip], no[1][ip], no[2][ip]);
+            for (int c = 0; c < 3; c++) out[c][ip] = f->c[c][p];
+        }
+        break;
+    case LINEAR: {
+        real *xg, *yg, *zg;
+        coord_lines(g, &xg, &yg, &zg);
+        const real *L[3] = {xg, yg, zg};
+        int nmax[3] = {d->ni + 1, d->nj + 1, d->nk + 1};
+#pragma omp parallel for schedule(static)
+        for (int ip = 0; ip < np; ip++) {
+            int i0[3], i1[3];
+            real t[3], mt[3];
+            for (int a = 0; a < 3; a++) {
+                int n0 = no[a][ip];
+                if (xp[a][ip] > L[a][n0]) { i0[a] = n0; i1[a] = n0 + 1; }
+                else { i0[a] = n0 - 1; i1[a] = n0; }
+                /* the reference leaves an out-of-range bracket undefined; keep it in the array */
+                i0[a] = clampi(i0[a], 0, nmax[a]); i1[a] = clampi(i1[a], 0, nmax[a]);
+                real x0 = L[a][i0[a]], x1 = L[a][i1[a]];
+                t[a] = (xp[a][ip] - x0) / (x1 - x0);
+                t[a] = rmax(rmin(t[a], (real)1.0), (real)0.0);
+                mt[a] = (real)1.0 - t[a];
+            }
+            long p0 = PX(d, i0[0], i0[1], i0[2]), p1 = PX(d, i1[0], i0[1], i0[2]);
+            long p2 = PX(d, i0[0], i1[1], i0[2]), p3 = PX(d, i1[0], i1[1], i0[2]);
+            long p4 = PX(d, i0[0], i0[1], i1[2]), p5 = PX(d, i1[0], i0[1], i1[2]);
+            long p6 = PX(d, i0[0], i1[1], i1[2]), p7 = PX(d, i1[0], i1[1], i1[2]);
+            for (int c = 0; c < 3; c++) {
+                const real *F = f->c[c];
+                out[c][ip] = mt[0] * mt[1] * mt[2] * F[p0] + t[0] * mt[1] * mt[2] * F[p1] + mt[0] * t[1] * mt[2] * F[p2] +
+                             t[0] * t[1] * mt[2] * F[p3] + mt[0] * mt[1] * t[2] * F[p4] + t[0] * mt[1] * t[2] * F[p5] +
+                             mt[0] * t[1] * t[2] * F[p6] + t[0] * t[1] * t[2] * F[p7];
+            }
+        }
+        free(xg); free(yg); free(zg);
+        break;
+    }
+    case QUADRATIC: case CUBIC: {
+        int deg = method == QUADRATIC ? 2 : 3;
+        real *xg, *yg, *zg;
+        coord_lines(g, &xg, &yg, &zg);
+        int nx = d->ni + 2, ny = d->nj + 2, nz = d->nk + 2;
+        int kx = imax(imin(deg + 1, nx - 1), 2), ky = imax(imin(deg + 1, ny - 1), 2), kz = imax(imin(deg + 1, nz - 1), 2);
+        bsp3_t s;
+        bsp3_setup(&s, xg, yg, zg, nx, ny, nz, kx, ky, kz);
+        for (int c = 0; c < 3; c++) {
+            bsp3_fit(&s, f->c[c]);
+#pragma omp parallel for schedule(static)
+            for (int ip = 0; ip < np; ip++) out[c][ip] = bsp3_eval(&s, xp[0][ip], xp[1][ip], xp[2][ip]);
+        }
+        bsp3_free(&s);
+        free(xg); free(yg); free(zg);
+        break;
+    }
+    default:
+        latch("interp: unsupported interpolator (TSE/TSE_LIMIT are not restated)");
+    }
+}
+
+/* ------------------------------------------------------------------------------------
+ * Particle integration, lp_motion_m.f90:129-360
+ * ------------------------------------------------------------------------------------ */
+static real stage_ct(real tt, real t0, real t1) {
+    /* ct = max(min((t-t0)/(t1-t0),1),0); the first update has t1 == t0 (0/0): the
+     * displacement is 0 for any finite ct, so ct := 0 there. */
+    if (t1 == t0) return 0;
+    return rmax(rmin((tt - t0) / (t1 - t0), (real)1.0), (real)0.0);
+}
+
+static void blend(sr1_t *u, real ct) {
+    const dims_t *d = &S.g.d;
+    for (int c = 0; c < 3; c++) {
+        real *U = u->c[c];
+        const real *A = S.u_n.c[c], *B = S.u_np1.c[c];
+#pragma omp parallel for schedule(static)
+        for (long p = 0; p < d->ntot; p++) U[p] = ((real)1.0 - ct) * A[p] + ct * B[p];
+    }
+}
+
+static void integrate_lp(lp_t *lp, real *t, real dt) {
+    const sgrid_t *g = &S.g;
+    int np = lp->np;
+    const real HALF = (real)1.0 / (real)2.0, THIRD = (real)1.0 / (real)3.0, TWOTHIRD = (real)2.0 / (real)3.0,
+               SIXTH = (real)1.0 / (real)6.0, TWO = (real)2.0;
+    sr1_t u;
+    sr1_alloc(&u, &g->d);
+    real *xn[3], *k[3] = {0, 0, 0}, *xnp1[3] = {0, 0, 0};
+    for (int c = 0; c < 3; c++) {
+        xn[c] = zalloc(np);
+        memcpy(xn[c], lp->xp[c], sizeof(real) * (size_t)np);
+        if (S.integrator == RK3 || S.integrator == RK4) {
+            k[c] = zalloc(np);
+            xnp1[c] = zalloc(np);
+        }
+    }
+    real t0 = S.t_n, t1 = S.t_np1, tt = *t;
+    real **X = lp->xp, **U = lp->up;
+    int *const *no = lp->no_scfd;
+#define STAGE(ctv)                                   \
+    do {                                             \
+        blend(&u, (ctv));                            \
+        interp_r1(g, S.interpolator, np, X, no, &u, U); \
+    } while (0)
+    switch (S.integrator) {
+    case EULER:
+        STAGE(stage_ct(tt, t0, t1));
+        for (int c = 0; c < 3; c++)
+            for (int ip = 0; ip < np; ip++) X[c][ip] = X[c][ip] + dt * U[c][ip];
+        break;
+    case TRAPEZOIDAL:
+        STAGE(stage_ct(tt + HALF * dt, t0, t1));
+        for (int c = 0; c < 3; c++)
+            for (int ip = 0; ip < np; ip++) X[c][ip] = X[c][ip] + dt * U[c][ip];
+        break;
+    case RK2:
+        STAGE(stage_ct(tt, t0, t1));
+        for (int c = 0; c < 3; c++)
+            for (int ip = 0; ip < np; ip++) X[c][ip] = X[c][ip] + HALF * dt * U[c][ip];
+        STAGE(stage_ct(tt + HALF * dt, t0, t1));
+        for (int c = 0; c < 3; c++)
+            for (int ip = 0; ip < np; ip++) X[c][ip] = xn[c][ip] + dt * U[c][ip];
+        break;
+    case RK3:
+        for (int c = 0; c < 3; c++) memcpy(xnp1[c], xn[c], sizeof(real) * (size_t)np);
+        STAGE(stage_ct(tt, t0, t1));
+        for (int c = 0; c < 3; c++)
+            for (int ip = 0; ip < np; ip++) {
+                k[c][ip] = dt * U[c][ip];
+                xnp1[c][ip] = xnp1[c][ip] + SIXTH * k[c][ip];
+            }
+        /* stage 2 at xn + k1/2; the position set to xn - k1 at :239-241 is overwritten
+         * before use, so stage 3 is evaluated at xn + 2*k2 (:245-247) */
+        blend(&u, stage_ct(tt + HALF * dt, t0, t1));
+        for (int c = 0; c < 3; c++)
+            for (int ip = 0; ip < np; ip++) X[c][ip] = xn[c][ip] + HALF * k[c][ip];
+        interp_r1(g, S.interpolator, np, X, no, &u, U);
+        for (int c = 0; c < 3; c++)
+            for (int ip = 0; ip < np; ip++) {
+                k[c][ip] = dt * U[c][ip];
+                X[c][ip] = xn[c][ip] + TWO * k[c][ip];
+                xnp1[c][ip] = xnp1[c][ip] + TWOTHIRD * k[c][ip];
+            }
+        STAGE(stage_ct(tt + dt, t0, t1));
+        for (int c = 0; c < 3; c++)
+            for (int ip = 0; ip < np; ip++) {
+                k[c][ip] = dt * U[c][ip];
+                X[c][ip] = xnp1[c][ip] + SIXTH * k[c][ip];
+            }
+        break;
+    case RK4:
+        for (int c = 0; c < 3; c++) memcpy(xnp1[c], xn[c], sizeof(real) * (size_t)np);
+        STAGE(stage_ct(tt, t0, t1));
+        for (int c = 0; c < 3; c++)
+            for (int ip = 0; ip < np; ip++) {
+                k[c][ip] = dt * U[c][ip];
+                xnp1[c][ip] = xnp1[c][ip] + SIXTH * k[c][ip];
+            }
+        blend(&u, stage_ct(tt + HALF * dt, t0, t1));
+        for (int c = 0; c < 3; c++)
+            for (int ip = 0; ip < np; ip++) X[c][ip] = xn[c][ip] + HALF * k[c][ip];
+        interp_r1(g, S.interpolator, np, X, no, &u, U);
+        for (int c = 0; c < 3; c++)
+            for (int ip = 0; ip < np; ip++) {
+                k[c][ip] = dt * U[c][ip];
+                xnp1[c][ip] = xnp1[c][ip] + THIRD * k[c][ip];
+            }
+        blend(&u, stage_ct(tt + HALF * dt, t0, t1));
+        for (int c = 0; c < 3; c++)
+            for (int ip = 0; ip < np; ip++) X[c][ip] = xn[c][ip] + HALF * k[c][ip];
+        interp_r1(g, S.interpolator, np, X, no, &u, U);
+        for (int c = 0; c < 3; c++)
+            for (int ip = 0; ip < np; ip++) {
+                k[c][ip] = dt * U[c][ip];
+                xnp1[c][ip] = xnp1[c][ip] + THIRD * k[c][ip];
+            }
+        blend(&u, stage_ct(tt + dt, t0, t1));
+        for (int c = 0; c < 3; c++)
+            for (int ip = 0; ip < np; ip++) X[c][ip] = xn[c][ip] + k[c][ip];
+        interp_r1(g, S.interpolator, np, X, no, &u, U);
+        for (int c = 0; c < 3; c++)
+            for (int ip = 0; ip < np; ip++) {
+                k[c][ip] = dt * U[c][ip];
+                X[c][ip] = xnp1[c][ip] + SIXTH * k[c][ip];
+            }
+        break;
+    default:
+        latch("integrate_lp: unknown integrator");
+    }
+#undef STAGE
+    *t = tt + dt;
+    project_lp2plane(g, lp, lp->no_scfd);
+    set_lp_bc(g, lp, lp->no_scfd);
+    for (int ip = 0; ip < np; ip++)
+        if (lp->flag[ip] == LP_STICK)
+            for (int c = 0; c < 3; c++) X[c][ip] = xn[c][ip];
+    for (int c = 0; c < 3; c++)
+        for (int ip = 0; ip < np; ip++) lp->dx[c][ip] = lp->dx[c][ip] + (X[c][ip] - xn[c][ip]);
+    for (int c = 0; c < 3; c++) {
+        free(xn[c]); free(k[c]); free(xnp1[c]);
+    }
+    sr1_free(&u);
+}
+
+/* set_dt, lp_motion_m.f90:56-127 */
+static int set_dt(const lp_t *lp, real *dt) {
+    const dims_t *d = &S.g.d;
+    real dt_f = S.t_np1 - S.t_n;
+    real mx = -R_HUGE;
+    int nan = 0;
+    for (int k = 1; k <= d->nk; k++)
+        for (int j = 1; j <= d->nj; j++)
+            for (int i = 1; i <= d->ni; i++) {
+                long p = PX(d, i, j, k);
+                real c = 0;
+                c = c + (real)fabs(S.u_np1.c[0][p] * S.delta.c[0][p]);
+                c = c + (real)fabs(S.u_np1.c[1][p] * S.delta.c[1][p]);
+                c = c + (real)fabs(S.u_np1.c[2][p] * S.delta.c[2][p]);
+                c = c * dt_f;
+                if (c != c) nan = 1;
+                mx = rmax(mx, c);
+            }
+    if (nan) {
+        latch("set_dt: non-finite velocity");
+        return 1;
+    }
+    double q = ceil((double)(mx / (S.cfl_max * lp->dt_factor)));
+    int nsub = (int)q;
+    if (nsub < 1) nsub = 1;
+    *dt = dt_f / (real)nsub;
+    if (lp->direction == BKWD) *dt = (real)-1.0 * *dt;
+    if (fabs(*dt) > 0) {
+        if (lp->direction == FWD) S.integrations_fwd += (long long)lp->np * nsub;
+        else S.integrations_bkwd += (long long)lp->np * nsub;
+    }
+    return nsub;
+}
+
+/* ------------------------------------------------------------------------------------
+ * Node tracking with the one-rank periodic wrap of exchange_lpdata:
+ * track_lp2node lp_tracking_m.f90:16-183, exchange_lpdata comms_m.f90:872-1189.
+ * A recursive search repeats single passes until nothing moves (every particle is
+ * independent, so "until this particle stops moving" is the same thing); the
+ * reference gives up after 2*max(gn) passes (:127-142).
+ * ------------------------------------------------------------------------------------ */
+static int track_one_pass(const sgrid_t *g, const real *pos, int *node) {
+    const dims_t *d = &g->d;
+    real best = R_HUGE;
+    int off[3] = {0, 0, 0};
+    for (int nb = 0; nb < 27; nb++) {
+        if (g->gn[0] == 1 && NBR[nb][0] != 0) continue;
+        if (g->gn[1] == 1 && NBR[nb][1] != 0) continue;
+        if (g->gn[2] == 1 && NBR[nb][2] != 0) continue;
+        int i = clampi(node[0] + NBR[nb][0], 0, d->ni + 1);
+        int j = clampi(node[1] + NBR[nb][1], 0, d->nj + 1);
+        int k = clampi(node[2] + NBR[nb][2], 0, d->nk + 1);
+        long p = PX(d, i, j, k);
+        real ex = g->grid.c[0][p] - pos[0], ey = g->grid.c[1][p] - pos[1], ez = g->grid.c[2][p] - pos[2];
+        real r = +ex * ex + ey * ey + ez * ez;
+        if (r < (real)0.99 * best) {
+            best = r;
+            off[0] = NBR[nb][0]; off[1] = NBR[nb][1]; off[2] = NBR[nb][2];
+        }
+    }
+    node[0] += off[0]; node[1] += off[1]; node[2] += off[2];
+    return off[0] != 0 || off[1] != 0 || off[2] != 0;
+}
+
+static void wrap_lpdata(const sgrid_t *g, lp_t *lp, int ip, int *const *no) {
+    const dims_t *d = &g->d;
+    int n[3] = {d->ni, d->nj, d->nk};
+    int cf[3];
+    for (int a = 0; a < 3; a++) cf[a] = no[a][ip] < 1 ? -1 : (no[a][ip] > n[a] ? 1 : 0);
+    if (cf[0] == 0 && cf[1] == 0 && cf[2] == 0) return;
+    if (g->scomm_flag[cf[2] + 1][cf[1] + 1][cf[0] + 1] == NO_COMM) return;
+    for (int a = 0; a < 3; a++) lp->xp[a][ip] = lp->xp[a][ip] + g->ps[cf[2] + 1][cf[1] + 1][cf[0] + 1][a];
+    for (int a = 0; a < 3; a++) {
+        int v = lp->no[a][ip];
+        if (v > g->gn[a]) v -= g->gn[a];
+        if (v < 1) v += g->gn[a];
+        lp->no[a][ip] = v;
+        v = lp->no_scfd[a][ip];
+        if (v > g->gn[a]) v -= g->gn[a];
+        if (v < 1) v += g->gn[a];
+        lp->no_scfd[a][ip] = v;
+    }
+    lp->flag[ip] = LP_IB;
+}
+
+static void track_lp2node(const sgrid_t *g, lp_t *lp, int *const *no) {
+    int recursive = lp->recursive_tracking;
+    int maxtrack = 2 * imax(imax(g->gn[0], g->gn[1]), g->gn[2]);
+    int fail = 0;
+#pragma omp parallel for schedule(dynamic, 4096) reduction(| : fail)
+    for (int ip = 0; ip < lp->np; ip++) {
+        int passes = 0;
+        while (1) {
+            real pos[3] = {lp->xp[0][ip], lp->xp[1][ip], lp->xp[2][ip]};
+            int node[3] = {no[0][ip], no[1][ip], no[2][ip]};
+            int moved = track_one_pass(g, pos, node);
+            no[0][ip] = node[0]; no[1][ip] = node[1]; no[2][ip] = node[2];
+            passes++;
+            if (recursive && passes > maxtrack) { fail = 1; break; }
+            if (lp->direction == FWD) wrap_lpdata(g, lp, ip, no);
+            if (!recursive || !moved) break;
+        }
+    }
+    if (fail) latch("track_lp2node: cannot locate all particles");
+    lp->recursive_tracking = 0;
+}
+
+/* ------------------------------------------------------------------------------------
+ * Backward SL flow-map update, flowmap_m.f90:17-104
+ * ------------------------------------------------------------------------------------ */
+static void update_flowmap_sl(lp_t *lp) {
+    const sgrid_t *g = &S.g;
+    const dims_t *d = &g->d;
+    int np = lp->np;
+    real dt;
+    int nsub = set_dt(lp, &dt);
+    if (S.error) return;
+    S.last_nsub_bkwd = nsub;
+    real *lpgrid[3], *fmp[3], *mask = zalloc(np);
+    for (int c = 0; c < 3; c++) {
+        lpgrid[c] = zalloc(np);
+        fmp[c] = zalloc(np);
+        memcpy(lpgrid[c], lp->xp[c], sizeof(real) * (size_t)np);
+    }
+    for (int ip = 0; ip < np; ip++)
+        if (g->bcflag[PX(d, lp->no_scfd[0][ip], lp->no_scfd[1][ip], lp->no_scfd[2][ip])] != LCS_MASK) mask[ip] = (real)1.0;
+    real lp_time = S.t_np1;
+    for (int sc = 1; sc <= nsub && !S.error; sc++) {
+        integrate_lp(lp, &lp_time, dt);
+        interp_r1(g, S.interpolator, np, lp->xp, lp->no, &lp->fm, fmp);
+        for (int ip = 0; ip < np; ip++) {
+            long p = PX(d, lp->no[0][ip], lp->no[1][ip], lp->no[2][ip]);
+            for (int c = 0; c < 3; c++) lp->fm.c[c][p] = (fmp[c][ip] + (lp->xp[c][ip] - lpgrid[c][ip])) * mask[ip];
+        }
+        pad_flowmap(g, &lp->fm);
+        for (int c = 0; c < 3; c++) memcpy(lp->xp[c], lpgrid[c], sizeof(real) * (size_t)np);
+    }
+    for (int c = 0; c < 3; c++) { free(lpgrid[c]); free(fmp[c]); }
+    free(mask);
+}
+
+/* Forward particle update, lp_motion_m.f90:15-54 */
+static void update_lp(lp_t *lp) {
+    real dt;
+    int nsub = set_dt(lp, &dt);
+    if (S.error) return;
+    S.last_nsub_fwd = nsub;
+    real lp_time = S.t_n;
+    for (int sc = 1; sc <= nsub && !S.error; sc++) {
+        integrate_lp(lp, &lp_time, dt);
+        track_lp2node(&S.g, lp, lp->no_scfd);
+    }
+}
+
+/* ------------------------------------------------------------------------------------
+ * Sub-flow-map ring and composition: write_flowmap_substep flowmap_m.f90:106-156,
+ * reconstruct_flowmap :158-323, exchange_lp_alltoall comms_m.f90:1378-1709,
+ * exchange_lpmap comms_m.f90:1191-1376.
+ * ------------------------------------------------------------------------------------ */
+static int ring_step(real t, real T, real h) {
+    real m = (real)fmod((double)t, (double)T);
+    return fnint(m / h);
+}
+
+static void write_substep(lcs_t *L) {
+    const dims_t *d = &S.g.d;
+    int step = ring_step(S.t_np1, L->T, L->h);
+    /* slot nint(T/h) (and negative slots) are written to files that reconstruct never
+     * reads back (it wraps step into [0, nstep-1] before reading) */
+    if (step < 0 || step >= L->nslot) return;
+    for (int c = 0; c < 3; c++) {
+        real *s = L->slot[c][step];
+        long q = 0;
+        for (int k = 1; k <= d->nk; k++)
+            for (int j = 1; j <= d->nj; j++)
+                for (int i = 1; i <= d->ni; i++) s[q++] = L->lp.fm.c[c][PX(d, i, j, k)];
+    }
+    L->written[step] = 1;
+}
+
+static void alltoall_wrap(const sgrid_t *g, lp_t *lp, int ip) {
+    const dims_t *d = &g->d;
+    real *x = &lp->xp[0][ip], *y = &lp->xp[1][ip], *z = &lp->xp[2][ip];
+    const real *bb = g->bb;
+    int inside = *x >= bb[0] && *x <= bb[3] && *y >= bb[1] && *y <= bb[4] && *z >= bb[2] && *z <= bb[5];
+    if (!inside) {
+        for (int kk = -1; kk <= 1 && !inside; kk++)
+            for (int jj = -1; jj <= 1 && !inside; jj++)
+                for (int ii = -1; ii <= 1 && !inside; ii++) {
+                    const real *s = g->ps[kk + 1][jj + 1][ii + 1];
+                    if (*x - s[0] >= bb[0] && *x - s[0] <= bb[3] && *y - s[1] >= bb[1] && *y - s[1] <= bb[4] && *z - s[2] >= bb[2] &&
+                        *z - s[2] <= bb[5]) {
+                        *x = *x - s[0]; *y = *y - s[1]; *z = *z - s[2];
+                        inside = 1;
+                    }
+                }
+    }
+    lp->up[0][ip] = lp->up[1][ip] = lp->up[2][ip] = 0;
+    real s = rmax(rmin((*x - bb[0]) / (bb[3] - bb[0]), (real)1.0), (real)0.0);
+    real t = rmax(rmin((*y - bb[1]) / (bb[4] - bb[1]), (real)1.0), (real)0.0);
+    real u = rmax(rmin((*z - bb[2]) / (bb[5] - bb[2]), (real)1.0), (real)0.0);
+    /* nint(real(ni)*s): real(ni) is a default (single precision) real */
+    lp->no[0][ip] = clampi(fnint((real)((float)d->ni) * s), 1, d->ni);
+    lp->no[1][ip] = clampi(fnint((real)((float)d->nj) * t), 1, d->nj);
+    lp->no[2][ip] = clampi(fnint((real)((float)d->nk) * u), 1, d->nk);
+    lp->flag[ip] = LP_UNKNOWN;
+}
+
+static int reconstruct(lcs_t *L) {
+    const sgrid_t *g = &S.g;
+    const dims_t *d = &g->d;
+    lp_t *lp = &L->lp;
+    int np = lp->np;
+    reset_lp(g, lp, 1);
+    int step = ring_step(S.t_np1, L->T, L->h);
+    int nstep = fnint(L->T / L->h);
+    int inc;
+    if (lp->direction == FWD) {
+        inc = 1;
+        step = step + inc;
+    } else {
+        inc = -1;
+    }
+    int saved_dir = lp->direction;
+    lp->direction = FWD;
+    int success = 1;
+    for (int i = 1; i <= nstep && !S.error; i++) {
+        if (step >= nstep) step = 0;
+        if (step < 0) step = nstep - 1;
+        if (step >= L->nslot || !L->written[step]) {
+            step = step + inc;
+            success = 0;
+            continue;
+        }
+        for (int c = 0; c < 3; c++) {
+            const real *s = L->slot[c][step];
+            long q = 0;
+            for (int k = 1; k <= d->nk; k++)
+                for (int j = 1; j <= d->nj; j++)
+                    for (int ii = 1; ii <= d->ni; ii++) lp->fm.c[c][PX(d, ii, j, k)] = s[q++];
+        }
+        pad_flowmap(g, &lp->fm);
+        project_lp2plane(g, lp, lp->no);
+        set_lp_bc(g, lp, lp->no);
+        interp_r1(g, S.interpolator, np, lp->xp, lp->no, &lp->fm, lp->up);
+        for (int c = 0; c < 3; c++)
+            for (int ip = 0; ip < np; ip++) {
+                lp->xp[c][ip] = lp->xp[c][ip] + lp->up[c][ip];
+                lp->dx[c][ip] = lp->dx[c][ip] + lp->up[c][ip];
+            }
+        for (int ip = 0; ip < np; ip++) alltoall_wrap(g, lp, ip);
+        lp->recursive_tracking = 1;
+        track_lp2node(g, lp, lp->no);
+        step = step + inc;
+    }
+    /* exchange_lpmap: fm(no0) = dx; particle order equals origin order on one rank */
+    {
+        int ip = 0;
+        for (int k = 1; k <= d->nk; k++)
+            for (int j = 1; j <= d->nj; j++)
+                for (int ii = 1; ii <= d->ni; ii++, ip++)
+                    for (int c = 0; c < 3; c++) lp->fm.c[c][PX(d, ii, j, k)] = lp->dx[c][ip];
+    }
+    pad_flowmap(g, &lp->fm);
+    lp->direction = saved_dir;
+    return success;
+}
+
+/* ------------------------------------------------------------------------------------
+ * FTLE: compute_ftle lcs_m.f90:66-193 with grad_sr1 gradient_m.f90:11-66.  The eigen
+ * solve replaces LAPACK DSYEV/SSYEV by cyclic Jacobi in long double (largest eigenvalue).
+ * ------------------------------------------------------------------------------------ */
+static long double eig3_max(const long double A_in[3][3]) {
+    long double a[3][3];
+    memcpy(a, A_in, sizeof(a));
+    for (int sweep = 0; sweep < 64; sweep++) {
+        long double off = fabsl(a[0][1]) + fabsl(a[0][2]) + fabsl(a[1][2]);
+        long double diag = fabsl(a[0][0]) + fabsl(a[1][1]) + fabsl(a[2][2]);
+        if (off == 0 || off <= 1e-30L * diag) break;
+        for (int p = 0; p < 2; p++)
+            for (int q = p + 1; q < 3; q++) {
+                if (a[p][q] == 0) continue;
+                long double theta = (a[q][q] - a[p][p]) / (2 * a[p][q]);
+                long double tt = (theta >= 0 ? 1 : -1) / (fabsl(theta) + sqrtl(theta * theta + 1));
+                long double c = 1 / sqrtl(tt * tt + 1), s = tt * c;
+                for (int r = 0; r < 3; r++) {
+                    long double arp = a[r][p], arq = a[r][q];
+                    a[r][p] = c * arp - s * arq;
+                    a[r][q] = s * arp + c * arq;
+                }
+                for (int r = 0; r < 3; r++) {
+                    long double apr = a[p][r], aqr = a[q][r];
+                    a[p][r] = c * apr - s * aqr;
+                    a[q][r] = s * apr + c * aqr;
+                }
+            }
+    }
+    long double m = a[0][0];
+    if (a[1][1] > m) m = a[1][1];
+    if (a[2][2] > m) m = a[2][2];
+    return m;
+}
+
+static void compute_ftle(lcs_t *L) {
+    const sgrid_t *g = &S.g;
+    const dims_t *d = &g->d;
+    sr1_t *fm = &L->lp.fm;
+    exchange_self(g, fm->c, 3, 0, 0); /* scomm_face_r1 */
+    const real *X = g->grid.c[0], *Y = g->grid.c[1], *Z = g->grid.c[2];
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 1; k <= d->nk; k++)
+        for (int j = 1; j <= d->nj; j++)
+            for (int i = 1; i <= d->ni; i++) {
+                long p = PX(d, i, j, k);
+                long pxp = PX(d, i + 1, j, k), pxm = PX(d, i - 1, j, k);
+                long pyp = PX(d, i, j + 1, k), pym = PX(d, i, j - 1, k);
+                long pzp = PX(d, i, j, k + 1), pzm = PX(d, i, j, k - 1);
+                real G[3][3]; /* G[c][a] = d fm_c / d x_a */
+                for (int c = 0; c < 3; c++) {
+                    const real *F = fm->c[c];
+                    G[c][0] = (F[pxp] - F[pxm]) / (X[pxp] - X[pxm]);
+                    G[c][1] = (F[pyp] - F[pym]) / (Y[pyp] - Y[pym]);
+                    G[c][2] = (F[pzp] - F[pzm]) / (Z[pzp] - Z[pzm]);
+                }
+                for (int a = 0; a < 3; a++)
+                    if (g->gn[a] == 1)
+                        for (int c = 0; c < 3; c++) G[c][a] = 0;
+                /* cg_ab = sum_c G[c][a]*G[c][b], lcs_m.f90:137-145 */
+                real C[3][3];
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) C[a][b] = G[0][a] * G[0][b] + G[1][a] * G[1][b] + G[2][a] * G[2][b];
+                long double A[3][3];
+                /* DSYEV('V','U') reads the upper triangle */
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) A[a][b] = (long double)(a <= b ? C[a][b] : C[b][a]);
+                real lam = (real)eig3_max(A);
+                real sq = (real)sqrt((double)lam);
+                /* max(sqrt(W3), tiny): a NaN from a rounding-negative W3 yields tiny */
+                real mxv = (sq > R_TINY) ? sq : R_TINY;
+                real v = (real)log((double)mxv) / L->T;
+                if (S.incompressible) v = rmax(v, (real)0.0);
+                L->ftle[p] = v;
+            }
+}
+
+/* ------------------------------------------------------------------------------------
+ * Entry points (cfd2lcs.f90:2-682 semantics, one rank, no output files).
+ * ------------------------------------------------------------------------------------ */
+#define EXPORT __attribute__((visibility("default")))
+
+EXPORT int orc_real_size(void) { return (int)sizeof(real); }
+EXPORT int orc_error(void) { return S.error; }
+EXPORT const char *orc_error_msg(void) { return S.msg; }
+EXPORT void orc_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+EXPORT int orc_get_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+static void free_lcs(lcs_t *L) {
+    if (!L) return;
+    for (int c = 0; c < 3; c++) {
+        free(L->lp.xp[c]); free(L->lp.up[c]); free(L->lp.dx[c]);
+        free(L->lp.no[c]); free(L->lp.no_scfd[c]);
+        if (L->slot[c]) {
+            for (int s = 0; s < L->nslot; s++) free(L->slot[c][s]);
+            free(L->slot[c]);
+        }
+    }
+    free(L->lp.flag);
+    sr1_free(&L->lp.fm);
+    sr1_free(&L->fm_out);
+    free(L->ftle);
+    free(L->written);
+    free(L);
+}
+
+/* Resets all state, including the error latch (a fresh process for the reference). */
+EXPORT void orc_reset(void) {
+    for (int i = 0; i < S.nlcs; i++) free_lcs(S.lcs[i]);
+    if (S.inited) {
+        sr1_free(&S.g.grid); sr1_free(&S.g.bcnorm); free(S.g.bcflag);
+        sr1_free(&S.u_n); sr1_free(&S.u_np1); sr1_free(&S.delta);
+    }
+    memset(&S, 0, sizeof(S));
+    S.integrator = RK2;
+    S.interpolator = LINEAR;
+    S.cfl_max = (real)0.5;
+}
+
+/* cfd2lcs_init, cfd2lcs.f90:2-53 */
+EXPORT void orc_init(const int n[3], const int offset[3], const real *x, const real *y, const real *z, const int *flag) {
+    (void)offset; /* one rank: offsets are normalised to 0 (sgrid_m.f90:90-93) */
+    if (S.error) return;
+    if (S.inited) orc_reset();
+    S.nlcs = 0;
+    S.integrations_fwd = S.integrations_bkwd = 0;
+    if (init_sgrid(&S.g, n, x, y, z, flag)) return;
+    if (!S.g.rectilinear) {
+        latch("init: grid is not rectilinear (the TSE/least-squares path is not restated)");
+        return;
+    }
+    sr1_alloc(&S.u_n, &S.g.d);
+    sr1_alloc(&S.u_np1, &S.g.d);
+    compute_delta(&S.g, &S.delta);
+    S.first_call = 1;
+    S.inited = 1;
+}
+
+/* cfd2lcs_diagnostic_init, cfd2lcs.f90:252-358 with init_ftle lcs_m.f90:16-64 */
+EXPORT int orc_diagnostic_init(int type, int resolution, real T, real h, const char *label) {
+    (void)label;
+    if (S.error) return -1;
+    if (!S.inited) { latch("diagnostic_init before init"); return -1; }
+    if (S.nlcs >= MAXLCS) { latch("diagnostic_init: too many diagnostics"); return -1; }
+    if (resolution != 0) { latch("diagnostic_init: resolution /= 0 (new_sgrid_from_sgrid) is not restated"); return -1; }
+    if (type != FTLE_FWD && type != FTLE_BKWD) {
+        latch("diagnostic_init: bad lcs_type (LP_TRACER is not restated)");
+        return -1;
+    }
+    lcs_t *L = (lcs_t *)calloc(1, sizeof(lcs_t));
+    L->id = S.nlcs + 1;
+    L->diagnostic = type;
+    L->T = T;
+    L->h = h;
+    const dims_t *d = &S.g.d;
+    L->ftle = zalloc(d->ntot);
+    lp_alloc(&L->lp, d->ni * d->nj * d->nk);
+    sr1_alloc(&L->lp.fm, d);
+    sr1_alloc(&L->fm_out, d);
+    L->lp.direction = type == FTLE_BKWD ? BKWD : FWD;
+    L->lp.dt_factor = type == FTLE_BKWD ? (real)1.0 / (real)imax(1 + resolution, 1) : (real)1.0;
+    reset_lp(&S.g, &L->lp, 1);
+    track_lp2node(&S.g, &L->lp, L->lp.no_scfd);
+    L->nslot = fnint(T / h);
+    if (L->nslot < 1) L->nslot = 1;
+    L->written = (int *)calloc((size_t)L->nslot, sizeof(int));
+    long nint_ = (long)d->ni * d->nj * d->nk;
+    for (int c = 0; c < 3; c++) {
+        L->slot[c] = (real **)calloc((size_t)L->nslot, sizeof(real *));
+        for (int s = 0; s < L->nslot; s++) L->slot[c][s] = zalloc(nint_);
+    }
+    S.lcs[S.nlcs++] = L;
+    return L->id;
+}
+
+/* cfd2lcs_update, cfd2lcs.f90:55-250 */
+EXPORT void orc_update(const int n[3], const real *u, const real *v, const real *w, real time) {
+    if (S.error) return;
+    if (!S.inited) { latch("update before init"); return; }
+    const dims_t *d = &S.g.d;
+    if (n[0] != d->ni || n[1] != d->nj || n[2] != d->nk) {
+        latch("update: velocity array of incorrect dimension");
+        return;
+    }
+    if (S.first_call) {
+        S.t_n = time;
+        S.t_np1 = time;
+        S.first_call = 0;
+    } else {
+        S.t_n = S.t_np1;
+        S.t_np1 = time;
+    }
+    for (int c = 0; c < 3; c++) memcpy(S.u_n.c[c], S.u_np1.c[c], sizeof(real) * (size_t)d->ntot);
+    const real *src[3] = {u, v, w};
+    for (int k = 1; k <= d->nk; k++)
+        for (int j = 1; j <= d->nj; j++)
+            for (int i = 1; i <= d->ni; i++) {
+                long s = (i - 1) + (long)d->ni * ((j - 1) + (long)d->nj * (k - 1));
+                for (int c = 0; c < 3; c++) S.u_np1.c[c][PX(d, i, j, k)] = src[c][s];
+            }
+    exchange_self(&S.g, S.u_np1.c, 3, 1, 0);
+    set_velocity_bc(&S.g, &S.u_np1);
+    for (int i = 0; i < S.nlcs && !S.error; i++) {
+        lp_t *lp = &S.lcs[i]->lp;
+        if (lp->direction == FWD) update_lp(lp);
+        else update_flowmap_sl(lp);
+    }
+    for (int i = 0; i < S.nlcs && !S.error; i++) {
+        lcs_t *L = S.lcs[i];
+        if ((long long)(S.t_np1 / L->h) == (long long)(S.t_n / L->h)) continue;
+        if (L->diagnostic == FTLE_FWD) {
+            /* exchange_lpmap: fm(no0) = dx */
+            int ip = 0;
+            for (int k = 1; k <= d->nk; k++)
+                for (int j = 1; j <= d->nj; j++)
+                    for (int ii = 1; ii <= d->ni; ii++, ip++)
+                        for (int c = 0; c < 3; c++) L->lp.fm.c[c][PX(d, ii, j, k)] = L->lp.dx[c][ip];
+        }
+        write_substep(L);
+        reconstruct(L);
+        compute_ftle(L);
+        for (int c = 0; c < 3; c++) memcpy(L->fm_out.c[c], L->lp.fm.c[c], sizeof(real) * (size_t)d->ntot);
+        S.ftle_frames++;
+        reset_lp(&S.g, &L->lp, 1);
+        track_lp2node(&S.g, &L->lp, L->lp.no_scfd);
+    }
+}
+
+/* cfd2lcs_set_option, cfd2lcs.f90:436-622 */
+EXPORT void orc_set_option(const char *opt, int val) {
+    if (S.error) return;
+    int ok = 1;
+    int tf = (val == LCS_TRUE || val == LCS_FALSE);
+    if (!strcmp(opt, "SYNCTIMER") || !strcmp(opt, "DEBUG") || !strcmp(opt, "WRITE_FLOWMAP") || !strcmp(opt, "WRITE_VELOCITY") ||
+        !strcmp(opt, "WRITE_BCFLAG")) {
+        ok = tf;
+    } else if (!strcmp(opt, "VELOCITY_INVARIANTS")) {
+        ok = tf;
+        if (ok) S.velocity_invariants = val;
+    } else if (!strcmp(opt, "INCOMPRESSIBLE")) {
+        ok = tf;
+        if (ok) S.incompressible = val;
+    } else if (!strcmp(opt, "AUX_GRID")) {
+        ok = tf;
+        if (ok) S.aux_grid = val;
+    } else if (!strcmp(opt, "UPDATE_FREQ")) {
+        ok = 1;
+    } else if (!strcmp(opt, "INTERPOLATOR")) {
+        ok = val == NEAREST_NBR || val == LINEAR || val == QUADRATIC || val == CUBIC || val == TSE || val == TSE_LIMIT;
+        S.interpolator = val; /* assigned even when the value is bad (cfd2lcs.f90:584) */
+    } else if (!strcmp(opt, "INTEGRATOR")) {
+        ok = val >= EULER && val <= RK4;
+        S.integrator = val;
+    } else {
+        ok = 0;
+    }
+    if (!ok) latch("bad libcfd2lcs option/val combination");
+}
+
+/* cfd2lcs_set_param, cfd2lcs.f90:624-682 */
+EXPORT void orc_set_param(const char *p, real val) {
+    if (S.error) return;
+    if (!strcmp(p, "CFL")) S.cfl_max = val;
+    else if (!strcmp(p, "TRACER_INJECT_X") || !strcmp(p, "TRACER_INJECT_Y") || !strcmp(p, "TRACER_INJECT_Z") ||
+             !strcmp(p, "TRACER_INJECT_RADIUS")) {
+    } else latch("unknown libcfd2lcs parameter");
+}
+
+static lcs_t *find_lcs(int handle) {
+    for (int i = 0; i < S.nlcs; i++)
+        if (S.lcs[i]->id == handle) return S.lcs[i];
+    return NULL;
+}
+
+/* FTLE field of a diagnostic, interior points, i fastest */
+EXPORT int orc_get_ftle(int handle, real *out) {
+    lcs_t *L = find_lcs(handle);
+    if (!L) return 1;
+    const dims_t *d = &S.g.d;
+    long q = 0;
+    for (int k = 1; k <= d->nk; k++)
+        for (int j = 1; j <= d->nj; j++)
+            for (int i = 1; i <= d->ni; i++) out[q++] = L->ftle[PX(d, i, j, k)];
+    return 0;
+}
+
+/* Flow map (3 x interior, component-major) of a diagnostic: which = 0 the working
+ * (sub-)flow map as currently stored, which = 1 the composed map of the last FTLE frame */
+EXPORT int orc_get_fm(int handle, real *out, int which) {
+    lcs_t *L = find_lcs(handle);
+    if (!L) return 1;
+    const dims_t *d = &S.g.d;
+    const sr1_t *f = which ? &L->fm_out : &L->lp.fm;
+    long q = 0;
+    for (int c = 0; c < 3; c++)
+        for (int k = 1; k <= d->nk; k++)
+            for (int j = 1; j <= d->nj; j++)
+                for (int i = 1; i <= d->ni; i++) out[q++] = f->c[c][PX(d, i, j, k)];
+    return 0;
+}
+
+/* Forward particle positions (3 x np) of a diagnostic */
+EXPORT int orc_get_particles(int handle, real *out) {
+    lcs_t *L = find_lcs(handle);
+    if (!L) return 1;
+    long q = 0;
+    for (int c = 0; c < 3; c++)
+        for (int ip = 0; ip < L->lp.np; ip++) out[q++] = L->lp.xp[c][ip];
+    return 0;
+}
+
+EXPORT long long orc_counter(int which) {
+    switch (which) {
+    case 0: return S.integrations_fwd;
+    case 1: return S.integrations_bkwd;
+    case 2: return S.last_nsub_fwd;
+    case 3: return S.last_nsub_bkwd;
+    case 4: return S.ftle_frames;
+    default: return -1;
+    }
+}
+
+/* Grid-derived quantities for host-logic tests: padded grid coordinates (3 x ntot),
+ * padded bcflag (ntot), bcnorm (3 x ntot), inverse deltas (3 x ntot), periodicity. */
+EXPORT long orc_padded_size(void) { return S.inited ? S.g.d.ntot : 0; }
+EXPORT void orc_get_grid(real *xyz, int *flag, real *nrm, real *inv_delta, int *per) {
+    const dims_t *d = &S.g.d;
+    for (int c = 0; c < 3; c++) {
+        if (xyz) memcpy(xyz + c * d->ntot, S.g.grid.c[c], sizeof(real) * (size_t)d->ntot);
+        if (nrm) memcpy(nrm + c * d->ntot, S.g.bcnorm.c[c], sizeof(real) * (size_t)d->ntot);
+        if (inv_delta) memcpy(inv_delta + c * d->ntot, S.delta.c[c], sizeof(real) * (size_t)d->ntot);
+    }
+    if (flag) memcpy(flag, S.g.bcflag, sizeof(int) * (size_t)d->ntot);
+    if (per)
+        for (int a = 0; a < 3; a++) per[a] = S.g.per[a];
+}
+
+/* Unit-level helpers (known-answer tests) */
+EXPORT double orc_eig3_max(const double *a9) {
+    long double A[3][3];
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) A[r][c] = (long double)a9[3 * r + c];
+    return (double)eig3_max(A);
+}
+
+/* Fit a tensor spline of order (kx,ky,kz) to f (nx*ny*nz, x fastest) on lines xg,yg,zg and
+ * evaluate it at npts points (px,py,pz). */
+EXPORT int orc_bspline3(const real *xg, const real *yg, const real *zg, int nx, int ny, int nz, int kx, int ky, int kz, const real *f,
+                        int npts, const real *px, const real *py, const real *pz, real *out) {
+    bsp3_t s;
+    bsp3_setup(&s, xg, yg, zg, nx, ny, nz, kx, ky, kz);
+    if (!s.ax[0].ok || !s.ax[1].ok || !s.ax[2].ok) {
+        bsp3_free(&s);
+        return 1;
+    }
+    bsp3_fit(&s, f);
+    for (int p = 0; p < npts; p++) out[p] = bsp3_eval(&s, px[p], py[p], pz[p]);
+    bsp3_free(&s);
+    return 0;
+}
+
+/* B-spline coefficients of the fit above (nx*ny*nz, x fastest) */
+EXPORT int orc_bspline3_coef(const real *xg, const real *yg, const real *zg, int nx, int ny, int nz, int kx, int ky, int kz, const real *f,
+                             real *coef) {
+    bsp3_t s;
+    bsp3_setup(&s, xg, yg, zg, nx, ny, nz, kx, ky, kz);
+    if (!s.ax[0].ok || !s.ax[1].ok || !s.ax[2].ok) {
+        bsp3_free(&s);
+        return 1;
+    }
+    bsp3_fit(&s, f);
+    memcpy(coef, s.coef, sizeof(real) * (size_t)(nx * ny * nz));
+    bsp3_free(&s);
+    return 0;
+}

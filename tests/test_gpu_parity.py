@@ -1,0 +1,88 @@
+"""Parity of the CUDA path (libcfd2lcs_b200, called through its C ABI) with the oracle
+(the CPU restatement of the reference) on seeded synthetic flows at small sizes.
+
+Tolerances (plain FP64): composed flow map max-abs <= 1e-12 * L (L the domain length),
+FTLE max-abs <= 1e-9 for LINEAR / NEAREST and <= 1e-8 for the B-spline interpolators.
+"""
+import numpy as np
+import pytest
+
+from tests import scenarios as SC
+
+pytestmark = pytest.mark.gpu
+
+FM_TOL_REL = 1e-12
+FTLE_TOL = {0: 1e-9, 1: 1e-9, 2: 1e-8, 3: 1e-8}
+
+
+@pytest.fixture(scope="module")
+def gpu_dp():
+    import libcfd2lcs_b200 as L
+    return L.Cfd2lcs("dp")
+
+
+def _compare(oracle, gpu, case, integrator, interpolator, directions=(SC.FTLE_BKWD, SC.FTLE_FWD), n=None, steps=None):
+    oracle.reset()
+    g, ho = SC.run(oracle, case, directions, integrator, interpolator, n=n, steps=steps)
+    assert oracle.error() == 0, oracle.error_msg()
+    gpu.reset()
+    _, hg = SC.run(gpu, case, directions, integrator, interpolator, n=n, steps=steps)
+    err, msg = gpu.error()
+    assert err == 0, msg
+    L = max(float(np.ptp(g.x)), float(np.ptp(g.y)), float(np.ptp(g.z)), 1e-30)
+    out = {}
+    for d, a, b in zip(directions, ho, hg):
+        fo, fg = oracle.flowmap(a), gpu.flowmap(b)
+        to, tg = oracle.ftle(a), gpu.ftle(b)
+        dfm = float(np.max(np.abs(fo - fg)))
+        dft = float(np.max(np.abs(to - tg)))
+        out[d] = (dfm, dft)
+        assert np.all(np.isfinite(tg))
+        assert dfm <= FM_TOL_REL * L, f"flow map max-abs {dfm:.3e} (dir {d}) > {FM_TOL_REL * L:.3e}"
+        assert dft <= FTLE_TOL[interpolator], f"FTLE max-abs {dft:.3e} (dir {d})"
+    cg, co = gpu.counters(), {k: oracle.counter(k) for k in ("integrations_fwd", "integrations_bkwd", "ftle_frames")}
+    for k in co:
+        assert cg[k] == co[k], (k, cg[k], co[k])
+    return out
+
+
+@pytest.mark.parametrize("integrator", [2, 3])
+def test_double_gyre_linear(oracle_dp, gpu_dp, integrator):
+    _compare(oracle_dp, gpu_dp, "dg", integrator, 1)
+
+
+@pytest.mark.parametrize("integrator", [0, 1, 4])
+def test_double_gyre_other_integrators(oracle_dp, gpu_dp, integrator):
+    _compare(oracle_dp, gpu_dp, "dg", integrator, 1, n=32, steps=20)
+
+
+def test_double_gyre_nearest(oracle_dp, gpu_dp):
+    _compare(oracle_dp, gpu_dp, "dg", 2, 0, n=32, steps=20)
+
+
+@pytest.mark.parametrize("integrator", [2, 3])
+def test_abc_linear(oracle_dp, gpu_dp, integrator):
+    _compare(oracle_dp, gpu_dp, "abc", integrator, 1)
+
+
+@pytest.mark.parametrize("interp", [2, 3])
+def test_abc_spline(oracle_dp, gpu_dp, interp):
+    _compare(oracle_dp, gpu_dp, "abc", 3, interp, n=12, steps=12)
+
+
+def test_abc_unsteady_rk4_cubic(oracle_dp, gpu_dp):
+    _compare(oracle_dp, gpu_dp, "abc_unsteady", 4, 3, n=10, steps=10)
+
+
+def test_double_gyre_cubic(oracle_dp, gpu_dp):
+    _compare(oracle_dp, gpu_dp, "dg", 3, 3, n=32, steps=20)
+
+
+@pytest.mark.parametrize("interp", [1, 3])
+def test_channel_walls_zquirk(oracle_dp, gpu_dp, interp):
+    _compare(oracle_dp, gpu_dp, "channel", 2, interp)
+
+
+@pytest.mark.parametrize("interp", [1, 3])
+def test_mixed_boundary_conditions(oracle_dp, gpu_dp, interp):
+    _compare(oracle_dp, gpu_dp, "mixed_bc", 3, interp)
