@@ -109,7 +109,7 @@ __device__ __forceinline__ void sample_velocity(const DevGrid<T> &g, const Splin
     for (int c = 0; c < 3; c++) out[c] = lin_apply_blend(st, V.un[c], V.unp1[c], omc, ct);
   } else {
     SplineStencil<T> st;
-    if (!spline_stencil(g, sa, x, st)) {
+    if (!spline_stencil(g, sa, x, no, st)) {
       out[0] = out[1] = out[2] = T(0);
       return;
     }
@@ -132,7 +132,7 @@ __device__ __forceinline__ void sample_field(const DevGrid<T> &g, const SplineAx
     for (int c = 0; c < 3; c++) out[c] = lin_apply(st, f[c]);
   } else {
     SplineStencil<T> st;
-    if (!spline_stencil(g, sa, x, st)) {
+    if (!spline_stencil(g, sa, x, no, st)) {
       out[0] = out[1] = out[2] = T(0);
       return;
     }

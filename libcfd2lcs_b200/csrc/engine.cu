@@ -627,9 +627,10 @@ class Engine : public EngineBase {
       if (src[c] != dst[c]) CK(cudaMemcpyAsync(dst[c], src[c], ntot_ * sizeof(T), cudaMemcpyDeviceToDevice, stream_));
       counters_.kernel_launches += 3;
       {
-        const int lines = ny * nz, wpb = 4;
-        const size_t smem = (size_t)wpb * sx * sizeof(T);
-        k_fit_axis_x<T><<<(lines + wpb - 1) / wpb, 32 * wpb, smem, stream_>>>(S.ax[0], dst[c], lines);
+        const int lines = ny * nz;
+        const size_t smem = (size_t)32 * (sx + 1) * sizeof(T);
+        if (smem > 48 * 1024) cudaFuncSetAttribute(k_fit_axis_x<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_fit_axis_x<T><<<(lines + 31) / 32, 32, smem, stream_>>>(S.ax[0], dst[c], lines);
       }
       {
         const dim3 blk(128, 1), grd((sx + 127) / 128, nz);

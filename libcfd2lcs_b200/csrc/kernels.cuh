@@ -393,22 +393,21 @@ __global__ void __launch_bounds__(256) k_fit_axis_yz(SplineAxis<T> A, T *f, int 
   band_solve_line(A, f + ix + (long)io * stride_other, stride_line);
 }
 
+// x-lines: a block stages 32 consecutive lines in shared memory with coalesced loads, then
+// each thread solves its own line there and the block writes them back.
 template <typename T>
-__global__ void __launch_bounds__(128) k_fit_axis_x(SplineAxis<T> A, T *f, int nlines) {
-  // one warp per line; lanes cooperate on loads/stores, lane 0 runs the recurrence in smem
+__global__ void __launch_bounds__(32) k_fit_axis_x(SplineAxis<T> A, T *f, int nlines) {
   extern __shared__ unsigned char smem_raw[];
   T *buf = reinterpret_cast<T *>(smem_raw);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int line = blockIdx.x * (blockDim.x >> 5) + warp;
-  if (line >= nlines) return;
-  const int n = A.n;
-  T *b = buf + (size_t)warp * n;
-  T *src = f + (long)line * n;
-  for (int v = lane; v < n; v += 32) b[v] = src[v];
-  __syncwarp();
-  if (lane == 0) band_solve_line(A, b, 1);
-  __syncwarp();
-  for (int v = lane; v < n; v += 32) src[v] = b[v];
+  const int n = A.n, ld = n + 1;  // odd leading dimension spreads the banks
+  const int line0 = blockIdx.x * 32;
+  const int nl = min(32, nlines - line0);
+  T *src = f + (long)line0 * n;
+  for (int q = threadIdx.x; q < nl * n; q += 32) buf[(q / n) * ld + (q % n)] = src[q];
+  __syncthreads();
+  if (threadIdx.x < nl) band_solve_line(A, buf + threadIdx.x * ld, 1);
+  __syncthreads();
+  for (int q = threadIdx.x; q < nl * n; q += 32) src[q] = buf[(q / n) * ld + (q % n)];
 }
 
 }  // namespace cfd2lcs

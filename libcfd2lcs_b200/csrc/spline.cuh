@@ -38,14 +38,15 @@ struct SplineStencil {
   T b[3][4];   // basis values per axis (only the first k used)
 };
 
-// largest l (1-based) with t(l) <= x, searching l in [lo, hi]; requires t(lo) <= x
+// largest l (1-based) in [lo, hi] with t(l) <= x, walking from a guess (t(lo) <= x holds).
+// Departure points and tracked particles sit within a cell or two of their node, so the
+// walk is short; it is exact for any guess.
 template <typename T>
-__device__ __forceinline__ int knot_interval(const T *t, T x, int lo, int hi) {
-  while (hi > lo) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(t + mid - 1) <= x) lo = mid; else hi = mid - 1;
-  }
-  return lo;
+__device__ __forceinline__ int knot_interval(const T *t, T x, int lo, int hi, int guess) {
+  int l = min(max(guess, lo), hi);
+  while (l < hi && __ldg(t + l) <= x) l++;      // t(l+1) <= x
+  while (l > lo && __ldg(t + l - 1) > x) l--;   // t(l) > x
+  return l;
 }
 
 template <typename T>
@@ -73,9 +74,11 @@ __device__ __forceinline__ void basis_values(const SplineAxis<T> &A, int l, T x,
   }
 }
 
-// Locates x in the padded spline; false where db3val returns 0.
+// Locates x in the padded spline; false where db3val returns 0.  no[] is the padded node
+// the point belongs to (its interval is near no + k - 1).
 template <typename T>
-__device__ __forceinline__ bool spline_stencil(const DevGrid<T> &g, const SplineAxes<T> &S, const T x[3], SplineStencil<T> &st) {
+__device__ __forceinline__ bool spline_stencil(const DevGrid<T> &g, const SplineAxes<T> &S, const T x[3], const int no[3],
+                                               SplineStencil<T> &st) {
   int c0[3];
 #pragma unroll
   for (int a = 0; a < 3; a++) {
@@ -86,11 +89,11 @@ __device__ __forceinline__ bool spline_stencil(const DevGrid<T> &g, const Spline
     int l;
     if (a == 0) {
       // dbvalu's search over t(1..n+1); x == t(n+1) takes the left limit at interval n
-      l = (x[a] >= __ldg(A.t + n)) ? n : knot_interval(A.t, x[a], k, n);
+      l = (x[a] >= __ldg(A.t + n)) ? n : knot_interval(A.t, x[a], k, n, no[a] + k - 1);
     } else {
       // db3val's search over the whole knot vector; x >= t(n+k) gives 0
       if (x[a] >= tlast) return false;
-      l = knot_interval(A.t, x[a], k, n);
+      l = knot_interval(A.t, x[a], k, n, no[a] + k - 1);
     }
     basis_values(A, l, x[a], st.b[a]);
     c0[a] = l - k;  // padded index of coefficient l-k+1 (1-based)

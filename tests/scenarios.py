@@ -45,22 +45,23 @@ def make_case(name: str, n: int | None = None):
 
         return g, vel, dict(T=0.6, h=0.2, dt=0.05, steps=16)
     if name == "mixed_bc":
-        # inflow / outflow in x, slip in y, periodic z, one masked interior node
-        nx, ny, nz = 9, 7, 5
-        xl, yl, zl = np.arange(nx) * 0.125, np.arange(ny) * 0.15, (np.arange(nz) + 0.5) * 0.2
+        # inflow / outflow in x, periodic y, slip in z, two masked interior nodes
+        nx, ny, nz = 9, 6, 7
+        xl, yl, zl = np.arange(nx) * 0.125, (np.arange(ny) + 0.5) / ny, np.arange(nz) * 0.15
         X, Y, Z = np.meshgrid(xl, yl, zl, indexing="ij")
         flag = np.zeros(X.shape, dtype=np.int32)
         flag[0, :, :] = W.LCS_INFLOW
         flag[-1, :, :] = W.LCS_OUTFLOW
-        flag[:, 0, :] = W.LCS_SLIP
-        flag[:, -1, :] = W.LCS_SLIP
-        flag[4, 3, 2] = W.LCS_MASK
+        flag[:, :, 0] = W.LCS_SLIP
+        flag[:, :, -1] = W.LCS_SLIP
+        flag[4, 3, 3] = W.LCS_MASK
+        flag[5, 3, 3] = W.LCS_MASK
         g = W.Grid((nx, ny, nz), np.asfortranarray(X), np.asfortranarray(Y), np.asfortranarray(Z), np.asfortranarray(flag))
 
         def vel(t):
-            u = np.asfortranarray(0.4 + 0.1 * np.sin(np.pi * g.y / 0.9) * np.cos(t))
-            v = np.asfortranarray(0.08 * np.sin(2 * np.pi * g.x) * np.sin(np.pi * g.y / 0.9))
-            w = np.asfortranarray(0.05 * np.cos(2 * np.pi * g.z))
+            u = np.asfortranarray(0.4 + 0.1 * np.sin(np.pi * g.z / 0.9) * np.cos(t))
+            v = np.asfortranarray(0.08 * np.sin(2 * np.pi * g.x) + 0.05 * np.cos(2 * np.pi * g.y))
+            w = np.asfortranarray(0.05 * np.sin(np.pi * g.z / 0.9) * np.sin(2 * np.pi * g.y))
             return u, v, w
 
         return g, vel, dict(T=0.4, h=0.1, dt=0.05, steps=12)
