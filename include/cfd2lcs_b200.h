@@ -64,6 +64,21 @@ void cfd2lcs_get_phase_times_c(double t[7]);
  * n[0], n[1] the number of launches timed. */
 void cfd2lcs_get_kernel_times_c(double t[2], long long n[2]);
 
+/* Recomputes the latest FTLE frame of a diagnostic -- the composition of its stored
+ * sub-flow maps and the FTLE -- into device buffers the caller owns, and allocates no memory
+ * while doing so.  No counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc at the point where they want the field, such as a CFD solver that hands the whole
+ * GPU to its own memory pool at start-up and forbids allocations inside its time loop.
+ *   d_ftle: n[0]*n[1]*n[2] values; d_fm: 3*n[0]*n[1]*n[2] values (x, y, z components), both
+ *   device memory of lcsdata_t, i fastest.  The result equals cfd2lcs_get_ftle_c and
+ *   cfd2lcs_get_flowmap_c of that frame when the options are unchanged since.
+ * The table of sub-flow-map pointers lives in a fixed device array (256 sub-flow maps, i.e.
+ * T/h <= 256; larger frames are rejected with an error).  The first call on a device looks
+ * up that array's address; make this first call before any stream capture.  All calls share
+ * the array, so calls that overlap on the GPU race.  Plain-precision form only.  Returns 0 on
+ * success, 1 on error (the error is latched as for every other call). */
+int cfd2lcs_reconstruct_noalloc_c(int lcs_handle, lcsdata_t *d_ftle, lcsdata_t *d_fm);
+
 #ifdef __cplusplus
 }
 #endif

@@ -37,7 +37,7 @@ EXPORTED_SYMBOLS = [
     # extensions (include/cfd2lcs_b200.h)
     "cfd2lcs_finalize_c", "cfd2lcs_get_error_c", "cfd2lcs_reset_c", "cfd2lcs_get_ftle_c", "cfd2lcs_get_flowmap_c",
     "cfd2lcs_update_device_c", "cfd2lcs_ftle_device_ptr_c", "cfd2lcs_get_counters_c", "cfd2lcs_get_phase_times_c",
-    "cfd2lcs_get_kernel_times_c",
+    "cfd2lcs_get_kernel_times_c", "cfd2lcs_reconstruct_noalloc_c",
 ]
 
 
@@ -87,6 +87,8 @@ def load(precision: str = "dp") -> C.CDLL:
     lib.cfd2lcs_get_counters_c.argtypes = [P]
     lib.cfd2lcs_get_phase_times_c.argtypes = [P]
     lib.cfd2lcs_get_kernel_times_c.argtypes = [P, P]
+    lib.cfd2lcs_reconstruct_noalloc_c.argtypes = [C.c_int, P, P]
+    lib.cfd2lcs_reconstruct_noalloc_c.restype = C.c_int
     lib.cfd2lcs_b200_grid_tables.argtypes = [P, P, P, P, P, P, P, P, P, P, C.c_char_p, C.c_size_t]
     lib.cfd2lcs_b200_grid_tables.restype = C.c_int
     _LIBS[precision] = lib
@@ -184,6 +186,11 @@ class Cfd2lcs:
         self.lib.cfd2lcs_get_phase_times_c(self._p(a))
         keys = ["ingest", "bkwd_advect", "fwd_advect", "snapshot", "compose", "ftle", "update_total"]
         return {k: float(v) for k, v in zip(keys, a)}
+
+    def reconstruct_noalloc(self, handle, d_ftle: int, d_fm: int) -> int:
+        """Latest FTLE frame recomputed into caller-owned device buffers (raw device
+        pointers: n values for the FTLE, 3n for the flow map) without allocating."""
+        return int(self.lib.cfd2lcs_reconstruct_noalloc_c(int(handle), C.c_void_p(d_ftle), C.c_void_p(d_fm)))
 
     def kernel_times(self) -> dict:
         t = np.zeros(2, dtype=np.float64)

@@ -304,3 +304,21 @@ CFD2LCS_EXPORT int cfd2lcs_b200_grid_tables(const int n[3], const lcsdata_t *x, 
   }
   return ok ? 0 : 1;
 }
+
+// Allocation-free recomputation of a diagnostic's latest FTLE frame into caller-owned device
+// buffers (see include/cfd2lcs_b200.h).  Returns 0 on success; on failure the error is
+// latched like any other library error and 1 is returned.
+CFD2LCS_EXPORT int cfd2lcs_reconstruct_noalloc_c(int lcs_handle, lcsdata_t *d_ftle, lcsdata_t *d_fm) {
+  Library &lib = L();
+  if (lib.error) return 1;
+  if (!lib.eng) {
+    latch("reconstruct_noalloc: cfd2lcs_init was not called");
+    return 1;
+  }
+  std::string msg;
+  if (!lib.eng->reconstruct_noalloc(lcs_handle, d_ftle, d_fm, msg)) {
+    latch(msg);
+    return 1;
+  }
+  return 0;
+}

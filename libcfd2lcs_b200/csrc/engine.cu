@@ -77,12 +77,45 @@ struct Diag {
   std::vector<int> written, coef_deg;
   T **slot_list_dev = nullptr;  // pointers of the slots used by one composition
   std::vector<T *> slot_list_host;
+  std::vector<int> last_order;  // slots composed by the latest frame, in order
   T *composed[3] = {nullptr, nullptr, nullptr};  // interior, last FTLE frame
   lcsdata_t *ftle = nullptr;                      // interior
   bool have_frame = false;
 };
 
 }  // namespace
+
+// ---------------------------------------------------------------------------------------
+// Scratch of the allocation-free reconstruction entry point: the table of sub-flow-map
+// pointers the composition kernel reads, as a file-scope device array instead of an
+// allocated buffer.  Every GPU that loads the library holds these 6 KiB until exit; all
+// calls share the table (calls that overlap on the GPU race on it).
+// ---------------------------------------------------------------------------------------
+#define NOALLOC_MAX_SUBMAPS 256
+static __device__ __align__(256) const void *g_noalloc_submap_table[3 * NOALLOC_MAX_SUBMAPS];
+
+// Device address of the table on the current device, looked up once per device (host code
+// must not pass the symbol itself to a kernel: on the host it is only a stand-in).
+static bool noalloc_table_address(void **out, std::string &msg) {
+  static void *addr[64] = {nullptr};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 64) {
+    msg = std::string("reconstruct_noalloc: no current CUDA device: ") + cudaGetErrorString(e);
+    return false;
+  }
+  if (!addr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_submap_table);
+    if (e != cudaSuccess || !p) {
+      msg = std::string("reconstruct_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e);
+      return false;
+    }
+    addr[dev] = p;
+  }
+  *out = addr[dev];
+  return true;
+}
 
 template <typename T>
 class Engine : public EngineBase {
@@ -447,6 +480,7 @@ class Engine : public EngineBase {
       const int inc = d.type == FTLE_FWD ? 1 : -1;
       if (d.type == FTLE_FWD) step += inc;
       int m = 0;
+      d.last_order.clear();
       for (int i = 0; i < nstep; i++) {
         if (step >= nstep) step = 0;
         if (step < 0) step = nstep - 1;
@@ -463,6 +497,7 @@ class Engine : public EngineBase {
           } else {
             for (int c = 0; c < 3; c++) d.slot_list_host[3 * m + c] = d.slot[3 * step + c];
           }
+          d.last_order.push_back((int)step);
           m++;
         }
         step += inc;
@@ -506,6 +541,59 @@ class Engine : public EngineBase {
     red_err_ |= err;
     if (red_err_) return err_msg(msg);
     return true;
+  }
+
+  bool reconstruct_noalloc(int handle, lcsdata_t *d_ftle, lcsdata_t *d_fm, std::string &msg) override {
+    Diag<T> *d = find(handle);
+    if (!d || !d->have_frame) {
+      msg = "reconstruct_noalloc: unknown handle or no FTLE frame yet";
+      return false;
+    }
+    if (sizeof(T) != sizeof(lcsdata_t)) {
+      msg = "reconstruct_noalloc: not available in the mixed-precision form";
+      return false;
+    }
+    const int m = (int)d->last_order.size();
+    if (m > NOALLOC_MAX_SUBMAPS) {
+      msg = "reconstruct_noalloc: the frame composes " + std::to_string(m) + " sub-flow maps, more than the maximum of " +
+            std::to_string(NOALLOC_MAX_SUBMAPS) + " (T/h too large)";
+      return false;
+    }
+    const int interp = opt_->interpolator;
+    const bool spline = interp == QUADRATIC || interp == CUBIC;
+    const int deg = interp == QUADRATIC ? 2 : 3;
+    const T *host_table[3 * NOALLOC_MAX_SUBMAPS];
+    for (int q = 0; q < m; q++) {
+      const int s = d->last_order[q];
+      if (spline && (d->coef_deg[s] != deg || !d->slotcoef[3 * s])) {
+        msg = "reconstruct_noalloc: the stored sub-flow maps have no spline coefficients for the current interpolator";
+        return false;
+      }
+      for (int c = 0; c < 3; c++) host_table[3 * q + c] = spline ? d->slotcoef[3 * s + c] : d->slot[3 * s + c];
+    }
+    void *table = nullptr;
+    if (!noalloc_table_address(&table, msg)) return false;
+    if (m > 0) CK(cudaMemcpyAsync(table, host_table, sizeof(T *) * 3 * m, cudaMemcpyHostToDevice, stream_));
+    const int iv = interp == NEAREST_NBR ? INTERP_NEAREST : (interp == LINEAR ? INTERP_LINEAR : INTERP_SPLINE);
+    const SplineAxes<T> sa = spline ? splines_[deg].axes : SplineAxes<T>{};
+    FieldPtrsW<T> out{};
+    for (int c = 0; c < 3; c++) out.f[c] = reinterpret_cast<T *>(d_fm) + (size_t)c * N_;
+    const dim3 blk(32, 8, 1), grd = node_grid();
+    int *err = &red_->err;
+    const bool F = dg_.P.has_flags != 0;
+    const T *const *sl = reinterpret_cast<const T *const *>(table);
+#define COMPOSE_NA(I, FL) k_compose<T, I, FL><<<grd, blk, 0, stream_>>>(dg_, sa, sl, m, out, err)
+    if (iv == INTERP_NEAREST) { if (F) COMPOSE_NA(INTERP_NEAREST, true); else COMPOSE_NA(INTERP_NEAREST, false); }
+    else if (iv == INTERP_LINEAR) { if (F) COMPOSE_NA(INTERP_LINEAR, true); else COMPOSE_NA(INTERP_LINEAR, false); }
+    else { if (F) COMPOSE_NA(INTERP_SPLINE, true); else COMPOSE_NA(INTERP_SPLINE, false); }
+#undef COMPOSE_NA
+    CK(cudaGetLastError());
+    FieldPtrs<T> f{};
+    for (int c = 0; c < 3; c++) f.f[c] = out.f[c];
+    if (F) k_ftle<T, lcsdata_t, true><<<grd, blk, 0, stream_>>>(dg_, f, d_ftle, d->T_, opt_->incompressible);
+    else k_ftle<T, lcsdata_t, false><<<grd, blk, 0, stream_>>>(dg_, f, d_ftle, d->T_, opt_->incompressible);
+    CK(cudaGetLastError());
+    return sync_errors(msg);
   }
 
   bool get_ftle(int handle, lcsdata_t *out, std::string &msg) override {
