@@ -108,13 +108,15 @@ __device__ __forceinline__ void sample_velocity(const DevGrid<T> &g, const Splin
 #pragma unroll
     for (int c = 0; c < 3; c++) out[c] = lin_apply_blend(st, V.un[c], V.unp1[c], omc, ct);
   } else {
+    constexpr int KC = INTERP == INTERP_SPLINE4 ? 4 : 0;
     SplineStencil<T> st;
-    if (!spline_stencil(g, sa, x, no, st)) {
+    if (!spline_stencil<T, KC>(g, sa, x, no, st)) {
       out[0] = out[1] = out[2] = T(0);
       return;
     }
 #pragma unroll
-    for (int c = 0; c < 3; c++) out[c] = omc * spline_apply(g, sa, st, V.cn[c]) + ct * spline_apply(g, sa, st, V.cnp1[c]);
+    for (int c = 0; c < 3; c++)
+      out[c] = omc * spline_apply<T, KC>(g, sa, st, V.cn[c]) + ct * spline_apply<T, KC>(g, sa, st, V.cnp1[c]);
   }
 }
 
@@ -131,13 +133,14 @@ __device__ __forceinline__ void sample_field(const DevGrid<T> &g, const SplineAx
 #pragma unroll
     for (int c = 0; c < 3; c++) out[c] = lin_apply(st, f[c]);
   } else {
+    constexpr int KC = INTERP == INTERP_SPLINE4 ? 4 : 0;
     SplineStencil<T> st;
-    if (!spline_stencil(g, sa, x, no, st)) {
+    if (!spline_stencil<T, KC>(g, sa, x, no, st)) {
       out[0] = out[1] = out[2] = T(0);
       return;
     }
 #pragma unroll
-    for (int c = 0; c < 3; c++) out[c] = spline_apply(g, sa, st, f[c]);
+    for (int c = 0; c < 3; c++) out[c] = spline_apply<T, KC>(g, sa, st, f[c]);
   }
 }
 

@@ -18,7 +18,8 @@ enum : int {
 };
 
 enum { EULER_ = 0, TRAPEZOIDAL_ = 1, RK2_ = 2, RK3_ = 3, RK4_ = 4 };
-enum { INTERP_NEAREST = 0, INTERP_LINEAR = 1, INTERP_SPLINE = 2 };
+// INTERP_SPLINE: B-spline of any order per axis; INTERP_SPLINE4: cubic on every axis (3-D grid)
+enum { INTERP_NEAREST = 0, INTERP_LINEAR = 1, INTERP_SPLINE = 2, INTERP_SPLINE4 = 3 };
 
 template <typename T>
 struct DevGrid {

@@ -388,8 +388,8 @@ class Engine : public EngineBase {
       V.cn[c] = spline ? ucoef_[cur_ ^ 1][c] : nullptr;
       V.cnp1[c] = spline ? ucoef_[cur_][c] : nullptr;
     }
-    const int iv = interp == NEAREST_NBR ? INTERP_NEAREST : (interp == LINEAR ? INTERP_LINEAR : INTERP_SPLINE);
     const SplineAxes<T> sa = spline ? splines_[deg].axes : SplineAxes<T>{};
+    const int iv = interp_variant(interp, sa);
 
     // --- per particle set: K1 (backward) / K6 (forward) --------------------------------
     for (auto &d : diags_) {
@@ -574,8 +574,8 @@ class Engine : public EngineBase {
     void *table = nullptr;
     if (!noalloc_table_address(&table, msg)) return false;
     if (m > 0) CK(cudaMemcpyAsync(table, host_table, sizeof(T *) * 3 * m, cudaMemcpyHostToDevice, stream_));
-    const int iv = interp == NEAREST_NBR ? INTERP_NEAREST : (interp == LINEAR ? INTERP_LINEAR : INTERP_SPLINE);
     const SplineAxes<T> sa = spline ? splines_[deg].axes : SplineAxes<T>{};
+    const int iv = interp_variant(interp, sa);
     FieldPtrsW<T> out{};
     for (int c = 0; c < 3; c++) out.f[c] = reinterpret_cast<T *>(d_fm) + (size_t)c * N_;
     const dim3 blk(32, 8, 1), grd = node_grid();
@@ -585,6 +585,7 @@ class Engine : public EngineBase {
 #define COMPOSE_NA(I, FL) k_compose<T, I, FL><<<grd, blk, 0, stream_>>>(dg_, sa, sl, m, out, err)
     if (iv == INTERP_NEAREST) { if (F) COMPOSE_NA(INTERP_NEAREST, true); else COMPOSE_NA(INTERP_NEAREST, false); }
     else if (iv == INTERP_LINEAR) { if (F) COMPOSE_NA(INTERP_LINEAR, true); else COMPOSE_NA(INTERP_LINEAR, false); }
+    else if (iv == INTERP_SPLINE4) { if (F) COMPOSE_NA(INTERP_SPLINE4, true); else COMPOSE_NA(INTERP_SPLINE4, false); }
     else { if (F) COMPOSE_NA(INTERP_SPLINE, true); else COMPOSE_NA(INTERP_SPLINE, false); }
 #undef COMPOSE_NA
     CK(cudaGetLastError());
@@ -708,29 +709,40 @@ class Engine : public EngineBase {
   }
 
   // coefficients of the padded fields src (3 components) into dst (db3ink, x then y then z)
+  template <int K>
+  void fit_axis(const SplineAxis<T> &A, FieldPtrsW<T> f, int nfast, int nlines, long stride_line, long stride_other) {
+    const int blk = 128;
+    const dim3 grd((nlines + blk - 1) / blk, 3);
+    k_fit_lines<T, K><<<grd, blk, 0, stream_>>>(A, f, nfast, nlines, stride_line, stride_other);
+  }
+
+  void fit_axis_any(const SplineAxis<T> &A, FieldPtrsW<T> f, int nfast, int nlines, long stride_line, long stride_other) {
+    if (A.k == 4) fit_axis<4>(A, f, nfast, nlines, stride_line, stride_other);
+    else if (A.k == 3) fit_axis<3>(A, f, nfast, nlines, stride_line, stride_other);
+    else fit_axis<2>(A, f, nfast, nlines, stride_line, stride_other);
+  }
+
   bool fit(T *const src[3], T *const dst[3], std::string &msg) {
     const SplineAxes<T> &S = splines_[opt_->interpolator == QUADRATIC ? 2 : 3].axes;
     const int sx = dg_.P.sx, sxy = dg_.P.sxy, nz = n_[2] + 2, ny = n_[1] + 2;
+    FieldPtrsW<T> f{};
     for (int c = 0; c < 3; c++) {
       if (src[c] != dst[c]) CK(cudaMemcpyAsync(dst[c], src[c], ntot_ * sizeof(T), cudaMemcpyDeviceToDevice, stream_));
-      counters_.kernel_launches += 3;
-      {
-        const int lines = ny * nz;
-        const size_t smem = (size_t)32 * (sx + 1) * sizeof(T);
-        if (smem > 48 * 1024) cudaFuncSetAttribute(k_fit_axis_x<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_fit_axis_x<T><<<(lines + 31) / 32, 32, smem, stream_>>>(S.ax[0], dst[c], lines);
-      }
-      {
-        const dim3 blk(128, 1), grd((sx + 127) / 128, nz);
-        k_fit_axis_yz<T><<<grd, blk, 0, stream_>>>(S.ax[1], dst[c], sx, nz, (long)sx, (long)sxy);
-      }
-      {
-        const dim3 blk(128, 1), grd((sxy + 127) / 128, 1);
-        k_fit_axis_yz<T><<<grd, blk, 0, stream_>>>(S.ax[2], dst[c], sxy, 1, (long)sxy, 0L);
-      }
-      CK(cudaGetLastError());
+      f.f[c] = dst[c];
     }
+    counters_.kernel_launches += 3;
+    fit_axis_any(S.ax[0], f, 1, ny * nz, 1L, (long)sx);         // x lines: contiguous
+    fit_axis_any(S.ax[1], f, sx, sx * nz, (long)sx, (long)sxy);  // y lines
+    fit_axis_any(S.ax[2], f, sxy, sxy, (long)sxy, 0L);           // z lines
+    CK(cudaGetLastError());
     return true;
+  }
+
+  static int interp_variant(int interp, const SplineAxes<T> &sa) {
+    if (interp == NEAREST_NBR) return INTERP_NEAREST;
+    if (interp == LINEAR) return INTERP_LINEAR;
+    if (sa.ax[0].k == 4 && sa.ax[1].k == 4 && sa.ax[2].k == 4) return INTERP_SPLINE4;
+    return INTERP_SPLINE;
   }
 
   dim3 node_grid() const { return dim3((n_[0] + 31) / 32, (n_[1] + 7) / 8, n_[2]); }
@@ -754,6 +766,7 @@ class Engine : public EngineBase {
     const bool F = dg_.P.has_flags != 0;
     if (iv == INTERP_NEAREST) F ? sl_integ<INTERP_NEAREST, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_NEAREST, false>(sa, V, fo, fn, S, dt);
     else if (iv == INTERP_LINEAR) F ? sl_integ<INTERP_LINEAR, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_LINEAR, false>(sa, V, fo, fn, S, dt);
+    else if (iv == INTERP_SPLINE4) F ? sl_integ<INTERP_SPLINE4, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_SPLINE4, false>(sa, V, fo, fn, S, dt);
     else F ? sl_integ<INTERP_SPLINE, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_SPLINE, false>(sa, V, fo, fn, S, dt);
     CK(cudaGetLastError());
     return true;
@@ -778,6 +791,7 @@ class Engine : public EngineBase {
     const bool F = dg_.P.has_flags != 0;
     if (iv == INTERP_NEAREST) F ? fwd_integ<INTERP_NEAREST, true>(sa, V, P, S, dt) : fwd_integ<INTERP_NEAREST, false>(sa, V, P, S, dt);
     else if (iv == INTERP_LINEAR) F ? fwd_integ<INTERP_LINEAR, true>(sa, V, P, S, dt) : fwd_integ<INTERP_LINEAR, false>(sa, V, P, S, dt);
+    else if (iv == INTERP_SPLINE4) F ? fwd_integ<INTERP_SPLINE4, true>(sa, V, P, S, dt) : fwd_integ<INTERP_SPLINE4, false>(sa, V, P, S, dt);
     else F ? fwd_integ<INTERP_SPLINE, true>(sa, V, P, S, dt) : fwd_integ<INTERP_SPLINE, false>(sa, V, P, S, dt);
     CK(cudaGetLastError());
     return true;
@@ -817,6 +831,7 @@ class Engine : public EngineBase {
 #define COMPOSE(I, FL) k_compose<T, I, FL><<<grd, blk, 0, stream_>>>(dg_, sa, sl, m, out, err)
     if (iv == INTERP_NEAREST) { if (F) COMPOSE(INTERP_NEAREST, true); else COMPOSE(INTERP_NEAREST, false); }
     else if (iv == INTERP_LINEAR) { if (F) COMPOSE(INTERP_LINEAR, true); else COMPOSE(INTERP_LINEAR, false); }
+    else if (iv == INTERP_SPLINE4) { if (F) COMPOSE(INTERP_SPLINE4, true); else COMPOSE(INTERP_SPLINE4, false); }
     else { if (F) COMPOSE(INTERP_SPLINE, true); else COMPOSE(INTERP_SPLINE, false); }
 #undef COMPOSE
     CK(cudaGetLastError());

@@ -379,35 +379,20 @@ __global__ void k_reset_particles(DevGrid<T> g, Particles<T> P) {
 }
 
 // ---------------------------------------------------------------------------------------
-// B-spline fit: banded solves along one axis for every line of a padded field
-// (the three dbtpcf passes of db3ink, src/bspline/bspline_sub_module.f90:451-533).
-// Lines along y and z are processed by adjacent threads at adjacent i (coalesced); lines
-// along x are staged through shared memory.
+// B-spline fit: banded solves along one axis for every line of the padded field (the three
+// dbtpcf passes of db3ink, src/bspline/bspline_sub_module.f90:451-533), one thread per line.
+// Lines along y and z are read by adjacent threads at adjacent i (coalesced); along x each
+// thread walks its own contiguous line through L1.
 // ---------------------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(256) k_fit_axis_yz(SplineAxis<T> A, T *f, int nx, int other, long stride_line, long stride_other) {
-  // thread (ix, io): line with x index ix and index io along the remaining axis
-  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
-  const int io = blockIdx.y * blockDim.y + threadIdx.y;
-  if (ix >= nx || io >= other) return;
-  band_solve_line(A, f + ix + (long)io * stride_other, stride_line);
-}
-
-// x-lines: a block stages 32 consecutive lines in shared memory with coalesced loads, then
-// each thread solves its own line there and the block writes them back.
-template <typename T>
-__global__ void __launch_bounds__(32) k_fit_axis_x(SplineAxis<T> A, T *f, int nlines) {
-  extern __shared__ unsigned char smem_raw[];
-  T *buf = reinterpret_cast<T *>(smem_raw);
-  const int n = A.n, ld = n + 1;  // odd leading dimension spreads the banks
-  const int line0 = blockIdx.x * 32;
-  const int nl = min(32, nlines - line0);
-  T *src = f + (long)line0 * n;
-  for (int q = threadIdx.x; q < nl * n; q += 32) buf[(q / n) * ld + (q % n)] = src[q];
-  __syncthreads();
-  if (threadIdx.x < nl) band_solve_line(A, buf + threadIdx.x * ld, 1);
-  __syncthreads();
-  for (int q = threadIdx.x; q < nl * n; q += 32) src[q] = buf[(q / n) * ld + (q % n)];
+// All lines of one axis of the three components in one launch: line l of component c
+// starts at f[c] + (l % nfast) + (l / nfast) * stride_other and steps by stride_line.
+template <typename T, int K>
+__global__ void __launch_bounds__(128) k_fit_lines(SplineAxis<T> A, FieldPtrsW<T> f, int nfast, int nlines, long stride_line,
+                                                    long stride_other) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= nlines) return;
+  T *base = f.f[blockIdx.y] + (l % nfast) + (long)(l / nfast) * stride_other;
+  band_solve_window<T, K>(A, base, stride_line);
 }
 
 }  // namespace cfd2lcs

@@ -49,10 +49,12 @@ __device__ __forceinline__ int knot_interval(const T *t, T x, int lo, int hi, in
   return l;
 }
 
-template <typename T>
+// KC: the order when it is known at compile time for every axis (4 for cubic on a 3-D grid),
+// 0 for the general case.
+template <typename T, int KC>
 __device__ __forceinline__ void basis_values(const SplineAxis<T> &A, int l, T x, T *b) {
   // Cox-de Boor recurrence with the reciprocal knot spans of interval l
-  const int k = A.k;
+  const int k = KC ? KC : A.k;
   const T *r = A.rinv + (size_t)(l - 1) * 6;
   T dr[4], dl[4];
   b[0] = T(1);
@@ -76,14 +78,14 @@ __device__ __forceinline__ void basis_values(const SplineAxis<T> &A, int l, T x,
 
 // Locates x in the padded spline; false where db3val returns 0.  no[] is the padded node
 // the point belongs to (its interval is near no + k - 1).
-template <typename T>
+template <typename T, int KC>
 __device__ __forceinline__ bool spline_stencil(const DevGrid<T> &g, const SplineAxes<T> &S, const T x[3], const int no[3],
                                                SplineStencil<T> &st) {
   int c0[3];
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     const SplineAxis<T> &A = S.ax[a];
-    const int n = A.n, k = A.k;
+    const int n = A.n, k = KC ? KC : A.k;
     const T tfirst = __ldg(A.t), tlast = __ldg(A.t + n + k - 1);
     if (!(x[a] >= tfirst) || x[a] > tlast) return false;
     int l;
@@ -95,17 +97,17 @@ __device__ __forceinline__ bool spline_stencil(const DevGrid<T> &g, const Spline
       if (x[a] >= tlast) return false;
       l = knot_interval(A.t, x[a], k, n, no[a] + k - 1);
     }
-    basis_values(A, l, x[a], st.b[a]);
+    basis_values<T, KC>(A, l, x[a], st.b[a]);
     c0[a] = l - k;  // padded index of coefficient l-k+1 (1-based)
   }
   st.p0 = pidx(g.P.sx, g.P.sxy, c0[0], c0[1], c0[2]);
   return true;
 }
 
-template <typename T>
+template <typename T, int KC>
 __device__ __forceinline__ T spline_apply(const DevGrid<T> &g, const SplineAxes<T> &S, const SplineStencil<T> &st,
                                           const T *__restrict__ coef) {
-  const int kx = S.ax[0].k, ky = S.ax[1].k, kz = S.ax[2].k;
+  const int kx = KC ? KC : S.ax[0].k, ky = KC ? KC : S.ax[1].k, kz = KC ? KC : S.ax[2].k;
   T vz = T(0);
 #pragma unroll
   for (int c2 = 0; c2 < 4; c2++) {
@@ -154,6 +156,50 @@ __device__ __forceinline__ void band_solve_line(const SplineAxis<T> &A, T *b, lo
   Bm(1) = Bm(1) / Wm(mid, 1);
 #undef Wm
 #undef Bm
+}
+
+// Same solve with a register window of k values per pass: every element is loaded and
+// stored once in the forward and once in the backward pass, and receives its updates in the
+// reference's order (forward: from rows i = m-k+1 .. m-1; backward: from i = m+k-1 .. m+1).
+template <typename T, int K>
+__device__ __forceinline__ void band_solve_window(const SplineAxis<T> &A, T *b, long stride) {
+  const int n = A.n, nr = 2 * K - 1, mid = K;
+  const T *w = A.lu;
+#define Wm(r, c) __ldg(w + ((r)-1) + (size_t)nr * ((c)-1))
+  T win[K];
+  if (n == 1) {
+    b[0] = b[0] / Wm(mid, 1);
+    return;
+  }
+  // forward elimination: window holds b(i) .. b(i+K-1)
+#pragma unroll
+  for (int q = 0; q < K; q++) win[q] = (q < n) ? b[(long)q * stride] : T(0);
+  for (int i = 1; i <= n - 1; i++) {
+    const T bi = win[0];
+    b[(long)(i - 1) * stride] = bi;
+#pragma unroll
+    for (int j = 1; j < K; j++)
+      if (i + j <= n) win[j] = win[j] - bi * Wm(mid + j, i);
+#pragma unroll
+    for (int q = 0; q < K - 1; q++) win[q] = win[q + 1];
+    win[K - 1] = (i + K <= n) ? b[(long)(i + K - 1) * stride] : T(0);
+  }
+  b[(long)(n - 1) * stride] = win[0];
+  // back substitution: window holds b(i), b(i-1), .., b(i-K+1)
+#pragma unroll
+  for (int q = 0; q < K; q++) win[q] = (n - q >= 1) ? b[(long)(n - 1 - q) * stride] : T(0);
+  for (int i = n; i >= 2; i--) {
+    const T bi = win[0] / Wm(mid, i);
+    b[(long)(i - 1) * stride] = bi;
+#pragma unroll
+    for (int j = 1; j < K; j++)
+      if (i - j >= 1) win[j] = win[j] - bi * Wm(mid - j, i);
+#pragma unroll
+    for (int q = 0; q < K - 1; q++) win[q] = win[q + 1];
+    win[K - 1] = (i - K >= 1) ? b[(long)(i - K - 1) * stride] : T(0);
+  }
+  b[0] = win[0] / Wm(mid, 1);
+#undef Wm
 }
 
 }  // namespace cfd2lcs
