@@ -42,7 +42,9 @@ EXPORTED_SYMBOLS = [
 
 
 def library_path(precision: str = "dp") -> str:
-    return os.path.join(HERE, f"libcfd2lcs_b200_{precision}.so")
+    """In-tree library, or the one in $CFD2LCS_B200_LIBDIR when that is set."""
+    d = os.environ.get("CFD2LCS_B200_LIBDIR") or HERE
+    return os.path.join(d, f"libcfd2lcs_b200_{precision}.so")
 
 
 def build(precisions=("dp", "sp"), force=False):

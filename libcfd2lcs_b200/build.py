@@ -15,7 +15,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-BUILD = os.path.join(HERE, "_build")
+BUILD = os.environ.get("CFD2LCS_B200_BUILDDIR") or os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["engine.cu", "grid.cpp", "spline_host.cpp", "capi.cpp"]
@@ -23,13 +23,14 @@ HEADERS = ["grid.h", "engine.h", "device_common.cuh", "advect.cuh", "spline.cuh"
 
 
 def lib_path(prec: str) -> str:
-    return os.path.join(HERE, f"libcfd2lcs_b200_{prec}.so")
+    return os.path.join(os.environ.get("CFD2LCS_B200_LIBDIR") or HERE, f"libcfd2lcs_b200_{prec}.so")
 
 
 def _flags(prec: str):
     f = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden,-O2", "-I", CSRC] + ARCH
     if prec == "sp":
         f += ["-DCFD2LCS_SP"]
+    f += os.environ.get("CFD2LCS_B200_NVCC_FLAGS", "").split()
     return f
 
 

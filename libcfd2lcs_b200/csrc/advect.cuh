@@ -90,13 +90,15 @@ template <typename T>
 struct VelFields {
   const T *un[3];
   const T *unp1[3];
-  const T *cn[3];    // spline coefficients of u_n (INTERP_SPLINE)
-  const T *cnp1[3];  // spline coefficients of u_np1
+  // B-spline interpolators: coefficients of the time-blended velocity of each stage,
+  // (1-ct) c(u_n) + ct c(u_np1) -- the spline of the blended field the reference fits per
+  // stage (src/lp_motion_m.f90:193-197 then src/lp_tracking_m.f90:509-511), by linearity
+  const T *cs[4][3];
 };
 
 template <typename T, int INTERP>
 __device__ __forceinline__ void sample_velocity(const DevGrid<T> &g, const SplineAxes<T> &sa, const VelFields<T> &V, const T x[3],
-                                                const int no[3], T ct, T out[3]) {
+                                                const int no[3], T ct, int stage, T out[3]) {
   const T omc = T(1) - ct;
   if (INTERP == INTERP_NEAREST) {
     const int p = pidx(g.P.sx, g.P.sxy, no[0], no[1], no[2]);
@@ -115,8 +117,7 @@ __device__ __forceinline__ void sample_velocity(const DevGrid<T> &g, const Splin
       return;
     }
 #pragma unroll
-    for (int c = 0; c < 3; c++)
-      out[c] = omc * spline_apply<T, KC>(g, sa, st, V.cn[c]) + ct * spline_apply<T, KC>(g, sa, st, V.cnp1[c]);
+    for (int c = 0; c < 3; c++) out[c] = spline_apply<T, KC>(g, sa, st, V.cs[stage][c]);
   }
 }
 
@@ -162,34 +163,34 @@ __device__ __forceinline__ void integrate(const DevGrid<T> &g, const SplineAxes<
   const T HALF = T(1) / T(2), THIRD = T(1) / T(3), TWOTHIRD = T(2) / T(3), SIXTH = T(1) / T(6), TWO = T(2);
   T u[3];
   if (INTEG == EULER_ || INTEG == TRAPEZOIDAL_) {
-    sample_velocity<T, INTERP>(g, sa, V, xn, no, T(S.ct[0]), u);
+    sample_velocity<T, INTERP>(g, sa, V, xn, no, T(S.ct[0]), 0, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) x[c] = xn[c] + dt * u[c];
   } else if (INTEG == RK2_) {
-    sample_velocity<T, INTERP>(g, sa, V, xn, no, T(S.ct[0]), u);
+    sample_velocity<T, INTERP>(g, sa, V, xn, no, T(S.ct[0]), 0, u);
     T xh[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) xh[c] = xn[c] + HALF * dt * u[c];
-    sample_velocity<T, INTERP>(g, sa, V, xh, no, T(S.ct[1]), u);
+    sample_velocity<T, INTERP>(g, sa, V, xh, no, T(S.ct[1]), 1, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) x[c] = xn[c] + dt * u[c];
   } else if (INTEG == RK3_) {
     T k[3], xs[3], acc[3];
-    sample_velocity<T, INTERP>(g, sa, V, xn, no, T(S.ct[0]), u);
+    sample_velocity<T, INTERP>(g, sa, V, xn, no, T(S.ct[0]), 0, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];
       acc[c] = xn[c] + SIXTH * k[c];
       xs[c] = xn[c] + HALF * k[c];
     }
-    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[1]), u);
+    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[1]), 1, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];
       xs[c] = xn[c] + TWO * k[c];
       acc[c] = acc[c] + TWOTHIRD * k[c];
     }
-    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[2]), u);
+    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[2]), 2, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];
@@ -197,28 +198,28 @@ __device__ __forceinline__ void integrate(const DevGrid<T> &g, const SplineAxes<
     }
   } else {  // RK4
     T k[3], xs[3], acc[3];
-    sample_velocity<T, INTERP>(g, sa, V, xn, no, T(S.ct[0]), u);
+    sample_velocity<T, INTERP>(g, sa, V, xn, no, T(S.ct[0]), 0, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];
       acc[c] = xn[c] + SIXTH * k[c];
       xs[c] = xn[c] + HALF * k[c];
     }
-    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[1]), u);
+    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[1]), 1, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];
       acc[c] = acc[c] + THIRD * k[c];
       xs[c] = xn[c] + HALF * k[c];
     }
-    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[2]), u);
+    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[2]), 2, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];
       acc[c] = acc[c] + THIRD * k[c];
       xs[c] = xn[c] + k[c];
     }
-    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[3]), u);
+    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[3]), 3, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];
@@ -296,6 +297,39 @@ __device__ __forceinline__ bool track_pass(const DevGrid<T> &g, const T x[3], in
   bool have = false;
   int off[3] = {0, 0, 0};
   const int sa = g.P.single_axis;
+  // fast path: every candidate node is an interior node, so its coordinates are the lines
+  // and the squared distances separate per axis (same values, same summation order)
+  bool inner = true;
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+    if (a != sa && (no[a] < 2 || no[a] > g.P.n[a] - 1)) inner = false;
+  if (inner) {
+    T sq[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int o = 0; o < 3; o++) {
+        const int v = (a == sa) ? no[a] : no[a] + o - 1;
+        const T e = __ldg(g.lt[a] + v) - x[a];
+        sq[a][o] = e * e;
+      }
+    for (int nb = 0; nb < 27; nb++) {
+      const int o0 = c_nbr[nb][0], o1 = c_nbr[nb][1], o2 = c_nbr[nb][2];
+      if ((sa == 0 && o0 != 0) || (sa == 1 && o1 != 0) || (sa == 2 && o2 != 0)) continue;
+      const T r = sq[0][sa == 0 ? 1 : o0 + 1] + sq[1][sa == 1 ? 1 : o1 + 1] + sq[2][sa == 2 ? 1 : o2 + 1];
+      if (!have || r < T(0.99) * best) {
+        best = r;
+        have = true;
+        off[0] = o0;
+        off[1] = o1;
+        off[2] = o2;
+      }
+    }
+    no[0] += off[0];
+    no[1] += off[1];
+    no[2] += off[2];
+    return off[0] != 0 || off[1] != 0 || off[2] != 0;
+  }
   for (int nb = 0; nb < 27; nb++) {
     const int o0 = c_nbr[nb][0], o1 = c_nbr[nb][1], o2 = c_nbr[nb][2];
     if ((sa == 0 && o0 != 0) || (sa == 1 && o1 != 0) || (sa == 2 && o2 != 0)) continue;

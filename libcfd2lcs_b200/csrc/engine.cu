@@ -78,6 +78,10 @@ struct Diag {
   T **slot_list_dev = nullptr;  // pointers of the slots used by one composition
   std::vector<T *> slot_list_host;
   std::vector<int> last_order;  // slots composed by the latest frame, in order
+  // time-blended spline coefficients of the stage velocities (B-spline interpolators)
+  T *blend[3][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  double blend_ct[3] = {-1, -1, -1};
+  long long blend_update[3] = {-1, -1, -1};
   T *composed[3] = {nullptr, nullptr, nullptr};  // interior, last FTLE frame
   lcsdata_t *ftle = nullptr;                      // interior
   bool have_frame = false;
@@ -381,12 +385,10 @@ class Engine : public EngineBase {
     CK(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
     counters_.phase_ms[0] += ms;
 
-    VelFields<T> V;
+    VelFields<T> V{};
     for (int c = 0; c < 3; c++) {
       V.un[c] = u_[cur_ ^ 1][c];
       V.unp1[c] = u_[cur_][c];
-      V.cn[c] = spline ? ucoef_[cur_ ^ 1][c] : nullptr;
-      V.cnp1[c] = spline ? ucoef_[cur_][c] : nullptr;
     }
     const SplineAxes<T> sa = spline ? splines_[deg].axes : SplineAxes<T>{};
     const int iv = interp_variant(interp, sa);
@@ -417,6 +419,7 @@ class Engine : public EngineBase {
       }
       for (long sc = 0; sc < nsub; sc++) {
         StageTimes S = stage_times(lp_time, dt);
+        if (spline && !stage_blends(d, S, V, msg)) return false;
         if (d.type == FTLE_BKWD) {
           FieldPtrs<T> fo;
           FieldPtrsW<T> fn;
@@ -685,6 +688,58 @@ class Engine : public EngineBase {
     return S;
   }
 
+  // Coefficients of the blended stage velocities of one subcycle, in the diagnostic's three
+  // blend buffers.  A buffer already holding the same ct of this update is reused (the last
+  // stage of a subcycle is the first of the next; RK4's two midpoint stages coincide).
+  bool stage_blends(Diag<T> &d, const StageTimes &S, VelFields<T> &V, std::string &msg) {
+    static const int nst[5] = {1, 1, 2, 3, 4};
+    const int ns = nst[std::min(std::max(opt_->integrator, 0), 4)];
+    const long long upd = counters_.updates;
+    bool used[3] = {false, false, false};
+    int pick[4] = {-1, -1, -1, -1};
+    for (int st = 0; st < ns; st++)
+      for (int b = 0; b < 3; b++)
+        if (d.blend[b][0] && d.blend_update[b] == upd && d.blend_ct[b] == S.ct[st]) {
+          pick[st] = b;
+          used[b] = true;
+          break;
+        }
+    for (int st = 0; st < ns; st++) {
+      if (pick[st] >= 0) continue;
+      for (int q = 0; q < st; q++)
+        if (S.ct[q] == S.ct[st] && pick[q] >= 0) pick[st] = pick[q];
+      if (pick[st] >= 0) continue;
+      int b = 0;
+      while (b < 3 && used[b]) b++;
+      if (b == 3) {
+        msg = "internal: no free blend buffer";
+        return false;
+      }
+      if (!d.blend[b][0])
+        for (int c = 0; c < 3; c++)
+          if (!(d.blend[b][c] = arena_.alloc<T>(ntot_, msg))) return false;
+      FieldPtrs<T> a{}, bb{};
+      FieldPtrsW<T> out{};
+      for (int c = 0; c < 3; c++) {
+        a.f[c] = ucoef_[cur_ ^ 1][c];
+        bb.f[c] = ucoef_[cur_][c];
+        out.f[c] = d.blend[b][c];
+      }
+      const T ct = (T)S.ct[st];
+      const dim3 grd((unsigned)((ntot_ + 255) / 256), 3);
+      k_blend<T><<<grd, 256, 0, stream_>>>(a, bb, out, T(1) - ct, ct, ntot_);
+      counters_.kernel_launches++;
+      CK(cudaGetLastError());
+      d.blend_ct[b] = S.ct[st];
+      d.blend_update[b] = upd;
+      used[b] = true;
+      pick[st] = b;
+    }
+    for (int st = 0; st < ns; st++)
+      for (int c = 0; c < 3; c++) V.cs[st][c] = d.blend[pick[st]][c];
+    return true;
+  }
+
   bool ensure_spline(int deg, std::string &msg) {
     if (splines_[deg].deg == deg) return true;
     SplineSet<T> s;
@@ -710,30 +765,43 @@ class Engine : public EngineBase {
 
   // coefficients of the padded fields src (3 components) into dst (db3ink, x then y then z)
   template <int K>
-  void fit_axis(const SplineAxis<T> &A, FieldPtrsW<T> f, int nfast, int nlines, long stride_line, long stride_other) {
-    const int blk = 128;
-    const dim3 grd((nlines + blk - 1) / blk, 3);
-    k_fit_lines<T, K><<<grd, blk, 0, stream_>>>(A, f, nfast, nlines, stride_line, stride_other);
+  void fit_axis(const SplineAxis<T> &A, FieldPtrsW<T> f, int adjacent, int nfast, int nother, long es, long ls, long so) {
+    const int nbf = (nfast + 31) / 32;
+    const dim3 grd(nbf * nother, 3);
+    const size_t smem = (size_t)A.n * 33 * sizeof(T);
+    static bool attr_done = false;
+    if (!attr_done) {
+      cudaFuncSetAttribute(k_fit_smem<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      attr_done = true;
+    }
+    k_fit_smem<T, K><<<grd, 128, smem, stream_>>>(A, f, adjacent, nfast, nbf, es, ls, so);
   }
 
-  void fit_axis_any(const SplineAxis<T> &A, FieldPtrsW<T> f, int nfast, int nlines, long stride_line, long stride_other) {
-    if (A.k == 4) fit_axis<4>(A, f, nfast, nlines, stride_line, stride_other);
-    else if (A.k == 3) fit_axis<3>(A, f, nfast, nlines, stride_line, stride_other);
-    else fit_axis<2>(A, f, nfast, nlines, stride_line, stride_other);
+  void fit_axis_any(const SplineAxis<T> &A, FieldPtrsW<T> f, int adjacent, int nfast, int nother, long es, long ls, long so) {
+    if (A.k == 4) fit_axis<4>(A, f, adjacent, nfast, nother, es, ls, so);
+    else if (A.k == 3) fit_axis<3>(A, f, adjacent, nfast, nother, es, ls, so);
+    else fit_axis<2>(A, f, adjacent, nfast, nother, es, ls, so);
   }
 
   bool fit(T *const src[3], T *const dst[3], std::string &msg) {
     const SplineAxes<T> &S = splines_[opt_->interpolator == QUADRATIC ? 2 : 3].axes;
     const int sx = dg_.P.sx, sxy = dg_.P.sxy, nz = n_[2] + 2, ny = n_[1] + 2;
+    if ((size_t)std::max(std::max(sx, ny), nz) * 33 * sizeof(T) > 200 * 1024) {
+      msg = "bspline fit: a grid line is too long for the shared-memory line solver";
+      return false;
+    }
     FieldPtrsW<T> f{};
     for (int c = 0; c < 3; c++) {
       if (src[c] != dst[c]) CK(cudaMemcpyAsync(dst[c], src[c], ntot_ * sizeof(T), cudaMemcpyDeviceToDevice, stream_));
       f.f[c] = dst[c];
     }
     counters_.kernel_launches += 3;
-    fit_axis_any(S.ax[0], f, 1, ny * nz, 1L, (long)sx);         // x lines: contiguous
-    fit_axis_any(S.ax[1], f, sx, sx * nz, (long)sx, (long)sxy);  // y lines
-    fit_axis_any(S.ax[2], f, sxy, sxy, (long)sxy, 0L);           // z lines
+    // x lines: 32 lines (consecutive j) per block, lines sx apart, ny*nz lines in all
+    fit_axis_any(S.ax[0], f, 0, ny, nz, 1L, (long)sx, (long)sxy);
+    // y lines: 32 adjacent lines (consecutive i) per block, elements sx apart, one block row per k
+    fit_axis_any(S.ax[1], f, 1, sx, nz, (long)sx, 0L, (long)sxy);
+    // z lines: 32 adjacent lines (consecutive i) per block over the x-y plane, elements sxy apart
+    fit_axis_any(S.ax[2], f, 1, sxy, 1, (long)sxy, 0L, 0L);
     CK(cudaGetLastError());
     return true;
   }

@@ -378,21 +378,65 @@ __global__ void k_reset_particles(DevGrid<T> g, Particles<T> P) {
   }
 }
 
+// Time blend of two padded coefficient fields for one RK stage: c = (1-ct) a + ct b.
+template <typename T>
+__global__ void __launch_bounds__(256) k_blend(FieldPtrs<T> a, FieldPtrs<T> b, FieldPtrsW<T> c, T omc, T ct, long ntot) {
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= ntot) return;
+  const int comp = blockIdx.y;
+  c.f[comp][q] = omc * __ldg(a.f[comp] + q) + ct * __ldg(b.f[comp] + q);
+}
+
 // ---------------------------------------------------------------------------------------
 // B-spline fit: banded solves along one axis for every line of the padded field (the three
 // dbtpcf passes of db3ink, src/bspline/bspline_sub_module.f90:451-533), one thread per line.
 // Lines along y and z are read by adjacent threads at adjacent i (coalesced); along x each
 // thread walks its own contiguous line through L1.
 // ---------------------------------------------------------------------------------------
-// All lines of one axis of the three components in one launch: line l of component c
-// starts at f[c] + (l % nfast) + (l / nfast) * stride_other and steps by stride_line.
+// A block of four warps stages 32 lines of one component in shared memory as
+// [element][line] (padded leading dimension), with coalesced loads and stores spread over
+// all four warps; warp 0 then solves one line per lane.
+//   lines_adjacent = true  (y and z passes): line l starts at base + l, elements step by es
+//   lines_adjacent = false (x pass):         line l starts at base + l * ls, elements step by 1
+// Block b covers lines 32*(b % nblk_fast) .. +31 of block row b / nblk_fast (stride_other).
 template <typename T, int K>
-__global__ void __launch_bounds__(128) k_fit_lines(SplineAxis<T> A, FieldPtrsW<T> f, int nfast, int nlines, long stride_line,
-                                                    long stride_other) {
-  const int l = blockIdx.x * blockDim.x + threadIdx.x;
-  if (l >= nlines) return;
-  T *base = f.f[blockIdx.y] + (l % nfast) + (long)(l / nfast) * stride_other;
-  band_solve_window<T, K>(A, base, stride_line);
+__global__ void __launch_bounds__(128) k_fit_smem(SplineAxis<T> A, FieldPtrsW<T> f, int lines_adjacent, int nfast, int nblk_fast,
+                                                   long es, long ls, long stride_other) {
+  extern __shared__ unsigned char smem_raw[];
+  T *buf = reinterpret_cast<T *>(smem_raw);
+  constexpr int LD = 33;
+  const int n = A.n, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T *fc = f.f[blockIdx.y];
+  const int bf = blockIdx.x % nblk_fast, bo = blockIdx.x / nblk_fast;
+  const int l0 = bf * 32;
+  const int nl = min(32, nfast - l0);
+  if (lines_adjacent) {
+    T *base = fc + l0 + (long)bo * stride_other;
+    if (lane < nl) {
+#pragma unroll 8
+      for (int e = warp; e < n; e += 4) buf[e * LD + lane] = base[(long)e * es + lane];
+    }
+    __syncthreads();
+    if (warp == 0 && lane < nl) band_solve_window<T, K>(A, buf + lane, LD);
+    __syncthreads();
+    if (lane < nl) {
+#pragma unroll 8
+      for (int e = warp; e < n; e += 4) base[(long)e * es + lane] = buf[e * LD + lane];
+    }
+  } else {
+    T *base = fc + (long)l0 * ls + (long)bo * stride_other;
+    for (int l = warp; l < nl; l += 4) {
+#pragma unroll 8
+      for (int e = lane; e < n; e += 32) buf[e * LD + l] = base[(long)l * ls + e];
+    }
+    __syncthreads();
+    if (warp == 0 && lane < nl) band_solve_window<T, K>(A, buf + lane, LD);
+    __syncthreads();
+    for (int l = warp; l < nl; l += 4) {
+#pragma unroll 8
+      for (int e = lane; e < n; e += 32) base[(long)l * ls + e] = buf[e * LD + l];
+    }
+  }
 }
 
 }  // namespace cfd2lcs
