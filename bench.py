@@ -59,6 +59,8 @@ WORKLOADS = {
     # capture holds about 1.5 GB on the device while every field is larger than L2
     "abcprof": dict(kind="abc", n=192, dt=0.05, T=2.0, h=1.0, integrator=3, interpolator=3, dirs=(1,), t0=0.95,
                     desc="ABC flow 192^3 periodic, dt=0.05, FTLE bkwd T=2 h=1, RK3, cubic B-spline (profiling case)"),
+    "abcproffwd": dict(kind="abc", n=192, dt=0.05, T=2.0, h=1.0, integrator=3, interpolator=3, dirs=(0,), t0=0.95,
+                       desc="ABC flow 192^3 periodic, dt=0.05, FTLE fwd T=2 h=1, RK3, cubic B-spline (profiling case)"),
     "abcproflin": dict(kind="abc", n=192, dt=0.05, T=2.0, h=1.0, integrator=2, interpolator=1, dirs=(1,), t0=0.95,
                        desc="ABC flow 192^3 periodic, dt=0.05, FTLE bkwd T=2 h=1, RK2, linear (profiling case)"),
     "abc256lin": dict(kind="abc", n=256, dt=0.05, T=10.0, h=1.0, integrator=2, interpolator=1, dirs=(0, 1), t0=0.95,
