@@ -330,7 +330,8 @@ def run_b200(args, w):
             "ftle_field_ms": ftle_ms, "ftle_frames_seen": frames,
             "slots_composed_per_frame": (c1["slots_composed"] / frames if frames else None),
             "nsub_per_update": {"fwd": c1["nsub_fwd"], "bkwd": c1["nsub_bkwd"]},
-            "gpu_launches": launches, "e2e": e2e, "roofline": roof}
+            "gpu_launches": launches, "e2e": e2e, "roofline": roof, "rooflines": rooflines,
+            "phase_ms_per_step": {k: (p1[k] - p0[k]) / args.steps for k in p1}}
     if rank == 0:
         line["clocks"] = clk.summary()
         if world == 1 and not args.no_cpu:
