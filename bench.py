@@ -42,13 +42,16 @@ UNIT = "grid-pt·RK-steps/s"
 STAGES = {0: 1, 1: 1, 2: 2, 3: 3, 4: 3}
 
 
-def sl_bytes_per_point(s: int, interp: int, integrator: int) -> int:
-    vel = 2 * 3 * s if interp in (0, 1) else STAGES[integrator] * 3 * s
+def sl_bytes_per_point(s: int, interp: int, integrator: int, sv: int = None) -> int:
+    """s: bytes of a flow-map value, sv: bytes of a velocity value (4 in the mixed form)."""
+    sv = sv or s
+    vel = 2 * 3 * sv if interp in (0, 1) else STAGES[integrator] * 3 * sv
     return vel + 3 * s + 3 * s
 
 
-def fwd_bytes_per_particle(s: int, interp: int, integrator: int) -> int:
-    vel = 2 * 3 * s if interp in (0, 1) else STAGES[integrator] * 3 * s
+def fwd_bytes_per_particle(s: int, interp: int, integrator: int, sv: int = None) -> int:
+    sv = sv or s
+    vel = 2 * 3 * sv if interp in (0, 1) else STAGES[integrator] * 3 * sv
     return vel + 2 * (6 * s + 12)
 
 
@@ -306,13 +309,14 @@ def run_b200(args, w):
     # --- roofline of the dominant hot kernel (by device time in the timed region) ---
     peaks = measured_peaks()
     hbm = peaks.get("hbm_gbs")
-    s_bytes = 8 if args.precision == "fp64" else 4
+    s_bytes = 8
+    v_bytes = 8 if args.precision == "fp64" else 4
     cands = []
     nsl, nfw = k1["sl_launches"] - k0["sl_launches"], k1["fwd_launches"] - k0["fwd_launches"]
     if nsl > 0:
-        cands.append(("k_sl_subcycle", k1["sl_ms"] - k0["sl_ms"], nsl, sl_bytes_per_point(s_bytes, w["interpolator"], w["integrator"])))
+        cands.append(("k_sl_subcycle", k1["sl_ms"] - k0["sl_ms"], nsl, sl_bytes_per_point(s_bytes, w["interpolator"], w["integrator"], v_bytes)))
     if nfw > 0:
-        cands.append(("k_fwd_subcycle", k1["fwd_ms"] - k0["fwd_ms"], nfw, fwd_bytes_per_particle(s_bytes, w["interpolator"], w["integrator"])))
+        cands.append(("k_fwd_subcycle", k1["fwd_ms"] - k0["fwd_ms"], nfw, fwd_bytes_per_particle(s_bytes, w["interpolator"], w["integrator"], v_bytes)))
     rooflines = {}
     for name, tot_ms, nl, bpp in cands:
         avg_s = tot_ms / nl / 1000.0
@@ -324,7 +328,7 @@ def run_b200(args, w):
     roof = max(rooflines.values(), key=lambda r: r["share_of_step"] or 0) if rooflines else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
+            "dtype": "f64" if args.precision == "fp64" else "f64 positions, f32 velocity", "data": "synthetic",
             "config": {"workload": w["desc"], "grid": list(g.n), "precision": args.precision, "l2": "inputs larger than L2 (126 MB)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "ftle_field_ms": ftle_ms, "ftle_frames_seen": frames,

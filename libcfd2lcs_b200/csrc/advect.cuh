@@ -67,18 +67,19 @@ __device__ __forceinline__ T lin_apply(const LinStencil<T> &st, const T *__restr
   return st.w[0] * f0 + st.w[1] * f1 + st.w[2] * f2 + st.w[3] * f3 + st.w[4] * f4 + st.w[5] * f5 + st.w[6] * f6 + st.w[7] * f7;
 }
 
-// time-blended field u = (1-ct) u_n + ct u_np1 sampled at the corners, then trilinear
-template <typename T>
-__device__ __forceinline__ T lin_apply_blend(const LinStencil<T> &st, const T *__restrict__ a, const T *__restrict__ b, T omc,
-                                             T ct) {
+// time-blended field u = (1-ct) u_n + ct u_np1 sampled at the corners, then trilinear; TV is
+// the velocity storage type (FP32 in the mixed-precision form, weights rounded to it)
+template <typename T, typename TV>
+__device__ __forceinline__ TV lin_apply_blend(const LinStencil<T> &st, const TV *__restrict__ a, const TV *__restrict__ b, TV omc,
+                                              TV ct) {
   const int p = st.p0;
   const int q[8] = {p, p + st.s[0], p + st.s[1], p + st.s[0] + st.s[1], p + st.s[2], p + st.s[0] + st.s[2], p + st.s[1] + st.s[2],
                     p + st.s[0] + st.s[1] + st.s[2]};
-  T acc = T(0);
+  TV acc = TV(0);
 #pragma unroll
   for (int c = 0; c < 8; c++) {
-    const T v = omc * __ldg(a + q[c]) + ct * __ldg(b + q[c]);
-    acc = c == 0 ? st.w[0] * v : acc + st.w[c] * v;
+    const TV v = omc * __ldg(a + q[c]) + ct * __ldg(b + q[c]);
+    acc = c == 0 ? TV(st.w[0]) * v : acc + TV(st.w[c]) * v;
   }
   return acc;
 }
@@ -87,7 +88,7 @@ __device__ __forceinline__ T lin_apply_blend(const LinStencil<T> &st, const T *_
 // Velocity sampler for one stage: NEAREST, LINEAR or B-spline, blended in time.
 // ---------------------------------------------------------------------------------------
 template <typename T>
-struct VelFields {
+struct VelFields {  // T: velocity storage type
   const T *un[3];
   const T *unp1[3];
   // B-spline interpolators: coefficients of the time-blended velocity of each stage,
@@ -96,19 +97,21 @@ struct VelFields {
   const T *cs[4][3];
 };
 
-template <typename T, int INTERP>
-__device__ __forceinline__ void sample_velocity(const DevGrid<T> &g, const SplineAxes<T> &sa, const VelFields<T> &V, const T x[3],
-                                                const int no[3], T ct, int stage, T out[3]) {
-  const T omc = T(1) - ct;
+// Positions and stencils in T (the position / flow-map type); velocity data in TV.
+template <typename T, typename TV, int INTERP>
+__device__ __forceinline__ void sample_velocity(const DevGrid<T> &g, const SplineAxes<T> &sa, const VelFields<TV> &V, const T x[3],
+                                                const int no[3], T ct_, int stage, T out[3]) {
+  const TV ct = TV(ct_);
+  const TV omc = TV(1) - ct;
   if (INTERP == INTERP_NEAREST) {
     const int p = pidx(g.P.sx, g.P.sxy, no[0], no[1], no[2]);
 #pragma unroll
-    for (int c = 0; c < 3; c++) out[c] = omc * __ldg(V.un[c] + p) + ct * __ldg(V.unp1[c] + p);
+    for (int c = 0; c < 3; c++) out[c] = T(omc * __ldg(V.un[c] + p) + ct * __ldg(V.unp1[c] + p));
   } else if (INTERP == INTERP_LINEAR) {
     LinStencil<T> st;
     lin_stencil(g, x, no, st);
 #pragma unroll
-    for (int c = 0; c < 3; c++) out[c] = lin_apply_blend(st, V.un[c], V.unp1[c], omc, ct);
+    for (int c = 0; c < 3; c++) out[c] = T(lin_apply_blend<T, TV>(st, V.un[c], V.unp1[c], omc, ct));
   } else {
     constexpr int KC = INTERP == INTERP_SPLINE4 ? 4 : 0;
     SplineStencil<T> st;
@@ -117,7 +120,7 @@ __device__ __forceinline__ void sample_velocity(const DevGrid<T> &g, const Splin
       return;
     }
 #pragma unroll
-    for (int c = 0; c < 3; c++) out[c] = spline_apply<T, KC>(g, sa, st, V.cs[stage][c]);
+    for (int c = 0; c < 3; c++) out[c] = T(spline_apply<T, KC, TV>(g, sa, st, V.cs[stage][c]));
   }
 }
 
@@ -157,40 +160,40 @@ struct StageTimes {
   double ct[4];
 };
 
-template <typename T, int INTEG, int INTERP>
-__device__ __forceinline__ void integrate(const DevGrid<T> &g, const SplineAxes<T> &sa, const VelFields<T> &V, const StageTimes &S,
+template <typename T, typename TV, int INTEG, int INTERP>
+__device__ __forceinline__ void integrate(const DevGrid<T> &g, const SplineAxes<T> &sa, const VelFields<TV> &V, const StageTimes &S,
                                           T dt, const T xn[3], const int no[3], T x[3]) {
   const T HALF = T(1) / T(2), THIRD = T(1) / T(3), TWOTHIRD = T(2) / T(3), SIXTH = T(1) / T(6), TWO = T(2);
   T u[3];
   if (INTEG == EULER_ || INTEG == TRAPEZOIDAL_) {
-    sample_velocity<T, INTERP>(g, sa, V, xn, no, T(S.ct[0]), 0, u);
+    sample_velocity<T, TV, INTERP>(g, sa, V, xn, no, T(S.ct[0]), 0, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) x[c] = xn[c] + dt * u[c];
   } else if (INTEG == RK2_) {
-    sample_velocity<T, INTERP>(g, sa, V, xn, no, T(S.ct[0]), 0, u);
+    sample_velocity<T, TV, INTERP>(g, sa, V, xn, no, T(S.ct[0]), 0, u);
     T xh[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) xh[c] = xn[c] + HALF * dt * u[c];
-    sample_velocity<T, INTERP>(g, sa, V, xh, no, T(S.ct[1]), 1, u);
+    sample_velocity<T, TV, INTERP>(g, sa, V, xh, no, T(S.ct[1]), 1, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) x[c] = xn[c] + dt * u[c];
   } else if (INTEG == RK3_) {
     T k[3], xs[3], acc[3];
-    sample_velocity<T, INTERP>(g, sa, V, xn, no, T(S.ct[0]), 0, u);
+    sample_velocity<T, TV, INTERP>(g, sa, V, xn, no, T(S.ct[0]), 0, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];
       acc[c] = xn[c] + SIXTH * k[c];
       xs[c] = xn[c] + HALF * k[c];
     }
-    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[1]), 1, u);
+    sample_velocity<T, TV, INTERP>(g, sa, V, xs, no, T(S.ct[1]), 1, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];
       xs[c] = xn[c] + TWO * k[c];
       acc[c] = acc[c] + TWOTHIRD * k[c];
     }
-    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[2]), 2, u);
+    sample_velocity<T, TV, INTERP>(g, sa, V, xs, no, T(S.ct[2]), 2, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];
@@ -198,28 +201,28 @@ __device__ __forceinline__ void integrate(const DevGrid<T> &g, const SplineAxes<
     }
   } else {  // RK4
     T k[3], xs[3], acc[3];
-    sample_velocity<T, INTERP>(g, sa, V, xn, no, T(S.ct[0]), 0, u);
+    sample_velocity<T, TV, INTERP>(g, sa, V, xn, no, T(S.ct[0]), 0, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];
       acc[c] = xn[c] + SIXTH * k[c];
       xs[c] = xn[c] + HALF * k[c];
     }
-    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[1]), 1, u);
+    sample_velocity<T, TV, INTERP>(g, sa, V, xs, no, T(S.ct[1]), 1, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];
       acc[c] = acc[c] + THIRD * k[c];
       xs[c] = xn[c] + HALF * k[c];
     }
-    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[2]), 2, u);
+    sample_velocity<T, TV, INTERP>(g, sa, V, xs, no, T(S.ct[2]), 2, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];
       acc[c] = acc[c] + THIRD * k[c];
       xs[c] = xn[c] + k[c];
     }
-    sample_velocity<T, INTERP>(g, sa, V, xs, no, T(S.ct[3]), 3, u);
+    sample_velocity<T, TV, INTERP>(g, sa, V, xs, no, T(S.ct[3]), 3, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];

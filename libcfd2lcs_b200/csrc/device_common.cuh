@@ -98,8 +98,8 @@ __device__ __forceinline__ int ghost_rule(int kind, int f) {
 // Every ghost cell has exactly one source node: its periodic image (rule 0) or its
 // nearest interior node (rules 1, 2).  The node (i,j,k) enumerates both candidate sets
 // and writes the cells whose rule points back at it, so no two threads write one cell.
-template <typename T, bool HAS_FLAGS, int KIND>
-__device__ void write_ghosts(const DevGrid<T> &g, T *const f[3], int i, int j, int k, const T vpre[3], const T vfin[3],
+template <typename T, bool HAS_FLAGS, int KIND, typename TF = T>
+__device__ void write_ghosts(const DevGrid<T> &g, TF *const f[3], int i, int j, int k, const TF vpre[3], const TF vfin[3],
                              int *err) {
   const int idx[3] = {i, j, k};
   bool edge = false;
@@ -130,7 +130,7 @@ __device__ void write_ghosts(const DevGrid<T> &g, T *const f[3], int i, int j, i
             continue;
           }
 #pragma unroll
-          for (int c = 0; c < 3; c++) f[c][p] = rule == 1 ? T(0) : vfin[c];
+          for (int c = 0; c < 3; c++) f[c][p] = rule == 1 ? TF(0) : vfin[c];
         }
   }
   // wrap side: index n+1 is the image of node 1 and index 0 of node n (rule 0)

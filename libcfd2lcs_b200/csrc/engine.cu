@@ -60,7 +60,7 @@ struct SplineSet {
   SplineAxes<T> axes{};
 };
 
-template <typename T>
+template <typename T, typename TV>
 struct Diag {
   int handle = 0, type = 0;
   lcsdata_t T_ = 0, h = 0, dt_factor = 1;
@@ -79,7 +79,7 @@ struct Diag {
   std::vector<T *> slot_list_host;
   std::vector<int> last_order;  // slots composed by the latest frame, in order
   // time-blended spline coefficients of the stage velocities (B-spline interpolators)
-  T *blend[3][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  TV *blend[3][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
   double blend_ct[3] = {-1, -1, -1};
   long long blend_update[3] = {-1, -1, -1};
   T *composed[3] = {nullptr, nullptr, nullptr};  // interior, last FTLE frame
@@ -121,8 +121,14 @@ static bool noalloc_table_address(void **out, std::string &msg) {
   return true;
 }
 
-template <typename T>
+// TV: storage type of the velocity levels, their spline coefficients and the blended stage
+// coefficients (FP32 in the mixed-precision form).  Positions, flow maps, sub-flow maps,
+// composition and FTLE stay in the interface type T = lcsdata_t.
+template <typename TV>
 class Engine : public EngineBase {
+  using T = lcsdata_t;
+  using DiagT = Diag<T, TV>;
+
  public:
   explicit Engine(const Options *opt) : opt_(opt) {}
   ~Engine() override {
@@ -234,8 +240,8 @@ class Engine : public EngineBase {
     // velocity levels (zero-initialised, as init_sr1 does, src/structured_m.f90:73-96)
     for (int l = 0; l < 2; l++)
       for (int c = 0; c < 3; c++) {
-        if (!(u_[l][c] = arena_.alloc<T>(ntot_, msg))) return false;
-        CK(cudaMemsetAsync(u_[l][c], 0, ntot_ * sizeof(T), stream_));
+        if (!(u_[l][c] = arena_.alloc<TV>(ntot_, msg))) return false;
+        CK(cudaMemsetAsync(u_[l][c], 0, ntot_ * sizeof(TV), stream_));
       }
     if (!(stage_ = arena_.alloc<lcsdata_t>((size_t)3 * N_, msg))) return false;
     if (!(red_ = arena_.alloc<DevReduce>(1, msg))) return false;
@@ -263,7 +269,7 @@ class Engine : public EngineBase {
       msg = "diagnostic_init: T and h must be positive";
       return -1;
     }
-    Diag<T> d;
+    DiagT d;
     d.handle = (int)diags_.size() + 1;
     d.type = type;
     d.T_ = Tint;
@@ -345,12 +351,12 @@ class Engine : public EngineBase {
     CK(cudaMemcpyAsync(red_, red_host_, sizeof(DevReduce), cudaMemcpyHostToDevice, stream_));
     {
       const dim3 blk(32, 8, 1), grd((n_[0] + 31) / 32, (n_[1] + 7) / 8, n_[2]);
-      T *const *U = u_[cur_];
+      TV *const *U = u_[cur_];
       counters_.kernel_launches++;
       if (dg_.P.has_flags)
-        k_ingest<T, lcsdata_t, true><<<grd, blk, 0, stream_>>>(dg_, su, sv, sw, U[0], U[1], U[2], red_);
+        k_ingest<T, TV, lcsdata_t, true><<<grd, blk, 0, stream_>>>(dg_, su, sv, sw, U[0], U[1], U[2], red_);
       else
-        k_ingest<T, lcsdata_t, false><<<grd, blk, 0, stream_>>>(dg_, su, sv, sw, U[0], U[1], U[2], red_);
+        k_ingest<T, TV, lcsdata_t, false><<<grd, blk, 0, stream_>>>(dg_, su, sv, sw, U[0], U[1], U[2], red_);
       CK(cudaGetLastError());
     }
     const bool spline = interp == QUADRATIC || interp == CUBIC;
@@ -360,12 +366,12 @@ class Engine : public EngineBase {
       for (int l = 0; l < 2; l++)
         if (!ucoef_[l][0])
           for (int c = 0; c < 3; c++)
-            if (!(ucoef_[l][c] = arena_.alloc<T>(ntot_, msg))) return false;
+            if (!(ucoef_[l][c] = arena_.alloc<TV>(ntot_, msg))) return false;
       if (ucoef_deg_[cur_ ^ 1] != deg) {  // coefficients of u_n missing (first spline use)
-        if (!fit(u_[cur_ ^ 1], ucoef_[cur_ ^ 1], msg)) return false;
+        if (!fit(vsplines_[deg].axes, u_[cur_ ^ 1], ucoef_[cur_ ^ 1], msg)) return false;
         ucoef_deg_[cur_ ^ 1] = deg;
       }
-      if (!fit(u_[cur_], ucoef_[cur_], msg)) return false;
+      if (!fit(vsplines_[deg].axes, u_[cur_], ucoef_[cur_], msg)) return false;
       ucoef_deg_[cur_] = deg;
     } else {
       ucoef_deg_[cur_] = 0;
@@ -385,7 +391,7 @@ class Engine : public EngineBase {
     CK(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
     counters_.phase_ms[0] += ms;
 
-    VelFields<T> V{};
+    VelFields<TV> V{};
     for (int c = 0; c < 3; c++) {
       V.un[c] = u_[cur_ ^ 1][c];
       V.unp1[c] = u_[cur_][c];
@@ -431,7 +437,7 @@ class Engine : public EngineBase {
             if (!d.fmcoef[0])
               for (int c = 0; c < 3; c++)
                 if (!(d.fmcoef[c] = arena_.alloc<T>(ntot_, msg))) return false;
-            if (!fit(d.fm[d.cur], d.fmcoef, msg)) return false;
+            if (!fit(splines_[deg].axes, d.fm[d.cur], d.fmcoef, msg)) return false;
             for (int c = 0; c < 3; c++) fo.f[c] = d.fmcoef[c];
           }
           CK(cudaEventRecord(kev_[2 * sc], stream_));
@@ -493,7 +499,7 @@ class Engine : public EngineBase {
               for (int c = 0; c < 3; c++)
                 if (!(d.slotcoef[3 * step + c] = arena_.alloc<T>(ntot_, msg))) return false;
             if (d.coef_deg[step] != deg) {
-              if (!fit(&d.slot[3 * step], &d.slotcoef[3 * step], msg)) return false;
+              if (!fit(splines_[deg].axes, &d.slot[3 * step], &d.slotcoef[3 * step], msg)) return false;
               d.coef_deg[step] = deg;
             }
             for (int c = 0; c < 3; c++) d.slot_list_host[3 * m + c] = d.slotcoef[3 * step + c];
@@ -547,13 +553,9 @@ class Engine : public EngineBase {
   }
 
   bool reconstruct_noalloc(int handle, lcsdata_t *d_ftle, lcsdata_t *d_fm, std::string &msg) override {
-    Diag<T> *d = find(handle);
+    DiagT *d = find(handle);
     if (!d || !d->have_frame) {
       msg = "reconstruct_noalloc: unknown handle or no FTLE frame yet";
-      return false;
-    }
-    if (sizeof(T) != sizeof(lcsdata_t)) {
-      msg = "reconstruct_noalloc: not available in the mixed-precision form";
       return false;
     }
     const int m = (int)d->last_order.size();
@@ -601,7 +603,7 @@ class Engine : public EngineBase {
   }
 
   bool get_ftle(int handle, lcsdata_t *out, std::string &msg) override {
-    Diag<T> *d = find(handle);
+    DiagT *d = find(handle);
     if (!d || !d->have_frame) {
       msg = "get_ftle: unknown handle or no FTLE frame yet";
       return false;
@@ -612,7 +614,7 @@ class Engine : public EngineBase {
   }
 
   bool get_flowmap(int handle, lcsdata_t *out, std::string &msg) override {
-    Diag<T> *d = find(handle);
+    DiagT *d = find(handle);
     if (!d || !d->have_frame) {
       msg = "get_flowmap: unknown handle or no FTLE frame yet";
       return false;
@@ -627,7 +629,7 @@ class Engine : public EngineBase {
   }
 
   const lcsdata_t *ftle_device_ptr(int handle) override {
-    Diag<T> *d = find(handle);
+    DiagT *d = find(handle);
     return d ? d->ftle : nullptr;
   }
 
@@ -647,20 +649,20 @@ class Engine : public EngineBase {
     return false;
   }
 
-  template <typename V>
-  T *upload(const std::vector<V> &h, std::string &msg) {
-    std::vector<T> tmp(h.size());
-    for (size_t q = 0; q < h.size(); q++) tmp[q] = (T)h[q];
-    T *d = arena_.alloc<T>(tmp.size(), msg);
+  template <typename D = T, typename V>
+  D *upload(const std::vector<V> &h, std::string &msg) {
+    std::vector<D> tmp(h.size());
+    for (size_t q = 0; q < h.size(); q++) tmp[q] = (D)h[q];
+    D *d = arena_.alloc<D>(tmp.size(), msg);
     if (!d) return nullptr;
-    if (cudaMemcpy(d, tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) {
+    if (cudaMemcpy(d, tmp.data(), tmp.size() * sizeof(D), cudaMemcpyHostToDevice) != cudaSuccess) {
       msg = "upload failed";
       return nullptr;
     }
     return d;
   }
 
-  Diag<T> *find(int handle) {
+  DiagT *find(int handle) {
     for (auto &d : diags_)
       if (d.handle == handle) return &d;
     return nullptr;
@@ -691,7 +693,7 @@ class Engine : public EngineBase {
   // Coefficients of the blended stage velocities of one subcycle, in the diagnostic's three
   // blend buffers.  A buffer already holding the same ct of this update is reused (the last
   // stage of a subcycle is the first of the next; RK4's two midpoint stages coincide).
-  bool stage_blends(Diag<T> &d, const StageTimes &S, VelFields<T> &V, std::string &msg) {
+  bool stage_blends(DiagT &d, const StageTimes &S, VelFields<TV> &V, std::string &msg) {
     static const int nst[5] = {1, 1, 2, 3, 4};
     const int ns = nst[std::min(std::max(opt_->integrator, 0), 4)];
     const long long upd = counters_.updates;
@@ -717,17 +719,17 @@ class Engine : public EngineBase {
       }
       if (!d.blend[b][0])
         for (int c = 0; c < 3; c++)
-          if (!(d.blend[b][c] = arena_.alloc<T>(ntot_, msg))) return false;
-      FieldPtrs<T> a{}, bb{};
-      FieldPtrsW<T> out{};
+          if (!(d.blend[b][c] = arena_.alloc<TV>(ntot_, msg))) return false;
+      FieldPtrs<TV> a{}, bb{};
+      FieldPtrsW<TV> out{};
       for (int c = 0; c < 3; c++) {
         a.f[c] = ucoef_[cur_ ^ 1][c];
         bb.f[c] = ucoef_[cur_][c];
         out.f[c] = d.blend[b][c];
       }
-      const T ct = (T)S.ct[st];
+      const TV ct = (TV)S.ct[st];
       const dim3 grd((unsigned)((ntot_ + 255) / 256), 3);
-      k_blend<T><<<grd, 256, 0, stream_>>>(a, bb, out, T(1) - ct, ct, ntot_);
+      k_blend<TV><<<grd, 256, 0, stream_>>>(a, bb, out, TV(1) - ct, ct, ntot_);
       counters_.kernel_launches++;
       CK(cudaGetLastError());
       d.blend_ct[b] = S.ct[st];
@@ -743,7 +745,8 @@ class Engine : public EngineBase {
   bool ensure_spline(int deg, std::string &msg) {
     if (splines_[deg].deg == deg) return true;
     SplineSet<T> s;
-    s.deg = deg;
+    SplineSet<TV> sv;
+    s.deg = sv.deg = deg;
     for (int a = 0; a < 3; a++) {
       SplineAxisHost<lcsdata_t> A;
       const int npts = n_[a] + 2;
@@ -757,51 +760,74 @@ class Engine : public EngineBase {
       D.k = A.k;
       if (!(D.t = upload(A.t, msg))) return false;
       if (!(D.rinv = upload(A.rinv, msg))) return false;
-      if (!(D.lu = upload(A.lu, msg))) return false;
+      const std::vector<lcsdata_t> pull = pull_table(A);
+      if (!(D.pull = upload(pull, msg))) return false;
+      // the velocity fits solve with the LU factors rounded to the velocity type
+      SplineAxis<TV> &E = sv.axes.ax[a];
+      E.n = A.n;
+      E.k = A.k;
+      if (!(E.t = upload<TV>(A.t, msg))) return false;
+      if (!(E.rinv = upload<TV>(A.rinv, msg))) return false;
+      if (!(E.pull = upload<TV>(pull, msg))) return false;
     }
     splines_[deg] = s;
+    vsplines_[deg] = sv;
     return true;
   }
 
   // coefficients of the padded fields src (3 components) into dst (db3ink, x then y then z)
-  template <int K>
-  void fit_axis(const SplineAxis<T> &A, FieldPtrsW<T> f, int adjacent, int nfast, int nother, long es, long ls, long so) {
-    const int nbf = (nfast + 31) / 32;
-    const dim3 grd(nbf * nother, 3);
-    const size_t smem = (size_t)A.n * 33 * sizeof(T);
-    static bool attr_done = false;
-    if (!attr_done) {
-      cudaFuncSetAttribute(k_fit_smem<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-      attr_done = true;
+  // Band LU of one axis in the pull form the device sweeps read (pull_forward / pull_backward)
+  static std::vector<lcsdata_t> pull_table(const SplineAxisHost<lcsdata_t> &A) {
+    const int n = A.n, k = A.k, nr = 2 * k - 1, mid = k;
+    auto W = [&](int r, int c) { return A.lu[(size_t)(r - 1) + (size_t)nr * (c - 1)]; };
+    std::vector<lcsdata_t> p((size_t)8 * n, lcsdata_t(0));
+    for (int i = 1; i <= n; i++) {
+      for (int j = 1; j <= k - 1; j++) {
+        if (i - j >= 1) p[(size_t)8 * (i - 1) + j - 1] = W(mid + j, i - j);
+        if (i + j <= n) p[(size_t)8 * (i - 1) + 3 + j - 1] = W(mid - j, i + j);
+      }
+      p[(size_t)8 * (i - 1) + 6] = lcsdata_t(1) / W(mid, i);
     }
-    k_fit_smem<T, K><<<grd, 128, smem, stream_>>>(A, f, adjacent, nfast, nbf, es, ls, so);
+    return p;
   }
 
-  void fit_axis_any(const SplineAxis<T> &A, FieldPtrsW<T> f, int adjacent, int nfast, int nother, long es, long ls, long so) {
-    if (A.k == 4) fit_axis<4>(A, f, adjacent, nfast, nother, es, ls, so);
-    else if (A.k == 3) fit_axis<3>(A, f, adjacent, nfast, nother, es, ls, so);
-    else fit_axis<2>(A, f, adjacent, nfast, nother, es, ls, so);
+  template <typename D, int K>
+  void fit_pass(const SplineAxis<D> &A, FieldPtrs<D> s, FieldPtrsW<D> d, int axis) {
+    const int sx = dg_.P.sx, sxy = dg_.P.sxy, ny = n_[1] + 2, nz = n_[2] + 2;
+    if (axis == 0) {
+      const long warps = (long)((ny + 31) / 32) * nz;
+      k_fit_xlines<D, K><<<dim3((unsigned)((warps + 3) / 4), 3), 128, 0, stream_>>>(A, s, d, ny, nz, (long)sx, (long)sxy);
+    } else {
+      // y lines: sx * nz of them, elements sx apart; z lines: sxy of them, elements sxy apart
+      const int nfast = axis == 1 ? sx : sxy;
+      const long nlines = axis == 1 ? (long)sx * nz : (long)sxy;
+      const long es = axis == 1 ? (long)sx : (long)sxy;
+      k_fit_lines<D, K><<<dim3((unsigned)((nlines + 255) / 256), 3), 256, 0, stream_>>>(A, s, d, nfast, nlines, es, (long)sxy);
+    }
   }
 
-  bool fit(T *const src[3], T *const dst[3], std::string &msg) {
-    const SplineAxes<T> &S = splines_[opt_->interpolator == QUADRATIC ? 2 : 3].axes;
-    const int sx = dg_.P.sx, sxy = dg_.P.sxy, nz = n_[2] + 2, ny = n_[1] + 2;
-    if ((size_t)std::max(std::max(sx, ny), nz) * 33 * sizeof(T) > 200 * 1024) {
-      msg = "bspline fit: a grid line is too long for the shared-memory line solver";
-      return false;
-    }
-    FieldPtrsW<T> f{};
+  template <typename D>
+  void fit_pass_any(const SplineAxis<D> &A, FieldPtrs<D> s, FieldPtrsW<D> d, int axis) {
+    if (A.k == 4) fit_pass<D, 4>(A, s, d, axis);
+    else if (A.k == 3) fit_pass<D, 3>(A, s, d, axis);
+    else fit_pass<D, 2>(A, s, d, axis);
+  }
+
+  // Coefficients of the padded fields src (3 components) into dst (db3ink: x, then y, then z).
+  // D is the field type: T for flow maps and sub-flow maps, TV for velocity levels.
+  template <typename D>
+  bool fit(const SplineAxes<D> &S, D *const src[3], D *const dst[3], std::string &msg) {
+    FieldPtrs<D> s{}, di{};
+    FieldPtrsW<D> d{};
     for (int c = 0; c < 3; c++) {
-      if (src[c] != dst[c]) CK(cudaMemcpyAsync(dst[c], src[c], ntot_ * sizeof(T), cudaMemcpyDeviceToDevice, stream_));
-      f.f[c] = dst[c];
+      s.f[c] = src[c];
+      di.f[c] = dst[c];
+      d.f[c] = dst[c];
     }
     counters_.kernel_launches += 3;
-    // x lines: 32 lines (consecutive j) per block, lines sx apart, ny*nz lines in all
-    fit_axis_any(S.ax[0], f, 0, ny, nz, 1L, (long)sx, (long)sxy);
-    // y lines: 32 adjacent lines (consecutive i) per block, elements sx apart, one block row per k
-    fit_axis_any(S.ax[1], f, 1, sx, nz, (long)sx, 0L, (long)sxy);
-    // z lines: 32 adjacent lines (consecutive i) per block over the x-y plane, elements sxy apart
-    fit_axis_any(S.ax[2], f, 1, sxy, 1, (long)sxy, 0L, 0L);
+    fit_pass_any(S.ax[0], s, d, 0);
+    fit_pass_any(S.ax[1], di, d, 1);
+    fit_pass_any(S.ax[2], di, d, 2);
     CK(cudaGetLastError());
     return true;
   }
@@ -816,20 +842,20 @@ class Engine : public EngineBase {
   dim3 node_grid() const { return dim3((n_[0] + 31) / 32, (n_[1] + 7) / 8, n_[2]); }
 
   template <int INTERP, bool F>
-  void sl_integ(const SplineAxes<T> &sa, const VelFields<T> &V, FieldPtrs<T> fo, FieldPtrsW<T> fn, StageTimes S, T dt) {
+  void sl_integ(const SplineAxes<T> &sa, const VelFields<TV> &V, FieldPtrs<T> fo, FieldPtrsW<T> fn, StageTimes S, T dt) {
     const dim3 blk(32, 8, 1), grd = node_grid();
     int *err = &red_->err;
     counters_.kernel_launches++;
     switch (opt_->integrator) {
-      case 0: k_sl_subcycle<T, EULER_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
-      case 1: k_sl_subcycle<T, TRAPEZOIDAL_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
-      case 2: k_sl_subcycle<T, RK2_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
-      case 3: k_sl_subcycle<T, RK3_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
-      default: k_sl_subcycle<T, RK4_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
+      case 0: k_sl_subcycle<T, TV, EULER_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
+      case 1: k_sl_subcycle<T, TV, TRAPEZOIDAL_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
+      case 2: k_sl_subcycle<T, TV, RK2_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
+      case 3: k_sl_subcycle<T, TV, RK3_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
+      default: k_sl_subcycle<T, TV, RK4_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
     }
   }
 
-  bool launch_sl(int iv, const SplineAxes<T> &sa, const VelFields<T> &V, FieldPtrs<T> fo, FieldPtrsW<T> fn, StageTimes S, T dt,
+  bool launch_sl(int iv, const SplineAxes<T> &sa, const VelFields<TV> &V, FieldPtrs<T> fo, FieldPtrsW<T> fn, StageTimes S, T dt,
                  std::string &msg) {
     const bool F = dg_.P.has_flags != 0;
     if (iv == INTERP_NEAREST) F ? sl_integ<INTERP_NEAREST, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_NEAREST, false>(sa, V, fo, fn, S, dt);
@@ -841,21 +867,21 @@ class Engine : public EngineBase {
   }
 
   template <int INTERP, bool F>
-  void fwd_integ(const SplineAxes<T> &sa, const VelFields<T> &V, Particles<T> P, StageTimes S, T dt) {
+  void fwd_integ(const SplineAxes<T> &sa, const VelFields<TV> &V, Particles<T> P, StageTimes S, T dt) {
     const int blk = 256, grd = (int)((N_ + blk - 1) / blk);
     int *err = &red_->err;
     const int np = (int)N_;
     counters_.kernel_launches++;
     switch (opt_->integrator) {
-      case 0: k_fwd_subcycle<T, EULER_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, P, S, dt, np, err); break;
-      case 1: k_fwd_subcycle<T, TRAPEZOIDAL_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, P, S, dt, np, err); break;
-      case 2: k_fwd_subcycle<T, RK2_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, P, S, dt, np, err); break;
-      case 3: k_fwd_subcycle<T, RK3_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, P, S, dt, np, err); break;
-      default: k_fwd_subcycle<T, RK4_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, P, S, dt, np, err); break;
+      case 0: k_fwd_subcycle<T, TV, EULER_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, P, S, dt, np, err); break;
+      case 1: k_fwd_subcycle<T, TV, TRAPEZOIDAL_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, P, S, dt, np, err); break;
+      case 2: k_fwd_subcycle<T, TV, RK2_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, P, S, dt, np, err); break;
+      case 3: k_fwd_subcycle<T, TV, RK3_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, P, S, dt, np, err); break;
+      default: k_fwd_subcycle<T, TV, RK4_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, P, S, dt, np, err); break;
     }
   }
 
-  bool launch_fwd(int iv, const SplineAxes<T> &sa, const VelFields<T> &V, Particles<T> P, StageTimes S, T dt, std::string &msg) {
+  bool launch_fwd(int iv, const SplineAxes<T> &sa, const VelFields<TV> &V, Particles<T> P, StageTimes S, T dt, std::string &msg) {
     const bool F = dg_.P.has_flags != 0;
     if (iv == INTERP_NEAREST) F ? fwd_integ<INTERP_NEAREST, true>(sa, V, P, S, dt) : fwd_integ<INTERP_NEAREST, false>(sa, V, P, S, dt);
     else if (iv == INTERP_LINEAR) F ? fwd_integ<INTERP_LINEAR, true>(sa, V, P, S, dt) : fwd_integ<INTERP_LINEAR, false>(sa, V, P, S, dt);
@@ -865,7 +891,7 @@ class Engine : public EngineBase {
     return true;
   }
 
-  bool launch_snapshot(Diag<T> &d, int s, std::string &msg) {
+  bool launch_snapshot(DiagT &d, int s, std::string &msg) {
     const dim3 blk(32, 8, 1), grd = node_grid();
     FieldPtrs<T> src{};
     FieldPtrsW<T> dst{};
@@ -887,7 +913,7 @@ class Engine : public EngineBase {
     return true;
   }
 
-  bool launch_compose(int iv, const SplineAxes<T> &sa, Diag<T> &d, int m, std::string &msg) {
+  bool launch_compose(int iv, const SplineAxes<T> &sa, DiagT &d, int m, std::string &msg) {
     const dim3 blk(32, 8, 1), grd = node_grid();
     FieldPtrsW<T> out{};
     for (int c = 0; c < 3; c++) out.f[c] = d.composed[c];
@@ -906,7 +932,7 @@ class Engine : public EngineBase {
     return true;
   }
 
-  bool launch_ftle(Diag<T> &d, std::string &msg) {
+  bool launch_ftle(DiagT &d, std::string &msg) {
     const dim3 blk(32, 8, 1), grd = node_grid();
     FieldPtrs<T> f{};
     for (int c = 0; c < 3; c++) f.f[c] = d.composed[c];
@@ -919,7 +945,7 @@ class Engine : public EngineBase {
     return true;
   }
 
-  void launch_reset(Diag<T> &d) {
+  void launch_reset(DiagT &d) {
     const dim3 blk(32, 8, 1), grd = node_grid();
     counters_.kernel_launches++;
     k_reset_particles<T><<<grd, blk, 0, stream_>>>(dg_, d.P);
@@ -933,15 +959,16 @@ class Engine : public EngineBase {
   std::vector<cudaEvent_t> ev_, kev_;
   int n_[3] = {0, 0, 0};
   long N_ = 0, ntot_ = 0;
-  T *u_[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
-  T *ucoef_[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  TV *u_[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  TV *ucoef_[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
   int ucoef_deg_[2] = {0, 0};
   int cur_ = 0;
   lcsdata_t *stage_ = nullptr;
   DevReduce *red_ = nullptr, *red_host_ = nullptr;
   int red_err_ = 0;
   SplineSet<T> splines_[4];
-  std::vector<Diag<T>> diags_;
+  SplineSet<TV> vsplines_[4];
+  std::vector<DiagT> diags_;
   lcsdata_t t_n_ = 0, t_np1_ = 0;
   bool first_call_ = true;
   Counters counters_;

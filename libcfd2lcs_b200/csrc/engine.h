@@ -24,7 +24,7 @@ struct Options {
   int aux_grid = 0;
   int velocity_invariants = 0;
   double cfl = 0.5;
-  int mixed_precision = 0;  // extension: FP32 advection/composition, FP64 Cauchy-Green + eigen
+  int mixed_precision = 0;  // extension: FP32 velocity fields and interpolation taps, FP64 positions / flow maps
 };
 
 struct Counters {

@@ -43,9 +43,12 @@ __device__ __forceinline__ T inv_half_span(const DevGrid<T> &g, int a, int i, in
 // copies + set_velocity_bc as ghost writes (src/cfd2lcs.f90:112-117), and the CFL maximum
 // of set_dt (src/lp_motion_m.f90:86-98) as a block reduction plus atomics.
 // ---------------------------------------------------------------------------------------
-template <typename T, typename U, bool HAS_FLAGS>
+// T: grid / interface type (lcsdata_t); TV: velocity storage type.  The CFL number is
+// computed from the caller's values in the interface precision, so the subcycle count does
+// not depend on the storage type.
+template <typename T, typename TV, typename U, bool HAS_FLAGS>
 __global__ void __launch_bounds__(256) k_ingest(DevGrid<T> g, const U *__restrict__ su, const U *__restrict__ sv,
-                                                 const U *__restrict__ sw, T *u0, T *u1, T *u2, DevReduce *red) {
+                                                 const U *__restrict__ sw, TV *u0, TV *u1, TV *u2, DevReduce *red) {
   int i, j, k;
   const bool ok = node_of_thread(g.P.n, i, j, k);
   double c = 0.0;
@@ -53,18 +56,20 @@ __global__ void __launch_bounds__(256) k_ingest(DevGrid<T> g, const U *__restric
   if (ok) {
     const int s = interior_index(g.P.n, i, j, k);
     const int p = pidx(g.P.sx, g.P.sxy, i, j, k);
-    T vpre[3] = {T(su[s]), T(sv[s]), T(sw[s])};
-    T vfin[3] = {vpre[0], vpre[1], vpre[2]};
-    if (HAS_FLAGS && g.flag[p] == LCS_MASK) vfin[0] = vfin[1] = vfin[2] = T(0);
+    T in[3] = {T(su[s]), T(sv[s]), T(sw[s])};
+    const bool masked = HAS_FLAGS && g.flag[p] == LCS_MASK;
+    if (masked) in[0] = in[1] = in[2] = T(0);
+    TV vpre[3] = {TV(su[s]), TV(sv[s]), TV(sw[s])};
+    TV vfin[3] = {TV(in[0]), TV(in[1]), TV(in[2])};
     u0[p] = vfin[0];
     u1[p] = vfin[1];
     u2[p] = vfin[2];
-    T *const f[3] = {u0, u1, u2};
-    write_ghosts<T, HAS_FLAGS, GHOST_VEL>(g, f, i, j, k, vpre, vfin, &red->err);
+    TV *const f[3] = {u0, u1, u2};
+    write_ghosts<T, HAS_FLAGS, GHOST_VEL, TV>(g, f, i, j, k, vpre, vfin, &red->err);
     T cf = T(0);
-    cf = cf + fabs(vfin[0] * inv_half_span(g, 0, i, j, k));
-    cf = cf + fabs(vfin[1] * inv_half_span(g, 1, i, j, k));
-    cf = cf + fabs(vfin[2] * inv_half_span(g, 2, i, j, k));
+    cf = cf + fabs(in[0] * inv_half_span(g, 0, i, j, k));
+    cf = cf + fabs(in[1] * inv_half_span(g, 1, i, j, k));
+    cf = cf + fabs(in[2] * inv_half_span(g, 2, i, j, k));
     c = (double)cf;
     bad = !(c <= DBL_MAX);
   }
@@ -106,8 +111,8 @@ __global__ void __launch_bounds__(256) k_ingest(DevGrid<T> g, const U *__restric
 // fm_new = (fm_old(x_dep) + (x_dep - x_grid)) * mask, then the flow-map ghost ring
 // (exchange_sdata + set_flowmap_bc) from the boundary threads.
 // ---------------------------------------------------------------------------------------
-template <typename T, int INTEG, int INTERP, bool HAS_FLAGS>
-__global__ void __launch_bounds__(256) k_sl_subcycle(DevGrid<T> g, SplineAxes<T> sa, VelFields<T> V, FieldPtrs<T> fmo,
+template <typename T, typename TV, int INTEG, int INTERP, bool HAS_FLAGS>
+__global__ void __launch_bounds__(256) k_sl_subcycle(DevGrid<T> g, SplineAxes<T> sa, VelFields<TV> V, FieldPtrs<T> fmo,
                                                       FieldPtrsW<T> fmn, StageTimes S, T dt, int *err) {
   int i, j, k;
   if (!node_of_thread(g.P.n, i, j, k)) return;
@@ -115,7 +120,7 @@ __global__ void __launch_bounds__(256) k_sl_subcycle(DevGrid<T> g, SplineAxes<T>
   const T x0[3] = {__ldg(g.lt[0] + i), __ldg(g.lt[1] + j), __ldg(g.lt[2] + k)};
   int no[3] = {i, j, k};
   T x[3];
-  integrate<T, INTEG, INTERP>(g, sa, V, S, dt, x0, no, x);
+  integrate<T, TV, INTEG, INTERP>(g, sa, V, S, dt, x0, no, x);
   project_plane(g, no, x);
   const bool stick = particle_bc<T, HAS_FLAGS>(g, no, x, err);
   if (stick) {
@@ -144,15 +149,15 @@ __global__ void __launch_bounds__(256) k_sl_subcycle(DevGrid<T> g, SplineAxes<T>
 // project, BC, stick, accumulate the displacement, one pass of the node search and the
 // periodic wrap of exchange_lpdata.  Particle q starts at interior node q.
 // ---------------------------------------------------------------------------------------
-template <typename T, int INTEG, int INTERP, bool HAS_FLAGS>
-__global__ void __launch_bounds__(256) k_fwd_subcycle(DevGrid<T> g, SplineAxes<T> sa, VelFields<T> V, Particles<T> P, StageTimes S,
+template <typename T, typename TV, int INTEG, int INTERP, bool HAS_FLAGS>
+__global__ void __launch_bounds__(256) k_fwd_subcycle(DevGrid<T> g, SplineAxes<T> sa, VelFields<TV> V, Particles<T> P, StageTimes S,
                                                        T dt, int np, int *err) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= np) return;
   T xn[3] = {P.x[0][q], P.x[1][q], P.x[2][q]};
   int no[3] = {P.no[0][q], P.no[1][q], P.no[2][q]};
   T x[3];
-  integrate<T, INTEG, INTERP>(g, sa, V, S, dt, xn, no, x);
+  integrate<T, TV, INTEG, INTERP>(g, sa, V, S, dt, xn, no, x);
   project_plane(g, no, x);
   const bool stick = particle_bc<T, HAS_FLAGS>(g, no, x, err);
   if (stick) {
@@ -389,53 +394,103 @@ __global__ void __launch_bounds__(256) k_blend(FieldPtrs<T> a, FieldPtrs<T> b, F
 
 // ---------------------------------------------------------------------------------------
 // B-spline fit: banded solves along one axis for every line of the padded field (the three
-// dbtpcf passes of db3ink, src/bspline/bspline_sub_module.f90:451-533), one thread per line.
-// Lines along y and z are read by adjacent threads at adjacent i (coalesced); along x each
-// thread walks its own contiguous line through L1.
+// dbtpcf passes of db3ink, src/bspline/bspline_sub_module.f90:451-533), one lane per line,
+// pull-form forward and backward sweeps (pull_forward / pull_backward).  The first pass of
+// a fit reads the source field and writes the coefficient field (the copy db3ink makes is
+// fused in); the later passes run in place (src == dst).
 // ---------------------------------------------------------------------------------------
-// A block of four warps stages 32 lines of one component in shared memory as
-// [element][line] (padded leading dimension), with coalesced loads and stores spread over
-// all four warps; warp 0 then solves one line per lane.
-//   lines_adjacent = true  (y and z passes): line l starts at base + l, elements step by es
-//   lines_adjacent = false (x pass):         line l starts at base + l * ls, elements step by 1
-// Block b covers lines 32*(b % nblk_fast) .. +31 of block row b / nblk_fast (stride_other).
+// y and z passes: lines start at adjacent addresses (consecutive i), so element e of 32 lines
+// is one coalesced row.  Line L starts at L % nfast + (L / nfast) * so; elements es apart.
+// Loads are issued G at a time ahead of the dependent sweep.
 template <typename T, int K>
-__global__ void __launch_bounds__(128) k_fit_smem(SplineAxis<T> A, FieldPtrsW<T> f, int lines_adjacent, int nfast, int nblk_fast,
-                                                   long es, long ls, long stride_other) {
-  extern __shared__ unsigned char smem_raw[];
-  T *buf = reinterpret_cast<T *>(smem_raw);
-  constexpr int LD = 33;
-  const int n = A.n, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  T *fc = f.f[blockIdx.y];
-  const int bf = blockIdx.x % nblk_fast, bo = blockIdx.x / nblk_fast;
-  const int l0 = bf * 32;
-  const int nl = min(32, nfast - l0);
-  if (lines_adjacent) {
-    T *base = fc + l0 + (long)bo * stride_other;
-    if (lane < nl) {
+__global__ void __launch_bounds__(256) k_fit_lines(SplineAxis<T> A, FieldPtrs<T> src, FieldPtrsW<T> dst, int nfast, long nlines,
+                                                    long es, long so) {
+  const long L = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (L >= nlines) return;
+  const long off = L % nfast + (L / nfast) * so;
+  const T *s = src.f[blockIdx.y] + off;
+  T *d = dst.f[blockIdx.y] + off;
+  const int n = A.n;
+  const T *pc = A.pull;
+  constexpr int G = 8;
+  T win[3] = {T(0), T(0), T(0)};
+  for (int i0 = 0; i0 < n; i0 += G) {
+    T v[G];
+#pragma unroll
+    for (int g = 0; g < G; g++) v[g] = (i0 + g < n) ? s[(long)(i0 + g) * es] : T(0);
+#pragma unroll
+    for (int g = 0; g < G; g++)
+      if (i0 + g < n) v[g] = pull_forward<T, K>(pc, i0 + g, v[g], win);
+#pragma unroll
+    for (int g = 0; g < G; g++)
+      if (i0 + g < n) d[(long)(i0 + g) * es] = v[g];
+  }
+  win[0] = win[1] = win[2] = T(0);
+  for (int i1 = n - 1; i1 >= 0; i1 -= G) {
+    T v[G];
+#pragma unroll
+    for (int g = 0; g < G; g++) v[g] = (i1 - g >= 0) ? d[(long)(i1 - g) * es] : T(0);
+#pragma unroll
+    for (int g = 0; g < G; g++)
+      if (i1 - g >= 0) v[g] = pull_backward<T, K>(pc, i1 - g, v[g], win);
+#pragma unroll
+    for (int g = 0; g < G; g++)
+      if (i1 - g >= 0) d[(long)(i1 - g) * es] = v[g];
+  }
+}
+
+// x pass: lines are contiguous.  One warp per 32 lines (consecutive j at one k): each chunk of
+// 32 elements of the 32 lines is staged through a shared tile with coalesced row loads,
+// swept by one lane per line inside the tile, and written back with coalesced row stores.
+template <typename T, int K>
+__global__ void __launch_bounds__(128) k_fit_xlines(SplineAxis<T> A, FieldPtrs<T> src, FieldPtrsW<T> dst, int ny, int nz, long sx,
+                                                     long sxy) {
+  __shared__ T tile[4][32][33];
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  const int nbf = (ny + 31) / 32;
+  const long gw = (long)blockIdx.x * 4 + wp;
+  if (gw >= (long)nbf * nz) return;  // warp-uniform
+  const int j0 = (int)(gw % nbf) * 32;
+  const int nl = min(32, ny - j0);
+  const long base = (long)j0 * sx + (gw / nbf) * sxy;
+  const T *s = src.f[blockIdx.y] + base;
+  T *d = dst.f[blockIdx.y] + base;
+  T(*t)[33] = tile[wp];
+  const int n = A.n;
+  const T *pc = A.pull;
+  T win[3] = {T(0), T(0), T(0)};
+  for (int c0 = 0; c0 < n; c0 += 32) {
+    const int ne = min(32, n - c0);
+    if (lane < ne) {
 #pragma unroll 8
-      for (int e = warp; e < n; e += 4) buf[e * LD + lane] = base[(long)e * es + lane];
+      for (int r = 0; r < nl; r++) t[r][lane] = s[(long)r * sx + c0 + lane];
     }
-    __syncthreads();
-    if (warp == 0 && lane < nl) band_solve_window<T, K>(A, buf + lane, LD);
-    __syncthreads();
-    if (lane < nl) {
+    __syncwarp();
+    if (lane < nl)
+      for (int e = 0; e < ne; e++) t[lane][e] = pull_forward<T, K>(pc, c0 + e, t[lane][e], win);
+    __syncwarp();
+    if (lane < ne) {
 #pragma unroll 8
-      for (int e = warp; e < n; e += 4) base[(long)e * es + lane] = buf[e * LD + lane];
+      for (int r = 0; r < nl; r++) d[(long)r * sx + c0 + lane] = t[r][lane];
     }
-  } else {
-    T *base = fc + (long)l0 * ls + (long)bo * stride_other;
-    for (int l = warp; l < nl; l += 4) {
+    __syncwarp();
+  }
+  win[0] = win[1] = win[2] = T(0);
+  for (int c0 = ((n - 1) / 32) * 32; c0 >= 0; c0 -= 32) {
+    const int ne = min(32, n - c0);
+    if (lane < ne) {
 #pragma unroll 8
-      for (int e = lane; e < n; e += 32) buf[e * LD + l] = base[(long)l * ls + e];
+      for (int r = 0; r < nl; r++) t[r][lane] = d[(long)r * sx + c0 + lane];
     }
-    __syncthreads();
-    if (warp == 0 && lane < nl) band_solve_window<T, K>(A, buf + lane, LD);
-    __syncthreads();
-    for (int l = warp; l < nl; l += 4) {
+    __syncwarp();
+    if (lane < nl)
+      for (int e = ne - 1; e >= 0; e--) t[lane][e] = pull_backward<T, K>(pc, c0 + e, t[lane][e], win);
+    __syncwarp();
+    if (lane < ne) {
 #pragma unroll 8
-      for (int e = lane; e < n; e += 32) base[(long)l * ls + e] = buf[e * LD + l];
+      for (int r = 0; r < nl; r++) d[(long)r * sx + c0 + lane] = t[r][lane];
     }
+    __syncwarp();
   }
 }
 

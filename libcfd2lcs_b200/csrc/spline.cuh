@@ -24,7 +24,7 @@ struct SplineAxis {
   int k;          // order (degree + 1)
   const T *t;     // n + k knots
   const T *rinv;  // per interval l (1-based, stored at l-1): 1/(t(l+r) - t(l+r-j)), 6 slots
-  const T *lu;    // band LU of the collocation matrix, (2k-1) x n column-major
+  const T *pull;  // band LU of the collocation matrix in pull form, 8 values per element
 };
 
 template <typename T>
@@ -104,28 +104,31 @@ __device__ __forceinline__ bool spline_stencil(const DevGrid<T> &g, const Spline
   return true;
 }
 
-template <typename T, int KC>
-__device__ __forceinline__ T spline_apply(const DevGrid<T> &g, const SplineAxes<T> &S, const SplineStencil<T> &st,
-                                          const T *__restrict__ coef) {
+// Tensor contraction of the k x k x k coefficients around the stencil, x then y then z.
+// TC is the coefficient type: the mixed-precision form contracts FP32 velocity coefficients
+// with the basis values rounded to FP32.
+template <typename T, int KC, typename TC = T>
+__device__ __forceinline__ TC spline_apply(const DevGrid<T> &g, const SplineAxes<T> &S, const SplineStencil<T> &st,
+                                           const TC *__restrict__ coef) {
   const int kx = KC ? KC : S.ax[0].k, ky = KC ? KC : S.ax[1].k, kz = KC ? KC : S.ax[2].k;
-  T vz = T(0);
+  TC vz = TC(0);
 #pragma unroll
   for (int c2 = 0; c2 < 4; c2++) {
     if (c2 >= kz) break;
-    T vy = T(0);
+    TC vy = TC(0);
 #pragma unroll
     for (int c1 = 0; c1 < 4; c1++) {
       if (c1 >= ky) break;
-      const T *row = coef + st.p0 + c1 * g.P.sx + c2 * g.P.sxy;
-      T vx = T(0);
+      const TC *row = coef + st.p0 + c1 * g.P.sx + c2 * g.P.sxy;
+      TC vx = TC(0);
 #pragma unroll
       for (int c0 = 0; c0 < 4; c0++) {
         if (c0 >= kx) break;
-        vx += st.b[0][c0] * __ldg(row + c0);
+        vx += TC(st.b[0][c0]) * __ldg(row + c0);
       }
-      vy += st.b[1][c1] * vx;
+      vy += TC(st.b[1][c1]) * vx;
     }
-    vz += st.b[2][c2] * vy;
+    vz += TC(st.b[2][c2]) * vy;
   }
   return vz;
 }
@@ -134,72 +137,37 @@ __device__ __forceinline__ T spline_apply(const DevGrid<T> &g, const SplineAxes<
 // Banded solve of one line in place (dbnslv, src/bspline/bspline_sub_module.f90:2202-2259):
 // forward elimination with the unit lower factor, then back substitution.
 // ---------------------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ void band_solve_line(const SplineAxis<T> &A, T *b, long stride) {
-  const int n = A.n, k = A.k, nr = 2 * k - 1, mid = k;  // mid is 1-based
-  const T *w = A.lu;
-#define Wm(r, c) __ldg(w + ((r)-1) + (size_t)nr * ((c)-1))
-#define Bm(i) b[(long)((i)-1) * stride]
-  if (n != 1) {
-    for (int i = 1; i <= n - 1; i++) {
-      const T bi = Bm(i);
-      const int jmax = min(k - 1, n - i);
-      for (int j = 1; j <= jmax; j++) Bm(i + j) = Bm(i + j) - bi * Wm(mid + j, i);
-    }
-    for (int i = n; i >= 2; i--) {
-      const T bi = Bm(i) / Wm(mid, i);
-      Bm(i) = bi;
-      const int jmax = min(k - 1, i - 1);
-      for (int j = 1; j <= jmax; j++) Bm(i - j) = Bm(i - j) - bi * Wm(mid - j, i);
-    }
-  }
-  Bm(1) = Bm(1) / Wm(mid, 1);
-#undef Wm
-#undef Bm
+// Banded substitutions of the collocation LU (dbnfac / dbnslv, src/bspline/
+// bspline_sub_module.f90:2098-2259) in pull form.  For element i (1-based) the host stores
+//   pull[8(i-1) + j-1]     = L(i, i-j) = W(mid+j, i-j)   j = 1..k-1  (0 where i-j < 1)
+//   pull[8(i-1) + 3 + j-1] = U(i, i+j) = W(mid-j, i+j)   j = 1..k-1  (0 where i+j > n)
+//   pull[8(i-1) + 6]       = 1 / W(mid, i)
+// Forward: x(i) = b(i) - L(i,i-k+1) x(i-k+1) - ... - L(i,i-1) x(i-1), the updates in the order
+// in which dbnslv's row-by-row elimination applies them.  Backward: x(i) = (b(i) - U(i,i+k-1)
+// x(i+k-1) - ... - U(i,i+1) x(i+1)) * (1 / W(mid,i)).  Each element needs only the k-1
+// solved neighbours before it, kept in registers, so a line streams through once per sweep.
+// win[0] holds the nearest solved neighbour.
+template <typename T, int K>
+__device__ __forceinline__ T pull_forward(const T *__restrict__ pc, int i0, T b, T (&win)[3]) {
+  const T *c = pc + 8 * i0;  // i0 = i - 1
+#pragma unroll
+  for (int j = K - 1; j >= 1; j--) b = b - win[j - 1] * __ldg(c + j - 1);
+  win[2] = win[1];
+  win[1] = win[0];
+  win[0] = b;
+  return b;
 }
 
-// Same solve with a register window of k values per pass: every element is loaded and
-// stored once in the forward and once in the backward pass, and receives its updates in the
-// reference's order (forward: from rows i = m-k+1 .. m-1; backward: from i = m+k-1 .. m+1).
 template <typename T, int K>
-__device__ __forceinline__ void band_solve_window(const SplineAxis<T> &A, T *b, long stride) {
-  const int n = A.n, nr = 2 * K - 1, mid = K;
-  const T *w = A.lu;
-#define Wm(r, c) __ldg(w + ((r)-1) + (size_t)nr * ((c)-1))
-  T win[K];
-  if (n == 1) {
-    b[0] = b[0] / Wm(mid, 1);
-    return;
-  }
-  // forward elimination: window holds b(i) .. b(i+K-1)
+__device__ __forceinline__ T pull_backward(const T *__restrict__ pc, int i0, T b, T (&win)[3]) {
+  const T *c = pc + 8 * i0;
 #pragma unroll
-  for (int q = 0; q < K; q++) win[q] = (q < n) ? b[(long)q * stride] : T(0);
-  for (int i = 1; i <= n - 1; i++) {
-    const T bi = win[0];
-    b[(long)(i - 1) * stride] = bi;
-#pragma unroll
-    for (int j = 1; j < K; j++)
-      if (i + j <= n) win[j] = win[j] - bi * Wm(mid + j, i);
-#pragma unroll
-    for (int q = 0; q < K - 1; q++) win[q] = win[q + 1];
-    win[K - 1] = (i + K <= n) ? b[(long)(i + K - 1) * stride] : T(0);
-  }
-  b[(long)(n - 1) * stride] = win[0];
-  // back substitution: window holds b(i), b(i-1), .., b(i-K+1)
-#pragma unroll
-  for (int q = 0; q < K; q++) win[q] = (n - q >= 1) ? b[(long)(n - 1 - q) * stride] : T(0);
-  for (int i = n; i >= 2; i--) {
-    const T bi = win[0] / Wm(mid, i);
-    b[(long)(i - 1) * stride] = bi;
-#pragma unroll
-    for (int j = 1; j < K; j++)
-      if (i - j >= 1) win[j] = win[j] - bi * Wm(mid - j, i);
-#pragma unroll
-    for (int q = 0; q < K - 1; q++) win[q] = win[q + 1];
-    win[K - 1] = (i - K >= 1) ? b[(long)(i - K - 1) * stride] : T(0);
-  }
-  b[0] = win[0] / Wm(mid, 1);
-#undef Wm
+  for (int j = K - 1; j >= 1; j--) b = b - win[j - 1] * __ldg(c + 3 + j - 1);
+  b = b * __ldg(c + 6);
+  win[2] = win[1];
+  win[1] = win[0];
+  win[0] = b;
+  return b;
 }
 
 }  // namespace cfd2lcs
