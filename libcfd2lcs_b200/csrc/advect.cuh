@@ -124,6 +124,20 @@ __device__ __forceinline__ void sample_velocity(const DevGrid<T> &g, const Splin
   }
 }
 
+// Velocity at a grid node, for a first stage that starts on the node (the backward SL
+// subcycle): every interpolator reproduces the nodal data there -- NEAREST and LINEAR
+// bitwise (the trilinear weights are exactly 0 and 1), the B-splines to rounding, since they
+// interpolate the padded data at the abscissae, which are the node lines -- so the stage
+// reads the two velocity levels at the node instead of the 64-tap stencil.
+template <typename T, typename TV>
+__device__ __forceinline__ void sample_velocity_node(const DevGrid<T> &g, const VelFields<TV> &V, const int no[3], T ct_, T out[3]) {
+  const TV ct = TV(ct_);
+  const TV omc = TV(1) - ct;
+  const int p = pidx(g.P.sx, g.P.sxy, no[0], no[1], no[2]);
+#pragma unroll
+  for (int c = 0; c < 3; c++) out[c] = T(omc * __ldg(V.un[c] + p) + ct * __ldg(V.unp1[c] + p));
+}
+
 template <typename T, int INTERP>
 __device__ __forceinline__ void sample_field(const DevGrid<T> &g, const SplineAxes<T> &sa, const T *const f[3], const T x[3],
                                              const int no[3], T out[3]) {
@@ -160,17 +174,22 @@ struct StageTimes {
   double ct[4];
 };
 
-template <typename T, typename TV, int INTEG, int INTERP>
+// AT_NODE: xn is the coordinate of node no (first stage by sample_velocity_node)
+template <typename T, typename TV, int INTEG, int INTERP, bool AT_NODE = false>
 __device__ __forceinline__ void integrate(const DevGrid<T> &g, const SplineAxes<T> &sa, const VelFields<TV> &V, const StageTimes &S,
                                           T dt, const T xn[3], const int no[3], T x[3]) {
   const T HALF = T(1) / T(2), THIRD = T(1) / T(3), TWOTHIRD = T(2) / T(3), SIXTH = T(1) / T(6), TWO = T(2);
   T u[3];
+  auto first_stage = [&](T ct) {
+    if (AT_NODE) sample_velocity_node<T, TV>(g, V, no, ct, u);
+    else sample_velocity<T, TV, INTERP>(g, sa, V, xn, no, ct, 0, u);
+  };
   if (INTEG == EULER_ || INTEG == TRAPEZOIDAL_) {
-    sample_velocity<T, TV, INTERP>(g, sa, V, xn, no, T(S.ct[0]), 0, u);
+    first_stage(T(S.ct[0]));
 #pragma unroll
     for (int c = 0; c < 3; c++) x[c] = xn[c] + dt * u[c];
   } else if (INTEG == RK2_) {
-    sample_velocity<T, TV, INTERP>(g, sa, V, xn, no, T(S.ct[0]), 0, u);
+    first_stage(T(S.ct[0]));
     T xh[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) xh[c] = xn[c] + HALF * dt * u[c];
@@ -179,7 +198,7 @@ __device__ __forceinline__ void integrate(const DevGrid<T> &g, const SplineAxes<
     for (int c = 0; c < 3; c++) x[c] = xn[c] + dt * u[c];
   } else if (INTEG == RK3_) {
     T k[3], xs[3], acc[3];
-    sample_velocity<T, TV, INTERP>(g, sa, V, xn, no, T(S.ct[0]), 0, u);
+    first_stage(T(S.ct[0]));
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];
@@ -201,7 +220,7 @@ __device__ __forceinline__ void integrate(const DevGrid<T> &g, const SplineAxes<
     }
   } else {  // RK4
     T k[3], xs[3], acc[3];
-    sample_velocity<T, TV, INTERP>(g, sa, V, xn, no, T(S.ct[0]), 0, u);
+    first_stage(T(S.ct[0]));
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];
@@ -289,60 +308,60 @@ __device__ __forceinline__ bool particle_bc(const DevGrid<T> &g, int no[3], T x[
 // neighbours (fewer on a 2-D grid) in NBR_OFFSET order (src/data_m.f90:124-152) and moves
 // to one that is closer than 0.99 of the best so far.
 // ---------------------------------------------------------------------------------------
-__constant__ int8_t c_nbr[27][3] = {
-    {0, 0, 0},   {-1, 0, 0},  {0, -1, 0}, {0, 0, -1}, {1, 0, 0},  {0, 1, 0},  {0, 0, 1},   {-1, -1, -1}, {0, -1, -1},
-    {1, -1, -1}, {-1, 0, -1}, {1, 0, -1}, {-1, 1, -1}, {0, 1, -1}, {1, 1, -1}, {-1, -1, 0}, {1, -1, 0},  {-1, 1, 0},
-    {1, 1, 0},   {-1, -1, 1}, {0, -1, 1}, {1, -1, 1},  {-1, 0, 1}, {1, 0, 1},  {-1, 1, 1},  {0, 1, 1},   {1, 1, 1}};
+// NBR_OFFSET as a constant expression; the search loop unrolls over it
+__device__ __forceinline__ constexpr int nbr_offset(int nb, int a) {
+  constexpr int8_t t[27][3] = {
+      {0, 0, 0},   {-1, 0, 0},  {0, -1, 0}, {0, 0, -1}, {1, 0, 0},  {0, 1, 0},  {0, 0, 1},   {-1, -1, -1}, {0, -1, -1},
+      {1, -1, -1}, {-1, 0, -1}, {1, 0, -1}, {-1, 1, -1}, {0, 1, -1}, {1, 1, -1}, {-1, -1, 0}, {1, -1, 0},  {-1, 1, 0},
+      {1, 1, 0},   {-1, -1, 1}, {0, -1, 1}, {1, -1, 1},  {-1, 0, 1}, {1, 0, 1},  {-1, 1, 1},  {0, 1, 1},   {1, 1, 1}};
+  return t[nb][a];
+}
+
+// product rounded on its own (never contracted into an FMA), as the reference's compiled
+// distance arithmetic forms it
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 
 template <typename T>
 __device__ __forceinline__ bool track_pass(const DevGrid<T> &g, const T x[3], int no[3]) {
+  // Per axis and offset o in {-1,0,1}: the squared axis distance to line no+o (clamped to
+  // the padded range).  Off the interior the padded grid (sgrid%grid, src/sgrid_m.f90:
+  // 182-359) holds one of two ghost coordinates: the periodic image when every out-of-range
+  // axis of the candidate is periodic (sqp), the extrapolated one otherwise (sqn).  A
+  // candidate's squared distance is then a sum of three register values; the 27 candidates
+  // are unrolled with constant offsets.
+  const int sa = g.P.single_axis;
+  T sqp[3][3], sqn[3][3];
+  unsigned ok = 0;  // bit 3a+o+1: line no[a]+o is interior, or axis a is periodic
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+#pragma unroll
+    for (int o = -1; o <= 1; o++) {
+      const int v = min(max(no[a] + o, 0), g.P.n[a] + 1);
+      const bool in = v >= 1 && v <= g.P.n[a];
+      T cp, cn;
+      if (in) {
+        cp = cn = __ldg(g.lt[a] + v);
+      } else {
+        cp = v < 1 ? g.P.gx[a][0][1] : g.P.gx[a][1][1];
+        cn = v < 1 ? g.P.gx[a][0][0] : g.P.gx[a][1][0];
+      }
+      const T dp = cp - x[a], dn = cn - x[a];
+      sqp[a][o + 1] = mul_rn(dp, dp);
+      sqn[a][o + 1] = mul_rn(dn, dn);
+      if (in || g.P.per[a]) ok |= 1u << (3 * a + o + 1);
+    }
+  }
   T best = T(0);
   bool have = false;
   int off[3] = {0, 0, 0};
-  const int sa = g.P.single_axis;
-  // fast path: every candidate node is an interior node, so its coordinates are the lines
-  // and the squared distances separate per axis (same values, same summation order)
-  bool inner = true;
 #pragma unroll
-  for (int a = 0; a < 3; a++)
-    if (a != sa && (no[a] < 2 || no[a] > g.P.n[a] - 1)) inner = false;
-  if (inner) {
-    T sq[3][3];
-#pragma unroll
-    for (int a = 0; a < 3; a++)
-#pragma unroll
-      for (int o = 0; o < 3; o++) {
-        const int v = (a == sa) ? no[a] : no[a] + o - 1;
-        const T e = __ldg(g.lt[a] + v) - x[a];
-        sq[a][o] = e * e;
-      }
-    for (int nb = 0; nb < 27; nb++) {
-      const int o0 = c_nbr[nb][0], o1 = c_nbr[nb][1], o2 = c_nbr[nb][2];
-      if ((sa == 0 && o0 != 0) || (sa == 1 && o1 != 0) || (sa == 2 && o2 != 0)) continue;
-      const T r = sq[0][sa == 0 ? 1 : o0 + 1] + sq[1][sa == 1 ? 1 : o1 + 1] + sq[2][sa == 2 ? 1 : o2 + 1];
-      if (!have || r < T(0.99) * best) {
-        best = r;
-        have = true;
-        off[0] = o0;
-        off[1] = o1;
-        off[2] = o2;
-      }
-    }
-    no[0] += off[0];
-    no[1] += off[1];
-    no[2] += off[2];
-    return off[0] != 0 || off[1] != 0 || off[2] != 0;
-  }
   for (int nb = 0; nb < 27; nb++) {
-    const int o0 = c_nbr[nb][0], o1 = c_nbr[nb][1], o2 = c_nbr[nb][2];
+    const int o0 = nbr_offset(nb, 0), o1 = nbr_offset(nb, 1), o2 = nbr_offset(nb, 2);
     if ((sa == 0 && o0 != 0) || (sa == 1 && o1 != 0) || (sa == 2 && o2 != 0)) continue;
-    const int i = min(max(no[0] + o0, 0), g.P.n[0] + 1);
-    const int j = min(max(no[1] + o1, 0), g.P.n[1] + 1);
-    const int k = min(max(no[2] + o2, 0), g.P.n[2] + 1);
-    const T ex = node_coord(g, 0, i, j, k) - x[0];
-    const T ey = node_coord(g, 1, i, j, k) - x[1];
-    const T ez = node_coord(g, 2, i, j, k) - x[2];
-    const T r = ex * ex + ey * ey + ez * ez;
+    const bool e = ((ok >> (o0 + 1)) & (ok >> (3 + o1 + 1)) & (ok >> (6 + o2 + 1)) & 1u) != 0;
+    const T r = (e ? sqp[0][o0 + 1] : sqn[0][o0 + 1]) + (e ? sqp[1][o1 + 1] : sqn[1][o1 + 1]) +
+                (e ? sqp[2][o2 + 1] : sqn[2][o2 + 1]);
     // rsq < 0.99*rsq_min with rsq_min starting at huge()
     if (!have || r < T(0.99) * best) {
       best = r;

@@ -41,13 +41,17 @@ struct FieldPtrsW {
   T *f[3];
 };
 
-// Forward particles (one per lcs node, index = interior node index): position, unwrapped
-// displacement and tracked node (the reference's lp%xp, lp%dx, lp%no_scfd).
+// Forward particles (one per lcs node): position, unwrapped displacement and tracked node
+// (the reference's lp%xp, lp%dx, lp%no_scfd).  Storage slot s holds the particle that started
+// at interior node id[s]; slot[q] is the inverse map.  The engine re-sorts the slots by grid
+// cell during an update, so that a block's particles gather neighbouring spline taps.
 template <typename T>
 struct Particles {
   T *x[3];
   T *dx[3];
   int *no[3];
+  int *id;
+  int *slot;
 };
 
 __device__ __forceinline__ int pidx(const int sx, const int sxy, int i, int j, int k) { return i + sx * j + sxy * k; }
@@ -56,19 +60,6 @@ template <typename T>
 __device__ __forceinline__ T clamp01(T v) {
   // max(min(v,1),0) of the reference; a NaN argument yields the bound as gfortran does
   return fmax(fmin(v, T(1)), T(0));
-}
-
-// Coordinate c of padded node (i,j,k) (the reference's sgrid%grid), src/sgrid_m.f90:182-359.
-template <typename T>
-__device__ __forceinline__ T node_coord(const DevGrid<T> &g, int c, int i, int j, int k) {
-  const int idx[3] = {i, j, k};
-  const int v = idx[c];
-  if (v >= 1 && v <= g.P.n[c]) return __ldg(g.lt[c] + v);
-  int e = 1;
-#pragma unroll
-  for (int a = 0; a < 3; a++)
-    if ((idx[a] < 1 || idx[a] > g.P.n[a]) && !g.P.per[a]) e = 0;
-  return g.P.gx[c][v < 1 ? 0 : 1][e];
 }
 
 // ---------------------------------------------------------------------------------------

@@ -69,8 +69,11 @@ struct Diag {
   T *fm[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
   int cur = 0;
   T *fmcoef[3] = {nullptr, nullptr, nullptr};
-  // forward: particles
-  Particles<T> P{};
+  // forward: particles (P current, P2 the target of the re-sort by grid cell) and the
+  // counting sort's keys, cell counts, offsets and chunk sums
+  Particles<T> P{}, P2{};
+  unsigned *pkey = nullptr;
+  int *pcnt = nullptr, *poffs = nullptr, *ptsum = nullptr;
   // ring of sub-flow maps (padded) and their spline coefficients
   std::vector<T *> slot;      // 3 per slot
   std::vector<T *> slotcoef;  // 3 per slot (allocated on first spline use)
@@ -283,11 +286,26 @@ class Engine : public EngineBase {
           if (cudaMemsetAsync(d.fm[b][c], 0, ntot_ * sizeof(T), stream_) != cudaSuccess) return fail(msg, "memset");
         }
     } else {
-      for (int c = 0; c < 3; c++) {
-        if (!(d.P.x[c] = arena_.alloc<T>(N_, msg))) return -1;
-        if (!(d.P.dx[c] = arena_.alloc<T>(N_, msg))) return -1;
-        if (!(d.P.no[c] = arena_.alloc<int>(N_, msg))) return -1;
+      for (Particles<T> *Q : {&d.P, &d.P2}) {
+        for (int c = 0; c < 3; c++) {
+          if (!(Q->x[c] = arena_.alloc<T>(N_, msg))) return -1;
+          if (!(Q->dx[c] = arena_.alloc<T>(N_, msg))) return -1;
+          if (!(Q->no[c] = arena_.alloc<int>(N_, msg))) return -1;
+        }
+        if (!(Q->id = arena_.alloc<int>(N_, msg))) return -1;
       }
+      if (!(d.P.slot = arena_.alloc<int>(N_, msg))) return -1;
+      d.P2.slot = d.P.slot;  // the inverse map is rewritten whole by every permutation
+      const long ncell = sort_key_space(n_);
+      if (ncell > (long)std::numeric_limits<int>::max()) {
+        msg = "diagnostic_init: grid too large for the forward particle sort";
+        return -1;
+      }
+      if (!(d.pkey = arena_.alloc<unsigned>(N_, msg))) return -1;
+      if (!(d.pcnt = arena_.alloc<int>(ncell, msg))) return -1;
+      if (!(d.poffs = arena_.alloc<int>(ncell, msg))) return -1;
+      if (!(d.ptsum = arena_.alloc<int>((ncell + SORT_TILE - 1) / SORT_TILE, msg))) return -1;
+      if (cudaMemsetAsync(d.pcnt, 0, ncell * sizeof(int), stream_) != cudaSuccess) return fail(msg, "memset");
       launch_reset(d);
     }
     d.slot.assign((size_t)3 * d.nslot, nullptr);
@@ -445,6 +463,7 @@ class Engine : public EngineBase {
           CK(cudaEventRecord(kev_[2 * sc + 1], stream_));
           d.cur ^= 1;
         } else {
+          if (sc % kSortInterval == 0 && !sort_particles(d, msg)) return false;
           CK(cudaEventRecord(kev_[2 * sc], stream_));
           if (!launch_fwd(iv, sa, V, d.P, S, (T)dt, msg)) return false;
           CK(cudaEventRecord(kev_[2 * sc + 1], stream_));
@@ -706,6 +725,8 @@ class Engine : public EngineBase {
           used[b] = true;
           break;
         }
+    BlendOut<TV> o{};
+    int nout = 0;
     for (int st = 0; st < ns; st++) {
       if (pick[st] >= 0) continue;
       for (int q = 0; q < st; q++)
@@ -720,22 +741,27 @@ class Engine : public EngineBase {
       if (!d.blend[b][0])
         for (int c = 0; c < 3; c++)
           if (!(d.blend[b][c] = arena_.alloc<TV>(ntot_, msg))) return false;
-      FieldPtrs<TV> a{}, bb{};
-      FieldPtrsW<TV> out{};
-      for (int c = 0; c < 3; c++) {
-        a.f[c] = ucoef_[cur_ ^ 1][c];
-        bb.f[c] = ucoef_[cur_][c];
-        out.f[c] = d.blend[b][c];
-      }
       const TV ct = (TV)S.ct[st];
-      const dim3 grd((unsigned)((ntot_ + 255) / 256), 3);
-      k_blend<TV><<<grd, 256, 0, stream_>>>(a, bb, out, TV(1) - ct, ct, ntot_);
-      counters_.kernel_launches++;
-      CK(cudaGetLastError());
+      for (int c = 0; c < 3; c++) o.f[nout][c] = d.blend[b][c];
+      o.omc[nout] = TV(1) - ct;
+      o.ct[nout] = ct;
+      nout++;
       d.blend_ct[b] = S.ct[st];
       d.blend_update[b] = upd;
       used[b] = true;
       pick[st] = b;
+    }
+    if (nout > 0) {
+      FieldPtrs<TV> a{}, bb{};
+      for (int c = 0; c < 3; c++) {
+        a.f[c] = ucoef_[cur_ ^ 1][c];
+        bb.f[c] = ucoef_[cur_][c];
+      }
+      const long npair = (ntot_ + 1) / 2;
+      const dim3 grd((unsigned)((npair + 255) / 256), 3);
+      k_blend<TV><<<grd, 256, 0, stream_>>>(a, bb, o, nout, ntot_);
+      counters_.kernel_launches++;
+      CK(cudaGetLastError());
     }
     for (int st = 0; st < ns; st++)
       for (int c = 0; c < 3; c++) V.cs[st][c] = d.blend[pick[st]][c];
@@ -796,7 +822,13 @@ class Engine : public EngineBase {
     const int sx = dg_.P.sx, sxy = dg_.P.sxy, ny = n_[1] + 2, nz = n_[2] + 2;
     if (axis == 0) {
       const long warps = (long)((ny + 31) / 32) * nz;
-      k_fit_xlines<D, K><<<dim3((unsigned)((warps + 3) / 4), 3), 128, 0, stream_>>>(A, s, d, ny, nz, (long)sx, (long)sxy);
+      const size_t smem = sizeof(D) * 4 * 2 * 32 * 33;  // two 32 x 33 tiles per warp
+      static bool attr_done = false;
+      if (!attr_done) {
+        cudaFuncSetAttribute(k_fit_xlines<D, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr_done = true;
+      }
+      k_fit_xlines<D, K><<<dim3((unsigned)((warps + 3) / 4), 3), 128, smem, stream_>>>(A, s, d, ny, nz, (long)sx, (long)sxy);
     } else {
       // y lines: sx * nz of them, elements sx apart; z lines: sxy of them, elements sxy apart
       const int nfast = axis == 1 ? sx : sxy;
@@ -949,6 +981,25 @@ class Engine : public EngineBase {
     const dim3 blk(32, 8, 1), grd = node_grid();
     counters_.kernel_launches++;
     k_reset_particles<T><<<grd, blk, 0, stream_>>>(dg_, d.P);
+  }
+
+  // Re-sorts the particle slots by grid cell (32 x 8 tiles, x fastest) every kSortInterval
+  // subcycles, so that the particles of a block gather neighbouring spline taps as the SL
+  // kernel's blocks do.  Results do not depend on the order: every particle is advanced
+  // independently and the snapshot reads it back through the inverse map.
+  static constexpr int kSortInterval = 6;
+  bool sort_particles(DiagT &d, std::string &msg) {
+    const int np = (int)N_, blk = 256, grd = (np + blk - 1) / blk;
+    const int ncell = (int)sort_key_space(n_);
+    const int ntile = (ncell + SORT_TILE - 1) / SORT_TILE;
+    k_particle_count<T><<<grd, blk, 0, stream_>>>(dg_, d.P, d.pkey, d.pcnt, np);
+    k_scan_tiles<<<ntile, 256, 0, stream_>>>(d.pcnt, d.poffs, d.ptsum, ncell);
+    k_scan_tile_sums<<<1, 1024, 0, stream_>>>(d.ptsum, ntile);
+    k_particle_scatter<T><<<grd, blk, 0, stream_>>>(d.P, d.P2, d.pkey, d.poffs, d.ptsum, np);
+    CK(cudaGetLastError());
+    std::swap(d.P, d.P2);
+    counters_.kernel_launches += 4;
+    return true;
   }
 
   const Options *opt_;

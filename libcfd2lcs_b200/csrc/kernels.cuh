@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(256) k_sl_subcycle(DevGrid<T> g, SplineAxes<T>
   const T x0[3] = {__ldg(g.lt[0] + i), __ldg(g.lt[1] + j), __ldg(g.lt[2] + k)};
   int no[3] = {i, j, k};
   T x[3];
-  integrate<T, TV, INTEG, INTERP>(g, sa, V, S, dt, x0, no, x);
+  integrate<T, TV, INTEG, INTERP, true>(g, sa, V, S, dt, x0, no, x);
   project_plane(g, no, x);
   const bool stick = particle_bc<T, HAS_FLAGS>(g, no, x, err);
   if (stick) {
@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(256) k_sl_subcycle(DevGrid<T> g, SplineAxes<T>
 // ---------------------------------------------------------------------------------------
 // K6  one forward particle subcycle (update_lp, src/lp_motion_m.f90:15-54): integrate,
 // project, BC, stick, accumulate the displacement, one pass of the node search and the
-// periodic wrap of exchange_lpdata.  Particle q starts at interior node q.
+// periodic wrap of exchange_lpdata.  Thread q advances the particle in storage slot q.
 // ---------------------------------------------------------------------------------------
 template <typename T, typename TV, int INTEG, int INTERP, bool HAS_FLAGS>
 __global__ void __launch_bounds__(256) k_fwd_subcycle(DevGrid<T> g, SplineAxes<T> sa, VelFields<TV> V, Particles<T> P, StageTimes S,
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(256) k_snapshot(DevGrid<T> g, FieldPtrs<T> src
   const int p = pidx(g.P.sx, g.P.sxy, i, j, k);
   T v[3];
   if (FROM_DX) {
-    const int q = interior_index(g.P.n, i, j, k);
+    const int q = P.slot[interior_index(g.P.n, i, j, k)];
 #pragma unroll
     for (int c = 0; c < 3; c++) v[c] = P.dx[c][q];
   } else {
@@ -367,7 +367,8 @@ __global__ void __launch_bounds__(256) k_ftle(DevGrid<T> g, FieldPtrs<T> fm, R *
   ftle[interior_index(g.P.n, i, j, k)] = v;
 }
 
-// Reset of forward particles to their grid nodes (reset_lp, src/lp_m.f90:228-294).
+// Reset of forward particles to their grid nodes (reset_lp, src/lp_m.f90:228-294), in node
+// order.
 template <typename T>
 __global__ void k_reset_particles(DevGrid<T> g, Particles<T> P) {
   int i, j, k;
@@ -381,15 +382,181 @@ __global__ void k_reset_particles(DevGrid<T> g, Particles<T> P) {
     P.dx[c][q] = T(0);
     P.no[c][q] = nd[c];
   }
+  P.id[q] = q;
+  P.slot[q] = q;
 }
 
-// Time blend of two padded coefficient fields for one RK stage: c = (1-ct) a + ct b.
+// ---------------------------------------------------------------------------------------
+// Counting sort of the forward particle slots by grid cell, in the order of the backward SL
+// kernel's thread blocks: tiles of 32 (x) x 8 (y) cells of one z layer, x fastest inside a
+// tile.  A block of 256 particles then covers about one such tile, so its warps share the
+// y and z spline rows the way the SL blocks do (L1 reuse across the block), and each warp
+// walks along x.  Steps: count per cell key, exclusive scan of the counts in chunks of
+// SORT_TILE, and a scatter that moves every particle to its key's next free slot.  Particles
+// of one cell land in arbitrary order, which no result depends on.  The count array returns
+// to zero inside the scan, ready for the next sort.
+// ---------------------------------------------------------------------------------------
+constexpr int SORT_TILE = 2048;  // 256 threads x 8 counts
+
+// key space of the cell order: cells c_a in 0..n_a per axis, padded to whole 32 x 8 tiles
+__host__ __device__ inline long sort_key_space(const int n[3]) {
+  const long ntx = (n[0] + 1 + 31) / 32, nty = (n[1] + 1 + 7) / 8;
+  return (long)(n[2] + 1) * nty * ntx * 256;
+}
+
+// cell c in 0..n along each axis: the tracked node (clamped to the interior), minus one when
+// the particle lies below the node's line
 template <typename T>
-__global__ void __launch_bounds__(256) k_blend(FieldPtrs<T> a, FieldPtrs<T> b, FieldPtrsW<T> c, T omc, T ct, long ntot) {
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= ntot) return;
+__global__ void __launch_bounds__(256) k_particle_count(DevGrid<T> g, Particles<T> P, unsigned *key, int *cnt, int np) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= np) return;
+  int c[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const int v = min(max(P.no[a][s], 1), g.P.n[a]);
+    c[a] = v - (P.x[a][s] < __ldg(g.lt[a] + v) ? 1 : 0);
+  }
+  const int ntx = (g.P.n[0] + 1 + 31) / 32, nty = (g.P.n[1] + 1 + 7) / 8;
+  const unsigned tile = (unsigned)((c[2] * nty + (c[1] >> 3)) * ntx + (c[0] >> 5));
+  const unsigned kq = tile * 256u + (unsigned)((c[1] & 7) * 32 + (c[0] & 31));
+  key[s] = kq;
+  atomicAdd(cnt + kq, 1);
+}
+
+// exclusive scan of cnt within each chunk into offs (cnt reset to 0), chunk totals to tsum
+__global__ void __launch_bounds__(256) k_scan_tiles(int *cnt, int *offs, int *tsum, int n) {
+  __shared__ int wsum[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long base = (long)blockIdx.x * SORT_TILE + threadIdx.x * 8;
+  int v[8], run = 0;
+#pragma unroll
+  for (int e = 0; e < 8; e++) {
+    const long q = base + e;
+    const int c = q < n ? cnt[q] : 0;
+    v[e] = run;
+    run += c;
+    if (q < n) cnt[q] = 0;
+  }
+  int x = run;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = lane < 8 ? wsum[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < 8) wsum[lane] = w;
+  }
+  __syncthreads();
+  const int excl = x - run + (warp ? wsum[warp - 1] : 0);
+#pragma unroll
+  for (int e = 0; e < 8; e++)
+    if (base + e < n) offs[base + e] = excl + v[e];
+  if (threadIdx.x == 255) tsum[blockIdx.x] = excl + run;
+}
+
+// exclusive scan of the chunk totals in place (one block)
+__global__ void __launch_bounds__(1024) k_scan_tile_sums(int *tsum, int nt) {
+  __shared__ int wsum[32];
+  __shared__ int carry;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int b0 = 0; b0 < nt; b0 += 1024) {
+    const int q = b0 + threadIdx.x;
+    const int c = q < nt ? tsum[q] : 0;
+    int x = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      int w = wsum[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      wsum[lane] = w;
+    }
+    __syncthreads();
+    const int incl = x + (warp ? wsum[warp - 1] : 0);
+    if (q < nt) tsum[q] = carry + incl - c;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry += incl;
+    __syncthreads();
+  }
+}
+
+// slot of particle s: its key's chunk base + in-chunk offset + arrival order at the key
+template <typename T>
+__global__ void __launch_bounds__(256) k_particle_scatter(Particles<T> src, Particles<T> dst, const unsigned *__restrict__ key,
+                                                           int *offs, const int *__restrict__ tsum, int np) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= np) return;
+  const unsigned kq = key[s];
+  const int d = __ldg(tsum + kq / SORT_TILE) + atomicAdd(offs + kq, 1);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    dst.x[c][d] = src.x[c][s];
+    dst.dx[c][d] = src.dx[c][s];
+    dst.no[c][d] = src.no[c][s];
+  }
+  const int id = src.id[s];
+  dst.id[d] = id;
+  dst.slot[id] = d;
+}
+
+// Time blends of two padded coefficient fields for the RK stages of a subcycle that have no
+// blend yet: out_m = (1-ct_m) a + ct_m b for m < nout, so a and b are read once for all of
+// them.  Two elements per thread (8- or 16-byte vector accesses), component blockIdx.y.
+template <typename T>
+struct Pair;
+template <>
+struct Pair<double> {
+  using type = double2;
+};
+template <>
+struct Pair<float> {
+  using type = float2;
+};
+
+template <typename T>
+struct BlendOut {
+  T *f[3][3];  // [output][component]
+  T omc[3], ct[3];
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_blend(const __grid_constant__ FieldPtrs<T> a, const __grid_constant__ FieldPtrs<T> b,
+                                                const __grid_constant__ BlendOut<T> o, int nout, long ntot) {
+  using P2 = typename Pair<T>::type;
+  const long h = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const int comp = blockIdx.y;
-  c.f[comp][q] = omc * __ldg(a.f[comp] + q) + ct * __ldg(b.f[comp] + q);
+  const long q = 2 * h;
+  if (q + 1 < ntot) {
+    const P2 va = __ldg(reinterpret_cast<const P2 *>(a.f[comp]) + h);
+    const P2 vb = __ldg(reinterpret_cast<const P2 *>(b.f[comp]) + h);
+    for (int m = 0; m < nout; m++) {
+      P2 r;
+      r.x = o.omc[m] * va.x + o.ct[m] * vb.x;
+      r.y = o.omc[m] * va.y + o.ct[m] * vb.y;
+      reinterpret_cast<P2 *>(o.f[m][comp])[h] = r;
+    }
+  } else if (q < ntot) {
+    const T va = __ldg(a.f[comp] + q), vb = __ldg(b.f[comp] + q);
+    for (int m = 0; m < nout; m++) o.f[m][comp][q] = o.omc[m] * va + o.ct[m] * vb;
+  }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -403,8 +570,9 @@ __global__ void __launch_bounds__(256) k_blend(FieldPtrs<T> a, FieldPtrs<T> b, F
 // is one coalesced row.  Line L starts at L % nfast + (L / nfast) * so; elements es apart.
 // Loads are issued G at a time ahead of the dependent sweep.
 template <typename T, int K>
-__global__ void __launch_bounds__(256) k_fit_lines(SplineAxis<T> A, FieldPtrs<T> src, FieldPtrsW<T> dst, int nfast, long nlines,
-                                                    long es, long so) {
+__global__ void __launch_bounds__(256, 3) k_fit_lines(SplineAxis<T> A, const __grid_constant__ FieldPtrs<T> src,
+                                                       const __grid_constant__ FieldPtrsW<T> dst, int nfast, long nlines, long es,
+                                                       long so) {
   const long L = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (L >= nlines) return;
   const long off = L % nfast + (L / nfast) * so;
@@ -414,39 +582,54 @@ __global__ void __launch_bounds__(256) k_fit_lines(SplineAxis<T> A, FieldPtrs<T>
   const T *pc = A.pull;
   constexpr int G = 8;
   T win[3] = {T(0), T(0), T(0)};
-  for (int i0 = 0; i0 < n; i0 += G) {
+  const T *sp = s;
+  T *dp = d;
+  for (int i0 = 0; i0 < n; i0 += G, sp += G * es, dp += G * es) {
     T v[G];
 #pragma unroll
-    for (int g = 0; g < G; g++) v[g] = (i0 + g < n) ? s[(long)(i0 + g) * es] : T(0);
+    for (int g = 0; g < G; g++) v[g] = (i0 + g < n) ? sp[g * es] : T(0);
 #pragma unroll
     for (int g = 0; g < G; g++)
       if (i0 + g < n) v[g] = pull_forward<T, K>(pc, i0 + g, v[g], win);
 #pragma unroll
     for (int g = 0; g < G; g++)
-      if (i0 + g < n) d[(long)(i0 + g) * es] = v[g];
+      if (i0 + g < n) dp[g * es] = v[g];
   }
   win[0] = win[1] = win[2] = T(0);
-  for (int i1 = n - 1; i1 >= 0; i1 -= G) {
+  dp = d + (long)(n - 1) * es;
+  for (int i1 = n - 1; i1 >= 0; i1 -= G, dp -= G * es) {
     T v[G];
 #pragma unroll
-    for (int g = 0; g < G; g++) v[g] = (i1 - g >= 0) ? d[(long)(i1 - g) * es] : T(0);
+    for (int g = 0; g < G; g++) v[g] = (i1 - g >= 0) ? dp[-g * es] : T(0);
 #pragma unroll
     for (int g = 0; g < G; g++)
       if (i1 - g >= 0) v[g] = pull_backward<T, K>(pc, i1 - g, v[g], win);
 #pragma unroll
     for (int g = 0; g < G; g++)
-      if (i1 - g >= 0) d[(long)(i1 - g) * es] = v[g];
+      if (i1 - g >= 0) dp[-g * es] = v[g];
   }
 }
 
-// x pass: lines are contiguous.  One warp per 32 lines (consecutive j at one k): each chunk of
-// 32 elements of the 32 lines is staged through a shared tile with coalesced row loads,
-// swept by one lane per line inside the tile, and written back with coalesced row stores.
+// asynchronous element copy global -> shared (LDGSTS), completed by cp_async_wait
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *smem, const T *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gmem), "n"(sizeof(T)) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// x pass: lines are contiguous.  One warp per 32 lines (consecutive j at one k).  Chunks of
+// 32 elements of the 32 lines are staged through two shared tiles per warp: the next chunk's
+// rows are copied asynchronously (one coalesced row per copy instruction) while one lane per
+// line sweeps the current tile, which then goes back to memory as coalesced row stores.
 template <typename T, int K>
-__global__ void __launch_bounds__(128) k_fit_xlines(SplineAxis<T> A, FieldPtrs<T> src, FieldPtrsW<T> dst, int ny, int nz, long sx,
-                                                     long sxy) {
-  __shared__ T tile[4][32][33];
+__global__ void __launch_bounds__(128) k_fit_xlines(SplineAxis<T> A, const __grid_constant__ FieldPtrs<T> src,
+                                                     const __grid_constant__ FieldPtrsW<T> dst, int ny, int nz, long sx, long sxy) {
+  extern __shared__ __align__(16) unsigned char fit_smem[];
   const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  T(*tiles)[32][33] = reinterpret_cast<T(*)[32][33]>(fit_smem) + 2 * wp;
   const int nbf = (ny + 31) / 32;
   const long gw = (long)blockIdx.x * 4 + wp;
   if (gw >= (long)nbf * nz) return;  // warp-uniform
@@ -455,42 +638,56 @@ __global__ void __launch_bounds__(128) k_fit_xlines(SplineAxis<T> A, FieldPtrs<T
   const long base = (long)j0 * sx + (gw / nbf) * sxy;
   const T *s = src.f[blockIdx.y] + base;
   T *d = dst.f[blockIdx.y] + base;
-  T(*t)[33] = tile[wp];
-  const int n = A.n;
+  const int n = A.n, nch = (n + 31) / 32;
   const T *pc = A.pull;
-  T win[3] = {T(0), T(0), T(0)};
-  for (int c0 = 0; c0 < n; c0 += 32) {
+  // chunk c of the sweep (forward: c-th from the start, backward: from the end)
+  auto chunk0 = [&](int c, bool fwd) { return fwd ? c * 32 : (nch - 1 - c) * 32; };
+  auto issue = [&](const T *from, int c0, T(*t)[33]) {
     const int ne = min(32, n - c0);
-    if (lane < ne) {
+    if (lane < ne)
+      for (int r = 0; r < nl; r++) cp_async_elem(&t[r][lane], from + (long)r * sx + c0 + lane);
+    cp_async_commit();
+  };
+  T win[3];
+  for (int pass = 0; pass < 2; pass++) {
+    const bool fwd = pass == 0;
+    const T *from = fwd ? s : d;
+    win[0] = win[1] = win[2] = T(0);
+    issue(from, chunk0(0, fwd), tiles[0]);
+    for (int c = 0; c < nch; c++) {
+      T(*t)[33] = tiles[c & 1];
+      if (c + 1 < nch) {
+        issue(from, chunk0(c + 1, fwd), tiles[(c + 1) & 1]);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncwarp();
+      const int c0 = chunk0(c, fwd), ne = min(32, n - c0);
+      if (lane < nl) {
+        if (fwd) {
+          if (ne == 32) {
+#pragma unroll
+            for (int e = 0; e < 32; e++) t[lane][e] = pull_forward<T, K>(pc, c0 + e, t[lane][e], win);
+          } else {
+            for (int e = 0; e < ne; e++) t[lane][e] = pull_forward<T, K>(pc, c0 + e, t[lane][e], win);
+          }
+        } else {
+          if (ne == 32) {
+#pragma unroll
+            for (int e = 31; e >= 0; e--) t[lane][e] = pull_backward<T, K>(pc, c0 + e, t[lane][e], win);
+          } else {
+            for (int e = ne - 1; e >= 0; e--) t[lane][e] = pull_backward<T, K>(pc, c0 + e, t[lane][e], win);
+          }
+        }
+      }
+      __syncwarp();
+      if (lane < ne) {
 #pragma unroll 8
-      for (int r = 0; r < nl; r++) t[r][lane] = s[(long)r * sx + c0 + lane];
+        for (int r = 0; r < nl; r++) d[(long)r * sx + c0 + lane] = t[r][lane];
+      }
+      __syncwarp();
     }
-    __syncwarp();
-    if (lane < nl)
-      for (int e = 0; e < ne; e++) t[lane][e] = pull_forward<T, K>(pc, c0 + e, t[lane][e], win);
-    __syncwarp();
-    if (lane < ne) {
-#pragma unroll 8
-      for (int r = 0; r < nl; r++) d[(long)r * sx + c0 + lane] = t[r][lane];
-    }
-    __syncwarp();
-  }
-  win[0] = win[1] = win[2] = T(0);
-  for (int c0 = ((n - 1) / 32) * 32; c0 >= 0; c0 -= 32) {
-    const int ne = min(32, n - c0);
-    if (lane < ne) {
-#pragma unroll 8
-      for (int r = 0; r < nl; r++) t[r][lane] = d[(long)r * sx + c0 + lane];
-    }
-    __syncwarp();
-    if (lane < nl)
-      for (int e = ne - 1; e >= 0; e--) t[lane][e] = pull_backward<T, K>(pc, c0 + e, t[lane][e], win);
-    __syncwarp();
-    if (lane < ne) {
-#pragma unroll 8
-      for (int r = 0; r < nl; r++) d[(long)r * sx + c0 + lane] = t[r][lane];
-    }
-    __syncwarp();
   }
 }
 
