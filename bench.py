@@ -70,17 +70,51 @@ WORKLOADS = {
                       desc="ABC flow 256^3 periodic, dt=0.05, FTLE fwd+bkwd T=10 h=1, RK2, linear"),
     "dg512": dict(kind="dg", n=512, dt=0.1, T=15.0, h=1.5, integrator=2, interpolator=1, dirs=(1,), t0=1.4,
                   desc="double gyre 512x256x1, dt=0.1, FTLE bkwd T=15 h=1.5, RK2, linear"),
+    "turb512": dict(kind="turb", n=512, dt=0.01, T=2.0, h=0.2, integrator=2, interpolator=1, dirs=(1,), t0=0.19,
+                    desc="synthetic periodic turbulence 512^3 (64 seeded Fourier modes, k^-5/3, FP32 field values), "
+                         "dt=0.01, FTLE bkwd T=2 h=0.2, RK2, linear"),
 }
 
 
 def make_grid(w, n=None):
+    """(grid, host velocity(t) -> 3 numpy arrays, steady?)"""
     from libcfd2lcs_b200 import workloads as W
     if w["kind"] == "abc":
         g = W.abc_grid(n or w["n"])
         vel = W.abc_velocity(g)
         return g, (lambda t: vel), True
+    if w["kind"] == "turb":
+        g = W.abc_grid(n or w["n"])
+        modes = W.turbulence_modes()
+        return g, (lambda t: tuple(a.astype(np.float64) for a in W.turbulence_velocity(g, t, modes))), False
     g = W.double_gyre_grid(n or w["n"], (n or w["n"]) // 2)
     return g, (lambda t: W.double_gyre_velocity(g, t)), False
+
+
+def turbulence_on_device(n, t, dev, chunk=16):
+    """The seeded turbulence field of workloads.turbulence_velocity evaluated on the GPU (the
+    host form takes minutes at 512^3): FP32 field values, returned as FP64 tensors in
+    i-fastest order."""
+    import torch
+    from libcfd2lcs_b200 import workloads as W
+    modes = W.turbulence_modes()
+    L = 2.0 * math.pi
+    line = (torch.arange(n, device=dev, dtype=torch.float64) + 0.5) * (L / n)
+    out = [torch.empty(n * n * n, device=dev, dtype=torch.float64) for _ in range(3)]
+    Y, X = torch.meshgrid(line, line, indexing="ij")  # (j, i), i fastest
+    for k0 in range(0, n, chunk):
+        kk = line[k0:k0 + chunk]
+        acc = [torch.zeros((kk.numel(), n, n), device=dev, dtype=torch.float64) for _ in range(3)]
+        for m in range(len(modes.k)):
+            kx, ky, kz = (float(v) for v in modes.k[m])
+            c0 = float(modes.omega[m]) * t + float(modes.phase[m])
+            arg = (kx * X + ky * Y)[None, :, :] + (kz * kk)[:, None, None] + c0
+            c = torch.cos(arg)
+            for a in range(3):
+                acc[a].add_(c, alpha=float(modes.a[m, a]))
+        for a in range(3):
+            out[a][k0 * n * n:(k0 + kk.numel()) * n * n] = acc[a].float().double().reshape(-1)
+    return out
 
 
 def measured_peaks():
@@ -224,13 +258,18 @@ def run_b200(args, w):
     total = args.warmup + args.steps
 
     def dev_fields(t):
+        if w["kind"] == "turb":
+            return turbulence_on_device(g.n[0], t, dev)
         u, v, wv = vel(t)
         return [torch.from_numpy(np.ascontiguousarray(a.ravel(order="F"))).to(dev) for a in (u, v, wv)]
 
-    fields = [dev_fields(w["t0"])] if steady else [dev_fields(w["t0"] + s * w["dt"]) for s in range(total + 1)]
+    # steady flows: one resident field; the turbulence is generated on the device before each
+    # step (outside the library's event-timed update); others: every step's field resident
+    lazy = w["kind"] == "turb"
+    fields = [dev_fields(w["t0"])] if steady else ([] if lazy else [dev_fields(w["t0"] + s * w["dt"]) for s in range(total + 1)])
 
     def step(s):
-        f = fields[0] if steady else fields[s]
+        f = fields[0] if steady else (dev_fields(w["t0"] + s * w["dt"]) if lazy else fields[s])
         api.update_device(f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr(), w["t0"] + s * w["dt"])
 
     step(0)  # first call (no advection)
@@ -271,12 +310,19 @@ def run_b200(args, w):
     pin = []
     for s in range(args.steps):
         t = w["t0"] + (total + 1 + s) * w["dt"]
-        u, v, wv = vel(t)
         arrs = []
-        for a in (u, v, wv):
-            tt = torch.empty(N, dtype=torch.float64, pin_memory=True)
-            tt.numpy()[:] = a.ravel(order="F")
-            arrs.append(tt)
+        if lazy:
+            for a in dev_fields(t):
+                tt = torch.empty(N, dtype=torch.float64, pin_memory=True)
+                tt.copy_(a)
+                arrs.append(tt)
+                del a
+        else:
+            u, v, wv = vel(t)
+            for a in (u, v, wv):
+                tt = torch.empty(N, dtype=torch.float64, pin_memory=True)
+                tt.numpy()[:] = a.ravel(order="F")
+                arrs.append(tt)
         pin.append((t, arrs))
         if steady:
             break
@@ -336,8 +382,21 @@ def run_b200(args, w):
             "nsub_per_update": {"fwd": c1["nsub_fwd"], "bkwd": c1["nsub_bkwd"]},
             "gpu_launches": launches, "e2e": e2e, "roofline": roof, "rooflines": rooflines,
             "phase_ms_per_step": {k: (p1[k] - p0[k]) / args.steps for k in p1}}
+    if args.precision == "fp64":
+        line["ftle_error"] = {"form": "plain FP64", "vs": "FP64 oracle (CPU restatement of the reference)",
+                              "max_abs_tolerance": 1e-8 if w["interpolator"] >= 2 else 1e-9,
+                              "where": "tests/test_gpu_parity.py, every integrator / interpolator on small grids"}
+    line["clocks"] = clk.summary() if rank == 0 else None
+    if args.precision == "mixed" and w["kind"] == "abc" and args.acc_n > 0 and rank == 0:
+        # FTLE error of the mixed form against the plain FP64 path (itself parity-tested against
+        # the FP64 oracle) on the same flow and options at a smaller grid, full T
+        from libcfd2lcs_b200 import accuracy as A
+        api.finalize()
+        acc = A.compare(args.acc_n, w["T"], w["h"], w["dt"], None, w["integrator"], w["interpolator"])
+        line["ftle_error"] = {"form": "mixed (FP32 velocity data, FP64 positions / flow maps / FTLE)",
+                              "vs": "plain FP64 GPU path", "case": acc["config"],
+                              **{d: acc[d] for d in ("fwd", "bkwd") if d in acc}}
     if rank == 0:
-        line["clocks"] = clk.summary()
         if world == 1 and not args.no_cpu:
             rate, threads, sample, _ = cpu_sample(w, 1)
             line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
@@ -355,6 +414,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="abc256", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--acc-n", type=int, default=64, help="grid of the mixed-vs-FP64 FTLE error run (0: skip)")
     ap.add_argument("--n", type=int, default=None, help="override the grid size (smaller smoke runs)")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()

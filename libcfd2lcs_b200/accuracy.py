@@ -61,7 +61,10 @@ def compare(n=64, T=2.0, h=1.0, dt=0.05, updates=None, integrator=3, interp=3):
         dfl = np.abs(f32 - f64)
         key = "fwd" if d == 0 else "bkwd"
         res[key] = {"ftle_max_err": float(dfl.max()), "ftle_rms_err": float(math.sqrt(float((dfl ** 2).mean()))),
-                    "ftle_range": [float(f64.min()), float(f64.max())], "fm_max_err": float(np.abs(m32 - m64).max())}
+                    "ftle_p9999_err": float(np.quantile(dfl, 0.9999)), "points_over_1e-4": int((dfl > 1e-4).sum()),
+                    "points": int(dfl.size), "ftle_range": [float(f64.min()), float(f64.max())],
+                    "fm_max_err": float(np.abs(m32 - m64).max()),
+                    "fm_points_over_1e-3": int((np.abs(m32 - m64).reshape(3, -1).max(axis=0) > 1e-3).sum())}
     return res
 
 

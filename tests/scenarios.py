@@ -65,6 +65,13 @@ def make_case(name: str, n: int | None = None):
             return u, v, w
 
         return g, vel, dict(T=0.4, h=0.1, dt=0.05, steps=12)
+    if name == "turb":
+        # seeded divergence-free Fourier-mode turbulence on a periodic cube (the synthetic
+        # turbulence config at a size the oracle runs in seconds; wavenumbers |k| <= 3 so the
+        # small grid resolves them)
+        g = W.abc_grid(n or 12)
+        modes = W.turbulence_modes(nmodes=16, kmin=1, kmax=3, seed=20261203)
+        return g, (lambda t: W.turbulence_velocity(g, t, modes, dtype=np.float64)), dict(T=0.2, h=0.05, dt=0.02, steps=16)
     raise KeyError(name)
 
 

@@ -1,8 +1,13 @@
 """Parity of the CUDA path (libcfd2lcs_b200, called through its C ABI) with the oracle
 (the CPU restatement of the reference) on seeded synthetic flows at small sizes.
 
-Tolerances (plain FP64): composed flow map max-abs <= 1e-12 * L (L the domain length),
-FTLE max-abs <= 1e-9 for LINEAR / NEAREST and <= 1e-8 for the B-spline interpolators.
+Tolerances:
+  plain FP64 (dp library) vs the FP64 oracle: composed flow map max-abs <= 1e-12 * L (L the
+    domain length), FTLE max-abs <= 1e-9 for LINEAR / NEAREST and <= 1e-8 for the B-splines;
+  plain FP32 (sp library) vs the FP32 oracle: flow map <= 2e-5 * L, FTLE <= 3e-4 (both round
+    every operation in FP32, the device with FMA contraction, the oracle without);
+  mixed precision (dp library, MIXED_PRECISION = 1: FP32 velocity data) vs the FP64 oracle:
+    flow map <= 1e-6 * L, FTLE <= 1e-5.
 """
 import numpy as np
 import pytest
@@ -21,11 +26,20 @@ def gpu_dp():
     return L.Cfd2lcs("dp")
 
 
-def _compare(oracle, gpu, case, integrator, interpolator, directions=(SC.FTLE_BKWD, SC.FTLE_FWD), n=None, steps=None):
+@pytest.fixture(scope="module")
+def gpu_sp():
+    import libcfd2lcs_b200 as L
+    return L.Cfd2lcs("sp")
+
+
+def _compare(oracle, gpu, case, integrator, interpolator, directions=(SC.FTLE_BKWD, SC.FTLE_FWD), n=None, steps=None,
+             fm_tol_rel=FM_TOL_REL, ftle_tol=None, mixed=False):
     oracle.reset()
     g, ho = SC.run(oracle, case, directions, integrator, interpolator, n=n, steps=steps)
     assert oracle.error() == 0, oracle.error_msg()
     gpu.reset()
+    if mixed:
+        gpu.set_option("MIXED_PRECISION", 1)
     _, hg = SC.run(gpu, case, directions, integrator, interpolator, n=n, steps=steps)
     err, msg = gpu.error()
     assert err == 0, msg
@@ -38,8 +52,9 @@ def _compare(oracle, gpu, case, integrator, interpolator, directions=(SC.FTLE_BK
         dft = float(np.max(np.abs(to - tg)))
         out[d] = (dfm, dft)
         assert np.all(np.isfinite(tg))
-        assert dfm <= FM_TOL_REL * L, f"flow map max-abs {dfm:.3e} (dir {d}) > {FM_TOL_REL * L:.3e}"
-        assert dft <= FTLE_TOL[interpolator], f"FTLE max-abs {dft:.3e} (dir {d})"
+        tol = FTLE_TOL[interpolator] if ftle_tol is None else ftle_tol
+        assert dfm <= fm_tol_rel * L, f"flow map max-abs {dfm:.3e} (dir {d}) > {fm_tol_rel * L:.3e}"
+        assert dft <= tol, f"FTLE max-abs {dft:.3e} (dir {d}) > {tol:.1e}"
     cg, co = gpu.counters(), {k: oracle.counter(k) for k in ("integrations_fwd", "integrations_bkwd", "ftle_frames")}
     for k in co:
         assert cg[k] == co[k], (k, cg[k], co[k])
@@ -99,3 +114,24 @@ def test_channel_cubic_is_rejected_like_the_oracle(oracle_dp, gpu_dp):
 @pytest.mark.parametrize("interp", [1, 3])
 def test_mixed_boundary_conditions(oracle_dp, gpu_dp, interp):
     _compare(oracle_dp, gpu_dp, "mixed_bc", 3, interp)
+
+
+@pytest.mark.parametrize("integrator,interp", [(2, 1), (3, 3)])
+def test_turbulence(oracle_dp, gpu_dp, integrator, interp):
+    _compare(oracle_dp, gpu_dp, "turb", integrator, interp)
+
+
+@pytest.mark.parametrize("case,integrator,interp", [("dg", 2, 1), ("abc", 3, 3), ("turb", 2, 1), ("mixed_bc", 3, 1)])
+def test_single_precision_build(oracle_sp, gpu_sp, case, integrator, interp):
+    """The sp library (lcsdata_t = float) against the FP32 oracle."""
+    _compare(oracle_sp, gpu_sp, case, integrator, interp, fm_tol_rel=2e-5, ftle_tol=3e-4)
+
+
+@pytest.mark.parametrize("case,integrator,interp", [("dg", 2, 1), ("abc", 3, 3), ("turb", 3, 3), ("abc_unsteady", 4, 3)])
+def test_mixed_precision_form(oracle_dp, gpu_dp, case, integrator, interp):
+    """MIXED_PRECISION = 1 (FP32 velocity levels, coefficients and tap contractions; FP64
+    positions, flow maps and FTLE) against the FP64 oracle."""
+    try:
+        _compare(oracle_dp, gpu_dp, case, integrator, interp, fm_tol_rel=1e-6, ftle_tol=1e-5, mixed=True)
+    finally:
+        gpu_dp.reset()
