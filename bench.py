@@ -41,6 +41,14 @@ UNIT = "grid-pt·RK-steps/s"
 # data as above.
 STAGES = {0: 1, 1: 1, 2: 2, 3: 3, 4: 3}
 
+# DRAM bytes per point of one launch (dram__bytes_read.sum + dram__bytes_write.sum) from the ncu
+# captures summarised in profiles/ (192^3 ABC, 7077888 points), scaled to the benchmark grid by
+# its point count: (kernel, precision, interpolator, integrator) -> bytes per point
+MEASURED_TRAFFIC = {
+    ("k_sl_subcycle", "fp64", 3, 3): (870.556160e6 + 169.014272e6) / 7077888,   # k_sl_subcycle_abc192_cubic_rk3_fp64.md
+    ("k_fwd_subcycle", "fp64", 3, 3): (963.253760e6 + 401.995008e6) / 7077888,  # k_fwd_subcycle_abc192_cubic_rk3_fp64.md
+}
+
 
 def sl_bytes_per_point(s: int, interp: int, integrator: int, sv: int = None) -> int:
     """s: bytes of a flow-map value, sv: bytes of a velocity value (4 in the mixed form)."""
@@ -180,6 +188,16 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def rank_max(x: float, world: int, device) -> float:
+    """Maximum of a per-rank time over all ranks (the job's time is its slowest rank's)."""
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -297,10 +315,7 @@ def run_b200(args, w):
         raise RuntimeError(msg)
     work = (c1["integrations_fwd"] + c1["integrations_bkwd"]) - (c0["integrations_fwd"] + c0["integrations_bkwd"])
     ms = p1["update_total"] - p0["update_total"]
-    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        torch.distributed.all_reduce(ms_t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
+    ms_max = rank_max(ms, world, dev)
     value = world * work / (ms_max / 1000.0)
     launches = c1["kernel_launches"] - c0["kernel_launches"]
     # FTLE-field time: snapshot + composition + FTLE of the frames seen so far
@@ -341,16 +356,15 @@ def run_b200(args, w):
             api.lib.cfd2lcs_get_ftle_c(int(h), out.data_ptr())
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t_e0
-    et = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+    e2e_max = rank_max(e2e_s, world, dev)
     if world > 1:
-        torch.distributed.all_reduce(et, op=torch.distributed.ReduceOp.MAX)
         torch.distributed.barrier()
     ce1 = api.counters()
     err, msg = api.error()
     if err:
         raise RuntimeError(msg)
     e2e_work = (ce1["integrations_fwd"] + ce1["integrations_bkwd"]) - (ce0["integrations_fwd"] + ce0["integrations_bkwd"])
-    e2e = {"value": world * e2e_work / float(et.item()), "unit": UNIT, "h2d_bytes_per_step": 3 * N * 8,
+    e2e = {"value": world * e2e_work / e2e_max, "unit": UNIT, "h2d_bytes_per_step": 3 * N * 8,
            "d2h_bytes_per_step": len(handles) * N * 8}
     # --- roofline of the dominant hot kernel (by device time in the timed region) ---
     peaks = measured_peaks()
@@ -371,6 +385,10 @@ def run_b200(args, w):
                            "frac": achieved / hbm if hbm else None, "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)",
                            "avg_launch_ms": avg_s * 1000.0, "share_of_step": tot_ms / ms if ms else None,
                            "algorithmic_bytes_per_point": bpp, "algorithmic_bytes_per_launch": N * bpp, "traffic": None}
+        tpp = MEASURED_TRAFFIC.get((name, args.precision, w["interpolator"], w["integrator"]))
+        if tpp is not None and w["kind"] == "abc":
+            rooflines[name]["traffic"] = tpp * N
+            rooflines[name]["traffic_source"] = "ncu capture at 192^3 (profiles/), scaled by points"
     roof = max(rooflines.values(), key=lambda r: r["share_of_step"] or 0) if rooflines else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

@@ -134,7 +134,7 @@ void do_set_option(const std::string &opt, int val) {
   } else if (opt == "INTEGRATOR") {
     ok = val >= EULER && val <= RK4;
     lib.opt.integrator = val;
-  } else if (opt == "MIXED_PRECISION") {  // extension: select the FP32-compensated form
+  } else if (opt == "MIXED_PRECISION") {  // extension: FP32 velocity data, FP64 positions and flow maps
     ok = tf;
     if (ok && lib.inited) {
       latch("MIXED_PRECISION must be set before cfd2lcs_init");
