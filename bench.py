@@ -424,18 +424,145 @@ def run_b200(args, w):
         torch.distributed.destroy_process_group()
 
 
+BATCH_DESC = ("batch of 64 independent instances: 32 double gyres 64x32..1024x512 (eps~U(.1,.3), A~U(.05,.15), dt=0.1) and "
+              "32 ABC flows n^3, n in [32,192] (A,B,C~U(.5,2), dt=0.05); T~U(2,15), h=T/10, forward or backward per instance; "
+              "RK2, linear; seed 64")
+
+
+def batch_specs(seed: int = 64):
+    """The 64 instances of the batched workload, drawn from one seed."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for _ in range(32):
+        nx = int(np.clip(round(2.0 ** rng.uniform(6.0, 10.0) / 32.0) * 32, 64, 1024))
+        specs.append(dict(kind="dg", n=(nx, nx // 2), eps=float(rng.uniform(0.1, 0.3)), A=float(rng.uniform(0.05, 0.15)),
+                          T=float(rng.uniform(2.0, 15.0)), dir=int(rng.integers(0, 2)), dt=0.1))
+    for _ in range(32):
+        n = int(rng.integers(2, 13)) * 16
+        specs.append(dict(kind="abc", n=n, A=float(rng.uniform(0.5, 2.0)), B=float(rng.uniform(0.5, 2.0)),
+                          C=float(rng.uniform(0.5, 2.0)), T=float(rng.uniform(2.0, 15.0)), dir=int(rng.integers(0, 2)), dt=0.05))
+    return specs
+
+
+def run_batch(args):
+    """The batched form: every instance of this rank advanced by one cfd2lcs_batch_update_device_c
+    per step (instances are dealt round-robin over ranks: strong scaling of a fixed batch).
+    Time = wall clock of the batch calls with the device synchronised on both sides (the calls
+    span one stream per instance); the same instances advanced one call per instance give the
+    unbatched comparison."""
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    import libcfd2lcs_b200 as L
+    from libcfd2lcs_b200 import workloads as W
+    dev = torch.device("cuda", local)
+    b = L.Batch("dp")
+    b.reset()
+    specs = [sp for i, sp in enumerate(batch_specs()) if i % world == rank]
+    ids, vels, npts = [], [], []
+    for sp in specs:
+        if sp["kind"] == "dg":
+            g = W.double_gyre_grid(*sp["n"])
+            vel = (lambda g, sp: lambda t: W.double_gyre_velocity(g, t, A=sp["A"], eps=sp["eps"]))(g, sp)
+        else:
+            g = W.abc_grid(sp["n"])
+            steady = W.abc_velocity(g, A=sp["A"], B=sp["B"], Cc=sp["C"])
+            steady_dev = [torch.from_numpy(np.ascontiguousarray(a.ravel(order="F"))).to(dev) for a in steady]
+            vel = (lambda f: lambda t: f)(steady_dev)
+        i = b.add(g.n, g.x, g.y, g.z, g.flag, 2, 1, 0.5, args.precision == "mixed")
+        if i < 0 or b.diagnostic_init(i, sp["dir"], sp["T"], sp["T"] / 10.0) < 0:
+            raise RuntimeError(b.error()[1])
+        ids.append(i)
+        vels.append(vel)
+        npts.append(int(np.prod(g.n)))
+
+    def fields(s):
+        out = []
+        for sp, vel in zip(specs, vels):
+            f = vel(s * sp["dt"])
+            if isinstance(f, tuple):
+                f = [torch.from_numpy(np.ascontiguousarray(a.ravel(order="F"))).to(dev) for a in f]
+            out.append(f)
+        return out
+
+    def counters():
+        return sum(b.counters(i)["integrations_fwd"] + b.counters(i)["integrations_bkwd"] for i in ids)
+
+    def advance(s, together):
+        f = fields(s)
+        times = [s * sp["dt"] for sp in specs]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if together:
+            rc = b.update_device(ids, [x[0].data_ptr() for x in f], [x[1].data_ptr() for x in f], [x[2].data_ptr() for x in f], times)
+        else:
+            rc = 0
+            for q, i in enumerate(ids):
+                rc |= b.update_device([i], [f[q][0].data_ptr()], [f[q][1].data_ptr()], [f[q][2].data_ptr()], [times[q]])
+        torch.cuda.synchronize()
+        if rc:
+            raise RuntimeError(b.error()[1])
+        return time.perf_counter() - t0
+
+    s = 0
+    for _ in range(args.warmup + 1):
+        advance(s, True)
+        s += 1
+    w0 = counters()
+    el = 0.0
+    for _ in range(args.steps):
+        el += advance(s, True)
+        s += 1
+    work = counters() - w0
+    w1 = counters()
+    el_seq = 0.0
+    for _ in range(args.steps):
+        el_seq += advance(s, False)
+        s += 1
+    work_seq = counters() - w1
+    el_max = rank_max(el, world, dev)
+    el_seq_max = rank_max(el_seq, world, dev)
+    tot = torch.tensor([float(work), float(work_seq), float(sum(npts))], device=dev, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(tot)
+    line = {"metric": METRIC, "value": float(tot[0]) / el_max, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * el_max / args.steps, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64 positions, f32 velocity", "data": "synthetic",
+            "config": {"workload": BATCH_DESC, "instances": 64, "points": int(tot[2]), "precision": args.precision,
+                       "timing": "wall clock of the batch calls, device synchronised on both sides",
+                       "parallelism": f"instances dealt over {world} GPUs" if world > 1 else "single GPU"},
+            "unbatched": {"value": float(tot[1]) / el_seq_max, "unit": UNIT,
+                          "what": "the same instances, one cfd2lcs_batch_update_device_c call per instance per step"}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    b.reset()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="abc256", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="abc256", choices=sorted(WORKLOADS) + ["batch64"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--acc-n", type=int, default=64, help="grid of the mixed-vs-FP64 FTLE error run (0: skip)")
     ap.add_argument("--n", type=int, default=None, help="override the grid size (smaller smoke runs)")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
+    if args.workload == "batch64":
+        if args.impl == "reference":
+            world, rank, _ = dist_setup()
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched form (one instance per process)"}))
+            return
+        run_batch(args)
+        return
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, w)

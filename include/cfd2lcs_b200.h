@@ -75,9 +75,46 @@ void cfd2lcs_get_kernel_times_c(double t[2], long long n[2]);
  * The table of sub-flow-map pointers lives in a fixed device array (256 sub-flow maps, i.e.
  * T/h <= 256; larger frames are rejected with an error).  The first call on a device looks
  * up that array's address; make this first call before any stream capture.  All calls share
- * the array, so calls that overlap on the GPU race.  Plain-precision form only.  Returns 0 on
- * success, 1 on error (the error is latched as for every other call). */
+ * the array, so calls that overlap on the GPU race.  Returns 0 on success, 1 on error (the
+ * error is latched as for every other call). */
 int cfd2lcs_reconstruct_noalloc_c(int lcs_handle, lcsdata_t *d_ftle, lcsdata_t *d_fm);
+
+/* ---------------------------------------------------------------------------------------
+ * Batched form.  No counterpart in the reference, which keeps one instance per process
+ * (module globals, src/data_m.f90:313-387): here any number of independent instances -- each
+ * with its own grid, options and diagnostics -- advance together.  A batch update starts the
+ * velocity ingest of every listed instance on the instance's own stream, then enqueues every
+ * instance's subcycles and FTLE frames, so the instances' kernels overlap on the GPU and the
+ * host waits once per instance (for its CFL number).  The batch has its own error state and
+ * leaves the reference-interface instance alone.  Functions return 0 (or an id >= 0) on
+ * success and 1 (or -1) on error; cfd2lcs_batch_error_c gives the first error message.
+ * ------------------------------------------------------------------------------------- */
+
+/* Adds an instance on the grid (x, y, z, flag as for cfd2lcs_init_c) with its options
+ * (integrator and interpolator codes of cfd2lcs_inc_*.h, CFL, MIXED_PRECISION 0/1).
+ * Returns the instance id. */
+int cfd2lcs_batch_add_c(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, const int *flag,
+                        int integrator, int interpolator, lcsdata_t cfl, int mixed_precision);
+
+/* cfd2lcs_diagnostic_init_c for one instance (resolution 0).  Returns the diagnostic handle
+ * within that instance. */
+int cfd2lcs_batch_diagnostic_init_c(int id, int lcs_type, lcsdata_t T, lcsdata_t h);
+
+/* One update of `count` instances: ids[q] receives the device-resident velocity d_u[q],
+ * d_v[q], d_w[q] (n[0]*n[1]*n[2] values of that instance, i fastest) at time[q]. */
+int cfd2lcs_batch_update_device_c(int count, const int *ids, const lcsdata_t *const *d_u, const lcsdata_t *const *d_v,
+                                  const lcsdata_t *const *d_w, const lcsdata_t *time);
+
+/* Results and counters of one instance (as cfd2lcs_get_ftle_c, cfd2lcs_get_flowmap_c and
+ * cfd2lcs_get_counters_c). */
+int cfd2lcs_batch_get_ftle_c(int id, int lcs_handle, lcsdata_t *ftle);
+int cfd2lcs_batch_get_flowmap_c(int id, int lcs_handle, lcsdata_t *fm);
+int cfd2lcs_batch_get_counters_c(int id, long long counters[8]);
+
+/* Number of instances; first error (0: none); release every instance and clear the error. */
+int cfd2lcs_batch_size_c(void);
+int cfd2lcs_batch_error_c(char *msg, size_t len);
+void cfd2lcs_batch_reset_c(void);
 
 #ifdef __cplusplus
 }

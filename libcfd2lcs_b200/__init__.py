@@ -38,6 +38,10 @@ EXPORTED_SYMBOLS = [
     "cfd2lcs_finalize_c", "cfd2lcs_get_error_c", "cfd2lcs_reset_c", "cfd2lcs_get_ftle_c", "cfd2lcs_get_flowmap_c",
     "cfd2lcs_update_device_c", "cfd2lcs_ftle_device_ptr_c", "cfd2lcs_get_counters_c", "cfd2lcs_get_phase_times_c",
     "cfd2lcs_get_kernel_times_c", "cfd2lcs_reconstruct_noalloc_c",
+    # batched form (include/cfd2lcs_b200.h)
+    "cfd2lcs_batch_add_c", "cfd2lcs_batch_diagnostic_init_c", "cfd2lcs_batch_update_device_c", "cfd2lcs_batch_get_ftle_c",
+    "cfd2lcs_batch_get_flowmap_c", "cfd2lcs_batch_get_counters_c", "cfd2lcs_batch_size_c", "cfd2lcs_batch_error_c",
+    "cfd2lcs_batch_reset_c",
 ]
 
 
@@ -93,6 +97,21 @@ def load(precision: str = "dp") -> C.CDLL:
     lib.cfd2lcs_reconstruct_noalloc_c.restype = C.c_int
     lib.cfd2lcs_b200_grid_tables.argtypes = [P, P, P, P, P, P, P, P, P, P, C.c_char_p, C.c_size_t]
     lib.cfd2lcs_b200_grid_tables.restype = C.c_int
+    lib.cfd2lcs_batch_add_c.argtypes = [P, P, P, P, P, C.c_int, C.c_int, R, C.c_int]
+    lib.cfd2lcs_batch_add_c.restype = C.c_int
+    lib.cfd2lcs_batch_diagnostic_init_c.argtypes = [C.c_int, C.c_int, R, R]
+    lib.cfd2lcs_batch_diagnostic_init_c.restype = C.c_int
+    lib.cfd2lcs_batch_update_device_c.argtypes = [C.c_int, P, P, P, P, P]
+    lib.cfd2lcs_batch_update_device_c.restype = C.c_int
+    for f in (lib.cfd2lcs_batch_get_ftle_c, lib.cfd2lcs_batch_get_flowmap_c):
+        f.argtypes = [C.c_int, C.c_int, P]
+        f.restype = C.c_int
+    lib.cfd2lcs_batch_get_counters_c.argtypes = [C.c_int, P]
+    lib.cfd2lcs_batch_get_counters_c.restype = C.c_int
+    lib.cfd2lcs_batch_size_c.restype = C.c_int
+    lib.cfd2lcs_batch_error_c.argtypes = [C.c_char_p, C.c_size_t]
+    lib.cfd2lcs_batch_error_c.restype = C.c_int
+    lib.cfd2lcs_batch_reset_c.restype = None
     _LIBS[precision] = lib
     return lib
 
@@ -225,3 +244,74 @@ class Cfd2lcs:
             inv_delta=inv.reshape((3,) + shp).transpose(0, 3, 2, 1),
             periodic=per.astype(bool),
         )
+
+
+class Batch:
+    """The batched form (cfd2lcs_batch_*): independent instances, each with its own grid,
+    options and diagnostics, advanced together by one call."""
+
+    COUNTER_KEYS = ["integrations_fwd", "integrations_bkwd", "nsub_fwd", "nsub_bkwd", "ftle_frames", "updates", "kernel_launches",
+                    "slots_composed"]
+
+    def __init__(self, precision: str = "dp"):
+        self.precision = precision
+        self.lib = load(precision)
+        self.dtype = np.float64 if precision == "dp" else np.float32
+        self.R = C.c_double if precision == "dp" else C.c_float
+        self.shapes = []
+
+    def reset(self):
+        self.lib.cfd2lcs_batch_reset_c()
+        self.shapes = []
+
+    def add(self, n, x, y, z, flag, integrator=2, interpolator=1, cfl=0.5, mixed=False) -> int:
+        r = lambda a: np.asfortranarray(a, dtype=self.dtype).ravel(order="F")
+        nn = np.ascontiguousarray(n, dtype=np.int32)
+        xs, ys, zs = r(x), r(y), r(z)
+        f = np.asfortranarray(flag, dtype=np.int32).ravel(order="F")
+        p = lambda a: a.ctypes.data_as(C.c_void_p)
+        i = self.lib.cfd2lcs_batch_add_c(p(nn), p(xs), p(ys), p(zs), p(f), int(integrator), int(interpolator), self.R(cfl),
+                                         1 if mixed else 0)
+        if i >= 0:
+            self.shapes.append(tuple(int(v) for v in n))
+        return i
+
+    def diagnostic_init(self, inst: int, lcs_type: int, T: float, h: float) -> int:
+        return self.lib.cfd2lcs_batch_diagnostic_init_c(int(inst), int(lcs_type), self.R(T), self.R(h))
+
+    def update_device(self, ids, d_u, d_v, d_w, times) -> int:
+        """ids: instance ids; d_u/d_v/d_w: device pointers (ints); times: per instance."""
+        k = len(ids)
+        I = np.ascontiguousarray(ids, dtype=np.int32)
+        U = (C.c_void_p * k)(*d_u)
+        V = (C.c_void_p * k)(*d_v)
+        W = (C.c_void_p * k)(*d_w)
+        Tm = np.ascontiguousarray(times, dtype=self.dtype)
+        return self.lib.cfd2lcs_batch_update_device_c(k, I.ctypes.data_as(C.c_void_p), C.cast(U, C.c_void_p), C.cast(V, C.c_void_p),
+                                                      C.cast(W, C.c_void_p), Tm.ctypes.data_as(C.c_void_p))
+
+    def ftle(self, inst: int, handle: int):
+        out = np.zeros(int(np.prod(self.shapes[inst])), dtype=self.dtype)
+        rc = self.lib.cfd2lcs_batch_get_ftle_c(int(inst), int(handle), out.ctypes.data_as(C.c_void_p))
+        if rc:
+            raise RuntimeError("no FTLE field for this instance / handle")
+        return out.reshape(self.shapes[inst], order="F")
+
+    def flowmap(self, inst: int, handle: int):
+        out = np.zeros(3 * int(np.prod(self.shapes[inst])), dtype=self.dtype)
+        rc = self.lib.cfd2lcs_batch_get_flowmap_c(int(inst), int(handle), out.ctypes.data_as(C.c_void_p))
+        if rc:
+            raise RuntimeError("no flow map for this instance / handle")
+        n = self.shapes[inst]
+        N = int(np.prod(n))
+        return np.stack([out[c * N:(c + 1) * N].reshape(n, order="F") for c in range(3)])
+
+    def counters(self, inst: int) -> dict:
+        c = np.zeros(8, dtype=np.int64)
+        self.lib.cfd2lcs_batch_get_counters_c(int(inst), c.ctypes.data_as(C.c_void_p))
+        return dict(zip(self.COUNTER_KEYS, (int(v) for v in c)))
+
+    def error(self):
+        buf = C.create_string_buffer(512)
+        e = self.lib.cfd2lcs_batch_error_c(buf, 512)
+        return int(e), buf.value.decode(errors="replace")

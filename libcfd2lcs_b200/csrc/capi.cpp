@@ -322,3 +322,148 @@ CFD2LCS_EXPORT int cfd2lcs_reconstruct_noalloc_c(int lcs_handle, lcsdata_t *d_ft
   }
   return 0;
 }
+
+// ----------------------------------------------------------------------- batched form
+// Many independent instances -- each with its own grid, options and diagnostics -- advanced
+// together.  An update of the batch runs update_begin for every listed instance (ingest + CFL
+// read-back, each instance on its own stream), then update_enqueue for every instance, then
+// update_collect: one host wait per instance for its CFL number, and the instances' kernels
+// overlap on the device.  The batch has its own error state (cfd2lcs_batch_error_c) and does
+// not touch the single instance of the reference API.
+namespace {
+
+struct BatchInstance {
+  Options opt;  // the engine keeps a pointer to it
+  std::unique_ptr<EngineBase> eng;
+  int n[3];
+};
+
+struct Batch {
+  std::vector<std::unique_ptr<BatchInstance>> inst;
+  int error = 0;
+  std::string msg;
+};
+
+Batch &BT() {
+  static Batch b;
+  return b;
+}
+
+int batch_fail(const std::string &m) {
+  Batch &b = BT();
+  if (!b.error) b.msg = m;
+  b.error = 1;
+  return -1;
+}
+
+int batch_fail_rc(const std::string &m) {
+  batch_fail(m);
+  return 1;
+}
+
+BatchInstance *batch_get(int id) {
+  Batch &b = BT();
+  if (id < 0 || id >= (int)b.inst.size()) return nullptr;
+  return b.inst[id].get();
+}
+
+}  // namespace
+
+CFD2LCS_EXPORT int cfd2lcs_batch_add_c(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, const int *flag,
+                                       int integrator, int interpolator, lcsdata_t cfl, int mixed_precision) {
+  Batch &b = BT();
+  if (b.error) return -1;
+  if (integrator < EULER || integrator > RK4) return batch_fail("batch_add: bad integrator");
+  if (interpolator != NEAREST_NBR && interpolator != LINEAR && interpolator != QUADRATIC && interpolator != CUBIC)
+    return batch_fail("batch_add: bad interpolator");
+  if (!(cfl > lcsdata_t(0))) return batch_fail("batch_add: CFL must be positive");
+  std::unique_ptr<BatchInstance> bi(new BatchInstance());
+  bi->opt.integrator = integrator;
+  bi->opt.interpolator = interpolator;
+  bi->opt.cfl = (double)cfl;
+  bi->opt.mixed_precision = mixed_precision ? 1 : 0;
+  for (int a = 0; a < 3; a++) bi->n[a] = n[a];
+  bi->eng = cfd2lcs::make_engine(&bi->opt);
+  std::string msg;
+  if (!bi->eng->init(n, x, y, z, flag, msg)) return batch_fail("batch_add: " + msg);
+  b.inst.push_back(std::move(bi));
+  return (int)b.inst.size() - 1;
+}
+
+CFD2LCS_EXPORT int cfd2lcs_batch_diagnostic_init_c(int id, int lcs_type, lcsdata_t T, lcsdata_t h) {
+  Batch &b = BT();
+  if (b.error) return -1;
+  BatchInstance *bi = batch_get(id);
+  if (!bi) return batch_fail("batch_diagnostic_init: unknown instance");
+  std::string msg;
+  const int hd = bi->eng->diagnostic_init(lcs_type, 0, T, h, "batch", msg);
+  if (hd < 0) return batch_fail("batch_diagnostic_init: " + msg);
+  return hd;
+}
+
+CFD2LCS_EXPORT int cfd2lcs_batch_update_device_c(int count, const int *ids, const lcsdata_t *const *d_u, const lcsdata_t *const *d_v,
+                                                 const lcsdata_t *const *d_w, const lcsdata_t *time) {
+  Batch &b = BT();
+  if (b.error) return 1;
+  std::vector<BatchInstance *> run;
+  for (int q = 0; q < count; q++) {
+    BatchInstance *bi = batch_get(ids[q]);
+    if (!bi) return batch_fail_rc("batch_update: unknown instance");
+    run.push_back(bi);
+  }
+  std::string msg;
+  for (int q = 0; q < count; q++)
+    if (!run[q]->eng->update_begin(run[q]->n, d_u[q], d_v[q], d_w[q], time[q], true, msg)) return batch_fail_rc(msg);
+  for (int q = 0; q < count; q++)
+    if (!run[q]->eng->update_enqueue(msg)) return batch_fail_rc(msg);
+  for (int q = 0; q < count; q++)
+    if (!run[q]->eng->update_collect(msg)) return batch_fail_rc(msg);
+  return 0;
+}
+
+CFD2LCS_EXPORT int cfd2lcs_batch_get_ftle_c(int id, int lcs_handle, lcsdata_t *ftle) {
+  BatchInstance *bi = batch_get(id);
+  if (!bi) return 1;
+  std::string m;
+  return bi->eng->get_ftle(lcs_handle, ftle, m) ? 0 : 1;
+}
+
+CFD2LCS_EXPORT int cfd2lcs_batch_get_flowmap_c(int id, int lcs_handle, lcsdata_t *fm) {
+  BatchInstance *bi = batch_get(id);
+  if (!bi) return 1;
+  std::string m;
+  return bi->eng->get_flowmap(lcs_handle, fm, m) ? 0 : 1;
+}
+
+CFD2LCS_EXPORT int cfd2lcs_batch_get_counters_c(int id, long long c[8]) {
+  BatchInstance *bi = batch_get(id);
+  if (!bi) return 1;
+  const Counters &k = bi->eng->counters();
+  c[0] = k.integrations_fwd;
+  c[1] = k.integrations_bkwd;
+  c[2] = k.nsub_fwd;
+  c[3] = k.nsub_bkwd;
+  c[4] = k.ftle_frames;
+  c[5] = k.updates;
+  c[6] = k.kernel_launches;
+  c[7] = k.slots_composed;
+  return 0;
+}
+
+CFD2LCS_EXPORT int cfd2lcs_batch_size_c(void) { return (int)BT().inst.size(); }
+
+CFD2LCS_EXPORT int cfd2lcs_batch_error_c(char *msg, size_t len) {
+  Batch &b = BT();
+  if (msg && len > 0) {
+    std::strncpy(msg, b.msg.c_str(), len - 1);
+    msg[len - 1] = 0;
+  }
+  return b.error;
+}
+
+CFD2LCS_EXPORT void cfd2lcs_batch_reset_c(void) {
+  Batch &b = BT();
+  b.inst.clear();
+  b.error = 0;
+  b.msg.clear();
+}

@@ -138,7 +138,7 @@ class Engine : public EngineBase {
     if (stream_) cudaStreamSynchronize(stream_);
     arena_.release();
     for (auto &e : ev_) cudaEventDestroy(e);
-    for (auto &e : kev_) cudaEventDestroy(e);
+    for (auto &e : evpool_) cudaEventDestroy(e);
     if (red_host_) cudaFreeHost(red_host_);
     if (stream_) cudaStreamDestroy(stream_);
   }
@@ -326,6 +326,17 @@ class Engine : public EngineBase {
 
   bool update(const int n[3], const lcsdata_t *u, const lcsdata_t *v, const lcsdata_t *w, lcsdata_t time, bool device_ptrs,
               std::string &msg) override {
+    return update_begin(n, u, v, w, time, device_ptrs, msg) && update_enqueue(msg) && update_collect(msg);
+  }
+
+  // First half of an update: time levels, velocity ingest (+ spline fits of the new level)
+  // and the asynchronous read-back of the CFL maximum.  Returns without waiting.
+  bool update_begin(const int n[3], const lcsdata_t *u, const lcsdata_t *v, const lcsdata_t *w, lcsdata_t time, bool device_ptrs,
+                    std::string &msg) override {
+    if (begun_) {
+      msg = "update: previous update not finished";
+      return false;
+    }
     if (n[0] != n_[0] || n[1] != n_[1] || n[2] != n_[2]) {
       msg = "update: received velocity array of incorrect dimension";
       return false;
@@ -396,7 +407,26 @@ class Engine : public EngineBase {
     }
     CK(cudaMemcpyAsync(red_host_, red_, sizeof(DevReduce), cudaMemcpyDeviceToHost, stream_));
     CK(cudaEventRecord(ev_[1], stream_));
-    CK(cudaStreamSynchronize(stream_));
+    begun_ = true;
+    return true;
+  }
+
+  // Second part: waits for the CFL maximum only, then enqueues every diagnostic's subcycles
+  // and the h-boundary work without further host waits (timings are read in update_collect).
+  // The batched form runs update_begin for all its instances, then update_enqueue for all,
+  // then update_collect, so the instances' kernels overlap on the device.
+  bool update_enqueue(std::string &msg) override {
+    if (!begun_) {
+      msg = "update: no update begun";
+      return false;
+    }
+    begun_ = false;
+    evnext_ = 0;
+    spans_.clear();
+    const int interp = opt_->interpolator;
+    const bool spline = interp == QUADRATIC || interp == CUBIC;
+    const int deg = interp == QUADRATIC ? 2 : 3;
+    CK(cudaEventSynchronize(ev_[1]));
     red_err_ = red_host_->err;
     if (red_err_) return err_msg(msg);
     double cmax, cmin;
@@ -434,14 +464,12 @@ class Engine : public EngineBase {
       }
       if (d.type == FTLE_FWD) counters_.nsub_fwd = nsub;
       else counters_.nsub_bkwd = nsub;
-      CK(cudaEventRecord(ev_[2], stream_));
+      cudaEvent_t adv0, adv1;
+      if (!mark(adv0, msg)) return false;
       lcsdata_t lp_time = d.type == FTLE_BKWD ? t_np1_ : t_n_;
-      while ((long)kev_.size() < 2 * nsub) {
-        cudaEvent_t e;
-        CK(cudaEventCreate(&e));
-        kev_.push_back(e);
-      }
+      const int kkind = d.type == FTLE_BKWD ? SPAN_SL : SPAN_FWD;
       for (long sc = 0; sc < nsub; sc++) {
+        cudaEvent_t k0, k1;
         StageTimes S = stage_times(lp_time, dt);
         if (spline && !stage_blends(d, S, V, msg)) return false;
         if (d.type == FTLE_BKWD) {
@@ -458,39 +486,29 @@ class Engine : public EngineBase {
             if (!fit(splines_[deg].axes, d.fm[d.cur], d.fmcoef, msg)) return false;
             for (int c = 0; c < 3; c++) fo.f[c] = d.fmcoef[c];
           }
-          CK(cudaEventRecord(kev_[2 * sc], stream_));
+          if (!mark(k0, msg)) return false;
           if (!launch_sl(iv, sa, V, fo, fn, S, (T)dt, msg)) return false;
-          CK(cudaEventRecord(kev_[2 * sc + 1], stream_));
+          if (!mark(k1, msg)) return false;
+          spans_.push_back({k0, k1, kkind});
           d.cur ^= 1;
         } else {
           if (sc % kSortInterval == 0 && !sort_particles(d, msg)) return false;
-          CK(cudaEventRecord(kev_[2 * sc], stream_));
+          if (!mark(k0, msg)) return false;
           if (!launch_fwd(iv, sa, V, d.P, S, (T)dt, msg)) return false;
-          CK(cudaEventRecord(kev_[2 * sc + 1], stream_));
+          if (!mark(k1, msg)) return false;
+          spans_.push_back({k0, k1, kkind});
         }
         lp_time = lp_time + dt;
       }
-      CK(cudaEventRecord(ev_[3], stream_));
-      CK(cudaEventSynchronize(ev_[3]));
-      CK(cudaEventElapsedTime(&ms, ev_[2], ev_[3]));
-      counters_.phase_ms[d.type == FTLE_BKWD ? 1 : 2] += ms;
-      for (long sc = 0; sc < nsub; sc++) {
-        float km = 0;
-        CK(cudaEventElapsedTime(&km, kev_[2 * sc], kev_[2 * sc + 1]));
-        if (d.type == FTLE_BKWD) {
-          counters_.sl_kernel_ms += km;
-          counters_.sl_kernel_launches++;
-        } else {
-          counters_.fwd_kernel_ms += km;
-          counters_.fwd_kernel_launches++;
-        }
-      }
+      if (!mark(adv1, msg)) return false;
+      spans_.push_back({adv0, adv1, d.type == FTLE_BKWD ? 1 : 2});
     }
 
     // --- h boundaries: K7 snapshot, K4 composition, K5 FTLE, reset ----------------------
     for (auto &d : diags_) {
       if ((long)(t_np1_ / d.h) == (long)(t_n_ / d.h)) continue;
-      CK(cudaEventRecord(ev_[4], stream_));
+      cudaEvent_t f4, f5, f6, f7;
+      if (!mark(f4, msg)) return false;
       const long step0 = fnint((double)(lcsdata_t)std::fmod((double)t_np1_, (double)d.T_) / (double)d.h);
       // the reference writes slot nint(mod(t,T)/h); slot nint(T/h) and negative slots go to
       // files reconstruct never reads back
@@ -501,7 +519,7 @@ class Engine : public EngineBase {
         d.written[wslot] = 1;
         d.coef_deg[wslot] = 0;
       }
-      CK(cudaEventRecord(ev_[5], stream_));
+      if (!mark(f5, msg)) return false;
       // composition order (reconstruct_flowmap, src/flowmap_m.f90:202-268)
       const int nstep = d.nslot;
       long step = wslot;
@@ -533,31 +551,47 @@ class Engine : public EngineBase {
       CK(cudaMemcpyAsync(d.slot_list_dev, d.slot_list_host.data(), sizeof(T *) * 3 * std::max(m, 1), cudaMemcpyHostToDevice,
                          stream_));
       if (!launch_compose(iv, sa, d, m, msg)) return false;
-      CK(cudaEventRecord(ev_[6], stream_));
+      if (!mark(f6, msg)) return false;
       if (!launch_ftle(d, msg)) return false;
-      CK(cudaEventRecord(ev_[7], stream_));
+      if (!mark(f7, msg)) return false;
       // reset_lp: particles back to the grid, flow map to zero (src/cfd2lcs.f90:208-209)
       if (d.type == FTLE_BKWD) {
         for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(d.fm[d.cur][c], 0, ntot_ * sizeof(T), stream_));
       } else {
         launch_reset(d);
       }
-      CK(cudaStreamSynchronize(stream_));
-      // the working map of the next interval starts from zero; the memcpy of the slot
-      // pointer list above must complete before the host buffer is reused
-      CK(cudaEventElapsedTime(&ms, ev_[4], ev_[5]));
-      counters_.phase_ms[3] += ms;
-      CK(cudaEventElapsedTime(&ms, ev_[5], ev_[6]));
-      counters_.phase_ms[4] += ms;
-      CK(cudaEventElapsedTime(&ms, ev_[6], ev_[7]));
-      counters_.phase_ms[5] += ms;
+      // (the slot pointer list was copied from pageable host memory: cudaMemcpyAsync returns
+      // once the source is staged, so the host vector may be rewritten by the next frame)
+      spans_.push_back({f4, f5, 3});
+      spans_.push_back({f5, f6, 4});
+      spans_.push_back({f6, f7, 5});
       d.have_frame = true;
       counters_.ftle_frames++;
     }
     CK(cudaEventRecord(ev_[9], stream_));
+    return true;
+  }
+
+  // Last part: waits for the update's final event, accumulates the event-timed phases and
+  // kernels, and folds the device error word into the result.
+  bool update_collect(std::string &msg) override {
     CK(cudaEventSynchronize(ev_[9]));
+    float ms = 0;
     CK(cudaEventElapsedTime(&ms, ev_[8], ev_[9]));
     counters_.phase_ms[6] += ms;
+    for (const Span &sp : spans_) {
+      CK(cudaEventElapsedTime(&ms, sp.a, sp.b));
+      if (sp.kind == SPAN_SL) {
+        counters_.sl_kernel_ms += ms;
+        counters_.sl_kernel_launches++;
+      } else if (sp.kind == SPAN_FWD) {
+        counters_.fwd_kernel_ms += ms;
+        counters_.fwd_kernel_launches++;
+      } else {
+        counters_.phase_ms[sp.kind] += ms;
+      }
+    }
+    spans_.clear();
     return sync_errors(msg);
   }
 
@@ -1007,7 +1041,7 @@ class Engine : public EngineBase {
   DevGrid<T> dg_{};
   DevArena arena_;
   cudaStream_t stream_ = nullptr;
-  std::vector<cudaEvent_t> ev_, kev_;
+  std::vector<cudaEvent_t> ev_;
   int n_[3] = {0, 0, 0};
   long N_ = 0, ntot_ = 0;
   TV *u_[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
@@ -1022,7 +1056,29 @@ class Engine : public EngineBase {
   std::vector<DiagT> diags_;
   lcsdata_t t_n_ = 0, t_np1_ = 0;
   bool first_call_ = true;
+  bool begun_ = false;
   Counters counters_;
+  // event-timed spans of the update in flight: phase index 1..5, or one of the hot kernels
+  enum { SPAN_SL = 100, SPAN_FWD = 101 };
+  struct Span {
+    cudaEvent_t a, b;
+    int kind;
+  };
+  std::vector<cudaEvent_t> evpool_;
+  size_t evnext_ = 0;
+  std::vector<Span> spans_;
+
+  // records the next pooled event on the stream (the pool grows to one update's needs)
+  bool mark(cudaEvent_t &e, std::string &msg) {
+    if (evnext_ == evpool_.size()) {
+      cudaEvent_t x;
+      CK(cudaEventCreate(&x));
+      evpool_.push_back(x);
+    }
+    e = evpool_[evnext_++];
+    CK(cudaEventRecord(e, stream_));
+    return true;
+  }
 };
 
 std::unique_ptr<EngineBase> make_engine(const Options *opt) {

@@ -47,6 +47,13 @@ class EngineBase {
   virtual int diagnostic_init(int type, int resolution, lcsdata_t T, lcsdata_t h, const char *label, std::string &msg) = 0;
   virtual bool update(const int n[3], const lcsdata_t *u, const lcsdata_t *v, const lcsdata_t *w, lcsdata_t time, bool device_ptrs,
                       std::string &msg) = 0;
+  // update() in three parts: begin enqueues the ingest and the CFL read-back without waiting;
+  // enqueue waits for that read-back only and enqueues the subcycles and the h-boundary work;
+  // collect waits for the update's end and reads its timings and device error word
+  virtual bool update_begin(const int n[3], const lcsdata_t *u, const lcsdata_t *v, const lcsdata_t *w, lcsdata_t time,
+                            bool device_ptrs, std::string &msg) = 0;
+  virtual bool update_enqueue(std::string &msg) = 0;
+  virtual bool update_collect(std::string &msg) = 0;
   virtual bool get_ftle(int handle, lcsdata_t *out, std::string &msg) = 0;
   virtual bool get_flowmap(int handle, lcsdata_t *out, std::string &msg) = 0;
   virtual const lcsdata_t *ftle_device_ptr(int handle) = 0;
