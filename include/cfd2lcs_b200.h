@@ -116,6 +116,24 @@ int cfd2lcs_batch_size_c(void);
 int cfd2lcs_batch_error_c(char *msg, size_t len);
 void cfd2lcs_batch_reset_c(void);
 
+/* ---------------------------------------------------------------------------------------
+ * Adjoint.  No counterpart in the reference.  Gradient of J = sum_x weight(x) FTLE(x), the
+ * backward FTLE of the whole horizon (the frame the library computes with h = T, T = time of
+ * the last level minus the first), with respect to the velocity at every level, by a
+ * hand-written reverse sweep through the semi-Lagrangian updates (LINEAR interpolation;
+ * integrator EULER, TRAPEZOIDAL or RK2) with a flow-map checkpoint every `checkpoint_every`
+ * updates.  Grid: rectilinear, three-dimensional, every direction periodic, no boundary
+ * flags.  d_u[l], d_v[l], d_w[l]: device arrays of level l (n[0]*n[1]*n[2], i fastest);
+ * times: host, increasing; d_weight: device, n[0]*n[1]*n[2].  Writes *J and, when d_gu,
+ * d_gv, d_gw are not NULL, dJ/du of every level into those device arrays.  Discrete choices
+ * of the forward map (subcycle counts, interpolation brackets, clamped weights) are held
+ * fixed.  Allocates device memory for the levels, their adjoints and the checkpoints.
+ * Returns 0, or 1 with the reason in msg (at most len bytes). */
+int cfd2lcs_adjoint_ftle_c(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, int integrator,
+                           lcsdata_t cfl, int nlevels, const lcsdata_t *const *d_u, const lcsdata_t *const *d_v,
+                           const lcsdata_t *const *d_w, const lcsdata_t *times, const lcsdata_t *d_weight, int checkpoint_every,
+                           double *J, lcsdata_t *const *d_gu, lcsdata_t *const *d_gv, lcsdata_t *const *d_gw, char *msg, size_t len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -42,6 +42,8 @@ EXPORTED_SYMBOLS = [
     "cfd2lcs_batch_add_c", "cfd2lcs_batch_diagnostic_init_c", "cfd2lcs_batch_update_device_c", "cfd2lcs_batch_get_ftle_c",
     "cfd2lcs_batch_get_flowmap_c", "cfd2lcs_batch_get_counters_c", "cfd2lcs_batch_size_c", "cfd2lcs_batch_error_c",
     "cfd2lcs_batch_reset_c",
+    # adjoint (include/cfd2lcs_b200.h)
+    "cfd2lcs_adjoint_ftle_c",
 ]
 
 
@@ -112,6 +114,8 @@ def load(precision: str = "dp") -> C.CDLL:
     lib.cfd2lcs_batch_error_c.argtypes = [C.c_char_p, C.c_size_t]
     lib.cfd2lcs_batch_error_c.restype = C.c_int
     lib.cfd2lcs_batch_reset_c.restype = None
+    lib.cfd2lcs_adjoint_ftle_c.argtypes = [P, P, P, P, C.c_int, R, C.c_int, P, P, P, P, P, C.c_int, P, P, P, P, C.c_char_p, C.c_size_t]
+    lib.cfd2lcs_adjoint_ftle_c.restype = C.c_int
     _LIBS[precision] = lib
     return lib
 
@@ -315,3 +319,35 @@ class Batch:
         buf = C.create_string_buffer(512)
         e = self.lib.cfd2lcs_batch_error_c(buf, 512)
         return int(e), buf.value.decode(errors="replace")
+
+
+def adjoint_ftle(grid, u, v, w, times, weight, integrator=2, cfl=0.5, checkpoint_every=20, precision="dp", gradient=True):
+    """J = sum(weight * FTLE) of the backward flow map over all levels and, with gradient,
+    dJ/du of every level (cfd2lcs_adjoint_ftle_c).  u, v, w: lists of CUDA tensors, one per
+    level (n[0]*n[1]*n[2] values, i fastest, the library's precision); weight: CUDA tensor.
+    Returns (J, gu, gv, gw) with gu, gv, gw lists of CUDA tensors (None without gradient)."""
+    import torch
+    lib = load(precision)
+    dt = np.float64 if precision == "dp" else np.float32
+    R = C.c_double if precision == "dp" else C.c_float
+    L = len(u)
+    n = np.ascontiguousarray(grid.n, dtype=np.int32)
+    xs, ys, zs = (np.asfortranarray(a, dtype=dt).ravel(order="F") for a in (grid.x, grid.y, grid.z))
+    ptrs = lambda ts: (C.c_void_p * L)(*[t.data_ptr() for t in ts])
+    tm = np.ascontiguousarray(times, dtype=dt)
+    J = C.c_double(0.0)
+    g = None
+    if gradient:
+        g = [[torch.empty_like(t) for t in comp] for comp in (u, v, w)]
+    msg = C.create_string_buffer(512)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    rc = lib.cfd2lcs_adjoint_ftle_c(p(n), p(xs), p(ys), p(zs), int(integrator), R(cfl), L, C.cast(ptrs(u), C.c_void_p),
+                                    C.cast(ptrs(v), C.c_void_p), C.cast(ptrs(w), C.c_void_p), p(tm), C.c_void_p(weight.data_ptr()),
+                                    int(checkpoint_every), C.byref(J),
+                                    C.cast(ptrs(g[0]), C.c_void_p) if g else None, C.cast(ptrs(g[1]), C.c_void_p) if g else None,
+                                    C.cast(ptrs(g[2]), C.c_void_p) if g else None, msg, 512)
+    if rc:
+        raise RuntimeError(msg.value.decode(errors="replace"))
+    if g:
+        return J.value, g[0], g[1], g[2]
+    return J.value, None, None, None

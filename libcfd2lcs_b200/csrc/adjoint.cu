@@ -1,0 +1,693 @@
+// Reverse-mode derivative of a backward-FTLE objective J = sum_x w(x) FTLE(x) with respect to
+// the gridded velocity at every time level.  No counterpart in the reference library; the
+// forward model is the library's own backward semi-Lagrangian path (update_flowmap_sl,
+// src/flowmap_m.f90:17-104, with LINEAR interpolation, src/lp_tracking_m.f90:342-474, and the
+// EULER / TRAPEZOIDAL / RK2 steps of integrate_lp, src/lp_motion_m.f90:129-210) over every
+// update from the first level to the last, and compute_ftle (src/lcs_m.f90:66-193) of the
+// final flow map -- the frame the library computes when h equals the whole horizon.
+//
+// Forward: the velocity levels are ingested once (padded, ghost-filled, CFL maxima read back
+// per level to fix every update's subcycle count); the flow map is stored every K updates
+// (checkpoints).  Reverse: from the FTLE adjoint (eigenvector of the Cauchy-Green tensor,
+// transpose of the central differences) back through every subcycle in reverse order; each
+// checkpoint segment is first recomputed forward, keeping the flow map before each subcycle.
+// The adjoint of one subcycle recomputes that subcycle's stage positions and scatters
+// (atomicAdd) into the adjoint of the previous flow map and of the two velocity levels with
+// the transposed trilinear weights; the position adjoint picks up the trilinear gradients.
+// Ghost cells, which the forward fills as periodic copies, are folded back into their source
+// nodes.  Discrete choices (subcycle counts, interpolation brackets, clamped weights) are
+// held fixed, as differentiation of the piecewise-smooth map requires.
+//
+// Scope: a rectilinear grid with every flag LCS_INTERNAL and every non-singleton direction
+// periodic (the ABC configuration); LINEAR interpolation; EULER, TRAPEZOIDAL or RK2.
+#include "adjoint.h"
+
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+#include "grid.h"
+#include "kernels.cuh"
+
+namespace cfd2lcs {
+
+namespace {
+
+#define ACK(call)                                                                                \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess) {                                                                     \
+      msg = std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " + #call;               \
+      return false;                                                                              \
+    }                                                                                            \
+  } while (0)
+
+enum { EULER = 0, TRAPEZOIDAL = 1, RK2 = 2 };
+
+// device memory of one adjoint call
+class Pool {
+ public:
+  ~Pool() {
+    for (void *p : ptrs_) cudaFree(p);
+  }
+  template <typename X>
+  X *alloc(size_t n, std::string &msg) {
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, n * sizeof(X) > 0 ? n * sizeof(X) : 1);
+    if (e != cudaSuccess) {
+      msg = std::string("device allocation failed: ") + cudaGetErrorString(e);
+      return nullptr;
+    }
+    ptrs_.push_back(p);
+    return static_cast<X *>(p);
+  }
+
+ private:
+  std::vector<void *> ptrs_;
+};
+
+// Trilinear stencil of lin_stencil (same brackets and clamped fractions) plus, per axis, the
+// derivative of the fraction with respect to the coordinate (0 where the fraction is clamped).
+template <typename T>
+struct LinStencilAD {
+  LinStencil<T> st;
+  T t[3], dtdx[3];
+};
+
+template <typename T>
+__device__ __forceinline__ void lin_stencil_ad(const DevGrid<T> &g, const T x[3], const int no[3], LinStencilAD<T> &s) {
+  lin_stencil(g, x, no, s.st);
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const T *L = g.li[a];
+    const int n0 = no[a];
+    int lo, hi;
+    if (x[a] > __ldg(L + n0)) {
+      lo = n0;
+      hi = n0 + 1;
+    } else {
+      lo = n0 - 1;
+      hi = n0;
+    }
+    lo = min(max(lo, 0), g.P.n[a] + 1);
+    hi = min(max(hi, 0), g.P.n[a] + 1);
+    const T x0 = __ldg(L + lo), x1 = __ldg(L + hi);
+    const T raw = (x[a] - x0) / (x1 - x0);
+    s.t[a] = clamp01(raw);
+    s.dtdx[a] = (raw > T(0) && raw < T(1)) ? T(1) / (x1 - x0) : T(0);
+  }
+}
+
+// corner q (bit 0: x, bit 1: y, bit 2: z) of a trilinear stencil
+template <typename T>
+__device__ __forceinline__ int corner(const LinStencil<T> &st, int q) {
+  return st.p0 + ((q & 1) ? st.s[0] : 0) + ((q & 2) ? st.s[1] : 0) + ((q & 4) ? st.s[2] : 0);
+}
+
+// d(weight_q)/d(t_a) of the trilinear weights
+template <typename T>
+__device__ __forceinline__ T dweight(const T t[3], int q, int a) {
+  T r = T(1);
+#pragma unroll
+  for (int b = 0; b < 3; b++) {
+    const bool up = (q >> b) & 1;
+    if (b == a) r *= up ? T(1) : T(-1);
+    else r *= up ? t[b] : T(1) - t[b];
+  }
+  return r;
+}
+
+// ---------------------------------------------------------------------------------------
+// Adjoint of one backward SL subcycle (k_sl_subcycle with LINEAR interpolation, no flags).
+// fbn: adjoint of the new flow map (interior values used); fbo, ubn, ubp: accumulated.
+// ---------------------------------------------------------------------------------------
+template <typename T, int INTEG>
+__global__ void __launch_bounds__(256) k_sl_adjoint(DevGrid<T> g, VelFields<T> V, FieldPtrs<T> fmo, FieldPtrs<T> fbn, FieldPtrsW<T> fbo,
+                                                     FieldPtrsW<T> ubn, FieldPtrsW<T> ubp, StageTimes S, T dt) {
+  int i, j, k;
+  if (!node_of_thread(g.P.n, i, j, k)) return;
+  const int p = pidx(g.P.sx, g.P.sxy, i, j, k);
+  const T a[3] = {fbn.f[0][p], fbn.f[1][p], fbn.f[2][p]};
+  if (a[0] == T(0) && a[1] == T(0) && a[2] == T(0)) return;
+  const T HALF = T(1) / T(2);
+  const int no[3] = {i, j, k};
+  const T x0[3] = {__ldg(g.lt[0] + i), __ldg(g.lt[1] + j), __ldg(g.lt[2] + k)};
+  // --- forward recomputation (integrate<>, first stage on the node) ---
+  const T ct0 = T(S.ct[0]), omc0 = T(1) - ct0;
+  T u1[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) u1[c] = omc0 * __ldg(V.un[c] + p) + ct0 * __ldg(V.unp1[c] + p);
+  T x[3], xh[3];
+  LinStencilAD<T> s2;
+  const T ct1 = T(S.ct[1]), omc1 = T(1) - ct1;
+  if (INTEG == RK2) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) xh[c] = x0[c] + HALF * dt * u1[c];
+    lin_stencil_ad(g, xh, no, s2);
+    T u2[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) u2[c] = lin_apply_blend<T, T>(s2.st, V.un[c], V.unp1[c], omc1, ct1);
+#pragma unroll
+    for (int c = 0; c < 3; c++) x[c] = x0[c] + dt * u2[c];
+  } else {
+#pragma unroll
+    for (int c = 0; c < 3; c++) x[c] = x0[c] + dt * u1[c];
+  }
+  LinStencilAD<T> s3;
+  lin_stencil_ad(g, x, no, s3);
+  // --- fm_new = fm_old(x) + (x - x0) ---
+  T xb[3] = {a[0], a[1], a[2]};
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    const int cq = corner(s3.st, q);
+    const T wq = s3.st.w[q];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const T f = __ldg(fmo.f[c] + cq);
+      atomicAdd(fbo.f[c] + cq, wq * a[c]);
+#pragma unroll
+      for (int d = 0; d < 3; d++) xb[d] += a[c] * dweight(s3.t, q, d) * s3.dtdx[d] * f;
+    }
+  }
+  // --- stages ---
+  T u1b[3];
+  if (INTEG == RK2) {
+    T u2b[3], xhb[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int c = 0; c < 3; c++) u2b[c] = dt * xb[c];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int cq = corner(s2.st, q);
+      const T wq = s2.st.w[q];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        atomicAdd(ubn.f[c] + cq, omc1 * wq * u2b[c]);
+        atomicAdd(ubp.f[c] + cq, ct1 * wq * u2b[c]);
+        const T vb = omc1 * __ldg(V.un[c] + cq) + ct1 * __ldg(V.unp1[c] + cq);
+#pragma unroll
+        for (int d = 0; d < 3; d++) xhb[d] += u2b[c] * dweight(s2.t, q, d) * s2.dtdx[d] * vb;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) u1b[c] = HALF * dt * xhb[c];
+  } else {
+#pragma unroll
+    for (int c = 0; c < 3; c++) u1b[c] = dt * xb[c];
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    atomicAdd(ubn.f[c] + p, omc0 * u1b[c]);
+    atomicAdd(ubp.f[c] + p, ct0 * u1b[c]);
+  }
+}
+
+// source interior index of a padded cell along one periodic axis
+__device__ __forceinline__ int wrap_index(int v, int n) { return v < 1 ? v + n : (v > n ? v - n : v); }
+
+// Adjoint of the periodic ghost fill (write_ghosts rule 0 on every face, edge and corner):
+// each ghost's adjoint is added to its source node and cleared.
+template <typename T>
+__global__ void __launch_bounds__(256) k_fold_ghosts(DevGrid<T> g, FieldPtrsW<T> f, long ntot) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= ntot) return;
+  const int i = (int)(p % g.P.sx), j = (int)((p / g.P.sx) % (g.P.sxy / g.P.sx)), k = (int)(p / g.P.sxy);
+  const int si = wrap_index(i, g.P.n[0]), sj = wrap_index(j, g.P.n[1]), sk = wrap_index(k, g.P.n[2]);
+  if (si == i && sj == j && sk == k) return;
+  const int q = pidx(g.P.sx, g.P.sxy, si, sj, sk);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const T v = f.f[c][p];
+    if (v != T(0)) atomicAdd(f.f[c] + q, v);
+    f.f[c][p] = T(0);
+  }
+}
+
+// interior of a padded field -> compact i-fastest arrays (the composed map of an h = T frame)
+template <typename T>
+__global__ void __launch_bounds__(256) k_interior(DevGrid<T> g, FieldPtrs<T> src, FieldPtrsW<T> dst) {
+  int i, j, k;
+  if (!node_of_thread(g.P.n, i, j, k)) return;
+  const int p = pidx(g.P.sx, g.P.sxy, i, j, k), q = interior_index(g.P.n, i, j, k);
+#pragma unroll
+  for (int c = 0; c < 3; c++) dst.f[c][q] = src.f[c][p];
+}
+
+// ---------------------------------------------------------------------------------------
+// Adjoint of compute_ftle on a periodic grid: FTLE = log(sqrt(lambda))/T with lambda the
+// largest eigenvalue of C = G^T G, G the central-difference gradient of the displacement.
+// d lambda / d G = 2 (G v) v^T with v the unit eigenvector; the central differences are
+// transposed onto the two neighbours (periodic images wrapped to their source nodes).
+// ---------------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_ftle_adjoint(DevGrid<T> g, FieldPtrs<T> fm, const T *__restrict__ wgt, T Tint, FieldPtrsW<T> fb) {
+  int i, j, k;
+  if (!node_of_thread(g.P.n, i, j, k)) return;
+  const double w = (double)wgt[interior_index(g.P.n, i, j, k)];
+  if (w == 0.0) return;
+  const int idx[3] = {i, j, k};
+  double G[3][3], den[3];
+  int qp[3], qm[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    if (g.P.n[a] == 1) {
+      for (int c = 0; c < 3; c++) G[c][a] = 0.0;
+      den[a] = 0.0;
+      qp[a] = qm[a] = -1;
+      continue;
+    }
+    int ip[3] = {i, j, k}, im[3] = {i, j, k};
+    ip[a] = wrap_index(idx[a] + 1, g.P.n[a]);
+    im[a] = wrap_index(idx[a] - 1, g.P.n[a]);
+    qp[a] = pidx(g.P.sx, g.P.sxy, ip[0], ip[1], ip[2]);
+    qm[a] = pidx(g.P.sx, g.P.sxy, im[0], im[1], im[2]);
+    den[a] = (double)(__ldg(g.lt[a] + idx[a] + 1) - __ldg(g.lt[a] + idx[a] - 1));
+    for (int c = 0; c < 3; c++) G[c][a] = (double)(fm.f[c][qp[a]] - fm.f[c][qm[a]]) / den[a];
+  }
+  double C[3][3];
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++) C[a][b] = G[0][a] * G[0][b] + G[1][a] * G[1][b] + G[2][a] * G[2][b];
+  const double lam = eig3_max(C[0][0], C[0][1], C[0][2], C[1][1], C[1][2], C[2][2]);
+  const double tiny = sizeof(T) == 8 ? DBL_MIN : (double)FLT_MIN;
+  if (!(sqrt(lam) > tiny)) return;  // max(sqrt(W3), tiny) is constant there
+  // unit eigenvector of lam: the largest cross product of two rows of C - lam I
+  const double r[3][3] = {{C[0][0] - lam, C[0][1], C[0][2]}, {C[1][0], C[1][1] - lam, C[1][2]}, {C[2][0], C[2][1], C[2][2] - lam}};
+  double v[3] = {0, 0, 0}, best = 0.0;
+  for (int m = 0; m < 3; m++) {
+    const double *x = r[m], *y = r[(m + 1) % 3];
+    const double cx[3] = {x[1] * y[2] - x[2] * y[1], x[2] * y[0] - x[0] * y[2], x[0] * y[1] - x[1] * y[0]};
+    const double nn = cx[0] * cx[0] + cx[1] * cx[1] + cx[2] * cx[2];
+    if (nn > best) {
+      best = nn;
+      v[0] = cx[0];
+      v[1] = cx[1];
+      v[2] = cx[2];
+    }
+  }
+  if (!(best > 0.0)) return;  // repeated largest eigenvalue: no unique derivative direction
+  const double s = 1.0 / sqrt(best);
+  v[0] *= s;
+  v[1] *= s;
+  v[2] *= s;
+  const double Gv[3] = {G[0][0] * v[0] + G[0][1] * v[1] + G[0][2] * v[2], G[1][0] * v[0] + G[1][1] * v[1] + G[1][2] * v[2],
+                        G[2][0] * v[0] + G[2][1] * v[1] + G[2][2] * v[2]};
+  // dJ/dG = w / (2 lam T) * 2 (G v) v^T
+  const double coef = w / (lam * (double)Tint);
+  for (int a = 0; a < 3; a++) {
+    if (qp[a] < 0) continue;
+    for (int c = 0; c < 3; c++) {
+      const double gb = coef * Gv[c] * v[a] / den[a];
+      atomicAdd(fb.f[c] + qp[a], T(gb));
+      atomicAdd(fb.f[c] + qm[a], T(-gb));
+    }
+  }
+}
+
+// adjoint velocity (after the ghost fold) -> caller's i-fastest arrays
+template <typename T>
+__global__ void __launch_bounds__(256) k_grad_out(DevGrid<T> g, FieldPtrs<T> src, T *gu, T *gv, T *gw) {
+  int i, j, k;
+  if (!node_of_thread(g.P.n, i, j, k)) return;
+  const int p = pidx(g.P.sx, g.P.sxy, i, j, k), q = interior_index(g.P.n, i, j, k);
+  gu[q] = src.f[0][p];
+  gv[q] = src.f[1][p];
+  gw[q] = src.f[2][p];
+}
+
+template <typename T>
+class Adjoint {
+ public:
+  explicit Adjoint(const AdjointProblem &pr) : pr_(pr) {}
+  ~Adjoint() {
+    if (stream_) {
+      cudaStreamSynchronize(stream_);
+      cudaStreamDestroy(stream_);
+    }
+    if (red_host_) cudaFreeHost(red_host_);
+  }
+
+  bool run(double *J, std::string &msg) {
+    if (!setup(msg)) return false;
+    if (!forward(J, msg)) return false;
+    if (pr_.gu && pr_.gv && pr_.gw && !backward(msg)) return false;
+    ACK(cudaStreamSynchronize(stream_));
+    DevReduce r{};
+    ACK(cudaMemcpy(&r, red_dev_, sizeof(DevReduce), cudaMemcpyDeviceToHost));
+    if (r.err) {
+      msg = "adjoint: device error in the advection kernels";
+      return false;
+    }
+    return true;
+  }
+
+ private:
+  bool setup(std::string &msg) {
+    const int *n = pr_.n;
+    if (pr_.nlevels < 2) {
+      msg = "adjoint: at least two velocity levels are needed";
+      return false;
+    }
+    if (pr_.integrator != EULER && pr_.integrator != TRAPEZOIDAL && pr_.integrator != RK2) {
+      msg = "adjoint: the integrator must be EULER, TRAPEZOIDAL or RK2";
+      return false;
+    }
+    if (pr_.checkpoint_every < 1 || !(pr_.cfl > 0)) {
+      msg = "adjoint: checkpoint interval and CFL must be positive";
+      return false;
+    }
+    for (int l = 1; l < pr_.nlevels; l++)
+      if (!(pr_.times[l] > pr_.times[l - 1])) {
+        msg = "adjoint: level times must increase";
+        return false;
+      }
+    std::vector<int> flag((size_t)n[0] * n[1] * n[2], 0);
+    if (!hg_.build(n, pr_.x, pr_.y, pr_.z, flag.data())) {
+      msg = "adjoint: " + hg_.error;
+      return false;
+    }
+    for (int a = 0; a < 3; a++)
+      if (n[a] > 1 && !hg_.P.per[a]) {
+        msg = "adjoint: every non-singleton direction must be periodic";
+        return false;
+      }
+    if (hg_.P.single_axis >= 0 || hg_.P.has_flags) {
+      msg = "adjoint: a three-dimensional grid without boundary flags is required";
+      return false;
+    }
+    N_ = (long)n[0] * n[1] * n[2];
+    ntot_ = hg_.ntot();
+    GridParams<T> P;
+    const GridParams<lcsdata_t> &H = hg_.P;
+    for (int a = 0; a < 3; a++) {
+      P.n[a] = H.n[a];
+      P.per[a] = H.per[a];
+      for (int s = 0; s < 2; s++)
+        for (int e = 0; e < 2; e++) P.gx[a][s][e] = (T)H.gx[a][s][e];
+    }
+    P.sx = H.sx;
+    P.sxy = H.sxy;
+    P.single_axis = H.single_axis;
+    P.zquirk = H.zquirk;
+    for (int q = 0; q < 6; q++) P.bb[q] = (T)H.bb[q];
+    for (int d = 0; d < 27; d++)
+      for (int c = 0; c < 3; c++) P.ps[d][c] = (T)H.ps[d][c];
+    P.has_flags = 0;
+    P.maxtrack = H.maxtrack;
+    dg_.P = P;
+    for (int a = 0; a < 3; a++) {
+      if (!(dg_.lt[a] = upload(hg_.lt[a], msg))) return false;
+      if (!(dg_.li[a] = upload(hg_.li[a], msg))) return false;
+      if (!(dg_.invd[a] = upload(hg_.invd[a], msg))) return false;
+      dg_.nrm[a] = nullptr;
+    }
+    dg_.flag = nullptr;
+    ACK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    ACK(cudaMallocHost(&red_host_, sizeof(DevReduce)));
+    if (!(red_dev_ = pool_.alloc<DevReduce>(1, msg))) return false;
+    return true;
+  }
+
+  template <typename V>
+  T *upload(const std::vector<V> &h, std::string &msg) {
+    std::vector<T> tmp(h.begin(), h.end());
+    T *d = pool_.alloc<T>(tmp.size(), msg);
+    if (!d) return nullptr;
+    if (cudaMemcpy(d, tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) {
+      msg = "adjoint: upload failed";
+      return nullptr;
+    }
+    return d;
+  }
+
+  dim3 node_grid() const { return dim3((dg_.P.n[0] + 31) / 32, (dg_.P.n[1] + 7) / 8, dg_.P.n[2]); }
+
+  bool field3(T *f[3], std::string &msg) {
+    for (int c = 0; c < 3; c++) {
+      if (!(f[c] = pool_.alloc<T>(ntot_, msg))) return false;
+      ACK(cudaMemsetAsync(f[c], 0, ntot_ * sizeof(T), stream_));
+    }
+    return true;
+  }
+
+  // stage time fractions as Engine::stage_times computes them
+  StageTimes stage_times(lcsdata_t t0, lcsdata_t t1, lcsdata_t t, lcsdata_t dt) const {
+    const lcsdata_t HALF = lcsdata_t(1) / lcsdata_t(2);
+    auto ct = [&](lcsdata_t tt) -> double {
+      if (t1 == t0) return 0.0;
+      lcsdata_t v = (tt - t0) / (t1 - t0);
+      v = std::max(std::min(v, lcsdata_t(1)), lcsdata_t(0));
+      return (double)v;
+    };
+    StageTimes S{};
+    if (pr_.integrator == EULER) S.ct[0] = ct(t);
+    else if (pr_.integrator == TRAPEZOIDAL) S.ct[0] = ct(t + HALF * dt);
+    else {
+      S.ct[0] = ct(t);
+      S.ct[1] = ct(t + HALF * dt);
+    }
+    return S;
+  }
+
+  bool forward(double *J, std::string &msg) {
+    const int L = pr_.nlevels;
+    // padded levels + CFL maxima -> subcycles of every update (set_dt, src/lp_motion_m.f90:56-127)
+    U_.assign((size_t)3 * L, nullptr);
+    cmax_.assign(L, 0.0);
+    for (int l = 0; l < L; l++) {
+      T *f[3];
+      if (!field3(f, msg)) return false;
+      for (int c = 0; c < 3; c++) U_[3 * l + c] = f[c];
+      DevReduce init{};
+      double big = std::numeric_limits<double>::max();
+      std::memcpy(&init.cmin, &big, sizeof(double));
+      *red_host_ = init;
+      ACK(cudaMemcpyAsync(red_dev_, red_host_, sizeof(DevReduce), cudaMemcpyHostToDevice, stream_));
+      k_ingest<T, T, lcsdata_t, false><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, pr_.u[l], pr_.v[l], pr_.w[l], f[0], f[1], f[2],
+                                                                                  red_dev_);
+      ACK(cudaGetLastError());
+      ACK(cudaMemcpyAsync(red_host_, red_dev_, sizeof(DevReduce), cudaMemcpyDeviceToHost, stream_));
+      ACK(cudaStreamSynchronize(stream_));
+      if (red_host_->err) {
+        msg = "adjoint: non-finite velocity";
+        return false;
+      }
+      std::memcpy(&cmax_[l], &red_host_->cmax, sizeof(double));
+    }
+    nsub_.assign(L, 0);
+    for (int l = 1; l < L; l++) {
+      const lcsdata_t dt_f = pr_.times[l] - pr_.times[l - 1];
+      const lcsdata_t q = ((lcsdata_t)cmax_[l] * dt_f) / lcsdata_t(pr_.cfl);
+      long ns = (long)std::ceil((double)q);
+      nsub_[l] = (int)std::max(1L, ns);
+    }
+    if (!field3(fm_[0], msg) || !field3(fm_[1], msg)) return false;
+    cur_ = 0;
+    const int K = pr_.checkpoint_every;
+    const int nseg = (L - 2) / K + 1;  // segments of updates 1..L-1
+    cp_.assign((size_t)3 * nseg, nullptr);
+    for (int l = 1; l < L; l++) {
+      if ((l - 1) % K == 0) {
+        const int s = (l - 1) / K;
+        for (int c = 0; c < 3; c++) {
+          if (!(cp_[3 * s + c] = pool_.alloc<T>(ntot_, msg))) return false;
+          ACK(cudaMemcpyAsync(cp_[3 * s + c], fm_[cur_][c], ntot_ * sizeof(T), cudaMemcpyDeviceToDevice, stream_));
+        }
+      }
+      if (!advance(l, fm_, cur_, nullptr, msg)) return false;
+    }
+    // FTLE of the final map and J
+    T *in[3];
+    for (int c = 0; c < 3; c++)
+      if (!(in[c] = pool_.alloc<T>(N_, msg))) return false;
+    T *ftle = pool_.alloc<T>(N_, msg);
+    if (!ftle) return false;
+    FieldPtrs<T> src{};
+    FieldPtrsW<T> dst{};
+    for (int c = 0; c < 3; c++) {
+      src.f[c] = fm_[cur_][c];
+      dst.f[c] = in[c];
+    }
+    k_interior<T><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, src, dst);
+    FieldPtrs<T> cm{};
+    for (int c = 0; c < 3; c++) cm.f[c] = in[c];
+    const T Tint = (T)(pr_.times[L - 1] - pr_.times[0]);
+    k_ftle<T, T, false><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, cm, ftle, Tint, 0);
+    ACK(cudaGetLastError());
+    std::vector<T> hf(N_), hw(N_);
+    ACK(cudaMemcpyAsync(hf.data(), ftle, N_ * sizeof(T), cudaMemcpyDeviceToHost, stream_));
+    ACK(cudaMemcpyAsync(hw.data(), pr_.weight, N_ * sizeof(T), cudaMemcpyDeviceToHost, stream_));
+    ACK(cudaStreamSynchronize(stream_));
+    double s = 0.0;
+    for (long q = 0; q < N_; q++) s += (double)hw[q] * (double)hf[q];
+    *J = s;
+    return true;
+  }
+
+  // every subcycle of update l (levels l-1 -> l) on the double buffer buf, starting from
+  // buf[cur]; cur follows the result.  With `keep`, the flow map before subcycle q is copied
+  // to keep[3 q + c].
+  bool advance(int l, T *buf[2][3], int &cur, T *const *keep, std::string &msg) {
+    const lcsdata_t t0 = pr_.times[l - 1], t1 = pr_.times[l];
+    const lcsdata_t dt_f = t1 - t0;
+    const int ns = nsub_[l];
+    const lcsdata_t dt = lcsdata_t(-1) * (dt_f / (lcsdata_t)ns);
+    VelFields<T> V{};
+    for (int c = 0; c < 3; c++) {
+      V.un[c] = U_[3 * (l - 1) + c];
+      V.unp1[c] = U_[3 * l + c];
+    }
+    lcsdata_t lp = t1;
+    for (int q = 0; q < ns; q++) {
+      if (keep)
+        for (int c = 0; c < 3; c++)
+          ACK(cudaMemcpyAsync(keep[3 * q + c], buf[cur][c], ntot_ * sizeof(T), cudaMemcpyDeviceToDevice, stream_));
+      const StageTimes S = stage_times(t0, t1, lp, dt);
+      FieldPtrs<T> fo{};
+      FieldPtrsW<T> fn{};
+      for (int c = 0; c < 3; c++) {
+        fo.f[c] = buf[cur][c];
+        fn.f[c] = buf[cur ^ 1][c];
+      }
+      const SplineAxes<T> sa{};
+      int *err = &red_dev_->err;
+      const dim3 grd = node_grid(), blk(32, 8, 1);
+      if (pr_.integrator == RK2)
+        k_sl_subcycle<T, T, RK2_, INTERP_LINEAR, false><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, (T)dt, err);
+      else if (pr_.integrator == TRAPEZOIDAL)
+        k_sl_subcycle<T, T, TRAPEZOIDAL_, INTERP_LINEAR, false><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, (T)dt, err);
+      else
+        k_sl_subcycle<T, T, EULER_, INTERP_LINEAR, false><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, (T)dt, err);
+      ACK(cudaGetLastError());
+      cur ^= 1;
+      lp = lp + dt;
+    }
+    return true;
+  }
+
+  bool backward(std::string &msg) {
+    const int L = pr_.nlevels, K = pr_.checkpoint_every;
+    Ub_.assign((size_t)3 * L, nullptr);
+    for (int l = 0; l < L; l++) {
+      T *f[3];
+      if (!field3(f, msg)) return false;
+      for (int c = 0; c < 3; c++) Ub_[3 * l + c] = f[c];
+    }
+    T *fbar[2][3];
+    if (!field3(fbar[0], msg) || !field3(fbar[1], msg)) return false;
+    int fb = 0;
+    // FTLE adjoint of the final map
+    {
+      FieldPtrs<T> fm{};
+      FieldPtrsW<T> out{};
+      for (int c = 0; c < 3; c++) {
+        fm.f[c] = fm_[cur_][c];
+        out.f[c] = fbar[fb][c];
+      }
+      const T Tint = (T)(pr_.times[L - 1] - pr_.times[0]);
+      k_ftle_adjoint<T><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, fm, pr_.weight, Tint, out);
+      ACK(cudaGetLastError());
+    }
+    const long nb = (ntot_ + 255) / 256;
+    const int nseg = (L - 2) / K + 1;
+    // flow maps before every subcycle of the largest segment
+    int maxsub = 0;
+    for (int s = 0; s < nseg; s++) {
+      int m = 0;
+      for (int l = s * K + 1; l <= std::min((s + 1) * K, L - 1); l++) m += nsub_[l];
+      maxsub = std::max(maxsub, m);
+    }
+    std::vector<T *> states((size_t)3 * maxsub, nullptr);
+    for (auto &ptr : states)
+      if (!(ptr = pool_.alloc<T>(ntot_, msg))) return false;
+    T *work[2][3];
+    for (int b = 0; b < 2; b++)
+      for (int c = 0; c < 3; c++) work[b][c] = fm_[b][c];  // the forward buffers are free now
+    for (int s = nseg - 1; s >= 0; s--) {
+      const int l0 = s * K + 1, l1 = std::min((s + 1) * K, L - 1);
+      // recompute the segment from its checkpoint, keeping the flow map before each subcycle
+      std::vector<int> first(l1 - l0 + 2, 0);
+      for (int l = l0; l <= l1; l++) first[l - l0 + 1] = first[l - l0] + nsub_[l];
+      for (int c = 0; c < 3; c++) ACK(cudaMemcpyAsync(work[0][c], cp_[3 * s + c], ntot_ * sizeof(T), cudaMemcpyDeviceToDevice, stream_));
+      int wc = 0;
+      for (int l = l0; l <= l1; l++)
+        if (!advance(l, work, wc, &states[(size_t)3 * first[l - l0]], msg)) return false;
+      // reverse through the segment
+      for (int l = l1; l >= l0; l--) {
+        const lcsdata_t t0 = pr_.times[l - 1], t1 = pr_.times[l];
+        const int ns = nsub_[l];
+        const lcsdata_t dt = lcsdata_t(-1) * ((t1 - t0) / (lcsdata_t)ns);
+        std::vector<lcsdata_t> lps(ns);
+        lcsdata_t lp = t1;
+        for (int q = 0; q < ns; q++) {
+          lps[q] = lp;
+          lp = lp + dt;
+        }
+        VelFields<T> V{};
+        FieldPtrsW<T> ubn{}, ubp{};
+        for (int c = 0; c < 3; c++) {
+          V.un[c] = U_[3 * (l - 1) + c];
+          V.unp1[c] = U_[3 * l + c];
+          ubn.f[c] = Ub_[3 * (l - 1) + c];
+          ubp.f[c] = Ub_[3 * l + c];
+        }
+        for (int q = ns - 1; q >= 0; q--) {
+          // the new map's ghosts were copies of its interior
+          FieldPtrsW<T> fw{};
+          for (int c = 0; c < 3; c++) fw.f[c] = fbar[fb][c];
+          k_fold_ghosts<T><<<(unsigned)nb, 256, 0, stream_>>>(dg_, fw, ntot_);
+          for (int c = 0; c < 3; c++) ACK(cudaMemsetAsync(fbar[fb ^ 1][c], 0, ntot_ * sizeof(T), stream_));
+          FieldPtrs<T> fo{}, fbn{};
+          FieldPtrsW<T> fbo{};
+          for (int c = 0; c < 3; c++) {
+            fo.f[c] = states[(size_t)3 * (first[l - l0] + q) + c];
+            fbn.f[c] = fbar[fb][c];
+            fbo.f[c] = fbar[fb ^ 1][c];
+          }
+          const StageTimes S = stage_times(t0, t1, lps[q], dt);
+          if (pr_.integrator == RK2)
+            k_sl_adjoint<T, RK2><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, V, fo, fbn, fbo, ubn, ubp, S, (T)dt);
+          else
+            k_sl_adjoint<T, EULER><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, V, fo, fbn, fbo, ubn, ubp, S, (T)dt);
+          ACK(cudaGetLastError());
+          fb ^= 1;
+        }
+      }
+    }
+    // velocity ghosts were copies of the ingested interior: fold, then hand out
+    for (int l = 0; l < L; l++) {
+      FieldPtrsW<T> f{};
+      FieldPtrs<T> fr{};
+      for (int c = 0; c < 3; c++) {
+        f.f[c] = Ub_[3 * l + c];
+        fr.f[c] = Ub_[3 * l + c];
+      }
+      k_fold_ghosts<T><<<(unsigned)nb, 256, 0, stream_>>>(dg_, f, ntot_);
+      k_grad_out<T><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, fr, pr_.gu[l], pr_.gv[l], pr_.gw[l]);
+      ACK(cudaGetLastError());
+    }
+    return true;
+  }
+
+
+  const AdjointProblem &pr_;
+  HostGrid<lcsdata_t> hg_;
+  DevGrid<T> dg_{};
+  Pool pool_;
+  cudaStream_t stream_ = nullptr;
+  DevReduce *red_host_ = nullptr, *red_dev_ = nullptr;
+  long N_ = 0, ntot_ = 0;
+  std::vector<T *> U_, Ub_, cp_;
+  std::vector<double> cmax_;
+  std::vector<int> nsub_;
+  T *fm_[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  int cur_ = 0;
+};
+
+}  // namespace
+
+bool adjoint_ftle(const AdjointProblem &p, double *J, std::string &msg) {
+  Adjoint<lcsdata_t> a(p);
+  return a.run(J, msg);
+}
+
+}  // namespace cfd2lcs

@@ -13,6 +13,7 @@
 #include <memory>
 #include <string>
 
+#include "adjoint.h"
 #include "engine.h"
 
 using cfd2lcs::Counters;
@@ -466,4 +467,23 @@ CFD2LCS_EXPORT void cfd2lcs_batch_reset_c(void) {
   b.inst.clear();
   b.error = 0;
   b.msg.clear();
+}
+
+// ----------------------------------------------------------------------- adjoint
+// Gradient of J = sum weight * FTLE (backward FTLE of the whole horizon) with respect to the
+// velocity at every level; see include/cfd2lcs_b200.h.  Returns 0, or 1 with msg.
+CFD2LCS_EXPORT int cfd2lcs_adjoint_ftle_c(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, int integrator,
+                                          lcsdata_t cfl, int nlevels, const lcsdata_t *const *d_u, const lcsdata_t *const *d_v,
+                                          const lcsdata_t *const *d_w, const lcsdata_t *times, const lcsdata_t *d_weight,
+                                          int checkpoint_every, double *J, lcsdata_t *const *d_gu, lcsdata_t *const *d_gv,
+                                          lcsdata_t *const *d_gw, char *msg, size_t len) {
+  cfd2lcs::AdjointProblem p{n, x, y, z, integrator, (double)cfl, nlevels, d_u, d_v, d_w, times, d_weight, checkpoint_every,
+                            d_gu, d_gv, d_gw};
+  std::string m;
+  const bool ok = cfd2lcs::adjoint_ftle(p, J, m);
+  if (msg && len > 0) {
+    std::strncpy(msg, m.c_str(), len - 1);
+    msg[len - 1] = 0;
+  }
+  return ok ? 0 : 1;
 }

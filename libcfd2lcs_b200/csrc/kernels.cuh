@@ -424,7 +424,7 @@ __global__ void __launch_bounds__(256) k_particle_count(DevGrid<T> g, Particles<
 }
 
 // exclusive scan of cnt within each chunk into offs (cnt reset to 0), chunk totals to tsum
-__global__ void __launch_bounds__(256) k_scan_tiles(int *cnt, int *offs, int *tsum, int n) {
+static __global__ void __launch_bounds__(256) k_scan_tiles(int *cnt, int *offs, int *tsum, int n) {
   __shared__ int wsum[8];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const long base = (long)blockIdx.x * SORT_TILE + threadIdx.x * 8;
@@ -463,7 +463,7 @@ __global__ void __launch_bounds__(256) k_scan_tiles(int *cnt, int *offs, int *ts
 }
 
 // exclusive scan of the chunk totals in place (one block)
-__global__ void __launch_bounds__(1024) k_scan_tile_sums(int *tsum, int nt) {
+static __global__ void __launch_bounds__(1024) k_scan_tile_sums(int *tsum, int nt) {
   __shared__ int wsum[32];
   __shared__ int carry;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

@@ -1,0 +1,105 @@
+"""The adjoint (cfd2lcs_adjoint_ftle_c): its forward objective equals the library's own FTLE
+frame for h = T, its gradient agrees with central finite differences of that objective along
+random directions, and it does not depend on the checkpoint interval."""
+import math
+
+import numpy as np
+import pytest
+
+from libcfd2lcs_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _levels(n, L, dt, sigma=0.05, seed=7):
+    import torch
+    g = W.abc_grid(n)
+    rng = np.random.default_rng(seed)
+    base = W.abc_velocity(g)
+    lev = [[], [], []]
+    for _ in range(L):
+        for c in range(3):
+            a = base[c] + sigma * rng.standard_normal(base[c].shape)
+            lev[c].append(torch.from_numpy(np.ascontiguousarray(a.ravel(order="F"))).cuda())
+    times = [k * dt for k in range(L)]
+    return g, lev, times
+
+
+def _weight(g):
+    import torch
+    x, y, z = g.x, g.y, g.z
+    box = (x > 0.5 * math.pi) & (x < 1.5 * math.pi) & (y > 0.5 * math.pi) & (y < 1.5 * math.pi) & (z > 0.5 * math.pi) & \
+          (z < 1.5 * math.pi)
+    w = box.astype(np.float64) / max(int(box.sum()), 1)
+    return torch.from_numpy(np.ascontiguousarray(w.ravel(order="F"))).cuda()
+
+
+@pytest.mark.parametrize("integrator", [0, 2])
+def test_forward_objective_is_the_library_frame(integrator):
+    import libcfd2lcs_b200 as L
+    n, nl, dt = 12, 9, 0.05
+    g, lev, times = _levels(n, nl, dt)
+    wgt = _weight(g)
+    J, *_ = L.adjoint_ftle(g, *lev, times, wgt, integrator=integrator, gradient=False)
+    api = L.Cfd2lcs("dp")
+    api.reset()
+    api.init(g.n, g.x, g.y, g.z, g.flag)
+    T = times[-1]
+    h = api.diagnostic_init(1, 0, T, T, "b")
+    api.set_option("INTEGRATOR", integrator)
+    api.set_option("INTERPOLATOR", 1)
+    for k in range(nl):
+        api.update_device(lev[0][k].data_ptr(), lev[1][k].data_ptr(), lev[2][k].data_ptr(), times[k])
+    assert api.error()[0] == 0, api.error()
+    ftle = api.ftle(h).ravel(order="F")
+    J_lib = float(np.dot(wgt.cpu().numpy(), ftle))
+    api.reset()
+    assert abs(J - J_lib) <= 1e-12 * max(abs(J_lib), 1e-30), (J, J_lib)
+
+
+@pytest.mark.parametrize("integrator", [0, 2])
+def test_gradient_matches_finite_differences(integrator):
+    import torch
+
+    import libcfd2lcs_b200 as L
+    n, nl, dt = 10, 7, 0.05
+    g, lev, times = _levels(n, nl, dt)
+    wgt = _weight(g)
+    J, gu, gv, gw = L.adjoint_ftle(g, *lev, times, wgt, integrator=integrator, checkpoint_every=2)
+    grads = (gu, gv, gw)
+    rng = np.random.default_rng(11)
+    for _ in range(4):
+        d = [[torch.from_numpy(rng.standard_normal(lev[c][k].numel())).cuda() for k in range(nl)] for c in range(3)]
+        eps = 1e-6
+        plus = [[lev[c][k] + eps * d[c][k] for k in range(nl)] for c in range(3)]
+        minus = [[lev[c][k] - eps * d[c][k] for k in range(nl)] for c in range(3)]
+        Jp, *_ = L.adjoint_ftle(g, *plus, times, wgt, integrator=integrator, gradient=False)
+        Jm, *_ = L.adjoint_ftle(g, *minus, times, wgt, integrator=integrator, gradient=False)
+        fd = (Jp - Jm) / (2 * eps)
+        ad = sum(float(torch.dot(grads[c][k], d[c][k])) for c in range(3) for k in range(nl))
+        assert abs(fd - ad) <= 1e-5 * max(abs(fd), abs(ad)), (fd, ad)
+
+
+def test_checkpoint_interval_does_not_change_the_gradient():
+    import torch
+
+    import libcfd2lcs_b200 as L
+    g, lev, times = _levels(10, 8, 0.05)
+    wgt = _weight(g)
+    ref = L.adjoint_ftle(g, *lev, times, wgt, checkpoint_every=100)
+    for K in (1, 3):
+        out = L.adjoint_ftle(g, *lev, times, wgt, checkpoint_every=K)
+        assert out[0] == ref[0]
+        for c in range(1, 4):
+            for a, b in zip(out[c], ref[c]):
+                torch.testing.assert_close(a, b, rtol=1e-12, atol=1e-15)
+
+
+def test_adjoint_rejects_walled_grids():
+    import torch
+
+    import libcfd2lcs_b200 as L
+    g = W.double_gyre_grid(16, 8)
+    u = [torch.zeros(16 * 8, dtype=torch.float64, device="cuda") for _ in range(3)]
+    with pytest.raises(RuntimeError, match="periodic|three-dimensional"):
+        L.adjoint_ftle(g, u, u, u, [0.0, 0.1, 0.2], torch.zeros(16 * 8, dtype=torch.float64, device="cuda"))
