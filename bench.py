@@ -543,18 +543,116 @@ def run_batch(args):
         torch.distributed.destroy_process_group()
 
 
+ADJ_DESC = ("adjoint: J = mean backward FTLE over [pi/2,3pi/2]^3 of ABC flow on a 128^3 grid, 201 velocity levels "
+            "(steady ABC + N(0, 0.01^2) noise from torch's CUDA generator, seed 7), 200 updates at dt=0.05, RK2, linear, "
+            "flow-map checkpoint every 20 updates")
+
+
+def run_adjoint(args):
+    """The adjoint workload: one gradient dJ/du of every level (FP32, the sp library) timed by
+    wall clock around the call (device synchronised on both sides); checked against the FP64
+    gradient (dp library) and against central finite differences of the FP64 objective along
+    random directions."""
+    import torch
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    import libcfd2lcs_b200 as L
+    from libcfd2lcs_b200 import workloads as W
+    n = args.n or 128
+    nl, dt, K = 201, 0.05, 20
+    g = W.abc_grid(n)
+    base = W.abc_velocity(g)
+    gen7 = torch.Generator(device="cuda")
+    gen7.manual_seed(7)
+    b64 = [torch.from_numpy(np.ascontiguousarray(a.ravel(order="F"))).cuda() for a in base]
+    lev64 = [[], [], []]
+    for _ in range(nl):
+        for c in range(3):
+            lev64[c].append(b64[c] + 0.01 * torch.randn(b64[c].numel(), generator=gen7, device="cuda", dtype=torch.float64))
+    times = [k * dt for k in range(nl)]
+    x, y, z = g.x, g.y, g.z
+    box = (x > 0.5 * math.pi) & (x < 1.5 * math.pi) & (y > 0.5 * math.pi) & (y < 1.5 * math.pi) & (z > 0.5 * math.pi) & (z < 1.5 * math.pi)
+    w64 = torch.from_numpy(np.ascontiguousarray((box / box.sum()).astype(np.float64).ravel(order="F"))).cuda()
+    lev32 = [[t.float() for t in comp] for comp in lev64]
+    w32 = w64.float()
+    # FP32 gradient (timed), after one untimed call
+    L.adjoint_ftle(g, *lev32, times, w32, checkpoint_every=K, precision="sp")
+    runs = []
+    for _ in range(max(1, args.steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        J32, g32u, g32v, g32w = L.adjoint_ftle(g, *lev32, times, w32, checkpoint_every=K, precision="sp")
+        torch.cuda.synchronize()
+        runs.append(time.perf_counter() - t0)
+    el = min(runs)
+    # FP64 gradient and finite differences
+    J64, gu, gv, gw = L.adjoint_ftle(g, *lev64, times, w64, checkpoint_every=K, precision="dp")
+    num = sum(float(torch.sum((a.double() - b) ** 2)) for A, B in ((g32u, gu), (g32v, gv), (g32w, gw)) for a, b in zip(A, B))
+    den = sum(float(torch.sum(b ** 2)) for B in (gu, gv, gw) for b in B)
+    rel32 = math.sqrt(num / den) if den > 0 else None
+    nfd = args.fd_dirs
+    fd_err = []
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(16)
+    for _ in range(nfd):
+        d = [[torch.randn(lev64[c][k].numel(), generator=gen, device="cuda", dtype=torch.float64) for k in range(nl)] for c in range(3)]
+        eps = 1e-7
+        Jp, *_ = L.adjoint_ftle(g, *[[lev64[c][k] + eps * d[c][k] for k in range(nl)] for c in range(3)], times, w64,
+                                checkpoint_every=K, precision="dp", gradient=False)
+        Jm, *_ = L.adjoint_ftle(g, *[[lev64[c][k] - eps * d[c][k] for k in range(nl)] for c in range(3)], times, w64,
+                                checkpoint_every=K, precision="dp", gradient=False)
+        fd = (Jp - Jm) / (2 * eps)
+        ad = sum(float(torch.dot(G[k], d[c][k])) for c, G in enumerate((gu, gv, gw)) for k in range(nl))
+        fd_err.append(abs(fd - ad) / max(abs(fd), abs(ad), 1e-300))
+    # work: grid points x subcycles of the forward map, run twice (forward + segment recompute)
+    api = L.Cfd2lcs("sp")
+    api.reset()
+    api.init(g.n, g.x, g.y, g.z, g.flag)
+    api.diagnostic_init(1, 0, times[-1], times[-1], "b")
+    api.set_option("INTEGRATOR", 2)
+    api.set_option("INTERPOLATOR", 1)
+    for k in range(nl):
+        api.update_device(lev32[0][k].data_ptr(), lev32[1][k].data_ptr(), lev32[2][k].data_ptr(), times[k])
+    work = api.counters()["integrations_bkwd"]
+    api.reset()
+    line = {"metric": METRIC, "value": work / el, "unit": UNIT, "n_gpus": 1, "steps": len(runs), "warmup": 1,
+            "ms_per_step": 1000.0 * el, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": ADJ_DESC, "grid": [n, n, n], "levels": nl,
+                                            "timing": "wall clock of one gradient call (forward, checkpoints, reverse sweep), best of steps",
+                                            "value_counts": "grid points x subcycles of the forward map per gradient"},
+            "gradient_s": el, "J_fp32": J32, "J_fp64": J64,
+            "gradient_fp32_vs_fp64_rel_l2": rel32,
+            "finite_difference_check": {"directions": nfd, "eps": 1e-7, "form": "FP64 objective, central differences",
+                                        "max_rel_err": max(fd_err) if fd_err else None,
+                                        "median_rel_err": float(np.median(fd_err)) if fd_err else None, "rel_errs": fd_err,
+                                        "note": "the objective is only piecewise smooth (trilinear interpolation, clamped "
+                                                "weights): central differences carry kink and rounding noise"}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="abc256", choices=sorted(WORKLOADS) + ["batch64"])
+    ap.add_argument("--workload", default="abc256", choices=sorted(WORKLOADS) + ["batch64", "adj128"])
+    ap.add_argument("--fd-dirs", type=int, default=16, help="adj128: finite-difference directions")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--acc-n", type=int, default=64, help="grid of the mixed-vs-FP64 FTLE error run (0: skip)")
     ap.add_argument("--n", type=int, default=None, help="override the grid size (smaller smoke runs)")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
+    if args.workload == "adj128":
+        if args.impl == "reference":
+            world, rank, _ = dist_setup()
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no adjoint"}))
+            return
+        run_adjoint(args)
+        return
     if args.workload == "batch64":
         if args.impl == "reference":
             world, rank, _ = dist_setup()
