@@ -4,6 +4,8 @@
 // boundary conditions on particles and the node search.
 #pragma once
 
+#include <type_traits>
+
 #include "device_common.cuh"
 #include "spline.cuh"
 
@@ -114,8 +116,9 @@ __device__ __forceinline__ void sample_velocity(const DevGrid<T> &g, const Splin
     for (int c = 0; c < 3; c++) out[c] = T(lin_apply_blend<T, TV>(st, V.un[c], V.unp1[c], omc, ct));
   } else {
     constexpr int KC = INTERP == INTERP_SPLINE4 ? 4 : 0;
+    constexpr bool UNI = !std::is_same<T, TV>::value;
     SplineStencil<T> st;
-    if (!spline_stencil<T, KC>(g, sa, x, no, st)) {
+    if (!spline_stencil<T, KC, UNI>(g, sa, x, no, st)) {
       out[0] = out[1] = out[2] = T(0);
       return;
     }
@@ -138,7 +141,7 @@ __device__ __forceinline__ void sample_velocity_node(const DevGrid<T> &g, const 
   for (int c = 0; c < 3; c++) out[c] = T(omc * __ldg(V.un[c] + p) + ct * __ldg(V.unp1[c] + p));
 }
 
-template <typename T, int INTERP>
+template <typename T, int INTERP, bool UNI = false>
 __device__ __forceinline__ void sample_field(const DevGrid<T> &g, const SplineAxes<T> &sa, const T *const f[3], const T x[3],
                                              const int no[3], T out[3]) {
   if (INTERP == INTERP_NEAREST) {
@@ -153,7 +156,7 @@ __device__ __forceinline__ void sample_field(const DevGrid<T> &g, const SplineAx
   } else {
     constexpr int KC = INTERP == INTERP_SPLINE4 ? 4 : 0;
     SplineStencil<T> st;
-    if (!spline_stencil<T, KC>(g, sa, x, no, st)) {
+    if (!spline_stencil<T, KC, UNI>(g, sa, x, no, st)) {
       out[0] = out[1] = out[2] = T(0);
       return;
     }

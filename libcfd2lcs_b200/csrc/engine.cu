@@ -820,6 +820,7 @@ class Engine : public EngineBase {
       D.k = A.k;
       if (!(D.t = upload(A.t, msg))) return false;
       if (!(D.rinv = upload(A.rinv, msg))) return false;
+      if (!(D.tu = upload(A.tu, msg))) return false;
       const std::vector<lcsdata_t> pull = pull_table(A);
       if (!(D.pull = upload(pull, msg))) return false;
       // the velocity fits solve with the LU factors rounded to the velocity type
@@ -828,6 +829,7 @@ class Engine : public EngineBase {
       E.k = A.k;
       if (!(E.t = upload<TV>(A.t, msg))) return false;
       if (!(E.rinv = upload<TV>(A.rinv, msg))) return false;
+      if (!(E.tu = upload<TV>(A.tu, msg))) return false;
       if (!(E.pull = upload<TV>(pull, msg))) return false;
     }
     splines_[deg] = s;

@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(256) k_sl_subcycle(DevGrid<T> g, SplineAxes<T>
   }
   T fmp[3];
   const int nod[3] = {i, j, k};
-  sample_field<T, INTERP>(g, sa, fmo.f, x, nod, fmp);
+  sample_field<T, INTERP, !std::is_same<T, TV>::value>(g, sa, fmo.f, x, nod, fmp);
   const int fl = HAS_FLAGS ? (int)g.flag[p] : (int)LCS_INTERNAL;
   const T mask = fl != LCS_MASK ? T(1) : T(0);
   T vpre[3], vfin[3];

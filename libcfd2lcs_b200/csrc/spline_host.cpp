@@ -5,6 +5,8 @@
 #include "spline_host.h"
 
 #include <algorithm>
+#include <cmath>
+#include <limits>
 
 namespace cfd2lcs {
 
@@ -104,6 +106,23 @@ bool SplineAxisHost<R>::build(const std::vector<R> &x, int order) {
         const R span = t[l + m - 1] - t[l + m - j - 1];
         rinv[(size_t)(l - 1) * 6 + slot++] = span != R(0) ? R(1) / span : R(0);
       }
+  }
+  // intervals whose basis depends on equally spaced knots only, t(l-k+2) .. t(l+k-1): there
+  // the k non-zero B-splines are the uniform polynomials of (x - t(l)) / h
+  tu.assign((size_t)2 * (n + k), R(0));
+  for (int l = 1; l <= n + k; l++) tu[(size_t)2 * (l - 1)] = t[l - 1];
+  // (relative tolerance above the rounding of coordinates built as x0 + i dx; the uniform
+  // polynomials then differ from the recurrence on the actual knots by about that much)
+  const R tol = std::max(R(1e-9), R(64) * std::numeric_limits<R>::epsilon());
+  for (int l = k; l <= n; l++) {
+    const R h = t[l] - t[l - 1];
+    if (!(h > R(0))) continue;
+    bool uni = true;
+    for (int m = l - k + 1; m + 1 <= l + k - 2; m++) {
+      const R d = t[m + 1] - t[m];
+      if (!(std::fabs(d - h) <= tol * h)) uni = false;
+    }
+    if (uni) tu[(size_t)2 * (l - 1) + 1] = R(1) / h;
   }
   return true;
 }
