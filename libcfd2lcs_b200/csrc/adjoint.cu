@@ -120,11 +120,14 @@ __device__ __forceinline__ T dweight(const T t[3], int q, int a) {
 
 // ---------------------------------------------------------------------------------------
 // Adjoint of one backward SL subcycle (k_sl_subcycle with LINEAR interpolation, no flags).
-// fbn: adjoint of the new flow map (interior values used); fbo, ubn, ubp: accumulated.
+// fbn: adjoint of the new flow map (interior values used); fbo: accumulated adjoint of the
+// previous map.  The velocity adjoint of the second stage goes to a2 (scattered, one blended
+// field: the time blend is distributed onto the two levels afterwards by k_distribute), that
+// of the first stage, which sits on the node, to a1 (plain stores).
 // ---------------------------------------------------------------------------------------
 template <typename T, int INTEG>
 __global__ void __launch_bounds__(256) k_sl_adjoint(DevGrid<T> g, VelFields<T> V, FieldPtrs<T> fmo, FieldPtrs<T> fbn, FieldPtrsW<T> fbo,
-                                                     FieldPtrsW<T> ubn, FieldPtrsW<T> ubp, StageTimes S, T dt) {
+                                                     FieldPtrsW<T> a1, FieldPtrsW<T> a2, StageTimes S, T dt) {
   int i, j, k;
   if (!node_of_thread(g.P.n, i, j, k)) return;
   const int p = pidx(g.P.sx, g.P.sxy, i, j, k);
@@ -182,8 +185,7 @@ __global__ void __launch_bounds__(256) k_sl_adjoint(DevGrid<T> g, VelFields<T> V
       const T wq = s2.st.w[q];
 #pragma unroll
       for (int c = 0; c < 3; c++) {
-        atomicAdd(ubn.f[c] + cq, omc1 * wq * u2b[c]);
-        atomicAdd(ubp.f[c] + cq, ct1 * wq * u2b[c]);
+        atomicAdd(a2.f[c] + cq, wq * u2b[c]);
         const T vb = omc1 * __ldg(V.un[c] + cq) + ct1 * __ldg(V.unp1[c] + cq);
 #pragma unroll
         for (int d = 0; d < 3; d++) xhb[d] += u2b[c] * dweight(s2.t, q, d) * s2.dtdx[d] * vb;
@@ -196,10 +198,23 @@ __global__ void __launch_bounds__(256) k_sl_adjoint(DevGrid<T> g, VelFields<T> V
     for (int c = 0; c < 3; c++) u1b[c] = dt * xb[c];
   }
 #pragma unroll
-  for (int c = 0; c < 3; c++) {
-    atomicAdd(ubn.f[c] + p, omc0 * u1b[c]);
-    atomicAdd(ubp.f[c] + p, ct0 * u1b[c]);
-  }
+  for (int c = 0; c < 3; c++) a1.f[c][p] = u1b[c];
+}
+
+// velocity adjoint of one subcycle onto the two levels: un += (1-ct0) a1 + (1-ct1) a2,
+// unp1 += ct0 a1 + ct1 a2; a1 and a2 are cleared for the next subcycle
+template <typename T>
+__global__ void __launch_bounds__(256) k_distribute(FieldPtrsW<T> a1, FieldPtrsW<T> a2, FieldPtrsW<T> ubn, FieldPtrsW<T> ubp, T ct0, T ct1,
+                                                     long ntot) {
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= ntot) return;
+  const int c = blockIdx.y;
+  const T x1 = a1.f[c][q], x2 = a2.f[c][q];
+  if (x1 == T(0) && x2 == T(0)) return;
+  ubn.f[c][q] += (T(1) - ct0) * x1 + (T(1) - ct1) * x2;
+  ubp.f[c][q] += ct0 * x1 + ct1 * x2;
+  a1.f[c][q] = T(0);
+  a2.f[c][q] = T(0);
 }
 
 // source interior index of a padded cell along one periodic axis
@@ -429,6 +444,16 @@ class Adjoint {
     return true;
   }
 
+  // `count` padded fields carved from one zeroed allocation (one cudaMalloc for all levels)
+  bool slab(std::vector<T *> &out, size_t count, std::string &msg) {
+    T *base = pool_.alloc<T>(count * (size_t)ntot_, msg);
+    if (!base) return false;
+    ACK(cudaMemsetAsync(base, 0, count * (size_t)ntot_ * sizeof(T), stream_));
+    out.assign(count, nullptr);
+    for (size_t q = 0; q < count; q++) out[q] = base + q * (size_t)ntot_;
+    return true;
+  }
+
   // stage time fractions as Engine::stage_times computes them
   StageTimes stage_times(lcsdata_t t0, lcsdata_t t1, lcsdata_t t, lcsdata_t dt) const {
     const lcsdata_t HALF = lcsdata_t(1) / lcsdata_t(2);
@@ -451,12 +476,10 @@ class Adjoint {
   bool forward(double *J, std::string &msg) {
     const int L = pr_.nlevels;
     // padded levels + CFL maxima -> subcycles of every update (set_dt, src/lp_motion_m.f90:56-127)
-    U_.assign((size_t)3 * L, nullptr);
+    if (!slab(U_, (size_t)3 * L, msg)) return false;
     cmax_.assign(L, 0.0);
     for (int l = 0; l < L; l++) {
-      T *f[3];
-      if (!field3(f, msg)) return false;
-      for (int c = 0; c < 3; c++) U_[3 * l + c] = f[c];
+      T *f[3] = {U_[3 * l], U_[3 * l + 1], U_[3 * l + 2]};
       DevReduce init{};
       double big = std::numeric_limits<double>::max();
       std::memcpy(&init.cmin, &big, sizeof(double));
@@ -484,14 +507,12 @@ class Adjoint {
     cur_ = 0;
     const int K = pr_.checkpoint_every;
     const int nseg = (L - 2) / K + 1;  // segments of updates 1..L-1
-    cp_.assign((size_t)3 * nseg, nullptr);
+    if (!slab(cp_, (size_t)3 * nseg, msg)) return false;
     for (int l = 1; l < L; l++) {
       if ((l - 1) % K == 0) {
         const int s = (l - 1) / K;
-        for (int c = 0; c < 3; c++) {
-          if (!(cp_[3 * s + c] = pool_.alloc<T>(ntot_, msg))) return false;
+        for (int c = 0; c < 3; c++)
           ACK(cudaMemcpyAsync(cp_[3 * s + c], fm_[cur_][c], ntot_ * sizeof(T), cudaMemcpyDeviceToDevice, stream_));
-        }
       }
       if (!advance(l, fm_, cur_, nullptr, msg)) return false;
     }
@@ -566,12 +587,7 @@ class Adjoint {
 
   bool backward(std::string &msg) {
     const int L = pr_.nlevels, K = pr_.checkpoint_every;
-    Ub_.assign((size_t)3 * L, nullptr);
-    for (int l = 0; l < L; l++) {
-      T *f[3];
-      if (!field3(f, msg)) return false;
-      for (int c = 0; c < 3; c++) Ub_[3 * l + c] = f[c];
-    }
+    if (!slab(Ub_, (size_t)3 * L, msg)) return false;
     T *fbar[2][3];
     if (!field3(fbar[0], msg) || !field3(fbar[1], msg)) return false;
     int fb = 0;
@@ -589,6 +605,16 @@ class Adjoint {
     }
     const long nb = (ntot_ + 255) / 256;
     const int nseg = (L - 2) / K + 1;
+    // per-subcycle velocity adjoints of the two stages (zero between subcycles)
+    FieldPtrsW<T> A1{}, A2{};
+    {
+      T *a[3], *b[3];
+      if (!field3(a, msg) || !field3(b, msg)) return false;
+      for (int c = 0; c < 3; c++) {
+        A1.f[c] = a[c];
+        A2.f[c] = b[c];
+      }
+    }
     // flow maps before every subcycle of the largest segment
     int maxsub = 0;
     for (int s = 0; s < nseg; s++) {
@@ -596,9 +622,8 @@ class Adjoint {
       for (int l = s * K + 1; l <= std::min((s + 1) * K, L - 1); l++) m += nsub_[l];
       maxsub = std::max(maxsub, m);
     }
-    std::vector<T *> states((size_t)3 * maxsub, nullptr);
-    for (auto &ptr : states)
-      if (!(ptr = pool_.alloc<T>(ntot_, msg))) return false;
+    std::vector<T *> states;
+    if (!slab(states, (size_t)3 * maxsub, msg)) return false;
     T *work[2][3];
     for (int b = 0; b < 2; b++)
       for (int c = 0; c < 3; c++) work[b][c] = fm_[b][c];  // the forward buffers are free now
@@ -645,9 +670,10 @@ class Adjoint {
           }
           const StageTimes S = stage_times(t0, t1, lps[q], dt);
           if (pr_.integrator == RK2)
-            k_sl_adjoint<T, RK2><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, V, fo, fbn, fbo, ubn, ubp, S, (T)dt);
+            k_sl_adjoint<T, RK2><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, V, fo, fbn, fbo, A1, A2, S, (T)dt);
           else
-            k_sl_adjoint<T, EULER><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, V, fo, fbn, fbo, ubn, ubp, S, (T)dt);
+            k_sl_adjoint<T, EULER><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, V, fo, fbn, fbo, A1, A2, S, (T)dt);
+          k_distribute<T><<<dim3((unsigned)nb, 3), 256, 0, stream_>>>(A1, A2, ubn, ubp, (T)S.ct[0], (T)S.ct[1], ntot_);
           ACK(cudaGetLastError());
           fb ^= 1;
         }
