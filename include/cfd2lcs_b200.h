@@ -41,6 +41,13 @@ int cfd2lcs_get_flowmap_c(int lcs_handle, lcsdata_t *fm);
  * each, i fastest, same precision as lcsdata_t); no host copies. */
 void cfd2lcs_update_device_c(int n[3], const lcsdata_t *d_u, const lcsdata_t *d_v, const lcsdata_t *d_w, lcsdata_t time);
 
+/* Velocity invariants of a diagnostic's latest frame, computed when the option
+ * VELOCITY_INVARIANTS is TRUE (compute_invariants, src/invariants_m.f90:15-208, which the
+ * reference writes to its output file): five consecutive arrays of n[0]*n[1]*n[2] values --
+ * Q-criterion flag, D zone (1..4), C (R_S > 0) flag, H and the lambda-2 flag.  Returns 0, or
+ * 1 for an unknown handle, no frame yet or the option off. */
+int cfd2lcs_get_invariants_c(int lcs_handle, lcsdata_t *inv);
+
 /* Device pointer of a diagnostic's latest FTLE field (n[0]*n[1]*n[2] doubles in the dp
  * build, floats in the sp build), valid until the next update or finalize. */
 const lcsdata_t *cfd2lcs_ftle_device_ptr_c(int lcs_handle);

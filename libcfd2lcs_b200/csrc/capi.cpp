@@ -250,6 +250,13 @@ CFD2LCS_EXPORT int cfd2lcs_get_flowmap_c(int lcs_handle, lcsdata_t *fm) {
   return lib.eng->get_flowmap(lcs_handle, fm, m) ? 0 : 1;
 }
 
+CFD2LCS_EXPORT int cfd2lcs_get_invariants_c(int lcs_handle, lcsdata_t *inv) {
+  Library &lib = L();
+  if (!lib.eng) return 1;
+  std::string m;
+  return lib.eng->get_invariants(lcs_handle, inv, m) ? 0 : 1;
+}
+
 CFD2LCS_EXPORT void cfd2lcs_update_device_c(int n[3], const lcsdata_t *d_u, const lcsdata_t *d_v, const lcsdata_t *d_w, lcsdata_t time) {
   do_update(n, d_u, d_v, d_w, time, true);
 }

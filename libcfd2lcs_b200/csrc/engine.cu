@@ -87,6 +87,7 @@ struct Diag {
   long long blend_update[3] = {-1, -1, -1};
   T *composed[3] = {nullptr, nullptr, nullptr};  // interior, last FTLE frame
   lcsdata_t *ftle = nullptr;                      // interior
+  lcsdata_t *inv[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // velocity invariants (interior)
   bool have_frame = false;
 };
 
@@ -514,6 +515,7 @@ class Engine : public EngineBase {
       // files reconstruct never reads back
       const long wslot = fnint((double)((lcsdata_t)std::fmod((double)t_np1_, (double)d.T_) / d.h));
       (void)step0;
+      if (opt_->velocity_invariants && !snapshot_velocity(wslot, msg)) return false;
       if (wslot >= 0 && wslot < d.nslot) {
         if (!launch_snapshot(d, (int)wslot, msg)) return false;
         d.written[wslot] = 1;
@@ -553,6 +555,9 @@ class Engine : public EngineBase {
       if (!launch_compose(iv, sa, d, m, msg)) return false;
       if (!mark(f6, msg)) return false;
       if (!launch_ftle(d, msg)) return false;
+      // compute_invariants from the velocity of the reconstruction's starting step: the
+      // current one (backward) or the next, not yet wrapped (forward), flowmap_m.f90:202-245
+      if (opt_->velocity_invariants && !launch_invariants(d, wslot + (d.type == FTLE_FWD ? 1 : 0), msg)) return false;
       if (!mark(f7, msg)) return false;
       // reset_lp: particles back to the grid, flow map to zero (src/cfd2lcs.f90:208-209)
       if (d.type == FTLE_BKWD) {
@@ -678,6 +683,17 @@ class Engine : public EngineBase {
       CK(cudaMemcpy(tmp.data(), d->composed[c], N_ * sizeof(T), cudaMemcpyDeviceToHost));
       for (long q = 0; q < N_; q++) out[c * N_ + q] = (lcsdata_t)tmp[q];
     }
+    return true;
+  }
+
+  bool get_invariants(int handle, lcsdata_t *out, std::string &msg) override {
+    DiagT *d = find(handle);
+    if (!d || !d->have_frame || !d->inv[0]) {
+      msg = "get_invariants: unknown handle, no frame yet, or VELOCITY_INVARIANTS off";
+      return false;
+    }
+    CK(cudaStreamSynchronize(stream_));
+    for (int q = 0; q < 5; q++) CK(cudaMemcpy(out + (size_t)q * N_, d->inv[q], N_ * sizeof(lcsdata_t), cudaMemcpyDeviceToHost));
     return true;
   }
 
@@ -1013,6 +1029,48 @@ class Engine : public EngineBase {
     return true;
   }
 
+  // velocity snapshot of ring step `step` (write_flowmap_substep's u_np1 file, shared by
+  // every diagnostic; steps 0 .. kMaxVelocitySteps-1 kept)
+  static constexpr int kMaxVelocitySteps = 4096;
+  bool snapshot_velocity(long step, std::string &msg) {
+    if (step < 0 || step >= kMaxVelocitySteps) return true;
+    if (vring_.empty()) {
+      vring_.assign((size_t)3 * kMaxVelocitySteps, nullptr);
+      vwritten_.assign(kMaxVelocitySteps, 0);
+    }
+    if (!vring_[3 * step])
+      for (int c = 0; c < 3; c++)
+        if (!(vring_[3 * step + c] = arena_.alloc<TV>(N_, msg))) return false;
+    FieldPtrs<TV> u{};
+    FieldPtrsW<TV> dst{};
+    for (int c = 0; c < 3; c++) {
+      u.f[c] = u_[cur_][c];
+      dst.f[c] = vring_[3 * step + c];
+    }
+    k_vel_snapshot<T, TV><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, u, dst);
+    counters_.kernel_launches++;
+    CK(cudaGetLastError());
+    vwritten_[step] = 1;
+    return true;
+  }
+
+  bool launch_invariants(DiagT &d, long ustep, std::string &msg) {
+    if (!d.inv[0])
+      for (int q = 0; q < 5; q++)
+        if (!(d.inv[q] = arena_.alloc<lcsdata_t>(N_, msg))) return false;
+    const bool have = ustep >= 0 && ustep < (long)vwritten_.size() && vwritten_[ustep];
+    FieldPtrs<TV> u{};
+    for (int c = 0; c < 3; c++) u.f[c] = have ? vring_[3 * ustep + c] : nullptr;
+    FieldPtrsW<T> o3{}, o2{};
+    for (int q = 0; q < 3; q++) o3.f[q] = d.inv[q];
+    o2.f[0] = d.inv[3];
+    o2.f[1] = d.inv[4];
+    k_invariants<T, TV><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, u, have ? 1 : 0, o3, o2);
+    counters_.kernel_launches++;
+    CK(cudaGetLastError());
+    return true;
+  }
+
   void launch_reset(DiagT &d) {
     const dim3 blk(32, 8, 1), grd = node_grid();
     counters_.kernel_launches++;
@@ -1054,6 +1112,8 @@ class Engine : public EngineBase {
   DevReduce *red_ = nullptr, *red_host_ = nullptr;
   int red_err_ = 0;
   SplineSet<T> splines_[4];
+  std::vector<TV *> vring_;     // velocity snapshots by ring step (VELOCITY_INVARIANTS)
+  std::vector<char> vwritten_;
   SplineSet<TV> vsplines_[4];
   std::vector<DiagT> diags_;
   lcsdata_t t_n_ = 0, t_np1_ = 0;

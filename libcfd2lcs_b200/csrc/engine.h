@@ -57,6 +57,8 @@ class EngineBase {
   virtual bool get_ftle(int handle, lcsdata_t *out, std::string &msg) = 0;
   virtual bool get_flowmap(int handle, lcsdata_t *out, std::string &msg) = 0;
   virtual const lcsdata_t *ftle_device_ptr(int handle) = 0;
+  // velocity invariants of the last frame (VELOCITY_INVARIANTS): 5 x interior (Q, D, C, H, L2)
+  virtual bool get_invariants(int handle, lcsdata_t *out, std::string &msg) = 0;
   virtual bool sync_errors(std::string &msg) = 0;
   // Recomputes the latest FTLE frame of a diagnostic into caller-owned device buffers
   // without allocating (pointer table in a static device array, see engine.cu).

@@ -367,6 +367,135 @@ __global__ void __launch_bounds__(256) k_ftle(DevGrid<T> g, FieldPtrs<T> fm, R *
   ftle[interior_index(g.P.n, i, j, k)] = v;
 }
 
+// ---------------------------------------------------------------------------------------
+// Velocity invariants (compute_invariants, src/invariants_m.f90:15-208) of one frame from
+// the velocity snapshot of the reconstruction's starting step (nodal values, interior
+// arrays; null: no snapshot, the zeroed lp%ugrid of the reference).  Gradient by central
+// differences with face neighbours: periodic images, zero ghosts elsewhere (grad_sr1,
+// src/gradient_m.f90:11-66, after exchange_sdata of the never-bounded ugrid).  Outputs the
+// Q, D, C fields (out) and H, lambda-2 (out2) in the reference's expressions and order.
+// ---------------------------------------------------------------------------------------
+// all three eigenvalues (ascending) of a symmetric 3x3, cyclic Jacobi in FP64
+__device__ __forceinline__ void eig3_all(double a00, double a01, double a02, double a11, double a12, double a22, double w[3]) {
+  double a[3][3] = {{a00, a01, a02}, {a01, a11, a12}, {a02, a12, a22}};
+  for (int sweep = 0; sweep < 32; sweep++) {
+    const double off = fabs(a[0][1]) + fabs(a[0][2]) + fabs(a[1][2]);
+    const double diag = fabs(a[0][0]) + fabs(a[1][1]) + fabs(a[2][2]);
+    if (off == 0.0 || off <= 1e-18 * diag) break;
+#pragma unroll
+    for (int pq = 0; pq < 3; pq++) {
+      const int pp = pq == 2 ? 1 : 0, qq = pq == 0 ? 1 : 2;
+      const double apq = a[pp][qq];
+      if (apq == 0.0) continue;
+      const double theta = (a[qq][qq] - a[pp][pp]) / (2.0 * apq);
+      const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+      const double c = rsqrt(t * t + 1.0), s = t * c;
+#pragma unroll
+      for (int r = 0; r < 3; r++) {
+        const double arp = a[r][pp], arq = a[r][qq];
+        a[r][pp] = c * arp - s * arq;
+        a[r][qq] = s * arp + c * arq;
+      }
+#pragma unroll
+      for (int r = 0; r < 3; r++) {
+        const double apr = a[pp][r], aqr = a[qq][r];
+        a[pp][r] = c * apr - s * aqr;
+        a[qq][r] = s * apr + c * aqr;
+      }
+    }
+  }
+  double x = a[0][0], y = a[1][1], z = a[2][2], t;
+  if (y < x) { t = y; y = x; x = t; }
+  if (z < y) { t = z; z = y; y = t; }
+  if (y < x) { t = y; y = x; x = t; }
+  w[0] = x;
+  w[1] = y;
+  w[2] = z;
+}
+
+template <typename T, typename TU>
+__device__ __forceinline__ T ugrid_neighbour(const DevGrid<T> &g, const TU *__restrict__ f, int a, int i, int j, int k, int step) {
+  int idx[3] = {i, j, k};
+  idx[a] += step;
+  const int n = g.P.n[a];
+  if (idx[a] < 1 || idx[a] > n) {
+    if (!g.P.per[a]) return T(0);
+    idx[a] = idx[a] < 1 ? idx[a] + n : idx[a] - n;
+  }
+  return T(__ldg(f + interior_index(g.P.n, idx[0], idx[1], idx[2])));
+}
+
+template <typename T, typename TU>
+__global__ void __launch_bounds__(256) k_invariants(DevGrid<T> g, FieldPtrs<TU> u, int have, FieldPtrsW<T> out, FieldPtrsW<T> out2) {
+  int i, j, k;
+  if (!node_of_thread(g.P.n, i, j, k)) return;
+  T G[3][3];  // G[c][a] = d u_c / d x_a
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const int idx[3] = {i, j, k};
+    const T den = __ldg(g.lt[a] + idx[a] + 1) - __ldg(g.lt[a] + idx[a] - 1);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const T fp = have ? ugrid_neighbour<T, TU>(g, u.f[c], a, i, j, k, +1) : T(0);
+      const T fq = have ? ugrid_neighbour<T, TU>(g, u.f[c], a, i, j, k, -1) : T(0);
+      G[c][a] = g.P.n[a] == 1 ? T(0) : (fp - fq) / den;
+    }
+  }
+  const T d1u1 = G[0][0], d2u1 = G[0][1], d3u1 = G[0][2];
+  const T d1u2 = G[1][0], d2u2 = G[1][1], d3u2 = G[1][2];
+  const T d1u3 = G[2][0], d2u3 = G[2][1], d3u3 = G[2][2];
+  const T S11 = d1u1 + d1u1, S12 = d1u2 + d2u1, S13 = d1u3 + d3u1;
+  const T S21 = d2u1 + d1u2, S22 = d2u2 + d2u2, S23 = d2u3 + d3u2;
+  const T S31 = d3u1 + d1u3, S32 = d3u2 + d2u3, S33 = d3u3 + d3u3;
+  const T W11 = d1u1 - d1u1, W12 = d1u2 - d2u1, W13 = d1u3 - d3u1;
+  const T W21 = d2u1 - d1u2, W22 = d2u2 - d2u2, W23 = d2u3 - d3u2;
+  const T W31 = d3u1 - d1u3, W32 = d3u2 - d2u3, W33 = d3u3 - d3u3;
+  const T eigth = T(1. / 8.), twenyforth = T(1. / 24.), coef = T(27. / 4.);
+  T INV[5];
+  INV[0] = -eigth * (S11 * S11 + S12 * S21 + S13 * S31 + S21 * S12 + S22 * S22 + S23 * S32 + S31 * S13 + S32 * S23 + S33 * S33);
+  INV[1] = -twenyforth * (S11 * S11 * S11 + S11 * S12 * S21 + S11 * S13 * S31 + S21 * S11 * S12 + S21 * S12 * S22 + S21 * S13 * S32 +
+                          S31 * S11 * S13 + S31 * S12 * S23 + S31 * S13 * S33 + S12 * S21 * S11 + S12 * S22 * S21 + S12 * S23 * S31 +
+                          S13 * S31 * S11 + S13 * S32 * S21 + S13 * S33 * S31 + S22 * S22 * S22 + S22 * S21 * S12 + S22 * S23 * S32 +
+                          S23 * S31 * S13 + S23 * S32 * S22 + S23 * S33 * S32 + S32 * S22 * S23 + S32 * S21 * S13 + S32 * S23 * S33 +
+                          S33 * S33 * S33 + S33 * S23 * S32 + S33 * S13 * S31);
+  INV[2] = INV[0] - eigth * (W11 * W11 + W12 * W21 + W13 * W31 + W21 * W12 + W22 * W22 + W23 * W32 + W31 * W13 + W32 * W23 + W33 * W33);
+  INV[3] = INV[1] - eigth * (W11 * W11 * S11 + W11 * W12 * S21 + W11 * W13 * S31 + W21 * W11 * S12 + W21 * W12 * S22 + W21 * W13 * S32 +
+                             W31 * W11 * S13 + W31 * W12 * S23 + W31 * W13 * S33 + W12 * W21 * S11 + W12 * W22 * S21 + W12 * W23 * S31 +
+                             W13 * W31 * S11 + W13 * W32 * S21 + W13 * W33 * S31 + W22 * W22 * S22 + W22 * W21 * S12 + W22 * W23 * S32 +
+                             W23 * W31 * S13 + W23 * W32 * S22 + W23 * W33 * S32 + W32 * W22 * S23 + W32 * W21 * S13 + W32 * W23 * S33 +
+                             W33 * W33 * S33 + W33 * W23 * S32 + W33 * W13 * S31);
+  INV[4] = INV[2] - INV[0];
+  const int q = interior_index(g.P.n, i, j, k);
+  out.f[0][q] = INV[2] > T(0) ? T(1) : T(0);
+  const T D = INV[2] * INV[2] * INV[2] + coef * INV[3] * INV[3];
+  out.f[1][q] = (D > T(0) && INV[3] > T(0)) ? T(1) : (D > T(0) ? T(2) : (INV[3] > T(0) ? T(3) : T(4)));
+  out.f[2][q] = INV[1] > T(0) ? T(1) : T(0);
+  out2.f[0][q] = sqrt(-INV[4] / INV[0]);
+  // S^2 + Omega^2 (upper triangle, third diagonal entry 0 as the reference sets it), with
+  // rounded products so that no multiply-add contraction moves a middle eigenvalue that sits
+  // at zero (A(3,3) = 0 makes exact zeros common) across the sign test
+  auto dot6 = [](T a0, T b0, T a1, T b1, T a2, T b2, T a3, T b3, T a4, T b4, T a5, T b5) {
+    return mul_rn(a0, b0) + mul_rn(a1, b1) + mul_rn(a2, b2) + mul_rn(a3, b3) + mul_rn(a4, b4) + mul_rn(a5, b5);
+  };
+  double w[3];
+  eig3_all((double)dot6(S11, S11, S21, S12, S31, S13, W11, W11, W21, W12, W31, W13),
+           (double)dot6(S12, S11, S22, S12, S32, S13, W12, W11, W22, W12, W32, W13),
+           (double)dot6(S13, S11, S23, S12, S33, S13, W13, W11, W23, W12, W33, W13),
+           (double)dot6(S12, S21, S22, S22, S32, S23, W12, W21, W22, W22, W32, W23),
+           (double)dot6(S13, S21, S23, S22, S33, S23, W13, W21, W23, W22, W33, W23), 0.0, w);
+  out2.f[1][q] = w[1] < 0.0 ? T(1) : T(0);
+}
+
+// velocity snapshot of the ring: interior of the padded level, in the storage type
+template <typename T, typename TV>
+__global__ void __launch_bounds__(256) k_vel_snapshot(DevGrid<T> g, FieldPtrs<TV> u, FieldPtrsW<TV> dst) {
+  int i, j, k;
+  if (!node_of_thread(g.P.n, i, j, k)) return;
+  const int p = pidx(g.P.sx, g.P.sxy, i, j, k), q = interior_index(g.P.n, i, j, k);
+#pragma unroll
+  for (int c = 0; c < 3; c++) dst.f[c][q] = u.f[c][p];
+}
+
 // Reset of forward particles to their grid nodes (reset_lp, src/lp_m.f90:228-294), in node
 // order.
 template <typename T>

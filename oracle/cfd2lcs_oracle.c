@@ -67,6 +67,7 @@ static const int NBR[27][3] = {
     {1, -1, 1},  {-1, 0, 1},  {1, 0, 1},   {-1, 1, 1}, {0, 1, 1},  {1, 1, 1}};
 
 #define MAXLCS 64
+#define MAXVSTEP 4096
 #define MAXMSG 512
 
 /* ------------------------------------------------------------------------------------
@@ -115,6 +116,8 @@ typedef struct {
     real T, h;
     lp_t lp;
     real *ftle; /* padded sr0 */
+    real *inv[5]; /* velocity invariants Q, D, C, H, L2 of the last frame (padded sr0) */
+    real *l2margin; /* checker aid: middle eigenvalue / largest magnitude (how close L2 is to a tie) */
     sr1_t fm_out; /* composed flow map of the last FTLE frame (written by write_lcs) */
     int nslot;
     real **slot[3]; /* slot[c][s] -> interior values of stored sub-flow map */
@@ -138,6 +141,11 @@ static struct {
     long long integrations_fwd, integrations_bkwd;
     int last_nsub_fwd, last_nsub_bkwd;
     long long ftle_frames;
+    /* velocity snapshots by ring step (the cfd2lcs_tmp/<rank>_<u label>_<step> files of
+     * write_flowmap_substep, flowmap_m.f90:139-151): one set shared by every diagnostic,
+     * interior values; steps 0 .. NVSTEP-1 */
+    real *vring[3][MAXVSTEP];
+    int vwritten[MAXVSTEP];
 } S = {0, "", RK2, LINEAR, 0, 0, 0, (real)0.5, 0};
 
 static void latch(const char *m) {
@@ -1355,6 +1363,20 @@ static int ring_step(real t, real T, real h) {
 static void write_substep(lcs_t *L) {
     const dims_t *d = &S.g.d;
     int step = ring_step(S.t_np1, L->T, L->h);
+    /* velocity snapshot (VELOCITY_INVARIANTS; step nint(T/h) is kept too: the forward
+     * reconstruction reads step+1 before wrapping it) */
+    if (S.velocity_invariants && step >= 0 && step < MAXVSTEP) {
+        long nint_ = (long)d->ni * d->nj * d->nk;
+        for (int c = 0; c < 3; c++) {
+            if (!S.vring[c][step]) S.vring[c][step] = zalloc(nint_);
+            real *v = S.vring[c][step];
+            long q = 0;
+            for (int k = 1; k <= d->nk; k++)
+                for (int j = 1; j <= d->nj; j++)
+                    for (int i = 1; i <= d->ni; i++) v[q++] = S.u_np1.c[c][PX(d, i, j, k)];
+        }
+        S.vwritten[step] = 1;
+    }
     /* slot nint(T/h) (and negative slots) are written to files that reconstruct never
      * reads back (it wraps step into [0, nstep-1] before reading) */
     if (step < 0 || step >= L->nslot) return;
@@ -1533,6 +1555,135 @@ static void compute_ftle(lcs_t *L) {
             }
 }
 
+/* All three eigenvalues (ascending) of a symmetric 3x3, cyclic Jacobi in long double (the
+ * DSYEV + sort3 of compute_invariants, invariants_m.f90:178-197, 210-237). */
+static void eig3_all(const long double A_in[3][3], long double w[3]) {
+    long double a[3][3];
+    memcpy(a, A_in, sizeof(a));
+    for (int sweep = 0; sweep < 64; sweep++) {
+        long double off = fabsl(a[0][1]) + fabsl(a[0][2]) + fabsl(a[1][2]);
+        long double diag = fabsl(a[0][0]) + fabsl(a[1][1]) + fabsl(a[2][2]);
+        if (off == 0 || off <= 1e-30L * diag) break;
+        for (int p = 0; p < 2; p++)
+            for (int q = p + 1; q < 3; q++) {
+                if (a[p][q] == 0) continue;
+                long double theta = (a[q][q] - a[p][p]) / (2 * a[p][q]);
+                long double tt = (theta >= 0 ? 1 : -1) / (fabsl(theta) + sqrtl(theta * theta + 1));
+                long double c = 1 / sqrtl(tt * tt + 1), sn = tt * c;
+                for (int r = 0; r < 3; r++) {
+                    long double arp = a[r][p], arq = a[r][q];
+                    a[r][p] = c * arp - sn * arq;
+                    a[r][q] = sn * arp + c * arq;
+                }
+                for (int r = 0; r < 3; r++) {
+                    long double apr = a[p][r], aqr = a[q][r];
+                    a[p][r] = c * apr - sn * aqr;
+                    a[q][r] = sn * apr + c * aqr;
+                }
+            }
+    }
+    long double x = a[0][0], y = a[1][1], z = a[2][2], t;
+    if (y < x) { t = y; y = x; x = t; }
+    if (z < y) { t = z; z = y; y = t; }
+    if (y < x) { t = y; y = x; x = t; }
+    w[0] = x; w[1] = y; w[2] = z;
+}
+
+/* compute_invariants, invariants_m.f90:15-208: the velocity at the frame's starting ring
+ * step (reconstruct_flowmap reads it back and samples it at the grid nodes,
+ * flowmap_m.f90:214-245 -- the nodal values, which LINEAR and NEAREST reproduce exactly and
+ * the B-splines to rounding; a missing snapshot leaves the zeroed lp%ugrid), its central-
+ * difference gradient with face exchange (grad_sr1, gradient_m.f90:11-66: periodic images,
+ * zero ghosts elsewhere), and the Q, D, C, H and lambda-2 indicators. */
+static void compute_invariants(lcs_t *L, int ustep) {
+    const sgrid_t *g = &S.g;
+    const dims_t *d = &g->d;
+    sr1_t ug;
+    sr1_alloc(&ug, d);
+    if (ustep >= 0 && ustep < MAXVSTEP && S.vwritten[ustep]) {
+        for (int c = 0; c < 3; c++) {
+            const real *v = S.vring[c][ustep];
+            long q = 0;
+            for (int k = 1; k <= d->nk; k++)
+                for (int j = 1; j <= d->nj; j++)
+                    for (int i = 1; i <= d->ni; i++) ug.c[c][PX(d, i, j, k)] = v[q++];
+        }
+        exchange_self(g, ug.c, 3, 1, 0); /* scomm_max_r1: periodic images, no boundary values */
+    }
+    const real *X = g->grid.c[0], *Y = g->grid.c[1], *Z = g->grid.c[2];
+    const real eigth = (real)(1. / 8.), twenyforth = (real)(1. / 24.), coef = (real)(27. / 4.);
+    for (int k = 1; k <= d->nk; k++)
+        for (int j = 1; j <= d->nj; j++)
+            for (int i = 1; i <= d->ni; i++) {
+                long p = PX(d, i, j, k);
+                long pxp = PX(d, i + 1, j, k), pxm = PX(d, i - 1, j, k);
+                long pyp = PX(d, i, j + 1, k), pym = PX(d, i, j - 1, k);
+                long pzp = PX(d, i, j, k + 1), pzm = PX(d, i, j, k - 1);
+                real G[3][3]; /* G[c][a] = d u_c / d x_a */
+                for (int c = 0; c < 3; c++) {
+                    const real *F = ug.c[c];
+                    G[c][0] = (F[pxp] - F[pxm]) / (X[pxp] - X[pxm]);
+                    G[c][1] = (F[pyp] - F[pym]) / (Y[pyp] - Y[pym]);
+                    G[c][2] = (F[pzp] - F[pzm]) / (Z[pzp] - Z[pzm]);
+                }
+                for (int a = 0; a < 3; a++)
+                    if (g->gn[a] == 1)
+                        for (int c = 0; c < 3; c++) G[c][a] = 0;
+                const real d1u1 = G[0][0], d2u1 = G[0][1], d3u1 = G[0][2];
+                const real d1u2 = G[1][0], d2u2 = G[1][1], d3u2 = G[1][2];
+                const real d1u3 = G[2][0], d2u3 = G[2][1], d3u3 = G[2][2];
+                const real S11 = d1u1 + d1u1, S12 = d1u2 + d2u1, S13 = d1u3 + d3u1;
+                const real S21 = d2u1 + d1u2, S22 = d2u2 + d2u2, S23 = d2u3 + d3u2;
+                const real S31 = d3u1 + d1u3, S32 = d3u2 + d2u3, S33 = d3u3 + d3u3;
+                const real W11 = d1u1 - d1u1, W12 = d1u2 - d2u1, W13 = d1u3 - d3u1;
+                const real W21 = d2u1 - d1u2, W22 = d2u2 - d2u2, W23 = d2u3 - d3u2;
+                const real W31 = d3u1 - d1u3, W32 = d3u2 - d2u3, W33 = d3u3 - d3u3;
+                real INV[5];
+                INV[0] = -eigth * (S11 * S11 + S12 * S21 + S13 * S31 + S21 * S12 + S22 * S22 + S23 * S32 + S31 * S13 + S32 * S23 +
+                                   S33 * S33);
+                INV[1] = -twenyforth *
+                         (S11 * S11 * S11 + S11 * S12 * S21 + S11 * S13 * S31 + S21 * S11 * S12 + S21 * S12 * S22 + S21 * S13 * S32 +
+                          S31 * S11 * S13 + S31 * S12 * S23 + S31 * S13 * S33 + S12 * S21 * S11 + S12 * S22 * S21 + S12 * S23 * S31 +
+                          S13 * S31 * S11 + S13 * S32 * S21 + S13 * S33 * S31 + S22 * S22 * S22 + S22 * S21 * S12 + S22 * S23 * S32 +
+                          S23 * S31 * S13 + S23 * S32 * S22 + S23 * S33 * S32 + S32 * S22 * S23 + S32 * S21 * S13 + S32 * S23 * S33 +
+                          S33 * S33 * S33 + S33 * S23 * S32 + S33 * S13 * S31);
+                INV[2] = INV[0] - eigth * (W11 * W11 + W12 * W21 + W13 * W31 + W21 * W12 + W22 * W22 + W23 * W32 + W31 * W13 +
+                                           W32 * W23 + W33 * W33);
+                INV[3] = INV[1] - eigth * (W11 * W11 * S11 + W11 * W12 * S21 + W11 * W13 * S31 + W21 * W11 * S12 + W21 * W12 * S22 +
+                                           W21 * W13 * S32 + W31 * W11 * S13 + W31 * W12 * S23 + W31 * W13 * S33 + W12 * W21 * S11 +
+                                           W12 * W22 * S21 + W12 * W23 * S31 + W13 * W31 * S11 + W13 * W32 * S21 + W13 * W33 * S31 +
+                                           W22 * W22 * S22 + W22 * W21 * S12 + W22 * W23 * S32 + W23 * W31 * S13 + W23 * W32 * S22 +
+                                           W23 * W33 * S32 + W32 * W22 * S23 + W32 * W21 * S13 + W32 * W23 * S33 + W33 * W33 * S33 +
+                                           W33 * W23 * S32 + W33 * W13 * S31);
+                INV[4] = INV[2] - INV[0];
+                L->inv[0][p] = INV[2] > 0 ? (real)1 : (real)0;
+                const real D = INV[2] * INV[2] * INV[2] + coef * INV[3] * INV[3];
+                if (D > 0 && INV[3] > 0) L->inv[1][p] = 1;
+                else if (D > 0 && INV[3] <= 0) L->inv[1][p] = 2;
+                else if (D <= 0 && INV[3] > 0) L->inv[1][p] = 3;
+                else L->inv[1][p] = 4;
+                L->inv[2][p] = INV[1] > 0 ? (real)1 : (real)0;
+                L->inv[3][p] = (real)sqrt((double)(-INV[4] / INV[0]));
+                /* S^2 + Omega^2, upper triangle (DSYEV 'U') */
+                long double A[3][3];
+                A[0][0] = S11 * S11 + S21 * S12 + S31 * S13 + W11 * W11 + W21 * W12 + W31 * W13;
+                A[0][1] = S12 * S11 + S22 * S12 + S32 * S13 + W12 * W11 + W22 * W12 + W32 * W13;
+                A[0][2] = S13 * S11 + S23 * S12 + S33 * S13 + W13 * W11 + W23 * W12 + W33 * W13;
+                A[1][1] = S12 * S21 + S22 * S22 + S32 * S23 + W12 * W21 + W22 * W22 + W32 * W23;
+                A[1][2] = S13 * S21 + S23 * S22 + S33 * S23 + W13 * W21 + W23 * W22 + W33 * W23;
+                A[2][2] = 0;
+                A[1][0] = A[0][1];
+                A[2][0] = A[0][2];
+                A[2][1] = A[1][2];
+                long double w[3];
+                eig3_all(A, w);
+                L->inv[4][p] = w[1] < 0 ? (real)1 : (real)0;
+                long double big = fabsl(w[0]) > fabsl(w[2]) ? fabsl(w[0]) : fabsl(w[2]);
+                L->l2margin[p] = big > 0 ? (real)(w[1] / big) : (real)0;
+            }
+    sr1_free(&ug);
+}
+
 /* ------------------------------------------------------------------------------------
  * Entry points (cfd2lcs.f90:2-682 semantics, one rank, no output files).
  * ------------------------------------------------------------------------------------ */
@@ -1567,6 +1718,8 @@ static void free_lcs(lcs_t *L) {
         }
     }
     free(L->lp.flag);
+    for (int q = 0; q < 5; q++) free(L->inv[q]);
+    free(L->l2margin);
     sr1_free(&L->lp.fm);
     sr1_free(&L->fm_out);
     free(L->ftle);
@@ -1577,6 +1730,8 @@ static void free_lcs(lcs_t *L) {
 /* Resets all state, including the error latch (a fresh process for the reference). */
 EXPORT void orc_reset(void) {
     for (int i = 0; i < S.nlcs; i++) free_lcs(S.lcs[i]);
+    for (int c = 0; c < 3; c++)
+        for (int q = 0; q < MAXVSTEP; q++) free(S.vring[c][q]);
     if (S.inited) {
         sr1_free(&S.g.grid); sr1_free(&S.g.bcnorm); free(S.g.bcflag);
         sr1_free(&S.u_n); sr1_free(&S.u_np1); sr1_free(&S.delta);
@@ -1624,6 +1779,8 @@ EXPORT int orc_diagnostic_init(int type, int resolution, real T, real h, const c
     L->h = h;
     const dims_t *d = &S.g.d;
     L->ftle = zalloc(d->ntot);
+    for (int q = 0; q < 5; q++) L->inv[q] = zalloc(d->ntot);
+    L->l2margin = zalloc(d->ntot);
     lp_alloc(&L->lp, d->ni * d->nj * d->nk);
     sr1_alloc(&L->lp.fm, d);
     sr1_alloc(&L->fm_out, d);
@@ -1687,8 +1844,12 @@ EXPORT void orc_update(const int n[3], const real *u, const real *v, const real 
                         for (int c = 0; c < 3; c++) L->lp.fm.c[c][PX(d, ii, j, k)] = L->lp.dx[c][ip];
         }
         write_substep(L);
+        /* the starting step of the reconstruction: the current one (backward) or the next,
+         * not yet wrapped (forward), flowmap_m.f90:202-209 */
+        const int ustep = ring_step(S.t_np1, L->T, L->h) + (L->diagnostic == FTLE_FWD ? 1 : 0);
         reconstruct(L);
         compute_ftle(L);
+        if (S.velocity_invariants) compute_invariants(L, ustep);
         for (int c = 0; c < 3; c++) memcpy(L->fm_out.c[c], L->lp.fm.c[c], sizeof(real) * (size_t)d->ntot);
         S.ftle_frames++;
         reset_lp(&S.g, &L->lp, 1);
@@ -1841,5 +2002,31 @@ EXPORT int orc_bspline3_coef(const real *xg, const real *yg, const real *zg, int
     bsp3_fit(&s, f);
     memcpy(coef, s.coef, sizeof(real) * (size_t)(nx * ny * nz));
     bsp3_free(&s);
+    return 0;
+}
+
+/* Velocity invariants of a diagnostic's last frame: 5 x interior (Q, D, C, H, L2). */
+EXPORT int orc_get_invariants(int handle, real *out) {
+    lcs_t *L = find_lcs(handle);
+    if (!L) return 1;
+    const dims_t *d = &S.g.d;
+    long q = 0;
+    for (int v = 0; v < 5; v++)
+        for (int k = 1; k <= d->nk; k++)
+            for (int j = 1; j <= d->nj; j++)
+                for (int i = 1; i <= d->ni; i++) out[q++] = L->inv[v][PX(d, i, j, k)];
+    return 0;
+}
+
+/* Checker aid, no reference counterpart: the lambda-2 tie margin of the last frame, so that
+ * a test can tell a rounding tie (|margin| at rounding level) from a real disagreement. */
+EXPORT int orc_get_l2margin(int handle, real *out) {
+    lcs_t *L = find_lcs(handle);
+    if (!L) return 1;
+    const dims_t *d = &S.g.d;
+    long q = 0;
+    for (int k = 1; k <= d->nk; k++)
+        for (int j = 1; j <= d->nj; j++)
+            for (int i = 1; i <= d->ni; i++) out[q++] = L->l2margin[PX(d, i, j, k)];
     return 0;
 }

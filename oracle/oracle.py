@@ -53,6 +53,10 @@ class Oracle:
         L.orc_get_ftle.restype = C.c_int
         L.orc_get_fm.argtypes = [C.c_int, P, C.c_int]
         L.orc_get_fm.restype = C.c_int
+        L.orc_get_invariants.argtypes = [C.c_int, P]
+        L.orc_get_invariants.restype = C.c_int
+        L.orc_get_l2margin.argtypes = [C.c_int, P]
+        L.orc_get_l2margin.restype = C.c_int
         L.orc_get_particles.argtypes = [C.c_int, P]
         L.orc_get_particles.restype = C.c_int
         L.orc_counter.argtypes = [C.c_int]
@@ -125,6 +129,18 @@ class Oracle:
         out = np.zeros(3 * int(np.prod(self.n)), dtype=self.dtype)
         assert self.lib.orc_get_fm(handle, self._p(out), int(composed)) == 0
         return out.reshape((3,) + tuple(self.n[::-1])).transpose(0, 3, 2, 1)
+
+    def invariants(self, handle):
+        """Q, D, C, H, L2 of the last frame (compute_invariants), shape (5, ni, nj, nk)."""
+        out = np.zeros(5 * int(np.prod(self.n)), dtype=self.dtype)
+        assert self.lib.orc_get_invariants(handle, self._p(out)) == 0
+        return out.reshape((5,) + tuple(self.n[::-1])).transpose(0, 3, 2, 1)
+
+    def l2margin(self, handle):
+        """Middle eigenvalue of the lambda-2 tensor over its largest magnitude, last frame."""
+        out = np.zeros(int(np.prod(self.n)), dtype=self.dtype)
+        assert self.lib.orc_get_l2margin(handle, self._p(out)) == 0
+        return out.reshape(tuple(self.n[::-1])).transpose(2, 1, 0)
 
     def particles(self, handle):
         out = np.zeros(3 * int(np.prod(self.n)), dtype=self.dtype)
