@@ -543,7 +543,7 @@ def run_batch(args):
         torch.distributed.destroy_process_group()
 
 
-FD_EPS = 1e-7  # central-difference step of the adjoint check (velocity units)
+FD_EPS = 1e-6  # central-difference step of the adjoint check (velocity units)
 
 ADJ_DESC = ("adjoint: J = mean backward FTLE over [pi/2,3pi/2]^3 of ABC flow on a 128^3 grid, 201 velocity levels "
             "(steady ABC + N(0, 0.01^2) noise from torch's CUDA generator, seed 7), 200 updates at dt=0.05, RK2, linear, "
@@ -595,7 +595,7 @@ def run_adjoint(args):
     den = sum(float(torch.sum(b ** 2)) for B in (gu, gv, gw) for b in B)
     rel32 = math.sqrt(num / den) if den > 0 else None
     nfd = args.fd_dirs
-    fd_err, fd_refined = [], []
+    fd_err, fd_abs, fd_ad, fd_refined, tl_err = [], [], [], [], []
     gen = torch.Generator(device="cuda")
     gen.manual_seed(16)
 
@@ -609,17 +609,23 @@ def run_adjoint(args):
     for q in range(nfd):
         d = [[torch.randn(lev64[c][k].numel(), generator=gen, device="cuda", dtype=torch.float64) for k in range(nl)] for c in range(3)]
         ad = sum(float(torch.dot(G[k], d[c][k])) for c, G in enumerate((gu, gv, gw)) for k in range(nl))
+        _, tl = L.tangent_ftle(g, *lev64, times, w64, *d, precision="dp")
+        tl_err.append(abs(tl - ad) / max(abs(tl), abs(ad), 1e-300))
         fd = central(d, FD_EPS)
+        fd_ad.append(ad)
+        fd_abs.append(abs(fd - ad))
         err = abs(fd - ad) / max(abs(fd), abs(ad), 1e-300)
         fd_err.append(err)
         if err > 1e-3:
-            # a trilinear stencil edge (a kink of the piecewise-smooth objective) inside
-            # [-eps, eps]: the central difference converges to the adjoint as eps shrinks
+            # a direction whose directional derivative is small: the objective's FP64
+            # rounding noise over 2 eps (grows as eps shrinks) and stencil-edge kinks inside
+            # [-eps, eps] (grow with eps) are both visible; the sweep shows which
             ref = [{"eps": FD_EPS, "rel_err": err, "fd": fd}]
-            for e in (FD_EPS / 10, FD_EPS / 100):
+            for e in (FD_EPS * 10, FD_EPS / 10):
                 f = central(d, e)
                 ref.append({"eps": e, "rel_err": abs(f - ad) / max(abs(f), abs(ad), 1e-300), "fd": f})
             fd_refined.append({"direction": q, "adjoint": ad, "steps": ref})
+    rms_ad = math.sqrt(sum(a * a for a in fd_ad) / len(fd_ad)) if fd_ad else 0.0
     # work: grid points x subcycles of the forward map, run twice (forward + segment recompute)
     api = L.Cfd2lcs("sp")
     api.reset()
@@ -638,12 +644,17 @@ def run_adjoint(args):
                                             "value_counts": "grid points x subcycles of the forward map per gradient"},
             "gradient_s": el, "J_fp32": J32, "J_fp64": J64,
             "gradient_fp32_vs_fp64_rel_l2": rel32,
+            "tangent_linear_check": {"directions": nfd, "form": "FP64 forward-mode sweep vs FP64 adjoint, same directions",
+                                     "max_rel_err": max(tl_err) if tl_err else None, "rel_errs": tl_err},
             "finite_difference_check": {"directions": nfd, "eps": FD_EPS, "form": "FP64 objective, central differences",
                                         "max_rel_err": max(fd_err) if fd_err else None,
                                         "median_rel_err": float(np.median(fd_err)) if fd_err else None, "rel_errs": fd_err,
-                                        "outliers_refined": fd_refined,
-                                        "note": "the objective is only piecewise smooth (trilinear interpolation, clamped "
-                                                "weights): central differences carry kink and rounding noise"}}
+                                        "max_abs_err_over_rms_derivative": max(fd_abs) / rms_ad if fd_abs and rms_ad > 0 else None,
+                                        "adjoint_directional": fd_ad, "outliers_refined": fd_refined,
+                                        "note": "relative errors above 1e-3 come from directions whose derivative is near zero "
+                                                "(random cancellation); there the objective's FP64 rounding noise over 2 eps "
+                                                "and trilinear stencil-edge kinks dominate, so the error is also given over "
+                                                "the RMS directional derivative"}}
     print(json.dumps(line), flush=True)
 
 

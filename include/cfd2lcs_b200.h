@@ -141,6 +141,18 @@ int cfd2lcs_adjoint_ftle_c(const int n[3], const lcsdata_t *x, const lcsdata_t *
                            const lcsdata_t *const *d_w, const lcsdata_t *times, const lcsdata_t *d_weight, int checkpoint_every,
                            double *J, lcsdata_t *const *d_gu, lcsdata_t *const *d_gv, lcsdata_t *const *d_gw, char *msg, size_t len);
 
+/* Tangent-linear model of the same objective (the forward-mode check of the adjoint): writes *J
+ * and *dJ = sum over levels of <dJ/du, d> for one direction d (d_du[l], d_dv[l], d_dw[l]:
+ * device arrays of level l, n[0]*n[1]*n[2], i fastest), propagating the flow map's first-order
+ * change alongside the flow map with the same held-fixed discrete choices as the adjoint, so
+ * that the two agree to rounding.  Same grid scope and arguments as cfd2lcs_adjoint_ftle_c.
+ * Returns 0, or 1 with the reason in msg. */
+int cfd2lcs_tangent_ftle_c(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, int integrator,
+                           lcsdata_t cfl, int nlevels, const lcsdata_t *const *d_u, const lcsdata_t *const *d_v,
+                           const lcsdata_t *const *d_w, const lcsdata_t *times, const lcsdata_t *d_weight,
+                           const lcsdata_t *const *d_du, const lcsdata_t *const *d_dv, const lcsdata_t *const *d_dw, double *J,
+                           double *dJ, char *msg, size_t len);
+
 #ifdef __cplusplus
 }
 #endif

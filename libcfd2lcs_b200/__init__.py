@@ -43,7 +43,7 @@ EXPORTED_SYMBOLS = [
     "cfd2lcs_batch_get_flowmap_c", "cfd2lcs_batch_get_counters_c", "cfd2lcs_batch_size_c", "cfd2lcs_batch_error_c",
     "cfd2lcs_batch_reset_c",
     # adjoint (include/cfd2lcs_b200.h)
-    "cfd2lcs_adjoint_ftle_c",
+    "cfd2lcs_adjoint_ftle_c", "cfd2lcs_tangent_ftle_c",
 ]
 
 
@@ -118,6 +118,8 @@ def load(precision: str = "dp") -> C.CDLL:
     lib.cfd2lcs_batch_reset_c.restype = None
     lib.cfd2lcs_adjoint_ftle_c.argtypes = [P, P, P, P, C.c_int, R, C.c_int, P, P, P, P, P, C.c_int, P, P, P, P, C.c_char_p, C.c_size_t]
     lib.cfd2lcs_adjoint_ftle_c.restype = C.c_int
+    lib.cfd2lcs_tangent_ftle_c.argtypes = [P, P, P, P, C.c_int, R, C.c_int, P, P, P, P, P, P, P, P, P, P, C.c_char_p, C.c_size_t]
+    lib.cfd2lcs_tangent_ftle_c.restype = C.c_int
     _LIBS[precision] = lib
     return lib
 
@@ -361,3 +363,25 @@ def adjoint_ftle(grid, u, v, w, times, weight, integrator=2, cfl=0.5, checkpoint
     if g:
         return J.value, g[0], g[1], g[2]
     return J.value, None, None, None
+
+
+def tangent_ftle(grid, u, v, w, times, weight, du, dv, dw, integrator=2, cfl=0.5, precision="dp"):
+    """J and dJ = <dJ/du, d> of the adjoint's objective for one direction d = (du, dv, dw) (lists of
+    CUDA tensors, one per level, like u, v, w), by the tangent-linear sweep
+    (cfd2lcs_tangent_ftle_c).  Returns (J, dJ)."""
+    lib = load(precision)
+    dt = np.float64 if precision == "dp" else np.float32
+    R = C.c_double if precision == "dp" else C.c_float
+    L = len(u)
+    n = np.ascontiguousarray(grid.n, dtype=np.int32)
+    xs, ys, zs = (np.asfortranarray(a, dtype=dt).ravel(order="F") for a in (grid.x, grid.y, grid.z))
+    ptrs = lambda ts: C.cast((C.c_void_p * L)(*[t.data_ptr() for t in ts]), C.c_void_p)
+    tm = np.ascontiguousarray(times, dtype=dt)
+    J, dJ = C.c_double(0.0), C.c_double(0.0)
+    msg = C.create_string_buffer(512)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    rc = lib.cfd2lcs_tangent_ftle_c(p(n), p(xs), p(ys), p(zs), int(integrator), R(cfl), L, ptrs(u), ptrs(v), ptrs(w), p(tm),
+                                    C.c_void_p(weight.data_ptr()), ptrs(du), ptrs(dv), ptrs(dw), C.byref(J), C.byref(dJ), msg, 512)
+    if rc:
+        raise RuntimeError(msg.value.decode(errors="replace"))
+    return J.value, dJ.value

@@ -217,6 +217,86 @@ __global__ void __launch_bounds__(256) k_distribute(FieldPtrsW<T> a1, FieldPtrsW
   a2.f[c][q] = T(0);
 }
 
+
+// ---------------------------------------------------------------------------------------
+// Tangent-linear form of one backward SL subcycle: with the velocity levels perturbed along
+// D (dun, dunp1) and the previous map along dfo, the first-order change of the new map at the
+// interior nodes (ghosts by k_periodic_ghosts).  Same recomputed stages, brackets and clamped
+// fractions as the forward kernel and k_sl_adjoint, so that for every direction d the
+// tangent's dJ equals the adjoint's <dJ/du, d> to rounding.
+// ---------------------------------------------------------------------------------------
+template <typename T, int INTEG>
+__global__ void __launch_bounds__(256) k_sl_tangent(DevGrid<T> g, VelFields<T> V, VelFields<T> D, FieldPtrs<T> fmo, FieldPtrs<T> dfo,
+                                                     FieldPtrsW<T> dfn, StageTimes S, T dt) {
+  int i, j, k;
+  if (!node_of_thread(g.P.n, i, j, k)) return;
+  const int p = pidx(g.P.sx, g.P.sxy, i, j, k);
+  const T HALF = T(1) / T(2);
+  const int no[3] = {i, j, k};
+  const T x0[3] = {__ldg(g.lt[0] + i), __ldg(g.lt[1] + j), __ldg(g.lt[2] + k)};
+  const T ct0 = T(S.ct[0]), omc0 = T(1) - ct0;
+  T u1[3], du1[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    u1[c] = omc0 * __ldg(V.un[c] + p) + ct0 * __ldg(V.unp1[c] + p);
+    du1[c] = omc0 * __ldg(D.un[c] + p) + ct0 * __ldg(D.unp1[c] + p);
+  }
+  T x[3], dx[3];
+  if (INTEG == RK2) {
+    const T ct1 = T(S.ct[1]), omc1 = T(1) - ct1;
+    T xh[3], dxh[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      xh[c] = x0[c] + HALF * dt * u1[c];
+      dxh[c] = HALF * dt * du1[c];
+    }
+    LinStencilAD<T> s2;
+    lin_stencil_ad(g, xh, no, s2);
+    T u2[3], du2[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      u2[c] = lin_apply_blend<T, T>(s2.st, V.un[c], V.unp1[c], omc1, ct1);
+      du2[c] = lin_apply_blend<T, T>(s2.st, D.un[c], D.unp1[c], omc1, ct1);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int cq = corner(s2.st, q);
+      T dwq = T(0);
+#pragma unroll
+      for (int d = 0; d < 3; d++) dwq += dweight(s2.t, q, d) * s2.dtdx[d] * dxh[d];
+#pragma unroll
+      for (int c = 0; c < 3; c++) du2[c] += dwq * (omc1 * __ldg(V.un[c] + cq) + ct1 * __ldg(V.unp1[c] + cq));
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      x[c] = x0[c] + dt * u2[c];
+      dx[c] = dt * du2[c];
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      x[c] = x0[c] + dt * u1[c];
+      dx[c] = dt * du1[c];
+    }
+  }
+  LinStencilAD<T> s3;
+  lin_stencil_ad(g, x, no, s3);
+  // fm_new = fm_old(x) + (x - x0)
+  T out[3] = {dx[0], dx[1], dx[2]};
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    const int cq = corner(s3.st, q);
+    const T wq = s3.st.w[q];
+    T dwq = T(0);
+#pragma unroll
+    for (int d = 0; d < 3; d++) dwq += dweight(s3.t, q, d) * s3.dtdx[d] * dx[d];
+#pragma unroll
+    for (int c = 0; c < 3; c++) out[c] += wq * __ldg(dfo.f[c] + cq) + dwq * __ldg(fmo.f[c] + cq);
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) dfn.f[c][p] = out[c];
+}
+
 // source interior index of a padded cell along one periodic axis
 __device__ __forceinline__ int wrap_index(int v, int n) { return v < 1 ? v + n : (v > n ? v - n : v); }
 
@@ -238,6 +318,20 @@ __global__ void __launch_bounds__(256) k_fold_ghosts(DevGrid<T> g, FieldPtrsW<T>
   }
 }
 
+// periodic ghost fill of a tangent map (write_ghosts rule 0 on every face, edge and corner;
+// the transpose of k_fold_ghosts)
+template <typename T>
+__global__ void __launch_bounds__(256) k_periodic_ghosts(DevGrid<T> g, FieldPtrsW<T> f, long ntot) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= ntot) return;
+  const int i = (int)(p % g.P.sx), j = (int)((p / g.P.sx) % (g.P.sxy / g.P.sx)), k = (int)(p / g.P.sxy);
+  const int si = wrap_index(i, g.P.n[0]), sj = wrap_index(j, g.P.n[1]), sk = wrap_index(k, g.P.n[2]);
+  if (si == i && sj == j && sk == k) return;
+  const int q = pidx(g.P.sx, g.P.sxy, si, sj, sk);
+#pragma unroll
+  for (int c = 0; c < 3; c++) f.f[c][p] = f.f[c][q];
+}
+
 // interior of a padded field -> compact i-fastest arrays (the composed map of an h = T frame)
 template <typename T>
 __global__ void __launch_bounds__(256) k_interior(DevGrid<T> g, FieldPtrs<T> src, FieldPtrsW<T> dst) {
@@ -246,6 +340,64 @@ __global__ void __launch_bounds__(256) k_interior(DevGrid<T> g, FieldPtrs<T> src
   const int p = pidx(g.P.sx, g.P.sxy, i, j, k), q = interior_index(g.P.n, i, j, k);
 #pragma unroll
   for (int c = 0; c < 3; c++) dst.f[c][q] = src.f[c][p];
+}
+
+// The FTLE at node (i, j, k) linearised in the flow map: the central-difference gradient G,
+// the neighbours and spacings it used, the largest eigenvalue lam of G^T G and its unit
+// eigenvector v.  False where the derivative is zero (FTLE at its tiny floor) or undefined
+// (repeated largest eigenvalue).
+template <typename T>
+struct FtleLin {
+  double G[3][3], den[3], v[3], Gv[3], lam;
+  int qp[3], qm[3];
+};
+
+template <typename T>
+__device__ __forceinline__ bool ftle_linearise(const DevGrid<T> &g, const FieldPtrs<T> &fm, int i, int j, int k, FtleLin<T> &L) {
+  const int idx[3] = {i, j, k};
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    if (g.P.n[a] == 1) {
+      for (int c = 0; c < 3; c++) L.G[c][a] = 0.0;
+      L.den[a] = 0.0;
+      L.qp[a] = L.qm[a] = -1;
+      continue;
+    }
+    int ip[3] = {i, j, k}, im[3] = {i, j, k};
+    ip[a] = wrap_index(idx[a] + 1, g.P.n[a]);
+    im[a] = wrap_index(idx[a] - 1, g.P.n[a]);
+    L.qp[a] = pidx(g.P.sx, g.P.sxy, ip[0], ip[1], ip[2]);
+    L.qm[a] = pidx(g.P.sx, g.P.sxy, im[0], im[1], im[2]);
+    L.den[a] = (double)(__ldg(g.lt[a] + idx[a] + 1) - __ldg(g.lt[a] + idx[a] - 1));
+    for (int c = 0; c < 3; c++) L.G[c][a] = (double)(fm.f[c][L.qp[a]] - fm.f[c][L.qm[a]]) / L.den[a];
+  }
+  double C[3][3];
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++) C[a][b] = L.G[0][a] * L.G[0][b] + L.G[1][a] * L.G[1][b] + L.G[2][a] * L.G[2][b];
+  const double lam = eig3_max(C[0][0], C[0][1], C[0][2], C[1][1], C[1][2], C[2][2]);
+  const double tiny = sizeof(T) == 8 ? DBL_MIN : (double)FLT_MIN;
+  if (!(sqrt(lam) > tiny)) return false;  // max(sqrt(W3), tiny) is constant there
+  // unit eigenvector of lam: the largest cross product of two rows of C - lam I
+  const double r[3][3] = {{C[0][0] - lam, C[0][1], C[0][2]}, {C[1][0], C[1][1] - lam, C[1][2]}, {C[2][0], C[2][1], C[2][2] - lam}};
+  double best = 0.0;
+  L.v[0] = L.v[1] = L.v[2] = 0.0;
+  for (int m = 0; m < 3; m++) {
+    const double *x = r[m], *y = r[(m + 1) % 3];
+    const double cx[3] = {x[1] * y[2] - x[2] * y[1], x[2] * y[0] - x[0] * y[2], x[0] * y[1] - x[1] * y[0]};
+    const double nn = cx[0] * cx[0] + cx[1] * cx[1] + cx[2] * cx[2];
+    if (nn > best) {
+      best = nn;
+      L.v[0] = cx[0];
+      L.v[1] = cx[1];
+      L.v[2] = cx[2];
+    }
+  }
+  if (!(best > 0.0)) return false;  // repeated largest eigenvalue: no unique derivative direction
+  const double s = 1.0 / sqrt(best);
+  for (int a = 0; a < 3; a++) L.v[a] *= s;
+  for (int c = 0; c < 3; c++) L.Gv[c] = L.G[c][0] * L.v[0] + L.G[c][1] * L.v[1] + L.G[c][2] * L.v[2];
+  L.lam = lam;
+  return true;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -260,62 +412,41 @@ __global__ void __launch_bounds__(256) k_ftle_adjoint(DevGrid<T> g, FieldPtrs<T>
   if (!node_of_thread(g.P.n, i, j, k)) return;
   const double w = (double)wgt[interior_index(g.P.n, i, j, k)];
   if (w == 0.0) return;
-  const int idx[3] = {i, j, k};
-  double G[3][3], den[3];
-  int qp[3], qm[3];
-#pragma unroll
-  for (int a = 0; a < 3; a++) {
-    if (g.P.n[a] == 1) {
-      for (int c = 0; c < 3; c++) G[c][a] = 0.0;
-      den[a] = 0.0;
-      qp[a] = qm[a] = -1;
-      continue;
-    }
-    int ip[3] = {i, j, k}, im[3] = {i, j, k};
-    ip[a] = wrap_index(idx[a] + 1, g.P.n[a]);
-    im[a] = wrap_index(idx[a] - 1, g.P.n[a]);
-    qp[a] = pidx(g.P.sx, g.P.sxy, ip[0], ip[1], ip[2]);
-    qm[a] = pidx(g.P.sx, g.P.sxy, im[0], im[1], im[2]);
-    den[a] = (double)(__ldg(g.lt[a] + idx[a] + 1) - __ldg(g.lt[a] + idx[a] - 1));
-    for (int c = 0; c < 3; c++) G[c][a] = (double)(fm.f[c][qp[a]] - fm.f[c][qm[a]]) / den[a];
-  }
-  double C[3][3];
-  for (int a = 0; a < 3; a++)
-    for (int b = 0; b < 3; b++) C[a][b] = G[0][a] * G[0][b] + G[1][a] * G[1][b] + G[2][a] * G[2][b];
-  const double lam = eig3_max(C[0][0], C[0][1], C[0][2], C[1][1], C[1][2], C[2][2]);
-  const double tiny = sizeof(T) == 8 ? DBL_MIN : (double)FLT_MIN;
-  if (!(sqrt(lam) > tiny)) return;  // max(sqrt(W3), tiny) is constant there
-  // unit eigenvector of lam: the largest cross product of two rows of C - lam I
-  const double r[3][3] = {{C[0][0] - lam, C[0][1], C[0][2]}, {C[1][0], C[1][1] - lam, C[1][2]}, {C[2][0], C[2][1], C[2][2] - lam}};
-  double v[3] = {0, 0, 0}, best = 0.0;
-  for (int m = 0; m < 3; m++) {
-    const double *x = r[m], *y = r[(m + 1) % 3];
-    const double cx[3] = {x[1] * y[2] - x[2] * y[1], x[2] * y[0] - x[0] * y[2], x[0] * y[1] - x[1] * y[0]};
-    const double nn = cx[0] * cx[0] + cx[1] * cx[1] + cx[2] * cx[2];
-    if (nn > best) {
-      best = nn;
-      v[0] = cx[0];
-      v[1] = cx[1];
-      v[2] = cx[2];
-    }
-  }
-  if (!(best > 0.0)) return;  // repeated largest eigenvalue: no unique derivative direction
-  const double s = 1.0 / sqrt(best);
-  v[0] *= s;
-  v[1] *= s;
-  v[2] *= s;
-  const double Gv[3] = {G[0][0] * v[0] + G[0][1] * v[1] + G[0][2] * v[2], G[1][0] * v[0] + G[1][1] * v[1] + G[1][2] * v[2],
-                        G[2][0] * v[0] + G[2][1] * v[1] + G[2][2] * v[2]};
+  FtleLin<T> L;
+  if (!ftle_linearise(g, fm, i, j, k, L)) return;
   // dJ/dG = w / (2 lam T) * 2 (G v) v^T
-  const double coef = w / (lam * (double)Tint);
+  const double coef = w / (L.lam * (double)Tint);
   for (int a = 0; a < 3; a++) {
-    if (qp[a] < 0) continue;
+    if (L.qp[a] < 0) continue;
     for (int c = 0; c < 3; c++) {
-      const double gb = coef * Gv[c] * v[a] / den[a];
-      atomicAdd(fb.f[c] + qp[a], T(gb));
-      atomicAdd(fb.f[c] + qm[a], T(-gb));
+      const double gb = coef * L.Gv[c] * L.v[a] / L.den[a];
+      atomicAdd(fb.f[c] + L.qp[a], T(gb));
+      atomicAdd(fb.f[c] + L.qm[a], T(-gb));
     }
   }
+}
+
+// Tangent of compute_ftle: d lambda = 2 (G v) . (dG v), so w dFTLE = w d lambda / (2 lam T)
+// per node (summed on the host).
+template <typename T>
+__global__ void __launch_bounds__(256) k_ftle_tangent(DevGrid<T> g, FieldPtrs<T> fm, FieldPtrs<T> dfm, const T *__restrict__ wgt, T Tint,
+                                                       double *out) {
+  int i, j, k;
+  if (!node_of_thread(g.P.n, i, j, k)) return;
+  const int q = interior_index(g.P.n, i, j, k);
+  out[q] = 0.0;
+  const double w = (double)wgt[q];
+  if (w == 0.0) return;
+  FtleLin<T> L;
+  if (!ftle_linearise(g, fm, i, j, k, L)) return;
+  double dlam = 0.0;
+  for (int c = 0; c < 3; c++) {
+    double dGv = 0.0;
+    for (int a = 0; a < 3; a++)
+      if (L.qp[a] >= 0) dGv += (double)(dfm.f[c][L.qp[a]] - dfm.f[c][L.qm[a]]) / L.den[a] * L.v[a];
+    dlam += 2.0 * L.Gv[c] * dGv;
+  }
+  out[q] = w * dlam / (2.0 * L.lam * (double)Tint);
 }
 
 // adjoint velocity (after the ghost fold) -> caller's i-fastest arrays
@@ -342,6 +473,7 @@ class Adjoint {
   }
 
   bool run(double *J, std::string &msg) {
+    tangent_ = pr_.du && pr_.dv && pr_.dw && pr_.dJ;
     if (!setup(msg)) return false;
     if (!forward(J, msg)) return false;
     if (pr_.gu && pr_.gv && pr_.gw && !backward(msg)) return false;
@@ -504,6 +636,24 @@ class Adjoint {
       nsub_[l] = (int)std::max(1L, ns);
     }
     if (!field3(fm_[0], msg) || !field3(fm_[1], msg)) return false;
+    if (tangent_) {
+      // the direction, padded and ghost-filled like the levels (its CFL maxima are unused)
+      if (!slab(DU_, (size_t)3 * L, msg)) return false;
+      if (!(red_tan_ = pool_.alloc<DevReduce>(1, msg))) return false;
+      ACK(cudaMemsetAsync(red_tan_, 0, sizeof(DevReduce), stream_));
+      for (int l = 0; l < L; l++)
+        k_ingest<T, T, lcsdata_t, false><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, pr_.du[l], pr_.dv[l], pr_.dw[l], DU_[3 * l],
+                                                                                    DU_[3 * l + 1], DU_[3 * l + 2], red_tan_);
+      ACK(cudaGetLastError());
+      int terr = 0;
+      ACK(cudaMemcpyAsync(&terr, &red_tan_->err, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+      ACK(cudaStreamSynchronize(stream_));
+      if (terr) {
+        msg = "adjoint: non-finite tangent direction";
+        return false;
+      }
+      if (!field3(dfm_[0], msg) || !field3(dfm_[1], msg)) return false;
+    }
     cur_ = 0;
     const int K = pr_.checkpoint_every;
     const int nseg = (L - 2) / K + 1;  // segments of updates 1..L-1
@@ -514,7 +664,7 @@ class Adjoint {
         for (int c = 0; c < 3; c++)
           ACK(cudaMemcpyAsync(cp_[3 * s + c], fm_[cur_][c], ntot_ * sizeof(T), cudaMemcpyDeviceToDevice, stream_));
       }
-      if (!advance(l, fm_, cur_, nullptr, msg)) return false;
+      if (!advance(l, fm_, cur_, nullptr, msg, tangent_)) return false;
     }
     // FTLE of the final map and J
     T *in[3];
@@ -541,13 +691,31 @@ class Adjoint {
     double s = 0.0;
     for (long q = 0; q < N_; q++) s += (double)hw[q] * (double)hf[q];
     *J = s;
+    if (tangent_) {
+      double *dj = pool_.alloc<double>(N_, msg);
+      if (!dj) return false;
+      FieldPtrs<T> fm{}, dfm{};
+      for (int c = 0; c < 3; c++) {
+        fm.f[c] = fm_[cur_][c];
+        dfm.f[c] = dfm_[cur_][c];
+      }
+      k_ftle_tangent<T><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, fm, dfm, pr_.weight, Tint, dj);
+      ACK(cudaGetLastError());
+      std::vector<double> hd(N_);
+      ACK(cudaMemcpyAsync(hd.data(), dj, N_ * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+      ACK(cudaStreamSynchronize(stream_));
+      double t = 0.0;
+      for (long q = 0; q < N_; q++) t += hd[q];
+      *pr_.dJ = t;
+    }
     return true;
   }
 
   // every subcycle of update l (levels l-1 -> l) on the double buffer buf, starting from
   // buf[cur]; cur follows the result.  With `keep`, the flow map before subcycle q is copied
   // to keep[3 q + c].
-  bool advance(int l, T *buf[2][3], int &cur, T *const *keep, std::string &msg) {
+  // With `tangent`, the tangent map dfm_ advances alongside (dfm_[cur] pairs with buf[cur]).
+  bool advance(int l, T *buf[2][3], int &cur, T *const *keep, std::string &msg, bool tangent = false) {
     const lcsdata_t t0 = pr_.times[l - 1], t1 = pr_.times[l];
     const lcsdata_t dt_f = t1 - t0;
     const int ns = nsub_[l];
@@ -572,6 +740,24 @@ class Adjoint {
       const SplineAxes<T> sa{};
       int *err = &red_dev_->err;
       const dim3 grd = node_grid(), blk(32, 8, 1);
+      if (tangent) {
+        // reads the map before the subcycle, so it runs before the forward kernel replaces it
+        VelFields<T> D{};
+        FieldPtrs<T> dfo{};
+        FieldPtrsW<T> dfn{};
+        for (int c = 0; c < 3; c++) {
+          D.un[c] = DU_[3 * (l - 1) + c];
+          D.unp1[c] = DU_[3 * l + c];
+          dfo.f[c] = dfm_[cur][c];
+          dfn.f[c] = dfm_[cur ^ 1][c];
+        }
+        if (pr_.integrator == RK2)
+          k_sl_tangent<T, RK2><<<grd, blk, 0, stream_>>>(dg_, V, D, fo, dfo, dfn, S, (T)dt);
+        else
+          k_sl_tangent<T, EULER><<<grd, blk, 0, stream_>>>(dg_, V, D, fo, dfo, dfn, S, (T)dt);
+        k_periodic_ghosts<T><<<(unsigned)((ntot_ + 255) / 256), 256, 0, stream_>>>(dg_, dfn, ntot_);
+        ACK(cudaGetLastError());
+      }
       if (pr_.integrator == RK2)
         k_sl_subcycle<T, T, RK2_, INTERP_LINEAR, false><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, (T)dt, err);
       else if (pr_.integrator == TRAPEZOIDAL)
@@ -707,6 +893,11 @@ class Adjoint {
   std::vector<int> nsub_;
   T *fm_[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
   int cur_ = 0;
+  // tangent-linear sweep: direction levels (padded) and the tangent map's double buffer
+  bool tangent_ = false;
+  std::vector<T *> DU_;
+  T *dfm_[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  DevReduce *red_tan_ = nullptr;
 };
 
 }  // namespace

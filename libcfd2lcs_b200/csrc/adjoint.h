@@ -19,10 +19,15 @@ struct AdjointProblem {
   const lcsdata_t *weight;           // device, n[0]n[1]n[2]: J = sum weight * FTLE
   int checkpoint_every;              // updates between stored flow maps (>= 1)
   lcsdata_t *const *gu, *const *gv, *const *gw;  // device outputs, one per level (may be null: J only)
+  // tangent-linear direction, device, one per level (may be null): with it, *dJ = dJ/du . d by
+  // a forward-mode sweep alongside the flow map
+  const lcsdata_t *const *du = nullptr, *const *dv = nullptr, *const *dw = nullptr;
+  double *dJ = nullptr;
 };
 
 // Runs the backward flow map over all levels (LINEAR interpolation), the FTLE of the final
-// map and J; with gradient outputs, the adjoint sweep.  Returns false with msg on error.
+// map and J; with gradient outputs, the adjoint sweep; with a tangent direction, the tangent-
+// linear sweep in the same forward pass.  Returns false with msg on error.
 bool adjoint_ftle(const AdjointProblem &p, double *J, std::string &msg);
 
 }  // namespace cfd2lcs

@@ -494,3 +494,28 @@ CFD2LCS_EXPORT int cfd2lcs_adjoint_ftle_c(const int n[3], const lcsdata_t *x, co
   }
   return ok ? 0 : 1;
 }
+
+// Tangent-linear check of the adjoint: J and dJ = <dJ/du, d> for one direction d, by a forward-
+// mode sweep alongside the flow map; see include/cfd2lcs_b200.h.  Returns 0, or 1 with msg.
+CFD2LCS_EXPORT int cfd2lcs_tangent_ftle_c(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, int integrator,
+                                          lcsdata_t cfl, int nlevels, const lcsdata_t *const *d_u, const lcsdata_t *const *d_v,
+                                          const lcsdata_t *const *d_w, const lcsdata_t *times, const lcsdata_t *d_weight,
+                                          const lcsdata_t *const *d_du, const lcsdata_t *const *d_dv, const lcsdata_t *const *d_dw,
+                                          double *J, double *dJ, char *msg, size_t len) {
+  std::string m;
+  bool ok = d_du && d_dv && d_dw && dJ;
+  if (!ok) m = "tangent: a direction (d_du, d_dv, d_dw) and dJ are required";
+  if (ok) {
+    cfd2lcs::AdjointProblem p{n, x, y, z, integrator, (double)cfl, nlevels, d_u, d_v, d_w, times, d_weight, 1, nullptr, nullptr, nullptr};
+    p.du = d_du;
+    p.dv = d_dv;
+    p.dw = d_dw;
+    p.dJ = dJ;
+    ok = cfd2lcs::adjoint_ftle(p, J, m);
+  }
+  if (msg && len > 0) {
+    std::strncpy(msg, m.c_str(), len - 1);
+    msg[len - 1] = 0;
+  }
+  return ok ? 0 : 1;
+}

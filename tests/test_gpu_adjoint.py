@@ -103,3 +103,38 @@ def test_adjoint_rejects_walled_grids():
     u = [torch.zeros(16 * 8, dtype=torch.float64, device="cuda") for _ in range(3)]
     with pytest.raises(RuntimeError, match="periodic|three-dimensional"):
         L.adjoint_ftle(g, u, u, u, [0.0, 0.1, 0.2], torch.zeros(16 * 8, dtype=torch.float64, device="cuda"))
+
+
+@pytest.mark.parametrize("integrator", [0, 1, 2])
+def test_tangent_linear_model_matches_adjoint(integrator):
+    """Dot-product test: the forward-mode sweep's dJ along a direction d equals <dJ/du, d> from
+    the reverse sweep to rounding (both differentiate the same discrete map with the same
+    held-fixed choices), and its J is the adjoint's J."""
+    import torch
+
+    import libcfd2lcs_b200 as L
+    n, nl, dt = 10, 7, 0.05
+    g, lev, times = _levels(n, nl, dt)
+    wgt = _weight(g)
+    J, gu, gv, gw = L.adjoint_ftle(g, *lev, times, wgt, integrator=integrator, checkpoint_every=3)
+    grads = (gu, gv, gw)
+    rng = np.random.default_rng(5)
+    for _ in range(3):
+        d = [[torch.from_numpy(rng.standard_normal(lev[c][k].numel())).cuda() for k in range(nl)] for c in range(3)]
+        Jt, dJ = L.tangent_ftle(g, *lev, times, wgt, *d, integrator=integrator)
+        assert Jt == J
+        ad = sum(float(torch.dot(grads[c][k], d[c][k])) for c in range(3) for k in range(nl))
+        assert abs(dJ - ad) <= 1e-11 * max(abs(dJ), abs(ad)), (dJ, ad)
+
+
+def test_tangent_requires_a_direction():
+    import ctypes as C
+
+    import libcfd2lcs_b200 as L
+    lib = L.load("dp")
+    msg = C.create_string_buffer(256)
+    J, dJ = C.c_double(0), C.c_double(0)
+    n = np.array([4, 4, 4], dtype=np.int32)
+    rc = lib.cfd2lcs_tangent_ftle_c(n.ctypes.data_as(C.c_void_p), None, None, None, 2, 0.5, 2, None, None, None, None, None, None,
+                                    None, None, C.byref(J), C.byref(dJ), msg, 256)
+    assert rc == 1 and b"direction" in msg.value
