@@ -15,6 +15,7 @@
 
 #include "adjoint.h"
 #include "engine.h"
+#include "writer.h"
 
 using cfd2lcs::Counters;
 using cfd2lcs::EngineBase;
@@ -112,8 +113,14 @@ void do_set_option(const std::string &opt, int val) {
   if (lib.error) return;
   const bool tf = (val == LCS_TRUE || val == LCS_FALSE);
   bool ok = true;
-  if (opt == "SYNCTIMER" || opt == "DEBUG" || opt == "WRITE_FLOWMAP" || opt == "WRITE_VELOCITY" || opt == "WRITE_BCFLAG") {
-    ok = tf;  // timing / verbosity / output switches: accepted, no effect on the results
+  if (opt == "SYNCTIMER" || opt == "DEBUG") {
+    ok = tf;  // timing / verbosity switches: accepted, no effect on the results
+  } else if (opt == "WRITE_FLOWMAP" || opt == "WRITE_VELOCITY" || opt == "WRITE_BCFLAG") {
+    ok = tf;  // variables of the output files (src/cfd2lcs.f90:494-531)
+    if (ok) (opt == "WRITE_FLOWMAP" ? lib.opt.write_flowmap : opt == "WRITE_VELOCITY" ? lib.opt.write_velocity : lib.opt.write_bcflag) = val;
+  } else if (opt == "WRITE_LCS" || opt == "WRITE_LCS_ASYNC") {  // extensions: output files on / background completion
+    ok = tf;
+    if (ok) (opt == "WRITE_LCS" ? lib.opt.write_lcs : lib.opt.write_lcs_async) = val;
   } else if (opt == "VELOCITY_INVARIANTS") {
     ok = tf;
     if (ok) lib.opt.velocity_invariants = val;
@@ -294,6 +301,14 @@ CFD2LCS_EXPORT void cfd2lcs_get_kernel_times_c(double t[2], long long n[2]) {
   t[1] = k.fwd_kernel_ms;
   n[0] = k.sl_kernel_launches;
   n[1] = k.fwd_kernel_launches;
+}
+
+// Host-only formatting hook (no device work): the Fortran ESw.d editing the output files use,
+// for checking the writer on machines without a GPU.  out receives w characters and a NUL.
+CFD2LCS_EXPORT void cfd2lcs_b200_format_es(double v, int w, int d, char *out) {
+  if (!out || w <= 0 || w > 60) return;
+  cfd2lcs::format_es(v, w, d, out);
+  out[w] = 0;
 }
 
 // Host-only grid set-up (no device work): the padded coordinates, flags, boundary normals

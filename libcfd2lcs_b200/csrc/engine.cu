@@ -6,10 +6,12 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <memory>
 
 #include "grid.h"
 #include "kernels.cuh"
 #include "spline_host.h"
+#include "writer.h"
 
 namespace cfd2lcs {
 
@@ -63,6 +65,7 @@ struct SplineSet {
 template <typename T, typename TV>
 struct Diag {
   int handle = 0, type = 0;
+  std::string label;  // lcs%label: names the output files
   lcsdata_t T_ = 0, h = 0, dt_factor = 1;
   int nslot = 0;
   // backward: working flow map (double buffered, padded)
@@ -136,6 +139,7 @@ class Engine : public EngineBase {
  public:
   explicit Engine(const Options *opt) : opt_(opt) {}
   ~Engine() override {
+    writer_.reset();  // finishes the queued files while their staged copies' stream still exists
     if (stream_) cudaStreamSynchronize(stream_);
     arena_.release();
     for (auto &e : ev_) cudaEventDestroy(e);
@@ -194,6 +198,14 @@ class Engine : public EngineBase {
     }
     CK(cudaMallocHost(&red_host_, sizeof(DevReduce)));
     for (int a = 0; a < 3; a++) n_[a] = n[a];
+    // coordinate lines and interior flags for the output files (the grid is a tensor product)
+    for (int a = 0; a < 3; a++)
+      out_lines_[a] = std::make_shared<std::vector<double>>(hg_.lt[a].begin() + 1, hg_.lt[a].begin() + 1 + n[a]);
+    {
+      auto fl = std::make_shared<std::vector<int8_t>>((size_t)n[0] * n[1] * n[2]);
+      for (size_t q = 0; q < fl->size(); q++) (*fl)[q] = (int8_t)flag[q];
+      out_flags_ = fl;
+    }
     N_ = (long)n[0] * n[1] * n[2];
     ntot_ = hg_.ntot();
     // grid tables
@@ -256,7 +268,6 @@ class Engine : public EngineBase {
   }
 
   int diagnostic_init(int type, int resolution, lcsdata_t Tint, lcsdata_t h, const char *label, std::string &msg) override {
-    (void)label;
     if (resolution != 0) {
       msg = "diagnostic_init: resolution /= 0 (a refined lcs grid, new_sgrid_from_sgrid) is not supported";
       return -1;
@@ -276,6 +287,8 @@ class Engine : public EngineBase {
     DiagT d;
     d.handle = (int)diags_.size() + 1;
     d.type = type;
+    d.label = label ? label : "";
+    while (!d.label.empty() && d.label.back() == ' ') d.label.pop_back();  // trim(label)
     d.T_ = Tint;
     d.h = h;
     d.dt_factor = type == FTLE_BKWD ? lcsdata_t(1) / lcsdata_t(std::max(1 + resolution, 1)) : lcsdata_t(1);
@@ -515,7 +528,7 @@ class Engine : public EngineBase {
       // files reconstruct never reads back
       const long wslot = fnint((double)((lcsdata_t)std::fmod((double)t_np1_, (double)d.T_) / d.h));
       (void)step0;
-      if (opt_->velocity_invariants && !snapshot_velocity(wslot, msg)) return false;
+      if (need_velocity_ring() && !snapshot_velocity(wslot, msg)) return false;
       if (wslot >= 0 && wslot < d.nslot) {
         if (!launch_snapshot(d, (int)wslot, msg)) return false;
         d.written[wslot] = 1;
@@ -558,6 +571,8 @@ class Engine : public EngineBase {
       // compute_invariants from the velocity of the reconstruction's starting step: the
       // current one (backward) or the next, not yet wrapped (forward), flowmap_m.f90:202-245
       if (opt_->velocity_invariants && !launch_invariants(d, wslot + (d.type == FTLE_FWD ? 1 : 0), msg)) return false;
+      // write_lcs (src/cfd2lcs.f90:202): the frame's file, staged now, written by the writer
+      if (opt_->write_lcs && !enqueue_output(d, wslot + (d.type == FTLE_FWD ? 1 : 0), msg)) return false;
       if (!mark(f7, msg)) return false;
       // reset_lp: particles back to the grid, flow map to zero (src/cfd2lcs.f90:208-209)
       if (d.type == FTLE_BKWD) {
@@ -597,6 +612,14 @@ class Engine : public EngineBase {
       }
     }
     spans_.clear();
+    if (writer_) {
+      if (!opt_->write_lcs_async) writer_->flush();  // the reference's file is complete on return
+      const std::string e = writer_->take_error();
+      if (!e.empty()) {
+        msg = e;
+        return false;
+      }
+    }
     return sync_errors(msg);
   }
 
@@ -1054,6 +1077,105 @@ class Engine : public EngineBase {
     return true;
   }
 
+  // the velocity snapshots are kept when VELOCITY_IO or VELOCITY_INVARIANTS asks for them
+  // (write_flowmap_substep, src/flowmap_m.f90:140); VELOCITY_IO matters only with files
+  bool need_velocity_ring() const { return opt_->velocity_invariants || (opt_->write_lcs && opt_->write_velocity); }
+
+  // The frame's output file (write_lcs / write_ftle, src/io_nohdf5_m.f90:47-264): name,
+  // header, and the device blocks copied into pinned staging on the stream; the writer thread
+  // formats and writes once the copies are done.
+  bool enqueue_output(DiagT &d, long ustep, std::string &msg) {
+    long long findex = (long long)fnint((double)(t_np1_ / d.h));
+    if (d.type == FTLE_FWD) findex -= (long long)fnint((double)(d.T_ / d.h));
+    std::string idx;
+    if (!lcs_file_index(findex, idx)) {
+      msg = "ERROR: unsupported range for file index, " + std::to_string(findex);
+      return false;
+    }
+    if (!writer_) writer_.reset(new LcsWriter());
+    OutputJob job;
+    job.path = "./cfd2lcs_output/" + d.label + "_" + idx + ".dat";
+    for (int a = 0; a < 3; a++) {
+      job.n[a] = n_[a];
+      job.lines[a] = out_lines_[a];
+    }
+    job.flags = out_flags_;
+    const std::string title = d.label + "-FTLE";
+    std::string h = "TITLE = \"" + title + "\"\nVARIABLES =\n\"X\"\n\"Y\"\n\"Z\"\n";
+    if (opt_->write_flowmap) h += "\"FM-X\"\n\"FM-Y\"\n\"FM-Z\"\n";
+    if (opt_->write_velocity) h += "\"U-X\"\n\"U-Y\"\n\"U-Z\"\n";
+    if (opt_->write_bcflag) h += "\"FLAG\"\n";
+    if (opt_->velocity_invariants) h += "\"Q\"\n\"C\"\n\"D\"\n\"H\"\n\"L2\"\n";
+    h += "\"FTLE\"\nZONE\nT = \"" + title + "\"\n";
+    char tbuf[32], line[128];
+    format_es((double)t_np1_, 18, 4, tbuf);
+    tbuf[18] = 0;
+    std::snprintf(line, sizeof(line), "STRANDID = %010d, SOLUTIONTIME = %s\n", 1, tbuf);
+    h += line;
+    std::snprintf(line, sizeof(line), "I = %010d J = %010d K = %010d\n", n_[0], n_[1], n_[2]);
+    h += line;
+    h += "ZONETYPE = Ordered, DATAPACKING = BLOCK\n";
+    job.header = h;
+    // blocks: X Y Z [FM] [U] [FLAG] [Q C D H L2] FTLE
+    struct Src {
+      const void *p;
+      size_t esize;
+    };
+    std::vector<Src> staged;
+    std::vector<OutputBlock> blocks;
+    size_t bytes = 0;
+    auto stage = [&](const void *p, size_t esize) {
+      OutputBlock b;
+      b.kind = esize == 8 ? OutputBlock::STAGED_F64 : OutputBlock::STAGED_F32;
+      b.offset = bytes;
+      bytes += ((size_t)N_ * esize + 255) / 256 * 256;
+      staged.push_back({p, esize});
+      blocks.push_back(b);
+    };
+    auto plain = [&](OutputBlock::Kind k) {
+      OutputBlock b;
+      b.kind = k;
+      blocks.push_back(b);
+    };
+    plain(OutputBlock::LINE_X);
+    plain(OutputBlock::LINE_Y);
+    plain(OutputBlock::LINE_Z);
+    if (opt_->write_flowmap)
+      for (int c = 0; c < 3; c++) stage(d.composed[c], sizeof(T));
+    if (opt_->write_velocity) {
+      // lp%ugrid: the frame's starting velocity when its snapshot exists, else zero (reset_lp)
+      const bool have = ustep >= 0 && ustep < (long)vwritten_.size() && vwritten_[ustep];
+      for (int c = 0; c < 3; c++) {
+        if (have) stage(vring_[3 * ustep + c], sizeof(TV));
+        else plain(OutputBlock::ZERO);
+      }
+    }
+    if (opt_->write_bcflag) plain(OutputBlock::FLAG);
+    if (opt_->velocity_invariants) {
+      const int order[5] = {0, 2, 1, 3, 4};  // Q, C, D, H, L2 (the fields are kept Q, D, C, H, L2)
+      for (int q : order) stage(d.inv[q], sizeof(lcsdata_t));
+    }
+    stage(d.ftle, sizeof(lcsdata_t));
+    void *buf = nullptr;
+    const int bi = writer_->acquire(std::max<size_t>(bytes, 1), &buf, msg);
+    if (bi < 0) return false;
+    size_t q = 0;
+    for (OutputBlock &b : blocks) {
+      if (b.kind != OutputBlock::STAGED_F64 && b.kind != OutputBlock::STAGED_F32) continue;
+      CK(cudaMemcpyAsync(static_cast<char *>(buf) + b.offset, staged[q].p, (size_t)N_ * staged[q].esize, cudaMemcpyDeviceToHost,
+                         stream_));
+      q++;
+    }
+    cudaEvent_t ev;
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(ev, stream_));
+    job.blocks = std::move(blocks);
+    job.ready = ev;
+    job.buffer = bi;
+    writer_->submit(std::move(job));
+    return true;
+  }
+
   bool launch_invariants(DiagT &d, long ustep, std::string &msg) {
     if (!d.inv[0])
       for (int q = 0; q < 5; q++)
@@ -1097,6 +1219,9 @@ class Engine : public EngineBase {
   }
 
   const Options *opt_;
+  std::unique_ptr<LcsWriter> writer_;  // created by the first output file
+  std::shared_ptr<const std::vector<double>> out_lines_[3];
+  std::shared_ptr<const std::vector<int8_t>> out_flags_;
   HostGrid<lcsdata_t> hg_;
   DevGrid<T> dg_{};
   DevArena arena_;

@@ -25,6 +25,11 @@ struct Options {
   int velocity_invariants = 0;
   double cfl = 0.5;
   int mixed_precision = 0;  // extension: FP32 velocity fields and interpolation taps, FP64 positions / flow maps
+  // output files (write_lcs, src/io_nohdf5_m.f90:47-264): the variables written follow the
+  // reference's FLOWMAP_IO, VELOCITY_IO and BCFLAG_IO defaults (src/data_m.f90:44-54)
+  int write_flowmap = 1, write_velocity = 1, write_bcflag = 0;
+  int write_lcs = 0;        // extension: write the files at all (off by default)
+  int write_lcs_async = 0;  // extension: let a frame's file complete after cfd2lcs_update returns
 };
 
 struct Counters {

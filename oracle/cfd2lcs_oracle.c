@@ -119,6 +119,7 @@ typedef struct {
     real *inv[5]; /* velocity invariants Q, D, C, H, L2 of the last frame (padded sr0) */
     real *l2margin; /* checker aid: middle eigenvalue / largest magnitude (how close L2 is to a tie) */
     sr1_t fm_out; /* composed flow map of the last FTLE frame (written by write_lcs) */
+    char label[136]; /* lcs%label, trimmed */
     int nslot;
     real **slot[3]; /* slot[c][s] -> interior values of stored sub-flow map */
     int *written;
@@ -146,6 +147,11 @@ static struct {
      * interior values; steps 0 .. NVSTEP-1 */
     real *vring[3][MAXVSTEP];
     int vwritten[MAXVSTEP];
+    /* output files (write_lcs): WRITE_LCS switches them on; FLOWMAP_IO and VELOCITY_IO
+     * default to TRUE (data_m.f90:44-49), kept here as their negations so that zeroed state
+     * means the defaults */
+    int write_lcs, no_flowmap_io, no_velocity_io, bcflag_io;
+    char outdir[512];
 } S = {0, "", RK2, LINEAR, 0, 0, 0, (real)0.5, 0};
 
 static void latch(const char *m) {
@@ -1365,7 +1371,7 @@ static void write_substep(lcs_t *L) {
     int step = ring_step(S.t_np1, L->T, L->h);
     /* velocity snapshot (VELOCITY_INVARIANTS; step nint(T/h) is kept too: the forward
      * reconstruction reads step+1 before wrapping it) */
-    if (S.velocity_invariants && step >= 0 && step < MAXVSTEP) {
+    if ((S.velocity_invariants || (S.write_lcs && !S.no_velocity_io)) && step >= 0 && step < MAXVSTEP) {
         long nint_ = (long)d->ni * d->nj * d->nk;
         for (int c = 0; c < 3; c++) {
             if (!S.vring[c][step]) S.vring[c][step] = zalloc(nint_);
@@ -1684,6 +1690,91 @@ static void compute_invariants(lcs_t *L, int ustep) {
     sr1_free(&ug);
 }
 
+/* Fortran ESw.d editing (the ES14.6 data and ES18.4 time fields of write_ftle): a signed
+ * significand d.ddd... with one non-zero digit before the point (zero prints as 0.000...),
+ * correctly rounded, then E+xx, or +xxx without the E for three-digit exponents; NaN and
+ * Infinity as gfortran spells them; right-justified in w columns. */
+static void es_edit(double v, int w, int d, char *out) {
+    char b[64];
+    int len;
+    if (v != v) len = snprintf(b, sizeof b, "NaN");
+    else if (v > DBL_MAX || v < -DBL_MAX) len = snprintf(b, sizeof b, "%s", v < 0 ? "-Infinity" : "Infinity");
+    else {
+        len = snprintf(b, sizeof b, "%.*E", d, v);
+        char *e = strchr(b, 'E');
+        if (e && (int)strlen(e + 2) == 3) { memmove(e, e + 1, strlen(e)); len--; }
+    }
+    if (len > w) { memset(out, '*', (size_t)w); return; }
+    memset(out, ' ', (size_t)(w - len));
+    memcpy(out + w - len, b, (size_t)len);
+}
+
+/* write_data_from_master (io_nohdf5_m.f90:266-332) at one rank: the interior of a padded
+ * field (or a compact interior array when compact), i fastest, 10 values per line
+ * (NDATA_PER_LINE; the MAX_CHUNK of 100000 is a multiple of 10, so chunking adds no breaks) */
+static void write_block(FILE *fp, const dims_t *d, const real *f, int compact) {
+    long count = (long)d->ni * d->nj * d->nk, q = 0;
+    char cell[16];
+    for (int k = 1; k <= d->nk; k++)
+        for (int j = 1; j <= d->nj; j++)
+            for (int i = 1; i <= d->ni; i++, q++) {
+                double v = f ? (double)(compact ? f[q] : f[PX(d, i, j, k)]) : 0.0;
+                es_edit(v, 14, 6, cell);
+                fwrite(cell, 1, 14, fp);
+                if ((q + 1) % 10 == 0 || q + 1 == count) fputc('\n', fp);
+            }
+}
+
+/* write_lcs + write_ftle (io_nohdf5_m.f90:47-133, 183-264): file name from the time index
+ * (minus T/h for FTLE_FWD) with the reference's per-range integer formats, the Tecplot
+ * header, then the X, Y, Z, [FM], [U], [FLAG], [Q C D H L2], FTLE blocks.  ustep: the ring
+ * step whose velocity snapshot is lp%ugrid (zero when it was never written, reset_lp). */
+static void write_lcs(lcs_t *L, int ustep) {
+    const dims_t *d = &S.g.d;
+    long long findex = (long long)fnint(S.t_np1 / L->h);
+    if (L->diagnostic == FTLE_FWD) findex -= (long long)fnint(L->T / L->h);
+    if (findex < -999999999LL || findex > 999999999LL) { latch("ERROR: unsupported range for file index"); return; }
+    char idx[32];
+    if (findex >= 1000 && findex <= 9999) snprintf(idx, sizeof idx, "%010lld", findex); /* i10.10 for this range */
+    else snprintf(idx, sizeof idx, "%lld", findex);
+    char path[1024];
+    snprintf(path, sizeof path, "%s/%s_%s.dat", S.outdir[0] ? S.outdir : "./cfd2lcs_output", L->label, idx);
+    FILE *fp = fopen(path, "w");
+    if (!fp) { latch("write_lcs: cannot open the output file"); return; }
+    fprintf(fp, "TITLE = \"%s-FTLE\"\nVARIABLES =\n\"X\"\n\"Y\"\n\"Z\"\n", L->label);
+    if (!S.no_flowmap_io) fprintf(fp, "\"FM-X\"\n\"FM-Y\"\n\"FM-Z\"\n");
+    if (!S.no_velocity_io) fprintf(fp, "\"U-X\"\n\"U-Y\"\n\"U-Z\"\n");
+    if (S.bcflag_io) fprintf(fp, "\"FLAG\"\n");
+    if (S.velocity_invariants) fprintf(fp, "\"Q\"\n\"C\"\n\"D\"\n\"H\"\n\"L2\"\n");
+    char tfield[24];
+    es_edit((double)S.t_np1, 18, 4, tfield);
+    tfield[18] = 0;
+    fprintf(fp, "\"FTLE\"\nZONE\nT = \"%s-FTLE\"\nSTRANDID = %010d, SOLUTIONTIME = %s\n", L->label, 1, tfield);
+    fprintf(fp, "I = %010d J = %010d K = %010d\nZONETYPE = Ordered, DATAPACKING = BLOCK\n", d->ni, d->nj, d->nk);
+    for (int c = 0; c < 3; c++) write_block(fp, d, S.g.grid.c[c], 0);
+    if (!S.no_flowmap_io)
+        for (int c = 0; c < 3; c++) write_block(fp, d, L->lp.fm.c[c], 0);
+    if (!S.no_velocity_io) {
+        const int have = ustep >= 0 && ustep < MAXVSTEP && S.vwritten[ustep];
+        for (int c = 0; c < 3; c++) write_block(fp, d, have ? S.vring[c][ustep] : NULL, 1);
+    }
+    if (S.bcflag_io) {
+        long n = (long)d->ni * d->nj * d->nk, q = 0;
+        real *fl = zalloc(n);
+        for (int k = 1; k <= d->nk; k++)
+            for (int j = 1; j <= d->nj; j++)
+                for (int i = 1; i <= d->ni; i++) fl[q++] = (real)S.g.bcflag[PX(d, i, j, k)];
+        write_block(fp, d, fl, 1);
+        free(fl);
+    }
+    if (S.velocity_invariants) {
+        const int order[5] = {0, 2, 1, 3, 4}; /* Q, C, D, H, L2 */
+        for (int q = 0; q < 5; q++) write_block(fp, d, L->inv[order[q]], 0);
+    }
+    write_block(fp, d, L->ftle, 0);
+    fclose(fp);
+}
+
 /* ------------------------------------------------------------------------------------
  * Entry points (cfd2lcs.f90:2-682 semantics, one rank, no output files).
  * ------------------------------------------------------------------------------------ */
@@ -1736,7 +1827,10 @@ EXPORT void orc_reset(void) {
         sr1_free(&S.g.grid); sr1_free(&S.g.bcnorm); free(S.g.bcflag);
         sr1_free(&S.u_n); sr1_free(&S.u_np1); sr1_free(&S.delta);
     }
+    char keep[sizeof S.outdir];
+    memcpy(keep, S.outdir, sizeof keep); /* the output directory outlives a reset */
     memset(&S, 0, sizeof(S));
+    memcpy(S.outdir, keep, sizeof keep);
     S.integrator = RK2;
     S.interpolator = LINEAR;
     S.cfl_max = (real)0.5;
@@ -1762,8 +1856,10 @@ EXPORT void orc_init(const int n[3], const int offset[3], const real *x, const r
 }
 
 /* cfd2lcs_diagnostic_init, cfd2lcs.f90:252-358 with init_ftle lcs_m.f90:16-64 */
+/* directory of the output files (the reference's ./cfd2lcs_output) */
+EXPORT void orc_set_output_dir(const char *dir) { snprintf(S.outdir, sizeof S.outdir, "%s", dir ? dir : ""); }
+
 EXPORT int orc_diagnostic_init(int type, int resolution, real T, real h, const char *label) {
-    (void)label;
     if (S.error) return -1;
     if (!S.inited) { latch("diagnostic_init before init"); return -1; }
     if (S.nlcs >= MAXLCS) { latch("diagnostic_init: too many diagnostics"); return -1; }
@@ -1777,6 +1873,8 @@ EXPORT int orc_diagnostic_init(int type, int resolution, real T, real h, const c
     L->diagnostic = type;
     L->T = T;
     L->h = h;
+    snprintf(L->label, sizeof L->label, "%s", label ? label : "");
+    for (size_t e = strlen(L->label); e > 0 && L->label[e - 1] == ' '; e--) L->label[e - 1] = 0; /* trim */
     const dims_t *d = &S.g.d;
     L->ftle = zalloc(d->ntot);
     for (int q = 0; q < 5; q++) L->inv[q] = zalloc(d->ntot);
@@ -1850,6 +1948,7 @@ EXPORT void orc_update(const int n[3], const real *u, const real *v, const real 
         reconstruct(L);
         compute_ftle(L);
         if (S.velocity_invariants) compute_invariants(L, ustep);
+        if (S.write_lcs) write_lcs(L, ustep);
         for (int c = 0; c < 3; c++) memcpy(L->fm_out.c[c], L->lp.fm.c[c], sizeof(real) * (size_t)d->ntot);
         S.ftle_frames++;
         reset_lp(&S.g, &L->lp, 1);
@@ -1862,9 +1961,20 @@ EXPORT void orc_set_option(const char *opt, int val) {
     if (S.error) return;
     int ok = 1;
     int tf = (val == LCS_TRUE || val == LCS_FALSE);
-    if (!strcmp(opt, "SYNCTIMER") || !strcmp(opt, "DEBUG") || !strcmp(opt, "WRITE_FLOWMAP") || !strcmp(opt, "WRITE_VELOCITY") ||
-        !strcmp(opt, "WRITE_BCFLAG")) {
+    if (!strcmp(opt, "SYNCTIMER") || !strcmp(opt, "DEBUG")) {
         ok = tf;
+    } else if (!strcmp(opt, "WRITE_FLOWMAP")) {
+        ok = tf;
+        if (ok) S.no_flowmap_io = !val;
+    } else if (!strcmp(opt, "WRITE_VELOCITY")) {
+        ok = tf;
+        if (ok) S.no_velocity_io = !val;
+    } else if (!strcmp(opt, "WRITE_BCFLAG")) {
+        ok = tf;
+        if (ok) S.bcflag_io = val;
+    } else if (!strcmp(opt, "WRITE_LCS")) { /* the library's switch for the output files */
+        ok = tf;
+        if (ok) S.write_lcs = val;
     } else if (!strcmp(opt, "VELOCITY_INVARIANTS")) {
         ok = tf;
         if (ok) S.velocity_invariants = val;

@@ -55,6 +55,7 @@ class Oracle:
         L.orc_get_fm.restype = C.c_int
         L.orc_get_invariants.argtypes = [C.c_int, P]
         L.orc_get_invariants.restype = C.c_int
+        L.orc_set_output_dir.argtypes = [C.c_char_p]
         L.orc_get_l2margin.argtypes = [C.c_int, P]
         L.orc_get_l2margin.restype = C.c_int
         L.orc_get_particles.argtypes = [C.c_int, P]
@@ -135,6 +136,10 @@ class Oracle:
         out = np.zeros(5 * int(np.prod(self.n)), dtype=self.dtype)
         assert self.lib.orc_get_invariants(handle, self._p(out)) == 0
         return out.reshape((5,) + tuple(self.n[::-1])).transpose(0, 3, 2, 1)
+
+    def set_output_dir(self, path: str):
+        """Directory of the write_lcs files (WRITE_LCS); the reference's ./cfd2lcs_output."""
+        self.lib.orc_set_output_dir(str(path).encode())
 
     def l2margin(self, handle):
         """Middle eigenvalue of the lambda-2 tensor over its largest magnitude, last frame."""
