@@ -48,6 +48,15 @@ void cfd2lcs_update_device_c(int n[3], const lcsdata_t *d_u, const lcsdata_t *d_
  * 1 for an unknown handle, no frame yet or the option off. */
 int cfd2lcs_get_invariants_c(int lcs_handle, lcsdata_t *inv);
 
+/* LP_TRACER diagnostics (cfd2lcs_diagnostic_init with LP_TRACER after setting the
+ * TRACER_INJECT_X/Y/Z/RADIUS parameters; init_lp_tracer, src/lp_m.f90:116-226): one tracer per
+ * grid node inside the injection sphere, advected forward every update until its lifetime
+ * exceeds T.  The reference only writes their positions to its output files; these return
+ * the count (-1 for a handle that is not a tracer set) and the positions, three consecutive
+ * arrays (x, y, z) of count values each, the last ones reached.  0 on success. */
+int cfd2lcs_tracer_count_c(int lcs_handle);
+int cfd2lcs_get_tracers_c(int lcs_handle, lcsdata_t *xyz);
+
 /* Device pointer of a diagnostic's latest FTLE field (n[0]*n[1]*n[2] doubles in the dp
  * build, floats in the sp build), valid until the next update or finalize. */
 const lcsdata_t *cfd2lcs_ftle_device_ptr_c(int lcs_handle);

@@ -38,6 +38,7 @@ EXPORTED_SYMBOLS = [
     "cfd2lcs_finalize_c", "cfd2lcs_get_error_c", "cfd2lcs_reset_c", "cfd2lcs_get_ftle_c", "cfd2lcs_get_flowmap_c",
     "cfd2lcs_update_device_c", "cfd2lcs_ftle_device_ptr_c", "cfd2lcs_get_counters_c", "cfd2lcs_get_phase_times_c",
     "cfd2lcs_get_kernel_times_c", "cfd2lcs_reconstruct_noalloc_c", "cfd2lcs_get_invariants_c",
+    "cfd2lcs_tracer_count_c", "cfd2lcs_get_tracers_c",
     # batched form (include/cfd2lcs_b200.h)
     "cfd2lcs_batch_add_c", "cfd2lcs_batch_diagnostic_init_c", "cfd2lcs_batch_update_device_c", "cfd2lcs_batch_get_ftle_c",
     "cfd2lcs_batch_get_flowmap_c", "cfd2lcs_batch_get_counters_c", "cfd2lcs_batch_size_c", "cfd2lcs_batch_error_c",
@@ -92,6 +93,10 @@ def load(precision: str = "dp") -> C.CDLL:
     lib.cfd2lcs_get_flowmap_c.restype = C.c_int
     lib.cfd2lcs_get_invariants_c.argtypes = [C.c_int, P]
     lib.cfd2lcs_get_invariants_c.restype = C.c_int
+    lib.cfd2lcs_tracer_count_c.argtypes = [C.c_int]
+    lib.cfd2lcs_tracer_count_c.restype = C.c_int
+    lib.cfd2lcs_get_tracers_c.argtypes = [C.c_int, P]
+    lib.cfd2lcs_get_tracers_c.restype = C.c_int
     lib.cfd2lcs_ftle_device_ptr_c.argtypes = [C.c_int]
     lib.cfd2lcs_ftle_device_ptr_c.restype = C.c_void_p
     lib.cfd2lcs_get_counters_c.argtypes = [P]
@@ -207,6 +212,16 @@ class Cfd2lcs:
             raise RuntimeError("no invariants for this handle")
         N = int(np.prod(self.n))
         return np.stack([out[q * N:(q + 1) * N].reshape(self.n, order="F") for q in range(5)])
+
+    def tracers(self, handle):
+        """Positions of an LP_TRACER set, shape (3, count)."""
+        n = self.lib.cfd2lcs_tracer_count_c(int(handle))
+        if n < 0:
+            raise RuntimeError("not an LP_TRACER handle")
+        out = np.zeros(3 * n, dtype=self.dtype)
+        if self.lib.cfd2lcs_get_tracers_c(int(handle), self._p(out)) != 0:
+            raise RuntimeError("get_tracers failed")
+        return out.reshape(3, n)
 
     def ftle_device_ptr(self, handle) -> int:
         return int(self.lib.cfd2lcs_ftle_device_ptr_c(int(handle)) or 0)

@@ -92,6 +92,7 @@ int do_diagnostic_init(int type, int resolution, lcsdata_t T, lcsdata_t h, const
   }
   std::string msg;
   const int id = lib.eng->diagnostic_init(type, resolution, T, h, label, msg);
+  if (id == -2) return -1;  // LP_TRACER with no node in the injection sphere: handle -1, no error
   if (id < 0) latch(msg);
   return id;
 }
@@ -160,8 +161,11 @@ void do_set_param(const std::string &p, lcsdata_t val) {
   Library &lib = L();
   if (lib.error) return;
   if (p == "CFL") lib.opt.cfl = (double)val;
-  else if (p == "TRACER_INJECT_X" || p == "TRACER_INJECT_Y" || p == "TRACER_INJECT_Z" || p == "TRACER_INJECT_RADIUS") {
-  } else latch("ERROR, unknown libcfd2lcs parameter: " + p);
+  else if (p == "TRACER_INJECT_X") lib.opt.tracer_x = (double)val;
+  else if (p == "TRACER_INJECT_Y") lib.opt.tracer_y = (double)val;
+  else if (p == "TRACER_INJECT_Z") lib.opt.tracer_z = (double)val;
+  else if (p == "TRACER_INJECT_RADIUS") lib.opt.tracer_r = (double)val;
+  else latch("ERROR, unknown libcfd2lcs parameter: " + p);
 }
 
 }  // namespace
@@ -262,6 +266,18 @@ CFD2LCS_EXPORT int cfd2lcs_get_invariants_c(int lcs_handle, lcsdata_t *inv) {
   if (!lib.eng) return 1;
   std::string m;
   return lib.eng->get_invariants(lcs_handle, inv, m) ? 0 : 1;
+}
+
+CFD2LCS_EXPORT int cfd2lcs_tracer_count_c(int lcs_handle) {
+  Library &lib = L();
+  return lib.eng ? lib.eng->tracer_count(lcs_handle) : -1;
+}
+
+CFD2LCS_EXPORT int cfd2lcs_get_tracers_c(int lcs_handle, lcsdata_t *xyz) {
+  Library &lib = L();
+  if (!lib.eng || !xyz) return 1;
+  std::string m;
+  return lib.eng->get_tracers(lcs_handle, xyz, m) ? 0 : 1;
 }
 
 CFD2LCS_EXPORT void cfd2lcs_update_device_c(int n[3], const lcsdata_t *d_u, const lcsdata_t *d_v, const lcsdata_t *d_w, lcsdata_t time) {

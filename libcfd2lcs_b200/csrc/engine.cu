@@ -92,6 +92,11 @@ struct Diag {
   lcsdata_t *ftle = nullptr;                      // interior
   lcsdata_t *inv[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // velocity invariants (interior)
   bool have_frame = false;
+  // LP_TRACER: particles in P (np of them), time advected, and whether they still move
+  // (destroy_lp once the lifetime exceeds T, src/cfd2lcs.f90:225-231)
+  int np = 0;
+  lcsdata_t lifetime = 0;
+  bool active = true;
 };
 
 }  // namespace
@@ -272,10 +277,7 @@ class Engine : public EngineBase {
       msg = "diagnostic_init: resolution /= 0 (a refined lcs grid, new_sgrid_from_sgrid) is not supported";
       return -1;
     }
-    if (type == LP_TRACER) {
-      msg = "diagnostic_init: LP_TRACER is not supported by this library";
-      return -1;
-    }
+    if (type == LP_TRACER) return tracer_init(Tint, h, label, msg);
     if (type != FTLE_FWD && type != FTLE_BKWD) {
       msg = "ERROR, bad specification for lcs_type. Options are: FTLE_FWD, FTLE_BKWD, LP_TRACER";
       return -1;
@@ -463,6 +465,7 @@ class Engine : public EngineBase {
 
     // --- per particle set: K1 (backward) / K6 (forward) --------------------------------
     for (auto &d : diags_) {
+      if (!d.active) continue;
       const lcsdata_t q = this_cfl / (lcsdata_t(opt_->cfl) * d.dt_factor);
       long nsub = (long)std::ceil((double)q);
       if (!(q == q)) {
@@ -472,11 +475,12 @@ class Engine : public EngineBase {
       if (nsub < 1) nsub = 1;
       lcsdata_t dt = dt_f / (lcsdata_t)nsub;
       if (d.type == FTLE_BKWD) dt = lcsdata_t(-1) * dt;
+      const long long npart = d.type == LP_TRACER ? (long long)d.np : (long long)N_;
       if (std::fabs((double)dt) > 0) {
-        if (d.type == FTLE_FWD) counters_.integrations_fwd += (long long)N_ * nsub;
-        else counters_.integrations_bkwd += (long long)N_ * nsub;
+        if (d.type != FTLE_BKWD) counters_.integrations_fwd += npart * nsub;
+        else counters_.integrations_bkwd += npart * nsub;
       }
-      if (d.type == FTLE_FWD) counters_.nsub_fwd = nsub;
+      if (d.type != FTLE_BKWD) counters_.nsub_fwd = nsub;
       else counters_.nsub_bkwd = nsub;
       cudaEvent_t adv0, adv1;
       if (!mark(adv0, msg)) return false;
@@ -505,6 +509,10 @@ class Engine : public EngineBase {
           if (!mark(k1, msg)) return false;
           spans_.push_back({k0, k1, kkind});
           d.cur ^= 1;
+        } else if (d.type == LP_TRACER) {
+          // tracers: the forward subcycle on their own particles (few, unsorted)
+          if (!launch_fwd(iv, sa, V, d.P, S, (T)dt, msg, d.np)) return false;
+          d.lifetime = d.lifetime + (lcsdata_t)std::fabs((double)dt);  // integrate_lp, lp_motion_m.f90:332
         } else {
           if (sc % kSortInterval == 0 && !sort_particles(d, msg)) return false;
           if (!mark(k0, msg)) return false;
@@ -520,7 +528,14 @@ class Engine : public EngineBase {
 
     // --- h boundaries: K7 snapshot, K4 composition, K5 FTLE, reset ----------------------
     for (auto &d : diags_) {
+      if (!d.active) continue;
       if ((long)(t_np1_ / d.h) == (long)(t_n_ / d.h)) continue;
+      if (d.type == LP_TRACER) {
+        // write_lcs, then the end of the tracers' lifetime (src/cfd2lcs.f90:225-231)
+        if (opt_->write_lcs && !enqueue_tracer_output(d, msg)) return false;
+        if (d.lifetime > d.T_) d.active = false;
+        continue;
+      }
       cudaEvent_t f4, f5, f6, f7;
       if (!mark(f4, msg)) return false;
       const long step0 = fnint((double)(lcsdata_t)std::fmod((double)t_np1_, (double)d.T_) / (double)d.h);
@@ -720,6 +735,28 @@ class Engine : public EngineBase {
     return true;
   }
 
+  int tracer_count(int handle) override {
+    DiagT *d = find(handle);
+    return d && d->type == LP_TRACER ? d->np : -1;
+  }
+
+  // positions of a tracer set (the last ones it reached: after its lifetime the reference
+  // destroys the set, here it stops moving)
+  bool get_tracers(int handle, lcsdata_t *out, std::string &msg) override {
+    DiagT *d = find(handle);
+    if (!d || d->type != LP_TRACER) {
+      msg = "get_tracers: not an LP_TRACER handle";
+      return false;
+    }
+    CK(cudaStreamSynchronize(stream_));
+    std::vector<T> tmp(d->np);
+    for (int c = 0; c < 3; c++) {
+      if (d->np) CK(cudaMemcpy(tmp.data(), d->P.x[c], d->np * sizeof(T), cudaMemcpyDeviceToHost));
+      for (int q = 0; q < d->np; q++) out[(size_t)c * d->np + q] = (lcsdata_t)tmp[q];
+    }
+    return true;
+  }
+
   const lcsdata_t *ftle_device_ptr(int handle) override {
     DiagT *d = find(handle);
     return d ? d->ftle : nullptr;
@@ -731,6 +768,99 @@ class Engine : public EngineBase {
   int fail(std::string &msg, const char *what) {
     msg = std::string("CUDA error in ") + what;
     return -1;
+  }
+
+  // LP_TRACER (init_lp_tracer, src/lp_m.f90:116-226, and diagnostic_init, src/cfd2lcs.f90:
+  // 327-337): one particle per grid node inside the injection sphere, r <= radius, in node
+  // order (i fastest), starting at the node (where node tracking leaves it).  With no node
+  // inside, the set is dropped and the handle is -1 (-2 here: not an error); its number is
+  // used up all the same, as the reference's diagnostic count is.
+  int tracer_init(lcsdata_t Tint, lcsdata_t h, const char *label, std::string &msg) {
+    if (!(h > lcsdata_t(0)) || !(Tint > lcsdata_t(0))) {
+      msg = "diagnostic_init: T and h must be positive";
+      return -1;
+    }
+    DiagT d;
+    d.handle = (int)diags_.size() + 1;
+    d.type = LP_TRACER;
+    d.T_ = Tint;
+    d.h = h;
+    d.dt_factor = lcsdata_t(1);
+    d.label = label ? label : "";
+    while (!d.label.empty() && d.label.back() == ' ') d.label.pop_back();
+    const lcsdata_t X = (lcsdata_t)opt_->tracer_x, Y = (lcsdata_t)opt_->tracer_y, Z = (lcsdata_t)opt_->tracer_z;
+    const lcsdata_t R = (lcsdata_t)opt_->tracer_r;
+    std::vector<T> px[3];
+    std::vector<int> pn[3];
+    for (int k = 1; k <= n_[2]; k++)
+      for (int j = 1; j <= n_[1]; j++)
+        for (int i = 1; i <= n_[0]; i++) {
+          const lcsdata_t dx = hg_.lt[0][i] - X, dy = hg_.lt[1][j] - Y, dz = hg_.lt[2][k] - Z;
+          const lcsdata_t r = std::sqrt(dx * dx + dy * dy + dz * dz);
+          if (!(r <= R)) continue;
+          const int nd[3] = {i, j, k};
+          for (int a = 0; a < 3; a++) {
+            px[a].push_back((T)hg_.lt[a][nd[a]]);
+            pn[a].push_back(nd[a]);
+          }
+        }
+    d.np = (int)px[0].size();
+    if (d.np == 0) {
+      d.active = false;
+      diags_.push_back(std::move(d));
+      return -2;
+    }
+    std::vector<T> zero(d.np, T(0));
+    for (int c = 0; c < 3; c++) {
+      if (!(d.P.x[c] = upload<T>(px[c], msg))) return -1;
+      if (!(d.P.dx[c] = upload<T>(zero, msg))) return -1;
+      if (!(d.P.no[c] = upload<int>(pn[c], msg))) return -1;
+    }
+    diags_.push_back(std::move(d));
+    return diags_.back().handle;
+  }
+
+  // write_tracers (src/io_nohdf5_m.f90:138-181): POINT-packed positions, one particle per line
+  bool enqueue_tracer_output(DiagT &d, std::string &msg) {
+    const long long findex = (long long)fnint((double)(t_np1_ / d.h));
+    std::string idx;
+    if (!lcs_file_index(findex, idx)) {
+      msg = "ERROR: unsupported range for file index, " + std::to_string(findex);
+      return false;
+    }
+    if (!writer_) writer_.reset(new LcsWriter());
+    OutputJob job;
+    job.path = "./cfd2lcs_output/" + d.label + "_" + idx + ".dat";
+    job.points = d.np;
+    const std::string lab = d.label + "-LP";
+    std::string h = "TITLE = \"" + lab + "\"\nVARIABLES =\n\"X\"\n\"Y\"\n\"Z\"\nZONE\nT = \"" + lab + "\"\n";
+    char tbuf[32], line[160];
+    format_es((double)t_np1_, 18, 4, tbuf);
+    tbuf[18] = 0;
+    std::snprintf(line, sizeof(line), "STRANDID = %010d, SOLUTIONTIME = %s\n", d.handle + 1, tbuf);
+    h += line;
+    std::snprintf(line, sizeof(line), "I = %010d J = %010d K = %010d\n", d.np, 1, 1);
+    h += line;
+    h += "ZONETYPE = Ordered, DATAPACKING = POINT\n";
+    job.header = h;
+    const size_t blk = ((size_t)d.np * sizeof(T) + 255) / 256 * 256;
+    void *buf = nullptr;
+    const int bi = writer_->acquire(std::max<size_t>(3 * blk, 1), &buf, msg);
+    if (bi < 0) return false;
+    for (int c = 0; c < 3; c++) {
+      OutputBlock b;
+      b.kind = sizeof(T) == 8 ? OutputBlock::STAGED_F64 : OutputBlock::STAGED_F32;
+      b.offset = c * blk;
+      job.blocks.push_back(b);
+      if (d.np) CK(cudaMemcpyAsync(static_cast<char *>(buf) + b.offset, d.P.x[c], d.np * sizeof(T), cudaMemcpyDeviceToHost, stream_));
+    }
+    cudaEvent_t ev;
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(ev, stream_));
+    job.ready = ev;
+    job.buffer = bi;
+    writer_->submit(std::move(job));
+    return true;
   }
 
   bool err_msg(std::string &msg) {
@@ -974,10 +1104,9 @@ class Engine : public EngineBase {
   }
 
   template <int INTERP, bool F>
-  void fwd_integ(const SplineAxes<T> &sa, const VelFields<TV> &V, Particles<T> P, StageTimes S, T dt) {
-    const int blk = 256, grd = (int)((N_ + blk - 1) / blk);
+  void fwd_integ(const SplineAxes<T> &sa, const VelFields<TV> &V, Particles<T> P, StageTimes S, T dt, int np) {
+    const int blk = 256, grd = (int)((np + blk - 1) / blk);
     int *err = &red_->err;
-    const int np = (int)N_;
     counters_.kernel_launches++;
     switch (opt_->integrator) {
       case 0: k_fwd_subcycle<T, TV, EULER_, INTERP, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, P, S, dt, np, err); break;
@@ -988,12 +1117,15 @@ class Engine : public EngineBase {
     }
   }
 
-  bool launch_fwd(int iv, const SplineAxes<T> &sa, const VelFields<TV> &V, Particles<T> P, StageTimes S, T dt, std::string &msg) {
+  bool launch_fwd(int iv, const SplineAxes<T> &sa, const VelFields<TV> &V, Particles<T> P, StageTimes S, T dt, std::string &msg,
+                  long np = -1) {
     const bool F = dg_.P.has_flags != 0;
-    if (iv == INTERP_NEAREST) F ? fwd_integ<INTERP_NEAREST, true>(sa, V, P, S, dt) : fwd_integ<INTERP_NEAREST, false>(sa, V, P, S, dt);
-    else if (iv == INTERP_LINEAR) F ? fwd_integ<INTERP_LINEAR, true>(sa, V, P, S, dt) : fwd_integ<INTERP_LINEAR, false>(sa, V, P, S, dt);
-    else if (iv == INTERP_SPLINE4) F ? fwd_integ<INTERP_SPLINE4, true>(sa, V, P, S, dt) : fwd_integ<INTERP_SPLINE4, false>(sa, V, P, S, dt);
-    else F ? fwd_integ<INTERP_SPLINE, true>(sa, V, P, S, dt) : fwd_integ<INTERP_SPLINE, false>(sa, V, P, S, dt);
+    const int n = (int)(np < 0 ? N_ : np);
+    if (n == 0) return true;
+    if (iv == INTERP_NEAREST) F ? fwd_integ<INTERP_NEAREST, true>(sa, V, P, S, dt, n) : fwd_integ<INTERP_NEAREST, false>(sa, V, P, S, dt, n);
+    else if (iv == INTERP_LINEAR) F ? fwd_integ<INTERP_LINEAR, true>(sa, V, P, S, dt, n) : fwd_integ<INTERP_LINEAR, false>(sa, V, P, S, dt, n);
+    else if (iv == INTERP_SPLINE4) F ? fwd_integ<INTERP_SPLINE4, true>(sa, V, P, S, dt, n) : fwd_integ<INTERP_SPLINE4, false>(sa, V, P, S, dt, n);
+    else F ? fwd_integ<INTERP_SPLINE, true>(sa, V, P, S, dt, n) : fwd_integ<INTERP_SPLINE, false>(sa, V, P, S, dt, n);
     CK(cudaGetLastError());
     return true;
   }

@@ -29,6 +29,9 @@ struct Options {
   // reference's FLOWMAP_IO, VELOCITY_IO and BCFLAG_IO defaults (src/data_m.f90:44-54)
   int write_flowmap = 1, write_velocity = 1, write_bcflag = 0;
   int write_lcs = 0;        // extension: write the files at all (off by default)
+  // LP_TRACER injection sphere (cfd2lcs_set_param TRACER_INJECT_*, src/data_m.f90:86-89):
+  // the default centre is huge(1.0), so no node is inside until the caller sets it
+  double tracer_x = 1.0e300, tracer_y = 1.0e300, tracer_z = 1.0e300, tracer_r = 0.0;
   int write_lcs_async = 0;  // extension: let a frame's file complete after cfd2lcs_update returns
 };
 
@@ -64,6 +67,9 @@ class EngineBase {
   virtual const lcsdata_t *ftle_device_ptr(int handle) = 0;
   // velocity invariants of the last frame (VELOCITY_INVARIANTS): 5 x interior (Q, D, C, H, L2)
   virtual bool get_invariants(int handle, lcsdata_t *out, std::string &msg) = 0;
+  // LP_TRACER: particle count (-1 for another handle) and positions (x block, y, z)
+  virtual int tracer_count(int handle) = 0;
+  virtual bool get_tracers(int handle, lcsdata_t *out, std::string &msg) = 0;
   virtual bool sync_errors(std::string &msg) = 0;
   // Recomputes the latest FTLE frame of a diagnostic into caller-owned device buffers
   // without allocating (pointer table in a static device array, see engine.cu).

@@ -111,8 +111,31 @@ __global__ void __launch_bounds__(256) k_ingest(DevGrid<T> g, const U *__restric
 // fm_new = (fm_old(x_dep) + (x_dep - x_grid)) * mask, then the flow-map ghost ring
 // (exchange_sdata + set_flowmap_bc) from the boundary threads.
 // ---------------------------------------------------------------------------------------
+// Resident blocks of 256 threads per SM asked of the compiler for the two advection kernels
+// (a register cap of 65536 / (256 * blocks)); 1 leaves the register count to the compiler.
+#ifndef CFD2LCS_SL_MINB_LINEAR
+#define CFD2LCS_SL_MINB_LINEAR 1
+#endif
+#ifndef CFD2LCS_SL_MINB_SPLINE
+#define CFD2LCS_SL_MINB_SPLINE 1
+#endif
+#ifndef CFD2LCS_FWD_MINB_LINEAR
+#define CFD2LCS_FWD_MINB_LINEAR 1
+#endif
+#ifndef CFD2LCS_FWD_MINB_SPLINE
+#define CFD2LCS_FWD_MINB_SPLINE 1
+#endif
+template <int INTERP>
+constexpr int sl_min_blocks() {
+  return INTERP >= INTERP_SPLINE ? CFD2LCS_SL_MINB_SPLINE : CFD2LCS_SL_MINB_LINEAR;
+}
+template <int INTERP>
+constexpr int fwd_min_blocks() {
+  return INTERP >= INTERP_SPLINE ? CFD2LCS_FWD_MINB_SPLINE : CFD2LCS_FWD_MINB_LINEAR;
+}
+
 template <typename T, typename TV, int INTEG, int INTERP, bool HAS_FLAGS>
-__global__ void __launch_bounds__(256) k_sl_subcycle(DevGrid<T> g, SplineAxes<T> sa, VelFields<TV> V, FieldPtrs<T> fmo,
+__global__ void __launch_bounds__(256, sl_min_blocks<INTERP>()) k_sl_subcycle(DevGrid<T> g, SplineAxes<T> sa, VelFields<TV> V, FieldPtrs<T> fmo,
                                                       FieldPtrsW<T> fmn, StageTimes S, T dt, int *err) {
   int i, j, k;
   if (!node_of_thread(g.P.n, i, j, k)) return;
@@ -150,7 +173,7 @@ __global__ void __launch_bounds__(256) k_sl_subcycle(DevGrid<T> g, SplineAxes<T>
 // periodic wrap of exchange_lpdata.  Thread q advances the particle in storage slot q.
 // ---------------------------------------------------------------------------------------
 template <typename T, typename TV, int INTEG, int INTERP, bool HAS_FLAGS>
-__global__ void __launch_bounds__(256) k_fwd_subcycle(DevGrid<T> g, SplineAxes<T> sa, VelFields<TV> V, Particles<T> P, StageTimes S,
+__global__ void __launch_bounds__(256, fwd_min_blocks<INTERP>()) k_fwd_subcycle(DevGrid<T> g, SplineAxes<T> sa, VelFields<TV> V, Particles<T> P, StageTimes S,
                                                        T dt, int np, int *err) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= np) return;

@@ -170,6 +170,26 @@ bool LcsWriter::write_job(const OutputJob &job, const char *staging, std::string
   }
   std::setvbuf(fp, nullptr, _IOFBF, 1 << 22);
   bool ok = std::fwrite(job.header.data(), 1, job.header.size(), fp) == job.header.size();
+  if (job.points >= 0) {
+    // write_tracers: '(3ES14.6)' per particle
+    std::string out;
+    out.reserve((size_t)job.points * (3 * kWidth + 1));
+    char cell[kWidth];
+    for (long q = 0; q < job.points && ok; q++) {
+      for (int c = 0; c < 3; c++) {
+        const OutputBlock &b = job.blocks[c];
+        const double v = b.kind == OutputBlock::STAGED_F64 ? reinterpret_cast<const double *>(staging + b.offset)[q]
+                                                           : (double)reinterpret_cast<const float *>(staging + b.offset)[q];
+        format_es(v, kWidth, kDigits, cell);
+        out.append(cell, kWidth);
+      }
+      out.push_back('\n');
+    }
+    if (ok && !out.empty()) ok = std::fwrite(out.data(), 1, out.size(), fp) == out.size();
+    if (std::fclose(fp) != 0) ok = false;
+    if (!ok) err = "write_lcs: write failed for " + job.path;
+    return ok;
+  }
   const long ni = job.n[0], nj = job.n[1], nk = job.n[2];
   const long count = ni * nj * nk;
   const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));

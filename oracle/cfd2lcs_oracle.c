@@ -108,6 +108,7 @@ typedef struct {
     int *no[3], *no_scfd[3];
     int *flag;
     sr1_t fm;
+    real lifetime; /* time advected (integrate_lp, lp_motion_m.f90:332) */
 } lp_t;
 
 typedef struct {
@@ -120,6 +121,7 @@ typedef struct {
     real *l2margin; /* checker aid: middle eigenvalue / largest magnitude (how close L2 is to a tie) */
     sr1_t fm_out; /* composed flow map of the last FTLE frame (written by write_lcs) */
     char label[136]; /* lcs%label, trimmed */
+    int dead;        /* an LP_TRACER set that was never injected or outlived T (destroy_lcs) */
     int nslot;
     real **slot[3]; /* slot[c][s] -> interior values of stored sub-flow map */
     int *written;
@@ -151,6 +153,10 @@ static struct {
      * default to TRUE (data_m.f90:44-49), kept here as their negations so that zeroed state
      * means the defaults */
     int write_lcs, no_flowmap_io, no_velocity_io, bcflag_io;
+    /* TRACER_INJECT_X/Y/Z/RADIUS (data_m.f90:86-89: the centre defaults to huge(1.0), the
+     * radius to 0); tracer_set marks the ones given */
+    real tracer_c[3], tracer_r;
+    int tracer_set[3];
     char outdir[512];
 } S = {0, "", RK2, LINEAR, 0, 0, 0, (real)0.5, 0};
 
@@ -1352,6 +1358,7 @@ static void update_lp(lp_t *lp) {
     real lp_time = S.t_n;
     for (int sc = 1; sc <= nsub && !S.error; sc++) {
         integrate_lp(lp, &lp_time, dt);
+        lp->lifetime = lp->lifetime + (real)fabs((double)dt);
         track_lp2node(&S.g, lp, lp->no_scfd);
     }
 }
@@ -1775,8 +1782,37 @@ static void write_lcs(lcs_t *L, int ustep) {
     fclose(fp);
 }
 
+/* write_tracers (io_nohdf5_m.f90:138-181) at one rank: POINT packing, x y z per particle;
+ * STRANDID is lp%id + 1 (the particle set's number, here the diagnostic's). */
+static void write_tracers(lcs_t *L) {
+    long long findex = (long long)fnint(S.t_np1 / L->h);
+    if (findex < -999999999LL || findex > 999999999LL) { latch("ERROR: unsupported range for file index"); return; }
+    char idx[32];
+    if (findex >= 1000 && findex <= 9999) snprintf(idx, sizeof idx, "%010lld", findex);
+    else snprintf(idx, sizeof idx, "%lld", findex);
+    char path[1024];
+    snprintf(path, sizeof path, "%s/%s_%s.dat", S.outdir[0] ? S.outdir : "./cfd2lcs_output", L->label, idx);
+    FILE *fp = fopen(path, "w");
+    if (!fp) { latch("write_lcs: cannot open the output file"); return; }
+    char tfield[24];
+    es_edit((double)S.t_np1, 18, 4, tfield);
+    tfield[18] = 0;
+    fprintf(fp, "TITLE = \"%s-LP\"\nVARIABLES =\n\"X\"\n\"Y\"\n\"Z\"\nZONE\nT = \"%s-LP\"\n", L->label, L->label);
+    fprintf(fp, "STRANDID = %010d, SOLUTIONTIME = %s\n", L->id + 1, tfield);
+    fprintf(fp, "I = %010d J = %010d K = %010d\nZONETYPE = Ordered, DATAPACKING = POINT\n", L->lp.np, 1, 1);
+    char cell[16];
+    for (int ip = 0; ip < L->lp.np; ip++) {
+        for (int c = 0; c < 3; c++) {
+            es_edit((double)L->lp.xp[c][ip], 14, 6, cell);
+            fwrite(cell, 1, 14, fp);
+        }
+        fputc('\n', fp);
+    }
+    fclose(fp);
+}
+
 /* ------------------------------------------------------------------------------------
- * Entry points (cfd2lcs.f90:2-682 semantics, one rank, no output files).
+ * Entry points (cfd2lcs.f90:2-682 semantics, one rank; output files only with WRITE_LCS).
  * ------------------------------------------------------------------------------------ */
 #define EXPORT __attribute__((visibility("default")))
 
@@ -1859,13 +1895,80 @@ EXPORT void orc_init(const int n[3], const int offset[3], const real *x, const r
 /* directory of the output files (the reference's ./cfd2lcs_output) */
 EXPORT void orc_set_output_dir(const char *dir) { snprintf(S.outdir, sizeof S.outdir, "%s", dir ? dir : ""); }
 
+/* LP_TRACER: init_lp_tracer (lp_m.f90:116-226) and diagnostic_init (cfd2lcs.f90:327-337):
+ * one tracer per node with r <= TRACER_INJECT_RADIUS from the injection point, in node
+ * order; none inside: the set is destroyed (its number used up) and the handle is -1. */
+static int tracer_init(real T, real h, const char *label) {
+    const dims_t *d = &S.g.d;
+    lcs_t *L = (lcs_t *)calloc(1, sizeof(lcs_t));
+    L->id = S.nlcs + 1;
+    L->diagnostic = LP_TRACER;
+    L->T = T;
+    L->h = h;
+    snprintf(L->label, sizeof L->label, "%s", label ? label : "");
+    for (size_t e = strlen(L->label); e > 0 && L->label[e - 1] == ' '; e--) L->label[e - 1] = 0;
+    S.lcs[S.nlcs++] = L;
+    real c0[3];
+    for (int a = 0; a < 3; a++) c0[a] = S.tracer_set[a] ? S.tracer_c[a] : (real)R_HUGE;
+    int np = 0;
+    for (int pass = 0; pass < 2; pass++) {
+        int ip = 0;
+        for (int k = 1; k <= d->nk; k++)
+            for (int j = 1; j <= d->nj; j++)
+                for (int i = 1; i <= d->ni; i++) {
+                    long p = PX(d, i, j, k);
+                    real dx = S.g.grid.c[0][p] - c0[0], dy = S.g.grid.c[1][p] - c0[1], dz = S.g.grid.c[2][p] - c0[2];
+                    real r = (real)sqrt((double)(dx * dx + dy * dy + dz * dz));
+                    if (!(r <= S.tracer_r)) continue;
+                    if (pass == 1) {
+                        for (int c = 0; c < 3; c++) L->lp.xp[c][ip] = S.g.grid.c[c][p];
+                        L->lp.no[0][ip] = i; L->lp.no[1][ip] = j; L->lp.no[2][ip] = k;
+                        /* the educated guess of init_lp_tracer is the node itself at resolution 0 */
+                        L->lp.no_scfd[0][ip] = i; L->lp.no_scfd[1][ip] = j; L->lp.no_scfd[2][ip] = k;
+                        L->lp.flag[ip] = LP_UNKNOWN;
+                    }
+                    ip++;
+                }
+        if (pass == 0) {
+            np = ip;
+            if (np == 0) { L->dead = 1; return -1; }
+            lp_alloc(&L->lp, np);
+            sr1_alloc(&L->lp.fm, d);
+        }
+    }
+    L->lp.direction = FWD;
+    L->lp.dt_factor = (real)1.0;
+    L->lp.recursive_tracking = 1;
+    L->lp.lifetime = 0;
+    track_lp2node(&S.g, &L->lp, L->lp.no_scfd);
+    return L->id;
+}
+
+EXPORT int orc_tracer_count(int handle) {
+    for (int i = 0; i < S.nlcs; i++)
+        if (S.lcs[i]->id == handle) return S.lcs[i]->diagnostic == LP_TRACER ? S.lcs[i]->lp.np : -1;
+    return -1;
+}
+
+EXPORT int orc_get_tracers(int handle, real *out) {
+    for (int i = 0; i < S.nlcs; i++)
+        if (S.lcs[i]->id == handle && S.lcs[i]->diagnostic == LP_TRACER) {
+            const lp_t *lp = &S.lcs[i]->lp;
+            for (int c = 0; c < 3; c++)
+                for (int q = 0; q < lp->np; q++) out[(long)c * lp->np + q] = lp->xp[c][q];
+            return 0;
+        }
+    return 1;
+}
+
 EXPORT int orc_diagnostic_init(int type, int resolution, real T, real h, const char *label) {
     if (S.error) return -1;
     if (!S.inited) { latch("diagnostic_init before init"); return -1; }
     if (S.nlcs >= MAXLCS) { latch("diagnostic_init: too many diagnostics"); return -1; }
     if (resolution != 0) { latch("diagnostic_init: resolution /= 0 (new_sgrid_from_sgrid) is not restated"); return -1; }
+    if (type == LP_TRACER) return tracer_init(T, h, label);
     if (type != FTLE_FWD && type != FTLE_BKWD) {
-        latch("diagnostic_init: bad lcs_type (LP_TRACER is not restated)");
+        latch("ERROR, bad specification for lcs_type. Options are: FTLE_FWD, FTLE_BKWD, LP_TRACER");
         return -1;
     }
     lcs_t *L = (lcs_t *)calloc(1, sizeof(lcs_t));
@@ -1926,13 +2029,20 @@ EXPORT void orc_update(const int n[3], const real *u, const real *v, const real 
     exchange_self(&S.g, S.u_np1.c, 3, 1, 0);
     set_velocity_bc(&S.g, &S.u_np1);
     for (int i = 0; i < S.nlcs && !S.error; i++) {
+        if (S.lcs[i]->dead) continue;
         lp_t *lp = &S.lcs[i]->lp;
         if (lp->direction == FWD) update_lp(lp);
         else update_flowmap_sl(lp);
     }
     for (int i = 0; i < S.nlcs && !S.error; i++) {
         lcs_t *L = S.lcs[i];
+        if (L->dead) continue;
         if ((long long)(S.t_np1 / L->h) == (long long)(S.t_n / L->h)) continue;
+        if (L->diagnostic == LP_TRACER) { /* cfd2lcs.f90:225-231 */
+            if (S.write_lcs) write_tracers(L);
+            if (L->lp.lifetime > L->T) L->dead = 1;
+            continue;
+        }
         if (L->diagnostic == FTLE_FWD) {
             /* exchange_lpmap: fm(no0) = dx */
             int ip = 0;
@@ -2002,9 +2112,11 @@ EXPORT void orc_set_option(const char *opt, int val) {
 EXPORT void orc_set_param(const char *p, real val) {
     if (S.error) return;
     if (!strcmp(p, "CFL")) S.cfl_max = val;
-    else if (!strcmp(p, "TRACER_INJECT_X") || !strcmp(p, "TRACER_INJECT_Y") || !strcmp(p, "TRACER_INJECT_Z") ||
-             !strcmp(p, "TRACER_INJECT_RADIUS")) {
-    } else latch("unknown libcfd2lcs parameter");
+    else if (!strcmp(p, "TRACER_INJECT_X")) { S.tracer_c[0] = val; S.tracer_set[0] = 1; }
+    else if (!strcmp(p, "TRACER_INJECT_Y")) { S.tracer_c[1] = val; S.tracer_set[1] = 1; }
+    else if (!strcmp(p, "TRACER_INJECT_Z")) { S.tracer_c[2] = val; S.tracer_set[2] = 1; }
+    else if (!strcmp(p, "TRACER_INJECT_RADIUS")) S.tracer_r = val;
+    else latch("unknown libcfd2lcs parameter");
 }
 
 static lcs_t *find_lcs(int handle) {

@@ -56,6 +56,10 @@ class Oracle:
         L.orc_get_invariants.argtypes = [C.c_int, P]
         L.orc_get_invariants.restype = C.c_int
         L.orc_set_output_dir.argtypes = [C.c_char_p]
+        L.orc_tracer_count.argtypes = [C.c_int]
+        L.orc_tracer_count.restype = C.c_int
+        L.orc_get_tracers.argtypes = [C.c_int, P]
+        L.orc_get_tracers.restype = C.c_int
         L.orc_get_l2margin.argtypes = [C.c_int, P]
         L.orc_get_l2margin.restype = C.c_int
         L.orc_get_particles.argtypes = [C.c_int, P]
@@ -136,6 +140,14 @@ class Oracle:
         out = np.zeros(5 * int(np.prod(self.n)), dtype=self.dtype)
         assert self.lib.orc_get_invariants(handle, self._p(out)) == 0
         return out.reshape((5,) + tuple(self.n[::-1])).transpose(0, 3, 2, 1)
+
+    def tracers(self, handle):
+        """Positions of an LP_TRACER set, shape (3, count)."""
+        n = int(self.lib.orc_tracer_count(int(handle)))
+        assert n >= 0
+        out = np.zeros(3 * n, dtype=self.dtype)
+        assert self.lib.orc_get_tracers(int(handle), self._p(out)) == 0
+        return out.reshape(3, n)
 
     def set_output_dir(self, path: str):
         """Directory of the write_lcs files (WRITE_LCS); the reference's ./cfd2lcs_output."""
