@@ -111,19 +111,24 @@ __global__ void __launch_bounds__(256) k_ingest(DevGrid<T> g, const U *__restric
 // fm_new = (fm_old(x_dep) + (x_dep - x_grid)) * mask, then the flow-map ghost ring
 // (exchange_sdata + set_flowmap_bc) from the boundary threads.
 // ---------------------------------------------------------------------------------------
-// Resident blocks of 256 threads per SM asked of the compiler for the two advection kernels
-// (a register cap of 65536 / (256 * blocks)); 1 leaves the register count to the compiler.
+// Resident blocks of 256 threads per SM asked of the compiler for the two advection kernels,
+// i.e. a register cap of 65536 / (256 * blocks).  Without a cap ptxas gives the FP64 RK3 B-spline
+// kernels 104 registers (2 blocks, 16 warps per SM); a minimum of 1 block lets it take up to
+// 255.  Measured on B200 (ABC 256^3 RK3 CUBIC, turbulence 512^3 RK2 LINEAR): 4 blocks (64
+// registers) for the B-spline kernels took the FP64 backward subcycle from 5.02 to 4.32 ms and
+// the forward one from 8.85 to 7.52 ms despite a few spilled registers; 5 blocks (48 registers)
+// suits the LINEAR backward kernel (6 blocks, 40 registers, was slower).
 #ifndef CFD2LCS_SL_MINB_LINEAR
-#define CFD2LCS_SL_MINB_LINEAR 1
+#define CFD2LCS_SL_MINB_LINEAR 5
 #endif
 #ifndef CFD2LCS_SL_MINB_SPLINE
-#define CFD2LCS_SL_MINB_SPLINE 1
+#define CFD2LCS_SL_MINB_SPLINE 4
 #endif
 #ifndef CFD2LCS_FWD_MINB_LINEAR
-#define CFD2LCS_FWD_MINB_LINEAR 1
+#define CFD2LCS_FWD_MINB_LINEAR 4
 #endif
 #ifndef CFD2LCS_FWD_MINB_SPLINE
-#define CFD2LCS_FWD_MINB_SPLINE 1
+#define CFD2LCS_FWD_MINB_SPLINE 4
 #endif
 template <int INTERP>
 constexpr int sl_min_blocks() {
