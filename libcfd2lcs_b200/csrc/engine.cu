@@ -1334,8 +1334,13 @@ class Engine : public EngineBase {
   // Re-sorts the particle slots by grid cell (32 x 8 tiles, x fastest) every kSortInterval
   // subcycles, so that the particles of a block gather neighbouring spline taps as the SL
   // kernel's blocks do.  Results do not depend on the order: every particle is advanced
-  // independently and the snapshot reads it back through the inverse map.
-  static constexpr int kSortInterval = 6;
+  // independently and the snapshot reads it back through the inverse map.  Measured on B200
+  // (ABC 256^3, RK3 CUBIC, FP64): every 6 / 4 / 3 / 2 subcycles gave 332.9 / 330.9 / 328.9 /
+  // 326.0 ms per update (the forward launch 7.55 -> 6.94 ms against 0.9 ms per sort).
+#ifndef CFD2LCS_SORT_INTERVAL
+#define CFD2LCS_SORT_INTERVAL 2
+#endif
+  static constexpr int kSortInterval = CFD2LCS_SORT_INTERVAL;
   bool sort_particles(DiagT &d, std::string &msg) {
     const int np = (int)N_, blk = 256, grd = (np + blk - 1) / blk;
     const int ncell = (int)sort_key_space(n_);
