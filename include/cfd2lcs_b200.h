@@ -48,6 +48,13 @@ void cfd2lcs_update_device_c(int n[3], const lcsdata_t *d_u, const lcsdata_t *d_
  * 1 for an unknown handle, no frame yet or the option off. */
 int cfd2lcs_get_invariants_c(int lcs_handle, lcsdata_t *inv);
 
+/* Points per direction of a diagnostic's lcs grid.  With resolution /= 0 in
+ * cfd2lcs_diagnostic_init (new_sgrid_from_sgrid, src/sgrid_m.f90:446-761) the FTLE field and
+ * flow map live on a refined (res > 0: res points between neighbouring nodes) or coarsened
+ * (res < 0: every (|res|+1)-th node) copy of the grid, and cfd2lcs_get_ftle_c /
+ * cfd2lcs_get_flowmap_c return n[0]*n[1]*n[2] values of that grid.  0 on success. */
+int cfd2lcs_diagnostic_size_c(int lcs_handle, int n[3]);
+
 /* LP_TRACER diagnostics (cfd2lcs_diagnostic_init with LP_TRACER after setting the
  * TRACER_INJECT_X/Y/Z/RADIUS parameters; init_lp_tracer, src/lp_m.f90:116-226): one tracer per
  * grid node inside the injection sphere, advected forward every update until its lifetime

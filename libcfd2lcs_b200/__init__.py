@@ -38,7 +38,7 @@ EXPORTED_SYMBOLS = [
     "cfd2lcs_finalize_c", "cfd2lcs_get_error_c", "cfd2lcs_reset_c", "cfd2lcs_get_ftle_c", "cfd2lcs_get_flowmap_c",
     "cfd2lcs_update_device_c", "cfd2lcs_ftle_device_ptr_c", "cfd2lcs_get_counters_c", "cfd2lcs_get_phase_times_c",
     "cfd2lcs_get_kernel_times_c", "cfd2lcs_reconstruct_noalloc_c", "cfd2lcs_get_invariants_c",
-    "cfd2lcs_tracer_count_c", "cfd2lcs_get_tracers_c",
+    "cfd2lcs_tracer_count_c", "cfd2lcs_get_tracers_c", "cfd2lcs_diagnostic_size_c",
     # batched form (include/cfd2lcs_b200.h)
     "cfd2lcs_batch_add_c", "cfd2lcs_batch_diagnostic_init_c", "cfd2lcs_batch_update_device_c", "cfd2lcs_batch_get_ftle_c",
     "cfd2lcs_batch_get_flowmap_c", "cfd2lcs_batch_get_counters_c", "cfd2lcs_batch_size_c", "cfd2lcs_batch_error_c",
@@ -93,6 +93,8 @@ def load(precision: str = "dp") -> C.CDLL:
     lib.cfd2lcs_get_flowmap_c.restype = C.c_int
     lib.cfd2lcs_get_invariants_c.argtypes = [C.c_int, P]
     lib.cfd2lcs_get_invariants_c.restype = C.c_int
+    lib.cfd2lcs_diagnostic_size_c.argtypes = [C.c_int, P]
+    lib.cfd2lcs_diagnostic_size_c.restype = C.c_int
     lib.cfd2lcs_tracer_count_c.argtypes = [C.c_int]
     lib.cfd2lcs_tracer_count_c.restype = C.c_int
     lib.cfd2lcs_get_tracers_c.argtypes = [C.c_int, P]
@@ -192,18 +194,28 @@ class Cfd2lcs:
         e = self.lib.cfd2lcs_get_error_c(buf, 512)
         return e, buf.value.decode()
 
+    def diag_size(self, handle):
+        """Points per direction of a diagnostic's lcs grid (differs from the grid's with
+        resolution /= 0)."""
+        n = np.zeros(3, dtype=np.int32)
+        if self.lib.cfd2lcs_diagnostic_size_c(int(handle), self._p(n)) != 0:
+            raise RuntimeError("unknown diagnostic handle")
+        return tuple(int(v) for v in n)
+
     def ftle(self, handle):
-        out = np.zeros(int(np.prod(self.n)), dtype=self.dtype)
+        n = self.diag_size(handle)
+        out = np.zeros(int(np.prod(n)), dtype=self.dtype)
         if self.lib.cfd2lcs_get_ftle_c(int(handle), self._p(out)) != 0:
             raise RuntimeError("no FTLE field for this handle yet")
-        return out.reshape(self.n, order="F")
+        return out.reshape(n, order="F")
 
     def flowmap(self, handle):
-        out = np.zeros(3 * int(np.prod(self.n)), dtype=self.dtype)
+        n = self.diag_size(handle)
+        out = np.zeros(3 * int(np.prod(n)), dtype=self.dtype)
         if self.lib.cfd2lcs_get_flowmap_c(int(handle), self._p(out)) != 0:
             raise RuntimeError("no flow map for this handle yet")
-        N = int(np.prod(self.n))
-        return np.stack([out[c * N:(c + 1) * N].reshape(self.n, order="F") for c in range(3)])
+        N = int(np.prod(n))
+        return np.stack([out[c * N:(c + 1) * N].reshape(n, order="F") for c in range(3)])
 
     def invariants(self, handle):
         """Q, D, C, H, L2 of the last frame (VELOCITY_INVARIANTS), shape (5, ni, nj, nk)."""

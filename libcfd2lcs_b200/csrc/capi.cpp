@@ -268,6 +268,12 @@ CFD2LCS_EXPORT int cfd2lcs_get_invariants_c(int lcs_handle, lcsdata_t *inv) {
   return lib.eng->get_invariants(lcs_handle, inv, m) ? 0 : 1;
 }
 
+CFD2LCS_EXPORT int cfd2lcs_diagnostic_size_c(int lcs_handle, int n[3]) {
+  Library &lib = L();
+  if (!lib.eng || !n) return 1;
+  return lib.eng->diagnostic_size(lcs_handle, n) ? 0 : 1;
+}
+
 CFD2LCS_EXPORT int cfd2lcs_tracer_count_c(int lcs_handle) {
   Library &lib = L();
   return lib.eng ? lib.eng->tracer_count(lcs_handle) : -1;

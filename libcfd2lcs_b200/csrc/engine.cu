@@ -62,6 +62,20 @@ struct SplineSet {
   SplineAxes<T> axes{};
 };
 
+// The lcs grid of a diagnostic with resolution /= 0 (new_sgrid_from_sgrid, src/sgrid_m.f90:
+// 446-761): its host set-up and device tables, each lcs node's position and solver-grid node
+// after tracking to the solver grid (init_lp + track_lp2node), and, for backward sets, the
+// working copy of those nodes (set_lp_bc clamps them in place during the updates).
+template <typename T>
+struct LcsGrid {
+  HostGrid<lcsdata_t> hg;
+  DevGrid<T> dg{};
+  long N = 0, ntot = 0;
+  T *pos[3] = {nullptr, nullptr, nullptr};
+  int *nos_reset[3] = {nullptr, nullptr, nullptr};
+  int *nos[3] = {nullptr, nullptr, nullptr};
+};
+
 template <typename T, typename TV>
 struct Diag {
   int handle = 0, type = 0;
@@ -97,6 +111,7 @@ struct Diag {
   int np = 0;
   lcsdata_t lifetime = 0;
   bool active = true;
+  std::shared_ptr<LcsGrid<T>> lg;  // refined / coarsened lcs grid (null: the solver grid)
 };
 
 }  // namespace
@@ -214,50 +229,7 @@ class Engine : public EngineBase {
     N_ = (long)n[0] * n[1] * n[2];
     ntot_ = hg_.ntot();
     // grid tables
-    GridParams<T> P;
-    const GridParams<lcsdata_t> &H = hg_.P;
-    for (int a = 0; a < 3; a++) {
-      P.n[a] = H.n[a];
-      P.per[a] = H.per[a];
-      for (int s = 0; s < 2; s++)
-        for (int e = 0; e < 2; e++) P.gx[a][s][e] = (T)H.gx[a][s][e];
-    }
-    P.sx = H.sx;
-    P.sxy = H.sxy;
-    P.single_axis = H.single_axis;
-    P.zquirk = H.zquirk;
-    for (int q = 0; q < 6; q++) P.bb[q] = (T)H.bb[q];
-    for (int d = 0; d < 27; d++)
-      for (int c = 0; c < 3; c++) P.ps[d][c] = (T)H.ps[d][c];
-    P.has_flags = H.has_flags;
-    P.maxtrack = H.maxtrack;
-    dg_.P = P;
-    for (int a = 0; a < 3; a++) {
-      if (!(dg_.lt[a] = upload(hg_.lt[a], msg))) return false;
-      if (!(dg_.li[a] = upload(hg_.li[a], msg))) return false;
-      if (!(dg_.invd[a] = upload(hg_.invd[a], msg))) return false;
-    }
-    dg_.flag = nullptr;
-    for (int a = 0; a < 3; a++) dg_.nrm[a] = nullptr;
-    if (H.has_flags) {
-      int8_t *f = arena_.alloc<int8_t>(hg_.flag.size(), msg);
-      if (!f) return false;
-      CK(cudaMemcpy(f, hg_.flag.data(), hg_.flag.size(), cudaMemcpyHostToDevice));
-      dg_.flag = f;
-      if (!hg_.bcnorm.empty()) {
-        for (int a = 0; a < 3; a++) {
-          std::vector<lcsdata_t> comp(hg_.bcnorm.begin() + (size_t)a * ntot_, hg_.bcnorm.begin() + (size_t)(a + 1) * ntot_);
-          if (!(dg_.nrm[a] = upload(comp, msg))) return false;
-        }
-      } else {
-        // flags without normals (e.g. only INFLOW/OUTFLOW or 2-D): a zero field keeps the
-        // kernels free of null checks
-        std::vector<lcsdata_t> zero(ntot_, lcsdata_t(0));
-        T *z0 = upload(zero, msg);
-        if (!z0) return false;
-        for (int a = 0; a < 3; a++) dg_.nrm[a] = z0;
-      }
-    }
+    if (!make_dev_grid(hg_, dg_, msg)) return false;
     // velocity levels (zero-initialised, as init_sr1 does, src/structured_m.f90:73-96)
     for (int l = 0; l < 2; l++)
       for (int c = 0; c < 3; c++) {
@@ -273,11 +245,13 @@ class Engine : public EngineBase {
   }
 
   int diagnostic_init(int type, int resolution, lcsdata_t Tint, lcsdata_t h, const char *label, std::string &msg) override {
-    if (resolution != 0) {
-      msg = "diagnostic_init: resolution /= 0 (a refined lcs grid, new_sgrid_from_sgrid) is not supported";
-      return -1;
+    if (type == LP_TRACER) {
+      if (resolution != 0) {
+        msg = "diagnostic_init: LP_TRACER with resolution /= 0 is not supported by this library";
+        return -1;
+      }
+      return tracer_init(Tint, h, label, msg);
     }
-    if (type == LP_TRACER) return tracer_init(Tint, h, label, msg);
     if (type != FTLE_FWD && type != FTLE_BKWD) {
       msg = "ERROR, bad specification for lcs_type. Options are: FTLE_FWD, FTLE_BKWD, LP_TRACER";
       return -1;
@@ -287,6 +261,8 @@ class Engine : public EngineBase {
       return -1;
     }
     DiagT d;
+    // lcs%sgrid (src/cfd2lcs.f90:302-310); new_sgrid_from_sgrid may reset the resolution to 0
+    if (resolution != 0 && !make_lcs_grid(d, type, resolution, msg)) return -1;
     d.handle = (int)diags_.size() + 1;
     d.type = type;
     d.label = label ? label : "";
@@ -295,29 +271,31 @@ class Engine : public EngineBase {
     d.h = h;
     d.dt_factor = type == FTLE_BKWD ? lcsdata_t(1) / lcsdata_t(std::max(1 + resolution, 1)) : lcsdata_t(1);
     d.nslot = (int)std::max(1L, fnint((double)(Tint / h)));
+    const long dn = dN(d), dt = dT(d);
     if (type == FTLE_BKWD) {
       for (int b = 0; b < 2; b++)
         for (int c = 0; c < 3; c++) {
-          if (!(d.fm[b][c] = arena_.alloc<T>(ntot_, msg))) return -1;
-          if (cudaMemsetAsync(d.fm[b][c], 0, ntot_ * sizeof(T), stream_) != cudaSuccess) return fail(msg, "memset");
+          if (!(d.fm[b][c] = arena_.alloc<T>(dt, msg))) return -1;
+          if (cudaMemsetAsync(d.fm[b][c], 0, dt * sizeof(T), stream_) != cudaSuccess) return fail(msg, "memset");
         }
+      if (d.lg && !reset_refined_nodes(d, msg)) return -1;
     } else {
       for (Particles<T> *Q : {&d.P, &d.P2}) {
         for (int c = 0; c < 3; c++) {
-          if (!(Q->x[c] = arena_.alloc<T>(N_, msg))) return -1;
-          if (!(Q->dx[c] = arena_.alloc<T>(N_, msg))) return -1;
-          if (!(Q->no[c] = arena_.alloc<int>(N_, msg))) return -1;
+          if (!(Q->x[c] = arena_.alloc<T>(dn, msg))) return -1;
+          if (!(Q->dx[c] = arena_.alloc<T>(dn, msg))) return -1;
+          if (!(Q->no[c] = arena_.alloc<int>(dn, msg))) return -1;
         }
-        if (!(Q->id = arena_.alloc<int>(N_, msg))) return -1;
+        if (!(Q->id = arena_.alloc<int>(dn, msg))) return -1;
       }
-      if (!(d.P.slot = arena_.alloc<int>(N_, msg))) return -1;
+      if (!(d.P.slot = arena_.alloc<int>(dn, msg))) return -1;
       d.P2.slot = d.P.slot;  // the inverse map is rewritten whole by every permutation
       const long ncell = sort_key_space(n_);
       if (ncell > (long)std::numeric_limits<int>::max()) {
         msg = "diagnostic_init: grid too large for the forward particle sort";
         return -1;
       }
-      if (!(d.pkey = arena_.alloc<unsigned>(N_, msg))) return -1;
+      if (!(d.pkey = arena_.alloc<unsigned>(dn, msg))) return -1;
       if (!(d.pcnt = arena_.alloc<int>(ncell, msg))) return -1;
       if (!(d.poffs = arena_.alloc<int>(ncell, msg))) return -1;
       if (!(d.ptsum = arena_.alloc<int>((ncell + SORT_TILE - 1) / SORT_TILE, msg))) return -1;
@@ -329,12 +307,12 @@ class Engine : public EngineBase {
     d.written.assign(d.nslot, 0);
     d.coef_deg.assign(d.nslot, 0);
     for (int s = 0; s < 3 * d.nslot; s++)
-      if (!(d.slot[s] = arena_.alloc<T>(ntot_, msg))) return -1;
+      if (!(d.slot[s] = arena_.alloc<T>(dt, msg))) return -1;
     if (!(d.slot_list_dev = arena_.alloc<T *>((size_t)3 * d.nslot, msg))) return -1;
     d.slot_list_host.assign((size_t)3 * d.nslot, nullptr);
     for (int c = 0; c < 3; c++)
-      if (!(d.composed[c] = arena_.alloc<T>(N_, msg))) return -1;
-    if (!(d.ftle = arena_.alloc<lcsdata_t>(N_, msg))) return -1;
+      if (!(d.composed[c] = arena_.alloc<T>(dn, msg))) return -1;
+    if (!(d.ftle = arena_.alloc<lcsdata_t>(dn, msg))) return -1;
     if (cudaStreamSynchronize(stream_) != cudaSuccess) return fail(msg, "sync");
     diags_.push_back(d);
     return d.handle;
@@ -463,6 +441,12 @@ class Engine : public EngineBase {
     const SplineAxes<T> sa = spline ? splines_[deg].axes : SplineAxes<T>{};
     const int iv = interp_variant(interp, sa);
 
+    if (spline)
+      for (auto &d : diags_)
+        if (d.lg) {
+          msg = "resolution /= 0 supports the NEAREST_NBR and LINEAR interpolators only";
+          return false;
+        }
     // --- per particle set: K1 (backward) / K6 (forward) --------------------------------
     for (auto &d : diags_) {
       if (!d.active) continue;
@@ -475,7 +459,7 @@ class Engine : public EngineBase {
       if (nsub < 1) nsub = 1;
       lcsdata_t dt = dt_f / (lcsdata_t)nsub;
       if (d.type == FTLE_BKWD) dt = lcsdata_t(-1) * dt;
-      const long long npart = d.type == LP_TRACER ? (long long)d.np : (long long)N_;
+      const long long npart = d.type == LP_TRACER ? (long long)d.np : (long long)dN(d);
       if (std::fabs((double)dt) > 0) {
         if (d.type != FTLE_BKWD) counters_.integrations_fwd += npart * nsub;
         else counters_.integrations_bkwd += npart * nsub;
@@ -505,7 +489,7 @@ class Engine : public EngineBase {
             for (int c = 0; c < 3; c++) fo.f[c] = d.fmcoef[c];
           }
           if (!mark(k0, msg)) return false;
-          if (!launch_sl(iv, sa, V, fo, fn, S, (T)dt, msg)) return false;
+          if (d.lg ? !launch_sl_refined(d, iv, V, fo, fn, S, (T)dt, msg) : !launch_sl(iv, sa, V, fo, fn, S, (T)dt, msg)) return false;
           if (!mark(k1, msg)) return false;
           spans_.push_back({k0, k1, kkind});
           d.cur ^= 1;
@@ -516,7 +500,7 @@ class Engine : public EngineBase {
         } else {
           if (sc % kSortInterval == 0 && !sort_particles(d, msg)) return false;
           if (!mark(k0, msg)) return false;
-          if (!launch_fwd(iv, sa, V, d.P, S, (T)dt, msg)) return false;
+          if (!launch_fwd(iv, sa, V, d.P, S, (T)dt, msg, dN(d))) return false;
           if (!mark(k1, msg)) return false;
           spans_.push_back({k0, k1, kkind});
         }
@@ -530,6 +514,10 @@ class Engine : public EngineBase {
     for (auto &d : diags_) {
       if (!d.active) continue;
       if ((long)(t_np1_ / d.h) == (long)(t_n_ / d.h)) continue;
+      if (d.lg && (opt_->velocity_invariants || opt_->write_lcs)) {
+        msg = "VELOCITY_INVARIANTS and WRITE_LCS are not supported for diagnostics with resolution /= 0";
+        return false;
+      }
       if (d.type == LP_TRACER) {
         // write_lcs, then the end of the tracers' lifetime (src/cfd2lcs.f90:225-231)
         if (opt_->write_lcs && !enqueue_tracer_output(d, msg)) return false;
@@ -591,7 +579,8 @@ class Engine : public EngineBase {
       if (!mark(f7, msg)) return false;
       // reset_lp: particles back to the grid, flow map to zero (src/cfd2lcs.f90:208-209)
       if (d.type == FTLE_BKWD) {
-        for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(d.fm[d.cur][c], 0, ntot_ * sizeof(T), stream_));
+        for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(d.fm[d.cur][c], 0, dT(d) * sizeof(T), stream_));
+        if (d.lg && !reset_refined_nodes(d, msg)) return false;
       } else {
         launch_reset(d);
       }
@@ -654,6 +643,10 @@ class Engine : public EngineBase {
       msg = "reconstruct_noalloc: unknown handle or no FTLE frame yet";
       return false;
     }
+    if (d->lg) {
+      msg = "reconstruct_noalloc: diagnostics with resolution /= 0 are not supported";
+      return false;
+    }
     const int m = (int)d->last_order.size();
     if (m > NOALLOC_MAX_SUBMAPS) {
       msg = "reconstruct_noalloc: the frame composes " + std::to_string(m) + " sub-flow maps, more than the maximum of " +
@@ -705,7 +698,7 @@ class Engine : public EngineBase {
       return false;
     }
     CK(cudaStreamSynchronize(stream_));
-    CK(cudaMemcpy(out, d->ftle, N_ * sizeof(lcsdata_t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(out, d->ftle, dN(*d) * sizeof(lcsdata_t), cudaMemcpyDeviceToHost));
     return true;
   }
 
@@ -716,10 +709,11 @@ class Engine : public EngineBase {
       return false;
     }
     CK(cudaStreamSynchronize(stream_));
-    std::vector<T> tmp(N_);
+    const long nd = dN(*d);
+    std::vector<T> tmp(nd);
     for (int c = 0; c < 3; c++) {
-      CK(cudaMemcpy(tmp.data(), d->composed[c], N_ * sizeof(T), cudaMemcpyDeviceToHost));
-      for (long q = 0; q < N_; q++) out[c * N_ + q] = (lcsdata_t)tmp[q];
+      CK(cudaMemcpy(tmp.data(), d->composed[c], nd * sizeof(T), cudaMemcpyDeviceToHost));
+      for (long q = 0; q < nd; q++) out[c * nd + q] = (lcsdata_t)tmp[q];
     }
     return true;
   }
@@ -732,6 +726,13 @@ class Engine : public EngineBase {
     }
     CK(cudaStreamSynchronize(stream_));
     for (int q = 0; q < 5; q++) CK(cudaMemcpy(out + (size_t)q * N_, d->inv[q], N_ * sizeof(lcsdata_t), cudaMemcpyDeviceToHost));
+    return true;
+  }
+
+  bool diagnostic_size(int handle, int n[3]) override {
+    DiagT *d = find(handle);
+    if (!d) return false;
+    for (int a = 0; a < 3; a++) n[a] = d->lg ? d->lg->dg.P.n[a] : n_[a];
     return true;
   }
 
@@ -1076,6 +1077,177 @@ class Engine : public EngineBase {
     return INTERP_SPLINE;
   }
 
+  const DevGrid<T> &dgrid(const DiagT &d) const { return d.lg ? d.lg->dg : dg_; }
+  long dN(const DiagT &d) const { return d.lg ? d.lg->N : N_; }
+  long dT(const DiagT &d) const { return d.lg ? d.lg->ntot : ntot_; }
+  static dim3 node_grid(const DevGrid<T> &g) { return dim3((g.P.n[0] + 31) / 32, (g.P.n[1] + 7) / 8, g.P.n[2]); }
+
+  // new_sgrid_from_sgrid (src/sgrid_m.f90:446-761) for this library's tensor-product grids,
+  // per axis: res > 0 puts res points between neighbouring nodes, x(ii) + dx * ir with
+  // dx = (x(ii+1) - x(ii)) / (res+1) (the ghost image past the last node where the axis is
+  // periodic, no points past it otherwise); res < 0 keeps every (|res|+1)-th node; singleton
+  // axes stay.  Each new point inherits the flag of the node it starts from.  |res| >= n on a
+  // non-singleton axis resets res to 0 (no new grid), as the reference does.  The new grid
+  // goes through the same host set-up as the solver grid, then every lcs node is tracked to
+  // the solver grid.
+  bool make_lcs_grid(DiagT &d, int type, int &res, std::string &msg) {
+    for (int a = 0; a < 3; a++)
+      if (n_[a] > 1 && std::abs(res) >= n_[a]) res = 0;
+    if (res == 0) return true;
+    std::vector<lcsdata_t> line[3];
+    std::vector<int> src[3];  // solver index each new point starts from
+    for (int a = 0; a < 3; a++) {
+      const int n = n_[a];
+      if (n == 1) {
+        line[a].push_back(hg_.lt[a][1]);
+        src[a].push_back(1);
+        continue;
+      }
+      const int e1[3] = {a == 0 ? 1 : 0, a == 1 ? 1 : 0, a == 2 ? 1 : 0};
+      for (int i = 1; i <= n; i++) {
+        if (res > 0) {
+          const lcsdata_t xi = hg_.coord(a, i * e1[0] + (1 - e1[0]), i * e1[1] + (1 - e1[1]), i * e1[2] + (1 - e1[2]));
+          const lcsdata_t xn = hg_.coord(a, (i + 1) * e1[0] + (1 - e1[0]), (i + 1) * e1[1] + (1 - e1[1]), (i + 1) * e1[2] + (1 - e1[2]));
+          const lcsdata_t dx = (xn - xi) / (lcsdata_t)(res + 1);
+          for (int r = 0; r <= res; r++) {
+            if (r > 0 && !hg_.P.per[a] && i == n) continue;
+            line[a].push_back(xi + dx * (lcsdata_t)r);
+            src[a].push_back(i);
+          }
+        } else if (i % (std::abs(res) + 1) == 0) {
+          line[a].push_back(hg_.lt[a][i]);
+          src[a].push_back(i);
+        }
+      }
+    }
+    auto lg = std::make_shared<LcsGrid<T>>();
+    const int nn[3] = {(int)line[0].size(), (int)line[1].size(), (int)line[2].size()};
+    const long N = (long)nn[0] * nn[1] * nn[2];
+    std::vector<lcsdata_t> X(N), Y(N), Z(N);
+    std::vector<int> F(N);
+    for (int k = 0; k < nn[2]; k++)
+      for (int j = 0; j < nn[1]; j++)
+        for (int i = 0; i < nn[0]; i++) {
+          const long q = i + (long)nn[0] * (j + (long)nn[1] * k);
+          X[q] = line[0][i];
+          Y[q] = line[1][j];
+          Z[q] = line[2][k];
+          F[q] = (*out_flags_)[(src[0][i] - 1) + (size_t)n_[0] * ((src[1][j] - 1) + (size_t)n_[1] * (src[2][k] - 1))];
+        }
+    if (!lg->hg.build(nn, X.data(), Y.data(), Z.data(), F.data())) {
+      msg = lg->hg.error;
+      return false;
+    }
+    if (!make_dev_grid(lg->hg, lg->dg, msg)) return false;
+    lg->N = N;
+    lg->ntot = lg->hg.ntot();
+    FieldPtrsW<T> pos{};
+    for (int c = 0; c < 3; c++) {
+      if (!(lg->pos[c] = arena_.alloc<T>(N, msg))) return false;
+      if (!(lg->nos_reset[c] = arena_.alloc<int>(N, msg))) return false;
+      if (!(lg->nos[c] = arena_.alloc<int>(N, msg))) return false;
+      pos.f[c] = lg->pos[c];
+    }
+    k_track_lcs_nodes<T><<<node_grid(lg->dg), dim3(32, 8, 1), 0, stream_>>>(dg_, lg->dg, pos, lg->nos_reset[0], lg->nos_reset[1],
+                                                                             lg->nos_reset[2], type == FTLE_FWD ? 1 : 0, &red_->err);
+    CK(cudaGetLastError());
+    counters_.kernel_launches++;
+    d.lg = lg;
+    return true;
+  }
+
+  // backward sets: the working solver nodes back to the tracked ones (reset_lp + track_lp2node)
+  bool reset_refined_nodes(DiagT &d, std::string &msg) {
+    for (int c = 0; c < 3; c++)
+      CK(cudaMemcpyAsync(d.lg->nos[c], d.lg->nos_reset[c], d.lg->N * sizeof(int), cudaMemcpyDeviceToDevice, stream_));
+    return true;
+  }
+
+  template <int INTERP, bool FS, bool FL>
+  void sl_refined_integ(DiagT &d, const VelFields<TV> &V, FieldPtrs<T> fo, FieldPtrsW<T> fn, StageTimes S, T dt) {
+    LcsGrid<T> &L = *d.lg;
+    FieldPtrs<T> pos{};
+    for (int c = 0; c < 3; c++) pos.f[c] = L.pos[c];
+    const dim3 grd = node_grid(L.dg), blk(32, 8, 1);
+    int *err = &red_->err;
+    counters_.kernel_launches++;
+#define SLR(IG) k_sl_refined<T, TV, IG, INTERP, FS, FL><<<grd, blk, 0, stream_>>>(L.dg, dg_, pos, L.nos[0], L.nos[1], L.nos[2], V, fo, fn, S, dt, err)
+    switch (opt_->integrator) {
+      case 0: SLR(EULER_); break;
+      case 1: SLR(TRAPEZOIDAL_); break;
+      case 2: SLR(RK2_); break;
+      case 3: SLR(RK3_); break;
+      default: SLR(RK4_); break;
+    }
+#undef SLR
+  }
+
+  bool launch_sl_refined(DiagT &d, int iv, const VelFields<TV> &V, FieldPtrs<T> fo, FieldPtrsW<T> fn, StageTimes S, T dt, std::string &msg) {
+    const bool FS = dg_.P.has_flags != 0, FL = d.lg->dg.P.has_flags != 0;
+    if (iv == INTERP_NEAREST) {
+      if (FS && FL) sl_refined_integ<INTERP_NEAREST, true, true>(d, V, fo, fn, S, dt);
+      else if (FS) sl_refined_integ<INTERP_NEAREST, true, false>(d, V, fo, fn, S, dt);
+      else if (FL) sl_refined_integ<INTERP_NEAREST, false, true>(d, V, fo, fn, S, dt);
+      else sl_refined_integ<INTERP_NEAREST, false, false>(d, V, fo, fn, S, dt);
+    } else {
+      if (FS && FL) sl_refined_integ<INTERP_LINEAR, true, true>(d, V, fo, fn, S, dt);
+      else if (FS) sl_refined_integ<INTERP_LINEAR, true, false>(d, V, fo, fn, S, dt);
+      else if (FL) sl_refined_integ<INTERP_LINEAR, false, true>(d, V, fo, fn, S, dt);
+      else sl_refined_integ<INTERP_LINEAR, false, false>(d, V, fo, fn, S, dt);
+    }
+    CK(cudaGetLastError());
+    return true;
+  }
+
+  // Device tables of a host grid set-up (coordinate lines, spans, flags, normals, constants)
+  bool make_dev_grid(const HostGrid<lcsdata_t> &hg, DevGrid<T> &dg, std::string &msg) {
+    GridParams<T> P;
+    const GridParams<lcsdata_t> &H = hg.P;
+    for (int a = 0; a < 3; a++) {
+      P.n[a] = H.n[a];
+      P.per[a] = H.per[a];
+      for (int s = 0; s < 2; s++)
+        for (int e = 0; e < 2; e++) P.gx[a][s][e] = (T)H.gx[a][s][e];
+    }
+    P.sx = H.sx;
+    P.sxy = H.sxy;
+    P.single_axis = H.single_axis;
+    P.zquirk = H.zquirk;
+    for (int q = 0; q < 6; q++) P.bb[q] = (T)H.bb[q];
+    for (int d = 0; d < 27; d++)
+      for (int c = 0; c < 3; c++) P.ps[d][c] = (T)H.ps[d][c];
+    P.has_flags = H.has_flags;
+    P.maxtrack = H.maxtrack;
+    dg.P = P;
+    for (int a = 0; a < 3; a++) {
+      if (!(dg.lt[a] = upload(hg.lt[a], msg))) return false;
+      if (!(dg.li[a] = upload(hg.li[a], msg))) return false;
+      if (!(dg.invd[a] = upload(hg.invd[a], msg))) return false;
+    }
+    dg.flag = nullptr;
+    for (int a = 0; a < 3; a++) dg.nrm[a] = nullptr;
+    if (H.has_flags) {
+      int8_t *f = arena_.alloc<int8_t>(hg.flag.size(), msg);
+      if (!f) return false;
+      CK(cudaMemcpy(f, hg.flag.data(), hg.flag.size(), cudaMemcpyHostToDevice));
+      dg.flag = f;
+      if (!hg.bcnorm.empty()) {
+        for (int a = 0; a < 3; a++) {
+          std::vector<lcsdata_t> comp(hg.bcnorm.begin() + (size_t)a * hg.ntot(), hg.bcnorm.begin() + (size_t)(a + 1) * hg.ntot());
+          if (!(dg.nrm[a] = upload(comp, msg))) return false;
+        }
+      } else {
+        // flags without normals (e.g. only INFLOW/OUTFLOW or 2-D): a zero field keeps the
+        // kernels free of null checks
+        std::vector<lcsdata_t> zero(hg.ntot(), lcsdata_t(0));
+        T *z0 = upload(zero, msg);
+        if (!z0) return false;
+        for (int a = 0; a < 3; a++) dg.nrm[a] = z0;
+      }
+    }
+    return true;
+  }
+
   dim3 node_grid() const { return dim3((n_[0] + 31) / 32, (n_[1] + 7) / 8, n_[2]); }
 
   template <int INTERP, bool F>
@@ -1131,7 +1303,8 @@ class Engine : public EngineBase {
   }
 
   bool launch_snapshot(DiagT &d, int s, std::string &msg) {
-    const dim3 blk(32, 8, 1), grd = node_grid();
+    const DevGrid<T> &g = dgrid(d);
+    const dim3 blk(32, 8, 1), grd = node_grid(g);
     FieldPtrs<T> src{};
     FieldPtrsW<T> dst{};
     for (int c = 0; c < 3; c++) {
@@ -1139,29 +1312,30 @@ class Engine : public EngineBase {
       src.f[c] = d.type == FTLE_BKWD ? d.fm[d.cur][c] : nullptr;
     }
     int *err = &red_->err;
-    const bool F = dg_.P.has_flags != 0;
+    const bool F = g.P.has_flags != 0;
     counters_.kernel_launches++;
     if (d.type == FTLE_BKWD) {
-      if (F) k_snapshot<T, true, false><<<grd, blk, 0, stream_>>>(dg_, src, d.P, dst, err);
-      else k_snapshot<T, false, false><<<grd, blk, 0, stream_>>>(dg_, src, d.P, dst, err);
+      if (F) k_snapshot<T, true, false><<<grd, blk, 0, stream_>>>(g, src, d.P, dst, err);
+      else k_snapshot<T, false, false><<<grd, blk, 0, stream_>>>(g, src, d.P, dst, err);
     } else {
-      if (F) k_snapshot<T, true, true><<<grd, blk, 0, stream_>>>(dg_, src, d.P, dst, err);
-      else k_snapshot<T, false, true><<<grd, blk, 0, stream_>>>(dg_, src, d.P, dst, err);
+      if (F) k_snapshot<T, true, true><<<grd, blk, 0, stream_>>>(g, src, d.P, dst, err);
+      else k_snapshot<T, false, true><<<grd, blk, 0, stream_>>>(g, src, d.P, dst, err);
     }
     CK(cudaGetLastError());
     return true;
   }
 
   bool launch_compose(int iv, const SplineAxes<T> &sa, DiagT &d, int m, std::string &msg) {
-    const dim3 blk(32, 8, 1), grd = node_grid();
+    const DevGrid<T> &g = dgrid(d);
+    const dim3 blk(32, 8, 1), grd = node_grid(g);
     FieldPtrsW<T> out{};
     for (int c = 0; c < 3; c++) out.f[c] = d.composed[c];
     int *err = &red_->err;
-    const bool F = dg_.P.has_flags != 0;
+    const bool F = g.P.has_flags != 0;
     const T *const *sl = d.slot_list_dev;
     counters_.kernel_launches++;
     counters_.slots_composed += m;
-#define COMPOSE(I, FL) k_compose<T, I, FL><<<grd, blk, 0, stream_>>>(dg_, sa, sl, m, out, err)
+#define COMPOSE(I, FL) k_compose<T, I, FL><<<grd, blk, 0, stream_>>>(g, sa, sl, m, out, err)
     if (iv == INTERP_NEAREST) { if (F) COMPOSE(INTERP_NEAREST, true); else COMPOSE(INTERP_NEAREST, false); }
     else if (iv == INTERP_LINEAR) { if (F) COMPOSE(INTERP_LINEAR, true); else COMPOSE(INTERP_LINEAR, false); }
     else if (iv == INTERP_SPLINE4) { if (F) COMPOSE(INTERP_SPLINE4, true); else COMPOSE(INTERP_SPLINE4, false); }
@@ -1172,14 +1346,15 @@ class Engine : public EngineBase {
   }
 
   bool launch_ftle(DiagT &d, std::string &msg) {
-    const dim3 blk(32, 8, 1), grd = node_grid();
+    const DevGrid<T> &g = dgrid(d);
+    const dim3 blk(32, 8, 1), grd = node_grid(g);
     FieldPtrs<T> f{};
     for (int c = 0; c < 3; c++) f.f[c] = d.composed[c];
     counters_.kernel_launches++;
-    if (dg_.P.has_flags)
-      k_ftle<T, lcsdata_t, true><<<grd, blk, 0, stream_>>>(dg_, f, d.ftle, d.T_, opt_->incompressible);
+    if (g.P.has_flags)
+      k_ftle<T, lcsdata_t, true><<<grd, blk, 0, stream_>>>(g, f, d.ftle, d.T_, opt_->incompressible);
     else
-      k_ftle<T, lcsdata_t, false><<<grd, blk, 0, stream_>>>(dg_, f, d.ftle, d.T_, opt_->incompressible);
+      k_ftle<T, lcsdata_t, false><<<grd, blk, 0, stream_>>>(g, f, d.ftle, d.T_, opt_->incompressible);
     CK(cudaGetLastError());
     return true;
   }
@@ -1326,9 +1501,16 @@ class Engine : public EngineBase {
   }
 
   void launch_reset(DiagT &d) {
-    const dim3 blk(32, 8, 1), grd = node_grid();
+    const dim3 blk(32, 8, 1);
     counters_.kernel_launches++;
-    k_reset_particles<T><<<grd, blk, 0, stream_>>>(dg_, d.P);
+    if (d.lg) {
+      FieldPtrs<T> pos{};
+      for (int c = 0; c < 3; c++) pos.f[c] = d.lg->pos[c];
+      k_reset_refined<T><<<node_grid(d.lg->dg), blk, 0, stream_>>>(d.lg->dg, pos, d.lg->nos_reset[0], d.lg->nos_reset[1], d.lg->nos_reset[2],
+                                                                   d.P);
+    } else {
+      k_reset_particles<T><<<node_grid(), blk, 0, stream_>>>(dg_, d.P);
+    }
   }
 
   // Re-sorts the particle slots by grid cell (32 x 8 tiles, x fastest) every kSortInterval
@@ -1342,7 +1524,7 @@ class Engine : public EngineBase {
 #endif
   static constexpr int kSortInterval = CFD2LCS_SORT_INTERVAL;
   bool sort_particles(DiagT &d, std::string &msg) {
-    const int np = (int)N_, blk = 256, grd = (np + blk - 1) / blk;
+    const int np = (int)dN(d), blk = 256, grd = (np + blk - 1) / blk;
     const int ncell = (int)sort_key_space(n_);
     const int ntile = (ncell + SORT_TILE - 1) / SORT_TILE;
     k_particle_count<T><<<grd, blk, 0, stream_>>>(dg_, d.P, d.pkey, d.pcnt, np);

@@ -69,6 +69,8 @@ class EngineBase {
   virtual bool get_invariants(int handle, lcsdata_t *out, std::string &msg) = 0;
   // LP_TRACER: particle count (-1 for another handle) and positions (x block, y, z)
   virtual int tracer_count(int handle) = 0;
+  // points per direction of a diagnostic's lcs grid (the solver grid's unless resolution /= 0)
+  virtual bool diagnostic_size(int handle, int n[3]) = 0;
   virtual bool get_tracers(int handle, lcsdata_t *out, std::string &msg) = 0;
   virtual bool sync_errors(std::string &msg) = 0;
   // Recomputes the latest FTLE frame of a diagnostic into caller-owned device buffers

@@ -173,6 +173,111 @@ __global__ void __launch_bounds__(256, sl_min_blocks<INTERP>()) k_sl_subcycle(De
 }
 
 // ---------------------------------------------------------------------------------------
+// Refined lcs grids (resolution /= 0, new_sgrid_from_sgrid, src/sgrid_m.f90:446-761): the
+// flow map lives on the lcs grid gl, the velocity on the solver grid gs.
+//
+// k_track_lcs_nodes: each lcs node's solver-grid node (init_lp / reset_lp, src/lp_m.f90:
+// 72-90, 261-280: the guess nint(real(i*ni_s)/real(ni_l)) in single precision, then the
+// recursive 27-neighbour search of track_lp2node on gs, with the periodic wrap of
+// exchange_lpdata for forward sets only), and the position after that tracking.
+// ---------------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_track_lcs_nodes(DevGrid<T> gs, DevGrid<T> gl, FieldPtrsW<T> pos, int *no0, int *no1, int *no2,
+                                                         int fwd, int *err) {
+  int i, j, k;
+  if (!node_of_thread(gl.P.n, i, j, k)) return;
+  const int q = interior_index(gl.P.n, i, j, k);
+  T x[3] = {__ldg(gl.lt[0] + i), __ldg(gl.lt[1] + j), __ldg(gl.lt[2] + k)};
+  const int nd[3] = {i, j, k};
+  int no[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const float r = (float)(nd[a] * gs.P.n[a]) / (float)gl.P.n[a];
+    no[a] = min(max((int)roundf(r), 1), gs.P.n[a]);  // nint: half away from zero
+  }
+  int passes = 0;
+  while (true) {
+    const bool moved = track_pass(gs, x, no);
+    passes++;
+    if (passes > gs.P.maxtrack) {
+      atomicOr(err, ERR_TRACKING);
+      break;
+    }
+    if (fwd) wrap_particle(gs, x, no);
+    if (!moved) break;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) pos.f[c][q] = x[c];
+  no0[q] = no[0];
+  no1[q] = no[1];
+  no2[q] = no[2];
+}
+
+// One backward SL subcycle on a refined lcs grid (update_flowmap_sl, src/flowmap_m.f90:17-104,
+// with lp%sgrid /= scfd%sgrid): the stages integrate from the node's tracked position with
+// the velocity on gs around its solver node (set_lp_bc clamps that node in place, so the
+// clamped node is written back and used by later subcycles, as lp%no_scfd is), the previous
+// flow map is sampled on gl around the lcs node, the mask comes from the solver node's flag
+// and the flow-map boundary rule from the lcs node's.  NEAREST and LINEAR interpolation.
+template <typename T, typename TV, int INTEG, int INTERP, bool FS, bool FL>
+__global__ void __launch_bounds__(256) k_sl_refined(DevGrid<T> gl, DevGrid<T> gs, FieldPtrs<T> pos, int *no0, int *no1, int *no2,
+                                                    VelFields<TV> V, FieldPtrs<T> fmo, FieldPtrsW<T> fmn, StageTimes S, T dt, int *err) {
+  int i, j, k;
+  if (!node_of_thread(gl.P.n, i, j, k)) return;
+  const int p = pidx(gl.P.sx, gl.P.sxy, i, j, k), q = interior_index(gl.P.n, i, j, k);
+  const T x0[3] = {pos.f[0][q], pos.f[1][q], pos.f[2][q]};
+  int no[3] = {no0[q], no1[q], no2[q]};
+  // the mask is taken before the clamp (update_flowmap_sl sets it before integrating)
+  const int fs = FS ? (int)gs.flag[pidx(gs.P.sx, gs.P.sxy, no[0], no[1], no[2])] : (int)LCS_INTERNAL;
+  const SplineAxes<T> sa{};
+  T x[3];
+  integrate<T, TV, INTEG, INTERP, false>(gs, sa, V, S, dt, x0, no, x);
+  project_plane(gs, no, x);
+  const bool stick = particle_bc<T, FS>(gs, no, x, err);
+  if (stick) {
+    x[0] = x0[0];
+    x[1] = x0[1];
+    x[2] = x0[2];
+  }
+  no0[q] = no[0];
+  no1[q] = no[1];
+  no2[q] = no[2];
+  T fmp[3];
+  const int nod[3] = {i, j, k};
+  sample_field<T, INTERP>(gl, sa, fmo.f, x, nod, fmp);
+  const T mask = fs != LCS_MASK ? T(1) : T(0);
+  const int fl = FL ? (int)gl.flag[p] : (int)LCS_INTERNAL;
+  const bool zero = FL && (fl == LCS_MASK || fl == LCS_INFLOW || fl == LCS_OUTFLOW);
+  T vpre[3], vfin[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    vpre[c] = (fmp[c] + (x[c] - x0[c])) * mask;
+    vfin[c] = zero ? T(0) : vpre[c];
+    fmn.f[c][p] = vfin[c];
+  }
+  write_ghosts<T, FL, GHOST_FM>(gl, fmn.f, i, j, k, vpre, vfin, err);
+}
+
+// Forward particles back to the lcs nodes (reset_lp + track_lp2node on the solver grid): the
+// positions and solver nodes k_track_lcs_nodes found, in node order.
+template <typename T>
+__global__ void __launch_bounds__(256) k_reset_refined(DevGrid<T> gl, FieldPtrs<T> pos, const int *no0, const int *no1, const int *no2,
+                                                       Particles<T> P) {
+  int i, j, k;
+  if (!node_of_thread(gl.P.n, i, j, k)) return;
+  const int q = interior_index(gl.P.n, i, j, k);
+  const int nd[3] = {no0[q], no1[q], no2[q]};
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    P.x[c][q] = pos.f[c][q];
+    P.dx[c][q] = T(0);
+    P.no[c][q] = nd[c];
+  }
+  P.id[q] = q;
+  P.slot[q] = q;
+}
+
+// ---------------------------------------------------------------------------------------
 // K6  one forward particle subcycle (update_lp, src/lp_motion_m.f90:15-54): integrate,
 // project, BC, stick, accumulate the displacement, one pass of the node search and the
 // periodic wrap of exchange_lpdata.  Thread q advances the particle in storage slot q.

@@ -85,7 +85,7 @@ typedef struct {
     real *c[3];
 } sr1_t;
 
-typedef struct {
+typedef struct sgrid_s {
     /* dimensions (one rank: local == global, offsets 0) */
     dims_t d;
     int gn[3];
@@ -109,6 +109,7 @@ typedef struct {
     int *flag;
     sr1_t fm;
     real lifetime; /* time advected (integrate_lp, lp_motion_m.f90:332) */
+    const struct sgrid_s *sg; /* lp%sgrid: the grid of the particle set (the lcs grid) */
 } lp_t;
 
 typedef struct {
@@ -122,6 +123,8 @@ typedef struct {
     sr1_t fm_out; /* composed flow map of the last FTLE frame (written by write_lcs) */
     char label[136]; /* lcs%label, trimmed */
     int dead;        /* an LP_TRACER set that was never injected or outlived T (destroy_lcs) */
+    sgrid_t *sg;     /* lcs%sgrid: the solver grid (resolution 0) or its own refined copy */
+    int own_sg;
     int nslot;
     real **slot[3]; /* slot[c][s] -> interior values of stored sub-flow map */
     int *written;
@@ -648,9 +651,10 @@ static void reset_lp(const sgrid_t *g, lp_t *lp, int zero_fm) {
                 }
                 lp->no[0][ip] = i; lp->no[1][ip] = j; lp->no[2][ip] = k;
                 /* educated guess, lp_m.f90:276-278: nint(real(i*ni)/real(ni)) == i */
-                lp->no_scfd[0][ip] = clampi(fnint((real)((float)(i * d->ni) / (float)d->ni)), 1, d->ni);
-                lp->no_scfd[1][ip] = clampi(fnint((real)((float)(j * d->nj) / (float)d->nj)), 1, d->nj);
-                lp->no_scfd[2][ip] = clampi(fnint((real)((float)(k * d->nk) / (float)d->nk)), 1, d->nk);
+                /* (the solver grid S.g; g is the set's own grid, the same one at resolution 0) */
+                lp->no_scfd[0][ip] = clampi(fnint((real)((float)(i * S.g.d.ni) / (float)d->ni)), 1, S.g.d.ni);
+                lp->no_scfd[1][ip] = clampi(fnint((real)((float)(j * S.g.d.nj) / (float)d->nj)), 1, S.g.d.nj);
+                lp->no_scfd[2][ip] = clampi(fnint((real)((float)(k * S.g.d.nk) / (float)d->nk)), 1, S.g.d.nk);
                 lp->flag[ip] = LP_UNKNOWN;
             }
     lp->recursive_tracking = 1;
@@ -1319,7 +1323,7 @@ static void track_lp2node(const sgrid_t *g, lp_t *lp, int *const *no) {
  * Backward SL flow-map update, flowmap_m.f90:17-104
  * ------------------------------------------------------------------------------------ */
 static void update_flowmap_sl(lp_t *lp) {
-    const sgrid_t *g = &S.g;
+    const sgrid_t *g = lp->sg;  /* the flow map's grid; the velocity is on S.g */
     const dims_t *d = &g->d;
     int np = lp->np;
     real dt;
@@ -1333,7 +1337,7 @@ static void update_flowmap_sl(lp_t *lp) {
         memcpy(lpgrid[c], lp->xp[c], sizeof(real) * (size_t)np);
     }
     for (int ip = 0; ip < np; ip++)
-        if (g->bcflag[PX(d, lp->no_scfd[0][ip], lp->no_scfd[1][ip], lp->no_scfd[2][ip])] != LCS_MASK) mask[ip] = (real)1.0;
+        if (S.g.bcflag[PX(&S.g.d, lp->no_scfd[0][ip], lp->no_scfd[1][ip], lp->no_scfd[2][ip])] != LCS_MASK) mask[ip] = (real)1.0;
     real lp_time = S.t_np1;
     for (int sc = 1; sc <= nsub && !S.error; sc++) {
         integrate_lp(lp, &lp_time, dt);
@@ -1375,6 +1379,7 @@ static int ring_step(real t, real T, real h) {
 
 static void write_substep(lcs_t *L) {
     const dims_t *d = &S.g.d;
+    const dims_t *dl = &L->sg->d;
     int step = ring_step(S.t_np1, L->T, L->h);
     /* velocity snapshot (VELOCITY_INVARIANTS; step nint(T/h) is kept too: the forward
      * reconstruction reads step+1 before wrapping it) */
@@ -1396,9 +1401,9 @@ static void write_substep(lcs_t *L) {
     for (int c = 0; c < 3; c++) {
         real *s = L->slot[c][step];
         long q = 0;
-        for (int k = 1; k <= d->nk; k++)
-            for (int j = 1; j <= d->nj; j++)
-                for (int i = 1; i <= d->ni; i++) s[q++] = L->lp.fm.c[c][PX(d, i, j, k)];
+        for (int k = 1; k <= dl->nk; k++)
+            for (int j = 1; j <= dl->nj; j++)
+                for (int i = 1; i <= dl->ni; i++) s[q++] = L->lp.fm.c[c][PX(dl, i, j, k)];
     }
     L->written[step] = 1;
 }
@@ -1432,7 +1437,7 @@ static void alltoall_wrap(const sgrid_t *g, lp_t *lp, int ip) {
 }
 
 static int reconstruct(lcs_t *L) {
-    const sgrid_t *g = &S.g;
+    const sgrid_t *g = L->sg;
     const dims_t *d = &g->d;
     lp_t *lp = &L->lp;
     int np = lp->np;
@@ -1527,7 +1532,7 @@ static long double eig3_max(const long double A_in[3][3]) {
 }
 
 static void compute_ftle(lcs_t *L) {
-    const sgrid_t *g = &S.g;
+    const sgrid_t *g = L->sg;
     const dims_t *d = &g->d;
     sr1_t *fm = &L->lp.fm;
     exchange_self(g, fm->c, 3, 0, 0); /* scomm_face_r1 */
@@ -1851,6 +1856,10 @@ static void free_lcs(lcs_t *L) {
     sr1_free(&L->fm_out);
     free(L->ftle);
     free(L->written);
+    if (L->own_sg) {
+        sr1_free(&L->sg->grid); sr1_free(&L->sg->bcnorm); free(L->sg->bcflag);
+        free(L->sg);
+    }
     free(L);
 }
 
@@ -1895,6 +1904,93 @@ EXPORT void orc_init(const int n[3], const int offset[3], const real *x, const r
 /* directory of the output files (the reference's ./cfd2lcs_output) */
 EXPORT void orc_set_output_dir(const char *dir) { snprintf(S.outdir, sizeof S.outdir, "%s", dir ? dir : ""); }
 
+/* new_sgrid_from_sgrid (sgrid_m.f90:446-761) at one rank on a rectilinear grid.  res > 0:
+ * res points between neighbouring nodes, x(ii) + dx * ir with dx = (x(ii+1) - x(ii)) / (res+1)
+ * (the ghost image past the last node where the direction is periodic, nothing past it
+ * otherwise); res < 0: every (|res|+1)-th node; singleton directions unchanged; each new point
+ * inherits the flag of the node it starts from.  |res| >= n in a non-singleton direction
+ * resets res to 0 (the reference's warning) and returns NULL, as res = 0 does. */
+static sgrid_t *new_sgrid(int *res_io) {
+    const sgrid_t *g = &S.g;
+    const dims_t *d = &g->d;
+    int res = *res_io;
+    const int n[3] = {d->ni, d->nj, d->nk};
+    for (int a = 0; a < 3; a++)
+        if (n[a] > 1 && abs(res) >= n[a]) res = 0;
+    *res_io = res;
+    if (res == 0) return NULL;
+    int nn[3];
+    for (int a = 0; a < 3; a++) {
+        if (n[a] == 1) { nn[a] = 1; continue; }
+        nn[a] = 0;
+        for (int i = 1; i <= n[a]; i++) {
+            if (res > 0) {
+                nn[a]++;
+                for (int r = 1; r <= res; r++)
+                    if (g->per[a] || i != n[a]) nn[a]++;
+            } else if (i % (abs(res) + 1) == 0) {
+                nn[a]++;
+            }
+        }
+    }
+    const long N = (long)nn[0] * nn[1] * nn[2];
+    real *x = zalloc(N), *y = zalloc(N), *z = zalloc(N);
+    int *fl = (int *)calloc((size_t)N, sizeof(int));
+    const real *X = g->grid.c[0], *Y = g->grid.c[1], *Z = g->grid.c[2];
+    if (res > 0) {
+        for (int kk = 1; kk <= d->nk; kk++)
+            for (int jj = 1; jj <= d->nj; jj++)
+                for (int ii = 1; ii <= d->ni; ii++)
+                    for (int kr = 0; kr <= res; kr++)
+                        for (int jr = 0; jr <= res; jr++)
+                            for (int ir = 0; ir <= res; ir++) {
+                                const int in = ii + (ii - 1) * res + ir, jn = jj + (jj - 1) * res + jr, kn = kk + (kk - 1) * res + kr;
+                                if (in > nn[0] || jn > nn[1] || kn > nn[2]) continue;
+                                const long p = PX(d, ii, jj, kk);
+                                const real dx0 = (X[PX(d, ii + 1, jj, kk)] - X[p]) / (real)(res + 1);
+                                const real dx1 = (Y[PX(d, ii, jj + 1, kk)] - Y[p]) / (real)(res + 1);
+                                const real dx2 = (Z[PX(d, ii, jj, kk + 1)] - Z[p]) / (real)(res + 1);
+                                const long q = (in - 1) + (long)nn[0] * ((jn - 1) + (long)nn[1] * (kn - 1));
+                                x[q] = X[p] + dx0 * (real)ir;
+                                y[q] = Y[p] + dx1 * (real)jr;
+                                z[q] = Z[p] + dx2 * (real)kr;
+                                fl[q] = g->bcflag[p];
+                            }
+    } else {
+        const int m = abs(res) + 1;
+        int kn = 0;
+        for (int k = 1; k <= d->nk; k++) {
+            if (d->nk != 1 && k % m != 0) continue;
+            kn++;
+            int jn = 0;
+            for (int j = 1; j <= d->nj; j++) {
+                if (d->nj != 1 && j % m != 0) continue;
+                jn++;
+                int in = 0;
+                for (int i = 1; i <= d->ni; i++) {
+                    if (d->ni != 1 && i % m != 0) continue;
+                    in++;
+                    const long p = PX(d, i, j, k);
+                    const long q = (in - 1) + (long)nn[0] * ((jn - 1) + (long)nn[1] * (kn - 1));
+                    x[q] = X[p];
+                    y[q] = Y[p];
+                    z[q] = Z[p];
+                    fl[q] = g->bcflag[p];
+                }
+            }
+        }
+    }
+    sgrid_t *ng = (sgrid_t *)calloc(1, sizeof(sgrid_t));
+    const int bad = init_sgrid(ng, nn, x, y, z, fl);
+    free(x); free(y); free(z); free(fl);
+    if (bad || !ng->rectilinear) {
+        if (!S.error) latch("new_sgrid_from_sgrid: the new lcs grid is not rectilinear");
+        free(ng);
+        return NULL;
+    }
+    return ng;
+}
+
 /* LP_TRACER: init_lp_tracer (lp_m.f90:116-226) and diagnostic_init (cfd2lcs.f90:327-337):
  * one tracer per node with r <= TRACER_INJECT_RADIUS from the injection point, in node
  * order; none inside: the set is destroyed (its number used up) and the handle is -1. */
@@ -1903,6 +1999,8 @@ static int tracer_init(real T, real h, const char *label) {
     lcs_t *L = (lcs_t *)calloc(1, sizeof(lcs_t));
     L->id = S.nlcs + 1;
     L->diagnostic = LP_TRACER;
+    L->sg = &S.g;
+    L->lp.sg = &S.g;
     L->T = T;
     L->h = h;
     snprintf(L->label, sizeof L->label, "%s", label ? label : "");
@@ -1965,20 +2063,34 @@ EXPORT int orc_diagnostic_init(int type, int resolution, real T, real h, const c
     if (S.error) return -1;
     if (!S.inited) { latch("diagnostic_init before init"); return -1; }
     if (S.nlcs >= MAXLCS) { latch("diagnostic_init: too many diagnostics"); return -1; }
-    if (resolution != 0) { latch("diagnostic_init: resolution /= 0 (new_sgrid_from_sgrid) is not restated"); return -1; }
-    if (type == LP_TRACER) return tracer_init(T, h, label);
+    if (type == LP_TRACER) {
+        if (resolution != 0) { latch("diagnostic_init: LP_TRACER with resolution /= 0 is not restated"); return -1; }
+        return tracer_init(T, h, label);
+    }
     if (type != FTLE_FWD && type != FTLE_BKWD) {
         latch("ERROR, bad specification for lcs_type. Options are: FTLE_FWD, FTLE_BKWD, LP_TRACER");
         return -1;
+    }
+    /* lcs%sgrid: the solver grid, or new_sgrid_from_sgrid's copy (which may reset the
+     * resolution to 0, changing dt_factor below as the reference's in-out argument does) */
+    sgrid_t *sg = &S.g;
+    int own = 0;
+    if (resolution != 0) {
+        sgrid_t *ng = new_sgrid(&resolution);
+        if (S.error) return -1;
+        if (ng) { sg = ng; own = 1; }
     }
     lcs_t *L = (lcs_t *)calloc(1, sizeof(lcs_t));
     L->id = S.nlcs + 1;
     L->diagnostic = type;
     L->T = T;
     L->h = h;
+    L->sg = sg;
+    L->own_sg = own;
+    L->lp.sg = sg;
     snprintf(L->label, sizeof L->label, "%s", label ? label : "");
     for (size_t e = strlen(L->label); e > 0 && L->label[e - 1] == ' '; e--) L->label[e - 1] = 0; /* trim */
-    const dims_t *d = &S.g.d;
+    const dims_t *d = &sg->d;
     L->ftle = zalloc(d->ntot);
     for (int q = 0; q < 5; q++) L->inv[q] = zalloc(d->ntot);
     L->l2margin = zalloc(d->ntot);
@@ -1987,7 +2099,7 @@ EXPORT int orc_diagnostic_init(int type, int resolution, real T, real h, const c
     sr1_alloc(&L->fm_out, d);
     L->lp.direction = type == FTLE_BKWD ? BKWD : FWD;
     L->lp.dt_factor = type == FTLE_BKWD ? (real)1.0 / (real)imax(1 + resolution, 1) : (real)1.0;
-    reset_lp(&S.g, &L->lp, 1);
+    reset_lp(sg, &L->lp, 1);
     track_lp2node(&S.g, &L->lp, L->lp.no_scfd);
     L->nslot = fnint(T / h);
     if (L->nslot < 1) L->nslot = 1;
@@ -2043,13 +2155,18 @@ EXPORT void orc_update(const int n[3], const real *u, const real *v, const real 
             if (L->lp.lifetime > L->T) L->dead = 1;
             continue;
         }
+        const dims_t *dl = &L->sg->d;
+        if (L->sg != &S.g && (S.velocity_invariants || S.write_lcs)) {
+            latch("VELOCITY_INVARIANTS and WRITE_LCS are not restated for resolution /= 0");
+            return;
+        }
         if (L->diagnostic == FTLE_FWD) {
             /* exchange_lpmap: fm(no0) = dx */
             int ip = 0;
-            for (int k = 1; k <= d->nk; k++)
-                for (int j = 1; j <= d->nj; j++)
-                    for (int ii = 1; ii <= d->ni; ii++, ip++)
-                        for (int c = 0; c < 3; c++) L->lp.fm.c[c][PX(d, ii, j, k)] = L->lp.dx[c][ip];
+            for (int k = 1; k <= dl->nk; k++)
+                for (int j = 1; j <= dl->nj; j++)
+                    for (int ii = 1; ii <= dl->ni; ii++, ip++)
+                        for (int c = 0; c < 3; c++) L->lp.fm.c[c][PX(dl, ii, j, k)] = L->lp.dx[c][ip];
         }
         write_substep(L);
         /* the starting step of the reconstruction: the current one (backward) or the next,
@@ -2059,9 +2176,9 @@ EXPORT void orc_update(const int n[3], const real *u, const real *v, const real 
         compute_ftle(L);
         if (S.velocity_invariants) compute_invariants(L, ustep);
         if (S.write_lcs) write_lcs(L, ustep);
-        for (int c = 0; c < 3; c++) memcpy(L->fm_out.c[c], L->lp.fm.c[c], sizeof(real) * (size_t)d->ntot);
+        for (int c = 0; c < 3; c++) memcpy(L->fm_out.c[c], L->lp.fm.c[c], sizeof(real) * (size_t)dl->ntot);
         S.ftle_frames++;
-        reset_lp(&S.g, &L->lp, 1);
+        reset_lp(L->sg, &L->lp, 1);
         track_lp2node(&S.g, &L->lp, L->lp.no_scfd);
     }
 }
@@ -2128,8 +2245,8 @@ static lcs_t *find_lcs(int handle) {
 /* FTLE field of a diagnostic, interior points, i fastest */
 EXPORT int orc_get_ftle(int handle, real *out) {
     lcs_t *L = find_lcs(handle);
-    if (!L) return 1;
-    const dims_t *d = &S.g.d;
+    if (!L || !L->sg) return 1;
+    const dims_t *d = &L->sg->d;
     long q = 0;
     for (int k = 1; k <= d->nk; k++)
         for (int j = 1; j <= d->nj; j++)
@@ -2141,14 +2258,22 @@ EXPORT int orc_get_ftle(int handle, real *out) {
  * (sub-)flow map as currently stored, which = 1 the composed map of the last FTLE frame */
 EXPORT int orc_get_fm(int handle, real *out, int which) {
     lcs_t *L = find_lcs(handle);
-    if (!L) return 1;
-    const dims_t *d = &S.g.d;
+    if (!L || !L->sg) return 1;
+    const dims_t *d = &L->sg->d;
     const sr1_t *f = which ? &L->fm_out : &L->lp.fm;
     long q = 0;
     for (int c = 0; c < 3; c++)
         for (int k = 1; k <= d->nk; k++)
             for (int j = 1; j <= d->nj; j++)
                 for (int i = 1; i <= d->ni; i++) out[q++] = f->c[c][PX(d, i, j, k)];
+    return 0;
+}
+
+/* Grid points per direction of a diagnostic's lcs grid (the solver grid at resolution 0) */
+EXPORT int orc_diag_size(int handle, int *n) {
+    lcs_t *L = find_lcs(handle);
+    if (!L || !L->sg) return 1;
+    n[0] = L->sg->d.ni; n[1] = L->sg->d.nj; n[2] = L->sg->d.nk;
     return 0;
 }
 

@@ -56,6 +56,8 @@ class Oracle:
         L.orc_get_invariants.argtypes = [C.c_int, P]
         L.orc_get_invariants.restype = C.c_int
         L.orc_set_output_dir.argtypes = [C.c_char_p]
+        L.orc_diag_size.argtypes = [C.c_int, P]
+        L.orc_diag_size.restype = C.c_int
         L.orc_tracer_count.argtypes = [C.c_int]
         L.orc_tracer_count.restype = C.c_int
         L.orc_get_tracers.argtypes = [C.c_int, P]
@@ -124,16 +126,24 @@ class Oracle:
     def error_msg(self) -> str:
         return self.lib.orc_error_msg().decode()
 
+    def diag_size(self, handle):
+        """Grid points per direction of a diagnostic's lcs grid (resolution /= 0 changes it)."""
+        n = np.zeros(3, dtype=np.int32)
+        assert self.lib.orc_diag_size(handle, n.ctypes.data_as(C.c_void_p)) == 0
+        return tuple(int(v) for v in n)
+
     def ftle(self, handle):
-        out = np.zeros(int(np.prod(self.n)), dtype=self.dtype)
+        n = self.diag_size(handle)
+        out = np.zeros(int(np.prod(n)), dtype=self.dtype)
         assert self.lib.orc_get_ftle(handle, self._p(out)) == 0
-        return out.reshape(self.n, order="F")
+        return out.reshape(n, order="F")
 
     def flowmap(self, handle, composed: bool = True):
         """composed=True: the T flow map of the last FTLE frame; False: the working map."""
-        out = np.zeros(3 * int(np.prod(self.n)), dtype=self.dtype)
+        n = self.diag_size(handle)
+        out = np.zeros(3 * int(np.prod(n)), dtype=self.dtype)
         assert self.lib.orc_get_fm(handle, self._p(out), int(composed)) == 0
-        return out.reshape((3,) + tuple(self.n[::-1])).transpose(0, 3, 2, 1)
+        return out.reshape((3,) + tuple(n[::-1])).transpose(0, 3, 2, 1)
 
     def invariants(self, handle):
         """Q, D, C, H, L2 of the last frame (compute_invariants), shape (5, ni, nj, nk)."""

@@ -1,0 +1,112 @@
+"""Diagnostics on a refined or coarsened lcs grid (resolution /= 0 in cfd2lcs_diagnostic_init;
+new_sgrid_from_sgrid, src/sgrid_m.f90:446-761; the flow map on the lcs grid, the velocity on the
+solver grid, update_flowmap_sl, src/flowmap_m.f90:17-104): the oracle's grid rule (CPU) and the
+library against the oracle (GPU)."""
+import numpy as np
+import pytest
+
+from libcfd2lcs_b200 import workloads as W
+from tests import scenarios as SC
+
+
+@pytest.fixture(scope="module")
+def gpu_dp():
+    import libcfd2lcs_b200 as L
+    return L.Cfd2lcs("dp")
+
+
+def _run(api, case, res, integrator, interp, directions=(SC.FTLE_BKWD, SC.FTLE_FWD), steps=None):
+    g, vel, prm = SC.make_case(case)
+    api.reset()
+    api.init(g.n, g.x, g.y, g.z, g.flag)
+    hs = [api.diagnostic_init(d, res, prm["T"], prm["h"], f"d{d}") for d in directions]
+    api.set_option("INTEGRATOR", integrator)
+    api.set_option("INTERPOLATOR", interp)
+    for k in range(steps or prm["steps"]):
+        t = W.time_at(k, prm["dt"])
+        api.update(*vel(t), t)
+    return g, hs
+
+
+def _expected_size(n, per, res):
+    """Points per axis: res > 0 adds res per node, none past the last node of a non-periodic
+    axis; res < 0 keeps every (|res|+1)-th node; singleton axes stay; |res| >= n resets to 0."""
+    if any(m > 1 and abs(res) >= m for m in n):
+        return tuple(n)
+    out = []
+    for m, p in zip(n, per):
+        if m == 1:
+            out.append(1)
+        elif res > 0:
+            out.append(m * (1 + res) - (0 if p else res))
+        else:
+            out.append(m // (abs(res) + 1))
+    return tuple(out)
+
+
+@pytest.mark.parametrize("case,res,per", [("abc_unsteady", 1, (1, 1, 1)), ("abc_unsteady", -1, (1, 1, 1)),
+                                          ("dg", 2, (0, 0, 0)), ("mixed_bc", 1, (0, 1, 0)), ("abc_unsteady", 12, (1, 1, 1))])
+def test_oracle_lcs_grid_size(oracle_dp, case, res, per):
+    g, hs = _run(oracle_dp, case, res, 2, 1, steps=12)
+    assert oracle_dp.error() == 0, oracle_dp.error_msg()
+    for h in hs:
+        assert oracle_dp.diag_size(h) == _expected_size(g.n, per, res)
+        assert np.all(np.isfinite(oracle_dp.ftle(h)))
+
+
+def test_oracle_coarsened_flags_follow_the_reference(oracle_dp):
+    """Coarsening the double gyre keeps interior (INTERNAL) nodes on its boundary faces, so the
+    new grid's flags no longer agree with a wall: init_sgrid's periodicity check fails, as it
+    does in the reference."""
+    g, vel, prm = SC.make_case("dg")
+    oracle_dp.reset()
+    oracle_dp.init(g.n, g.x, g.y, g.z, g.flag)
+    assert oracle_dp.diagnostic_init(SC.FTLE_BKWD, -1, prm["T"], prm["h"], "b") == -1
+    assert "periodicity" in oracle_dp.error_msg()
+    oracle_dp.reset()
+
+
+CASES = [
+    ("abc_unsteady", 1, 2, 1),
+    ("abc_unsteady", -1, 3, 0),
+    ("dg", 2, 2, 1),
+    ("dg", 1, 4, 0),
+    ("mixed_bc", 1, 3, 1),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case,res,integrator,interp", CASES)
+def test_resolution_matches_oracle(oracle_dp, gpu_dp, case, res, integrator, interp):
+    g, ho = _run(oracle_dp, case, res, integrator, interp)
+    assert oracle_dp.error() == 0, oracle_dp.error_msg()
+    try:
+        _, hg = _run(gpu_dp, case, res, integrator, interp)
+        err, msg = gpu_dp.error()
+        assert err == 0, msg
+        L = max(float(np.ptp(g.x)), float(np.ptp(g.y)), float(np.ptp(g.z)))
+        for a, b in zip(ho, hg):
+            assert gpu_dp.diag_size(b) == oracle_dp.diag_size(a)
+            fo, fg = oracle_dp.flowmap(a), gpu_dp.flowmap(b)
+            to, tg = oracle_dp.ftle(a), gpu_dp.ftle(b)
+            assert np.all(np.isfinite(tg))
+            assert float(np.max(np.abs(fo - fg))) <= 1e-12 * L
+            assert float(np.max(np.abs(to - tg))) <= 1e-9
+        cg = gpu_dp.counters()
+        for k in ("integrations_fwd", "integrations_bkwd", "ftle_frames"):
+            assert cg[k] == oracle_dp.counter(k), k
+    finally:
+        gpu_dp.reset()
+
+
+@pytest.mark.gpu
+def test_resolution_rejects_spline_interpolation(gpu_dp):
+    g, vel, prm = SC.make_case("abc_unsteady")
+    gpu_dp.reset()
+    gpu_dp.init(g.n, g.x, g.y, g.z, g.flag)
+    gpu_dp.diagnostic_init(SC.FTLE_BKWD, 1, prm["T"], prm["h"], "b")
+    gpu_dp.set_option("INTERPOLATOR", 3)
+    gpu_dp.update(*vel(0.0), 0.0)
+    err, msg = gpu_dp.error()
+    assert err != 0 and "LINEAR" in msg
+    gpu_dp.reset()
