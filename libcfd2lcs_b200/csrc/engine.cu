@@ -74,6 +74,7 @@ struct LcsGrid {
   T *pos[3] = {nullptr, nullptr, nullptr};
   int *nos_reset[3] = {nullptr, nullptr, nullptr};
   int *nos[3] = {nullptr, nullptr, nullptr};
+  SplineSet<T> sp[4];  // B-spline axes of the lcs grid by degree (flow-map fits and samples)
 };
 
 template <typename T, typename TV>
@@ -443,10 +444,7 @@ class Engine : public EngineBase {
 
     if (spline)
       for (auto &d : diags_)
-        if (d.lg) {
-          msg = "resolution /= 0 supports the NEAREST_NBR and LINEAR interpolators only";
-          return false;
-        }
+        if (d.lg && !ensure_lcs_spline(*d.lg, deg, msg)) return false;
     // --- per particle set: K1 (backward) / K6 (forward) --------------------------------
     for (auto &d : diags_) {
       if (!d.active) continue;
@@ -484,12 +482,14 @@ class Engine : public EngineBase {
           if (spline) {
             if (!d.fmcoef[0])
               for (int c = 0; c < 3; c++)
-                if (!(d.fmcoef[c] = arena_.alloc<T>(ntot_, msg))) return false;
-            if (!fit(splines_[deg].axes, d.fm[d.cur], d.fmcoef, msg)) return false;
+                if (!(d.fmcoef[c] = arena_.alloc<T>(dT(d), msg))) return false;
+            if (!fit(d.lg ? d.lg->sp[deg].axes : splines_[deg].axes, d.fm[d.cur], d.fmcoef, msg, &dgrid(d))) return false;
             for (int c = 0; c < 3; c++) fo.f[c] = d.fmcoef[c];
           }
           if (!mark(k0, msg)) return false;
-          if (d.lg ? !launch_sl_refined(d, iv, V, fo, fn, S, (T)dt, msg) : !launch_sl(iv, sa, V, fo, fn, S, (T)dt, msg)) return false;
+          if (d.lg ? !launch_sl_refined(d, sa, spline ? d.lg->sp[deg].axes : SplineAxes<T>{}, V, fo, fn, S, (T)dt, msg)
+                   : !launch_sl(iv, sa, V, fo, fn, S, (T)dt, msg))
+            return false;
           if (!mark(k1, msg)) return false;
           spans_.push_back({k0, k1, kkind});
           d.cur ^= 1;
@@ -552,9 +552,10 @@ class Engine : public EngineBase {
           if (spline) {
             if (!d.slotcoef[3 * step])
               for (int c = 0; c < 3; c++)
-                if (!(d.slotcoef[3 * step + c] = arena_.alloc<T>(ntot_, msg))) return false;
+                if (!(d.slotcoef[3 * step + c] = arena_.alloc<T>(dT(d), msg))) return false;
             if (d.coef_deg[step] != deg) {
-              if (!fit(splines_[deg].axes, &d.slot[3 * step], &d.slotcoef[3 * step], msg)) return false;
+              if (!fit(d.lg ? d.lg->sp[deg].axes : splines_[deg].axes, &d.slot[3 * step], &d.slotcoef[3 * step], msg, &dgrid(d)))
+                return false;
               d.coef_deg[step] = deg;
             }
             for (int c = 0; c < 3; c++) d.slot_list_host[3 * m + c] = d.slotcoef[3 * step + c];
@@ -568,7 +569,12 @@ class Engine : public EngineBase {
       }
       CK(cudaMemcpyAsync(d.slot_list_dev, d.slot_list_host.data(), sizeof(T *) * 3 * std::max(m, 1), cudaMemcpyHostToDevice,
                          stream_));
-      if (!launch_compose(iv, sa, d, m, msg)) return false;
+      if (d.lg && spline) {
+        const SplineAxes<T> &la = d.lg->sp[deg].axes;
+        if (!launch_compose(interp_variant(interp, la), la, d, m, msg)) return false;
+      } else if (!launch_compose(iv, sa, d, m, msg)) {
+        return false;
+      }
       if (!mark(f6, msg)) return false;
       if (!launch_ftle(d, msg)) return false;
       // compute_invariants from the velocity of the reconstruction's starting step: the
@@ -972,6 +978,31 @@ class Engine : public EngineBase {
     return true;
   }
 
+  // B-spline axes (flow-map type) of an lcs grid, as ensure_spline builds the solver grid's
+  bool ensure_lcs_spline(LcsGrid<T> &L, int deg, std::string &msg) {
+    if (L.sp[deg].deg == deg) return true;
+    SplineSet<T> s;
+    s.deg = deg;
+    for (int a = 0; a < 3; a++) {
+      SplineAxisHost<lcsdata_t> A;
+      const int npts = L.dg.P.n[a] + 2;
+      const int k = std::max(std::min(deg + 1, npts - 1), 2);
+      if (!A.build(L.hg.li[a], k)) {
+        msg = "bspline: singular collocation system or bad abscissae";
+        return false;
+      }
+      SplineAxis<T> &D = s.axes.ax[a];
+      D.n = A.n;
+      D.k = A.k;
+      if (!(D.t = upload(A.t, msg))) return false;
+      if (!(D.rinv = upload(A.rinv, msg))) return false;
+      if (!(D.tu = upload(A.tu, msg))) return false;
+      if (!(D.pull = upload(pull_table(A), msg))) return false;
+    }
+    L.sp[deg] = s;
+    return true;
+  }
+
   bool ensure_spline(int deg, std::string &msg) {
     if (splines_[deg].deg == deg) return true;
     SplineSet<T> s;
@@ -1024,8 +1055,8 @@ class Engine : public EngineBase {
   }
 
   template <typename D, int K>
-  void fit_pass(const SplineAxis<D> &A, FieldPtrs<D> s, FieldPtrsW<D> d, int axis) {
-    const int sx = dg_.P.sx, sxy = dg_.P.sxy, ny = n_[1] + 2, nz = n_[2] + 2;
+  void fit_pass(const SplineAxis<D> &A, FieldPtrs<D> s, FieldPtrsW<D> d, int axis, const DevGrid<T> &g) {
+    const int sx = g.P.sx, sxy = g.P.sxy, ny = g.P.n[1] + 2, nz = g.P.n[2] + 2;
     if (axis == 0) {
       const long warps = (long)((ny + 31) / 32) * nz;
       const size_t smem = sizeof(D) * 4 * 2 * 32 * 33;  // two 32 x 33 tiles per warp
@@ -1045,16 +1076,17 @@ class Engine : public EngineBase {
   }
 
   template <typename D>
-  void fit_pass_any(const SplineAxis<D> &A, FieldPtrs<D> s, FieldPtrsW<D> d, int axis) {
-    if (A.k == 4) fit_pass<D, 4>(A, s, d, axis);
-    else if (A.k == 3) fit_pass<D, 3>(A, s, d, axis);
-    else fit_pass<D, 2>(A, s, d, axis);
+  void fit_pass_any(const SplineAxis<D> &A, FieldPtrs<D> s, FieldPtrsW<D> d, int axis, const DevGrid<T> &g) {
+    if (A.k == 4) fit_pass<D, 4>(A, s, d, axis, g);
+    else if (A.k == 3) fit_pass<D, 3>(A, s, d, axis, g);
+    else fit_pass<D, 2>(A, s, d, axis, g);
   }
 
   // Coefficients of the padded fields src (3 components) into dst (db3ink: x, then y, then z).
   // D is the field type: T for flow maps and sub-flow maps, TV for velocity levels.
   template <typename D>
-  bool fit(const SplineAxes<D> &S, D *const src[3], D *const dst[3], std::string &msg) {
+  bool fit(const SplineAxes<D> &S, D *const src[3], D *const dst[3], std::string &msg, const DevGrid<T> *grid = nullptr) {
+    const DevGrid<T> &g = grid ? *grid : dg_;
     FieldPtrs<D> s{}, di{};
     FieldPtrsW<D> d{};
     for (int c = 0; c < 3; c++) {
@@ -1063,9 +1095,9 @@ class Engine : public EngineBase {
       d.f[c] = dst[c];
     }
     counters_.kernel_launches += 3;
-    fit_pass_any(S.ax[0], s, d, 0);
-    fit_pass_any(S.ax[1], di, d, 1);
-    fit_pass_any(S.ax[2], di, d, 2);
+    fit_pass_any(S.ax[0], s, d, 0, g);
+    fit_pass_any(S.ax[1], di, d, 1, g);
+    fit_pass_any(S.ax[2], di, d, 2, g);
     CK(cudaGetLastError());
     return true;
   }
@@ -1164,14 +1196,17 @@ class Engine : public EngineBase {
   }
 
   template <int INTERP, bool FS, bool FL>
-  void sl_refined_integ(DiagT &d, const VelFields<TV> &V, FieldPtrs<T> fo, FieldPtrsW<T> fn, StageTimes S, T dt) {
+  void sl_refined_integ(DiagT &d, const SplineAxes<T> &sas, const SplineAxes<T> &sal, const VelFields<TV> &V, FieldPtrs<T> fo,
+                        FieldPtrsW<T> fn, StageTimes S, T dt) {
     LcsGrid<T> &L = *d.lg;
     FieldPtrs<T> pos{};
     for (int c = 0; c < 3; c++) pos.f[c] = L.pos[c];
     const dim3 grd = node_grid(L.dg), blk(32, 8, 1);
     int *err = &red_->err;
     counters_.kernel_launches++;
-#define SLR(IG) k_sl_refined<T, TV, IG, INTERP, FS, FL><<<grd, blk, 0, stream_>>>(L.dg, dg_, pos, L.nos[0], L.nos[1], L.nos[2], V, fo, fn, S, dt, err)
+#define SLR(IG)                                                                                                   \
+  k_sl_refined<T, TV, IG, INTERP, FS, FL><<<grd, blk, 0, stream_>>>(L.dg, dg_, sas, sal, pos, L.nos[0], L.nos[1], L.nos[2], V, fo, fn, \
+                                                                     S, dt, err)
     switch (opt_->integrator) {
       case 0: SLR(EULER_); break;
       case 1: SLR(TRAPEZOIDAL_); break;
@@ -1182,19 +1217,26 @@ class Engine : public EngineBase {
 #undef SLR
   }
 
-  bool launch_sl_refined(DiagT &d, int iv, const VelFields<TV> &V, FieldPtrs<T> fo, FieldPtrsW<T> fn, StageTimes S, T dt, std::string &msg) {
+  template <int INTERP>
+  void sl_refined_flags(DiagT &d, const SplineAxes<T> &sas, const SplineAxes<T> &sal, const VelFields<TV> &V, FieldPtrs<T> fo,
+                        FieldPtrsW<T> fn, StageTimes S, T dt) {
     const bool FS = dg_.P.has_flags != 0, FL = d.lg->dg.P.has_flags != 0;
-    if (iv == INTERP_NEAREST) {
-      if (FS && FL) sl_refined_integ<INTERP_NEAREST, true, true>(d, V, fo, fn, S, dt);
-      else if (FS) sl_refined_integ<INTERP_NEAREST, true, false>(d, V, fo, fn, S, dt);
-      else if (FL) sl_refined_integ<INTERP_NEAREST, false, true>(d, V, fo, fn, S, dt);
-      else sl_refined_integ<INTERP_NEAREST, false, false>(d, V, fo, fn, S, dt);
-    } else {
-      if (FS && FL) sl_refined_integ<INTERP_LINEAR, true, true>(d, V, fo, fn, S, dt);
-      else if (FS) sl_refined_integ<INTERP_LINEAR, true, false>(d, V, fo, fn, S, dt);
-      else if (FL) sl_refined_integ<INTERP_LINEAR, false, true>(d, V, fo, fn, S, dt);
-      else sl_refined_integ<INTERP_LINEAR, false, false>(d, V, fo, fn, S, dt);
-    }
+    if (FS && FL) sl_refined_integ<INTERP, true, true>(d, sas, sal, V, fo, fn, S, dt);
+    else if (FS) sl_refined_integ<INTERP, true, false>(d, sas, sal, V, fo, fn, S, dt);
+    else if (FL) sl_refined_integ<INTERP, false, true>(d, sas, sal, V, fo, fn, S, dt);
+    else sl_refined_integ<INTERP, false, false>(d, sas, sal, V, fo, fn, S, dt);
+  }
+
+  // sas: the solver grid's spline axes (velocity), sal: the lcs grid's (flow map); the kernel
+  // takes the all-cubic specialisation only when both grids allow it
+  bool launch_sl_refined(DiagT &d, const SplineAxes<T> &sas, const SplineAxes<T> &sal, const VelFields<TV> &V, FieldPtrs<T> fo,
+                         FieldPtrsW<T> fn, StageTimes S, T dt, std::string &msg) {
+    const int interp = opt_->interpolator;
+    if (interp == NEAREST_NBR) sl_refined_flags<INTERP_NEAREST>(d, sas, sal, V, fo, fn, S, dt);
+    else if (interp == LINEAR) sl_refined_flags<INTERP_LINEAR>(d, sas, sal, V, fo, fn, S, dt);
+    else if (interp_variant(interp, sas) == INTERP_SPLINE4 && interp_variant(interp, sal) == INTERP_SPLINE4)
+      sl_refined_flags<INTERP_SPLINE4>(d, sas, sal, V, fo, fn, S, dt);
+    else sl_refined_flags<INTERP_SPLINE>(d, sas, sal, V, fo, fn, S, dt);
     CK(cudaGetLastError());
     return true;
   }

@@ -218,10 +218,13 @@ __global__ void __launch_bounds__(256) k_track_lcs_nodes(DevGrid<T> gs, DevGrid<
 // the velocity on gs around its solver node (set_lp_bc clamps that node in place, so the
 // clamped node is written back and used by later subcycles, as lp%no_scfd is), the previous
 // flow map is sampled on gl around the lcs node, the mask comes from the solver node's flag
-// and the flow-map boundary rule from the lcs node's.  NEAREST and LINEAR interpolation.
+// and the flow-map boundary rule from the lcs node's.  B-spline interpolation samples the
+// velocity blends with the solver grid's axes sas and the flow-map coefficients with the lcs
+// grid's axes sal.
 template <typename T, typename TV, int INTEG, int INTERP, bool FS, bool FL>
-__global__ void __launch_bounds__(256) k_sl_refined(DevGrid<T> gl, DevGrid<T> gs, FieldPtrs<T> pos, int *no0, int *no1, int *no2,
-                                                    VelFields<TV> V, FieldPtrs<T> fmo, FieldPtrsW<T> fmn, StageTimes S, T dt, int *err) {
+__global__ void __launch_bounds__(256) k_sl_refined(DevGrid<T> gl, DevGrid<T> gs, SplineAxes<T> sas, SplineAxes<T> sal, FieldPtrs<T> pos,
+                                                    int *no0, int *no1, int *no2, VelFields<TV> V, FieldPtrs<T> fmo, FieldPtrsW<T> fmn,
+                                                    StageTimes S, T dt, int *err) {
   int i, j, k;
   if (!node_of_thread(gl.P.n, i, j, k)) return;
   const int p = pidx(gl.P.sx, gl.P.sxy, i, j, k), q = interior_index(gl.P.n, i, j, k);
@@ -229,9 +232,8 @@ __global__ void __launch_bounds__(256) k_sl_refined(DevGrid<T> gl, DevGrid<T> gs
   int no[3] = {no0[q], no1[q], no2[q]};
   // the mask is taken before the clamp (update_flowmap_sl sets it before integrating)
   const int fs = FS ? (int)gs.flag[pidx(gs.P.sx, gs.P.sxy, no[0], no[1], no[2])] : (int)LCS_INTERNAL;
-  const SplineAxes<T> sa{};
   T x[3];
-  integrate<T, TV, INTEG, INTERP, false>(gs, sa, V, S, dt, x0, no, x);
+  integrate<T, TV, INTEG, INTERP, false>(gs, sas, V, S, dt, x0, no, x);
   project_plane(gs, no, x);
   const bool stick = particle_bc<T, FS>(gs, no, x, err);
   if (stick) {
@@ -244,7 +246,7 @@ __global__ void __launch_bounds__(256) k_sl_refined(DevGrid<T> gl, DevGrid<T> gs
   no2[q] = no[2];
   T fmp[3];
   const int nod[3] = {i, j, k};
-  sample_field<T, INTERP>(gl, sa, fmo.f, x, nod, fmp);
+  sample_field<T, INTERP, !std::is_same<T, TV>::value>(gl, sal, fmo.f, x, nod, fmp);
   const T mask = fs != LCS_MASK ? T(1) : T(0);
   const int fl = FL ? (int)gl.flag[p] : (int)LCS_INTERNAL;
   const bool zero = FL && (fl == LCS_MASK || fl == LCS_INFLOW || fl == LCS_OUTFLOW);
