@@ -129,11 +129,7 @@ void do_set_option(const std::string &opt, int val) {
     ok = tf;
     if (ok) lib.opt.incompressible = val;
   } else if (opt == "AUX_GRID") {
-    ok = tf;
-    if (ok && val == LCS_TRUE) {
-      latch("AUX_GRID = TRUE (auxiliary-grid Cauchy-Green gradient) is not supported by this library");
-      return;
-    }
+    ok = tf;  // read by cfd2lcs_diagnostic_init (the auxiliary sets are made there) and at each frame
     if (ok) lib.opt.aux_grid = val;
   } else if (opt == "UPDATE_FREQ") {
     ok = true;

@@ -113,6 +113,12 @@ struct Diag {
   lcsdata_t lifetime = 0;
   bool active = true;
   std::shared_ptr<LcsGrid<T>> lg;  // refined / coarsened lcs grid (null: the solver grid)
+  // AUX_GRID: an auxiliary set (aux_parent = index + 1 of its diagnostic in the engine's list,
+  // handle 0), or a diagnostic's six sets X0, Y0, Z0, X1, Y1, Z1 (indices) and the per-node
+  // separations of each pair
+  int aux_parent = 0;
+  std::vector<int> aux;
+  T *auxden[3] = {nullptr, nullptr, nullptr};
 };
 
 }  // namespace
@@ -264,7 +270,7 @@ class Engine : public EngineBase {
     DiagT d;
     // lcs%sgrid (src/cfd2lcs.f90:302-310); new_sgrid_from_sgrid may reset the resolution to 0
     if (resolution != 0 && !make_lcs_grid(d, type, resolution, msg)) return -1;
-    d.handle = (int)diags_.size() + 1;
+    d.handle = ++handle_count_;
     d.type = type;
     d.label = label ? label : "";
     while (!d.label.empty() && d.label.back() == ' ') d.label.pop_back();  // trim(label)
@@ -272,35 +278,47 @@ class Engine : public EngineBase {
     d.h = h;
     d.dt_factor = type == FTLE_BKWD ? lcsdata_t(1) / lcsdata_t(std::max(1 + resolution, 1)) : lcsdata_t(1);
     d.nslot = (int)std::max(1L, fnint((double)(Tint / h)));
+    if (!alloc_diag(d, msg)) return -1;
+    if (cudaStreamSynchronize(stream_) != cudaSuccess) return fail(msg, "sync");
+    const int handle = d.handle;
+    diags_.push_back(d);
+    // AUX_GRID (init_ftle, src/lcs_m.f90:50-53): six auxiliary particle sets around the nodes
+    if (opt_->aux_grid && !create_aux((int)diags_.size() - 1, msg)) return -1;
+    return handle;
+  }
+
+  // Device buffers of a diagnostic (or auxiliary set) on its grid: working flow maps or
+  // particles and their sort tables, the ring of sub-flow maps, the composed map and the FTLE.
+  bool alloc_diag(DiagT &d, std::string &msg) {
     const long dn = dN(d), dt = dT(d);
-    if (type == FTLE_BKWD) {
+    if (d.type == FTLE_BKWD) {
       for (int b = 0; b < 2; b++)
         for (int c = 0; c < 3; c++) {
-          if (!(d.fm[b][c] = arena_.alloc<T>(dt, msg))) return -1;
-          if (cudaMemsetAsync(d.fm[b][c], 0, dt * sizeof(T), stream_) != cudaSuccess) return fail(msg, "memset");
+          if (!(d.fm[b][c] = arena_.alloc<T>(dt, msg))) return false;
+          if (cudaMemsetAsync(d.fm[b][c], 0, dt * sizeof(T), stream_) != cudaSuccess) { msg = "CUDA error in memset"; return false; }
         }
-      if (d.lg && !reset_refined_nodes(d, msg)) return -1;
+      if (d.lg && !reset_refined_nodes(d, msg)) return false;
     } else {
       for (Particles<T> *Q : {&d.P, &d.P2}) {
         for (int c = 0; c < 3; c++) {
-          if (!(Q->x[c] = arena_.alloc<T>(dn, msg))) return -1;
-          if (!(Q->dx[c] = arena_.alloc<T>(dn, msg))) return -1;
-          if (!(Q->no[c] = arena_.alloc<int>(dn, msg))) return -1;
+          if (!(Q->x[c] = arena_.alloc<T>(dn, msg))) return false;
+          if (!(Q->dx[c] = arena_.alloc<T>(dn, msg))) return false;
+          if (!(Q->no[c] = arena_.alloc<int>(dn, msg))) return false;
         }
-        if (!(Q->id = arena_.alloc<int>(dn, msg))) return -1;
+        if (!(Q->id = arena_.alloc<int>(dn, msg))) return false;
       }
-      if (!(d.P.slot = arena_.alloc<int>(dn, msg))) return -1;
+      if (!(d.P.slot = arena_.alloc<int>(dn, msg))) return false;
       d.P2.slot = d.P.slot;  // the inverse map is rewritten whole by every permutation
       const long ncell = sort_key_space(n_);
       if (ncell > (long)std::numeric_limits<int>::max()) {
         msg = "diagnostic_init: grid too large for the forward particle sort";
-        return -1;
+        return false;
       }
-      if (!(d.pkey = arena_.alloc<unsigned>(dn, msg))) return -1;
-      if (!(d.pcnt = arena_.alloc<int>(ncell, msg))) return -1;
-      if (!(d.poffs = arena_.alloc<int>(ncell, msg))) return -1;
-      if (!(d.ptsum = arena_.alloc<int>((ncell + SORT_TILE - 1) / SORT_TILE, msg))) return -1;
-      if (cudaMemsetAsync(d.pcnt, 0, ncell * sizeof(int), stream_) != cudaSuccess) return fail(msg, "memset");
+      if (!(d.pkey = arena_.alloc<unsigned>(dn, msg))) return false;
+      if (!(d.pcnt = arena_.alloc<int>(ncell, msg))) return false;
+      if (!(d.poffs = arena_.alloc<int>(ncell, msg))) return false;
+      if (!(d.ptsum = arena_.alloc<int>((ncell + SORT_TILE - 1) / SORT_TILE, msg))) return false;
+      if (cudaMemsetAsync(d.pcnt, 0, ncell * sizeof(int), stream_) != cudaSuccess) { msg = "CUDA error in memset"; return false; }
       launch_reset(d);
     }
     d.slot.assign((size_t)3 * d.nslot, nullptr);
@@ -308,15 +326,13 @@ class Engine : public EngineBase {
     d.written.assign(d.nslot, 0);
     d.coef_deg.assign(d.nslot, 0);
     for (int s = 0; s < 3 * d.nslot; s++)
-      if (!(d.slot[s] = arena_.alloc<T>(dt, msg))) return -1;
-    if (!(d.slot_list_dev = arena_.alloc<T *>((size_t)3 * d.nslot, msg))) return -1;
+      if (!(d.slot[s] = arena_.alloc<T>(dt, msg))) return false;
+    if (!(d.slot_list_dev = arena_.alloc<T *>((size_t)3 * d.nslot, msg))) return false;
     d.slot_list_host.assign((size_t)3 * d.nslot, nullptr);
     for (int c = 0; c < 3; c++)
-      if (!(d.composed[c] = arena_.alloc<T>(dn, msg))) return -1;
-    if (!(d.ftle = arena_.alloc<lcsdata_t>(dn, msg))) return -1;
-    if (cudaStreamSynchronize(stream_) != cudaSuccess) return fail(msg, "sync");
-    diags_.push_back(d);
-    return d.handle;
+      if (!(d.composed[c] = arena_.alloc<T>(dn, msg))) return false;
+    if (!(d.ftle = arena_.alloc<lcsdata_t>(dn, msg))) return false;
+    return true;
   }
 
   bool update(const int n[3], const lcsdata_t *u, const lcsdata_t *v, const lcsdata_t *w, lcsdata_t time, bool device_ptrs,
@@ -511,10 +527,13 @@ class Engine : public EngineBase {
     }
 
     // --- h boundaries: K7 snapshot, K4 composition, K5 FTLE, reset ----------------------
+    // (auxiliary sets first: a diagnostic's AUX_GRID FTLE reads their composed maps)
+    for (int pass = 0; pass < 2; pass++)
     for (auto &d : diags_) {
+      if ((d.aux_parent != 0) != (pass == 0)) continue;
       if (!d.active) continue;
       if ((long)(t_np1_ / d.h) == (long)(t_n_ / d.h)) continue;
-      if (d.lg && (opt_->velocity_invariants || opt_->write_lcs)) {
+      if (d.lg && !d.aux_parent && (opt_->velocity_invariants || opt_->write_lcs)) {
         msg = "VELOCITY_INVARIANTS and WRITE_LCS are not supported for diagnostics with resolution /= 0";
         return false;
       }
@@ -576,12 +595,18 @@ class Engine : public EngineBase {
         return false;
       }
       if (!mark(f6, msg)) return false;
-      if (!launch_ftle(d, msg)) return false;
-      // compute_invariants from the velocity of the reconstruction's starting step: the
-      // current one (backward) or the next, not yet wrapped (forward), flowmap_m.f90:202-245
-      if (opt_->velocity_invariants && !launch_invariants(d, wslot + (d.type == FTLE_FWD ? 1 : 0), msg)) return false;
-      // write_lcs (src/cfd2lcs.f90:202): the frame's file, staged now, written by the writer
-      if (opt_->write_lcs && !enqueue_output(d, wslot + (d.type == FTLE_FWD ? 1 : 0), msg)) return false;
+      if (!d.aux_parent) {
+        if (opt_->aux_grid && d.aux.empty()) {
+          msg = "AUX_GRID was set after cfd2lcs_diagnostic_init: this diagnostic has no auxiliary particle sets";
+          return false;
+        }
+        if (d.aux.empty() ? !launch_ftle(d, msg) : !launch_ftle_aux(d, msg)) return false;
+        // compute_invariants from the velocity of the reconstruction's starting step: the
+        // current one (backward) or the next, not yet wrapped (forward), flowmap_m.f90:202-245
+        if (opt_->velocity_invariants && !launch_invariants(d, wslot + (d.type == FTLE_FWD ? 1 : 0), msg)) return false;
+        // write_lcs (src/cfd2lcs.f90:202): the frame's file, staged now, written by the writer
+        if (opt_->write_lcs && !enqueue_output(d, wslot + (d.type == FTLE_FWD ? 1 : 0), msg)) return false;
+      }
       if (!mark(f7, msg)) return false;
       // reset_lp: particles back to the grid, flow map to zero (src/cfd2lcs.f90:208-209)
       if (d.type == FTLE_BKWD) {
@@ -596,7 +621,7 @@ class Engine : public EngineBase {
       spans_.push_back({f5, f6, 4});
       spans_.push_back({f6, f7, 5});
       d.have_frame = true;
-      counters_.ftle_frames++;
+      if (!d.aux_parent) counters_.ftle_frames++;
     }
     CK(cudaEventRecord(ev_[9], stream_));
     return true;
@@ -649,8 +674,8 @@ class Engine : public EngineBase {
       msg = "reconstruct_noalloc: unknown handle or no FTLE frame yet";
       return false;
     }
-    if (d->lg) {
-      msg = "reconstruct_noalloc: diagnostics with resolution /= 0 are not supported";
+    if (d->lg || !d->aux.empty()) {
+      msg = "reconstruct_noalloc: diagnostics with resolution /= 0 or AUX_GRID are not supported";
       return false;
     }
     const int m = (int)d->last_order.size();
@@ -788,7 +813,7 @@ class Engine : public EngineBase {
       return -1;
     }
     DiagT d;
-    d.handle = (int)diags_.size() + 1;
+    d.handle = ++handle_count_;
     d.type = LP_TRACER;
     d.T_ = Tint;
     d.h = h;
@@ -1152,11 +1177,23 @@ class Engine : public EngineBase {
         }
       }
     }
+    const int nn[3] = {(int)line[0].size(), (int)line[1].size(), (int)line[2].size()};
+    std::vector<int> F((size_t)nn[0] * nn[1] * nn[2]);
+    for (int k = 0; k < nn[2]; k++)
+      for (int j = 0; j < nn[1]; j++)
+        for (int i = 0; i < nn[0]; i++)
+          F[i + (size_t)nn[0] * (j + (size_t)nn[1] * k)] =
+              (*out_flags_)[(src[0][i] - 1) + (size_t)n_[0] * ((src[1][j] - 1) + (size_t)n_[1] * (src[2][k] - 1))];
+    return lcs_grid_from_lines(d, line, F, type, msg);
+  }
+
+  // An lcs grid from its coordinate lines and interior flags: host set-up, device tables, and
+  // every node tracked to the solver grid (forward sets with the periodic wrap).
+  bool lcs_grid_from_lines(DiagT &d, const std::vector<lcsdata_t> line[3], const std::vector<int> &F, int type, std::string &msg) {
     auto lg = std::make_shared<LcsGrid<T>>();
     const int nn[3] = {(int)line[0].size(), (int)line[1].size(), (int)line[2].size()};
     const long N = (long)nn[0] * nn[1] * nn[2];
     std::vector<lcsdata_t> X(N), Y(N), Z(N);
-    std::vector<int> F(N);
     for (int k = 0; k < nn[2]; k++)
       for (int j = 0; j < nn[1]; j++)
         for (int i = 0; i < nn[0]; i++) {
@@ -1164,7 +1201,6 @@ class Engine : public EngineBase {
           X[q] = line[0][i];
           Y[q] = line[1][j];
           Z[q] = line[2][k];
-          F[q] = (*out_flags_)[(src[0][i] - 1) + (size_t)n_[0] * ((src[1][j] - 1) + (size_t)n_[1] * (src[2][k] - 1))];
         }
     if (!lg->hg.build(nn, X.data(), Y.data(), Z.data(), F.data())) {
       msg = lg->hg.error;
@@ -1185,6 +1221,118 @@ class Engine : public EngineBase {
     CK(cudaGetLastError());
     counters_.kernel_launches++;
     d.lg = lg;
+    return true;
+  }
+
+  // create_aux_grid (src/lcs_m.f90:225-435) for diagnostic diags_[pi]: per node, 0.2
+  // (AUX_GRID_SCALING) times the mean distance to its in-bounds face neighbours; six copies of
+  // the nodes shifted by -/+ that along x, y, z (projected back into the data plane on a 2-D
+  // grid), each the nodes of an auxiliary grid with the lcs grid's flags and a particle set of
+  // its own.  The device keeps coordinate lines, so each auxiliary grid must be a tensor
+  // product to rounding (uniform spacing around every node, as on a cube); the per-node
+  // separations of each pair are kept exactly for the gradient.
+  bool create_aux(int pi, std::string &msg) {
+    const DiagT par = diags_[pi];  // copy: diags_ grows below
+    const HostGrid<lcsdata_t> &bg = par.lg ? par.lg->hg : hg_;
+    const int n[3] = {bg.P.n[0], bg.P.n[1], bg.P.n[2]};
+    const long N = (long)n[0] * n[1] * n[2];
+    static const int face[6][3] = {{-1, 0, 0}, {0, -1, 0}, {0, 0, -1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    std::vector<lcsdata_t> delta(N), x3[6][3];
+    std::vector<int> F(N);
+    long q = 0;
+    for (int k = 1; k <= n[2]; k++)
+      for (int j = 1; j <= n[1]; j++)
+        for (int i = 1; i <= n[0]; i++, q++) {
+          lcsdata_t nbrsum = 0, distsum = 0;
+          for (int nb = 0; nb < 6; nb++) {
+            const int ii = i + face[nb][0], jj = j + face[nb][1], kk = k + face[nb][2];
+            if (ii > 0 && jj > 0 && kk > 0 && ii <= n[0] && jj <= n[1] && kk <= n[2]) {
+              nbrsum = nbrsum + lcsdata_t(1);
+              const lcsdata_t dx = bg.coord(0, i, j, k) - bg.coord(0, ii, jj, kk), dy = bg.coord(1, i, j, k) - bg.coord(1, ii, jj, kk),
+                              dz = bg.coord(2, i, j, k) - bg.coord(2, ii, jj, kk);
+              distsum = distsum + std::sqrt(dx * dx + dy * dy + dz * dz);
+            }
+          }
+          delta[q] = distsum / nbrsum * lcsdata_t(0.2);
+          F[q] = bg.flag.empty() ? 0 : (int)bg.flag[bg.pidx(i, j, k)];
+        }
+    const int sa = bg.P.single_axis;
+    for (int m = 0; m < 6; m++) {
+      const int a = m % 3;
+      for (int c = 0; c < 3; c++) x3[m][c].resize(N);
+      q = 0;
+      for (int k = 1; k <= n[2]; k++)
+        for (int j = 1; j <= n[1]; j++)
+          for (int i = 1; i <= n[0]; i++, q++) {
+            for (int c = 0; c < 3; c++) x3[m][c][q] = bg.coord(c, i, j, k);
+            x3[m][a][q] = m < 3 ? x3[m][a][q] - delta[q] : x3[m][a][q] + delta[q];
+            // project_lp2plane on an axis-aligned plane: x - ((x - x_node) . n) n
+            if (sa >= 0) x3[m][sa][q] = x3[m][sa][q] - (x3[m][sa][q] - bg.coord(sa, i, j, k));
+          }
+    }
+    // each auxiliary grid's coordinate lines (first row), checked against every node
+    std::vector<int> idx;
+    for (int m = 0; m < 6; m++) {
+      std::vector<lcsdata_t> line[3];
+      for (int i = 0; i < n[0]; i++) line[0].push_back(x3[m][0][i]);
+      for (int j = 0; j < n[1]; j++) line[1].push_back(x3[m][1][(size_t)n[0] * j]);
+      for (int k = 0; k < n[2]; k++) line[2].push_back(x3[m][2][(size_t)n[0] * n[1] * k]);
+      lcsdata_t span = 0, dev = 0;
+      q = 0;
+      for (int k = 0; k < n[2]; k++)
+        for (int j = 0; j < n[1]; j++)
+          for (int i = 0; i < n[0]; i++, q++) {
+            const int id[3] = {i, j, k};
+            for (int c = 0; c < 3; c++) {
+              dev = std::max(dev, (lcsdata_t)std::fabs((double)(x3[m][c][q] - line[c][id[c]])));
+              span = std::max(span, (lcsdata_t)std::fabs((double)x3[m][c][q]));
+            }
+          }
+      if (dev > lcsdata_t(64) * std::numeric_limits<lcsdata_t>::epsilon() * std::max(span, lcsdata_t(1))) {
+        msg = "AUX_GRID: an auxiliary grid is not a tensor product (the grid spacing differs around some node); "
+              "this library supports AUX_GRID on uniformly spaced grids only";
+        return false;
+      }
+      DiagT A;
+      A.handle = 0;
+      A.type = par.type;
+      A.T_ = par.T_;
+      A.h = par.h;
+      A.dt_factor = par.dt_factor;
+      A.nslot = par.nslot;
+      A.aux_parent = pi + 1;
+      if (!lcs_grid_from_lines(A, line, F, par.type, msg)) return false;
+      if (!alloc_diag(A, msg)) return false;
+      diags_.push_back(A);
+      idx.push_back((int)diags_.size() - 1);
+    }
+    DiagT &P = diags_[pi];
+    P.aux = idx;
+    for (int a = 0; a < 3; a++) {
+      std::vector<lcsdata_t> den(N);
+      for (long r = 0; r < N; r++) den[r] = x3[a + 3][a][r] - x3[a][a][r];
+      if (!(P.auxden[a] = upload(den, msg))) return false;
+    }
+    if (cudaStreamSynchronize(stream_) != cudaSuccess) {
+      msg = "CUDA error in sync";
+      return false;
+    }
+    return true;
+  }
+
+  bool launch_ftle_aux(DiagT &d, std::string &msg) {
+    const DevGrid<T> &g = dgrid(d);
+    AuxMaps<T> M{};
+    for (int a = 0; a < 3; a++) {
+      for (int c = 0; c < 3; c++) {
+        M.lo[a][c] = diags_[d.aux[a]].composed[c];
+        M.hi[a][c] = diags_[d.aux[a + 3]].composed[c];
+      }
+      M.den[a] = d.auxden[a];
+    }
+    counters_.kernel_launches++;
+    k_ftle_aux<T, lcsdata_t><<<node_grid(g), dim3(32, 8, 1), 0, stream_>>>(g, M, d.ftle, d.T_, opt_->incompressible);
+    CK(cudaGetLastError());
     return true;
   }
 
@@ -1580,6 +1728,7 @@ class Engine : public EngineBase {
   }
 
   const Options *opt_;
+  int handle_count_ = 0;  // handles given out so far (a failed LP_TRACER injection uses one up)
   std::unique_ptr<LcsWriter> writer_;  // created by the first output file
   std::shared_ptr<const std::vector<double>> out_lines_[3];
   std::shared_ptr<const std::vector<int8_t>> out_flags_;

@@ -502,6 +502,45 @@ __global__ void __launch_bounds__(256) k_ftle(DevGrid<T> g, FieldPtrs<T> fm, R *
   ftle[interior_index(g.P.n, i, j, k)] = v;
 }
 
+// FTLE with AUX_GRID (compute_ftle, src/lcs_m.f90:95-127): the displacement gradient from the
+// composed maps of the six auxiliary particle sets, d fm_c / d x_a = (fm_c[a+ side] - fm_c[a-
+// side]) / den_a, den_a the separation of the two auxiliary nodes (left 0 where it is not
+// above 100 tiny); then the same Cauchy-Green, eigenvalue and log as k_ftle.
+template <typename T>
+struct AuxMaps {
+  const T *lo[3][3];  // [axis][component]: composed maps of the X0, Y0, Z0 sets (interior)
+  const T *hi[3][3];  // X1, Y1, Z1
+  const T *den[3];    // per node separation along each axis
+};
+
+template <typename T, typename R>
+__global__ void __launch_bounds__(256) k_ftle_aux(DevGrid<T> g, const __grid_constant__ AuxMaps<T> M, R *__restrict__ ftle, R Tint,
+                                                  int incompressible) {
+  int i, j, k;
+  if (!node_of_thread(g.P.n, i, j, k)) return;
+  const int q = interior_index(g.P.n, i, j, k);
+  const T small = T(100) * (sizeof(T) == 8 ? (T)DBL_MIN : (T)FLT_MIN);
+  double G[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const T den = M.den[a][q];
+#pragma unroll
+    for (int c = 0; c < 3; c++) G[c][a] = fabs(den) > small ? (double)((M.hi[a][c][q] - M.lo[a][c][q]) / den) : 0.0;
+  }
+  double C[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) C[a][b] = G[0][a] * G[0][b] + G[1][a] * G[1][b] + G[2][a] * G[2][b];
+  const double lam = eig3_max(C[0][0], C[0][1], C[0][2], C[1][1], C[1][2], C[2][2]);
+  const R sq = sqrt((R)lam);
+  const R tiny = sizeof(R) == 8 ? (R)DBL_MIN : (R)FLT_MIN;
+  const R mx = sq > tiny ? sq : tiny;
+  R v = log(mx) / Tint;
+  if (incompressible) v = v > R(0) ? v : R(0);
+  ftle[q] = v;
+}
+
 // ---------------------------------------------------------------------------------------
 // Velocity invariants (compute_invariants, src/invariants_m.f90:15-208) of one frame from
 // the velocity snapshot of the reconstruction's starting step (nodal values, interior

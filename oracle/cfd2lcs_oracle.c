@@ -112,7 +112,7 @@ typedef struct {
     const struct sgrid_s *sg; /* lp%sgrid: the grid of the particle set (the lcs grid) */
 } lp_t;
 
-typedef struct {
+typedef struct lcs_s {
     int id;
     int diagnostic;
     real T, h;
@@ -125,6 +125,8 @@ typedef struct {
     int dead;        /* an LP_TRACER set that was never injected or outlived T (destroy_lcs) */
     sgrid_t *sg;     /* lcs%sgrid: the solver grid (resolution 0) or its own refined copy */
     int own_sg;
+    struct lcs_s *aux[6]; /* AUX_GRID particle sets X0, Y0, Z0, X1, Y1, Z1 (lcs%lpX0 ...) */
+    int naux;
     int nslot;
     real **slot[3]; /* slot[c][s] -> interior values of stored sub-flow map */
     int *written;
@@ -1353,6 +1355,16 @@ static void update_flowmap_sl(lp_t *lp) {
     free(mask);
 }
 
+/* exchange_lpmap at one rank (comms_m.f90:1191-1376): fm(no0) = dx, particle order = node order */
+static void lpmap_to_fm(lcs_t *L) {
+    const dims_t *dl = &L->sg->d;
+    int ip = 0;
+    for (int k = 1; k <= dl->nk; k++)
+        for (int j = 1; j <= dl->nj; j++)
+            for (int ii = 1; ii <= dl->ni; ii++, ip++)
+                for (int c = 0; c < 3; c++) L->lp.fm.c[c][PX(dl, ii, j, k)] = L->lp.dx[c][ip];
+}
+
 /* Forward particle update, lp_motion_m.f90:15-54 */
 static void update_lp(lp_t *lp) {
     real dt;
@@ -1546,15 +1558,27 @@ static void compute_ftle(lcs_t *L) {
                 long pyp = PX(d, i, j + 1, k), pym = PX(d, i, j - 1, k);
                 long pzp = PX(d, i, j, k + 1), pzm = PX(d, i, j, k - 1);
                 real G[3][3]; /* G[c][a] = d fm_c / d x_a */
-                for (int c = 0; c < 3; c++) {
-                    const real *F = fm->c[c];
-                    G[c][0] = (F[pxp] - F[pxm]) / (X[pxp] - X[pxm]);
-                    G[c][1] = (F[pyp] - F[pym]) / (Y[pyp] - Y[pym]);
-                    G[c][2] = (F[pzp] - F[pzm]) / (Z[pzp] - Z[pzm]);
+                if (L->naux) {
+                    /* AUX_GRID (lcs_m.f90:95-127): differences of the X1/X0, Y1/Y0, Z1/Z0 maps over
+                     * the aux grids' separation, left 0 where that is not above SMALL */
+                    const real SMALL = (real)100.0 * R_TINY;
+                    for (int a = 0; a < 3; a++) {
+                        const lcs_t *A0 = L->aux[a], *A1 = L->aux[a + 3];
+                        const real den = A1->sg->grid.c[a][p] - A0->sg->grid.c[a][p];
+                        for (int c = 0; c < 3; c++)
+                            G[c][a] = (real)fabs((double)den) > SMALL ? (A1->lp.fm.c[c][p] - A0->lp.fm.c[c][p]) / den : (real)0;
+                    }
+                } else {
+                    for (int c = 0; c < 3; c++) {
+                        const real *F = fm->c[c];
+                        G[c][0] = (F[pxp] - F[pxm]) / (X[pxp] - X[pxm]);
+                        G[c][1] = (F[pyp] - F[pym]) / (Y[pyp] - Y[pym]);
+                        G[c][2] = (F[pzp] - F[pzm]) / (Z[pzp] - Z[pzm]);
+                    }
+                    for (int a = 0; a < 3; a++)
+                        if (g->gn[a] == 1)
+                            for (int c = 0; c < 3; c++) G[c][a] = 0;
                 }
-                for (int a = 0; a < 3; a++)
-                    if (g->gn[a] == 1)
-                        for (int c = 0; c < 3; c++) G[c][a] = 0;
                 /* cg_ab = sum_c G[c][a]*G[c][b], lcs_m.f90:137-145 */
                 real C[3][3];
                 for (int a = 0; a < 3; a++)
@@ -1841,6 +1865,7 @@ EXPORT int orc_get_threads(void) {
 
 static void free_lcs(lcs_t *L) {
     if (!L) return;
+    for (int m = 0; m < L->naux; m++) free_lcs(L->aux[m]);
     for (int c = 0; c < 3; c++) {
         free(L->lp.xp[c]); free(L->lp.up[c]); free(L->lp.dx[c]);
         free(L->lp.no[c]); free(L->lp.no_scfd[c]);
@@ -2059,6 +2084,97 @@ EXPORT int orc_get_tracers(int handle, real *out) {
     return 1;
 }
 
+/* One auxiliary particle set on grid ag (init_lp on lcs%lpX0 ...): the parent's direction,
+ * dt_factor, T and h, its own flow map and ring. */
+static lcs_t *aux_set(const lcs_t *P, sgrid_t *ag) {
+    const dims_t *d = &ag->d;
+    lcs_t *A = (lcs_t *)calloc(1, sizeof(lcs_t));
+    A->diagnostic = P->diagnostic;
+    A->T = P->T;
+    A->h = P->h;
+    A->sg = ag;
+    A->own_sg = 1;
+    A->lp.sg = ag;
+    lp_alloc(&A->lp, d->ni * d->nj * d->nk);
+    sr1_alloc(&A->lp.fm, d);
+    sr1_alloc(&A->fm_out, d);
+    A->lp.direction = P->lp.direction;
+    A->lp.dt_factor = P->lp.dt_factor;
+    reset_lp(ag, &A->lp, 1);
+    track_lp2node(&S.g, &A->lp, A->lp.no_scfd);
+    A->nslot = P->nslot;
+    A->written = (int *)calloc((size_t)A->nslot, sizeof(int));
+    long nint_ = (long)d->ni * d->nj * d->nk;
+    for (int c = 0; c < 3; c++) {
+        A->slot[c] = (real **)calloc((size_t)A->nslot, sizeof(real *));
+        for (int q = 0; q < A->nslot; q++) A->slot[c][q] = zalloc(nint_);
+    }
+    return A;
+}
+
+/* create_aux_grid (lcs_m.f90:225-435): per node, AUX_GRID_SCALING (0.2) times the mean
+ * distance to its in-bounds face neighbours; six copies of the set's particles shifted by
+ * -/+ that along x, y, z, projected into the data plane (2-D), each the nodes of a new grid
+ * with the lcs grid's flags and a particle set of its own. */
+static void create_aux(lcs_t *L) {
+    const sgrid_t *g = L->sg;
+    const dims_t *d = &g->d;
+    const long N = (long)d->ni * d->nj * d->nk;
+    const int n[3] = {d->ni, d->nj, d->nk};
+    real *delta = zalloc(N);
+    const real *X = g->grid.c[0], *Y = g->grid.c[1], *Z = g->grid.c[2];
+    long q = 0;
+    for (int k = 1; k <= d->nk; k++)
+        for (int j = 1; j <= d->nj; j++)
+            for (int i = 1; i <= d->ni; i++, q++) {
+                real nbrsum = 0, distsum = 0;
+                for (int nb = 1; nb <= 6; nb++) {
+                    const int ii = i + NBR[nb][0], jj = j + NBR[nb][1], kk = k + NBR[nb][2];
+                    if (ii > 0 && jj > 0 && kk > 0 && ii <= d->ni && jj <= d->nj && kk <= d->nk) {
+                        nbrsum = nbrsum + (real)1.0;
+                        const long p = PX(d, i, j, k), pn = PX(d, ii, jj, kk);
+                        const real dx = X[p] - X[pn], dy = Y[p] - Y[pn], dz = Z[p] - Z[pn];
+                        distsum = distsum + (real)sqrt((double)(dx * dx + dy * dy + dz * dz));
+                    }
+                }
+                delta[q] = distsum / nbrsum * (real)0.2;
+            }
+    real *xs[3] = {zalloc(N), zalloc(N), zalloc(N)};
+    int *fl = (int *)calloc((size_t)N, sizeof(int));
+    q = 0;
+    for (int k = 1; k <= d->nk; k++)
+        for (int j = 1; j <= d->nj; j++)
+            for (int i = 1; i <= d->ni; i++) fl[q++] = g->bcflag[PX(d, i, j, k)];
+    for (int m = 0; m < 6 && !S.error; m++) {
+        const int a = m % 3;
+        lp_t dum;
+        memset(&dum, 0, sizeof dum);
+        lp_alloc(&dum, (int)N);
+        q = 0;
+        for (int k = 1; k <= d->nk; k++)
+            for (int j = 1; j <= d->nj; j++)
+                for (int i = 1; i <= d->ni; i++, q++) {
+                    for (int c = 0; c < 3; c++) dum.xp[c][q] = L->lp.xp[c][q];
+                    dum.xp[a][q] = m < 3 ? L->lp.xp[a][q] - delta[q] : L->lp.xp[a][q] + delta[q];
+                    dum.no[0][q] = i; dum.no[1][q] = j; dum.no[2][q] = k;
+                }
+        project_lp2plane(g, &dum, dum.no);
+        for (int c = 0; c < 3; c++) memcpy(xs[c], dum.xp[c], sizeof(real) * (size_t)N);
+        for (int c = 0; c < 3; c++) { free(dum.xp[c]); free(dum.up[c]); free(dum.dx[c]); free(dum.no[c]); free(dum.no_scfd[c]); }
+        free(dum.flag);
+        sgrid_t *ag = (sgrid_t *)calloc(1, sizeof(sgrid_t));
+        if (init_sgrid(ag, n, xs[0], xs[1], xs[2], fl) || !ag->rectilinear) {
+            if (!S.error) latch("AUX_GRID: an auxiliary grid is not rectilinear (the TSE path is not restated)");
+            free(ag);
+            break;
+        }
+        L->aux[m] = aux_set(L, ag);
+        L->naux = m + 1;
+    }
+    free(delta); free(fl);
+    for (int c = 0; c < 3; c++) free(xs[c]);
+}
+
 EXPORT int orc_diagnostic_init(int type, int resolution, real T, real h, const char *label) {
     if (S.error) return -1;
     if (!S.inited) { latch("diagnostic_init before init"); return -1; }
@@ -2110,6 +2226,10 @@ EXPORT int orc_diagnostic_init(int type, int resolution, real T, real h, const c
         for (int s = 0; s < L->nslot; s++) L->slot[c][s] = zalloc(nint_);
     }
     S.lcs[S.nlcs++] = L;
+    if (S.aux_grid) {
+        create_aux(L);
+        if (S.error) return -1;
+    }
     return L->id;
 }
 
@@ -2142,9 +2262,11 @@ EXPORT void orc_update(const int n[3], const real *u, const real *v, const real 
     set_velocity_bc(&S.g, &S.u_np1);
     for (int i = 0; i < S.nlcs && !S.error; i++) {
         if (S.lcs[i]->dead) continue;
-        lp_t *lp = &S.lcs[i]->lp;
-        if (lp->direction == FWD) update_lp(lp);
-        else update_flowmap_sl(lp);
+        for (int m = -1; m < S.lcs[i]->naux && !S.error; m++) {
+            lp_t *lp = m < 0 ? &S.lcs[i]->lp : &S.lcs[i]->aux[m]->lp;
+            if (lp->direction == FWD) update_lp(lp);
+            else update_flowmap_sl(lp);
+        }
     }
     for (int i = 0; i < S.nlcs && !S.error; i++) {
         lcs_t *L = S.lcs[i];
@@ -2168,6 +2290,17 @@ EXPORT void orc_update(const int n[3], const real *u, const real *v, const real 
                     for (int ii = 1; ii <= dl->ni; ii++, ip++)
                         for (int c = 0; c < 3; c++) L->lp.fm.c[c][PX(dl, ii, j, k)] = L->lp.dx[c][ip];
         }
+        if (S.aux_grid && !L->naux) {
+            latch("AUX_GRID was set after cfd2lcs_diagnostic_init: no auxiliary particle sets exist");
+            return;
+        }
+        /* the auxiliary sets go through the same substep, reconstruction and reset
+         * (cfd2lcs.f90:151-222) */
+        for (int m = 0; m < L->naux; m++) {
+            if (L->diagnostic == FTLE_FWD) lpmap_to_fm(L->aux[m]);
+            write_substep(L->aux[m]);
+            reconstruct(L->aux[m]);
+        }
         write_substep(L);
         /* the starting step of the reconstruction: the current one (backward) or the next,
          * not yet wrapped (forward), flowmap_m.f90:202-209 */
@@ -2180,6 +2313,10 @@ EXPORT void orc_update(const int n[3], const real *u, const real *v, const real 
         S.ftle_frames++;
         reset_lp(L->sg, &L->lp, 1);
         track_lp2node(&S.g, &L->lp, L->lp.no_scfd);
+        for (int m = 0; m < L->naux; m++) {
+            reset_lp(L->aux[m]->sg, &L->aux[m]->lp, 1);
+            track_lp2node(&S.g, &L->aux[m]->lp, L->aux[m]->lp.no_scfd);
+        }
     }
 }
 
