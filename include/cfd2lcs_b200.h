@@ -43,7 +43,8 @@ void cfd2lcs_update_device_c(int n[3], const lcsdata_t *d_u, const lcsdata_t *d_
 
 /* Velocity invariants of a diagnostic's latest frame, computed when the option
  * VELOCITY_INVARIANTS is TRUE (compute_invariants, src/invariants_m.f90:15-208, which the
- * reference writes to its output file): five consecutive arrays of n[0]*n[1]*n[2] values --
+ * reference writes to its output file): five consecutive arrays of n[0]*n[1]*n[2] values (the
+ * diagnostic's grid, cfd2lcs_diagnostic_size_c) --
  * Q-criterion flag, D zone (1..4), C (R_S > 0) flag, H and the lambda-2 flag.  Returns 0, or
  * 1 for an unknown handle, no frame yet or the option off. */
 int cfd2lcs_get_invariants_c(int lcs_handle, lcsdata_t *inv);

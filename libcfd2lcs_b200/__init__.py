@@ -219,11 +219,12 @@ class Cfd2lcs:
 
     def invariants(self, handle):
         """Q, D, C, H, L2 of the last frame (VELOCITY_INVARIANTS), shape (5, ni, nj, nk)."""
-        out = np.zeros(5 * int(np.prod(self.n)), dtype=self.dtype)
+        n = self.diag_size(handle)
+        out = np.zeros(5 * int(np.prod(n)), dtype=self.dtype)
         if self.lib.cfd2lcs_get_invariants_c(int(handle), self._p(out)) != 0:
             raise RuntimeError("no invariants for this handle")
-        N = int(np.prod(self.n))
-        return np.stack([out[q * N:(q + 1) * N].reshape(self.n, order="F") for q in range(5)])
+        N = int(np.prod(n))
+        return np.stack([out[q * N:(q + 1) * N].reshape(n, order="F") for q in range(5)])
 
     def tracers(self, handle):
         """Positions of an LP_TRACER set, shape (3, count)."""

@@ -75,6 +75,11 @@ struct LcsGrid {
   int *nos_reset[3] = {nullptr, nullptr, nullptr};
   int *nos[3] = {nullptr, nullptr, nullptr};
   SplineSet<T> sp[4];  // B-spline axes of the lcs grid by degree (flow-map fits and samples)
+  // output files: coordinate lines and interior flags; lp%ugrid (the frame's velocity at the
+  // nodes, T) and the padded snapshot / its coefficients it is sampled from (solver grid, TV)
+  std::shared_ptr<const std::vector<double>> out_lines[3];
+  std::shared_ptr<const std::vector<int8_t>> out_flags;
+  T *ugrid[3] = {nullptr, nullptr, nullptr};
 };
 
 template <typename T, typename TV>
@@ -533,10 +538,6 @@ class Engine : public EngineBase {
       if ((d.aux_parent != 0) != (pass == 0)) continue;
       if (!d.active) continue;
       if ((long)(t_np1_ / d.h) == (long)(t_n_ / d.h)) continue;
-      if (d.lg && !d.aux_parent && (opt_->velocity_invariants || opt_->write_lcs)) {
-        msg = "VELOCITY_INVARIANTS and WRITE_LCS are not supported for diagnostics with resolution /= 0";
-        return false;
-      }
       if (d.type == LP_TRACER) {
         // write_lcs, then the end of the tracers' lifetime (src/cfd2lcs.f90:225-231)
         if (opt_->write_lcs && !enqueue_tracer_output(d, msg)) return false;
@@ -601,6 +602,8 @@ class Engine : public EngineBase {
           return false;
         }
         if (d.aux.empty() ? !launch_ftle(d, msg) : !launch_ftle_aux(d, msg)) return false;
+        // lp%ugrid of a refined lcs grid, read by the invariants and the output file
+        if (d.lg && need_velocity_ring() && !make_ugrid(d, wslot + (d.type == FTLE_FWD ? 1 : 0), msg)) return false;
         // compute_invariants from the velocity of the reconstruction's starting step: the
         // current one (backward) or the next, not yet wrapped (forward), flowmap_m.f90:202-245
         if (opt_->velocity_invariants && !launch_invariants(d, wslot + (d.type == FTLE_FWD ? 1 : 0), msg)) return false;
@@ -756,7 +759,8 @@ class Engine : public EngineBase {
       return false;
     }
     CK(cudaStreamSynchronize(stream_));
-    for (int q = 0; q < 5; q++) CK(cudaMemcpy(out + (size_t)q * N_, d->inv[q], N_ * sizeof(lcsdata_t), cudaMemcpyDeviceToHost));
+    const long nd = dN(*d);
+    for (int q = 0; q < 5; q++) CK(cudaMemcpy(out + (size_t)q * nd, d->inv[q], nd * sizeof(lcsdata_t), cudaMemcpyDeviceToHost));
     return true;
   }
 
@@ -1206,6 +1210,8 @@ class Engine : public EngineBase {
       msg = lg->hg.error;
       return false;
     }
+    for (int a = 0; a < 3; a++) lg->out_lines[a] = std::make_shared<std::vector<double>>(line[a].begin(), line[a].end());
+    lg->out_flags = std::make_shared<std::vector<int8_t>>(F.begin(), F.end());
     if (!make_dev_grid(lg->hg, lg->dg, msg)) return false;
     lg->N = N;
     lg->ntot = lg->hg.ntot();
@@ -1592,11 +1598,14 @@ class Engine : public EngineBase {
     if (!writer_) writer_.reset(new LcsWriter());
     OutputJob job;
     job.path = "./cfd2lcs_output/" + d.label + "_" + idx + ".dat";
+    const long NN = dN(d);
+    int nn[3];
     for (int a = 0; a < 3; a++) {
-      job.n[a] = n_[a];
-      job.lines[a] = out_lines_[a];
+      nn[a] = d.lg ? d.lg->dg.P.n[a] : n_[a];
+      job.n[a] = nn[a];
+      job.lines[a] = d.lg ? d.lg->out_lines[a] : out_lines_[a];
     }
-    job.flags = out_flags_;
+    job.flags = d.lg ? d.lg->out_flags : out_flags_;
     const std::string title = d.label + "-FTLE";
     std::string h = "TITLE = \"" + title + "\"\nVARIABLES =\n\"X\"\n\"Y\"\n\"Z\"\n";
     if (opt_->write_flowmap) h += "\"FM-X\"\n\"FM-Y\"\n\"FM-Z\"\n";
@@ -1609,7 +1618,7 @@ class Engine : public EngineBase {
     tbuf[18] = 0;
     std::snprintf(line, sizeof(line), "STRANDID = %010d, SOLUTIONTIME = %s\n", 1, tbuf);
     h += line;
-    std::snprintf(line, sizeof(line), "I = %010d J = %010d K = %010d\n", n_[0], n_[1], n_[2]);
+    std::snprintf(line, sizeof(line), "I = %010d J = %010d K = %010d\n", nn[0], nn[1], nn[2]);
     h += line;
     h += "ZONETYPE = Ordered, DATAPACKING = BLOCK\n";
     job.header = h;
@@ -1625,7 +1634,7 @@ class Engine : public EngineBase {
       OutputBlock b;
       b.kind = esize == 8 ? OutputBlock::STAGED_F64 : OutputBlock::STAGED_F32;
       b.offset = bytes;
-      bytes += ((size_t)N_ * esize + 255) / 256 * 256;
+      bytes += ((size_t)NN * esize + 255) / 256 * 256;
       staged.push_back({p, esize});
       blocks.push_back(b);
     };
@@ -1643,7 +1652,8 @@ class Engine : public EngineBase {
       // lp%ugrid: the frame's starting velocity when its snapshot exists, else zero (reset_lp)
       const bool have = ustep >= 0 && ustep < (long)vwritten_.size() && vwritten_[ustep];
       for (int c = 0; c < 3; c++) {
-        if (have) stage(vring_[3 * ustep + c], sizeof(TV));
+        if (d.lg) stage(d.lg->ugrid[c], sizeof(T));
+        else if (have) stage(vring_[3 * ustep + c], sizeof(TV));
         else plain(OutputBlock::ZERO);
       }
     }
@@ -1659,7 +1669,7 @@ class Engine : public EngineBase {
     size_t q = 0;
     for (OutputBlock &b : blocks) {
       if (b.kind != OutputBlock::STAGED_F64 && b.kind != OutputBlock::STAGED_F32) continue;
-      CK(cudaMemcpyAsync(static_cast<char *>(buf) + b.offset, staged[q].p, (size_t)N_ * staged[q].esize, cudaMemcpyDeviceToHost,
+      CK(cudaMemcpyAsync(static_cast<char *>(buf) + b.offset, staged[q].p, (size_t)NN * staged[q].esize, cudaMemcpyDeviceToHost,
                          stream_));
       q++;
     }
@@ -1673,10 +1683,71 @@ class Engine : public EngineBase {
     return true;
   }
 
+  // lp%ugrid of a refined diagnostic (reconstruct_flowmap, src/flowmap_m.f90:214-245): zero
+  // (reset_lp) unless the snapshot of ring step ustep exists, else that snapshot padded with
+  // its periodic images, fitted when the interpolator is a B-spline, and sampled at the nodes.
+  bool make_ugrid(DiagT &d, long ustep, std::string &msg) {
+    LcsGrid<T> &L = *d.lg;
+    if (!L.ugrid[0])
+      for (int c = 0; c < 3; c++)
+        if (!(L.ugrid[c] = arena_.alloc<T>(L.N, msg))) return false;
+    const bool have = ustep >= 0 && ustep < (long)vwritten_.size() && vwritten_[ustep];
+    if (!have) {
+      for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(L.ugrid[c], 0, L.N * sizeof(T), stream_));
+      return true;
+    }
+    if (!upad_[0])
+      for (int c = 0; c < 3; c++)
+        if (!(upad_[c] = arena_.alloc<TV>(ntot_, msg)) || !(upcoef_[c] = arena_.alloc<TV>(ntot_, msg))) return false;
+    FieldPtrs<TV> src{};
+    FieldPtrsW<TV> dst{};
+    for (int c = 0; c < 3; c++) {
+      src.f[c] = vring_[3 * ustep + c];
+      dst.f[c] = upad_[c];
+    }
+    k_pad_snapshot<T, TV><<<(unsigned)((ntot_ + 255) / 256), 256, 0, stream_>>>(dg_, src, dst, ntot_);
+    counters_.kernel_launches++;
+    const int interp = opt_->interpolator;
+    const bool spline = interp == QUADRATIC || interp == CUBIC;
+    VelFields<TV> V{};
+    SplineAxes<T> sa{};
+    for (int c = 0; c < 3; c++) V.un[c] = V.unp1[c] = upad_[c];
+    if (spline) {
+      const int deg = interp == QUADRATIC ? 2 : 3;
+      if (!ensure_spline(deg, msg) || !fit(vsplines_[deg].axes, upad_, upcoef_, msg)) return false;
+      for (int c = 0; c < 3; c++) V.cs[0][c] = upcoef_[c];
+      sa = splines_[deg].axes;
+    }
+    FieldPtrsW<T> out{};
+    for (int c = 0; c < 3; c++) out.f[c] = L.ugrid[c];
+    const dim3 grd = node_grid(L.dg), blk(32, 8, 1);
+    const int iv = interp_variant(interp, sa);
+    if (iv == INTERP_NEAREST) k_sample_ugrid<T, TV, INTERP_NEAREST><<<grd, blk, 0, stream_>>>(L.dg, dg_, sa, V, out);
+    else if (iv == INTERP_LINEAR) k_sample_ugrid<T, TV, INTERP_LINEAR><<<grd, blk, 0, stream_>>>(L.dg, dg_, sa, V, out);
+    else if (iv == INTERP_SPLINE4) k_sample_ugrid<T, TV, INTERP_SPLINE4><<<grd, blk, 0, stream_>>>(L.dg, dg_, sa, V, out);
+    else k_sample_ugrid<T, TV, INTERP_SPLINE><<<grd, blk, 0, stream_>>>(L.dg, dg_, sa, V, out);
+    counters_.kernel_launches++;
+    CK(cudaGetLastError());
+    return true;
+  }
+
   bool launch_invariants(DiagT &d, long ustep, std::string &msg) {
     if (!d.inv[0])
       for (int q = 0; q < 5; q++)
-        if (!(d.inv[q] = arena_.alloc<lcsdata_t>(N_, msg))) return false;
+        if (!(d.inv[q] = arena_.alloc<lcsdata_t>(dN(d), msg))) return false;
+    if (d.lg) {
+      // the invariants of the lcs grid's lp%ugrid (gradient on the lcs grid)
+      FieldPtrs<T> u{};
+      for (int c = 0; c < 3; c++) u.f[c] = d.lg->ugrid[c];
+      FieldPtrsW<T> o3{}, o2{};
+      for (int q = 0; q < 3; q++) o3.f[q] = d.inv[q];
+      o2.f[0] = d.inv[3];
+      o2.f[1] = d.inv[4];
+      k_invariants<T, T><<<node_grid(d.lg->dg), dim3(32, 8, 1), 0, stream_>>>(d.lg->dg, u, 1, o3, o2);
+      counters_.kernel_launches++;
+      CK(cudaGetLastError());
+      return true;
+    }
     const bool have = ustep >= 0 && ustep < (long)vwritten_.size() && vwritten_[ustep];
     FieldPtrs<TV> u{};
     for (int c = 0; c < 3; c++) u.f[c] = have ? vring_[3 * ustep + c] : nullptr;
@@ -1729,6 +1800,7 @@ class Engine : public EngineBase {
 
   const Options *opt_;
   int handle_count_ = 0;  // handles given out so far (a failed LP_TRACER injection uses one up)
+  TV *upad_[3] = {nullptr, nullptr, nullptr}, *upcoef_[3] = {nullptr, nullptr, nullptr};  // refined lp%ugrid scratch
   std::unique_ptr<LcsWriter> writer_;  // created by the first output file
   std::shared_ptr<const std::vector<double>> out_lines_[3];
   std::shared_ptr<const std::vector<int8_t>> out_flags_;

@@ -260,6 +260,51 @@ __global__ void __launch_bounds__(256) k_sl_refined(DevGrid<T> gl, DevGrid<T> gs
   write_ghosts<T, FL, GHOST_FM>(gl, fmn.f, i, j, k, vpre, vfin, err);
 }
 
+// The velocity snapshot on the padded solver grid as reconstruct_flowmap reads it back
+// (src/flowmap_m.f90:214-234): interior values, ghosts copied from their periodic images
+// (exchange_sdata with max connectivity: a ghost all of whose out-of-range directions are
+// periodic), every other ghost 0 (init_sr1; no velocity boundary rule here).
+template <typename T, typename TV>
+__global__ void __launch_bounds__(256) k_pad_snapshot(DevGrid<T> g, FieldPtrs<TV> src, FieldPtrsW<TV> dst, long ntot) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= ntot) return;
+  int idx[3] = {(int)(p % g.P.sx), (int)((p / g.P.sx) % (g.P.sxy / g.P.sx)), (int)(p / g.P.sxy)};
+  bool ok = true;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const int n = g.P.n[a];
+    if (idx[a] < 1 || idx[a] > n) {
+      if (!g.P.per[a]) ok = false;
+      idx[a] = idx[a] < 1 ? idx[a] + n : idx[a] - n;
+    }
+  }
+  const int q = ok ? interior_index(g.P.n, idx[0], idx[1], idx[2]) : 0;
+#pragma unroll
+  for (int c = 0; c < 3; c++) dst.f[c][p] = ok ? src.f[c][q] : TV(0);
+}
+
+// lp%ugrid of a refined lcs grid: the padded snapshot (V: its values as un = unp1, or its
+// spline coefficients as the stage-0 blend) sampled with the interpolator at every lcs node,
+// around the node reset_lp guesses (nint(real(i*ni_s)/real(ni_l)), not tracked).
+template <typename T, typename TV, int INTERP>
+__global__ void __launch_bounds__(256) k_sample_ugrid(DevGrid<T> gl, DevGrid<T> gs, SplineAxes<T> sa, VelFields<TV> V, FieldPtrsW<T> out) {
+  int i, j, k;
+  if (!node_of_thread(gl.P.n, i, j, k)) return;
+  const int q = interior_index(gl.P.n, i, j, k);
+  const T x[3] = {__ldg(gl.lt[0] + i), __ldg(gl.lt[1] + j), __ldg(gl.lt[2] + k)};
+  const int nd[3] = {i, j, k};
+  int no[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const float r = (float)(nd[a] * gs.P.n[a]) / (float)gl.P.n[a];
+    no[a] = min(max((int)roundf(r), 1), gs.P.n[a]);
+  }
+  T u[3];
+  sample_velocity<T, TV, INTERP>(gs, sa, V, x, no, T(0), 0, u);
+#pragma unroll
+  for (int c = 0; c < 3; c++) out.f[c][q] = u[c];
+}
+
 // Forward particles back to the lcs nodes (reset_lp + track_lp2node on the solver grid): the
 // positions and solver nodes k_track_lcs_nodes found, in node order.
 template <typename T>

@@ -1637,21 +1637,70 @@ static void eig3_all(const long double A_in[3][3], long double w[3]) {
  * the B-splines to rounding; a missing snapshot leaves the zeroed lp%ugrid), its central-
  * difference gradient with face exchange (grad_sr1, gradient_m.f90:11-66: periodic images,
  * zero ghosts elsewhere), and the Q, D, C, H and lambda-2 indicators. */
-static void compute_invariants(lcs_t *L, int ustep) {
-    const sgrid_t *g = &S.g;
+/* lp%ugrid of a frame (reconstruct_flowmap, flowmap_m.f90:214-245), on the set's own grid,
+ * zero (reset_lp) unless the snapshot of ring step ustep exists.  On the solver grid: the nodal
+ * values (the interpolators reproduce them at the nodes).  On a refined lcs grid: the
+ * snapshot padded with its periodic images (other ghosts 0), interpolated with the global
+ * interpolator at the lcs nodes around reset_lp's guessed solver nodes.  Periodic images of
+ * the result (exchange_sdata, scomm_max_r1). */
+static void make_ugrid(lcs_t *L, int ustep, sr1_t *ug) {
+    const sgrid_t *g = L->sg;
     const dims_t *d = &g->d;
-    sr1_t ug;
-    sr1_alloc(&ug, d);
-    if (ustep >= 0 && ustep < MAXVSTEP && S.vwritten[ustep]) {
+    sr1_alloc(ug, d);
+    if (!(ustep >= 0 && ustep < MAXVSTEP && S.vwritten[ustep])) return;
+    if (g == &S.g) {
         for (int c = 0; c < 3; c++) {
             const real *v = S.vring[c][ustep];
             long q = 0;
             for (int k = 1; k <= d->nk; k++)
                 for (int j = 1; j <= d->nj; j++)
-                    for (int i = 1; i <= d->ni; i++) ug.c[c][PX(d, i, j, k)] = v[q++];
+                    for (int i = 1; i <= d->ni; i++) ug->c[c][PX(d, i, j, k)] = v[q++];
         }
-        exchange_self(g, ug.c, 3, 1, 0); /* scomm_max_r1: periodic images, no boundary values */
+    } else {
+        const dims_t *ds = &S.g.d;
+        sr1_t ut;
+        sr1_alloc(&ut, ds);
+        for (int c = 0; c < 3; c++) {
+            const real *v = S.vring[c][ustep];
+            long q = 0;
+            for (int k = 1; k <= ds->nk; k++)
+                for (int j = 1; j <= ds->nj; j++)
+                    for (int i = 1; i <= ds->ni; i++) ut.c[c][PX(ds, i, j, k)] = v[q++];
+        }
+        exchange_self(&S.g, ut.c, 3, 1, 0);
+        const int np = d->ni * d->nj * d->nk;
+        real *xp[3], *up[3];
+        int *no[3];
+        for (int c = 0; c < 3; c++) {
+            xp[c] = zalloc(np);
+            up[c] = zalloc(np);
+            no[c] = (int *)calloc((size_t)np, sizeof(int));
+        }
+        int ip = 0;
+        for (int k = 1; k <= d->nk; k++)
+            for (int j = 1; j <= d->nj; j++)
+                for (int i = 1; i <= d->ni; i++, ip++) {
+                    for (int c = 0; c < 3; c++) xp[c][ip] = g->grid.c[c][PX(d, i, j, k)];
+                    no[0][ip] = clampi(fnint((real)((float)(i * ds->ni) / (float)d->ni)), 1, ds->ni);
+                    no[1][ip] = clampi(fnint((real)((float)(j * ds->nj) / (float)d->nj)), 1, ds->nj);
+                    no[2][ip] = clampi(fnint((real)((float)(k * ds->nk) / (float)d->nk)), 1, ds->nk);
+                }
+        interp_r1(&S.g, S.interpolator, np, xp, no, &ut, up);
+        ip = 0;
+        for (int k = 1; k <= d->nk; k++)
+            for (int j = 1; j <= d->nj; j++)
+                for (int i = 1; i <= d->ni; i++, ip++)
+                    for (int c = 0; c < 3; c++) ug->c[c][PX(d, i, j, k)] = up[c][ip];
+        for (int c = 0; c < 3; c++) { free(xp[c]); free(up[c]); free(no[c]); }
+        sr1_free(&ut);
     }
+    exchange_self(g, ug->c, 3, 1, 0); /* scomm_max_r1: periodic images, no boundary values */
+}
+
+static void compute_invariants(lcs_t *L, const sr1_t *ugp) {
+    const sgrid_t *g = L->sg;
+    const dims_t *d = &g->d;
+    const sr1_t ug = *ugp;
     const real *X = g->grid.c[0], *Y = g->grid.c[1], *Z = g->grid.c[2];
     const real eigth = (real)(1. / 8.), twenyforth = (real)(1. / 24.), coef = (real)(27. / 4.);
     for (int k = 1; k <= d->nk; k++)
@@ -1723,7 +1772,6 @@ static void compute_invariants(lcs_t *L, int ustep) {
                 long double big = fabsl(w[0]) > fabsl(w[2]) ? fabsl(w[0]) : fabsl(w[2]);
                 L->l2margin[p] = big > 0 ? (real)(w[1] / big) : (real)0;
             }
-    sr1_free(&ug);
 }
 
 /* Fortran ESw.d editing (the ES14.6 data and ES18.4 time fields of write_ftle): a signed
@@ -1763,10 +1811,11 @@ static void write_block(FILE *fp, const dims_t *d, const real *f, int compact) {
 
 /* write_lcs + write_ftle (io_nohdf5_m.f90:47-133, 183-264): file name from the time index
  * (minus T/h for FTLE_FWD) with the reference's per-range integer formats, the Tecplot
- * header, then the X, Y, Z, [FM], [U], [FLAG], [Q C D H L2], FTLE blocks.  ustep: the ring
- * step whose velocity snapshot is lp%ugrid (zero when it was never written, reset_lp). */
-static void write_lcs(lcs_t *L, int ustep) {
-    const dims_t *d = &S.g.d;
+ * header, then the X, Y, Z, [FM], [U], [FLAG], [Q C D H L2], FTLE blocks on the set's grid.
+ * ug: lp%ugrid of the frame (make_ugrid). */
+static void write_lcs(lcs_t *L, const sr1_t *ug) {
+    const sgrid_t *g = L->sg;
+    const dims_t *d = &g->d;
     long long findex = (long long)fnint(S.t_np1 / L->h);
     if (L->diagnostic == FTLE_FWD) findex -= (long long)fnint(L->T / L->h);
     if (findex < -999999999LL || findex > 999999999LL) { latch("ERROR: unsupported range for file index"); return; }
@@ -1787,19 +1836,17 @@ static void write_lcs(lcs_t *L, int ustep) {
     tfield[18] = 0;
     fprintf(fp, "\"FTLE\"\nZONE\nT = \"%s-FTLE\"\nSTRANDID = %010d, SOLUTIONTIME = %s\n", L->label, 1, tfield);
     fprintf(fp, "I = %010d J = %010d K = %010d\nZONETYPE = Ordered, DATAPACKING = BLOCK\n", d->ni, d->nj, d->nk);
-    for (int c = 0; c < 3; c++) write_block(fp, d, S.g.grid.c[c], 0);
+    for (int c = 0; c < 3; c++) write_block(fp, d, g->grid.c[c], 0);
     if (!S.no_flowmap_io)
         for (int c = 0; c < 3; c++) write_block(fp, d, L->lp.fm.c[c], 0);
-    if (!S.no_velocity_io) {
-        const int have = ustep >= 0 && ustep < MAXVSTEP && S.vwritten[ustep];
-        for (int c = 0; c < 3; c++) write_block(fp, d, have ? S.vring[c][ustep] : NULL, 1);
-    }
+    if (!S.no_velocity_io)
+        for (int c = 0; c < 3; c++) write_block(fp, d, ug->c[c], 0);
     if (S.bcflag_io) {
         long n = (long)d->ni * d->nj * d->nk, q = 0;
         real *fl = zalloc(n);
         for (int k = 1; k <= d->nk; k++)
             for (int j = 1; j <= d->nj; j++)
-                for (int i = 1; i <= d->ni; i++) fl[q++] = (real)S.g.bcflag[PX(d, i, j, k)];
+                for (int i = 1; i <= d->ni; i++) fl[q++] = (real)g->bcflag[PX(d, i, j, k)];
         write_block(fp, d, fl, 1);
         free(fl);
     }
@@ -2278,10 +2325,6 @@ EXPORT void orc_update(const int n[3], const real *u, const real *v, const real 
             continue;
         }
         const dims_t *dl = &L->sg->d;
-        if (L->sg != &S.g && (S.velocity_invariants || S.write_lcs)) {
-            latch("VELOCITY_INVARIANTS and WRITE_LCS are not restated for resolution /= 0");
-            return;
-        }
         if (L->diagnostic == FTLE_FWD) {
             /* exchange_lpmap: fm(no0) = dx */
             int ip = 0;
@@ -2307,8 +2350,11 @@ EXPORT void orc_update(const int n[3], const real *u, const real *v, const real 
         const int ustep = ring_step(S.t_np1, L->T, L->h) + (L->diagnostic == FTLE_FWD ? 1 : 0);
         reconstruct(L);
         compute_ftle(L);
-        if (S.velocity_invariants) compute_invariants(L, ustep);
-        if (S.write_lcs) write_lcs(L, ustep);
+        sr1_t ug = {{NULL, NULL, NULL}};
+        if (S.velocity_invariants || (S.write_lcs && !S.no_velocity_io)) make_ugrid(L, ustep, &ug);
+        if (S.velocity_invariants) compute_invariants(L, &ug);
+        if (S.write_lcs) write_lcs(L, &ug);
+        sr1_free(&ug);
         for (int c = 0; c < 3; c++) memcpy(L->fm_out.c[c], L->lp.fm.c[c], sizeof(real) * (size_t)dl->ntot);
         S.ftle_frames++;
         reset_lp(L->sg, &L->lp, 1);
@@ -2492,8 +2538,8 @@ EXPORT int orc_bspline3_coef(const real *xg, const real *yg, const real *zg, int
 /* Velocity invariants of a diagnostic's last frame: 5 x interior (Q, D, C, H, L2). */
 EXPORT int orc_get_invariants(int handle, real *out) {
     lcs_t *L = find_lcs(handle);
-    if (!L) return 1;
-    const dims_t *d = &S.g.d;
+    if (!L || !L->sg) return 1;
+    const dims_t *d = &L->sg->d;
     long q = 0;
     for (int v = 0; v < 5; v++)
         for (int k = 1; k <= d->nk; k++)
@@ -2506,8 +2552,8 @@ EXPORT int orc_get_invariants(int handle, real *out) {
  * a test can tell a rounding tie (|margin| at rounding level) from a real disagreement. */
 EXPORT int orc_get_l2margin(int handle, real *out) {
     lcs_t *L = find_lcs(handle);
-    if (!L) return 1;
-    const dims_t *d = &S.g.d;
+    if (!L || !L->sg) return 1;
+    const dims_t *d = &L->sg->d;
     long q = 0;
     for (int k = 1; k <= d->nk; k++)
         for (int j = 1; j <= d->nj; j++)

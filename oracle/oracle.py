@@ -147,9 +147,10 @@ class Oracle:
 
     def invariants(self, handle):
         """Q, D, C, H, L2 of the last frame (compute_invariants), shape (5, ni, nj, nk)."""
-        out = np.zeros(5 * int(np.prod(self.n)), dtype=self.dtype)
+        n = self.diag_size(handle)
+        out = np.zeros(5 * int(np.prod(n)), dtype=self.dtype)
         assert self.lib.orc_get_invariants(handle, self._p(out)) == 0
-        return out.reshape((5,) + tuple(self.n[::-1])).transpose(0, 3, 2, 1)
+        return out.reshape((5,) + tuple(n[::-1])).transpose(0, 3, 2, 1)
 
     def tracers(self, handle):
         """Positions of an LP_TRACER set, shape (3, count)."""
@@ -165,9 +166,10 @@ class Oracle:
 
     def l2margin(self, handle):
         """Middle eigenvalue of the lambda-2 tensor over its largest magnitude, last frame."""
-        out = np.zeros(int(np.prod(self.n)), dtype=self.dtype)
+        n = self.diag_size(handle)
+        out = np.zeros(int(np.prod(n)), dtype=self.dtype)
         assert self.lib.orc_get_l2margin(handle, self._p(out)) == 0
-        return out.reshape(tuple(self.n[::-1])).transpose(2, 1, 0)
+        return out.reshape(tuple(n[::-1])).transpose(2, 1, 0)
 
     def particles(self, handle):
         out = np.zeros(3 * int(np.prod(self.n)), dtype=self.dtype)

@@ -131,7 +131,10 @@ def _values(lines):
     return [s[14 * q:14 * q + 14] for s in lines for q in range(len(s) // 14)]
 
 
-def _compare_files(pa, pb, rtol, bitwise_blocks):
+def _compare_files(pa, pb, rtol, bitwise_blocks, flag_blocks=(), skip_blocks=()):
+    """flag_blocks: 0/1/... indicator blocks (the invariants' Q, C, D, L2 flags), which may
+    differ at a few nodes where the indicator sits at a rounding tie, as the invariants'
+    parity test allows (max(2, n/500) nodes)."""
     ha, da = _parse(pa)
     hb, db = _parse(pb)
     assert ha == hb
@@ -141,8 +144,13 @@ def _compare_files(pa, pb, rtol, bitwise_blocks):
     per = len(va) // nb
     for b in range(nb):
         A, B = va[b * per:(b + 1) * per], vb[b * per:(b + 1) * per]
+        if b in skip_blocks:
+            continue
         if b in bitwise_blocks:
             assert A == B, b
+            continue
+        if b in flag_blocks:
+            assert sum(x != y for x, y in zip(A, B)) <= max(2, len(A) // 500), b
             continue
         fa = np.array([float(s) for s in A])
         fb = np.array([float(s) for s in B])
