@@ -257,13 +257,7 @@ class Engine : public EngineBase {
   }
 
   int diagnostic_init(int type, int resolution, lcsdata_t Tint, lcsdata_t h, const char *label, std::string &msg) override {
-    if (type == LP_TRACER) {
-      if (resolution != 0) {
-        msg = "diagnostic_init: LP_TRACER with resolution /= 0 is not supported by this library";
-        return -1;
-      }
-      return tracer_init(Tint, h, label, msg);
-    }
+    if (type == LP_TRACER) return tracer_init(Tint, h, label, resolution, msg);
     if (type != FTLE_FWD && type != FTLE_BKWD) {
       msg = "ERROR, bad specification for lcs_type. Options are: FTLE_FWD, FTLE_BKWD, LP_TRACER";
       return -1;
@@ -811,7 +805,7 @@ class Engine : public EngineBase {
   // order (i fastest), starting at the node (where node tracking leaves it).  With no node
   // inside, the set is dropped and the handle is -1 (-2 here: not an error); its number is
   // used up all the same, as the reference's diagnostic count is.
-  int tracer_init(lcsdata_t Tint, lcsdata_t h, const char *label, std::string &msg) {
+  int tracer_init(lcsdata_t Tint, lcsdata_t h, const char *label, int resolution, std::string &msg) {
     if (!(h > lcsdata_t(0)) || !(Tint > lcsdata_t(0))) {
       msg = "diagnostic_init: T and h must be positive";
       return -1;
@@ -828,16 +822,34 @@ class Engine : public EngineBase {
     const lcsdata_t R = (lcsdata_t)opt_->tracer_r;
     std::vector<T> px[3];
     std::vector<int> pn[3];
-    for (int k = 1; k <= n_[2]; k++)
-      for (int j = 1; j <= n_[1]; j++)
-        for (int i = 1; i <= n_[0]; i++) {
-          const lcsdata_t dx = hg_.lt[0][i] - X, dy = hg_.lt[1][j] - Y, dz = hg_.lt[2][k] - Z;
+    // on a refined lcs grid (resolution /= 0) the injected nodes are that grid's, tracked to
+    // the solver grid with the periodic wrap (track_lp2node of init_lp_tracer's set)
+    DiagT tmp;
+    if (resolution != 0 && !make_lcs_grid(tmp, FTLE_FWD, resolution, msg)) return -1;
+    const HostGrid<lcsdata_t> &G = tmp.lg ? tmp.lg->hg : hg_;
+    std::vector<T> tpos[3];
+    std::vector<int> tnos[3];
+    if (tmp.lg) {
+      if (cudaStreamSynchronize(stream_) != cudaSuccess) return fail(msg, "sync");
+      for (int c = 0; c < 3; c++) {
+        tpos[c].resize(tmp.lg->N);
+        tnos[c].resize(tmp.lg->N);
+        if (cudaMemcpy(tpos[c].data(), tmp.lg->pos[c], tmp.lg->N * sizeof(T), cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(tnos[c].data(), tmp.lg->nos_reset[c], tmp.lg->N * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+          return fail(msg, "tracer node copy");
+      }
+    }
+    long q = 0;
+    for (int k = 1; k <= G.P.n[2]; k++)
+      for (int j = 1; j <= G.P.n[1]; j++)
+        for (int i = 1; i <= G.P.n[0]; i++, q++) {
+          const lcsdata_t dx = G.lt[0][i] - X, dy = G.lt[1][j] - Y, dz = G.lt[2][k] - Z;
           const lcsdata_t r = std::sqrt(dx * dx + dy * dy + dz * dz);
           if (!(r <= R)) continue;
           const int nd[3] = {i, j, k};
           for (int a = 0; a < 3; a++) {
-            px[a].push_back((T)hg_.lt[a][nd[a]]);
-            pn[a].push_back(nd[a]);
+            px[a].push_back(tmp.lg ? tpos[a][q] : (T)G.lt[a][nd[a]]);
+            pn[a].push_back(tmp.lg ? tnos[a][q] : nd[a]);
           }
         }
     d.np = (int)px[0].size();

@@ -2066,13 +2066,22 @@ static sgrid_t *new_sgrid(int *res_io) {
 /* LP_TRACER: init_lp_tracer (lp_m.f90:116-226) and diagnostic_init (cfd2lcs.f90:327-337):
  * one tracer per node with r <= TRACER_INJECT_RADIUS from the injection point, in node
  * order; none inside: the set is destroyed (its number used up) and the handle is -1. */
-static int tracer_init(real T, real h, const char *label) {
-    const dims_t *d = &S.g.d;
+static int tracer_init(real T, real h, const char *label, int resolution) {
+    /* lcs%sgrid: a refined copy when resolution /= 0 (its nodes are injected) */
+    sgrid_t *sg = &S.g;
+    int own = 0;
+    if (resolution != 0) {
+        sgrid_t *ng = new_sgrid(&resolution);
+        if (S.error) return -1;
+        if (ng) { sg = ng; own = 1; }
+    }
+    const dims_t *d = &sg->d;
     lcs_t *L = (lcs_t *)calloc(1, sizeof(lcs_t));
     L->id = S.nlcs + 1;
     L->diagnostic = LP_TRACER;
-    L->sg = &S.g;
-    L->lp.sg = &S.g;
+    L->sg = sg;
+    L->own_sg = own;
+    L->lp.sg = sg;
     L->T = T;
     L->h = h;
     snprintf(L->label, sizeof L->label, "%s", label ? label : "");
@@ -2087,14 +2096,16 @@ static int tracer_init(real T, real h, const char *label) {
             for (int j = 1; j <= d->nj; j++)
                 for (int i = 1; i <= d->ni; i++) {
                     long p = PX(d, i, j, k);
-                    real dx = S.g.grid.c[0][p] - c0[0], dy = S.g.grid.c[1][p] - c0[1], dz = S.g.grid.c[2][p] - c0[2];
+                    real dx = sg->grid.c[0][p] - c0[0], dy = sg->grid.c[1][p] - c0[1], dz = sg->grid.c[2][p] - c0[2];
                     real r = (real)sqrt((double)(dx * dx + dy * dy + dz * dz));
                     if (!(r <= S.tracer_r)) continue;
                     if (pass == 1) {
-                        for (int c = 0; c < 3; c++) L->lp.xp[c][ip] = S.g.grid.c[c][p];
+                        for (int c = 0; c < 3; c++) L->lp.xp[c][ip] = sg->grid.c[c][p];
                         L->lp.no[0][ip] = i; L->lp.no[1][ip] = j; L->lp.no[2][ip] = k;
-                        /* the educated guess of init_lp_tracer is the node itself at resolution 0 */
-                        L->lp.no_scfd[0][ip] = i; L->lp.no_scfd[1][ip] = j; L->lp.no_scfd[2][ip] = k;
+                        /* init_lp_tracer's educated guess of the solver node */
+                        L->lp.no_scfd[0][ip] = clampi(fnint((real)((float)(i * S.g.d.ni) / (float)d->ni)), 1, S.g.d.ni);
+                        L->lp.no_scfd[1][ip] = clampi(fnint((real)((float)(j * S.g.d.nj) / (float)d->nj)), 1, S.g.d.nj);
+                        L->lp.no_scfd[2][ip] = clampi(fnint((real)((float)(k * S.g.d.nk) / (float)d->nk)), 1, S.g.d.nk);
                         L->lp.flag[ip] = LP_UNKNOWN;
                     }
                     ip++;
@@ -2226,10 +2237,7 @@ EXPORT int orc_diagnostic_init(int type, int resolution, real T, real h, const c
     if (S.error) return -1;
     if (!S.inited) { latch("diagnostic_init before init"); return -1; }
     if (S.nlcs >= MAXLCS) { latch("diagnostic_init: too many diagnostics"); return -1; }
-    if (type == LP_TRACER) {
-        if (resolution != 0) { latch("diagnostic_init: LP_TRACER with resolution /= 0 is not restated"); return -1; }
-        return tracer_init(T, h, label);
-    }
+    if (type == LP_TRACER) return tracer_init(T, h, label, resolution);
     if (type != FTLE_FWD && type != FTLE_BKWD) {
         latch("ERROR, bad specification for lcs_type. Options are: FTLE_FWD, FTLE_BKWD, LP_TRACER");
         return -1;

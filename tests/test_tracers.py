@@ -100,6 +100,37 @@ CASES = [
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("case,res", [("abc_unsteady", 1), ("dg", 2)])
+def test_tracers_on_refined_grid_match_oracle(oracle_dp, gpu_dp, case, res):
+    """resolution /= 0: the refined lcs grid's nodes inside the sphere are injected and tracked
+    to the solver grid (with the periodic wrap), then advected on the solver grid."""
+    def run(api):
+        g, vel, prm = SC.make_case(case)
+        api.reset()
+        api.init(g.n, g.x, g.y, g.z, g.flag)
+        _inject(api, g, (2.0, 3.0, 4.0) if case == "abc_unsteady" else (1.0, 0.5, 0.0), 1.6 if case == "abc_unsteady" else 0.3)
+        h = api.diagnostic_init(LP_TRACER, res, prm["T"], prm["h"], "tr")
+        api.set_option("INTEGRATOR", 2)
+        api.set_option("INTERPOLATOR", 1)
+        for k in range(prm["steps"]):
+            t = W.time_at(k, prm["dt"])
+            api.update(*vel(t), t)
+        return g, h
+    g, ho = run(oracle_dp)
+    assert oracle_dp.error() == 0, oracle_dp.error_msg()
+    xo = oracle_dp.tracers(ho)
+    try:
+        _, hg = run(gpu_dp)
+        assert gpu_dp.error()[0] == 0, gpu_dp.error()
+        xg = gpu_dp.tracers(hg)
+        assert xg.shape == xo.shape and xo.shape[1] > 0
+        span = max(float(np.ptp(a)) for a in (g.x, g.y, g.z))
+        np.testing.assert_allclose(xg, xo, rtol=0, atol=1e-12 * span)
+    finally:
+        gpu_dp.reset()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("case,integrator,interp,centre,radius", CASES)
 def test_tracers_match_oracle(oracle_dp, gpu_dp, case, integrator, interp, centre, radius):
     g, hb, ht = _run(oracle_dp, case, integrator, interp, centre, radius)
