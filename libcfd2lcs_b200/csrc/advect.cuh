@@ -86,6 +86,22 @@ __device__ __forceinline__ TV lin_apply_blend(const LinStencil<T> &st, const TV 
   return acc;
 }
 
+// a stage's time blend written beforehand (k_blend), sampled trilinearly with the same weights
+// and accumulation as lin_apply_blend
+template <typename T, typename TV>
+__device__ __forceinline__ TV lin_apply_tv(const LinStencil<T> &st, const TV *__restrict__ f) {
+  const int p = st.p0;
+  const int q[8] = {p, p + st.s[0], p + st.s[1], p + st.s[0] + st.s[1], p + st.s[2], p + st.s[0] + st.s[2], p + st.s[1] + st.s[2],
+                    p + st.s[0] + st.s[1] + st.s[2]};
+  TV acc = TV(0);
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    const TV v = __ldg(f + q[c]);
+    acc = c == 0 ? TV(st.w[0]) * v : acc + TV(st.w[c]) * v;
+  }
+  return acc;
+}
+
 // ---------------------------------------------------------------------------------------
 // Velocity sampler for one stage: NEAREST, LINEAR or B-spline, blended in time.
 // ---------------------------------------------------------------------------------------
@@ -113,7 +129,13 @@ __device__ __forceinline__ void sample_velocity(const DevGrid<T> &g, const Splin
     LinStencil<T> st;
     lin_stencil(g, x, no, st);
 #pragma unroll
-    for (int c = 0; c < 3; c++) out[c] = T(lin_apply_blend<T, TV>(st, V.un[c], V.unp1[c], omc, ct));
+    if (V.cs[stage][0]) {  // the stage's blend, written once per subcycle on large grids
+#pragma unroll
+      for (int c = 0; c < 3; c++) out[c] = T(lin_apply_tv<T, TV>(st, V.cs[stage][c]));
+    } else {
+#pragma unroll
+      for (int c = 0; c < 3; c++) out[c] = T(lin_apply_blend<T, TV>(st, V.un[c], V.unp1[c], omc, ct));
+    }
   } else {
     constexpr int KC = INTERP == INTERP_SPLINE4 ? 4 : 0;
     constexpr bool UNI = !std::is_same<T, TV>::value;

@@ -3,6 +3,7 @@
 #include "engine.h"
 
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <limits>
@@ -229,6 +230,7 @@ class Engine : public EngineBase {
       ev_.push_back(ev);
     }
     CK(cudaMallocHost(&red_host_, sizeof(DevReduce)));
+    if (const char *e = std::getenv("CFD2LCS_B200_LINEAR_BLEND_MIN")) lin_blend_min_ = std::atol(e);
     for (int a = 0; a < 3; a++) n_[a] = n[a];
     // coordinate lines and interior flags for the output files (the grid is a tensor product)
     for (int a = 0; a < 3; a++)
@@ -486,7 +488,8 @@ class Engine : public EngineBase {
       for (long sc = 0; sc < nsub; sc++) {
         cudaEvent_t k0, k1;
         StageTimes S = stage_times(lp_time, dt);
-        if (spline && !stage_blends(d, S, V, msg)) return false;
+        if ((spline || (interp == LINEAR && N_ >= lin_blend_min_ && (d.type != FTLE_BKWD || d.lg))) && !stage_blends(d, S, V, msg))
+          return false;
         if (d.type == FTLE_BKWD) {
           FieldPtrs<T> fo;
           FieldPtrsW<T> fn;
@@ -1004,9 +1007,11 @@ class Engine : public EngineBase {
     }
     if (nout > 0) {
       FieldPtrs<TV> a{}, bb{};
+      // B-splines blend the levels' coefficients, LINEAR the levels themselves
+      const bool spl = opt_->interpolator == QUADRATIC || opt_->interpolator == CUBIC;
       for (int c = 0; c < 3; c++) {
-        a.f[c] = ucoef_[cur_ ^ 1][c];
-        bb.f[c] = ucoef_[cur_][c];
+        a.f[c] = spl ? ucoef_[cur_ ^ 1][c] : u_[cur_ ^ 1][c];
+        bb.f[c] = spl ? ucoef_[cur_][c] : u_[cur_][c];
       }
       const long npair = (ntot_ + 1) / 2;
       const dim3 grd((unsigned)((npair + 255) / 256), 3);
@@ -1018,6 +1023,20 @@ class Engine : public EngineBase {
       for (int c = 0; c < 3; c++) V.cs[st][c] = d.blend[pick[st]][c];
     return true;
   }
+
+  // LINEAR interpolation writes each stage's time blend once per subcycle (k_blend) for the
+  // particle sets whose every stage is off the nodes (forward particles, refined backward sets)
+  // on grids of at least this many points, so that every particle gathers 8 blended corners
+  // instead of 8 x 2 levels.  Measured on B200: the forward kernel 1.64 -> 1.17 ms per launch on
+  // ABC 256^3 RK2; the backward SL kernel, whose first stage reads the nodal values, gained less
+  // than the blend pass cost (turbulence 512^3: 140 -> 155 ms per update), so it keeps the
+  // per-corner blend; on small grids the extra pass costs more than it saves.  The environment
+  // variable CFD2LCS_B200_LINEAR_BLEND_MIN, read at cfd2lcs_init, overrides it (the tests take
+  // the blended path on small grids with it).
+#ifndef CFD2LCS_LINEAR_BLEND_MIN
+#define CFD2LCS_LINEAR_BLEND_MIN (1L << 22)
+#endif
+  long lin_blend_min_ = CFD2LCS_LINEAR_BLEND_MIN;
 
   // B-spline axes (flow-map type) of an lcs grid, as ensure_spline builds the solver grid's
   bool ensure_lcs_spline(LcsGrid<T> &L, int deg, std::string &msg) {

@@ -178,3 +178,12 @@ def test_velocity_invariants(oracle_dp, gpu_dp, case, integrator, interp):
             assert np.all(np.abs(io[3][fin] - ig[3][fin]) <= 1e-9 * np.maximum(1.0, np.abs(io[3][fin])))
     finally:
         gpu_dp.reset()
+
+
+@pytest.mark.parametrize("case,integrator,directions", [("abc_unsteady", 2, (SC.FTLE_BKWD, SC.FTLE_FWD)), ("dg", 3, (SC.FTLE_BKWD,)),
+                                                        ("mixed_bc", 4, (SC.FTLE_BKWD, SC.FTLE_FWD))])
+def test_linear_stage_blends(oracle_dp, gpu_dp, case, integrator, directions, monkeypatch):
+    """LINEAR with the stage blends written once per subcycle (the large-grid path, forced on
+    small grids through CFD2LCS_B200_LINEAR_BLEND_MIN): the same parity bounds."""
+    monkeypatch.setenv("CFD2LCS_B200_LINEAR_BLEND_MIN", "0")
+    _compare(oracle_dp, gpu_dp, case, integrator, 1, directions=directions)
