@@ -1810,7 +1810,7 @@ class Engine : public EngineBase {
     }
   }
 
-  // Re-sorts the particle slots by grid cell (32 x 8 tiles, x fastest) every kSortInterval
+  // Re-sorts the particle slots by grid cell (32 x 4 x 2 tiles, x fastest) every kSortInterval
   // subcycles, so that the particles of a block gather neighbouring spline taps as the SL
   // kernel's blocks do.  Results do not depend on the order: every particle is advanced
   // independently and the snapshot reads it back through the inverse map.  Measured on B200
