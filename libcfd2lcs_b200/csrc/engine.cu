@@ -1119,7 +1119,7 @@ class Engine : public EngineBase {
     const int sx = g.P.sx, sxy = g.P.sxy, ny = g.P.n[1] + 2, nz = g.P.n[2] + 2;
     if (axis == 0) {
       const long warps = (long)((ny + 31) / 32) * nz;
-      const size_t smem = sizeof(D) * 4 * 2 * 32 * 33;  // two 32 x 33 tiles per warp
+      const size_t smem = sizeof(D) * 4 * 2 * 32 * (XFIT_W + 1);  // two 32 x (XFIT_W + 1) tiles per warp
       static bool attr_done = false;
       if (!attr_done) {
         cudaFuncSetAttribute(k_fit_xlines<D, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
