@@ -923,8 +923,13 @@ __global__ void __launch_bounds__(256) k_blend(const __grid_constant__ FieldPtrs
 // y and z passes: lines start at adjacent addresses (consecutive i), so element e of 32 lines
 // is one coalesced row.  Line L starts at L % nfast + (L / nfast) * so; elements es apart.
 // Loads are issued G at a time ahead of the dependent sweep.
+// resident blocks asked of the compiler: measured on B200 (192^3, FP64, K = 4) 2 / 3 / 4 blocks
+// took 0.153 / 0.129 / 0.159 ms per launch
+#ifndef CFD2LCS_FIT_MINB
+#define CFD2LCS_FIT_MINB 3
+#endif
 template <typename T, int K>
-__global__ void __launch_bounds__(256, 3) k_fit_lines(SplineAxis<T> A, const __grid_constant__ FieldPtrs<T> src,
+__global__ void __launch_bounds__(256, CFD2LCS_FIT_MINB) k_fit_lines(SplineAxis<T> A, const __grid_constant__ FieldPtrs<T> src,
                                                        const __grid_constant__ FieldPtrsW<T> dst, int nfast, long nlines, long es,
                                                        long so) {
   const long L = (long)blockIdx.x * blockDim.x + threadIdx.x;
