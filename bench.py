@@ -45,8 +45,8 @@ STAGES = {0: 1, 1: 1, 2: 2, 3: 3, 4: 3}
 # captures summarised in profiles/ (192^3 ABC, 7077888 points), scaled to the benchmark grid by
 # its point count: (kernel, precision, interpolator, integrator) -> bytes per point
 MEASURED_TRAFFIC = {
-    ("k_sl_subcycle", "fp64", 3, 3): (874.453504e6 + 204.906496e6) / 7077888,   # k_sl_subcycle_abc192_cubic_rk3_fp64.md
-    ("k_fwd_subcycle", "fp64", 3, 3): (965.291264e6 + 459.383808e6) / 7077888,  # k_fwd_subcycle_abc192_cubic_rk3_fp64.md
+    ("k_sl_subcycle", "fp64", 3, 3): (877.944576e6 + 201.871872e6) / 7077888,   # k_sl_subcycle_abc192_cubic_rk3_fp64.md
+    ("k_fwd_subcycle", "fp64", 3, 3): (964.329472e6 + 459.971072e6) / 7077888,  # k_fwd_subcycle_abc192_cubic_rk3_fp64.md
 }
 
 
