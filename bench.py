@@ -207,13 +207,14 @@ def dist_setup():
 
 def cpu_sample(w, steps: int, threads: int | None = None):
     """The oracle (CPU restatement of the reference path) on a bounded sample of the
-    workload: the same flow, options, dt, T and h on a coarser grid, one update per step."""
+    workload: the same flow, options, dt, T and h on a coarser grid, one update per step.
+    96^3 for the ABC flow: about 10 s of oracle work per update on 16 host cores."""
     from oracle.oracle import Oracle
     o = Oracle("dp")
     o.reset()
     if threads:
         o.set_threads(threads)
-    nsample = 48 if w["kind"] == "abc" else 128
+    nsample = 96 if w["kind"] == "abc" else 128
     g, vel, steady = make_grid(w, nsample)
     o.init(g.n, g.x, g.y, g.z, g.flag)
     for d in w["dirs"]:
