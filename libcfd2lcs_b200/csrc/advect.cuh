@@ -11,6 +11,13 @@
 
 namespace cfd2lcs {
 
+// product and sum rounded on their own (never contracted into an FMA), as the reference's
+// compiled arithmetic forms them
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+
 // ---------------------------------------------------------------------------------------
 // Trilinear stencil around a node, interp_s2u_r1 LINEAR (src/lp_tracking_m.f90:342-474):
 // per axis the bracket is [no, no+1] when x > line(no), else [no-1, no]; t is clamped to
@@ -103,6 +110,53 @@ __device__ __forceinline__ TV lin_apply_tv(const LinStencil<T> &st, const TV *__
 }
 
 // ---------------------------------------------------------------------------------------
+// Taylor series about the tracked node, interp_s2u_r1 TSE / TSE_LIMIT
+// (src/lp_tracking_m.f90:526-654), on this library's rectilinear grids:
+//   phi(x) = phi(no) + grad(phi)(no) . (x - x(no)),
+// grad by grad_sr1's second-order central differences over the node coordinates
+// (src/gradient_m.f90:11-66), which the reference evaluates at interior nodes only (the
+// gradient array stays zero on the ghost layer) and zeroes along a singleton axis; the
+// three terms are added in the reference's order, each product and sum rounded on its own.
+// TSE_LIMIT then clamps the value to the range of the 27 values around no (max with the
+// minimum first, then min with the maximum).  At a ghost node that window reaches past the
+// padded array -- the reference reads outside its allocation there -- and is clipped to it.
+// val(p) returns the sampled field at padded index p in T.
+// ---------------------------------------------------------------------------------------
+template <typename T, bool LIMIT, typename F>
+__device__ __forceinline__ T tse_apply(const DevGrid<T> &g, const T x[3], const int no[3], F val) {
+  const int str[3] = {1, g.P.sx, g.P.sxy};
+  const int p = pidx(g.P.sx, g.P.sxy, no[0], no[1], no[2]);
+  const T v0 = val(p);
+  T r = v0;
+  const bool interior = no[0] >= 1 && no[0] <= g.P.n[0] && no[1] >= 1 && no[1] <= g.P.n[1] && no[2] >= 1 && no[2] <= g.P.n[2];
+  if (interior) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      if (g.P.n[a] == 1) continue;
+      const T *L = g.lt[a];
+      const T d = (val(p + str[a]) - val(p - str[a])) / (__ldg(L + no[a] + 1) - __ldg(L + no[a] - 1));
+      r = add_rn(r, mul_rn(x[a] - __ldg(L + no[a]), d));
+    }
+  }
+  if (LIMIT) {
+    T mn = v0, mx = v0;
+    const int i0 = max(no[0] - 1, 0), i1 = min(no[0] + 1, g.P.n[0] + 1);
+    const int j0 = max(no[1] - 1, 0), j1 = min(no[1] + 1, g.P.n[1] + 1);
+    const int k0 = max(no[2] - 1, 0), k1 = min(no[2] + 1, g.P.n[2] + 1);
+    for (int k = k0; k <= k1; k++)
+      for (int j = j0; j <= j1; j++)
+        for (int i = i0; i <= i1; i++) {
+          const T v = val(pidx(g.P.sx, g.P.sxy, i, j, k));
+          mn = v < mn ? v : mn;
+          mx = v > mx ? v : mx;
+        }
+    r = r < mn ? mn : r;
+    r = r > mx ? mx : r;
+  }
+  return r;
+}
+
+// ---------------------------------------------------------------------------------------
 // Velocity sampler for one stage: NEAREST, LINEAR or B-spline, blended in time.
 // ---------------------------------------------------------------------------------------
 template <typename T>
@@ -135,6 +189,14 @@ __device__ __forceinline__ void sample_velocity(const DevGrid<T> &g, const Splin
     } else {
 #pragma unroll
       for (int c = 0; c < 3; c++) out[c] = T(lin_apply_blend<T, TV>(st, V.un[c], V.unp1[c], omc, ct));
+    }
+  } else if (INTERP == INTERP_TSE || INTERP == INTERP_TSE_LIMIT) {
+    // the stage's field (1-ct) u_n + ct u_np1 at each node the expansion reads, as
+    // integrate_lp blends the whole field before interpolating (src/lp_motion_m.f90:193-197)
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const TV *a = V.un[c], *b = V.unp1[c];
+      out[c] = tse_apply<T, INTERP == INTERP_TSE_LIMIT>(g, x, no, [&](int p) { return T(omc * __ldg(a + p) + ct * __ldg(b + p)); });
     }
   } else {
     constexpr int KC = INTERP == INTERP_SPLINE4 ? 4 : 0;
@@ -175,6 +237,12 @@ __device__ __forceinline__ void sample_field(const DevGrid<T> &g, const SplineAx
     lin_stencil(g, x, no, st);
 #pragma unroll
     for (int c = 0; c < 3; c++) out[c] = lin_apply(st, f[c]);
+  } else if (INTERP == INTERP_TSE || INTERP == INTERP_TSE_LIMIT) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const T *fc = f[c];
+      out[c] = tse_apply<T, INTERP == INTERP_TSE_LIMIT>(g, x, no, [&](int p) { return __ldg(fc + p); });
+    }
   } else {
     constexpr int KC = INTERP == INTERP_SPLINE4 ? 4 : 0;
     SplineStencil<T> st;
@@ -342,10 +410,6 @@ __device__ __forceinline__ constexpr int nbr_offset(int nb, int a) {
   return t[nb][a];
 }
 
-// product rounded on its own (never contracted into an FMA), as the reference's compiled
-// distance arithmetic forms it
-__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
-__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 
 template <typename T>
 __device__ __forceinline__ bool track_pass(const DevGrid<T> &g, const T x[3], int no[3]) {

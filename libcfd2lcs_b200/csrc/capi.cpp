@@ -415,7 +415,8 @@ CFD2LCS_EXPORT int cfd2lcs_batch_add_c(const int n[3], const lcsdata_t *x, const
   Batch &b = BT();
   if (b.error) return -1;
   if (integrator < EULER || integrator > RK4) return batch_fail("batch_add: bad integrator");
-  if (interpolator != NEAREST_NBR && interpolator != LINEAR && interpolator != QUADRATIC && interpolator != CUBIC)
+  if (interpolator != NEAREST_NBR && interpolator != LINEAR && interpolator != QUADRATIC && interpolator != CUBIC && interpolator != TSE &&
+      interpolator != TSE_LIMIT)
     return batch_fail("batch_add: bad interpolator");
   if (!(cfl > lcsdata_t(0))) return batch_fail("batch_add: CFL must be positive");
   std::unique_ptr<BatchInstance> bi(new BatchInstance());

@@ -18,8 +18,11 @@ enum : int {
 };
 
 enum { EULER_ = 0, TRAPEZOIDAL_ = 1, RK2_ = 2, RK3_ = 3, RK4_ = 4 };
-// INTERP_SPLINE: B-spline of any order per axis; INTERP_SPLINE4: cubic on every axis (3-D grid)
-enum { INTERP_NEAREST = 0, INTERP_LINEAR = 1, INTERP_SPLINE = 2, INTERP_SPLINE4 = 3 };
+// INTERP_SPLINE: B-spline of any order per axis; INTERP_SPLINE4: cubic on every axis (3-D grid);
+// INTERP_TSE / INTERP_TSE_LIMIT: Taylor series about the tracked node, without / with limiter
+enum { INTERP_NEAREST = 0, INTERP_LINEAR = 1, INTERP_SPLINE = 2, INTERP_SPLINE4 = 3, INTERP_TSE = 4, INTERP_TSE_LIMIT = 5 };
+
+__host__ __device__ constexpr bool interp_is_spline(int interp) { return interp == INTERP_SPLINE || interp == INTERP_SPLINE4; }
 
 template <typename T>
 struct DevGrid {

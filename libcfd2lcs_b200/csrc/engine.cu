@@ -363,11 +363,7 @@ class Engine : public EngineBase {
     }
     cur_ ^= 1;  // u_n = u_np1 (buffer swap); u_np1 is rewritten below
     const int interp = opt_->interpolator;
-    if (interp == TSE || interp == TSE_LIMIT) {
-      msg = "update: TSE / TSE_LIMIT interpolation (non-rectilinear grids) is not supported";
-      return false;
-    }
-    if (interp != NEAREST_NBR && interp != LINEAR && interp != QUADRATIC && interp != CUBIC) {
+    if (interp != NEAREST_NBR && interp != LINEAR && interp != QUADRATIC && interp != CUBIC && interp != TSE && interp != TSE_LIMIT) {
       msg = "ERROR: Unrecognized interpolator";
       return false;
     }
@@ -710,6 +706,8 @@ class Engine : public EngineBase {
 #define COMPOSE_NA(I, FL) k_compose<T, I, FL><<<grd, blk, 0, stream_>>>(dg_, sa, sl, m, out, err)
     if (iv == INTERP_NEAREST) { if (F) COMPOSE_NA(INTERP_NEAREST, true); else COMPOSE_NA(INTERP_NEAREST, false); }
     else if (iv == INTERP_LINEAR) { if (F) COMPOSE_NA(INTERP_LINEAR, true); else COMPOSE_NA(INTERP_LINEAR, false); }
+    else if (iv == INTERP_TSE) { if (F) COMPOSE_NA(INTERP_TSE, true); else COMPOSE_NA(INTERP_TSE, false); }
+    else if (iv == INTERP_TSE_LIMIT) { if (F) COMPOSE_NA(INTERP_TSE_LIMIT, true); else COMPOSE_NA(INTERP_TSE_LIMIT, false); }
     else if (iv == INTERP_SPLINE4) { if (F) COMPOSE_NA(INTERP_SPLINE4, true); else COMPOSE_NA(INTERP_SPLINE4, false); }
     else { if (F) COMPOSE_NA(INTERP_SPLINE, true); else COMPOSE_NA(INTERP_SPLINE, false); }
 #undef COMPOSE_NA
@@ -1165,6 +1163,8 @@ class Engine : public EngineBase {
   static int interp_variant(int interp, const SplineAxes<T> &sa) {
     if (interp == NEAREST_NBR) return INTERP_NEAREST;
     if (interp == LINEAR) return INTERP_LINEAR;
+    if (interp == TSE) return INTERP_TSE;
+    if (interp == TSE_LIMIT) return INTERP_TSE_LIMIT;
     if (sa.ax[0].k == 4 && sa.ax[1].k == 4 && sa.ax[2].k == 4) return INTERP_SPLINE4;
     return INTERP_SPLINE;
   }
@@ -1419,6 +1419,8 @@ class Engine : public EngineBase {
     const int interp = opt_->interpolator;
     if (interp == NEAREST_NBR) sl_refined_flags<INTERP_NEAREST>(d, sas, sal, V, fo, fn, S, dt);
     else if (interp == LINEAR) sl_refined_flags<INTERP_LINEAR>(d, sas, sal, V, fo, fn, S, dt);
+    else if (interp == TSE) sl_refined_flags<INTERP_TSE>(d, sas, sal, V, fo, fn, S, dt);
+    else if (interp == TSE_LIMIT) sl_refined_flags<INTERP_TSE_LIMIT>(d, sas, sal, V, fo, fn, S, dt);
     else if (interp_variant(interp, sas) == INTERP_SPLINE4 && interp_variant(interp, sal) == INTERP_SPLINE4)
       sl_refined_flags<INTERP_SPLINE4>(d, sas, sal, V, fo, fn, S, dt);
     else sl_refined_flags<INTERP_SPLINE>(d, sas, sal, V, fo, fn, S, dt);
@@ -1501,6 +1503,8 @@ class Engine : public EngineBase {
     const bool F = dg_.P.has_flags != 0;
     if (iv == INTERP_NEAREST) F ? sl_integ<INTERP_NEAREST, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_NEAREST, false>(sa, V, fo, fn, S, dt);
     else if (iv == INTERP_LINEAR) F ? sl_integ<INTERP_LINEAR, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_LINEAR, false>(sa, V, fo, fn, S, dt);
+    else if (iv == INTERP_TSE) F ? sl_integ<INTERP_TSE, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_TSE, false>(sa, V, fo, fn, S, dt);
+    else if (iv == INTERP_TSE_LIMIT) F ? sl_integ<INTERP_TSE_LIMIT, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_TSE_LIMIT, false>(sa, V, fo, fn, S, dt);
     else if (iv == INTERP_SPLINE4) F ? sl_integ<INTERP_SPLINE4, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_SPLINE4, false>(sa, V, fo, fn, S, dt);
     else F ? sl_integ<INTERP_SPLINE, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_SPLINE, false>(sa, V, fo, fn, S, dt);
     CK(cudaGetLastError());
@@ -1528,6 +1532,8 @@ class Engine : public EngineBase {
     if (n == 0) return true;
     if (iv == INTERP_NEAREST) F ? fwd_integ<INTERP_NEAREST, true>(sa, V, P, S, dt, n) : fwd_integ<INTERP_NEAREST, false>(sa, V, P, S, dt, n);
     else if (iv == INTERP_LINEAR) F ? fwd_integ<INTERP_LINEAR, true>(sa, V, P, S, dt, n) : fwd_integ<INTERP_LINEAR, false>(sa, V, P, S, dt, n);
+    else if (iv == INTERP_TSE) F ? fwd_integ<INTERP_TSE, true>(sa, V, P, S, dt, n) : fwd_integ<INTERP_TSE, false>(sa, V, P, S, dt, n);
+    else if (iv == INTERP_TSE_LIMIT) F ? fwd_integ<INTERP_TSE_LIMIT, true>(sa, V, P, S, dt, n) : fwd_integ<INTERP_TSE_LIMIT, false>(sa, V, P, S, dt, n);
     else if (iv == INTERP_SPLINE4) F ? fwd_integ<INTERP_SPLINE4, true>(sa, V, P, S, dt, n) : fwd_integ<INTERP_SPLINE4, false>(sa, V, P, S, dt, n);
     else F ? fwd_integ<INTERP_SPLINE, true>(sa, V, P, S, dt, n) : fwd_integ<INTERP_SPLINE, false>(sa, V, P, S, dt, n);
     CK(cudaGetLastError());
@@ -1570,6 +1576,8 @@ class Engine : public EngineBase {
 #define COMPOSE(I, FL) k_compose<T, I, FL><<<grd, blk, 0, stream_>>>(g, sa, sl, m, out, err)
     if (iv == INTERP_NEAREST) { if (F) COMPOSE(INTERP_NEAREST, true); else COMPOSE(INTERP_NEAREST, false); }
     else if (iv == INTERP_LINEAR) { if (F) COMPOSE(INTERP_LINEAR, true); else COMPOSE(INTERP_LINEAR, false); }
+    else if (iv == INTERP_TSE) { if (F) COMPOSE(INTERP_TSE, true); else COMPOSE(INTERP_TSE, false); }
+    else if (iv == INTERP_TSE_LIMIT) { if (F) COMPOSE(INTERP_TSE_LIMIT, true); else COMPOSE(INTERP_TSE_LIMIT, false); }
     else if (iv == INTERP_SPLINE4) { if (F) COMPOSE(INTERP_SPLINE4, true); else COMPOSE(INTERP_SPLINE4, false); }
     else { if (F) COMPOSE(INTERP_SPLINE, true); else COMPOSE(INTERP_SPLINE, false); }
 #undef COMPOSE
@@ -1760,6 +1768,8 @@ class Engine : public EngineBase {
     const int iv = interp_variant(interp, sa);
     if (iv == INTERP_NEAREST) k_sample_ugrid<T, TV, INTERP_NEAREST><<<grd, blk, 0, stream_>>>(L.dg, dg_, sa, V, out);
     else if (iv == INTERP_LINEAR) k_sample_ugrid<T, TV, INTERP_LINEAR><<<grd, blk, 0, stream_>>>(L.dg, dg_, sa, V, out);
+    else if (iv == INTERP_TSE) k_sample_ugrid<T, TV, INTERP_TSE><<<grd, blk, 0, stream_>>>(L.dg, dg_, sa, V, out);
+    else if (iv == INTERP_TSE_LIMIT) k_sample_ugrid<T, TV, INTERP_TSE_LIMIT><<<grd, blk, 0, stream_>>>(L.dg, dg_, sa, V, out);
     else if (iv == INTERP_SPLINE4) k_sample_ugrid<T, TV, INTERP_SPLINE4><<<grd, blk, 0, stream_>>>(L.dg, dg_, sa, V, out);
     else k_sample_ugrid<T, TV, INTERP_SPLINE><<<grd, blk, 0, stream_>>>(L.dg, dg_, sa, V, out);
     counters_.kernel_launches++;

@@ -89,7 +89,7 @@ bool HostGrid<R>::build(const int n[3], const R *x, const R *y, const R *z, cons
         const long s = at(i, j, k);
         if (x[s] != line[0][i] || y[s] != line[1][j] || z[s] != line[2][k]) {
           error = "init: grid is not an exact tensor product of coordinate lines (curvilinear grids need "
-                  "TSE/TSE_LIMIT, which this library does not provide)";
+                  "least-squares gradients, which this library does not provide)";
           return false;
         }
       }

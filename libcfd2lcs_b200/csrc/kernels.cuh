@@ -132,11 +132,11 @@ __global__ void __launch_bounds__(256) k_ingest(DevGrid<T> g, const U *__restric
 #endif
 template <int INTERP>
 constexpr int sl_min_blocks() {
-  return INTERP >= INTERP_SPLINE ? CFD2LCS_SL_MINB_SPLINE : CFD2LCS_SL_MINB_LINEAR;
+  return interp_is_spline(INTERP) ? CFD2LCS_SL_MINB_SPLINE : CFD2LCS_SL_MINB_LINEAR;
 }
 template <int INTERP>
 constexpr int fwd_min_blocks() {
-  return INTERP >= INTERP_SPLINE ? CFD2LCS_FWD_MINB_SPLINE : CFD2LCS_FWD_MINB_LINEAR;
+  return interp_is_spline(INTERP) ? CFD2LCS_FWD_MINB_SPLINE : CFD2LCS_FWD_MINB_LINEAR;
 }
 
 template <typename T, typename TV, int INTEG, int INTERP, bool HAS_FLAGS>

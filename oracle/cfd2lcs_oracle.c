@@ -988,9 +988,10 @@ static real bsp3_eval(const bsp3_t *s, real x, real y, real z) {
 }
 
 /* ------------------------------------------------------------------------------------
- * interp_s2u_r1, lp_tracking_m.f90:279-662 (NEAREST_NBR, LINEAR, QUADRATIC, CUBIC;
- * TSE / TSE_LIMIT are used by the reference only for non-rectilinear grids, which this
- * restatement rejects at init).
+ * interp_s2u_r1, lp_tracking_m.f90:279-662 (NEAREST_NBR, LINEAR, QUADRATIC, CUBIC, and
+ * TSE / TSE_LIMIT with grad_sr1's central differences, gradient_m.f90:11-66; the
+ * least-squares gradients of non-rectilinear grids are not restated: such grids are
+ * rejected at init).
  * ------------------------------------------------------------------------------------ */
 static void coord_lines(const sgrid_t *g, real **xg, real **yg, real **zg) {
     const dims_t *d = &g->d;
@@ -1065,8 +1066,48 @@ static void interp_r1(const sgrid_t *g, int method, int np, real *const *xp, int
         free(xg); free(yg); free(zg);
         break;
     }
+    case TSE: case TSE_LIMIT: {
+        /* lp_tracking_m.f90:526-654: phi(no) + grad(phi)(no) . (x - x(no)); grad_sr1 fills
+         * interior nodes only (the ghost layer of the gradient array stays zero) and zeroes
+         * the derivatives along a singleton axis.  TSE_LIMIT clamps to the 27 values around no;
+         * at a ghost node the reference reads outside its array there, and this restatement
+         * clips the window to the padded array. */
+        const int lim = method == TSE_LIMIT;
+        const int nn[3] = {d->ni, d->nj, d->nk};
+        const long st[3] = {PX(d, 1, 0, 0) - PX(d, 0, 0, 0), PX(d, 0, 1, 0) - PX(d, 0, 0, 0), PX(d, 0, 0, 1) - PX(d, 0, 0, 0)};
+#pragma omp parallel for schedule(static)
+        for (int ip = 0; ip < np; ip++) {
+            const int *q = (int[3]){no[0][ip], no[1][ip], no[2][ip]};
+            long p = PX(d, q[0], q[1], q[2]);
+            int interior = 1;
+            for (int a = 0; a < 3; a++) interior &= q[a] >= 1 && q[a] <= nn[a];
+            for (int c = 0; c < 3; c++) {
+                const real *F = f->c[c];
+                real gr[3] = {0, 0, 0}, dl[3];
+                for (int a = 0; a < 3; a++) {
+                    const real *X = g->grid.c[a];
+                    if (interior && g->gn[a] != 1) gr[a] = (F[p + st[a]] - F[p - st[a]]) / (X[p + st[a]] - X[p - st[a]]);
+                    dl[a] = xp[a][ip] - X[p];
+                }
+                real r = F[p] + dl[0] * gr[0] + dl[1] * gr[1] + dl[2] * gr[2];
+                if (lim) {
+                    real mn = F[p], mx = F[p];
+                    for (int k = imax(q[2] - 1, 0); k <= imin(q[2] + 1, d->nk + 1); k++)
+                        for (int j = imax(q[1] - 1, 0); j <= imin(q[1] + 1, d->nj + 1); j++)
+                            for (int i = imax(q[0] - 1, 0); i <= imin(q[0] + 1, d->ni + 1); i++) {
+                                real v = F[PX(d, i, j, k)];
+                                mn = rmin(mn, v);
+                                mx = rmax(mx, v);
+                            }
+                    r = rmin(rmax(r, mn), mx);
+                }
+                out[c][ip] = r;
+            }
+        }
+        break;
+    }
     default:
-        latch("interp: unsupported interpolator (TSE/TSE_LIMIT are not restated)");
+        latch("interp: unsupported interpolator");
     }
 }
 
