@@ -47,6 +47,17 @@ STAGES = {0: 1, 1: 1, 2: 2, 3: 3, 4: 3}
 MEASURED_TRAFFIC = {
     ("k_sl_subcycle", "fp64", 3, 3): (877.944576e6 + 201.871872e6) / 7077888,   # k_sl_subcycle_abc192_cubic_rk3_fp64.md
     ("k_fwd_subcycle", "fp64", 3, 3): (964.329472e6 + 459.971072e6) / 7077888,  # k_fwd_subcycle_abc192_cubic_rk3_fp64.md
+    ("k_sl_subcycle", "mixed", 3, 3): (524.9e6 + 171.9e6) / 7077888,  # advection_kernels_abc192_cubic_rk3_mixed.md
+    ("k_fwd_subcycle", "mixed", 3, 3): (693.8e6 + 393.1e6) / 7077888,  # advection_kernels_abc192_cubic_rk3_mixed.md
+}
+
+# The unit that bounds these kernels is the L1 load path, not HBM: the share of its peak that the
+# same captures measured (l1tex__data_pipe_lsu_wavefronts.avg.pct_of_peak_sustained_elapsed)
+MEASURED_L1_PIPE = {
+    ("k_sl_subcycle", "fp64", 3, 3): 0.9072,
+    ("k_fwd_subcycle", "fp64", 3, 3): 0.9545,
+    ("k_sl_subcycle", "mixed", 3, 3): 0.866,
+    ("k_fwd_subcycle", "mixed", 3, 3): 0.883,
 }
 
 
@@ -390,6 +401,10 @@ def run_b200(args, w):
         if tpp is not None and w["kind"] == "abc":
             rooflines[name]["traffic"] = tpp * N
             rooflines[name]["traffic_source"] = "ncu capture at 192^3 (profiles/), scaled by points"
+        l1 = MEASURED_L1_PIPE.get((name, args.precision, w["interpolator"], w["integrator"]))
+        if l1 is not None and w["kind"] == "abc":
+            rooflines[name]["limiter"] = {"unit": "L1 data pipe (LSU wavefronts)", "frac": l1,
+                                          "source": "ncu capture at 192^3 (profiles/)"}
     roof = max(rooflines.values(), key=lambda r: r["share_of_step"] or 0) if rooflines else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
