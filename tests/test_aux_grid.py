@@ -57,8 +57,9 @@ CASES = [
     ("abc", 3, 3, 0),
     ("turb", 3, 1, 0),
     ("abc_unsteady", 2, 1, 1),
+    ("abc_unsteady", 3, 5, 0),
 ]
-FTLE_TOL = {0: 1e-9, 1: 1e-9, 2: 1e-8, 3: 1e-8}
+FTLE_TOL = {0: 1e-9, 1: 1e-9, 2: 1e-8, 3: 1e-8, 5: 1e-9, 6: 1e-9}
 
 
 @pytest.mark.gpu

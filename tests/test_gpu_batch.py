@@ -16,6 +16,7 @@ INSTANCES = [
     ("dg", 48, SC.FTLE_FWD, 1.0, 0.2, 3, 3, False),
     ("abc", 16, SC.FTLE_BKWD, 1.0, 0.25, 3, 3, False),
     ("turb", 12, SC.FTLE_BKWD, 0.2, 0.05, 2, 1, True),
+    ("abc", 12, SC.FTLE_BKWD, 0.6, 0.2, 3, 6, False),
 ]
 STEPS = 20
 

@@ -96,6 +96,7 @@ CASES = [
     ("abc_unsteady", 2, 1, (2.0, 3.0, 4.0), 1.6),
     ("mixed_bc", 3, 3, (0.5, 0.5, 0.45), 0.35),
     ("dg", 4, 1, (1.0, 0.5, 0.0), 0.3),
+    ("abc_unsteady", 3, 6, (2.0, 3.0, 4.0), 1.6),
 ]
 
 
