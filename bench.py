@@ -74,6 +74,30 @@ def fwd_bytes_per_particle(s: int, interp: int, integrator: int, sv: int = None)
     return vel + 2 * (6 * s + 12)
 
 
+# interpolated points per integration step (the B-spline samples of the velocity)
+SAMPLES = {0: 1, 1: 1, 2: 2, 3: 3, 4: 4}
+
+
+def spline_flops_per_sample(interp: int) -> int:
+    """Algorithmic FP64 flops of one B-spline sample of a 3-component field: per component
+    the tensor-product contraction K^3 + K^2 + K FMAs (2 flops each), plus the basis of the
+    three axes, 3K(K-1)/2 flops each (de Boor recurrence).  K = 4 (CUBIC) or 3 (QUADRATIC)."""
+    K = 4 if interp == 3 else 3
+    return 3 * 2 * (K ** 3 + K ** 2 + K) + 3 * (3 * K * (K - 1) // 2)
+
+
+def advect_flops_per_point(kernel: str, interp: int, integrator: int):
+    """B-spline interpolators only (None otherwise): samples per point times the sample cost,
+    plus 6 flops of Runge-Kutta arithmetic per stage.  The backward SL kernel samples every
+    stage but the first (which starts on the node) and the flow map once; the forward kernel
+    samples every stage."""
+    if interp not in (2, 3):
+        return None
+    n = SAMPLES[integrator]
+    samples = n  # SL: n - 1 velocity stages + 1 flow-map sample; forward: n velocity stages
+    return samples * spline_flops_per_sample(interp) + 6 * n
+
+
 WORKLOADS = {
     "abc256": dict(kind="abc", n=256, dt=0.05, T=10.0, h=1.0, integrator=3, interpolator=3, dirs=(0, 1), t0=0.95,
                    desc="ABC flow 256^3 periodic, dt=0.05, FTLE fwd+bkwd T=10 h=1, RK3, cubic B-spline"),
@@ -380,6 +404,7 @@ def run_b200(args, w):
            "d2h_bytes_per_step": len(handles) * N * 8}
     # --- roofline of the dominant hot kernel (by device time in the timed region) ---
     peaks = measured_peaks()
+    fp64_peak = api.fp64_fma_tflops() if w["interpolator"] in (2, 3) and args.precision == "fp64" else None
     hbm = peaks.get("hbm_gbs")
     s_bytes = 8
     v_bytes = 8 if args.precision == "fp64" else 4
@@ -401,6 +426,12 @@ def run_b200(args, w):
         if tpp is not None and w["kind"] == "abc":
             rooflines[name]["traffic"] = tpp * N
             rooflines[name]["traffic_source"] = "ncu capture at 192^3 (profiles/), scaled by points"
+        fpp = advect_flops_per_point(name, w["interpolator"], w["integrator"])
+        if fpp is not None and fp64_peak:
+            tf = N * fpp / avg_s / 1e12
+            rooflines[name]["fp64"] = {"achieved": tf, "peak": fp64_peak, "unit": "TFLOP/s", "frac": tf / fp64_peak,
+                                       "flops_per_point": fpp,
+                                       "peak_source": "FMA micro-benchmark (cfd2lcs_b200_fp64_fma_rate), this run"}
         l1 = MEASURED_L1_PIPE.get((name, args.precision, w["interpolator"], w["integrator"]))
         if l1 is not None and w["kind"] == "abc":
             rooflines[name]["limiter"] = {"unit": "L1 data pipe (LSU wavefronts)", "frac": l1,
