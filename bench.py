@@ -240,7 +240,7 @@ def dist_setup():
     return world, rank, local
 
 
-def cpu_sample(w, steps: int, threads: int | None = None):
+def cpu_sample(w, steps: int, threads: int | None = None, n: int | None = None):
     """The oracle (CPU restatement of the reference path) on a bounded sample of the
     workload: the same flow, options, dt, T and h on a coarser grid, one update per step.
     96^3 for the ABC flow: about 10 s of oracle work per update on 16 host cores."""
@@ -249,7 +249,7 @@ def cpu_sample(w, steps: int, threads: int | None = None):
     o.reset()
     if threads:
         o.set_threads(threads)
-    nsample = 96 if w["kind"] == "abc" else 128
+    nsample = n or (96 if w["kind"] == "abc" else 128)
     g, vel, steady = make_grid(w, nsample)
     o.init(g.n, g.x, g.y, g.z, g.flag)
     for d in w["dirs"]:
@@ -465,6 +465,9 @@ def run_b200(args, w):
         if world == 1 and not args.no_cpu:
             rate, threads, sample, _ = cpu_sample(w, 1)
             line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+            # the per-rank work of the reference: one thread, on a smaller sample of the workload
+            rate1, _, sample1, _ = cpu_sample(w, 1, threads=1, n=48 if w["kind"] == "abc" else 64)
+            line["cpu_baseline"]["single_thread"] = {"value": rate1, "unit": UNIT, "cores": 1, "sample": sample1}
         print(json.dumps(line), flush=True)
     api.finalize()
     if world > 1:
