@@ -49,6 +49,7 @@ MEASURED_TRAFFIC = {
     ("k_fwd_subcycle", "fp64", 3, 3): (964.329472e6 + 459.971072e6) / 7077888,  # k_fwd_subcycle_abc192_cubic_rk3_fp64.md
     ("k_sl_subcycle", "mixed", 3, 3): (524.9e6 + 171.9e6) / 7077888,  # advection_kernels_abc192_cubic_rk3_mixed.md
     ("k_fwd_subcycle", "mixed", 3, 3): (693.8e6 + 393.1e6) / 7077888,  # advection_kernels_abc192_cubic_rk3_mixed.md
+    ("k_sl_subcycle", "fp64", 1, 2): 1957.404e9 * 0.352992e-3 / 7077888,  # k_sl_subcycle_abc192_linear_rk2_fp64.md
 }
 
 # The unit that bounds these kernels is the L1 load path, not HBM: the share of its peak that the
