@@ -116,10 +116,12 @@ __global__ void __launch_bounds__(256) k_ingest(DevGrid<T> g, const U *__restric
 // kernels 104 registers (2 blocks, 16 warps per SM); a minimum of 1 block lets it take up to
 // 255.  Measured on B200 (ABC 256^3 RK3 CUBIC, turbulence 512^3 RK2 LINEAR): 4 blocks (64
 // registers) for the B-spline kernels took the FP64 backward subcycle from 5.02 to 4.32 ms and
-// the forward one from 8.85 to 7.52 ms despite a few spilled registers; 5 blocks (48 registers)
-// suits the LINEAR backward kernel (6 blocks, 40 registers, was slower).
+// the forward one from 8.85 to 7.52 ms despite a few spilled registers.  The LINEAR backward
+// kernel (latency-bound: three dependent gathers per point) with 3 / 4 / 5 blocks: ABC 256^3
+// RK2 0.848 / 0.742 / 0.800 ms, turbulence 512^3 8.06 / 7.58 / 7.56 ms (6 blocks, 40
+// registers, was 7 % slower than 5 on the turbulence).
 #ifndef CFD2LCS_SL_MINB_LINEAR
-#define CFD2LCS_SL_MINB_LINEAR 5
+#define CFD2LCS_SL_MINB_LINEAR 4
 #endif
 #ifndef CFD2LCS_SL_MINB_SPLINE
 #define CFD2LCS_SL_MINB_SPLINE 4
