@@ -2546,6 +2546,26 @@ EXPORT void orc_get_grid(real *xyz, int *flag, real *nrm, real *inv_delta, int *
 }
 
 /* Unit-level helpers (known-answer tests) */
+
+/* interp_s2u_r1 with `method` on the initialised solver grid for np points (pts: x block, y
+ * block, z block) with their nodes (padded indices, same layout); f3 holds three padded fields
+ * of orc_padded_size() values, x fastest.  out receives the three components, one block each. */
+EXPORT int orc_interp_points(int method, const real *f3, int np, const real *pts, const int *nodes, real *out) {
+    if (!S.inited) return 1;
+    const long nt = S.g.d.ntot;
+    sr1_t f;
+    for (int c = 0; c < 3; c++) f.c[c] = (real *)f3 + c * nt;
+    real *xp[3];
+    int *no[3];
+    real *o[3];
+    for (int c = 0; c < 3; c++) {
+        xp[c] = (real *)pts + (long)c * np;
+        no[c] = (int *)nodes + (long)c * np;
+        o[c] = out + (long)c * np;
+    }
+    interp_r1(&S.g, method, np, xp, no, &f, o);
+    return S.error;
+}
 EXPORT double orc_eig3_max(const double *a9) {
     long double A[3][3];
     for (int r = 0; r < 3; r++)

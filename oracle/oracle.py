@@ -76,6 +76,8 @@ class Oracle:
         L.orc_bspline3.restype = C.c_int
         L.orc_bspline3_coef.argtypes = [P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, P]
         L.orc_bspline3_coef.restype = C.c_int
+        L.orc_interp_points.argtypes = [C.c_int, P, C.c_int, P, P, P]
+        L.orc_interp_points.restype = C.c_int
         assert L.orc_real_size() == np.dtype(self.dtype).itemsize
         self.n = None
 
@@ -212,6 +214,18 @@ class Oracle:
         rc = self.lib.orc_bspline3(self._p(xg), self._p(yg), self._p(zg), len(xg), len(yg), len(zg), kx, ky, kz, self._p(f),
                                    len(pts), self._p(px), self._p(py), self._p(pz), self._p(out))
         assert rc == 0
+        return out
+
+    def interp_points(self, method, f3, pts, nodes):
+        """interp_s2u_r1 on the initialised grid: f3 (3, n1+2, n2+2, n3+2) padded fields, pts
+        (3, np) positions, nodes (3, np) padded node indices; returns (3, np)."""
+        f = np.ascontiguousarray(np.asarray(f3, dtype=self.dtype).transpose(0, 3, 2, 1)).ravel()
+        p = np.ascontiguousarray(np.asarray(pts, dtype=self.dtype))
+        q = np.ascontiguousarray(np.asarray(nodes, dtype=np.int32))
+        out = np.zeros(p.shape, dtype=self.dtype)
+        rc = self.lib.orc_interp_points(int(method), self._p(f), p.shape[1], self._p(p), self._p(q), self._p(out))
+        if rc:
+            raise RuntimeError(self.error_msg())
         return out
 
     def bspline3_coef(self, xg, yg, zg, f, order):
