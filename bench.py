@@ -248,8 +248,9 @@ def cpu_sample(w, steps: int, threads: int | None = None, n: int | None = None):
     from oracle.oracle import Oracle
     o = Oracle("dp")
     o.reset()
-    if threads:
-        o.set_threads(threads)
+    # every usable host core unless told otherwise: a launcher's OMP_NUM_THREADS (torchrun sets
+    # 1 for N > 1) must not turn the baseline into a single-thread one
+    o.set_threads(threads or len(os.sched_getaffinity(0)))
     nsample = n or (96 if w["kind"] == "abc" else 128)
     g, vel, steady = make_grid(w, nsample)
     o.init(g.n, g.x, g.y, g.z, g.flag)
