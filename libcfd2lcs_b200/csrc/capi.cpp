@@ -6,6 +6,7 @@
 // Error convention as in the reference (src/cfd2lcs.f90:684-706): no return codes; the
 // first error latches a flag, is reported once on stdout, and every later call returns
 // immediately.
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -29,13 +30,25 @@ enum { LCS_FALSE = 0, LCS_TRUE = 1 };
 enum { NEAREST_NBR = 0, LINEAR = 1, QUADRATIC = 2, CUBIC = 3, TSE = 5, TSE_LIMIT = 6 };
 enum { EULER = 0, TRAPEZOIDAL = 1, RK2 = 2, RK3 = 3, RK4 = 4 };
 
+// State of the cfd2lcs_info table (cumulative times in seconds)
+struct InfoState {
+  bool started = false;
+  std::chrono::steady_clock::time_point t_last;
+  Counters prev;
+  double total_sim = 0, total_lcs = 0, fwd = 0, bkwd = 0, reconstruct = 0, ftle = 0;
+  long long fwd_n = 0, bkwd_n = 0;
+  double fwd_s = 0, bkwd_s = 0;
+};
+
 struct Library {
   int error = 0;
   std::string msg;
   Options opt;
   std::unique_ptr<EngineBase> eng;
   bool inited = false;
+  bool sync_timer = false;
   Counters zero;
+  InfoState info;
 };
 
 Library &L() {
@@ -73,6 +86,7 @@ void do_init(const int *n, const int *offset, const lcsdata_t *x, const lcsdata_
   if (lib.error) return;
   lib.eng.reset();
   lib.inited = false;
+  lib.info = InfoState();
   lib.eng = cfd2lcs::make_engine(&lib.opt);
   std::string msg;
   if (!lib.eng->init(n, x, y, z, flag, msg)) {
@@ -97,6 +111,81 @@ int do_diagnostic_init(int type, int resolution, lcsdata_t T, lcsdata_t h, const
   return id;
 }
 
+// cfd2lcs_info (src/cfd2lcs.f90:708-810): the reference's table of time per phase and particle
+// integration rates after every update, printed here when CFD2LCS_B200_INFO is set (off by
+// default, so that a solver's standard output stays its own).  The first call only starts the
+// clock, as in the reference.  Phase times are the device's (CUDA events): FWD / BKWD Advect,
+// Reconstruct (snapshot + composition), LCS (FTLE); the I/O, LP re-map and error-check phases of
+// the reference have no device counterpart here (0); "Other" is the rest of the update (ingest
+// and the CFL read-back).  Application total is the wall clock from one update's end to the next.
+void print_info() {
+  Library &lib = L();
+  const char *e = std::getenv("CFD2LCS_B200_INFO");
+  if (lib.error || !lib.eng || !e || !e[0] || e[0] == '0') return;
+  InfoState &I = lib.info;
+  const auto now = std::chrono::steady_clock::now();
+  const Counters &c = lib.eng->counters();
+  if (!I.started) {
+    I = InfoState();
+    I.started = true;
+    I.t_last = now;
+    I.prev = c;
+    return;
+  }
+  const Counters &p = I.prev;
+  const double s_fwd = (c.phase_ms[2] - p.phase_ms[2]) * 1e-3, s_bkwd = (c.phase_ms[1] - p.phase_ms[1]) * 1e-3;
+  const double s_rec = (c.phase_ms[3] - p.phase_ms[3] + c.phase_ms[4] - p.phase_ms[4]) * 1e-3;
+  const double s_ftle = (c.phase_ms[5] - p.phase_ms[5]) * 1e-3, s_lcs = (c.phase_ms[6] - p.phase_ms[6]) * 1e-3;
+  const long long n_fwd = c.integrations_fwd - p.integrations_fwd, n_bkwd = c.integrations_bkwd - p.integrations_bkwd;
+  I.total_sim += std::chrono::duration<double>(now - I.t_last).count();
+  I.total_lcs += s_lcs;
+  I.fwd += s_fwd;
+  I.bkwd += s_bkwd;
+  I.reconstruct += s_rec;
+  I.ftle += s_ftle;
+  I.fwd_n += n_fwd;
+  I.bkwd_n += n_bkwd;
+  I.fwd_s += s_fwd;
+  I.bkwd_s += s_bkwd;
+  I.t_last = now;
+  I.prev = c;
+  char a[32], b[32];
+  auto es = [](double v, char *out) {
+    cfd2lcs::format_es(v, 18, 4, out);
+    out[18] = 0;
+  };
+  auto row = [&](const char *label, double t) {
+    es(t, a);
+    std::printf("%s%s | %17.4f%% |\n", label, a, I.total_sim > 0 ? t / I.total_sim * 100.0 : 0.0);
+  };
+  auto rate = [&](const char *label, long long n, double t) {
+    es((double)n, a);
+    es(t > 0 ? (double)n / t : 0.0, b);
+    std::printf("%s%s | %s |\n", label, a, b);
+  };
+  std::printf("%s\n", lib.sync_timer ? "-----libcfd2lcs CPU overhead (MPI synchronized)-------------------"
+                                     : "-----libcfd2lcs CPU overhead (NOT synchronized, rank 0 only)------");
+  std::printf("|      TASK             |  WALL CLOCK [SEC] |     %% OF TOTAL     |\n");
+  es(I.total_sim, a);
+  std::printf("|Application, Total:    |%s |          -         |\n", a);
+  row("|cfd2lcs, Total:        |", I.total_lcs);
+  row("|cfd2lcs, FWD Advect:   |", I.fwd);
+  row("|cfd2lcs, BKWD Advect:  |", I.bkwd);
+  row("|cfd2lcs, Reconstruct:  |", I.reconstruct);
+  row("|cfd2lcs, LP Re-map:    |", 0.0);
+  row("|cfd2lcs, I/O:          |", 0.0);
+  row("|cfd2lcs, LCS:          |", I.ftle);
+  row("|cfd2lcs, Error Check:  |", 0.0);
+  row("|cfd2lcs, Other:        |", I.total_lcs - (I.fwd + I.bkwd + I.reconstruct + I.ftle));
+  std::printf("| PARTICLE INTEGRATIONS |  NUMBER [N/STEP]  |     RATE [N/SEC]   |\n");
+  rate("|Forward (this step):   |", n_fwd, s_fwd);
+  rate("|Backward (this step):  |", n_bkwd, s_bkwd);
+  rate("|Forward (cumulative):  |", I.fwd_n, I.fwd_s);
+  rate("|Backward (cumulative): |", I.bkwd_n, I.bkwd_s);
+  std::printf("------------------------------------------------------------------\n");
+  std::fflush(stdout);
+}
+
 void do_update(const int *n, const lcsdata_t *u, const lcsdata_t *v, const lcsdata_t *w, lcsdata_t time, bool dev) {
   Library &lib = L();
   if (lib.error) return;
@@ -106,6 +195,7 @@ void do_update(const int *n, const lcsdata_t *u, const lcsdata_t *v, const lcsda
   }
   std::string msg;
   if (!lib.eng->update(n, u, v, w, time, dev, msg)) latch(msg);
+  print_info();
 }
 
 // cfd2lcs_set_option, src/cfd2lcs.f90:436-622
@@ -116,6 +206,7 @@ void do_set_option(const std::string &opt, int val) {
   bool ok = true;
   if (opt == "SYNCTIMER" || opt == "DEBUG") {
     ok = tf;  // timing / verbosity switches: accepted, no effect on the results
+    if (ok && opt == "SYNCTIMER") lib.sync_timer = val == LCS_TRUE;
   } else if (opt == "WRITE_FLOWMAP" || opt == "WRITE_VELOCITY" || opt == "WRITE_BCFLAG") {
     ok = tf;  // variables of the output files (src/cfd2lcs.f90:494-531)
     if (ok) (opt == "WRITE_FLOWMAP" ? lib.opt.write_flowmap : opt == "WRITE_VELOCITY" ? lib.opt.write_velocity : lib.opt.write_bcflag) = val;
@@ -241,6 +332,8 @@ CFD2LCS_EXPORT void cfd2lcs_reset_c(void) {
   lib.error = 0;
   lib.msg.clear();
   lib.opt = Options();
+  lib.sync_timer = false;
+  lib.info = InfoState();
 }
 
 CFD2LCS_EXPORT int cfd2lcs_get_ftle_c(int lcs_handle, lcsdata_t *ftle) {

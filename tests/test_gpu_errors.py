@@ -76,3 +76,29 @@ def test_bad_option_latches(api, opt, val, text):
     err, msg = api.error()
     assert err != 0 and text in msg, msg
     _clean_run_after(api)
+
+
+def test_info_table(api, capfd, monkeypatch):
+    """cfd2lcs_info's table (src/cfd2lcs.f90:708-810) after each update but the first, when
+    CFD2LCS_B200_INFO is set: the reference's rows, and this step's backward integrations equal
+    to the library's counter."""
+    monkeypatch.setenv("CFD2LCS_B200_INFO", "1")
+    g, vel, prm, h = _start(api)
+    capfd.readouterr()
+    counts = []
+    for k in range(4):
+        t = W.time_at(k, prm["dt"])
+        c0 = api.counters()["integrations_bkwd"]
+        api.update(*vel(t), t)
+        counts.append(api.counters()["integrations_bkwd"] - c0)
+    out = capfd.readouterr().out
+    monkeypatch.delenv("CFD2LCS_B200_INFO")
+    api.reset()
+    tables = out.split("-----libcfd2lcs CPU overhead (NOT synchronized, rank 0 only)------")[1:]
+    assert len(tables) == 3, out
+    for label in ("|Application, Total:    |", "|cfd2lcs, BKWD Advect:  |", "|cfd2lcs, LCS:          |",
+                  "| PARTICLE INTEGRATIONS |", "|Backward (cumulative): |"):
+        assert label in tables[-1]
+    line = [ln for ln in tables[-1].splitlines() if ln.startswith("|Backward (this step):  |")][0]
+    assert counts[-1] > 0
+    assert abs(float(line.split("|")[2]) - counts[-1]) <= 1e-4 * counts[-1]  # ES18.4: 4 significant digits
