@@ -54,3 +54,20 @@ def test_two_gloo_ranks():
     assert [r[1] for r in res] == [2.5, 2.5]
     assert [r[2] for r in res] == [(2, 0, 0), (2, 1, 1)]
     assert res[1][3] == ""
+
+
+def test_cpu_baseline_uses_every_usable_core(monkeypatch):
+    """A launcher's OMP_NUM_THREADS (torchrun sets 1 for N > 1) does not shrink the CPU
+    baseline: the oracle is given every usable core unless a thread count is asked for."""
+    sys.path.insert(0, ROOT)
+    import bench
+    monkeypatch.setenv("OMP_NUM_THREADS", "1")
+    w = bench.WORKLOADS["dg512"]
+    _, threads, sample, _ = bench.cpu_sample(w, 1, n=32)
+    assert threads == len(os.sched_getaffinity(0)), sample
+    try:
+        _, one, _, _ = bench.cpu_sample(w, 1, threads=1, n=32)
+        assert one == 1
+    finally:  # the OpenMP thread count is process-wide: give later oracle tests every core back
+        from oracle.oracle import Oracle
+        Oracle("dp").set_threads(len(os.sched_getaffinity(0)))
