@@ -41,24 +41,15 @@ UNIT = "grid-pt·RK-steps/s"
 # data as above.
 STAGES = {0: 1, 1: 1, 2: 2, 3: 3, 4: 3}
 
-# DRAM bytes per point of one launch (dram__bytes_read.sum + dram__bytes_write.sum) from the ncu
-# captures summarised in profiles/ (192^3 ABC, 7077888 points), scaled to the benchmark grid by
-# its point count: (kernel, precision, interpolator, integrator) -> bytes per point
+# DRAM bytes per point of one launch (dram__bytes_read.sum + dram__bytes_write.sum) from ncu
+# captures at 192^3 (ABC flow, 7077888 points), scaled to the benchmark grid by its point count:
+# (kernel, precision, interpolator, integrator) -> (bytes per point, where the figure comes from)
 MEASURED_TRAFFIC = {
-    ("k_sl_subcycle", "fp64", 3, 3): (877.944576e6 + 201.871872e6) / 7077888,   # k_sl_subcycle_abc192_cubic_rk3_fp64.md
-    ("k_fwd_subcycle", "fp64", 3, 3): (964.329472e6 + 459.971072e6) / 7077888,  # k_fwd_subcycle_abc192_cubic_rk3_fp64.md
-    ("k_sl_subcycle", "mixed", 3, 3): (524.9e6 + 171.9e6) / 7077888,  # advection_kernels_abc192_cubic_rk3_mixed.md
-    ("k_fwd_subcycle", "mixed", 3, 3): (693.8e6 + 393.1e6) / 7077888,  # advection_kernels_abc192_cubic_rk3_mixed.md
-    ("k_sl_subcycle", "fp64", 1, 2): 1957.404e9 * 0.352992e-3 / 7077888,  # k_sl_subcycle_abc192_linear_rk2_fp64.md
-}
-
-# The unit that bounds these kernels is the L1 load path, not HBM: the share of its peak that the
-# same captures measured (l1tex__data_pipe_lsu_wavefronts.avg.pct_of_peak_sustained_elapsed)
-MEASURED_L1_PIPE = {
-    ("k_sl_subcycle", "fp64", 3, 3): 0.9072,
-    ("k_fwd_subcycle", "fp64", 3, 3): 0.9545,
-    ("k_sl_subcycle", "mixed", 3, 3): 0.866,
-    ("k_fwd_subcycle", "mixed", 3, 3): 0.883,
+    ("k_sl_subcycle", "fp64", 3, 3): ((877.944576e6 + 201.871872e6) / 7077888, "ncu capture 2026-12-03, ABC 192^3, scaled by points"),
+    ("k_fwd_subcycle", "fp64", 3, 3): ((964.329472e6 + 459.971072e6) / 7077888, "ncu capture 2026-12-03, ABC 192^3, scaled by points"),
+    ("k_sl_subcycle", "mixed", 3, 3): ((524.9e6 + 171.9e6) / 7077888, "ncu capture 2026-12-03, ABC 192^3, scaled by points"),
+    ("k_fwd_subcycle", "mixed", 3, 3): ((693.8e6 + 393.1e6) / 7077888, "ncu capture 2026-12-03, ABC 192^3, scaled by points"),
+    ("k_sl_subcycle", "fp64", 1, 2): (1957.404e9 * 0.352992e-3 / 7077888, "ncu capture 2026-12-03, ABC 192^3, scaled by points"),
 }
 
 
@@ -289,17 +280,28 @@ def run_reference(args, w):
     print(json.dumps(line), flush=True)
 
 
-def run_b200(args, w):
+def full_frame_update(w) -> int:
+    """Index of the update whose FTLE frame composes nint(T/h) sub-flow maps that each span a
+    whole h interval: the first h boundary after t0, plus T."""
+    b1 = (math.floor(w["t0"] / w["h"] + 1e-9) + 1) * w["h"]
+    return int(round((b1 + w["T"] - w["t0"]) / w["dt"]))
+
+
+def ftle_error(a, b):
+    d = np.abs(np.asarray(a, dtype=np.float64) - np.asarray(b, dtype=np.float64)).ravel()
+    return {"max": float(d.max()), "rms": float(np.sqrt(np.mean(d * d))), "p99_99": float(np.quantile(d, 0.9999)),
+            "points_above_1e-4": int(np.count_nonzero(d > 1e-4)), "points": int(d.size)}
+
+
+def run_form(args, w, precision, local, world, rank, clocks=False, e2e=False, horizon=None):
+    """One library instance of the workload in one precision form: W warm-up updates, K timed
+    updates (inputs resident in HBM), optionally K end-to-end updates through cfd2lcs_update_c,
+    optionally continued (untimed) to update `horizon`, whose frame's FTLE fields it returns."""
     import torch
-    world, rank, local = dist_setup()
-    torch.cuda.set_device(local)
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
     import libcfd2lcs_b200 as L
     api = L.Cfd2lcs("dp")
     api.reset()
-    if args.precision == "mixed":
+    if precision == "mixed":
         api.set_option("MIXED_PRECISION", 1)
     g, vel, steady = make_grid(w, args.n)
     api.init(g.n, g.x, g.y, g.z, g.flag)
@@ -325,7 +327,7 @@ def run_b200(args, w):
     fields = [dev_fields(w["t0"])] if steady else ([] if lazy else [dev_fields(w["t0"] + s * w["dt"]) for s in range(total + 1)])
 
     def step(s):
-        f = fields[0] if steady else (dev_fields(w["t0"] + s * w["dt"]) if lazy else fields[s])
+        f = fields[0] if steady else (dev_fields(w["t0"] + s * w["dt"]) if lazy or s >= len(fields) else fields[s])
         api.update_device(f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr(), w["t0"] + s * w["dt"])
 
     step(0)  # first call (no advection)
@@ -334,17 +336,19 @@ def run_b200(args, w):
     err, msg = api.error()
     if err:
         raise RuntimeError(msg)
-    frame_ph = api.phase_times_ms()
-    frame_cnt = api.counters()
     # --- timed region (inputs resident in HBM) ---
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     c0, p0, k0 = api.counters(), api.phase_times_ms(), api.kernel_times()
-    with ClockSampler(local) as clk:
-        for s in range(args.warmup + 1, total + 1):
-            step(s)
-        torch.cuda.synchronize()
+    sampler = ClockSampler(local) if clocks else None
+    if sampler:
+        sampler.__enter__()
+    for s in range(args.warmup + 1, total + 1):
+        step(s)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.__exit__(None, None, None)
     if world > 1:
         torch.distributed.barrier()
     c1, p1, k1 = api.counters(), api.phase_times_ms(), api.kernel_times()
@@ -354,111 +358,185 @@ def run_b200(args, w):
     work = (c1["integrations_fwd"] + c1["integrations_bkwd"]) - (c0["integrations_fwd"] + c0["integrations_bkwd"])
     ms = p1["update_total"] - p0["update_total"]
     ms_max = rank_max(ms, world, dev)
-    value = world * work / (ms_max / 1000.0)
-    launches = c1["kernel_launches"] - c0["kernel_launches"]
-    # FTLE-field time: snapshot + composition + FTLE of the frames seen so far
-    frames = c1["ftle_frames"]
-    ftle_ms = (p1["snapshot"] + p1["compose"] + p1["ftle"]) / frames if frames else None
-    # --- end to end: host arrays through cfd2lcs_update_c, FTLE read back each step ---
-    pin = []
-    for s in range(args.steps):
-        t = w["t0"] + (total + 1 + s) * w["dt"]
-        arrs = []
-        if lazy:
-            for a in dev_fields(t):
-                tt = torch.empty(N, dtype=torch.float64, pin_memory=True)
-                tt.copy_(a)
-                arrs.append(tt)
-                del a
-        else:
-            u, v, wv = vel(t)
-            for a in (u, v, wv):
-                tt = torch.empty(N, dtype=torch.float64, pin_memory=True)
-                tt.numpy()[:] = a.ravel(order="F")
-                arrs.append(tt)
-        pin.append((t, arrs))
-        if steady:
-            break
-    out = torch.empty(N, dtype=torch.float64, pin_memory=True)
-    nint = np.ascontiguousarray(g.n, dtype=np.int32)
-    ce0 = api.counters()
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    t_e0 = time.perf_counter()
-    for s in range(args.steps):
-        tt, arrs = pin[0] if steady else pin[s]
-        tt = w["t0"] + (total + 1 + s) * w["dt"]
-        api.lib.cfd2lcs_update_c(api._p(nint), arrs[0].data_ptr(), arrs[1].data_ptr(), arrs[2].data_ptr(), api.R(tt))
-        for h in handles:
-            api.lib.cfd2lcs_get_ftle_c(int(h), out.data_ptr())
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t_e0
-    e2e_max = rank_max(e2e_s, world, dev)
-    if world > 1:
-        torch.distributed.barrier()
-    ce1 = api.counters()
-    err, msg = api.error()
-    if err:
-        raise RuntimeError(msg)
-    e2e_work = (ce1["integrations_fwd"] + ce1["integrations_bkwd"]) - (ce0["integrations_fwd"] + ce0["integrations_bkwd"])
-    e2e = {"value": world * e2e_work / e2e_max, "unit": UNIT, "h2d_bytes_per_step": 3 * N * 8,
-           "d2h_bytes_per_step": len(handles) * N * 8}
-    # --- roofline of the dominant hot kernel (by device time in the timed region) ---
-    peaks = measured_peaks()
-    fp64_peak = api.fp64_fma_tflops() if w["interpolator"] in (2, 3) and args.precision == "fp64" else None
-    hbm = peaks.get("hbm_gbs")
+    out = dict(api=api, g=g, N=N, handles=handles, work=work, ms=ms, ms_max=ms_max, value=world * work / (ms_max / 1000.0),
+               launches=c1["kernel_launches"] - c0["kernel_launches"], c0=c0, c1=c1, p0=p0, p1=p1, k0=k0, k1=k1,
+               clocks=sampler.summary() if sampler else None, staged=api.staged_launches())
+    nxt = total + 1
+    if e2e:
+        # --- end to end: host arrays through cfd2lcs_update_c, FTLE read back each step ---
+        pin = []
+        for s in range(args.steps):
+            t = w["t0"] + (total + 1 + s) * w["dt"]
+            arrs = []
+            if lazy:
+                for a in dev_fields(t):
+                    tt = torch.empty(N, dtype=torch.float64, pin_memory=True)
+                    tt.copy_(a)
+                    arrs.append(tt)
+                    del a
+            else:
+                u, v, wv = vel(t)
+                for a in (u, v, wv):
+                    tt = torch.empty(N, dtype=torch.float64, pin_memory=True)
+                    tt.numpy()[:] = a.ravel(order="F")
+                    arrs.append(tt)
+            pin.append(arrs)
+            if steady:
+                break
+        res = torch.empty(N, dtype=torch.float64, pin_memory=True)
+        nint = np.ascontiguousarray(g.n, dtype=np.int32)
+        ce0 = api.counters()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        t_e0 = time.perf_counter()
+        for s in range(args.steps):
+            arrs = pin[0] if steady else pin[s]
+            tt = w["t0"] + (total + 1 + s) * w["dt"]
+            api.lib.cfd2lcs_update_c(api._p(nint), arrs[0].data_ptr(), arrs[1].data_ptr(), arrs[2].data_ptr(), api.R(tt))
+            for h in handles:
+                api.lib.cfd2lcs_get_ftle_c(int(h), res.data_ptr())
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t_e0
+        e2e_max = rank_max(e2e_s, world, dev)
+        if world > 1:
+            torch.distributed.barrier()
+        ce1 = api.counters()
+        err, msg = api.error()
+        if err:
+            raise RuntimeError(msg)
+        e2e_work = (ce1["integrations_fwd"] + ce1["integrations_bkwd"]) - (ce0["integrations_fwd"] + ce0["integrations_bkwd"])
+        out["e2e"] = {"value": world * e2e_work / e2e_max, "unit": UNIT, "h2d_bytes_per_step": 3 * N * 8,
+                      "d2h_bytes_per_step": len(handles) * N * 8}
+        nxt = total + 1 + args.steps
+    if horizon is not None:
+        fields.clear()
+        for s in range(nxt, horizon + 1):
+            step(s)
+        err, msg = api.error()
+        if err:
+            raise RuntimeError(msg)
+        out["ftle"] = {d: np.array(api.ftle(h), copy=True) for d, h in zip(w["dirs"], handles)}
+        out["horizon_t"] = w["t0"] + horizon * w["dt"]
+    return out
+
+
+def hot_kernel_rooflines(r, w, precision, hbm, fp64_peak):
+    """Roofline of the two hot kernels from one form's timed region: algorithmic bytes per
+    launch over the CUDA-event launch time, against the measured HBM copy bandwidth."""
+    N = r["N"]
     s_bytes = 8
-    v_bytes = 8 if args.precision == "fp64" else 4
+    v_bytes = 8 if precision == "fp64" else 4
+    k0, k1 = r["k0"], r["k1"]
     cands = []
     nsl, nfw = k1["sl_launches"] - k0["sl_launches"], k1["fwd_launches"] - k0["fwd_launches"]
     if nsl > 0:
-        cands.append(("k_sl_subcycle", k1["sl_ms"] - k0["sl_ms"], nsl, sl_bytes_per_point(s_bytes, w["interpolator"], w["integrator"], v_bytes)))
+        cands.append(("k_sl_tile" if r["staged"]["sl"] > 0 else "k_sl_subcycle", k1["sl_ms"] - k0["sl_ms"], nsl,
+                      sl_bytes_per_point(s_bytes, w["interpolator"], w["integrator"], v_bytes)))
     if nfw > 0:
-        cands.append(("k_fwd_subcycle", k1["fwd_ms"] - k0["fwd_ms"], nfw, fwd_bytes_per_particle(s_bytes, w["interpolator"], w["integrator"], v_bytes)))
+        cands.append(("k_fwd_tile" if r["staged"]["fwd"] > 0 else "k_fwd_subcycle", k1["fwd_ms"] - k0["fwd_ms"], nfw,
+                      fwd_bytes_per_particle(s_bytes, w["interpolator"], w["integrator"], v_bytes)))
     rooflines = {}
     for name, tot_ms, nl, bpp in cands:
         avg_s = tot_ms / nl / 1000.0
         achieved = N * bpp / avg_s / 1e9
         rooflines[name] = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                            "frac": achieved / hbm if hbm else None, "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)",
-                           "avg_launch_ms": avg_s * 1000.0, "share_of_step": tot_ms / ms if ms else None,
+                           "avg_launch_ms": avg_s * 1000.0, "share_of_step": tot_ms / r["ms"] if r["ms"] else None,
                            "algorithmic_bytes_per_point": bpp, "algorithmic_bytes_per_launch": N * bpp, "traffic": None}
-        tpp = MEASURED_TRAFFIC.get((name, args.precision, w["interpolator"], w["integrator"]))
+        tpp = MEASURED_TRAFFIC.get((name, precision, w["interpolator"], w["integrator"]))
         if tpp is not None and w["kind"] == "abc":
-            rooflines[name]["traffic"] = tpp * N
-            rooflines[name]["traffic_source"] = "ncu capture at 192^3 (profiles/), scaled by points"
+            rooflines[name]["traffic"] = tpp[0] * N
+            rooflines[name]["traffic_source"] = tpp[1]
         fpp = advect_flops_per_point(name, w["interpolator"], w["integrator"])
         if fpp is not None and fp64_peak:
             tf = N * fpp / avg_s / 1e12
             rooflines[name]["fp64"] = {"achieved": tf, "peak": fp64_peak, "unit": "TFLOP/s", "frac": tf / fp64_peak,
                                        "flops_per_point": fpp,
                                        "peak_source": "FMA micro-benchmark (cfd2lcs_b200_fp64_fma_rate), this run"}
-        l1 = MEASURED_L1_PIPE.get((name, args.precision, w["interpolator"], w["integrator"]))
-        if l1 is not None and w["kind"] == "abc":
-            rooflines[name]["limiter"] = {"unit": "L1 data pipe (LSU wavefronts)", "frac": l1,
-                                          "source": "ncu capture at 192^3 (profiles/)"}
-    roof = max(rooflines.values(), key=lambda r: r["share_of_step"] or 0) if rooflines else None
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+    return rooflines
+
+
+def ftle_field_roofline(r, w, hbm):
+    """FTLE-field time per frame (ring snapshot + composition + FTLE, event-timed over every
+    frame so far) against its HBM bound: per point nslot sub-map reads (3 FP64 each), the
+    composed map (3) and the FTLE (1) -- (nslot*24 + 24 + 8) bytes."""
+    p1, c1 = r["p1"], r["c1"]
+    frames = c1["ftle_frames"]
+    if not frames:
+        return None
+    ms = (p1["snapshot"] + p1["compose"] + p1["ftle"]) / frames
+    nslot = int(round(w["T"] / w["h"]))
+    byts = r["N"] * (nslot * 24 + 24 + 8)
+    ach = byts / (ms / 1000.0) / 1e9
+    return {"ms_per_frame": ms, "snapshot_ms": p1["snapshot"] / frames, "compose_ms": p1["compose"] / frames,
+            "ftle_ms": p1["ftle"] / frames, "frames": frames, "algorithmic_bytes": byts, "bound_ms": byts / (hbm * 1e9) * 1e3 if hbm else None,
+            "achieved_gbs": ach, "frac": ach / hbm if hbm else None}
+
+
+def run_b200(args, w):
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    import libcfd2lcs_b200 as L  # noqa: F401
+    dev = torch.device("cuda", local)
+    # the mixed form beside the plain FP64 one: same run, same workload, FTLE error over the
+    # workload's full horizon (the ABC flow: 201 updates at 256^3)
+    with_mixed = args.precision == "fp64" and args.mixed == "on" or (args.mixed == "auto" and args.precision == "fp64"
+                                                                      and w["kind"] == "abc" and world == 1)
+    horizon = full_frame_update(w) if with_mixed else None
+    r = run_form(args, w, args.precision, local, world, rank, clocks=True, e2e=True, horizon=horizon)
+    api = r["api"]
+    peaks = measured_peaks()
+    fp64_peak = api.fp64_fma_tflops() if w["interpolator"] in (2, 3) and args.precision == "fp64" else None
+    hbm = peaks.get("hbm_gbs")
+    rooflines = hot_kernel_rooflines(r, w, args.precision, hbm, fp64_peak)
+    roof = max(rooflines.values(), key=lambda x: x["share_of_step"] or 0) if rooflines else None
+    c1, p0, p1 = r["c1"], r["p0"], r["p1"]
+    frames = c1["ftle_frames"]
+    ffr = ftle_field_roofline(r, w, hbm)
+    g = r["g"]
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": r["ms_max"] / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f64 positions, f32 velocity", "data": "synthetic",
             "config": {"workload": w["desc"], "grid": list(g.n), "precision": args.precision, "l2": "inputs larger than L2 (126 MB)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-            "ftle_field_ms": ftle_ms, "ftle_frames_seen": frames,
+            "ftle_field_ms": ffr["ms_per_frame"] if ffr else None, "ftle_field": ffr, "ftle_frames_seen": frames,
             "slots_composed_per_frame": (c1["slots_composed"] / frames if frames else None),
             "nsub_per_update": {"fwd": c1["nsub_fwd"], "bkwd": c1["nsub_bkwd"]},
-            "gpu_launches": launches, "e2e": e2e, "roofline": roof, "rooflines": rooflines,
+            "gpu_launches": r["launches"], "staged_launches": r["staged"], "e2e": r["e2e"], "roofline": roof, "rooflines": rooflines,
             "phase_ms_per_step": {k: (p1[k] - p0[k]) / args.steps for k in p1}}
     if args.precision == "fp64":
         line["ftle_error"] = {"form": "plain FP64", "vs": "FP64 oracle (CPU restatement of the reference)",
                               "max_abs_tolerance": 1e-8 if w["interpolator"] >= 2 else 1e-9,
-                              "where": "tests/test_gpu_parity.py, every integrator / interpolator on small grids"}
-    line["clocks"] = clk.summary() if rank == 0 else None
+                              "where": "tests/test_golden_configs.py (benchmark configurations at 48^3 / 512x256 over their "
+                                       "full horizon) and tests/test_gpu_parity.py (every integrator / interpolator)"}
+    line["clocks"] = r["clocks"] if rank == 0 else None
+    ftle64 = r.get("ftle")
+    api.finalize()
+    del r, api
+    if with_mixed:
+        m = run_form(args, w, "mixed", local, world, rank, horizon=horizon)
+        mixed_ftle = m["ftle"]
+        mroof = hot_kernel_rooflines(m, w, "mixed", hbm, None)
+        line["mixed"] = {
+            "form": "mixed: FP32 velocity levels, spline coefficients and stage blends; FP64 positions, flow maps, "
+                    "composition, Cauchy-Green and eigen-solve",
+            "value": m["value"], "unit": UNIT, "ms_per_step": m["ms_max"] / args.steps, "ratio_vs_fp64": m["value"] / line["value"],
+            "ftle_field_ms": (ftle_field_roofline(m, w, hbm) or {}).get("ms_per_frame"), "rooflines": mroof,
+            "phase_ms_per_step": {k: (m["p1"][k] - m["p0"][k]) / args.steps for k in m["p1"]},
+            "ftle_error": {"vs": "plain FP64 GPU path of this run (itself parity-tested against the FP64 oracle)",
+                           "grid": list(g.n), "updates": horizon, "frame_t": m["horizon_t"],
+                           **{("fwd" if d == 0 else "bkwd"): ftle_error(mixed_ftle[d], ftle64[d]) for d in w["dirs"]}}}
+        m["api"].finalize()
+        del m
     if args.precision == "mixed" and w["kind"] == "abc" and args.acc_n > 0 and rank == 0:
-        # FTLE error of the mixed form against the plain FP64 path (itself parity-tested against
-        # the FP64 oracle) on the same flow and options at a smaller grid, full T
+        # FTLE error of the mixed form against the plain FP64 path on the same flow and options
+        # at a smaller grid, full T
         from libcfd2lcs_b200 import accuracy as A
-        api.finalize()
         acc = A.compare(args.acc_n, w["T"], w["h"], w["dt"], None, w["integrator"], w["interpolator"])
         line["ftle_error"] = {"form": "mixed (FP32 velocity data, FP64 positions / flow maps / FTLE)",
                               "vs": "plain FP64 GPU path", "case": acc["config"],
@@ -471,7 +549,6 @@ def run_b200(args, w):
             rate1, _, sample1, _ = cpu_sample(w, 1, threads=1, n=48 if w["kind"] == "abc" else 64)
             line["cpu_baseline"]["single_thread"] = {"value": rate1, "unit": UNIT, "cores": 1, "sample": sample1}
         print(json.dumps(line), flush=True)
-    api.finalize()
     if world > 1:
         torch.distributed.destroy_process_group()
 
@@ -719,7 +796,10 @@ def main():
     ap.add_argument("--workload", default="abc256", choices=sorted(WORKLOADS) + ["batch64", "adj128"])
     ap.add_argument("--fd-dirs", type=int, default=16, help="adj128: finite-difference directions")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--acc-n", type=int, default=64, help="grid of the mixed-vs-FP64 FTLE error run (0: skip)")
+    ap.add_argument("--acc-n", type=int, default=64, help="--precision mixed: grid of its FTLE error run (0: skip)")
+    ap.add_argument("--mixed", default="auto", choices=["auto", "on", "off"],
+                    help="also time the mixed form and state its FTLE error against this run's FP64 path over the full horizon "
+                         "(auto: the ABC workloads on one GPU)")
     ap.add_argument("--n", type=int, default=None, help="override the grid size (smaller smoke runs)")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()

@@ -88,6 +88,11 @@ void cfd2lcs_get_phase_times_c(double t[7]);
  * n[0], n[1] the number of launches timed. */
 void cfd2lcs_get_kernel_times_c(double t[2], long long n[2]);
 
+/* Launches of the B-spline subcycle kernels that stage their coefficient taps in shared
+ * memory (the cubic interpolator on 3-D grids), cumulative: n[0] backward semi-Lagrangian,
+ * n[1] forward particle.  The rest of those launches gathered their taps from global memory. */
+void cfd2lcs_get_staged_launches_c(long long n[2]);
+
 /* Recomputes the latest FTLE frame of a diagnostic -- the composition of its stored
  * sub-flow maps and the FTLE -- into device buffers the caller owns, and allocates no memory
  * while doing so.  No counterpart in the reference: it exists for callers that cannot call
@@ -98,9 +103,14 @@ void cfd2lcs_get_kernel_times_c(double t[2], long long n[2]);
  *   cfd2lcs_get_flowmap_c of that frame when the options are unchanged since.
  * The table of sub-flow-map pointers lives in a fixed device array (256 sub-flow maps, i.e.
  * T/h <= 256; larger frames are rejected with an error).  The first call on a device looks
- * up that array's address; make this first call before any stream capture.  All calls share
- * the array, so calls that overlap on the GPU race.  Returns 0 on success, 1 on error (the
- * error is latched as for every other call). */
+ * up that array's address.  The call copies the table from host memory and waits for its
+ * own work, so it must not be made while a stream capture is active.  All calls share the
+ * array, so calls that overlap on the GPU (from several host threads) race.
+ * Ordering: the library writes d_ftle and d_fm on its own stream, which does not wait for
+ * work the caller queued on other streams -- finish that work on both buffers before the
+ * call.  The results are complete when the call returns.  The current CUDA device must be
+ * the one cfd2lcs_init ran on.  Diagnostics with resolution /= 0 or AUX_GRID are rejected.
+ * Returns 0 on success, 1 on error (the error is latched as for every other call). */
 int cfd2lcs_reconstruct_noalloc_c(int lcs_handle, lcsdata_t *d_ftle, lcsdata_t *d_fm);
 
 /* ---------------------------------------------------------------------------------------

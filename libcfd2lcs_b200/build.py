@@ -19,7 +19,7 @@ BUILD = os.environ.get("CFD2LCS_B200_BUILDDIR") or os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["engine.cu", "adjoint.cu", "probe.cu", "grid.cpp", "spline_host.cpp", "writer.cpp", "capi.cpp"]
-HEADERS = ["grid.h", "engine.h", "adjoint.h", "device_common.cuh", "advect.cuh", "spline.cuh", "kernels.cuh", "spline_host.h", "writer.h"]
+HEADERS = ["grid.h", "engine.h", "adjoint.h", "device_common.cuh", "advect.cuh", "spline.cuh", "kernels.cuh", "tile.cuh", "spline_host.h", "writer.h"]
 
 
 def lib_path(prec: str) -> str:

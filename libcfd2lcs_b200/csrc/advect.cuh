@@ -182,7 +182,6 @@ __device__ __forceinline__ void sample_velocity(const DevGrid<T> &g, const Splin
   } else if (INTERP == INTERP_LINEAR) {
     LinStencil<T> st;
     lin_stencil(g, x, no, st);
-#pragma unroll
     if (V.cs[stage][0]) {  // the stage's blend, written once per subcycle on large grids
 #pragma unroll
       for (int c = 0; c < 3; c++) out[c] = T(lin_apply_tv<T, TV>(st, V.cs[stage][c]));

@@ -414,6 +414,15 @@ CFD2LCS_EXPORT void cfd2lcs_get_kernel_times_c(double t[2], long long n[2]) {
   n[1] = k.fwd_kernel_launches;
 }
 
+// Launches of the kernels that stage their spline taps in shared memory: n[0] backward
+// semi-Lagrangian subcycles, n[1] forward particle subcycles (cumulative).
+CFD2LCS_EXPORT void cfd2lcs_get_staged_launches_c(long long n[2]) {
+  Library &lib = L();
+  const Counters &k = lib.eng ? lib.eng->counters() : lib.zero;
+  n[0] = k.sl_staged_launches;
+  n[1] = k.fwd_staged_launches;
+}
+
 // Host-only formatting hook (no device work): the Fortran ESw.d editing the output files use,
 // for checking the writer on machines without a GPU.  out receives w characters and a NUL.
 CFD2LCS_EXPORT void cfd2lcs_b200_format_es(double v, int w, int d, char *out) {

@@ -15,6 +15,7 @@ enum : int {
   ERR_TRACKING = 2,
   ERR_UNKNOWN_FLAG = 4,
   ERR_SPLINE_RANGE = 8,
+  ERR_ASYNC_COPY = 16,  // a shared-memory staging copy did not complete within its wait limit
 };
 
 enum { EULER_ = 0, TRAPEZOIDAL_ = 1, RK2_ = 2, RK3_ = 3, RK4_ = 4 };

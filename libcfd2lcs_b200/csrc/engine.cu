@@ -8,9 +8,11 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <mutex>
 
 #include "grid.h"
 #include "kernels.cuh"
+#include "tile.cuh"
 #include "spline_host.h"
 #include "writer.h"
 
@@ -41,10 +43,12 @@ class DevArena {
     for (void *p : ptrs_) cudaFree(p);
     ptrs_.clear();
   }
+  // Every buffer gets 256 bytes of slack past its end: the staged-tile kernels copy rows in
+  // whole 16-byte units, so the copy of an array's last row may read up to 15 bytes past it.
   template <typename X>
   X *alloc(size_t n, std::string &msg) {
     void *p = nullptr;
-    cudaError_t e = cudaMalloc(&p, n * sizeof(X) > 0 ? n * sizeof(X) : 1);
+    cudaError_t e = cudaMalloc(&p, n * sizeof(X) + 256);
     if (e != cudaSuccess) {
       msg = std::string("device allocation failed: ") + cudaGetErrorString(e);
       return nullptr;
@@ -138,19 +142,25 @@ struct Diag {
 #define NOALLOC_MAX_SUBMAPS 256
 static __device__ __align__(256) const void *g_noalloc_submap_table[3 * NOALLOC_MAX_SUBMAPS];
 
-// Device address of the table on the current device, looked up once per device (host code
-// must not pass the symbol itself to a kernel: on the host it is only a stand-in).
-static bool noalloc_table_address(void **out, std::string &msg) {
+// Device address of the table on device dev, looked up once per device with that device
+// current (host code must not pass the symbol itself to a kernel: on the host it is only a
+// stand-in).  The cache is filled under a lock, so first calls from several host threads do
+// not race on it; the caller's current device is restored afterwards.
+static bool noalloc_table_address(int dev, void **out, std::string &msg) {
+  static std::mutex lock;
   static void *addr[64] = {nullptr};
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= 64) {
-    msg = std::string("reconstruct_noalloc: no current CUDA device: ") + cudaGetErrorString(e);
+  if (dev < 0 || dev >= 64) {
+    msg = "reconstruct_noalloc: device index out of range";
     return false;
   }
+  std::lock_guard<std::mutex> guard(lock);
   if (!addr[dev]) {
+    int cur = -1;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e == cudaSuccess && cur != dev) e = cudaSetDevice(dev);
     void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_submap_table);
+    if (e == cudaSuccess) e = cudaGetSymbolAddress(&p, g_noalloc_submap_table);
+    if (cur >= 0 && cur != dev) cudaSetDevice(cur);
     if (e != cudaSuccess || !p) {
       msg = std::string("reconstruct_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e);
       return false;
@@ -223,6 +233,7 @@ class Engine : public EngineBase {
       msg = hg_.error;
       return false;
     }
+    CK(cudaGetDevice(&dev_));  // the device this engine's stream and buffers live on
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     for (int e = 0; e < 10; e++) {
       cudaEvent_t ev;
@@ -231,6 +242,7 @@ class Engine : public EngineBase {
     }
     CK(cudaMallocHost(&red_host_, sizeof(DevReduce)));
     if (const char *e = std::getenv("CFD2LCS_B200_LINEAR_BLEND_MIN")) lin_blend_min_ = std::atol(e);
+    if (const char *e = std::getenv("CFD2LCS_B200_SL_TILE")) sl_tile_ = std::atoi(e) != 0;
     for (int a = 0; a < 3; a++) n_[a] = n[a];
     // coordinate lines and interior flags for the output files (the grid is a tensor product)
     for (int a = 0; a < 3; a++)
@@ -692,8 +704,15 @@ class Engine : public EngineBase {
       }
       for (int c = 0; c < 3; c++) host_table[3 * q + c] = spline ? d->slotcoef[3 * s + c] : d->slot[3 * s + c];
     }
+    int cur = -1;
+    CK(cudaGetDevice(&cur));
+    if (cur != dev_) {
+      msg = "reconstruct_noalloc: the current CUDA device (" + std::to_string(cur) + ") is not the device cfd2lcs_init ran on (" +
+            std::to_string(dev_) + ")";
+      return false;
+    }
     void *table = nullptr;
-    if (!noalloc_table_address(&table, msg)) return false;
+    if (!noalloc_table_address(dev_, &table, msg)) return false;
     if (m > 0) CK(cudaMemcpyAsync(table, host_table, sizeof(T *) * 3 * m, cudaMemcpyHostToDevice, stream_));
     const SplineAxes<T> sa = spline ? splines_[deg].axes : SplineAxes<T>{};
     const int iv = interp_variant(interp, sa);
@@ -916,6 +935,7 @@ class Engine : public EngineBase {
     if (red_err_ & ERR_NONFINITE_VELOCITY) msg = "update: non-finite velocity (CFL number is not finite)";
     else if (red_err_ & ERR_TRACKING) msg = "ERROR: cannot locate all particles (node search did not converge)";
     else if (red_err_ & ERR_UNKNOWN_FLAG) msg = "ERROR: Unknown bcflag";
+    else if (red_err_ & ERR_ASYNC_COPY) msg = "device error: a shared-memory staging copy did not complete";
     else msg = "device error";
     return false;
   }
@@ -1479,8 +1499,47 @@ class Engine : public EngineBase {
 
   dim3 node_grid() const { return dim3((n_[0] + 31) / 32, (n_[1] + 7) / 8, n_[2]); }
 
+  // The cubic backward subcycle with its taps staged in shared memory (k_sl_tile) replaces the
+  // gathering kernel unless CFD2LCS_B200_SL_TILE=0 at cfd2lcs_init (kept for A/B comparison).
+  bool sl_tile_ = true;
+  int dev_ = 0;  // CUDA device current at cfd2lcs_init
+
+  template <int IG, bool F>
+  void launch_sl_tile(const SplineAxes<T> &sa, const VelFields<TV> &V, FieldPtrs<T> fo, FieldPtrsW<T> fn, StageTimes S, T dt) {
+    const size_t smem = slt_field_bytes<T>();
+    cudaFuncSetAttribute(k_sl_tile<T, TV, IG, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const dim3 blk(32, SLT_Y, 2), grd((n_[0] + SLT_X - 1) / SLT_X, (n_[1] + SLT_Y - 1) / SLT_Y, (n_[2] + SLT_Z - 1) / SLT_Z);
+    k_sl_tile<T, TV, IG, F><<<grd, blk, smem, stream_>>>(dg_, sa, V, fo, fn, S, dt, &red_->err);
+  }
+
+  // the bulk copies need 16-byte aligned sources (cudaMalloc gives 256)
+  bool sl_tile_usable(const VelFields<TV> &V, FieldPtrs<T> fo) const {
+    if (!sl_tile_) return false;
+    const int noff = opt_->integrator == 2 ? 1 : (opt_->integrator == 3 ? 2 : (opt_->integrator == 4 ? 3 : 0));
+    for (int c = 0; c < 3; c++) {
+      if (reinterpret_cast<uintptr_t>(fo.f[c]) % 16) return false;
+      for (int s = 1; s <= noff; s++)
+        if (!V.cs[s][c] || reinterpret_cast<uintptr_t>(V.cs[s][c]) % 16) return false;
+    }
+    return true;
+  }
+
   template <int INTERP, bool F>
   void sl_integ(const SplineAxes<T> &sa, const VelFields<TV> &V, FieldPtrs<T> fo, FieldPtrsW<T> fn, StageTimes S, T dt) {
+    if constexpr (INTERP == INTERP_SPLINE4) {
+      if (sl_tile_usable(V, fo)) {
+        counters_.kernel_launches++;
+        counters_.sl_staged_launches++;
+        switch (opt_->integrator) {
+          case 0: launch_sl_tile<EULER_, F>(sa, V, fo, fn, S, dt); break;
+          case 1: launch_sl_tile<TRAPEZOIDAL_, F>(sa, V, fo, fn, S, dt); break;
+          case 2: launch_sl_tile<RK2_, F>(sa, V, fo, fn, S, dt); break;
+          case 3: launch_sl_tile<RK3_, F>(sa, V, fo, fn, S, dt); break;
+          default: launch_sl_tile<RK4_, F>(sa, V, fo, fn, S, dt); break;
+        }
+        return;
+      }
+    }
     // blocks of 32 x 8/bz x bz nodes: spanning z layers lets a block's warps share the corners
     // of the layers between them in L1.  Measured on B200 (bz = 1 / 2 / 4): FP64 velocity, ABC
     // 256^3 CUBIC 4.30 / 4.12 / 4.10 ms and turbulence 512^3 LINEAR 7.84 / 7.64 / 7.50 ms per

@@ -43,6 +43,8 @@ struct Counters {
   // event-timed hot kernels: backward SL subcycle and forward particle subcycle
   double sl_kernel_ms = 0, fwd_kernel_ms = 0;
   long long sl_kernel_launches = 0, fwd_kernel_launches = 0;
+  // launches of the kernels that stage their spline taps in shared memory (backward, forward)
+  long long sl_staged_launches = 0, fwd_staged_launches = 0;
   // ingest, bkwd advect, fwd advect, snapshot, compose, ftle, whole update (event span)
   double phase_ms[7] = {0, 0, 0, 0, 0, 0, 0};
 };

@@ -47,6 +47,7 @@ struct SplineAxes {
 template <typename T>
 struct SplineStencil {
   int p0;      // padded index of the first coefficient
+  int c0[3];   // padded index of the first coefficient along each axis
   T b[3][4];   // basis values per axis (only the first k used)
 };
 
@@ -142,6 +143,7 @@ __device__ __forceinline__ bool spline_stencil(const DevGrid<T> &g, const Spline
     }
     basis_values<T, KC, UNI>(A, l, x[a], st.b[a]);
     c0[a] = l - k;  // padded index of coefficient l-k+1 (1-based)
+    st.c0[a] = c0[a];
   }
   st.p0 = pidx(g.P.sx, g.P.sxy, c0[0], c0[1], c0[2]);
   return true;
@@ -149,10 +151,11 @@ __device__ __forceinline__ bool spline_stencil(const DevGrid<T> &g, const Spline
 
 // Tensor contraction of the k x k x k coefficients around the stencil, x then y then z.
 // TC is the coefficient type: the mixed-precision form contracts FP32 velocity coefficients
-// with the basis values rounded to FP32.
-template <typename T, int KC, typename TC = T>
-__device__ __forceinline__ TC spline_apply(const DevGrid<T> &g, const SplineAxes<T> &S, const SplineStencil<T> &st,
-                                           const TC *__restrict__ coef) {
+// with the basis values rounded to FP32.  tap(c1, c2, c0) returns coefficient (c0, c1, c2)
+// of the stencil: from global memory (spline_apply) or from a tile staged in shared memory
+// (the tiled backward kernel) -- one FMA sequence for both, so both give the same bits.
+template <typename T, int KC, typename TC, typename Tap>
+__device__ __forceinline__ TC spline_contract(const SplineAxes<T> &S, const SplineStencil<T> &st, Tap tap) {
   const int kx = KC ? KC : S.ax[0].k, ky = KC ? KC : S.ax[1].k, kz = KC ? KC : S.ax[2].k;
   TC vz = TC(0);
 #pragma unroll
@@ -162,18 +165,24 @@ __device__ __forceinline__ TC spline_apply(const DevGrid<T> &g, const SplineAxes
 #pragma unroll
     for (int c1 = 0; c1 < 4; c1++) {
       if (c1 >= ky) break;
-      const TC *row = coef + st.p0 + c1 * g.P.sx + c2 * g.P.sxy;
       TC vx = TC(0);
 #pragma unroll
       for (int c0 = 0; c0 < 4; c0++) {
         if (c0 >= kx) break;
-        vx += TC(st.b[0][c0]) * __ldg(row + c0);
+        vx += TC(st.b[0][c0]) * tap(c1, c2, c0);
       }
       vy += TC(st.b[1][c1]) * vx;
     }
     vz += TC(st.b[2][c2]) * vy;
   }
   return vz;
+}
+
+template <typename T, int KC, typename TC = T>
+__device__ __forceinline__ TC spline_apply(const DevGrid<T> &g, const SplineAxes<T> &S, const SplineStencil<T> &st,
+                                           const TC *__restrict__ coef) {
+  const int sx = g.P.sx, sxy = g.P.sxy, p0 = st.p0;
+  return spline_contract<T, KC, TC>(S, st, [&](int c1, int c2, int c0) { return __ldg(coef + p0 + c1 * sx + c2 * sxy + c0); });
 }
 
 // ---------------------------------------------------------------------------------------

@@ -1,0 +1,70 @@
+"""The cubic backward subcycle with its spline taps staged in shared memory (k_sl_tile) against
+the gathering kernel it replaces (k_sl_subcycle, selected with CFD2LCS_B200_SL_TILE=0 at
+cfd2lcs_init): both contract the same taps in the same order, so flow maps and FTLE must be
+bitwise equal.  Grids of 38^3 leave partial tiles in x (38 = 32 + 6), y and z (38 = 9 x 4 + 2);
+the small walled / mixed-boundary cases clip the staged box at the padded array's edges.
+The oracle parity of the same path is in test_gpu_parity.py and test_golden_configs.py."""
+import os
+
+import numpy as np
+import pytest
+
+from tests import scenarios as SC
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gpu_dp():
+    import libcfd2lcs_b200 as L
+    return L.Cfd2lcs("dp")
+
+
+@pytest.fixture(scope="module")
+def gpu_sp():
+    import libcfd2lcs_b200 as L
+    return L.Cfd2lcs("sp")
+
+
+def _run(gpu, case, integrator, staged, n=None, steps=None, mixed=False, dirs=(SC.FTLE_BKWD,)):
+    os.environ["CFD2LCS_B200_SL_TILE"] = "1" if staged else "0"
+    try:
+        gpu.reset()
+        if mixed:
+            gpu.set_option("MIXED_PRECISION", 1)
+        _, hs = SC.run(gpu, case, dirs, integrator, 3, n=n, steps=steps)
+    finally:
+        os.environ.pop("CFD2LCS_B200_SL_TILE", None)
+    err, msg = gpu.error()
+    assert err == 0, msg
+    return [gpu.flowmap(h) for h in hs], [gpu.ftle(h) for h in hs], gpu.counters(), gpu.staged_launches()
+
+
+def _same(gpu, case, integrator, **kw):
+    fa, ta, ca, sa = _run(gpu, case, integrator, True, **kw)
+    fb, tb, cb, sb = _run(gpu, case, integrator, False, **kw)
+    assert sa["sl"] > 0, "the staged kernel did not run"
+    assert sb["sl"] == 0
+    assert ca["integrations_bkwd"] == cb["integrations_bkwd"] and ca["ftle_frames"] == cb["ftle_frames"]
+    for x, y in zip(fa, fb):
+        assert np.array_equal(x, y), f"flow maps differ: max {np.max(np.abs(x - y)):.3e}"
+    for x, y in zip(ta, tb):
+        assert np.array_equal(x, y), f"FTLE differs: max {np.max(np.abs(x - y)):.3e}"
+
+
+@pytest.mark.parametrize("integrator", [0, 2, 3, 4])
+def test_staged_abc_partial_tiles(gpu_dp, integrator):
+    _same(gpu_dp, "abc", integrator, n=38, steps=14)
+
+
+def test_staged_abc_unsteady_mixed_precision(gpu_dp):
+    _same(gpu_dp, "abc_unsteady", 3, n=38, mixed=True)
+
+
+@pytest.mark.parametrize("case", ["mixed_bc", "turb"])
+def test_staged_small_and_walled(gpu_dp, case):
+    _same(gpu_dp, case, 3)
+
+
+def test_staged_single_precision(gpu_sp):
+    _same(gpu_sp, "abc", 3, n=38, steps=14)
