@@ -152,11 +152,38 @@ def turbulence_on_device(n, t, dev, chunk=16):
     return out
 
 
+HBM_FALLBACK_GBS = 6650.0  # an earlier copy-bandwidth measurement on this B200 pool, used when no measured file exists
+
+
 def measured_peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         return {}
+
+
+def fp64_fma_tflops(iters: int = 16384, reps: int = 5) -> float:
+    """The device's FP64 FMA rate (TFLOP/s) from the bench-only micro-benchmark library
+    (libcfd2lcs_b200_fp64probe.so: eight independent FMA chains per thread, eight 256-thread
+    blocks per SM, best of `reps` launches)."""
+    import ctypes
+    from libcfd2lcs_b200.build import build_probe
+    lib = ctypes.CDLL(build_probe())
+    lib.cfd2lcs_b200_fp64_fma_rate.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    lib.cfd2lcs_b200_fp64_fma_rate.restype = ctypes.c_int
+    out = np.zeros(1, dtype=np.float64)
+    rc = lib.cfd2lcs_b200_fp64_fma_rate(int(iters), int(reps), out.ctypes.data_as(ctypes.c_void_p))
+    if rc != 0:
+        raise RuntimeError(f"fp64 FMA probe failed (CUDA error {rc})")
+    return float(out[0])
+
+
+def hbm_peak():
+    """(GB/s, source): the measured copy bandwidth of MEASURED_PEAKS.json, else the fallback."""
+    v = measured_peaks().get("hbm_gbs")
+    if v:
+        return float(v), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return HBM_FALLBACK_GBS, "fallback (no MEASURED_PEAKS.json on this box): 6650 GB/s"
 
 
 class ClockSampler:
@@ -410,18 +437,29 @@ def run_form(args, w, precision, local, world, rank, clocks=False, e2e=False, ho
                       "d2h_bytes_per_step": len(handles) * N * 8}
         nxt = total + 1 + args.steps
     if horizon is not None:
-        fields.clear()
-        for s in range(nxt, horizon + 1):
+        if not steady:
+            fields.clear()
+        for s in range(nxt, horizon):
             step(s)
+        # the update that ends the horizon: its frames compose every ring slot
+        torch.cuda.synchronize()
+        ph0, cf0 = api.phase_times_ms(), api.counters()
+        step(horizon)
+        torch.cuda.synchronize()
+        ph1, cf1 = api.phase_times_ms(), api.counters()
         err, msg = api.error()
         if err:
             raise RuntimeError(msg)
+        nfr = cf1["ftle_frames"] - cf0["ftle_frames"]
+        if nfr > 0:
+            out["full_frame"] = {"frames": nfr, "slots_composed_per_frame": (cf1["slots_composed"] - cf0["slots_composed"]) / nfr,
+                                 **{k: (ph1[k] - ph0[k]) / nfr for k in ("snapshot", "compose", "ftle")}}
         out["ftle"] = {d: np.array(api.ftle(h), copy=True) for d, h in zip(w["dirs"], handles)}
         out["horizon_t"] = w["t0"] + horizon * w["dt"]
     return out
 
 
-def hot_kernel_rooflines(r, w, precision, hbm, fp64_peak):
+def hot_kernel_rooflines(r, w, precision, hbm, fp64_peak, hbm_src=None):
     """Roofline of the two hot kernels from one form's timed region: algorithmic bytes per
     launch over the CUDA-event launch time, against the measured HBM copy bandwidth."""
     N = r["N"]
@@ -441,7 +479,7 @@ def hot_kernel_rooflines(r, w, precision, hbm, fp64_peak):
         avg_s = tot_ms / nl / 1000.0
         achieved = N * bpp / avg_s / 1e9
         rooflines[name] = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                           "frac": achieved / hbm if hbm else None, "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)",
+                           "frac": achieved / hbm if hbm else None, "peak_source": hbm_src,
                            "avg_launch_ms": avg_s * 1000.0, "share_of_step": tot_ms / r["ms"] if r["ms"] else None,
                            "algorithmic_bytes_per_point": bpp, "algorithmic_bytes_per_launch": N * bpp, "traffic": None}
         tpp = MEASURED_TRAFFIC.get((name, precision, w["interpolator"], w["integrator"]))
@@ -453,25 +491,34 @@ def hot_kernel_rooflines(r, w, precision, hbm, fp64_peak):
             tf = N * fpp / avg_s / 1e12
             rooflines[name]["fp64"] = {"achieved": tf, "peak": fp64_peak, "unit": "TFLOP/s", "frac": tf / fp64_peak,
                                        "flops_per_point": fpp,
-                                       "peak_source": "FMA micro-benchmark (cfd2lcs_b200_fp64_fma_rate), this run"}
+                                       "peak_source": "FMA micro-benchmark (libcfd2lcs_b200_fp64probe.so), this run"}
     return rooflines
 
 
-def ftle_field_roofline(r, w, hbm):
-    """FTLE-field time per frame (ring snapshot + composition + FTLE, event-timed over every
-    frame so far) against its HBM bound: per point nslot sub-map reads (3 FP64 each), the
-    composed map (3) and the FTLE (1) -- (nslot*24 + 24 + 8) bytes."""
-    p1, c1 = r["p1"], r["c1"]
-    frames = c1["ftle_frames"]
-    if not frames:
-        return None
-    ms = (p1["snapshot"] + p1["compose"] + p1["ftle"]) / frames
+def ftle_field_roofline(r, w, hbm, hbm_src=None):
+    """FTLE-field time per frame (ring snapshot + composition + FTLE, CUDA events on the
+    library's stream) against its HBM bound: per point nslot sub-map reads (3 FP64 each), the
+    composed map (3) and the FTLE (1) -- (nslot*24 + 24 + 8) bytes.  Measured at the frame that
+    ends the full horizon (every ring slot composed) when the run reached it, else averaged
+    over the frames seen so far (rings still filling)."""
     nslot = int(round(w["T"] / w["h"]))
-    byts = r["N"] * (nslot * 24 + 24 + 8)
+    ff = r.get("full_frame")
+    if ff:
+        ms, parts, frames, where = ff["snapshot"] + ff["compose"] + ff["ftle"], ff, ff["frames"], "full-horizon frame"
+        slots = ff["slots_composed_per_frame"]
+    else:
+        p1, c1 = r["p1"], r["c1"]
+        frames = c1["ftle_frames"]
+        if not frames:
+            return None
+        parts = {k: p1[k] / frames for k in ("snapshot", "compose", "ftle")}
+        ms, where, slots = sum(parts.values()), "average over the frames so far (rings filling)", c1["slots_composed"] / frames
+    byts = r["N"] * (slots * 24 + 24 + 8)
     ach = byts / (ms / 1000.0) / 1e9
-    return {"ms_per_frame": ms, "snapshot_ms": p1["snapshot"] / frames, "compose_ms": p1["compose"] / frames,
-            "ftle_ms": p1["ftle"] / frames, "frames": frames, "algorithmic_bytes": byts, "bound_ms": byts / (hbm * 1e9) * 1e3 if hbm else None,
-            "achieved_gbs": ach, "frac": ach / hbm if hbm else None}
+    return {"ms_per_frame": ms, "snapshot_ms": parts["snapshot"], "compose_ms": parts["compose"], "ftle_ms": parts["ftle"],
+            "frames": frames, "slots_composed_per_frame": slots, "measured_at": where, "nslot": nslot, "algorithmic_bytes": byts,
+            "bound_ms": byts / (hbm * 1e9) * 1e3 if hbm else None, "achieved_gbs": ach, "frac": ach / hbm if hbm else None,
+            "peak_source": hbm_src}
 
 
 def run_b200(args, w):
@@ -490,14 +537,13 @@ def run_b200(args, w):
     horizon = full_frame_update(w) if with_mixed else None
     r = run_form(args, w, args.precision, local, world, rank, clocks=True, e2e=True, horizon=horizon)
     api = r["api"]
-    peaks = measured_peaks()
-    fp64_peak = api.fp64_fma_tflops() if w["interpolator"] in (2, 3) and args.precision == "fp64" else None
-    hbm = peaks.get("hbm_gbs")
-    rooflines = hot_kernel_rooflines(r, w, args.precision, hbm, fp64_peak)
+    fp64_peak = fp64_fma_tflops() if w["interpolator"] in (2, 3) and args.precision == "fp64" else None
+    hbm, hbm_src = hbm_peak()
+    rooflines = hot_kernel_rooflines(r, w, args.precision, hbm, fp64_peak, hbm_src)
     roof = max(rooflines.values(), key=lambda x: x["share_of_step"] or 0) if rooflines else None
     c1, p0, p1 = r["c1"], r["p0"], r["p1"]
     frames = c1["ftle_frames"]
-    ffr = ftle_field_roofline(r, w, hbm)
+    ffr = ftle_field_roofline(r, w, hbm, hbm_src)
     g = r["g"]
     line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": r["ms_max"] / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -521,12 +567,12 @@ def run_b200(args, w):
     if with_mixed:
         m = run_form(args, w, "mixed", local, world, rank, horizon=horizon)
         mixed_ftle = m["ftle"]
-        mroof = hot_kernel_rooflines(m, w, "mixed", hbm, None)
+        mroof = hot_kernel_rooflines(m, w, "mixed", hbm, None, hbm_src)
         line["mixed"] = {
             "form": "mixed: FP32 velocity levels, spline coefficients and stage blends; FP64 positions, flow maps, "
                     "composition, Cauchy-Green and eigen-solve",
             "value": m["value"], "unit": UNIT, "ms_per_step": m["ms_max"] / args.steps, "ratio_vs_fp64": m["value"] / line["value"],
-            "ftle_field_ms": (ftle_field_roofline(m, w, hbm) or {}).get("ms_per_frame"), "rooflines": mroof,
+            "ftle_field": ftle_field_roofline(m, w, hbm, hbm_src), "rooflines": mroof,
             "phase_ms_per_step": {k: (m["p1"][k] - m["p0"][k]) / args.steps for k in m["p1"]},
             "ftle_error": {"vs": "plain FP64 GPU path of this run (itself parity-tested against the FP64 oracle)",
                            "grid": list(g.n), "updates": horizon, "frame_t": m["horizon_t"],

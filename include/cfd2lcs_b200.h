@@ -180,11 +180,6 @@ int cfd2lcs_tangent_ftle_c(const int n[3], const lcsdata_t *x, const lcsdata_t *
                            const lcsdata_t *const *d_du, const lcsdata_t *const *d_dv, const lcsdata_t *const *d_dw, double *J,
                            double *dJ, char *msg, size_t len);
 
-/* Measurement hook (no library state): the current device's FP64 FMA rate in TFLOP/s, measured
- * by the library's own kernel (eight independent FMA chains per thread, eight 256-thread blocks
- * per SM), best of `reps` launches of `iters` iterations.  The ceiling against which the
- * B-spline advection kernels' FP64 arithmetic is reported.  Returns 0, or a CUDA error code. */
-int cfd2lcs_b200_fp64_fma_rate(int iters, int reps, double *tflops);
 
 #ifdef __cplusplus
 }

@@ -46,7 +46,6 @@ EXPORTED_SYMBOLS = [
     # adjoint (include/cfd2lcs_b200.h)
     "cfd2lcs_adjoint_ftle_c", "cfd2lcs_tangent_ftle_c",
     # measurement hook (include/cfd2lcs_b200.h)
-    "cfd2lcs_b200_fp64_fma_rate",
 ]
 
 
@@ -111,8 +110,6 @@ def load(precision: str = "dp") -> C.CDLL:
     lib.cfd2lcs_reconstruct_noalloc_c.restype = C.c_int
     lib.cfd2lcs_b200_grid_tables.argtypes = [P, P, P, P, P, P, P, P, P, P, C.c_char_p, C.c_size_t]
     lib.cfd2lcs_b200_grid_tables.restype = C.c_int
-    lib.cfd2lcs_b200_fp64_fma_rate.argtypes = [C.c_int, C.c_int, P]
-    lib.cfd2lcs_b200_fp64_fma_rate.restype = C.c_int
     lib.cfd2lcs_batch_add_c.argtypes = [P, P, P, P, P, C.c_int, C.c_int, R, C.c_int]
     lib.cfd2lcs_batch_add_c.restype = C.c_int
     lib.cfd2lcs_batch_diagnostic_init_c.argtypes = [C.c_int, C.c_int, R, R]
@@ -250,14 +247,6 @@ class Cfd2lcs:
         keys = ["integrations_fwd", "integrations_bkwd", "nsub_fwd", "nsub_bkwd", "ftle_frames", "updates", "kernel_launches",
                 "slots_composed"]
         return {k: int(v) for k, v in zip(keys, a)}
-
-    def fp64_fma_tflops(self, iters: int = 16384, reps: int = 5) -> float:
-        """The device's FP64 FMA rate (TFLOP/s) from the library's own micro-benchmark kernel."""
-        out = np.zeros(1, dtype=np.float64)
-        rc = self.lib.cfd2lcs_b200_fp64_fma_rate(int(iters), int(reps), self._p(out))
-        if rc != 0:
-            raise RuntimeError(f"fp64 FMA probe failed (CUDA error {rc})")
-        return float(out[0])
 
     def phase_times_ms(self) -> dict:
         a = np.zeros(7, dtype=np.float64)

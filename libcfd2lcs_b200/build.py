@@ -18,12 +18,31 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.environ.get("CFD2LCS_B200_BUILDDIR") or os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["engine.cu", "adjoint.cu", "probe.cu", "grid.cpp", "spline_host.cpp", "writer.cpp", "capi.cpp"]
-HEADERS = ["grid.h", "engine.h", "adjoint.h", "device_common.cuh", "advect.cuh", "spline.cuh", "kernels.cuh", "tile.cuh", "spline_host.h", "writer.h"]
+SOURCES = ["engine.cu", "engine_mixed.cu", "adjoint.cu", "grid.cpp", "spline_host.cpp", "writer.cpp", "capi.cpp"]
+# the FP64 FMA micro-benchmark bench.py reports the B-spline kernels against: a separate
+# measurement library, not part of the drop-in
+PROBE_SOURCE = "probe.cu"
+HEADERS = ["grid.h", "engine.h", "engine_impl.cuh", "adjoint.h", "device_common.cuh", "advect.cuh", "spline.cuh", "kernels.cuh", "tile.cuh", "eig3.h", "spline_host.h", "writer.h"]
 
 
 def lib_path(prec: str) -> str:
     return os.path.join(os.environ.get("CFD2LCS_B200_LIBDIR") or HERE, f"libcfd2lcs_b200_{prec}.so")
+
+
+def probe_path() -> str:
+    return os.path.join(os.environ.get("CFD2LCS_B200_LIBDIR") or HERE, "libcfd2lcs_b200_fp64probe.so")
+
+
+def build_probe(force: bool = False) -> str:
+    """The bench-only FP64 FMA micro-benchmark library (one source file)."""
+    out, src = probe_path(), os.path.join(CSRC, PROBE_SOURCE)
+    if not force and os.path.exists(out) and os.path.getmtime(out) >= os.path.getmtime(src):
+        return out
+    cmd = [NVCC, "-shared", src, "-o", out, "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden"] + ARCH
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {PROBE_SOURCE}:\n{r.stdout}\n{r.stderr}")
+    return out
 
 
 def _flags(prec: str):
@@ -80,3 +99,4 @@ def build(precisions=("dp", "sp"), force: bool = False, verbose: bool = False) -
 if __name__ == "__main__":
     precs = tuple(a for a in sys.argv[1:] if a in ("dp", "sp")) or ("dp", "sp")
     print(build(precs, force="--force" in sys.argv, verbose=True))
+    print(build_probe(force="--force" in sys.argv))

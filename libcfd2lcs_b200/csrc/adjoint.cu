@@ -374,7 +374,7 @@ __device__ __forceinline__ bool ftle_linearise(const DevGrid<T> &g, const FieldP
   double C[3][3];
   for (int a = 0; a < 3; a++)
     for (int b = 0; b < 3; b++) C[a][b] = L.G[0][a] * L.G[0][b] + L.G[1][a] * L.G[1][b] + L.G[2][a] * L.G[2][b];
-  const double lam = eig3_max(C[0][0], C[0][1], C[0][2], C[1][1], C[1][2], C[2][2]);
+  const double lam = eig3_max_closed(C[0][0], C[0][1], C[0][2], C[1][1], C[1][2], C[2][2]);
   const double tiny = sizeof(T) == 8 ? DBL_MIN : (double)FLT_MIN;
   if (!(sqrt(lam) > tiny)) return false;  // max(sqrt(W3), tiny) is constant there
   // unit eigenvector of lam: the largest cross product of two rows of C - lam I

@@ -27,6 +27,8 @@ template <typename T>
 struct LinStencil {
   int p0;         // padded index of the lower corner
   int s[3];       // padded stride of the upper corner along each axis (0 if clamped onto p0)
+  int i0[3];      // padded index of the lower corner along each axis
+  int d[3];       // 1 where the upper corner differs from the lower one, else 0
   T w[8];
 };
 
@@ -54,6 +56,8 @@ __device__ __forceinline__ void lin_stencil(const DevGrid<T> &g, const T x[3], c
     t[a] = clamp01((x[a] - x0) / (x1 - x0));
     mt[a] = T(1) - t[a];
     i0[a] = lo;
+    st.i0[a] = lo;
+    st.d[a] = hi - lo;
     st.s[a] = (hi - lo) * str[a];
   }
   st.p0 = pidx(g.P.sx, g.P.sxy, i0[0], i0[1], i0[2]);
@@ -67,43 +71,54 @@ __device__ __forceinline__ void lin_stencil(const DevGrid<T> &g, const T x[3], c
   st.w[7] = t[0] * t[1] * t[2];
 }
 
+// Corner c of the stencil (bit 0: x, bit 1: y, bit 2: z upper corner) as a padded index; the
+// contractions below take the corner values through a loader, so the gathering kernels and the
+// shared-memory tile kernels run one expression (and get the same bits).
 template <typename T>
-__device__ __forceinline__ T lin_apply(const LinStencil<T> &st, const T *__restrict__ f) {
-  const int p = st.p0;
-  const T f0 = __ldg(f + p), f1 = __ldg(f + p + st.s[0]), f2 = __ldg(f + p + st.s[1]), f3 = __ldg(f + p + st.s[0] + st.s[1]);
-  const T f4 = __ldg(f + p + st.s[2]), f5 = __ldg(f + p + st.s[0] + st.s[2]), f6 = __ldg(f + p + st.s[1] + st.s[2]),
-          f7 = __ldg(f + p + st.s[0] + st.s[1] + st.s[2]);
-  return st.w[0] * f0 + st.w[1] * f1 + st.w[2] * f2 + st.w[3] * f3 + st.w[4] * f4 + st.w[5] * f5 + st.w[6] * f6 + st.w[7] * f7;
+__device__ __forceinline__ int lin_corner(const LinStencil<T> &st, int c) {
+  return st.p0 + ((c & 1) ? st.s[0] : 0) + ((c & 2) ? st.s[1] : 0) + ((c & 4) ? st.s[2] : 0);
 }
 
-// time-blended field u = (1-ct) u_n + ct u_np1 sampled at the corners, then trilinear; TV is
-// the velocity storage type (FP32 in the mixed-precision form, weights rounded to it)
-template <typename T, typename TV>
-__device__ __forceinline__ TV lin_apply_blend(const LinStencil<T> &st, const TV *__restrict__ a, const TV *__restrict__ b, TV omc,
-                                              TV ct) {
-  const int p = st.p0;
-  const int q[8] = {p, p + st.s[0], p + st.s[1], p + st.s[0] + st.s[1], p + st.s[2], p + st.s[0] + st.s[2], p + st.s[1] + st.s[2],
-                    p + st.s[0] + st.s[1] + st.s[2]};
+template <typename T, typename V>
+__device__ __forceinline__ T lin_contract(const LinStencil<T> &st, V v) {
+  return st.w[0] * v(0) + st.w[1] * v(1) + st.w[2] * v(2) + st.w[3] * v(3) + st.w[4] * v(4) + st.w[5] * v(5) + st.w[6] * v(6) +
+         st.w[7] * v(7);
+}
+
+template <typename T>
+__device__ __forceinline__ T lin_apply(const LinStencil<T> &st, const T *__restrict__ f) {
+  return lin_contract<T>(st, [&](int c) { return __ldg(f + lin_corner(st, c)); });
+}
+
+// time-blended field u = (1-ct) u_n + ct u_np1 at the corners, then trilinear; TV is the
+// velocity storage type (FP32 in the mixed-precision form, weights rounded to it).  va(c), vb(c)
+// return corner c of u_n and u_np1.
+template <typename T, typename TV, typename VA, typename VB>
+__device__ __forceinline__ TV lin_blend_contract(const LinStencil<T> &st, TV omc, TV ct, VA va, VB vb) {
   TV acc = TV(0);
 #pragma unroll
   for (int c = 0; c < 8; c++) {
-    const TV v = omc * __ldg(a + q[c]) + ct * __ldg(b + q[c]);
+    const TV v = omc * va(c) + ct * vb(c);
     acc = c == 0 ? TV(st.w[0]) * v : acc + TV(st.w[c]) * v;
   }
   return acc;
+}
+
+template <typename T, typename TV>
+__device__ __forceinline__ TV lin_apply_blend(const LinStencil<T> &st, const TV *__restrict__ a, const TV *__restrict__ b, TV omc,
+                                              TV ct) {
+  return lin_blend_contract<T, TV>(st, omc, ct, [&](int c) { return __ldg(a + lin_corner(st, c)); },
+                                   [&](int c) { return __ldg(b + lin_corner(st, c)); });
 }
 
 // a stage's time blend written beforehand (k_blend), sampled trilinearly with the same weights
 // and accumulation as lin_apply_blend
 template <typename T, typename TV>
 __device__ __forceinline__ TV lin_apply_tv(const LinStencil<T> &st, const TV *__restrict__ f) {
-  const int p = st.p0;
-  const int q[8] = {p, p + st.s[0], p + st.s[1], p + st.s[0] + st.s[1], p + st.s[2], p + st.s[0] + st.s[2], p + st.s[1] + st.s[2],
-                    p + st.s[0] + st.s[1] + st.s[2]};
   TV acc = TV(0);
 #pragma unroll
   for (int c = 0; c < 8; c++) {
-    const TV v = __ldg(f + q[c]);
+    const TV v = __ldg(f + lin_corner(st, c));
     acc = c == 0 ? TV(st.w[0]) * v : acc + TV(st.w[c]) * v;
   }
   return acc;

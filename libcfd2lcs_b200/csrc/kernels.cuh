@@ -5,6 +5,7 @@
 #include <cfloat>
 
 #include "advect.cuh"
+#include "eig3.h"
 
 namespace cfd2lcs {
 
@@ -465,39 +466,9 @@ __global__ void __launch_bounds__(256) k_compose(DevGrid<T> g, SplineAxes<T> sa,
 // K5  FTLE (compute_ftle, src/lcs_m.f90:66-193 with grad_sr1, src/gradient_m.f90:11-66):
 // central differences of the composed displacement map (face ghosts: periodic image, or
 // the flow-map ghost rule), right Cauchy-Green tensor of the displacement gradient in
-// FP64, largest eigenvalue by cyclic Jacobi, ftle = log(max(sqrt(lam), tiny))/T.
+// FP64, largest eigenvalue in closed form (eig3.h; the reference calls LAPACK DSYEV),
+// ftle = log(max(sqrt(lam), tiny))/T.
 // ---------------------------------------------------------------------------------------
-__device__ __forceinline__ double eig3_max(double a00, double a01, double a02, double a11, double a12, double a22) {
-  double a[3][3] = {{a00, a01, a02}, {a01, a11, a12}, {a02, a12, a22}};
-  for (int sweep = 0; sweep < 32; sweep++) {
-    const double off = fabs(a[0][1]) + fabs(a[0][2]) + fabs(a[1][2]);
-    const double diag = fabs(a[0][0]) + fabs(a[1][1]) + fabs(a[2][2]);
-    if (off == 0.0 || off <= 1e-18 * diag) break;
-#pragma unroll
-    for (int pq = 0; pq < 3; pq++) {
-      const int pp = pq == 2 ? 1 : 0, qq = pq == 0 ? 1 : 2;
-      const double apq = a[pp][qq];
-      if (apq == 0.0) continue;
-      const double theta = (a[qq][qq] - a[pp][pp]) / (2.0 * apq);
-      const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-      const double c = rsqrt(t * t + 1.0), s = t * c;
-#pragma unroll
-      for (int r = 0; r < 3; r++) {
-        const double arp = a[r][pp], arq = a[r][qq];
-        a[r][pp] = c * arp - s * arq;
-        a[r][qq] = s * arp + c * arq;
-      }
-#pragma unroll
-      for (int r = 0; r < 3; r++) {
-        const double apr = a[pp][r], aqr = a[qq][r];
-        a[pp][r] = c * apr - s * aqr;
-        a[qq][r] = s * apr + c * aqr;
-      }
-    }
-  }
-  return fmax(fmax(a[0][0], a[1][1]), a[2][2]);
-}
-
 template <typename T, typename R, bool HAS_FLAGS>
 __device__ __forceinline__ T fm_neighbour(const DevGrid<T> &g, const T *__restrict__ f, int a, int i, int j, int k, int step) {
   int idx[3] = {i, j, k};
@@ -540,7 +511,7 @@ __global__ void __launch_bounds__(256) k_ftle(DevGrid<T> g, FieldPtrs<T> fm, R *
   for (int a = 0; a < 3; a++)
 #pragma unroll
     for (int b = 0; b < 3; b++) C[a][b] = G[0][a] * G[0][b] + G[1][a] * G[1][b] + G[2][a] * G[2][b];
-  const double lam = eig3_max(C[0][0], C[0][1], C[0][2], C[1][1], C[1][2], C[2][2]);
+  const double lam = eig3_max_closed(C[0][0], C[0][1], C[0][2], C[1][1], C[1][2], C[2][2]);
   const R sq = sqrt((R)lam);
   const R tiny = sizeof(R) == 8 ? (R)DBL_MIN : (R)FLT_MIN;
   const R mx = sq > tiny ? sq : tiny;  // max(sqrt(W3), tiny): NaN yields tiny
@@ -579,7 +550,7 @@ __global__ void __launch_bounds__(256) k_ftle_aux(DevGrid<T> g, const __grid_con
   for (int a = 0; a < 3; a++)
 #pragma unroll
     for (int b = 0; b < 3; b++) C[a][b] = G[0][a] * G[0][b] + G[1][a] * G[1][b] + G[2][a] * G[2][b];
-  const double lam = eig3_max(C[0][0], C[0][1], C[0][2], C[1][1], C[1][2], C[2][2]);
+  const double lam = eig3_max_closed(C[0][0], C[0][1], C[0][2], C[1][1], C[1][2], C[2][2]);
   const R sq = sqrt((R)lam);
   const R tiny = sizeof(R) == 8 ? (R)DBL_MIN : (R)FLT_MIN;
   const R mx = sq > tiny ? sq : tiny;
@@ -749,21 +720,37 @@ __global__ void k_reset_particles(DevGrid<T> g, Particles<T> P) {
 // ---------------------------------------------------------------------------------------
 constexpr int SORT_TILE = 2048;  // 256 threads x 8 counts
 
-// key space of the cell order: cells c_a in 0..n_a per axis, padded to whole tiles
+// Cell tiles of the order: tx x ty x tz cells (tx ty tz = 256), x fastest inside a tile and
+// tiles in x, y, z order; cells c_a in 0..n_a per axis, padded to whole tiles.  The gathering
+// forward kernel takes 32 x 4 x 2 (32 x 8/SORT_TZ x SORT_TZ; measured on B200, see the engine),
+// the staged forward kernel 16 x 4 x 4 (its shared-memory box is that tile widened by 4 cells).
 #ifndef CFD2LCS_SORT_TZ
 #define CFD2LCS_SORT_TZ 2
 #endif
-constexpr int SORT_TZ = CFD2LCS_SORT_TZ, SORT_TY = 8 / SORT_TZ;  // cell tiles of 32 x SORT_TY x SORT_TZ
+constexpr int SORT_TZ = CFD2LCS_SORT_TZ, SORT_TY = 8 / SORT_TZ;
 
-__host__ __device__ inline long sort_key_space(const int n[3]) {
-  const long ntx = (n[0] + 1 + 31) / 32, nty = (n[1] + 1 + SORT_TY - 1) / SORT_TY, ntz = (n[2] + 1 + SORT_TZ - 1) / SORT_TZ;
-  return ntz * nty * ntx * 256;
+struct SortTiles {
+  int tx, ty, tz;     // cells per tile along each axis
+  int ntx, nty, ntz;  // tiles along each axis
+};
+
+__host__ __device__ inline SortTiles sort_tiles(const int n[3], int tx, int ty, int tz) {
+  SortTiles s;
+  s.tx = tx;
+  s.ty = ty;
+  s.tz = tz;
+  s.ntx = (n[0] + 1 + tx - 1) / tx;
+  s.nty = (n[1] + 1 + ty - 1) / ty;
+  s.ntz = (n[2] + 1 + tz - 1) / tz;
+  return s;
 }
+
+__host__ __device__ inline long sort_key_space(const SortTiles &s) { return (long)s.ntz * s.nty * s.ntx * 256; }
 
 // cell c in 0..n along each axis: the tracked node (clamped to the interior), minus one when
 // the particle lies below the node's line
 template <typename T>
-__global__ void __launch_bounds__(256) k_particle_count(DevGrid<T> g, Particles<T> P, unsigned *key, int *cnt, int np) {
+__global__ void __launch_bounds__(256) k_particle_count(DevGrid<T> g, Particles<T> P, unsigned *key, int *cnt, int np, SortTiles st) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= np) return;
   int c[3];
@@ -772,11 +759,19 @@ __global__ void __launch_bounds__(256) k_particle_count(DevGrid<T> g, Particles<
     const int v = min(max(P.no[a][s], 1), g.P.n[a]);
     c[a] = v - (P.x[a][s] < __ldg(g.lt[a] + v) ? 1 : 0);
   }
-  const int ntx = (g.P.n[0] + 1 + 31) / 32, nty = (g.P.n[1] + 1 + SORT_TY - 1) / SORT_TY;
-  const unsigned tile = (unsigned)(((c[2] / SORT_TZ) * nty + c[1] / SORT_TY) * ntx + (c[0] >> 5));
-  const unsigned kq = tile * 256u + (unsigned)(((c[2] % SORT_TZ) * SORT_TY + c[1] % SORT_TY) * 32 + (c[0] & 31));
+  const unsigned tile = (unsigned)(((c[2] / st.tz) * st.nty + c[1] / st.ty) * st.ntx + c[0] / st.tx);
+  const unsigned kq = tile * 256u + (unsigned)(((c[2] % st.tz) * st.ty + c[1] % st.ty) * st.tx + c[0] % st.tx);
   key[s] = kq;
   atomicAdd(cnt + kq, 1);
+}
+
+// First slot of sort tile t after k_particle_scatter, which leaves offs[k] at the end of key k's
+// slots within its SORT_TILE chunk and tsum[c] at the chunk's first slot; t = the number of
+// tiles gives np.
+__device__ __forceinline__ int sort_tile_start(const int *offs, const int *tsum, long t, long ntiles, int np) {
+  if (t >= ntiles) return np;
+  const long k0 = t * 256;
+  return __ldg(tsum + k0 / SORT_TILE) + ((k0 % SORT_TILE) ? __ldg(offs + k0 - 1) : 0);
 }
 
 // exclusive scan of cnt within each chunk into offs (cnt reset to 0), chunk totals to tsum

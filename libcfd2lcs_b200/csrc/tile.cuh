@@ -72,29 +72,25 @@ __device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, unsign
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // ---------------------------------------------------------------------------------------
-// Tile geometry
+// Staged boxes: a block of TX x TY x TZ nodes copies the box of its nodes widened by HALO on
+// every side, one row (x line) per bulk copy.  A row copy starts at the 16-byte boundary at or
+// below its first element, so a row in shared memory is preceded by up to 16/sizeof - 1
+// extra elements (its alignment shift, (xlo + y sx + z sxy) mod 16/sizeof).
 // ---------------------------------------------------------------------------------------
-constexpr int SLT_X = 32, SLT_Y = 4, SLT_Z = 4;  // nodes per block (block of 32 x 4 x 2 threads, 2 nodes each)
-constexpr int SLT_HALO = 2;
-constexpr int SLT_SX = SLT_X + 2 * SLT_HALO, SLT_SY = SLT_Y + 2 * SLT_HALO, SLT_SZ = SLT_Z + 2 * SLT_HALO;
-constexpr int SLT_ROWS = SLT_SY * SLT_SZ;  // rows of the box per component
-constexpr int SLT_THREADS = 256;
-
-// Row pitch (elements) of the box in shared memory: a row copy starts at the 16-byte boundary
-// at or below its first element, so a row holds up to 16/sizeof - 1 leading extra elements.
-template <typename TC>
-__host__ __device__ constexpr int slt_pitch() {
-  return ((SLT_SX + 2 * (16 / (int)sizeof(TC) - 1)) / (16 / (int)sizeof(TC))) * (16 / (int)sizeof(TC));
-}
-template <typename TC>
-__host__ __device__ constexpr int slt_comp() {
-  return SLT_ROWS * slt_pitch<TC>();
-}
-// shared memory of one staged field (3 components); the flow map's type is the widest
-template <typename TC>
-__host__ __device__ constexpr size_t slt_field_bytes() {
-  return (size_t)3 * slt_comp<TC>() * sizeof(TC);
-}
+template <int TX_, int TY_, int TZ_, int HALO_>
+struct TileGeom {
+  static constexpr int TX = TX_, TY = TY_, TZ = TZ_, HALO = HALO_;
+  static constexpr int SX = TX + 2 * HALO, SY = TY + 2 * HALO, SZ = TZ + 2 * HALO;
+  static constexpr int ROWS = SY * SZ;  // rows of the box per component
+  template <typename TC>
+  __host__ __device__ static constexpr int pitch() {
+    return ((SX + 2 * (16 / (int)sizeof(TC) - 1)) / (16 / (int)sizeof(TC))) * (16 / (int)sizeof(TC));
+  }
+  template <typename TC>
+  __host__ __device__ static constexpr int comp() {  // elements of one component
+    return ROWS * pitch<TC>();
+  }
+};
 
 // The staged box of a block: origin (padded indices, may lie outside the array) and the part
 // inside the padded array, [lo, hi) per axis.
@@ -103,25 +99,70 @@ struct TileBox {
   int xlo, xhi, ylo, yhi, zlo, zhi;
 };
 
-// Issues the row copies of one 3-component field into buf; threads 0..3*SLT_ROWS-1 each
-// arrive once on bar (with the bytes of their row, or none for a row outside the array).
-template <typename TC>
-__device__ __forceinline__ void slt_fill(TC *buf, const TC *f0, const TC *f1, const TC *f2, const TileBox &b, int sx, int sxy,
-                                         uint64_t *bar, int tid) {
+template <typename G, typename T>
+__device__ __forceinline__ TileBox tile_box(const DevGrid<T> &g) {
+  TileBox b;
+  b.xs = 1 + (int)blockIdx.x * G::TX - G::HALO;
+  b.ys = 1 + (int)blockIdx.y * G::TY - G::HALO;
+  b.zs = 1 + (int)blockIdx.z * G::TZ - G::HALO;
+  b.xlo = max(b.xs, 0);
+  b.xhi = min(b.xs + G::SX, g.P.sx);
+  b.ylo = max(b.ys, 0);
+  b.yhi = min(b.ys + G::SY, g.P.n[1] + 2);
+  b.zlo = max(b.zs, 0);
+  b.zhi = min(b.zs + G::SZ, g.P.n[2] + 2);
+  return b;
+}
+
+// Issues the row copies of a 3-component field into buf (component c at buf + c * comp): the
+// 3 * ROWS copies are dealt over the block's threads, each arriving once per copy on bar (with
+// the row's bytes, or none for a row outside the padded array), so bar expects 3 * ROWS
+// arrivals per field.
+template <typename G, typename TC>
+__device__ __forceinline__ void tile_fill(TC *buf, const TC *f0, const TC *f1, const TC *f2, const TileBox &b, int sx, int sxy,
+                                          uint64_t *bar, int tid, int nthreads) {
   constexpr int E = 16 / (int)sizeof(TC);
-  if (tid >= 3 * SLT_ROWS) return;
-  const int c = tid / SLT_ROWS, r = tid - c * SLT_ROWS;
-  const TC *const src = c == 0 ? f0 : (c == 1 ? f1 : f2);
-  const int y = b.ys + r % SLT_SY, z = b.zs + r / SLT_SY;
-  if (y >= b.ylo && y < b.yhi && z >= b.zlo && z < b.zhi && b.xhi > b.xlo) {
-    const long e = (long)b.xlo + (long)y * sx + (long)z * sxy;
-    const long a = e & ~(long)(E - 1);
-    const unsigned bytes = (unsigned)((((e - a) + (b.xhi - b.xlo)) * (long)sizeof(TC) + 15) & ~15L);
-    mbar_arrive_expect_tx(bar, bytes);
-    bulk_copy_g2s(buf + (size_t)c * slt_comp<TC>() + (size_t)r * slt_pitch<TC>(), src + a, bytes, bar);
-  } else {
-    mbar_arrive(bar);
+  for (int task = tid; task < 3 * G::ROWS; task += nthreads) {
+    const int c = task / G::ROWS, r = task - c * G::ROWS;
+    const TC *const src = c == 0 ? f0 : (c == 1 ? f1 : f2);
+    const int y = b.ys + r % G::SY, z = b.zs + r / G::SY;
+    if (y >= b.ylo && y < b.yhi && z >= b.zlo && z < b.zhi && b.xhi > b.xlo) {
+      const long e = (long)b.xlo + (long)y * sx + (long)z * sxy;
+      const long a = e & ~(long)(E - 1);
+      const unsigned bytes = (unsigned)((((e - a) + (b.xhi - b.xlo)) * (long)sizeof(TC) + 15) & ~15L);
+      mbar_arrive_expect_tx(bar, bytes);
+      bulk_copy_g2s(buf + (size_t)c * G::template comp<TC>() + (size_t)r * G::template pitch<TC>(), src + a, bytes, bar);
+    } else {
+      mbar_arrive(bar);
+    }
   }
+}
+
+// shared-memory index of padded element (x, y, z) of a staged component
+template <typename G, typename TC>
+__device__ __forceinline__ int tile_index(const TileBox &b, int sx, int sxy, int x, int y, int z) {
+  constexpr int E = 16 / (int)sizeof(TC);
+  return ((z - b.zs) * G::SY + (y - b.ys)) * G::template pitch<TC>() + ((b.xlo + y * sx + z * sxy) & (E - 1)) + (x - b.xlo);
+}
+
+// ---------------------------------------------------------------------------------------
+// Cubic tile geometry: 32 x 4 x 4 nodes (block of 32 x 4 x 2 threads, 2 nodes each), halo 2
+// ---------------------------------------------------------------------------------------
+using CubicGeom = TileGeom<32, 4, 4, 2>;
+constexpr int SLT_X = CubicGeom::TX, SLT_Y = CubicGeom::TY, SLT_Z = CubicGeom::TZ;
+constexpr int SLT_THREADS = 256;
+template <typename TC>
+__host__ __device__ constexpr int slt_pitch() {
+  return CubicGeom::pitch<TC>();
+}
+template <typename TC>
+__host__ __device__ constexpr int slt_comp() {
+  return CubicGeom::comp<TC>();
+}
+// shared memory of one staged field (3 components); the flow map's type is the widest
+template <typename TC>
+__host__ __device__ constexpr size_t slt_field_bytes() {
+  return (size_t)3 * slt_comp<TC>() * sizeof(TC);
 }
 
 // true when the stencil's 4 x 4 x 4 coefficients are all in the staged box
@@ -129,18 +170,102 @@ __device__ __forceinline__ bool slt_inside(const TileBox &b, const int c0[3]) {
   return c0[0] >= b.xlo && c0[0] + 4 <= b.xhi && c0[1] >= b.ylo && c0[1] + 4 <= b.yhi && c0[2] >= b.zlo && c0[2] + 4 <= b.zhi;
 }
 
-// One component from the staged box: coefficient (x, y, z) sits in row (z-zs)*SLT_SY + (y-ys)
-// at column x - xlo plus the row's alignment shift ((xlo + y sx + z sxy) mod 16/sizeof).
+// One component from the staged box of geometry G: coefficient (x, y, z) sits in row
+// (z-zs)*SY + (y-ys) at column x - xlo plus the row's alignment shift
+// ((xlo + y sx + z sxy) mod 16/sizeof).
+template <typename G, typename T, typename TC>
+__device__ __forceinline__ TC tile_apply(const SplineAxes<T> &sa, const SplineStencil<T> &st, const TC *comp, const TileBox &b, int sx,
+                                         int sxy) {
+  constexpr int E = 16 / (int)sizeof(TC);
+  const int gy = st.c0[1] * sx + st.c0[2] * sxy + b.xlo;  // global offset of row (c0y, c0z) at column xlo
+  const int rb = ((st.c0[2] - b.zs) * G::SY + (st.c0[1] - b.ys)) * G::template pitch<TC>() + (st.c0[0] - b.xlo);
+  return spline_contract<T, 4, TC>(sa, st, [&](int c1, int c2, int c0) {
+    const int shift = (gy + c1 * sx + c2 * sxy) & (E - 1);
+    return comp[rb + (c2 * G::SY + c1) * G::template pitch<TC>() + shift + c0];
+  });
+}
+
 template <typename T, typename TC>
 __device__ __forceinline__ TC slt_apply(const SplineAxes<T> &sa, const SplineStencil<T> &st, const TC *comp, const TileBox &b, int sx,
                                         int sxy) {
+  return tile_apply<CubicGeom, T, TC>(sa, st, comp, b, sx, sxy);
+}
+
+// Two vertical neighbours whose stencils share the x and y intervals and sit one z row apart
+// (B.c0 = A.c0 + (0, 0, 1), the common case: neighbouring nodes move alike): one pass over the
+// 5 z rows they span reads each shared tap once (80 shared-memory loads instead of 2 x 64)
+// and accumulates both points in spline_contract's order (c2, c1, c0 increasing), so each
+// result has the bits of its own contraction.
+template <typename T, typename TC>
+__device__ __forceinline__ void slt_apply_pair(const SplineStencil<T> &A, const SplineStencil<T> &B, const TC *comp, const TileBox &b,
+                                               int sx, int sxy, TC &oa, TC &ob) {
   constexpr int E = 16 / (int)sizeof(TC);
-  const int gy = st.c0[1] * sx + st.c0[2] * sxy + b.xlo;  // global offset of row (c0y, c0z) at column xlo
-  const int rb = ((st.c0[2] - b.zs) * SLT_SY + (st.c0[1] - b.ys)) * slt_pitch<TC>() + (st.c0[0] - b.xlo);
-  return spline_contract<T, 4, TC>(sa, st, [&](int c1, int c2, int c0) {
-    const int shift = (gy + c1 * sx + c2 * sxy) & (E - 1);
-    return comp[rb + (c2 * SLT_SY + c1) * slt_pitch<TC>() + shift + c0];
-  });
+  const int gy = A.c0[1] * sx + A.c0[2] * sxy + b.xlo;
+  const int rb = ((A.c0[2] - b.zs) * CubicGeom::SY + (A.c0[1] - b.ys)) * slt_pitch<TC>() + (A.c0[0] - b.xlo);
+  TC vza = TC(0), vzb = TC(0);
+#pragma unroll
+  for (int c2 = 0; c2 < 5; c2++) {
+    TC vya = TC(0), vyb = TC(0);
+#pragma unroll
+    for (int c1 = 0; c1 < 4; c1++) {
+      const int shift = (gy + c1 * sx + c2 * sxy) & (E - 1);
+      const TC *row = comp + rb + (c2 * CubicGeom::SY + c1) * slt_pitch<TC>() + shift;
+      TC vxa = TC(0), vxb = TC(0);
+#pragma unroll
+      for (int c0 = 0; c0 < 4; c0++) {
+        const TC tap = row[c0];
+        if (c2 < 4) vxa += TC(A.b[0][c0]) * tap;
+        if (c2 > 0) vxb += TC(B.b[0][c0]) * tap;
+      }
+      if (c2 < 4) vya += TC(A.b[1][c1]) * vxa;
+      if (c2 > 0) vyb += TC(B.b[1][c1]) * vxb;
+    }
+    if (c2 < 4) vza += TC(A.b[2][c2]) * vya;
+    if (c2 > 0) vzb += TC(B.b[2][c2 - 1]) * vyb;
+  }
+  oa = vza;
+  ob = vzb;
+}
+
+// A 3-component field (staged box `box`, global arrays g0..g2) at the thread's two points
+// x[q] around nodes (i, j, kq[q]): the pair pass where it applies, else each point from the box
+// or, when its stencil leaves the box, from global memory; 0 where db3val returns 0.
+template <typename T, typename TC, bool UNI>
+__device__ __forceinline__ void slt_sample2(const DevGrid<T> &g, const SplineAxes<T> &sa, const TileBox &b, const TC *box, const TC *g0,
+                                            const TC *g1, const TC *g2, const bool ok[2], const T x[2][3], int i, int j,
+                                            const int kq[2], T out[2][3]) {
+  const int sx = g.P.sx, sxy = g.P.sxy;
+  SplineStencil<T> st[2];
+  bool in[2], inbox[2];
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    const int no[3] = {i, j, kq[q]};
+    in[q] = ok[q] && spline_stencil<T, 4, UNI>(g, sa, x[q], no, st[q]);
+    inbox[q] = in[q] && slt_inside(b, st[q].c0);
+    if (!in[q]) out[q][0] = out[q][1] = out[q][2] = T(0);
+  }
+  if (inbox[0] && inbox[1] && st[0].c0[0] == st[1].c0[0] && st[0].c0[1] == st[1].c0[1] && st[1].c0[2] == st[0].c0[2] + 1) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      TC a, bb;
+      slt_apply_pair<T, TC>(st[0], st[1], box + (size_t)c * slt_comp<TC>(), b, sx, sxy, a, bb);
+      out[0][c] = T(a);
+      out[1][c] = T(bb);
+    }
+    return;
+  }
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    if (!in[q]) continue;
+    if (inbox[q]) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) out[q][c] = T(slt_apply<T, TC>(sa, st[q], box + (size_t)c * slt_comp<TC>(), b, sx, sxy));
+    } else {
+      out[q][0] = T(spline_apply<T, 4, TC>(g, sa, st[q], g0));
+      out[q][1] = T(spline_apply<T, 4, TC>(g, sa, st[q], g1));
+      out[q][2] = T(spline_apply<T, 4, TC>(g, sa, st[q], g2));
+    }
+  }
 }
 
 #ifndef CFD2LCS_SLT_MINB
@@ -157,27 +282,18 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLT_MINB)
   const T HALF = T(1) / T(2), THIRD = T(1) / T(3), TWOTHIRD = T(2) / T(3), SIXTH = T(1) / T(6), TWO = T(2);
   const int tid = threadIdx.x + 32 * (threadIdx.y + SLT_Y * threadIdx.z);
   const int sx = g.P.sx, sxy = g.P.sxy;
-  TileBox b;
+  const TileBox b = tile_box<CubicGeom>(g);
   const int I0 = 1 + (int)blockIdx.x * SLT_X, J0 = 1 + (int)blockIdx.y * SLT_Y, K0 = 1 + (int)blockIdx.z * SLT_Z;
-  b.xs = I0 - SLT_HALO;
-  b.ys = J0 - SLT_HALO;
-  b.zs = K0 - SLT_HALO;
-  b.xlo = max(b.xs, 0);
-  b.xhi = min(b.xs + SLT_SX, sx);
-  b.ylo = max(b.ys, 0);
-  b.yhi = min(b.ys + SLT_SY, g.P.n[1] + 2);
-  b.zlo = max(b.zs, 0);
-  b.zhi = min(b.zs + SLT_SZ, g.P.n[2] + 2);
   TV *const tv = reinterpret_cast<TV *>(slt_smem);
   T *const tf = reinterpret_cast<T *>(slt_smem);
-  if (tid == 0) mbar_init(&bar, 3 * SLT_ROWS);
+  if (tid == 0) mbar_init(&bar, 3 * CubicGeom::ROWS);
   __syncthreads();
-  if (NOFF > 0) slt_fill<TV>(tv, V.cs[1][0], V.cs[1][1], V.cs[1][2], b, sx, sxy, &bar, tid);
-  else slt_fill<T>(tf, fmo.f[0], fmo.f[1], fmo.f[2], b, sx, sxy, &bar, tid);
+  if (NOFF > 0) tile_fill<CubicGeom, TV>(tv, V.cs[1][0], V.cs[1][1], V.cs[1][2], b, sx, sxy, &bar, tid, SLT_THREADS);
+  else tile_fill<CubicGeom, T>(tf, fmo.f[0], fmo.f[1], fmo.f[2], b, sx, sxy, &bar, tid, SLT_THREADS);
 
-  // the thread's two nodes: (i, j, k) and (i, j, k + 2)
+  // the thread's two nodes: vertical neighbours (i, j, k) and (i, j, k + 1)
   const int i = I0 + (int)threadIdx.x, j = J0 + (int)threadIdx.y;
-  int kq[2] = {K0 + (int)threadIdx.z, K0 + (int)threadIdx.z + 2};
+  const int kq[2] = {K0 + 2 * (int)threadIdx.z, K0 + 2 * (int)threadIdx.z + 1};
   bool ok[2];
   T xn[2][3], xs[2][3], acc[2][3];
 #pragma unroll
@@ -211,21 +327,12 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLT_MINB)
     if (alive) alive = __syncthreads_and(mbar_wait_bounded(&bar, parity));
     if (!alive) continue;
     parity ^= 1u;
+    T us[2][3];
+    slt_sample2<T, TV, UNI>(g, sa, b, tv, V.cs[s][0], V.cs[s][1], V.cs[s][2], ok, xs, i, j, kq, us);
 #pragma unroll
     for (int q = 0; q < 2; q++) {
       if (!ok[q]) continue;
-      const int no[3] = {i, j, kq[q]};
-      T u[3];
-      SplineStencil<T> st;
-      if (!spline_stencil<T, 4, UNI>(g, sa, xs[q], no, st)) {
-        u[0] = u[1] = u[2] = T(0);
-      } else if (slt_inside(b, st.c0)) {
-#pragma unroll
-        for (int c = 0; c < 3; c++) u[c] = T(slt_apply<T, TV>(sa, st, tv + (size_t)c * slt_comp<TV>(), b, sx, sxy));
-      } else {
-#pragma unroll
-        for (int c = 0; c < 3; c++) u[c] = T(spline_apply<T, 4, TV>(g, sa, st, V.cs[s][c]));
-      }
+      const T *u = us[q];
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         const T k = dt * u[c];
@@ -253,8 +360,8 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLT_MINB)
     }
     __syncthreads();  // every thread is done reading the box
     fence_proxy_async_smem();
-    if (s < NOFF) slt_fill<TV>(tv, V.cs[s + 1][0], V.cs[s + 1][1], V.cs[s + 1][2], b, sx, sxy, &bar, tid);
-    else slt_fill<T>(tf, fmo.f[0], fmo.f[1], fmo.f[2], b, sx, sxy, &bar, tid);
+    if (s < NOFF) tile_fill<CubicGeom, TV>(tv, V.cs[s + 1][0], V.cs[s + 1][1], V.cs[s + 1][2], b, sx, sxy, &bar, tid, SLT_THREADS);
+    else tile_fill<CubicGeom, T>(tf, fmo.f[0], fmo.f[1], fmo.f[2], b, sx, sxy, &bar, tid, SLT_THREADS);
   }
   if (alive) {
     // departure points (xs now holds x): 2-D projection, particle BC, stick
@@ -276,23 +383,14 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLT_MINB)
     mbar_wait_bounded(&bar, parity);
     return;
   }
+  T fms[2][3];
+  slt_sample2<T, T, UNI>(g, sa, b, tf, fmo.f[0], fmo.f[1], fmo.f[2], ok, xs, i, j, kq, fms);
 #pragma unroll
   for (int q = 0; q < 2; q++) {
     if (!ok[q]) continue;
     const int k = kq[q];
     const int p = pidx(sx, sxy, i, j, k);
-    const int nod[3] = {i, j, k};
-    T fmp[3];
-    SplineStencil<T> st;
-    if (!spline_stencil<T, 4, UNI>(g, sa, xs[q], nod, st)) {
-      fmp[0] = fmp[1] = fmp[2] = T(0);
-    } else if (slt_inside(b, st.c0)) {
-#pragma unroll
-      for (int c = 0; c < 3; c++) fmp[c] = slt_apply<T, T>(sa, st, tf + (size_t)c * slt_comp<T>(), b, sx, sxy);
-    } else {
-#pragma unroll
-      for (int c = 0; c < 3; c++) fmp[c] = spline_apply<T, 4>(g, sa, st, fmo.f[c]);
-    }
+    const T *fmp = fms[q];
     const int fl = HAS_FLAGS ? (int)g.flag[p] : (int)LCS_INTERNAL;
     const T mask = fl != LCS_MASK ? T(1) : T(0);
     const bool zero = HAS_FLAGS && (fl == LCS_MASK || fl == LCS_INFLOW || fl == LCS_OUTFLOW);
@@ -304,6 +402,365 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLT_MINB)
       fmn.f[c][p] = vfin[c];
     }
     write_ghosts<T, HAS_FLAGS, GHOST_FM>(g, fmn.f, i, j, k, vpre, vfin, err);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// LINEAR backward subcycle from a staged box (interp_s2u_r1 LINEAR, src/lp_tracking_m.f90:
+// 342-474, inside update_flowmap_sl): the bracket of every stage and of the departure point
+// is [no-1, no] or [no, no+1] around the node (clamped t), so a block of 32 x 4 x 4 nodes reads
+// only the box of its nodes widened by 1 -- for both velocity levels and the previous flow map.
+// The block copies the nine component boxes with one mbarrier phase, then every point runs
+// from shared memory with the expressions of k_sl_subcycle (lin_blend_contract, lin_contract),
+// so the results are bitwise equal.  The gathering kernel is latency-bound (three dependent
+// gather phases per point); here the only global reads are the bulk copies.
+// ---------------------------------------------------------------------------------------
+using LinGeom = TileGeom<32, 4, 4, 1>;
+
+// shared memory of the LINEAR tile: u_n, u_np1 (velocity type) and the flow map (3 each)
+template <typename T, typename TV>
+__host__ __device__ constexpr size_t sll_bytes() {
+  return (size_t)6 * LinGeom::comp<TV>() * sizeof(TV) + (size_t)3 * LinGeom::comp<T>() * sizeof(T);
+}
+
+#ifndef CFD2LCS_SLL_MINB
+#define CFD2LCS_SLL_MINB 2
+#endif
+
+template <typename T, typename TV, int INTEG, bool HAS_FLAGS>
+__global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLL_MINB)
+    k_sl_tile_lin(DevGrid<T> g, VelFields<TV> V, FieldPtrs<T> fmo, FieldPtrsW<T> fmn, StageTimes S, T dt, int *err) {
+  extern __shared__ __align__(128) unsigned char sll_smem[];
+  __shared__ __align__(8) uint64_t bar;
+  constexpr int NOFF = INTEG == RK2_ ? 1 : (INTEG == RK3_ ? 2 : (INTEG == RK4_ ? 3 : 0));
+  const T HALF = T(1) / T(2), THIRD = T(1) / T(3), TWOTHIRD = T(2) / T(3), SIXTH = T(1) / T(6), TWO = T(2);
+  const int tid = threadIdx.x + 32 * (threadIdx.y + LinGeom::TY * threadIdx.z);
+  const int sx = g.P.sx, sxy = g.P.sxy;
+  const TileBox b = tile_box<LinGeom>(g);
+  TV *const su0 = reinterpret_cast<TV *>(sll_smem);
+  TV *const su1 = su0 + 3 * LinGeom::comp<TV>();
+  T *const sf = reinterpret_cast<T *>(sll_smem + (size_t)6 * LinGeom::comp<TV>() * sizeof(TV));
+  if (tid == 0) mbar_init(&bar, 9 * LinGeom::ROWS);
+  __syncthreads();
+  tile_fill<LinGeom, TV>(su0, V.un[0], V.un[1], V.un[2], b, sx, sxy, &bar, tid, SLT_THREADS);
+  tile_fill<LinGeom, TV>(su1, V.unp1[0], V.unp1[1], V.unp1[2], b, sx, sxy, &bar, tid, SLT_THREADS);
+  tile_fill<LinGeom, T>(sf, fmo.f[0], fmo.f[1], fmo.f[2], b, sx, sxy, &bar, tid, SLT_THREADS);
+
+  const int I0 = 1 + (int)blockIdx.x * LinGeom::TX, J0 = 1 + (int)blockIdx.y * LinGeom::TY, K0 = 1 + (int)blockIdx.z * LinGeom::TZ;
+  const int i = I0 + (int)threadIdx.x, j = J0 + (int)threadIdx.y;
+  const int kq[2] = {K0 + (int)threadIdx.z, K0 + (int)threadIdx.z + 2};
+  bool ok[2];
+  T xn[2][3];
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    ok[q] = i <= g.P.n[0] && j <= g.P.n[1] && kq[q] <= g.P.n[2];
+    xn[q][0] = __ldg(g.lt[0] + min(i, g.P.n[0] + 1));
+    xn[q][1] = __ldg(g.lt[1] + min(j, g.P.n[1] + 1));
+    xn[q][2] = __ldg(g.lt[2] + min(kq[q], g.P.n[2] + 1));
+  }
+  if (!__syncthreads_and(mbar_wait_bounded(&bar, 0))) {
+    if (tid == 0) atomicOr(err, ERR_ASYNC_COPY);
+    mbar_wait_bounded(&bar, 0);  // let the copies in flight land before the block leaves
+    return;
+  }
+  auto vel_sample = [&](const T x[3], const int no[3], T ct_, T u[3]) {
+    const TV ct = TV(ct_), omc = TV(1) - ct;
+    LinStencil<T> st;
+    lin_stencil(g, x, no, st);
+    int idx[8];
+#pragma unroll
+    for (int c = 0; c < 8; c++)
+      idx[c] = tile_index<LinGeom, TV>(b, sx, sxy, st.i0[0] + ((c & 1) ? st.d[0] : 0), st.i0[1] + ((c & 2) ? st.d[1] : 0),
+                                       st.i0[2] + ((c & 4) ? st.d[2] : 0));
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const TV *a = su0 + (size_t)c * LinGeom::comp<TV>(), *bb = su1 + (size_t)c * LinGeom::comp<TV>();
+      u[c] = T(lin_blend_contract<T, TV>(st, omc, ct, [&](int e) { return a[idx[e]]; }, [&](int e) { return bb[idx[e]]; }));
+    }
+  };
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    if (!ok[q]) continue;
+    const int k = kq[q];
+    const int no[3] = {i, j, k};
+    T u[3], x[3];
+    {  // first stage on the node (sample_velocity_node)
+      const TV ct = TV(T(S.ct[0])), omc = TV(1) - ct;
+      const int pv = tile_index<LinGeom, TV>(b, sx, sxy, i, j, k);
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+        u[c] = T(omc * su0[(size_t)c * LinGeom::comp<TV>() + pv] + ct * su1[(size_t)c * LinGeom::comp<TV>() + pv]);
+    }
+    // integrate_lp (src/lp_motion_m.f90:129-360) with the stage placement of integrate<>
+    if (NOFF == 0) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) x[c] = xn[q][c] + dt * u[c];
+    } else if (NOFF == 1) {
+      T xh[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) xh[c] = xn[q][c] + HALF * dt * u[c];
+      vel_sample(xh, no, T(S.ct[1]), u);
+#pragma unroll
+      for (int c = 0; c < 3; c++) x[c] = xn[q][c] + dt * u[c];
+    } else if (NOFF == 2) {
+      T kk[3], xs[3], acc[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        kk[c] = dt * u[c];
+        acc[c] = xn[q][c] + SIXTH * kk[c];
+        xs[c] = xn[q][c] + HALF * kk[c];
+      }
+      vel_sample(xs, no, T(S.ct[1]), u);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        kk[c] = dt * u[c];
+        xs[c] = xn[q][c] + TWO * kk[c];
+        acc[c] = acc[c] + TWOTHIRD * kk[c];
+      }
+      vel_sample(xs, no, T(S.ct[2]), u);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        kk[c] = dt * u[c];
+        x[c] = acc[c] + SIXTH * kk[c];
+      }
+    } else {
+      T kk[3], xs[3], acc[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        kk[c] = dt * u[c];
+        acc[c] = xn[q][c] + SIXTH * kk[c];
+        xs[c] = xn[q][c] + HALF * kk[c];
+      }
+      vel_sample(xs, no, T(S.ct[1]), u);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        kk[c] = dt * u[c];
+        acc[c] = acc[c] + THIRD * kk[c];
+        xs[c] = xn[q][c] + HALF * kk[c];
+      }
+      vel_sample(xs, no, T(S.ct[2]), u);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        kk[c] = dt * u[c];
+        acc[c] = acc[c] + THIRD * kk[c];
+        xs[c] = xn[q][c] + kk[c];
+      }
+      vel_sample(xs, no, T(S.ct[3]), u);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        kk[c] = dt * u[c];
+        x[c] = acc[c] + SIXTH * kk[c];
+      }
+    }
+    int nb[3] = {i, j, k};
+    project_plane(g, nb, x);
+    if (particle_bc<T, HAS_FLAGS>(g, nb, x, err)) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) x[c] = xn[q][c];
+    }
+    // previous flow map at the departure point (sample_field LINEAR around the node)
+    LinStencil<T> st;
+    lin_stencil(g, x, no, st);
+    int idx[8];
+#pragma unroll
+    for (int c = 0; c < 8; c++)
+      idx[c] = tile_index<LinGeom, T>(b, sx, sxy, st.i0[0] + ((c & 1) ? st.d[0] : 0), st.i0[1] + ((c & 2) ? st.d[1] : 0),
+                                      st.i0[2] + ((c & 4) ? st.d[2] : 0));
+    T fmp[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const T *f = sf + (size_t)c * LinGeom::comp<T>();
+      fmp[c] = lin_contract<T>(st, [&](int e) { return f[idx[e]]; });
+    }
+    const int p = pidx(sx, sxy, i, j, k);
+    const int fl = HAS_FLAGS ? (int)g.flag[p] : (int)LCS_INTERNAL;
+    const T mask = fl != LCS_MASK ? T(1) : T(0);
+    const bool zero = HAS_FLAGS && (fl == LCS_MASK || fl == LCS_INFLOW || fl == LCS_OUTFLOW);
+    T vpre[3], vfin[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      vpre[c] = (fmp[c] + (x[c] - xn[q][c])) * mask;
+      vfin[c] = zero ? T(0) : vpre[c];
+      fmn.f[c][p] = vfin[c];
+    }
+    write_ghosts<T, HAS_FLAGS, GHOST_FM>(g, fmn.f, i, j, k, vpre, vfin, err);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Forward particle subcycle with the B-spline taps staged in shared memory: the cubic form of
+// k_fwd_subcycle (update_lp, src/lp_motion_m.f90:15-54, with integrate_lp and the CUBIC branch
+// of interp_s2u_r1).  The particles are sorted by cell in tiles of 16 x 4 x 4 cells
+// (k_particle_count / k_particle_scatter, every other subcycle); one block advances the
+// particles of one tile.  At the sort a particle lies in its cell c; one unsorted subcycle and
+// the RK stages move it at most 1.5 cells per axis (the CFL bound), so its stencils read the
+// coefficients c-3 .. c+4: the tile widened by 4 cells (24 x 12 x 12 per component), which the
+// block copies into shared memory once per RK stage -- the stage's blend -- with row bulk copies
+// on an mbarrier.  Stencils outside the box read global memory; both paths run spline_contract,
+// so the particles move bitwise as in k_fwd_subcycle.
+// ---------------------------------------------------------------------------------------
+using FwdGeom = TileGeom<16, 4, 4, 4>;
+constexpr int FWT_TX = FwdGeom::TX, FWT_TY = FwdGeom::TY, FWT_TZ = FwdGeom::TZ;
+
+template <typename TV>
+__host__ __device__ constexpr size_t fwt_bytes() {
+  return (size_t)3 * FwdGeom::comp<TV>() * sizeof(TV);
+}
+
+// the box of sort tile (tx, ty, tz): cells tx*TX .. widened by HALO - 1 below, HALO above
+template <typename G, typename T>
+__device__ __forceinline__ TileBox tile_box_at(const DevGrid<T> &g, int tx, int ty, int tz) {
+  TileBox b;
+  b.xs = 1 + tx * G::TX - G::HALO;
+  b.ys = 1 + ty * G::TY - G::HALO;
+  b.zs = 1 + tz * G::TZ - G::HALO;
+  b.xlo = max(b.xs, 0);
+  b.xhi = min(b.xs + G::SX, g.P.sx);
+  b.ylo = max(b.ys, 0);
+  b.yhi = min(b.ys + G::SY, g.P.n[1] + 2);
+  b.zlo = max(b.zs, 0);
+  b.zhi = min(b.zs + G::SZ, g.P.n[2] + 2);
+  return b;
+}
+
+// one 3-component B-spline sample from a staged box (global memory where the stencil leaves it)
+template <typename G, typename T, typename TC, bool UNI>
+__device__ __forceinline__ void tile_sample1(const DevGrid<T> &g, const SplineAxes<T> &sa, const TileBox &b, const TC *box, const TC *g0,
+                                             const TC *g1, const TC *g2, const T x[3], const int no[3], T out[3]) {
+  SplineStencil<T> st;
+  if (!spline_stencil<T, 4, UNI>(g, sa, x, no, st)) {
+    out[0] = out[1] = out[2] = T(0);
+    return;
+  }
+  if (slt_inside(b, st.c0)) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) out[c] = T(tile_apply<G, T, TC>(sa, st, box + (size_t)c * G::template comp<TC>(), b, g.P.sx, g.P.sxy));
+  } else {
+    out[0] = T(spline_apply<T, 4, TC>(g, sa, st, g0));
+    out[1] = T(spline_apply<T, 4, TC>(g, sa, st, g1));
+    out[2] = T(spline_apply<T, 4, TC>(g, sa, st, g2));
+  }
+}
+
+#ifndef CFD2LCS_FWT_MINB
+#define CFD2LCS_FWT_MINB 2
+#endif
+
+template <typename T, typename TV, int INTEG, bool HAS_FLAGS>
+__global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_FWT_MINB)
+    k_fwd_tile(DevGrid<T> g, SplineAxes<T> sa, VelFields<TV> V, Particles<T> P, StageTimes S, T dt, const int *offs, const int *tsum,
+               SortTiles st, int np, int *err) {
+  extern __shared__ __align__(128) unsigned char fwt_smem[];
+  __shared__ __align__(8) uint64_t bar;
+  constexpr bool UNI = !std::is_same<T, TV>::value;
+  constexpr int NS = INTEG == RK2_ ? 2 : (INTEG == RK3_ ? 3 : (INTEG == RK4_ ? 4 : 1));  // samples per step
+  const T HALF = T(1) / T(2), THIRD = T(1) / T(3), TWOTHIRD = T(2) / T(3), SIXTH = T(1) / T(6), TWO = T(2);
+  const long ntiles = (long)st.ntx * st.nty * st.ntz;
+  const long t = blockIdx.x;
+  const int start = sort_tile_start(offs, tsum, t, ntiles, np), end = sort_tile_start(offs, tsum, t + 1, ntiles, np);
+  if (start >= end) return;  // an empty tile (the whole block leaves)
+  const int tx = (int)(t % st.ntx), ty = (int)((t / st.ntx) % st.nty), tz = (int)(t / ((long)st.ntx * st.nty));
+  const TileBox b = tile_box_at<FwdGeom>(g, tx, ty, tz);
+  const int tid = threadIdx.x, sx = g.P.sx, sxy = g.P.sxy;
+  TV *const tv = reinterpret_cast<TV *>(fwt_smem);
+  if (tid == 0) mbar_init(&bar, 3 * FwdGeom::ROWS);
+  __syncthreads();
+  unsigned parity = 0;
+  bool alive = true;
+  for (int r0 = start; r0 < end && alive; r0 += 2 * SLT_THREADS) {  // rounds of 512 particles (block-uniform)
+    tile_fill<FwdGeom, TV>(tv, V.cs[0][0], V.cs[0][1], V.cs[0][2], b, sx, sxy, &bar, tid, SLT_THREADS);
+    const int qs[2] = {r0 + tid, r0 + SLT_THREADS + tid};
+    bool ok[2];
+    T xn[2][3], xs[2][3], acc[2][3];
+    int no[2][3];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      ok[q] = qs[q] < end;
+      if (!ok[q]) continue;
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        xn[q][c] = P.x[c][qs[q]];
+        xs[q][c] = xn[q][c];
+        no[q][c] = P.no[c][qs[q]];
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+      // (no break: the loop must unroll, so that V.cs[s] indexes the kernel parameters by constants)
+      if (alive) alive = __syncthreads_and(mbar_wait_bounded(&bar, parity));
+      if (!alive) continue;
+      parity ^= 1u;
+#pragma unroll
+      for (int q = 0; q < 2; q++) {
+        if (!ok[q]) continue;
+        T u[3];
+        tile_sample1<FwdGeom, T, TV, UNI>(g, sa, b, tv, V.cs[s][0], V.cs[s][1], V.cs[s][2], xs[q], no[q], u);
+        // integrate_lp (src/lp_motion_m.f90:129-360) with the stage placement of integrate<>
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          const T k = dt * u[c];
+          if (NS == 1) {
+            xs[q][c] = xn[q][c] + dt * u[c];
+          } else if (NS == 2) {
+            xs[q][c] = s == 0 ? xn[q][c] + HALF * dt * u[c] : xn[q][c] + dt * u[c];
+          } else if (NS == 3) {
+            if (s == 0) {
+              acc[q][c] = xn[q][c] + SIXTH * k;
+              xs[q][c] = xn[q][c] + HALF * k;
+            } else if (s == 1) {
+              xs[q][c] = xn[q][c] + TWO * k;
+              acc[q][c] = acc[q][c] + TWOTHIRD * k;
+            } else {
+              xs[q][c] = acc[q][c] + SIXTH * k;
+            }
+          } else {
+            if (s == 0) {
+              acc[q][c] = xn[q][c] + SIXTH * k;
+              xs[q][c] = xn[q][c] + HALF * k;
+            } else if (s == 1) {
+              acc[q][c] = acc[q][c] + THIRD * k;
+              xs[q][c] = xn[q][c] + HALF * k;
+            } else if (s == 2) {
+              acc[q][c] = acc[q][c] + THIRD * k;
+              xs[q][c] = xn[q][c] + k;
+            } else {
+              xs[q][c] = acc[q][c] + SIXTH * k;
+            }
+          }
+        }
+      }
+      __syncthreads();  // every thread is done reading the box
+      fence_proxy_async_smem();
+      if (s + 1 < NS) tile_fill<FwdGeom, TV>(tv, V.cs[s + 1][0], V.cs[s + 1][1], V.cs[s + 1][2], b, sx, sxy, &bar, tid, SLT_THREADS);
+    }
+    if (!alive) break;
+    // project, particle BC, stick, displacement, one node-search pass, periodic wrap
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      if (!ok[q]) continue;
+      const int sl = qs[q];
+      T *x = xs[q];
+      int *nd = no[q];
+      project_plane(g, nd, x);
+      if (particle_bc<T, HAS_FLAGS>(g, nd, x, err)) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) x[c] = xn[q][c];
+      }
+#pragma unroll
+      for (int c = 0; c < 3; c++) P.dx[c][sl] = P.dx[c][sl] + (x[c] - xn[q][c]);
+      track_pass(g, x, nd);
+      wrap_particle(g, x, nd);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        P.x[c][sl] = x[c];
+        P.no[c][sl] = nd[c];
+      }
+    }
+  }
+  if (!alive) {
+    // a copy did not complete: record it, let the copies in flight land, and leave
+    if (tid == 0) atomicOr(err, ERR_ASYNC_COPY);
+    mbar_wait_bounded(&bar, parity);
   }
 }
 

@@ -181,7 +181,9 @@ def test_velocity_invariants(oracle_dp, gpu_dp, case, integrator, interp):
 
 
 @pytest.mark.parametrize("case,integrator,directions", [("abc_unsteady", 2, (SC.FTLE_BKWD, SC.FTLE_FWD)), ("dg", 3, (SC.FTLE_BKWD,)),
-                                                        ("mixed_bc", 4, (SC.FTLE_BKWD, SC.FTLE_FWD))])
+                                                        ("mixed_bc", 4, (SC.FTLE_BKWD, SC.FTLE_FWD)),
+                                                        # forward set first: its blends must not leak into the backward set
+                                                        ("abc_unsteady", 3, (SC.FTLE_FWD, SC.FTLE_BKWD))])
 def test_linear_stage_blends(oracle_dp, gpu_dp, case, integrator, directions, monkeypatch):
     """LINEAR with the stage blends written once per subcycle (the large-grid path, forced on
     small grids through CFD2LCS_B200_LINEAR_BLEND_MIN): the same parity bounds."""

@@ -1,7 +1,8 @@
-"""The cubic backward subcycle with its spline taps staged in shared memory (k_sl_tile) against
-the gathering kernel it replaces (k_sl_subcycle, selected with CFD2LCS_B200_SL_TILE=0 at
-cfd2lcs_init): both contract the same taps in the same order, so flow maps and FTLE must be
-bitwise equal.  Grids of 38^3 leave partial tiles in x (38 = 32 + 6), y and z (38 = 9 x 4 + 2);
+"""The subcycle kernels that stage their taps in shared memory -- backward cubic (k_sl_tile),
+backward LINEAR (k_sl_tile_lin) and forward cubic (k_fwd_tile, one block per 16 x 4 x 4-cell
+sort tile) -- against the gathering kernels they replace (k_sl_subcycle, k_fwd_subcycle,
+selected with CFD2LCS_B200_SL_TILE=0 at cfd2lcs_init): both contract the same taps in the same
+order, so flow maps and FTLE must be bitwise equal.  Grids of 38^3 leave partial tiles in x (38 = 32 + 6), y and z (38 = 9 x 4 + 2);
 the small walled / mixed-boundary cases clip the staged box at the padded array's edges.
 The oracle parity of the same path is in test_gpu_parity.py and test_golden_configs.py."""
 import os
@@ -26,13 +27,14 @@ def gpu_sp():
     return L.Cfd2lcs("sp")
 
 
-def _run(gpu, case, integrator, staged, n=None, steps=None, mixed=False, dirs=(SC.FTLE_BKWD,)):
-    os.environ["CFD2LCS_B200_SL_TILE"] = "1" if staged else "0"
+def _run(gpu, case, integrator, staged, n=None, steps=None, mixed=False, dirs=(SC.FTLE_BKWD,), interp=3):
+    # 2 also stages the LINEAR backward kernel (off by default: slower than its gathering form)
+    os.environ["CFD2LCS_B200_SL_TILE"] = "2" if staged else "0"
     try:
         gpu.reset()
         if mixed:
             gpu.set_option("MIXED_PRECISION", 1)
-        _, hs = SC.run(gpu, case, dirs, integrator, 3, n=n, steps=steps)
+        _, hs = SC.run(gpu, case, dirs, integrator, interp, n=n, steps=steps)
     finally:
         os.environ.pop("CFD2LCS_B200_SL_TILE", None)
     err, msg = gpu.error()
@@ -43,8 +45,9 @@ def _run(gpu, case, integrator, staged, n=None, steps=None, mixed=False, dirs=(S
 def _same(gpu, case, integrator, **kw):
     fa, ta, ca, sa = _run(gpu, case, integrator, True, **kw)
     fb, tb, cb, sb = _run(gpu, case, integrator, False, **kw)
-    assert sa["sl"] > 0, "the staged kernel did not run"
-    assert sb["sl"] == 0
+    key = "fwd" if kw.get("dirs") == (SC.FTLE_FWD,) else "sl"
+    assert sa[key] > 0, "the staged kernel did not run"
+    assert sb["sl"] == 0 and sb["fwd"] == 0
     assert ca["integrations_bkwd"] == cb["integrations_bkwd"] and ca["ftle_frames"] == cb["ftle_frames"]
     for x, y in zip(fa, fb):
         assert np.array_equal(x, y), f"flow maps differ: max {np.max(np.abs(x - y)):.3e}"
@@ -68,3 +71,48 @@ def test_staged_small_and_walled(gpu_dp, case):
 
 def test_staged_single_precision(gpu_sp):
     _same(gpu_sp, "abc", 3, n=38, steps=14)
+
+
+@pytest.mark.parametrize("integrator", [0, 2, 3, 4])
+def test_staged_linear_abc_partial_tiles(gpu_dp, integrator):
+    _same(gpu_dp, "abc", integrator, n=38, steps=14, interp=1)
+
+
+def test_staged_linear_unsteady_mixed_precision(gpu_dp):
+    _same(gpu_dp, "abc_unsteady", 2, n=38, mixed=True, interp=1)
+
+
+@pytest.mark.parametrize("case", ["mixed_bc", "turb", "channel"])
+def test_staged_linear_small_and_walled(gpu_dp, case):
+    _same(gpu_dp, case, 2, interp=1)
+
+
+def test_staged_linear_single_precision(gpu_sp):
+    _same(gpu_sp, "turb", 3, n=20, interp=1)
+
+
+@pytest.mark.parametrize("integrator", [0, 2, 3, 4])
+def test_staged_forward_abc_partial_tiles(gpu_dp, integrator):
+    _same(gpu_dp, "abc", integrator, n=38, steps=14, dirs=(SC.FTLE_FWD,))
+
+
+def test_staged_forward_unsteady_mixed_precision(gpu_dp):
+    _same(gpu_dp, "abc_unsteady", 3, n=38, mixed=True, dirs=(SC.FTLE_FWD,))
+
+
+@pytest.mark.parametrize("case", ["mixed_bc", "turb"])
+def test_staged_forward_small_and_walled(gpu_dp, case):
+    _same(gpu_dp, case, 3, dirs=(SC.FTLE_FWD,))
+
+
+def test_staged_forward_single_precision(gpu_sp):
+    _same(gpu_sp, "abc", 3, n=38, steps=14, dirs=(SC.FTLE_FWD,))
+
+
+def test_staged_both_directions(gpu_dp):
+    """Forward and backward sets of one run (the benchmark's configuration)."""
+    fa, ta, _, sa = _run(gpu_dp, "abc", 3, True, n=38, steps=14, dirs=(SC.FTLE_FWD, SC.FTLE_BKWD))
+    fb, tb, _, _ = _run(gpu_dp, "abc", 3, False, n=38, steps=14, dirs=(SC.FTLE_FWD, SC.FTLE_BKWD))
+    assert sa["sl"] > 0 and sa["fwd"] > 0
+    for x, y in zip(fa + ta, fb + tb):
+        assert np.array_equal(x, y)
