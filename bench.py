@@ -367,7 +367,7 @@ def run_form(args, w, precision, local, world, rank, clocks=False, e2e=False, ho
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    c0, p0, k0 = api.counters(), api.phase_times_ms(), api.kernel_times()
+    c0, p0, k0, s0 = api.counters(), api.phase_times_ms(), api.kernel_times(), api.staged_launches()
     sampler = ClockSampler(local) if clocks else None
     if sampler:
         sampler.__enter__()
@@ -378,7 +378,7 @@ def run_form(args, w, precision, local, world, rank, clocks=False, e2e=False, ho
         sampler.__exit__(None, None, None)
     if world > 1:
         torch.distributed.barrier()
-    c1, p1, k1 = api.counters(), api.phase_times_ms(), api.kernel_times()
+    c1, p1, k1, s1 = api.counters(), api.phase_times_ms(), api.kernel_times(), api.staged_launches()
     err, msg = api.error()
     if err:
         raise RuntimeError(msg)
@@ -387,7 +387,7 @@ def run_form(args, w, precision, local, world, rank, clocks=False, e2e=False, ho
     ms_max = rank_max(ms, world, dev)
     out = dict(api=api, g=g, N=N, handles=handles, work=work, ms=ms, ms_max=ms_max, value=world * work / (ms_max / 1000.0),
                launches=c1["kernel_launches"] - c0["kernel_launches"], c0=c0, c1=c1, p0=p0, p1=p1, k0=k0, k1=k1,
-               clocks=sampler.summary() if sampler else None, staged=api.staged_launches())
+               clocks=sampler.summary() if sampler else None, staged={k: s1[k] - s0[k] for k in s1}, tuning=api.tuning())
     nxt = total + 1
     if e2e:
         # --- end to end: host arrays through cfd2lcs_update_c, FTLE read back each step ---
@@ -468,11 +468,15 @@ def hot_kernel_rooflines(r, w, precision, hbm, fp64_peak, hbm_src=None):
     k0, k1 = r["k0"], r["k1"]
     cands = []
     nsl, nfw = k1["sl_launches"] - k0["sl_launches"], k1["fwd_launches"] - k0["fwd_launches"]
+    # the kernels that ran in the timed region (staged, gathering, or both while the tuner sampled)
+    def kname(staged, n, st, ga):
+        return st if staged == n else (ga if staged == 0 else st + "+" + ga)
+    stl = "k_sl_tile_lin" if w["interpolator"] == 1 else "k_sl_tile"
     if nsl > 0:
-        cands.append(("k_sl_tile" if r["staged"]["sl"] > 0 else "k_sl_subcycle", k1["sl_ms"] - k0["sl_ms"], nsl,
+        cands.append((kname(r["staged"]["sl"], nsl, stl, "k_sl_subcycle"), k1["sl_ms"] - k0["sl_ms"], nsl,
                       sl_bytes_per_point(s_bytes, w["interpolator"], w["integrator"], v_bytes)))
     if nfw > 0:
-        cands.append(("k_fwd_tile" if r["staged"]["fwd"] > 0 else "k_fwd_subcycle", k1["fwd_ms"] - k0["fwd_ms"], nfw,
+        cands.append((kname(r["staged"]["fwd"], nfw, "k_fwd_tile", "k_fwd_subcycle"), k1["fwd_ms"] - k0["fwd_ms"], nfw,
                       fwd_bytes_per_particle(s_bytes, w["interpolator"], w["integrator"], v_bytes)))
     rooflines = {}
     for name, tot_ms, nl, bpp in cands:
@@ -553,7 +557,8 @@ def run_b200(args, w):
             "ftle_field_ms": ffr["ms_per_frame"] if ffr else None, "ftle_field": ffr, "ftle_frames_seen": frames,
             "slots_composed_per_frame": (c1["slots_composed"] / frames if frames else None),
             "nsub_per_update": {"fwd": c1["nsub_fwd"], "bkwd": c1["nsub_bkwd"]},
-            "gpu_launches": r["launches"], "staged_launches": r["staged"], "e2e": r["e2e"], "roofline": roof, "rooflines": rooflines,
+            "gpu_launches": r["launches"], "staged_launches": r["staged"], "tuning": r["tuning"], "e2e": r["e2e"], "roofline": roof,
+            "rooflines": rooflines,
             "phase_ms_per_step": {k: (p1[k] - p0[k]) / args.steps for k in p1}}
     if args.precision == "fp64":
         line["ftle_error"] = {"form": "plain FP64", "vs": "FP64 oracle (CPU restatement of the reference)",
@@ -572,7 +577,7 @@ def run_b200(args, w):
             "form": "mixed: FP32 velocity levels, spline coefficients and stage blends; FP64 positions, flow maps, "
                     "composition, Cauchy-Green and eigen-solve",
             "value": m["value"], "unit": UNIT, "ms_per_step": m["ms_max"] / args.steps, "ratio_vs_fp64": m["value"] / line["value"],
-            "ftle_field": ftle_field_roofline(m, w, hbm, hbm_src), "rooflines": mroof,
+            "ftle_field": ftle_field_roofline(m, w, hbm, hbm_src), "rooflines": mroof, "tuning": m["tuning"],
             "phase_ms_per_step": {k: (m["p1"][k] - m["p0"][k]) / args.steps for k in m["p1"]},
             "ftle_error": {"vs": "plain FP64 GPU path of this run (itself parity-tested against the FP64 oracle)",
                            "grid": list(g.n), "updates": horizon, "frame_t": m["horizon_t"],

@@ -93,6 +93,15 @@ void cfd2lcs_get_kernel_times_c(double t[2], long long n[2]);
  * n[1] forward particle.  The rest of those launches gathered their taps from global memory. */
 void cfd2lcs_get_staged_launches_c(long long n[2]);
 
+/* The library times both forms of the cubic / LINEAR subcycle kernels -- taps staged in shared
+ * memory or gathered from global memory, which give the same bits -- on an instance's first
+ * launches and keeps the faster (environment CFD2LCS_B200_SL_TILE at cfd2lcs_init: 0 gathering
+ * only, 1 tuned, the default, 2 staged wherever it applies).  choice[0] backward, choice[1]
+ * forward kernel: -1 while sampling or where staging does not apply, 0 gathering, 1 staged;
+ * ms[0], ms[1] the mean backward launch times measured for gathering and staged, ms[2], ms[3]
+ * the forward ones. */
+void cfd2lcs_get_tuning_c(int choice[2], double ms[4]);
+
 /* Recomputes the latest FTLE frame of a diagnostic -- the composition of its stored
  * sub-flow maps and the FTLE -- into device buffers the caller owns, and allocates no memory
  * while doing so.  No counterpart in the reference: it exists for callers that cannot call

@@ -37,7 +37,7 @@ EXPORTED_SYMBOLS = [
     # extensions (include/cfd2lcs_b200.h)
     "cfd2lcs_finalize_c", "cfd2lcs_get_error_c", "cfd2lcs_reset_c", "cfd2lcs_get_ftle_c", "cfd2lcs_get_flowmap_c",
     "cfd2lcs_update_device_c", "cfd2lcs_ftle_device_ptr_c", "cfd2lcs_get_counters_c", "cfd2lcs_get_phase_times_c",
-    "cfd2lcs_get_kernel_times_c", "cfd2lcs_get_staged_launches_c", "cfd2lcs_reconstruct_noalloc_c", "cfd2lcs_get_invariants_c",
+    "cfd2lcs_get_kernel_times_c", "cfd2lcs_get_staged_launches_c", "cfd2lcs_get_tuning_c", "cfd2lcs_reconstruct_noalloc_c", "cfd2lcs_get_invariants_c",
     "cfd2lcs_tracer_count_c", "cfd2lcs_get_tracers_c", "cfd2lcs_diagnostic_size_c",
     # batched form (include/cfd2lcs_b200.h)
     "cfd2lcs_batch_add_c", "cfd2lcs_batch_diagnostic_init_c", "cfd2lcs_batch_update_device_c", "cfd2lcs_batch_get_ftle_c",
@@ -106,6 +106,7 @@ def load(precision: str = "dp") -> C.CDLL:
     lib.cfd2lcs_get_phase_times_c.argtypes = [P]
     lib.cfd2lcs_get_kernel_times_c.argtypes = [P, P]
     lib.cfd2lcs_get_staged_launches_c.argtypes = [P]
+    lib.cfd2lcs_get_tuning_c.argtypes = [P, P]
     lib.cfd2lcs_reconstruct_noalloc_c.argtypes = [C.c_int, P, P]
     lib.cfd2lcs_reconstruct_noalloc_c.restype = C.c_int
     lib.cfd2lcs_b200_grid_tables.argtypes = [P, P, P, P, P, P, P, P, P, P, C.c_char_p, C.c_size_t]
@@ -264,6 +265,14 @@ class Cfd2lcs:
         n = np.zeros(2, dtype=np.int64)
         self.lib.cfd2lcs_get_staged_launches_c(self._p(n))
         return {"sl": int(n[0]), "fwd": int(n[1])}
+
+    def tuning(self) -> dict:
+        """The staged-versus-gathering choice of the backward and forward subcycle kernels (-1
+        sampling or not applicable, 0 gathering, 1 staged) and the mean launch ms measured."""
+        ch = np.zeros(2, dtype=np.int32)
+        ms = np.zeros(4, dtype=np.float64)
+        self.lib.cfd2lcs_get_tuning_c(self._p(ch), self._p(ms))
+        return {"bkwd": int(ch[0]), "fwd": int(ch[1]), "bkwd_ms": [float(ms[0]), float(ms[1])], "fwd_ms": [float(ms[2]), float(ms[3])]}
 
     def kernel_times(self) -> dict:
         t = np.zeros(2, dtype=np.float64)

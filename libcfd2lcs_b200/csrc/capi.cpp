@@ -423,6 +423,16 @@ CFD2LCS_EXPORT void cfd2lcs_get_staged_launches_c(long long n[2]) {
   n[1] = k.fwd_staged_launches;
 }
 
+// The engine's choice between staged and gathering subcycle kernels: choice[f] for the backward
+// (f = 0) and forward (f = 1) kernel, -1 while sampling or where staging does not apply, 0
+// gathering, 1 staged; ms[2f], ms[2f+1] the mean launch times measured for the two.
+CFD2LCS_EXPORT void cfd2lcs_get_tuning_c(int choice[2], double ms[4]) {
+  Library &lib = L();
+  for (int f = 0; f < 2; f++) choice[f] = -1;
+  for (int q = 0; q < 4; q++) ms[q] = 0.0;
+  if (lib.eng) lib.eng->tuning(choice, ms);
+}
+
 // Host-only formatting hook (no device work): the Fortran ESw.d editing the output files use,
 // for checking the writer on machines without a GPU.  out receives w characters and a NUL.
 CFD2LCS_EXPORT void cfd2lcs_b200_format_es(double v, int w, int d, char *out) {

@@ -78,6 +78,9 @@ class EngineBase {
   // Recomputes the latest FTLE frame of a diagnostic into caller-owned device buffers
   // without allocating (pointer table in a static device array, see engine.cu).
   virtual bool reconstruct_noalloc(int handle, lcsdata_t *d_ftle, lcsdata_t *d_fm, std::string &msg) = 0;
+  // choices of the staged-versus-gathering tuner (family 0 backward, 1 forward) and the mean
+  // launch times it measured per variant
+  virtual void tuning(int choice[2], double ms[4]) const = 0;
   virtual const Counters &counters() const = 0;
   virtual bool host_grid_tables(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, const int *flag,
                                 lcsdata_t *xyz_pad, int *flag_pad, lcsdata_t *nrm_pad, lcsdata_t *inv_delta, int *per,

@@ -10,7 +10,11 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <map>
 #include <mutex>
+#include <array>
+
+#include <cuda.h>
 
 #include "grid.h"
 #include "kernels.cuh"
@@ -105,6 +109,7 @@ struct Diag {
   unsigned *pkey = nullptr;
   int *pcnt = nullptr, *poffs = nullptr, *ptsum = nullptr;
   SortTiles sort_geom{};  // cell tiles of the last sort (the staged forward kernel reads one tile per block)
+  int fwd_variant = 0;    // forward kernel until the next sort: 0 gathering, 1 staged
   // ring of sub-flow maps (padded) and their spline coefficients
   std::vector<T *> slot;      // 3 per slot
   std::vector<T *> slotcoef;  // 3 per slot (allocated on first spline use)
@@ -135,6 +140,22 @@ struct Diag {
 };
 
 }  // namespace
+
+// cuTensorMapEncodeTiled of the driver, looked up once through the runtime's entry-point query
+// (the library links the runtime statically and no driver library); null where unavailable.
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *, const cuuint64_t *,
+                                   const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+inline EncodeTiledFn encode_tiled_fn() {
+  static const EncodeTiledFn fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+      return (EncodeTiledFn) nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
 
 // The allocation-free entry point's table of sub-flow-map pointers (engine.cu): its size (in
 // sub-flow maps) and its device address on device dev.
@@ -212,10 +233,9 @@ class Engine : public EngineBase {
     }
     CK(cudaMallocHost(&red_host_, sizeof(DevReduce)));
     if (const char *e = std::getenv("CFD2LCS_B200_LINEAR_BLEND_MIN")) lin_blend_min_ = std::atol(e);
-    if (const char *e = std::getenv("CFD2LCS_B200_SL_TILE")) {
-      sl_tile_ = std::atoi(e) != 0;
-      sl_tile_lin_ = std::atoi(e) >= 2;
-    }
+    if (const char *e = std::getenv("CFD2LCS_B200_TMA_TENSOR")) tma_tensor_ = std::atoi(e) != 0;
+    if (const char *e = std::getenv("CFD2LCS_B200_COMPOSE_SORT_MIN")) compose_sort_min_ = std::atol(e);
+    if (const char *e = std::getenv("CFD2LCS_B200_SL_TILE")) tile_mode_ = std::max(0, std::min(2, std::atoi(e)));
     for (int a = 0; a < 3; a++) n_[a] = n[a];
     // coordinate lines and interior flags for the output files (the grid is a tensor product)
     for (int a = 0; a < 3; a++)
@@ -319,6 +339,48 @@ class Engine : public EngineBase {
     for (int c = 0; c < 3; c++)
       if (!(d.composed[c] = arena_.alloc<T>(dn, msg))) return false;
     if (!(d.ftle = arena_.alloc<lcsdata_t>(dn, msg))) return false;
+    if (!d.lg && (d.type == FTLE_FWD || d.type == FTLE_BKWD) && !ensure_compose_scratch(msg)) return false;
+    return true;
+  }
+
+  // Composition one sub-map at a time with the particles re-sorted between sub-maps (k_compose_step)
+  // on grids of at least this many points (the sort costs more than it saves on small grids);
+  // CFD2LCS_B200_COMPOSE_SORT_MIN at cfd2lcs_init overrides it (the tests take both paths on
+  // small grids).
+#ifndef CFD2LCS_COMPOSE_SORT_MIN
+#define CFD2LCS_COMPOSE_SORT_MIN (1L << 20)
+#endif
+  long compose_sort_min_ = CFD2LCS_COMPOSE_SORT_MIN;
+  // the composition particles of every solver-grid frame (one frame at a time uses them)
+  Particles<T> cp_[2]{};
+  unsigned *cp_key_ = nullptr;
+  int *cp_cnt_ = nullptr, *cp_offs_ = nullptr, *cp_tsum_ = nullptr;
+
+  bool ensure_compose_scratch(std::string &msg) {
+    if (N_ < compose_sort_min_ || cp_[0].x[0]) return true;
+    for (Particles<T> *Q : {&cp_[0], &cp_[1]}) {
+      for (int c = 0; c < 3; c++) {
+        if (!(Q->x[c] = arena_.alloc<T>(N_, msg))) return false;
+        if (!(Q->dx[c] = arena_.alloc<T>(N_, msg))) return false;
+        if (!(Q->no[c] = arena_.alloc<int>(N_, msg))) return false;
+      }
+      if (!(Q->id = arena_.alloc<int>(N_, msg))) return false;
+    }
+    if (!(cp_[0].slot = arena_.alloc<int>(N_, msg))) return false;
+    cp_[1].slot = cp_[0].slot;
+    const long ncell = sort_key_space(sort_tiles(n_, 32, SORT_TY, SORT_TZ));
+    if (ncell > (long)std::numeric_limits<int>::max()) {
+      msg = "diagnostic_init: grid too large for the composition sort";
+      return false;
+    }
+    if (!(cp_key_ = arena_.alloc<unsigned>(N_, msg))) return false;
+    if (!(cp_cnt_ = arena_.alloc<int>(ncell, msg))) return false;
+    if (!(cp_offs_ = arena_.alloc<int>(ncell, msg))) return false;
+    if (!(cp_tsum_ = arena_.alloc<int>((ncell + SORT_TILE - 1) / SORT_TILE, msg))) return false;
+    if (cudaMemsetAsync(cp_cnt_, 0, ncell * sizeof(int), stream_) != cudaSuccess) {
+      msg = "CUDA error in memset";
+      return false;
+    }
     return true;
   }
 
@@ -506,19 +568,24 @@ class Engine : public EngineBase {
                    : !launch_sl(iv, sa, V, fo, fn, S, (T)dt, msg))
             return false;
           if (!mark(k1, msg)) return false;
-          spans_.push_back({k0, k1, kkind});
+          spans_.push_back({k0, k1, kkind, !d.lg && sl_variant_ >= 0 && tune_[0].choice < 0 && tile_mode_ == 1 ? sl_variant_ : -1});
           d.cur ^= 1;
         } else if (d.type == LP_TRACER) {
           // tracers: the forward subcycle on their own particles (few, unsorted)
           if (!launch_fwd(iv, sa, V, d.P, S, (T)dt, msg, d.np)) return false;
           d.lifetime = d.lifetime + (lcsdata_t)std::fabs((double)dt);  // integrate_lp, lp_motion_m.f90:332
         } else {
-          const bool staged = fwd_tile_usable(iv, V);
-          if (sc % kSortInterval == 0 && !sort_particles(d, msg, staged)) return false;
+          // the variant holds from one sort to the next (the staged kernel reads the sort's tiles)
+          const bool usable = fwd_tile_usable(iv, V);
+          if (sc % kSortInterval == 0) {
+            d.fwd_variant = usable ? tile_variant(1) : 0;
+            if (!sort_particles(d, msg, d.fwd_variant == 1)) return false;
+          }
+          const bool staged = usable && d.fwd_variant == 1;
           if (!mark(k0, msg)) return false;
           if (staged ? !launch_fwd_tile(d, sa, V, S, (T)dt, msg) : !launch_fwd(iv, sa, V, d.P, S, (T)dt, msg, dN(d))) return false;
           if (!mark(k1, msg)) return false;
-          spans_.push_back({k0, k1, kkind});
+          spans_.push_back({k0, k1, kkind, usable && tune_[1].choice < 0 && tile_mode_ == 1 ? 2 + d.fwd_variant : -1});
         }
         lp_time = lp_time + dt;
       }
@@ -634,6 +701,7 @@ class Engine : public EngineBase {
     counters_.phase_ms[6] += ms;
     for (const Span &sp : spans_) {
       CK(cudaEventElapsedTime(&ms, sp.a, sp.b));
+      if (sp.tune >= 0) tune_record(sp.tune, ms);
       if (sp.kind == SPAN_SL) {
         counters_.sl_kernel_ms += ms;
         counters_.sl_kernel_launches++;
@@ -1489,25 +1557,110 @@ class Engine : public EngineBase {
 
   dim3 node_grid() const { return dim3((n_[0] + 31) / 32, (n_[1] + 7) / 8, n_[2]); }
 
-  // The cubic subcycles with their taps staged in shared memory (k_sl_tile, k_fwd_tile) replace
-  // the gathering kernels unless CFD2LCS_B200_SL_TILE=0 at cfd2lcs_init (kept for A/B
-  // comparison).  The staged LINEAR backward kernel (k_sl_tile_lin) runs only with
-  // CFD2LCS_B200_SL_TILE=2: measured on B200 it is slower than the gathering kernel (ABC 256^3
-  // RK2: 1.04 against 0.89 ms per launch; turbulence 512^3: 9.2 against 7.6 ms).
-  bool sl_tile_ = true, sl_tile_lin_ = false;
+  // Subcycle kernels that stage their taps in shared memory (k_sl_tile, k_sl_tile_lin,
+  // k_fwd_tile) are bitwise equal to the gathering kernels they replace, so which of the two runs
+  // is a question of speed only, and the engine measures it: for the backward kernel (family 0)
+  // and the forward kernel (family 1) it alternates the two variants -- launch by launch, or
+  // sort interval by sort interval for the forward kernel, whose staged variant needs its own
+  // sort tiles -- times each launch with the CUDA events that bracket it, and once each variant
+  // has kTuneSamples launches keeps the one with the smaller mean for the rest of the engine's
+  // life (per instance: the batched form tunes every instance for its own grid and options).
+  // Measured on B200, ABC 256^3 FP64 per launch: staged cubic backward 3.22 against 4.63 ms,
+  // staged forward 8.39 against 6.68 ms, staged LINEAR backward 0.79 against 0.90 ms.
+  // CFD2LCS_B200_SL_TILE at cfd2lcs_init: 0 = gathering kernels only, 1 = tuned (default),
+  // 2 = staged kernels wherever they apply.  cfd2lcs_get_tuning_c reports the choices.
+  static constexpr int kTuneSamples = 4;
+  int tile_mode_ = 1;
+  struct Tuner {
+    int choice = -1;  // -1: sampling, 0: gathering, 1: staged
+    double ms[2] = {0, 0};
+    int n[2] = {0, 0};
+  } tune_[2];
+  long tune_idx_[2] = {0, 0};
+
+  // the variant of the next launch (or sort interval) of family fam, for which staging applies
+  int tile_variant(int fam) {
+    if (tile_mode_ != 1) return tile_mode_ == 2 ? 1 : 0;
+    if (tune_[fam].choice >= 0) return tune_[fam].choice;
+    return (int)(tune_idx_[fam]++ & 1);
+  }
+
+  void tune_record(int tag, double ms) {
+    Tuner &t = tune_[tag / 2];
+    if (t.choice >= 0) return;
+    t.ms[tag % 2] += ms;
+    t.n[tag % 2]++;
+    if (t.n[0] >= kTuneSamples && t.n[1] >= kTuneSamples) t.choice = t.ms[1] / t.n[1] < t.ms[0] / t.n[0] ? 1 : 0;
+  }
+
+  void tuning(int choice[2], double ms[4]) const override {
+    for (int f = 0; f < 2; f++) {
+      choice[f] = tune_[f].choice;
+      for (int v = 0; v < 2; v++) ms[2 * f + v] = tune_[f].n[v] ? tune_[f].ms[v] / tune_[f].n[v] : 0.0;
+    }
+  }
+
+  int sl_variant_ = -1;  // variant of the last backward launch while sampling (-1: none)
+
+  // Tensor maps of the staged fields (one per padded component buffer and box shape), so that a
+  // block copies each component's box with one cp.async.bulk.tensor instead of one bulk copy per
+  // row; CFD2LCS_B200_TMA_TENSOR=0 at cfd2lcs_init keeps the row copies.  A map needs rows of a
+  // multiple of 16 bytes (padded x extent * element size); other grids copy rows.
+  bool tma_tensor_ = true;
+  std::map<std::array<uintptr_t, 5>, CUtensorMap> tmaps_;
+
+  template <typename TC>
+  bool tensor_map(const TC *ptr, int bx, int by, int bz, CUtensorMap &out) {
+    if (!tma_tensor_ || !ptr) return false;
+    const long sx = dg_.P.sx, sxy = dg_.P.sxy, es = (long)sizeof(TC);
+    if ((sx * es) % 16 || reinterpret_cast<uintptr_t>(ptr) % 16) return false;
+    const std::array<uintptr_t, 5> key = {reinterpret_cast<uintptr_t>(ptr), (uintptr_t)es, (uintptr_t)bx, (uintptr_t)by, (uintptr_t)bz};
+    auto it = tmaps_.find(key);
+    if (it != tmaps_.end()) {
+      out = it->second;
+      return true;
+    }
+    const EncodeTiledFn fn = encode_tiled_fn();
+    if (!fn) return false;
+    const cuuint64_t dim[3] = {(cuuint64_t)sx, (cuuint64_t)(sxy / sx), (cuuint64_t)(n_[2] + 2)};
+    const cuuint64_t stride[2] = {(cuuint64_t)(sx * es), (cuuint64_t)(sxy * es)};
+    const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz}, estr[3] = {1, 1, 1};
+    CUtensorMap m;
+    if (fn(&m, es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<TC *>(ptr), dim, stride, box, estr,
+           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+    tmaps_[key] = m;
+    out = m;
+    return true;
+  }
+
+  // the maps of fields f0..: three component pointers each, boxes of geometry G
+  template <typename G, typename TC>
+  bool tensor_maps3(const TC *const f[3], CUtensorMap *out) {
+    for (int c = 0; c < 3; c++)
+      if (!tensor_map<TC>(f[c], G::template pitch<TC>(), G::SY, G::SZ, out[c])) return false;
+    return true;
+  }
   int dev_ = 0;  // CUDA device current at cfd2lcs_init
 
   template <int IG, bool F>
   void launch_sl_tile(const SplineAxes<T> &sa, const VelFields<TV> &V, FieldPtrs<T> fo, FieldPtrsW<T> fn, StageTimes S, T dt) {
-    const size_t smem = slt_field_bytes<T>();
+    const size_t smem = slt_field_bytes<T>() + 128;
     cudaFuncSetAttribute(k_sl_tile<T, TV, IG, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const dim3 blk(32, SLT_Y, 2), grd((n_[0] + SLT_X - 1) / SLT_X, (n_[1] + SLT_Y - 1) / SLT_Y, (n_[2] + SLT_Z - 1) / SLT_Z);
-    k_sl_tile<T, TV, IG, F><<<grd, blk, smem, stream_>>>(dg_, sa, V, fo, fn, S, dt, &red_->err);
+    constexpr int noff = IG == RK2_ ? 1 : (IG == RK3_ ? 2 : (IG == RK4_ ? 3 : 0));
+    TileMaps tm{};
+    bool ok = true;
+    for (int f = 0; f < noff && ok; f++) ok = tensor_maps3<CubicGeom, TV>(V.cs[f + 1], tm.m + 3 * f);
+    ok = ok && tensor_maps3<CubicGeom, T>(fo.f, tm.m + 3 * noff);
+    tm.on = ok ? 1 : 0;
+    k_sl_tile<T, TV, IG, F><<<grd, blk, smem, stream_>>>(dg_, sa, V, fo, fn, S, dt, &red_->err, tm);
   }
 
   // the bulk copies need 16-byte aligned sources (cudaMalloc gives 256)
   bool sl_tile_usable(const VelFields<TV> &V, FieldPtrs<T> fo) const {
-    if (!sl_tile_) return false;
+    if (!tile_mode_) return false;
     const int noff = opt_->integrator == 2 ? 1 : (opt_->integrator == 3 ? 2 : (opt_->integrator == 4 ? 3 : 0));
     for (int c = 0; c < 3; c++) {
       if (reinterpret_cast<uintptr_t>(fo.f[c]) % 16) return false;
@@ -1519,16 +1672,20 @@ class Engine : public EngineBase {
 
   template <int IG, bool F>
   void launch_sl_tile_lin(const VelFields<TV> &V, FieldPtrs<T> fo, FieldPtrsW<T> fn, StageTimes S, T dt) {
-    const size_t smem = sll_bytes<T, TV>();
+    const size_t smem = sll_bytes<T, TV>() + 128;
     cudaFuncSetAttribute(k_sl_tile_lin<T, TV, IG, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const dim3 blk(32, LinGeom::TY, 2),
         grd((n_[0] + LinGeom::TX - 1) / LinGeom::TX, (n_[1] + LinGeom::TY - 1) / LinGeom::TY, (n_[2] + LinGeom::TZ - 1) / LinGeom::TZ);
-    k_sl_tile_lin<T, TV, IG, F><<<grd, blk, smem, stream_>>>(dg_, V, fo, fn, S, dt, &red_->err);
+    TileMaps tm{};
+    tm.on = tensor_maps3<LinGeom, TV>(V.un, tm.m) && tensor_maps3<LinGeom, TV>(V.unp1, tm.m + 3) && tensor_maps3<LinGeom, T>(fo.f, tm.m + 6)
+                ? 1
+                : 0;
+    k_sl_tile_lin<T, TV, IG, F><<<grd, blk, smem, stream_>>>(dg_, V, fo, fn, S, dt, &red_->err, tm);
   }
 
   // LINEAR: 3-D grids whose backward set samples both levels per corner (no stage blends)
   bool sl_tile_lin_usable(const VelFields<TV> &V, FieldPtrs<T> fo) const {
-    if (!sl_tile_lin_ || n_[2] < 4 || dg_.P.single_axis >= 0) return false;
+    if (!tile_mode_ || n_[2] < 4 || dg_.P.single_axis >= 0) return false;
     for (int c = 0; c < 3; c++) {
       if (V.cs[1][c] || reinterpret_cast<uintptr_t>(fo.f[c]) % 16 || reinterpret_cast<uintptr_t>(V.un[c]) % 16 ||
           reinterpret_cast<uintptr_t>(V.unp1[c]) % 16)
@@ -1539,8 +1696,9 @@ class Engine : public EngineBase {
 
   template <int INTERP, bool F>
   void sl_integ(const SplineAxes<T> &sa, const VelFields<TV> &V, FieldPtrs<T> fo, FieldPtrsW<T> fn, StageTimes S, T dt) {
+    sl_variant_ = -1;
     if constexpr (INTERP == INTERP_LINEAR) {
-      if (sl_tile_lin_usable(V, fo)) {
+      if (sl_tile_lin_usable(V, fo) && (sl_variant_ = tile_variant(0)) == 1) {
         counters_.kernel_launches++;
         counters_.sl_staged_launches++;
         switch (opt_->integrator) {
@@ -1554,7 +1712,7 @@ class Engine : public EngineBase {
       }
     }
     if constexpr (INTERP == INTERP_SPLINE4) {
-      if (sl_tile_usable(V, fo)) {
+      if (sl_tile_usable(V, fo) && (sl_variant_ = tile_variant(0)) == 1) {
         counters_.kernel_launches++;
         counters_.sl_staged_launches++;
         switch (opt_->integrator) {
@@ -1629,7 +1787,7 @@ class Engine : public EngineBase {
   // The cubic forward subcycle with its taps staged in shared memory (k_fwd_tile): sorted
   // particle sets on 3-D grids, unless CFD2LCS_B200_SL_TILE=0 at cfd2lcs_init.
   bool fwd_tile_usable(int iv, const VelFields<TV> &V) const {
-    if (!sl_tile_ || iv != INTERP_SPLINE4) return false;
+    if (!tile_mode_ || iv != INTERP_SPLINE4) return false;
     const int ns = opt_->integrator == 2 ? 2 : (opt_->integrator == 3 ? 3 : (opt_->integrator == 4 ? 4 : 1));
     for (int s = 0; s < ns; s++)
       for (int c = 0; c < 3; c++)
@@ -1639,11 +1797,16 @@ class Engine : public EngineBase {
 
   template <int IG, bool F>
   void fwd_tile_integ(const SplineAxes<T> &sa, const VelFields<TV> &V, DiagT &d, StageTimes S, T dt) {
-    const size_t smem = fwt_bytes<TV>();
+    const size_t smem = fwt_bytes<TV>() + 128;
     cudaFuncSetAttribute(k_fwd_tile<T, TV, IG, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const long ntiles = (long)d.sort_geom.ntx * d.sort_geom.nty * d.sort_geom.ntz;
+    constexpr int ns = IG == RK2_ ? 2 : (IG == RK3_ ? 3 : (IG == RK4_ ? 4 : 1));
+    TileMaps tm{};
+    bool ok = true;
+    for (int st = 0; st < ns && ok; st++) ok = tensor_maps3<FwdGeom, TV>(V.cs[st], tm.m + 3 * st);
+    tm.on = ok ? 1 : 0;
     k_fwd_tile<T, TV, IG, F><<<(unsigned)ntiles, SLT_THREADS, smem, stream_>>>(dg_, sa, V, d.P, S, dt, d.poffs, d.ptsum, d.sort_geom,
-                                                                              (int)dN(d), &red_->err);
+                                                                              (int)dN(d), &red_->err, tm);
   }
 
   bool launch_fwd_tile(DiagT &d, const SplineAxes<T> &sa, const VelFields<TV> &V, StageTimes S, T dt, std::string &msg) {
@@ -1684,7 +1847,46 @@ class Engine : public EngineBase {
     return true;
   }
 
+  template <int I, bool FL>
+  void compose_steps(const SplineAxes<T> &sa, DiagT &d, int m, FieldPtrsW<T> out) {
+    const int np = (int)N_, grd = (np + 255) / 256;
+    int *err = &red_->err;
+    const SortTiles st = sort_tiles(n_, 32, SORT_TY, SORT_TZ);
+    std::string dummy;
+    k_reset_particles<T><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, cp_[0]);
+    counters_.kernel_launches++;
+    int cur = 0;
+    for (int s = 0; s < m; s++) {
+      if (s > 0) {
+        sort_slots(cp_[cur], cp_[cur ^ 1], cp_key_, cp_cnt_, cp_offs_, cp_tsum_, np, st, dummy);
+        cur ^= 1;
+      }
+      FieldPtrs<T> f{};
+      for (int c = 0; c < 3; c++) f.f[c] = d.slot_list_host[3 * s + c];
+      k_compose_step<T, I, FL><<<grd, 256, 0, stream_>>>(dg_, sa, f, cp_[cur], np, err);
+      counters_.kernel_launches++;
+    }
+    k_compose_finish<T, FL><<<grd, 256, 0, stream_>>>(dg_, cp_[cur], out, np);
+    counters_.kernel_launches++;
+  }
+
   bool launch_compose(int iv, const SplineAxes<T> &sa, DiagT &d, int m, std::string &msg) {
+    if (!d.lg && cp_[0].x[0] && N_ >= compose_sort_min_) {
+      FieldPtrsW<T> out{};
+      for (int c = 0; c < 3; c++) out.f[c] = d.composed[c];
+      counters_.slots_composed += m;
+      const bool F = dg_.P.has_flags != 0;
+#define COMPOSE_STEPS(I) (F ? compose_steps<I, true>(sa, d, m, out) : compose_steps<I, false>(sa, d, m, out))
+      if (iv == INTERP_NEAREST) COMPOSE_STEPS(INTERP_NEAREST);
+      else if (iv == INTERP_LINEAR) COMPOSE_STEPS(INTERP_LINEAR);
+      else if (iv == INTERP_TSE) COMPOSE_STEPS(INTERP_TSE);
+      else if (iv == INTERP_TSE_LIMIT) COMPOSE_STEPS(INTERP_TSE_LIMIT);
+      else if (iv == INTERP_SPLINE4) COMPOSE_STEPS(INTERP_SPLINE4);
+      else COMPOSE_STEPS(INTERP_SPLINE);
+#undef COMPOSE_STEPS
+      CK(cudaGetLastError());
+      return true;
+    }
     const DevGrid<T> &g = dgrid(d);
     const dim3 blk(32, 8, 1), grd = node_grid(g);
     FieldPtrsW<T> out{};
@@ -1954,16 +2156,23 @@ class Engine : public EngineBase {
   // fwd_tile: the 16 x 4 x 4-cell tiles the staged forward kernel reads, else the 32 x 4 x 2
   // tiles that suit the gathering kernel
   bool sort_particles(DiagT &d, std::string &msg, bool fwd_tile = false) {
-    const int np = (int)dN(d), blk = 256, grd = (np + blk - 1) / blk;
     d.sort_geom = fwd_tile ? sort_tiles(n_, FWT_TX, FWT_TY, FWT_TZ) : sort_tiles(n_, 32, SORT_TY, SORT_TZ);
-    const int ncell = (int)sort_key_space(d.sort_geom);
-    const int ntile = (ncell + SORT_TILE - 1) / SORT_TILE;
-    k_particle_count<T><<<grd, blk, 0, stream_>>>(dg_, d.P, d.pkey, d.pcnt, np, d.sort_geom);
-    k_scan_tiles<<<ntile, 256, 0, stream_>>>(d.pcnt, d.poffs, d.ptsum, ncell);
-    k_scan_tile_sums<<<1, 1024, 0, stream_>>>(d.ptsum, ntile);
-    k_particle_scatter<T><<<grd, blk, 0, stream_>>>(d.P, d.P2, d.pkey, d.poffs, d.ptsum, np);
-    CK(cudaGetLastError());
+    if (!sort_slots(d.P, d.P2, d.pkey, d.pcnt, d.poffs, d.ptsum, (int)dN(d), d.sort_geom, msg)) return false;
     std::swap(d.P, d.P2);
+    return true;
+  }
+
+  // counting sort of np particle slots of a by cell into b (tiles of geometry st)
+  bool sort_slots(const Particles<T> &a, const Particles<T> &b, unsigned *key, int *cnt, int *offs, int *tsum, int np, const SortTiles &st,
+                  std::string &msg) {
+    const int blk = 256, grd = (np + blk - 1) / blk;
+    const int ncell = (int)sort_key_space(st);
+    const int ntile = (ncell + SORT_TILE - 1) / SORT_TILE;
+    k_particle_count<T><<<grd, blk, 0, stream_>>>(dg_, a, key, cnt, np, st);
+    k_scan_tiles<<<ntile, 256, 0, stream_>>>(cnt, offs, tsum, ncell);
+    k_scan_tile_sums<<<1, 1024, 0, stream_>>>(tsum, ntile);
+    k_particle_scatter<T><<<grd, blk, 0, stream_>>>(a, b, key, offs, tsum, np);
+    CK(cudaGetLastError());
     counters_.kernel_launches += 4;
     return true;
   }
@@ -2002,6 +2211,7 @@ class Engine : public EngineBase {
   struct Span {
     cudaEvent_t a, b;
     int kind;
+    int tune = -1;  // hot-kernel spans while the tuner samples: family * 2 + variant
   };
   std::vector<cudaEvent_t> evpool_;
   size_t evnext_ = 0;

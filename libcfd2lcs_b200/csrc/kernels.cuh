@@ -462,6 +462,65 @@ __global__ void __launch_bounds__(256) k_compose(DevGrid<T> g, SplineAxes<T> sa,
   for (int c = 0; c < 3; c++) out.f[c][q] = zero ? T(0) : d[c];
 }
 
+// K4 one sub-flow map at a time, for large grids: the composition particles (one per lcs node:
+// position P.x, accumulated displacement P.dx, tracked node P.no, origin node P.id) are
+// re-sorted by cell between sub-maps (k_particle_count / k_particle_scatter), so the warps of
+// one step gather neighbouring taps -- after a few sub-maps the particles of neighbouring nodes
+// are far apart and the node-ordered k_compose gathers each tap sector from HBM.  The per-point
+// sequence is k_compose's loop body, the state kept exactly between steps, so the composed map
+// is bitwise k_compose's.  k_reset_particles starts the particles at their nodes.
+template <typename T, int INTERP, bool HAS_FLAGS>
+__global__ void __launch_bounds__(256) k_compose_step(DevGrid<T> g, SplineAxes<T> sa, FieldPtrs<T> f, Particles<T> P, int np, int *err) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= np) return;
+  T x[3] = {P.x[0][q], P.x[1][q], P.x[2][q]};
+  int no[3] = {P.no[0][q], P.no[1][q], P.no[2][q]};
+  T d[3] = {P.dx[0][q], P.dx[1][q], P.dx[2][q]};
+  project_plane(g, no, x);
+  particle_bc<T, HAS_FLAGS>(g, no, x, err);
+  T up[3];
+  sample_field<T, INTERP>(g, sa, f.f, x, no, up);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    x[c] = x[c] + up[c];
+    d[c] = d[c] + up[c];
+  }
+  alltoall_wrap(g, x, no);
+  int passes = 0;
+  while (true) {
+    const bool moved = track_pass(g, x, no);
+    passes++;
+    if (passes > g.P.maxtrack) {
+      atomicOr(err, ERR_TRACKING);
+      break;
+    }
+    wrap_particle(g, x, no);
+    if (!moved) break;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    P.x[c][q] = x[c];
+    P.no[c][q] = no[c];
+    P.dx[c][q] = d[c];
+  }
+}
+
+// the composed map in node order (exchange_lpmap), after the interior flow-map BC
+template <typename T, bool HAS_FLAGS>
+__global__ void __launch_bounds__(256) k_compose_finish(DevGrid<T> g, Particles<T> P, FieldPtrsW<T> out, int np) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= np) return;
+  const int id = P.id[q];
+  bool zero = false;
+  if (HAS_FLAGS) {
+    const int i = id % g.P.n[0] + 1, j = (id / g.P.n[0]) % g.P.n[1] + 1, k = id / (g.P.n[0] * g.P.n[1]) + 1;
+    const int fl = (int)g.flag[pidx(g.P.sx, g.P.sxy, i, j, k)];
+    zero = fl == LCS_MASK || fl == LCS_INFLOW || fl == LCS_OUTFLOW;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) out.f[c][id] = zero ? T(0) : P.dx[c][q];
+}
+
 // ---------------------------------------------------------------------------------------
 // K5  FTLE (compute_ftle, src/lcs_m.f90:66-193 with grad_sr1, src/gradient_m.f90:11-66):
 // central differences of the composed displacement map (face ghosts: periodic image, or

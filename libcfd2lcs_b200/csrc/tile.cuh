@@ -17,6 +17,8 @@
 // the same FMA sequence (spline_contract), so the result is bitwise that of k_sl_subcycle.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (the descriptor type only; maps are encoded by the engine)
+
 #include "kernels.cuh"
 
 namespace cfd2lcs {
@@ -66,6 +68,16 @@ __device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, unsign
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
                "l"(src), "r"(bytes), "r"(smem_addr(bar))
                : "memory");
+}
+
+// one 3-D box of a tensor map (coordinates x, y, z in elements; out-of-range parts read as 0)
+// to 128-byte aligned shared dst
+__device__ __forceinline__ void tensor_copy_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+          smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+      : "memory");
 }
 
 // orders this thread's earlier shared-memory accesses before later bulk copies into them
@@ -136,6 +148,35 @@ __device__ __forceinline__ void tile_fill(TC *buf, const TC *f0, const TC *f1, c
       mbar_arrive(bar);
     }
   }
+}
+
+// Tensor maps of the staged fields of one launch (the engine encodes them; `on` = 0: copy the
+// boxes row by row instead).  A map describes one padded component as a 3-D array with box
+// (pitch, SY, SZ); it exists only where a row of the array is a multiple of 16 bytes, and then
+// every row has the same alignment shift (xlo mod 16/sizeof), so a box copied from x0 = xlo
+// rounded down to 16 bytes lands each element exactly where tile_index expects it.
+struct TileMaps {
+  CUtensorMap m[12];
+  int on;
+};
+
+// The 3-component field of maps m[0..2] into buf: one box copy per component, all issued by
+// thread 0, which arrives once on bar with their bytes.
+template <typename G, typename TC>
+__device__ __forceinline__ void tile_fill_tensor(TC *buf, const CUtensorMap *m, const TileBox &b, uint64_t *bar, int tid) {
+  if (tid != 0) return;
+  constexpr int E = 16 / (int)sizeof(TC);
+  constexpr unsigned bytes = (unsigned)(G::ROWS * G::template pitch<TC>() * sizeof(TC));
+  mbar_arrive_expect_tx(bar, 3 * bytes);
+  const int x0 = b.xlo & ~(E - 1);
+#pragma unroll
+  for (int c = 0; c < 3; c++) tensor_copy_3d(buf + (size_t)c * G::template comp<TC>(), m + c, x0, b.ys, b.zs, bar);
+}
+
+// 128-byte aligned start of the dynamic shared memory (box copies need it); launches ask for
+// 128 bytes more than their boxes
+__device__ __forceinline__ unsigned char *smem_aligned128(unsigned char *p) {
+  return reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(p) + 127) & ~(uintptr_t)127);
 }
 
 // shared-memory index of padded element (x, y, z) of a staged component
@@ -274,8 +315,10 @@ __device__ __forceinline__ void slt_sample2(const DevGrid<T> &g, const SplineAxe
 
 template <typename T, typename TV, int INTEG, bool HAS_FLAGS>
 __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLT_MINB)
-    k_sl_tile(DevGrid<T> g, SplineAxes<T> sa, VelFields<TV> V, FieldPtrs<T> fmo, FieldPtrsW<T> fmn, StageTimes S, T dt, int *err) {
-  extern __shared__ __align__(128) unsigned char slt_smem[];
+    k_sl_tile(DevGrid<T> g, SplineAxes<T> sa, VelFields<TV> V, FieldPtrs<T> fmo, FieldPtrsW<T> fmn, StageTimes S, T dt, int *err,
+              const __grid_constant__ TileMaps tm) {
+  extern __shared__ __align__(128) unsigned char slt_smem_raw[];
+  unsigned char *const slt_smem = smem_aligned128(slt_smem_raw);
   __shared__ __align__(8) uint64_t bar;
   constexpr bool UNI = !std::is_same<T, TV>::value;
   constexpr int NOFF = INTEG == RK2_ ? 1 : (INTEG == RK3_ ? 2 : (INTEG == RK4_ ? 3 : 0));  // stages off the node
@@ -286,10 +329,20 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLT_MINB)
   const int I0 = 1 + (int)blockIdx.x * SLT_X, J0 = 1 + (int)blockIdx.y * SLT_Y, K0 = 1 + (int)blockIdx.z * SLT_Z;
   TV *const tv = reinterpret_cast<TV *>(slt_smem);
   T *const tf = reinterpret_cast<T *>(slt_smem);
-  if (tid == 0) mbar_init(&bar, 3 * CubicGeom::ROWS);
+  if (tid == 0) mbar_init(&bar, tm.on ? 1 : 3 * CubicGeom::ROWS);
   __syncthreads();
-  if (NOFF > 0) tile_fill<CubicGeom, TV>(tv, V.cs[1][0], V.cs[1][1], V.cs[1][2], b, sx, sxy, &bar, tid, SLT_THREADS);
-  else tile_fill<CubicGeom, T>(tf, fmo.f[0], fmo.f[1], fmo.f[2], b, sx, sxy, &bar, tid, SLT_THREADS);
+  // field f: the blend of off-node stage f + 1 (f < NOFF), then the flow map (f = NOFF); maps 3f..3f+2
+  auto fill = [&](int f) {
+    if (tm.on) {
+      if (f < NOFF) tile_fill_tensor<CubicGeom, TV>(tv, tm.m + 3 * f, b, &bar, tid);
+      else tile_fill_tensor<CubicGeom, T>(tf, tm.m + 3 * f, b, &bar, tid);
+    } else if (f < NOFF) {
+      tile_fill<CubicGeom, TV>(tv, V.cs[f + 1][0], V.cs[f + 1][1], V.cs[f + 1][2], b, sx, sxy, &bar, tid, SLT_THREADS);
+    } else {
+      tile_fill<CubicGeom, T>(tf, fmo.f[0], fmo.f[1], fmo.f[2], b, sx, sxy, &bar, tid, SLT_THREADS);
+    }
+  };
+  fill(0);
 
   // the thread's two nodes: vertical neighbours (i, j, k) and (i, j, k + 1)
   const int i = I0 + (int)threadIdx.x, j = J0 + (int)threadIdx.y;
@@ -360,8 +413,7 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLT_MINB)
     }
     __syncthreads();  // every thread is done reading the box
     fence_proxy_async_smem();
-    if (s < NOFF) tile_fill<CubicGeom, TV>(tv, V.cs[s + 1][0], V.cs[s + 1][1], V.cs[s + 1][2], b, sx, sxy, &bar, tid, SLT_THREADS);
-    else tile_fill<CubicGeom, T>(tf, fmo.f[0], fmo.f[1], fmo.f[2], b, sx, sxy, &bar, tid, SLT_THREADS);
+    fill(s);
   }
   if (alive) {
     // departure points (xs now holds x): 2-D projection, particle BC, stick
@@ -429,8 +481,10 @@ __host__ __device__ constexpr size_t sll_bytes() {
 
 template <typename T, typename TV, int INTEG, bool HAS_FLAGS>
 __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLL_MINB)
-    k_sl_tile_lin(DevGrid<T> g, VelFields<TV> V, FieldPtrs<T> fmo, FieldPtrsW<T> fmn, StageTimes S, T dt, int *err) {
-  extern __shared__ __align__(128) unsigned char sll_smem[];
+    k_sl_tile_lin(DevGrid<T> g, VelFields<TV> V, FieldPtrs<T> fmo, FieldPtrsW<T> fmn, StageTimes S, T dt, int *err,
+                  const __grid_constant__ TileMaps tm) {
+  extern __shared__ __align__(128) unsigned char sll_smem_raw[];
+  unsigned char *const sll_smem = smem_aligned128(sll_smem_raw);
   __shared__ __align__(8) uint64_t bar;
   constexpr int NOFF = INTEG == RK2_ ? 1 : (INTEG == RK3_ ? 2 : (INTEG == RK4_ ? 3 : 0));
   const T HALF = T(1) / T(2), THIRD = T(1) / T(3), TWOTHIRD = T(2) / T(3), SIXTH = T(1) / T(6), TWO = T(2);
@@ -440,11 +494,17 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLL_MINB)
   TV *const su0 = reinterpret_cast<TV *>(sll_smem);
   TV *const su1 = su0 + 3 * LinGeom::comp<TV>();
   T *const sf = reinterpret_cast<T *>(sll_smem + (size_t)6 * LinGeom::comp<TV>() * sizeof(TV));
-  if (tid == 0) mbar_init(&bar, 9 * LinGeom::ROWS);
+  if (tid == 0) mbar_init(&bar, tm.on ? 3 : 9 * LinGeom::ROWS);
   __syncthreads();
-  tile_fill<LinGeom, TV>(su0, V.un[0], V.un[1], V.un[2], b, sx, sxy, &bar, tid, SLT_THREADS);
-  tile_fill<LinGeom, TV>(su1, V.unp1[0], V.unp1[1], V.unp1[2], b, sx, sxy, &bar, tid, SLT_THREADS);
-  tile_fill<LinGeom, T>(sf, fmo.f[0], fmo.f[1], fmo.f[2], b, sx, sxy, &bar, tid, SLT_THREADS);
+  if (tm.on) {  // maps 0-2: u_n, 3-5: u_np1, 6-8: flow map
+    tile_fill_tensor<LinGeom, TV>(su0, tm.m, b, &bar, tid);
+    tile_fill_tensor<LinGeom, TV>(su1, tm.m + 3, b, &bar, tid);
+    tile_fill_tensor<LinGeom, T>(sf, tm.m + 6, b, &bar, tid);
+  } else {
+    tile_fill<LinGeom, TV>(su0, V.un[0], V.un[1], V.un[2], b, sx, sxy, &bar, tid, SLT_THREADS);
+    tile_fill<LinGeom, TV>(su1, V.unp1[0], V.unp1[1], V.unp1[2], b, sx, sxy, &bar, tid, SLT_THREADS);
+    tile_fill<LinGeom, T>(sf, fmo.f[0], fmo.f[1], fmo.f[2], b, sx, sxy, &bar, tid, SLT_THREADS);
+  }
 
   const int I0 = 1 + (int)blockIdx.x * LinGeom::TX, J0 = 1 + (int)blockIdx.y * LinGeom::TY, K0 = 1 + (int)blockIdx.z * LinGeom::TZ;
   const int i = I0 + (int)threadIdx.x, j = J0 + (int)threadIdx.y;
@@ -649,8 +709,9 @@ __device__ __forceinline__ void tile_sample1(const DevGrid<T> &g, const SplineAx
 template <typename T, typename TV, int INTEG, bool HAS_FLAGS>
 __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_FWT_MINB)
     k_fwd_tile(DevGrid<T> g, SplineAxes<T> sa, VelFields<TV> V, Particles<T> P, StageTimes S, T dt, const int *offs, const int *tsum,
-               SortTiles st, int np, int *err) {
-  extern __shared__ __align__(128) unsigned char fwt_smem[];
+               SortTiles st, int np, int *err, const __grid_constant__ TileMaps tm) {
+  extern __shared__ __align__(128) unsigned char fwt_smem_raw[];
+  unsigned char *const fwt_smem = smem_aligned128(fwt_smem_raw);
   __shared__ __align__(8) uint64_t bar;
   constexpr bool UNI = !std::is_same<T, TV>::value;
   constexpr int NS = INTEG == RK2_ ? 2 : (INTEG == RK3_ ? 3 : (INTEG == RK4_ ? 4 : 1));  // samples per step
@@ -663,12 +724,17 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_FWT_MINB)
   const TileBox b = tile_box_at<FwdGeom>(g, tx, ty, tz);
   const int tid = threadIdx.x, sx = g.P.sx, sxy = g.P.sxy;
   TV *const tv = reinterpret_cast<TV *>(fwt_smem);
-  if (tid == 0) mbar_init(&bar, 3 * FwdGeom::ROWS);
+  if (tid == 0) mbar_init(&bar, tm.on ? 1 : 3 * FwdGeom::ROWS);
   __syncthreads();
+  // the blend of stage s (maps 3s..3s+2)
+  auto fill = [&](int s) {
+    if (tm.on) tile_fill_tensor<FwdGeom, TV>(tv, tm.m + 3 * s, b, &bar, tid);
+    else tile_fill<FwdGeom, TV>(tv, V.cs[s][0], V.cs[s][1], V.cs[s][2], b, sx, sxy, &bar, tid, SLT_THREADS);
+  };
   unsigned parity = 0;
   bool alive = true;
   for (int r0 = start; r0 < end && alive; r0 += 2 * SLT_THREADS) {  // rounds of 512 particles (block-uniform)
-    tile_fill<FwdGeom, TV>(tv, V.cs[0][0], V.cs[0][1], V.cs[0][2], b, sx, sxy, &bar, tid, SLT_THREADS);
+    fill(0);
     const int qs[2] = {r0 + tid, r0 + SLT_THREADS + tid};
     bool ok[2];
     T xn[2][3], xs[2][3], acc[2][3];
@@ -731,7 +797,7 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_FWT_MINB)
       }
       __syncthreads();  // every thread is done reading the box
       fence_proxy_async_smem();
-      if (s + 1 < NS) tile_fill<FwdGeom, TV>(tv, V.cs[s + 1][0], V.cs[s + 1][1], V.cs[s + 1][2], b, sx, sxy, &bar, tid, SLT_THREADS);
+      if (s + 1 < NS) fill(s + 1);
     }
     if (!alive) break;
     // project, particle BC, stick, displacement, one node-search pass, periodic wrap

@@ -27,16 +27,18 @@ def gpu_sp():
     return L.Cfd2lcs("sp")
 
 
-def _run(gpu, case, integrator, staged, n=None, steps=None, mixed=False, dirs=(SC.FTLE_BKWD,), interp=3):
+def _run(gpu, case, integrator, staged, n=None, steps=None, mixed=False, dirs=(SC.FTLE_BKWD,), interp=3, env=None):
     # 2 also stages the LINEAR backward kernel (off by default: slower than its gathering form)
-    os.environ["CFD2LCS_B200_SL_TILE"] = "2" if staged else "0"
+    extra = dict(env or {}, CFD2LCS_B200_SL_TILE="2" if staged else "0")
+    os.environ.update(extra)
     try:
         gpu.reset()
         if mixed:
             gpu.set_option("MIXED_PRECISION", 1)
         _, hs = SC.run(gpu, case, dirs, integrator, interp, n=n, steps=steps)
     finally:
-        os.environ.pop("CFD2LCS_B200_SL_TILE", None)
+        for k in extra:
+            os.environ.pop(k, None)
     err, msg = gpu.error()
     assert err == 0, msg
     return [gpu.flowmap(h) for h in hs], [gpu.ftle(h) for h in hs], gpu.counters(), gpu.staged_launches()
@@ -115,4 +117,39 @@ def test_staged_both_directions(gpu_dp):
     fb, tb, _, _ = _run(gpu_dp, "abc", 3, False, n=38, steps=14, dirs=(SC.FTLE_FWD, SC.FTLE_BKWD))
     assert sa["sl"] > 0 and sa["fwd"] > 0
     for x, y in zip(fa + ta, fb + tb):
+        assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("dirs", [(SC.FTLE_BKWD,), (SC.FTLE_FWD,)])
+def test_staged_row_copies(gpu_dp, dirs):
+    """The boxes copied row by row (CFD2LCS_B200_TMA_TENSOR=0) instead of one tensor-map box per
+    component: the same bits."""
+    _same(gpu_dp, "abc", 3, n=38, steps=14, dirs=dirs, env={"CFD2LCS_B200_TMA_TENSOR": "0"})
+
+
+@pytest.mark.parametrize("dirs", [(SC.FTLE_BKWD,), (SC.FTLE_FWD,)])
+def test_staged_odd_pitch(gpu_dp, dirs):
+    """37^3: a padded row of 39 FP64 values is not a multiple of 16 bytes, so no tensor map
+    exists and the rows are copied with their per-row alignment shifts."""
+    _same(gpu_dp, "abc", 3, n=37, steps=14, dirs=dirs)
+
+
+def test_tuner_decides_and_keeps_bits(gpu_dp):
+    """The default mode times both forms of each kernel on the first launches and keeps the
+    faster: it reaches a choice for the backward and the forward kernel, and the run is bitwise
+    the gathering-only run whichever it chose."""
+    os.environ["CFD2LCS_B200_SL_TILE"] = "1"
+    try:
+        gpu_dp.reset()
+        _, hs = SC.run(gpu_dp, "abc", (SC.FTLE_FWD, SC.FTLE_BKWD), 3, 3, n=38, steps=14)
+    finally:
+        os.environ.pop("CFD2LCS_B200_SL_TILE", None)
+    err, msg = gpu_dp.error()
+    assert err == 0, msg
+    tu = gpu_dp.tuning()
+    out = [gpu_dp.flowmap(h) for h in hs] + [gpu_dp.ftle(h) for h in hs]
+    assert tu["bkwd"] in (0, 1) and tu["fwd"] in (0, 1), tu
+    assert min(tu["bkwd_ms"]) > 0 and min(tu["fwd_ms"]) > 0, tu
+    fb, tb, _, _ = _run(gpu_dp, "abc", 3, False, n=38, steps=14, dirs=(SC.FTLE_FWD, SC.FTLE_BKWD))
+    for x, y in zip(out, fb + tb):
         assert np.array_equal(x, y)
