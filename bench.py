@@ -101,6 +101,9 @@ WORKLOADS = {
                        desc="ABC flow 192^3 periodic, dt=0.05, FTLE fwd T=2 h=1, RK3, cubic B-spline (profiling case)"),
     "abcproflin": dict(kind="abc", n=192, dt=0.05, T=2.0, h=1.0, integrator=2, interpolator=1, dirs=(1,), t0=0.95,
                        desc="ABC flow 192^3 periodic, dt=0.05, FTLE bkwd T=2 h=1, RK2, linear (profiling case)"),
+    # profiling case for the FTLE-field phase: frames of 10 sub-flow maps after 22 updates
+    "abcring": dict(kind="abc", n=128, dt=0.05, T=1.0, h=0.1, integrator=3, interpolator=3, dirs=(0, 1), t0=0.95,
+                    desc="ABC flow 128^3 periodic, dt=0.05, FTLE fwd+bkwd T=1 h=0.1, RK3, cubic B-spline (profiling case)"),
     "abc256lin": dict(kind="abc", n=256, dt=0.05, T=10.0, h=1.0, integrator=2, interpolator=1, dirs=(0, 1), t0=0.95,
                       desc="ABC flow 256^3 periodic, dt=0.05, FTLE fwd+bkwd T=10 h=1, RK2, linear"),
     "dg512": dict(kind="dg", n=512, dt=0.1, T=15.0, h=1.5, integrator=2, interpolator=1, dirs=(1,), t0=1.4,

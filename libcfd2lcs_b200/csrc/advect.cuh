@@ -366,16 +366,22 @@ __device__ __forceinline__ void integrate(const DevGrid<T> &g, const SplineAxes<
 // it moved outward; INFLOW/OUTFLOW boundary nodes stick it to the node.
 // Returns true when the particle sticks.
 // ---------------------------------------------------------------------------------------
+// (the singleton axis is selected by an unrolled comparison, not used as an index, so the
+// position and node arrays stay in registers)
 template <typename T>
 __device__ __forceinline__ void project_plane(const DevGrid<T> &g, int no[3], T x[3]) {
-  const int a = g.P.single_axis;
-  if (a < 0) return;
-  no[a] = 1;
-  const T plane = __ldg(g.lt[a] + 1);
-  T d = x[a] - plane;
-  const T dist = d < T(0) ? -d : d;
-  const T nrm = d < T(0) ? T(-1) : T(1);
-  x[a] = x[a] - dist * nrm;
+  const int sa = g.P.single_axis;
+  if (sa < 0) return;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    if (a != sa) continue;
+    no[a] = 1;
+    const T plane = __ldg(g.lt[a] + 1);
+    T d = x[a] - plane;
+    const T dist = d < T(0) ? -d : d;
+    const T nrm = d < T(0) ? T(-1) : T(1);
+    x[a] = x[a] - dist * nrm;
+  }
 }
 
 template <typename T, bool HAS_FLAGS>
