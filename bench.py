@@ -104,6 +104,8 @@ WORKLOADS = {
     # profiling case for the FTLE-field phase: frames of 10 sub-flow maps after 22 updates
     "abcring": dict(kind="abc", n=128, dt=0.05, T=1.0, h=0.1, integrator=3, interpolator=3, dirs=(0, 1), t0=0.95,
                     desc="ABC flow 128^3 periodic, dt=0.05, FTLE fwd+bkwd T=1 h=0.1, RK3, cubic B-spline (profiling case)"),
+    "abcring256": dict(kind="abc", n=256, dt=0.05, T=1.0, h=0.1, integrator=3, interpolator=3, dirs=(0, 1), t0=0.95,
+                       desc="ABC flow 256^3 periodic, dt=0.05, FTLE fwd+bkwd T=1 h=0.1, RK3, cubic B-spline (FTLE-field case)"),
     "abc256lin": dict(kind="abc", n=256, dt=0.05, T=10.0, h=1.0, integrator=2, interpolator=1, dirs=(0, 1), t0=0.95,
                       desc="ABC flow 256^3 periodic, dt=0.05, FTLE fwd+bkwd T=10 h=1, RK2, linear"),
     "dg512": dict(kind="dg", n=512, dt=0.1, T=15.0, h=1.5, integrator=2, interpolator=1, dirs=(1,), t0=1.4,
@@ -541,7 +543,7 @@ def run_b200(args, w):
     # workload's full horizon (the ABC flow: 201 updates at 256^3)
     with_mixed = args.precision == "fp64" and args.mixed == "on" or (args.mixed == "auto" and args.precision == "fp64"
                                                                       and w["kind"] == "abc" and world == 1)
-    horizon = full_frame_update(w) if with_mixed else None
+    horizon = full_frame_update(w) if (with_mixed or args.full_frame) else None
     r = run_form(args, w, args.precision, local, world, rank, clocks=True, e2e=True, horizon=horizon)
     api = r["api"]
     fp64_peak = fp64_fma_tflops() if w["interpolator"] in (2, 3) and args.precision == "fp64" else None
@@ -855,6 +857,7 @@ def main():
                     help="also time the mixed form and state its FTLE error against this run's FP64 path over the full horizon "
                          "(auto: the ABC workloads on one GPU)")
     ap.add_argument("--n", type=int, default=None, help="override the grid size (smaller smoke runs)")
+    ap.add_argument("--full-frame", action="store_true", help="run on to the full-horizon frame and time its FTLE field")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     if args.workload == "adj128":

@@ -235,6 +235,8 @@ class Engine : public EngineBase {
     if (const char *e = std::getenv("CFD2LCS_B200_LINEAR_BLEND_MIN")) lin_blend_min_ = std::atol(e);
     if (const char *e = std::getenv("CFD2LCS_B200_TMA_TENSOR")) tma_tensor_ = std::atoi(e) != 0;
     if (const char *e = std::getenv("CFD2LCS_B200_COMPOSE_SORT_MIN")) compose_sort_min_ = std::atol(e);
+    if (const char *e = std::getenv("CFD2LCS_B200_COMPOSE_SORT_EVERY")) compose_sort_every_ = std::max(1, std::atoi(e));
+    if (const char *e = std::getenv("CFD2LCS_B200_COMPOSE_MINB")) compose_minb_ = std::atoi(e) >= 4 ? 4 : 2;
     if (const char *e = std::getenv("CFD2LCS_B200_SL_TILE")) tile_mode_ = std::max(0, std::min(2, std::atoi(e)));
     for (int a = 0; a < 3; a++) n_[a] = n[a];
     // coordinate lines and interior flags for the output files (the grid is a tensor product)
@@ -351,6 +353,13 @@ class Engine : public EngineBase {
 #define CFD2LCS_COMPOSE_SORT_MIN (1L << 20)
 #endif
   long compose_sort_min_ = CFD2LCS_COMPOSE_SORT_MIN;
+  // Re-sort every this many sub-maps, and resident blocks per SM of k_compose_step (2 or 4;
+  // CFD2LCS_B200_COMPOSE_SORT_EVERY / _MINB override them).  Measured on B200, ABC 256^3 RK3
+  // CUBIC, frames of 10 sub-maps with h = 0.1 (ms per frame): node-ordered k_compose 34.8; steps
+  // with 2 blocks, sorted every sub-map 39.5; 4 blocks: every sub-map 35.2, every 2nd 34.2, every
+  // 3rd 33.6.  With h = 1 (sub-maps that move points ~120 cells, the ABC 256^3 T = 10 workload)
+  // the node-ordered kernel took 72.6 and the steps sorted every sub-map (2 blocks) 69.0.
+  int compose_sort_every_ = 2, compose_minb_ = 4;
   // the composition particles of every solver-grid frame (one frame at a time uses them)
   Particles<T> cp_[2]{};
   unsigned *cp_key_ = nullptr;
@@ -1805,7 +1814,7 @@ class Engine : public EngineBase {
     bool ok = true;
     for (int st = 0; st < ns && ok; st++) ok = tensor_maps3<FwdGeom, TV>(V.cs[st], tm.m + 3 * st);
     tm.on = ok ? 1 : 0;
-    k_fwd_tile<T, TV, IG, F><<<(unsigned)ntiles, SLT_THREADS, smem, stream_>>>(dg_, sa, V, d.P, S, dt, d.poffs, d.ptsum, d.sort_geom,
+    k_fwd_tile<T, TV, IG, F><<<(unsigned)ntiles, FWT_THREADS, smem, stream_>>>(dg_, sa, V, d.P, S, dt, d.poffs, d.ptsum, d.sort_geom,
                                                                               (int)dN(d), &red_->err, tm);
   }
 
@@ -1857,13 +1866,14 @@ class Engine : public EngineBase {
     counters_.kernel_launches++;
     int cur = 0;
     for (int s = 0; s < m; s++) {
-      if (s > 0) {
+      if (s > 0 && s % compose_sort_every_ == 0) {
         sort_slots(cp_[cur], cp_[cur ^ 1], cp_key_, cp_cnt_, cp_offs_, cp_tsum_, np, st, dummy);
         cur ^= 1;
       }
       FieldPtrs<T> f{};
       for (int c = 0; c < 3; c++) f.f[c] = d.slot_list_host[3 * s + c];
-      k_compose_step<T, I, FL><<<grd, 256, 0, stream_>>>(dg_, sa, f, cp_[cur], np, err);
+      if (compose_minb_ == 4) k_compose_step<T, I, FL, 4><<<grd, 256, 0, stream_>>>(dg_, sa, f, cp_[cur], np, err);
+      else k_compose_step<T, I, FL, 2><<<grd, 256, 0, stream_>>>(dg_, sa, f, cp_[cur], np, err);
       counters_.kernel_launches++;
     }
     k_compose_finish<T, FL><<<grd, 256, 0, stream_>>>(dg_, cp_[cur], out, np);

@@ -469,8 +469,9 @@ __global__ void __launch_bounds__(256) k_compose(DevGrid<T> g, SplineAxes<T> sa,
 // are far apart and the node-ordered k_compose gathers each tap sector from HBM.  The per-point
 // sequence is k_compose's loop body, the state kept exactly between steps, so the composed map
 // is bitwise k_compose's.  k_reset_particles starts the particles at their nodes.
-template <typename T, int INTERP, bool HAS_FLAGS>
-__global__ void __launch_bounds__(256) k_compose_step(DevGrid<T> g, SplineAxes<T> sa, FieldPtrs<T> f, Particles<T> P, int np, int *err) {
+// MINB: resident blocks of 256 threads per SM asked of the compiler (register cap 65536 / (256 MINB))
+template <typename T, int INTERP, bool HAS_FLAGS, int MINB = 2>
+__global__ void __launch_bounds__(256, MINB) k_compose_step(DevGrid<T> g, SplineAxes<T> sa, FieldPtrs<T> f, Particles<T> P, int np, int *err) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= np) return;
   T x[3] = {P.x[0][q], P.x[1][q], P.x[2][q]};

@@ -702,12 +702,15 @@ __device__ __forceinline__ void tile_sample1(const DevGrid<T> &g, const SplineAx
   }
 }
 
+// One particle per thread in blocks of 512 (a tile holds about 256 particles, so a round rarely
+// repeats), 2 resident blocks (64 registers) per SM: 32 warps, as the gathering kernel runs.
+constexpr int FWT_THREADS = 512, FWT_PPT = 1;
 #ifndef CFD2LCS_FWT_MINB
 #define CFD2LCS_FWT_MINB 2
 #endif
 
 template <typename T, typename TV, int INTEG, bool HAS_FLAGS>
-__global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_FWT_MINB)
+__global__ void __launch_bounds__(FWT_THREADS, CFD2LCS_FWT_MINB)
     k_fwd_tile(DevGrid<T> g, SplineAxes<T> sa, VelFields<TV> V, Particles<T> P, StageTimes S, T dt, const int *offs, const int *tsum,
                SortTiles st, int np, int *err, const __grid_constant__ TileMaps tm) {
   extern __shared__ __align__(128) unsigned char fwt_smem_raw[];
@@ -729,18 +732,19 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_FWT_MINB)
   // the blend of stage s (maps 3s..3s+2)
   auto fill = [&](int s) {
     if (tm.on) tile_fill_tensor<FwdGeom, TV>(tv, tm.m + 3 * s, b, &bar, tid);
-    else tile_fill<FwdGeom, TV>(tv, V.cs[s][0], V.cs[s][1], V.cs[s][2], b, sx, sxy, &bar, tid, SLT_THREADS);
+    else tile_fill<FwdGeom, TV>(tv, V.cs[s][0], V.cs[s][1], V.cs[s][2], b, sx, sxy, &bar, tid, FWT_THREADS);
   };
   unsigned parity = 0;
   bool alive = true;
-  for (int r0 = start; r0 < end && alive; r0 += 2 * SLT_THREADS) {  // rounds of 512 particles (block-uniform)
+  for (int r0 = start; r0 < end && alive; r0 += FWT_PPT * FWT_THREADS) {  // rounds (block-uniform)
     fill(0);
-    const int qs[2] = {r0 + tid, r0 + SLT_THREADS + tid};
-    bool ok[2];
-    T xn[2][3], xs[2][3], acc[2][3];
-    int no[2][3];
+    int qs[FWT_PPT];
+    bool ok[FWT_PPT];
+    T xn[FWT_PPT][3], xs[FWT_PPT][3], acc[FWT_PPT][3];
+    int no[FWT_PPT][3];
 #pragma unroll
-    for (int q = 0; q < 2; q++) {
+    for (int q = 0; q < FWT_PPT; q++) {
+      qs[q] = r0 + q * FWT_THREADS + tid;
       ok[q] = qs[q] < end;
       if (!ok[q]) continue;
 #pragma unroll
@@ -757,7 +761,7 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_FWT_MINB)
       if (!alive) continue;
       parity ^= 1u;
 #pragma unroll
-      for (int q = 0; q < 2; q++) {
+      for (int q = 0; q < FWT_PPT; q++) {
         if (!ok[q]) continue;
         T u[3];
         tile_sample1<FwdGeom, T, TV, UNI>(g, sa, b, tv, V.cs[s][0], V.cs[s][1], V.cs[s][2], xs[q], no[q], u);
@@ -802,7 +806,7 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_FWT_MINB)
     if (!alive) break;
     // project, particle BC, stick, displacement, one node-search pass, periodic wrap
 #pragma unroll
-    for (int q = 0; q < 2; q++) {
+    for (int q = 0; q < FWT_PPT; q++) {
       if (!ok[q]) continue;
       const int sl = qs[q];
       T *x = xs[q];
