@@ -98,8 +98,8 @@ void cfd2lcs_get_staged_launches_c(long long n[2]);
  * launches and keeps the faster (environment CFD2LCS_B200_SL_TILE at cfd2lcs_init: 0 gathering
  * only, 1 tuned, the default, 2 staged wherever it applies).  choice[0] backward, choice[1]
  * forward kernel: -1 while sampling or where staging does not apply, 0 gathering, 1 staged;
- * ms[0], ms[1] the mean backward launch times measured for gathering and staged, ms[2], ms[3]
- * the forward ones. */
+ * ms[0], ms[1] the shortest backward launch times measured for gathering and staged (each
+ * form's first launch left out), ms[2], ms[3] the forward ones. */
 void cfd2lcs_get_tuning_c(int choice[2], double ms[4]);
 
 /* Recomputes the latest FTLE frame of a diagnostic -- the composition of its stored
@@ -164,7 +164,7 @@ void cfd2lcs_batch_reset_c(void);
  * backward FTLE of the whole horizon (the frame the library computes with h = T, T = time of
  * the last level minus the first), with respect to the velocity at every level, by a
  * hand-written reverse sweep through the semi-Lagrangian updates (LINEAR interpolation;
- * integrator EULER, TRAPEZOIDAL or RK2) with a flow-map checkpoint every `checkpoint_every`
+ * integrator EULER, TRAPEZOIDAL, RK2 or RK3) with a flow-map checkpoint every `checkpoint_every`
  * updates.  Grid: rectilinear, three-dimensional, every direction periodic, no boundary
  * flags.  d_u[l], d_v[l], d_w[l]: device arrays of level l (n[0]*n[1]*n[2], i fastest);
  * times: host, increasing; d_weight: device, n[0]*n[1]*n[2].  Writes *J and, when d_gu,

@@ -268,7 +268,7 @@ class Cfd2lcs:
 
     def tuning(self) -> dict:
         """The staged-versus-gathering choice of the backward and forward subcycle kernels (-1
-        sampling or not applicable, 0 gathering, 1 staged) and the mean launch ms measured."""
+        sampling or not applicable, 0 gathering, 1 staged) and the shortest launch ms measured."""
         ch = np.zeros(2, dtype=np.int32)
         ms = np.zeros(4, dtype=np.float64)
         self.lib.cfd2lcs_get_tuning_c(self._p(ch), self._p(ms))

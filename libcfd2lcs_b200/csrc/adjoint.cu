@@ -43,7 +43,7 @@ namespace {
     }                                                                                            \
   } while (0)
 
-enum { EULER = 0, TRAPEZOIDAL = 1, RK2 = 2 };
+enum { EULER = 0, TRAPEZOIDAL = 1, RK2 = 2, RK3 = 3 };
 
 // device memory of one adjoint call
 class Pool {
@@ -125,9 +125,11 @@ __device__ __forceinline__ T dweight(const T t[3], int q, int a) {
 // field: the time blend is distributed onto the two levels afterwards by k_distribute), that
 // of the first stage, which sits on the node, to a1 (plain stores).
 // ---------------------------------------------------------------------------------------
+// RK3 (integrate_lp, src/lp_motion_m.f90:212-263, with the third stage at xn + 2 k2): the
+// third stage's velocity adjoint goes to a3 (scattered) and k_distribute takes its ct[2].
 template <typename T, int INTEG>
 __global__ void __launch_bounds__(256) k_sl_adjoint(DevGrid<T> g, VelFields<T> V, FieldPtrs<T> fmo, FieldPtrs<T> fbn, FieldPtrsW<T> fbo,
-                                                     FieldPtrsW<T> a1, FieldPtrsW<T> a2, StageTimes S, T dt) {
+                                                     FieldPtrsW<T> a1, FieldPtrsW<T> a2, FieldPtrsW<T> a3, StageTimes S, T dt) {
   int i, j, k;
   if (!node_of_thread(g.P.n, i, j, k)) return;
   const int p = pidx(g.P.sx, g.P.sxy, i, j, k);
@@ -141,10 +143,33 @@ __global__ void __launch_bounds__(256) k_sl_adjoint(DevGrid<T> g, VelFields<T> V
   T u1[3];
 #pragma unroll
   for (int c = 0; c < 3; c++) u1[c] = omc0 * __ldg(V.un[c] + p) + ct0 * __ldg(V.unp1[c] + p);
-  T x[3], xh[3];
-  LinStencilAD<T> s2;
+  T x[3], xh[3], xs3[3];
+  LinStencilAD<T> s2, s2b;
   const T ct1 = T(S.ct[1]), omc1 = T(1) - ct1;
-  if (INTEG == RK2) {
+  const T ct2 = T(S.ct[2]), omc2 = T(1) - ct2;
+  const T SIXTH = T(1) / T(6), TWOTHIRD = T(2) / T(3), TWO = T(2);
+  if (INTEG == RK3) {
+    T k[3], acc[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k[c] = dt * u1[c];
+      acc[c] = x0[c] + SIXTH * k[c];
+      xh[c] = x0[c] + HALF * k[c];
+    }
+    lin_stencil_ad(g, xh, no, s2);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k[c] = dt * lin_apply_blend<T, T>(s2.st, V.un[c], V.unp1[c], omc1, ct1);
+      xs3[c] = x0[c] + TWO * k[c];
+      acc[c] = acc[c] + TWOTHIRD * k[c];
+    }
+    lin_stencil_ad(g, xs3, no, s2b);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k[c] = dt * lin_apply_blend<T, T>(s2b.st, V.un[c], V.unp1[c], omc2, ct2);
+      x[c] = acc[c] + SIXTH * k[c];
+    }
+  } else if (INTEG == RK2) {
 #pragma unroll
     for (int c = 0; c < 3; c++) xh[c] = x0[c] + HALF * dt * u1[c];
     lin_stencil_ad(g, xh, no, s2);
@@ -175,7 +200,43 @@ __global__ void __launch_bounds__(256) k_sl_adjoint(DevGrid<T> g, VelFields<T> V
   }
   // --- stages ---
   T u1b[3];
-  if (INTEG == RK2) {
+  // scatter of a sampled stage's velocity adjoint ub (weights of stencil st, blend omc/ct) into
+  // a, returning the adjoint of the sample position in pb
+  auto stage_back = [&](const LinStencilAD<T> &st, const T ub[3], FieldPtrsW<T> a, T omc, T ct, T pb[3]) {
+    pb[0] = pb[1] = pb[2] = T(0);
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int cq = corner(st.st, q);
+      const T wq = st.st.w[q];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        atomicAdd(a.f[c] + cq, wq * ub[c]);
+        const T vb = omc * __ldg(V.un[c] + cq) + ct * __ldg(V.unp1[c] + cq);
+#pragma unroll
+        for (int d = 0; d < 3; d++) pb[d] += ub[c] * dweight(st.t, q, d) * st.dtdx[d] * vb;
+      }
+    }
+  };
+  if (INTEG == RK3) {
+    // x = xn + k1/6 + 2 k2/3 + k3/6, k3 = dt u(xs3), xs3 = xn + 2 k2, k2 = dt u(xh), xh = xn + k1/2
+    T k3b[3], k2b[3], k1b[3], ub[3], pb[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k3b[c] = SIXTH * xb[c];
+      k2b[c] = TWOTHIRD * xb[c];
+      k1b[c] = SIXTH * xb[c];
+      ub[c] = dt * k3b[c];
+    }
+    stage_back(s2b, ub, a3, omc2, ct2, pb);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k2b[c] += TWO * pb[c];
+      ub[c] = dt * k2b[c];
+    }
+    stage_back(s2, ub, a2, omc1, ct1, pb);
+#pragma unroll
+    for (int c = 0; c < 3; c++) u1b[c] = dt * (k1b[c] + HALF * pb[c]);
+  } else if (INTEG == RK2) {
     T u2b[3], xhb[3] = {T(0), T(0), T(0)};
 #pragma unroll
     for (int c = 0; c < 3; c++) u2b[c] = dt * xb[c];
@@ -203,16 +264,23 @@ __global__ void __launch_bounds__(256) k_sl_adjoint(DevGrid<T> g, VelFields<T> V
 
 // velocity adjoint of one subcycle onto the two levels: un += (1-ct0) a1 + (1-ct1) a2,
 // unp1 += ct0 a1 + ct1 a2; a1 and a2 are cleared for the next subcycle
-template <typename T>
-__global__ void __launch_bounds__(256) k_distribute(FieldPtrsW<T> a1, FieldPtrsW<T> a2, FieldPtrsW<T> ubn, FieldPtrsW<T> ubp, T ct0, T ct1,
-                                                     long ntot) {
+// (three stage fields for RK3: a3 with ct2, else a3 is unused)
+template <typename T, bool THREE>
+__global__ void __launch_bounds__(256) k_distribute(FieldPtrsW<T> a1, FieldPtrsW<T> a2, FieldPtrsW<T> a3, FieldPtrsW<T> ubn,
+                                                     FieldPtrsW<T> ubp, T ct0, T ct1, T ct2, long ntot) {
   const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= ntot) return;
   const int c = blockIdx.y;
-  const T x1 = a1.f[c][q], x2 = a2.f[c][q];
-  if (x1 == T(0) && x2 == T(0)) return;
-  ubn.f[c][q] += (T(1) - ct0) * x1 + (T(1) - ct1) * x2;
-  ubp.f[c][q] += ct0 * x1 + ct1 * x2;
+  const T x1 = a1.f[c][q], x2 = a2.f[c][q], x3 = THREE ? a3.f[c][q] : T(0);
+  if (x1 == T(0) && x2 == T(0) && x3 == T(0)) return;
+  if (THREE) {
+    ubn.f[c][q] += (T(1) - ct0) * x1 + (T(1) - ct1) * x2 + (T(1) - ct2) * x3;
+    ubp.f[c][q] += ct0 * x1 + ct1 * x2 + ct2 * x3;
+    a3.f[c][q] = T(0);
+  } else {
+    ubn.f[c][q] += (T(1) - ct0) * x1 + (T(1) - ct1) * x2;
+    ubp.f[c][q] += ct0 * x1 + ct1 * x2;
+  }
   a1.f[c][q] = T(0);
   a2.f[c][q] = T(0);
 }
@@ -242,7 +310,56 @@ __global__ void __launch_bounds__(256) k_sl_tangent(DevGrid<T> g, VelFields<T> V
     du1[c] = omc0 * __ldg(D.un[c] + p) + ct0 * __ldg(D.unp1[c] + p);
   }
   T x[3], dx[3];
-  if (INTEG == RK2) {
+  // one LINEAR stage sample at xs (moved by dxs) of V (value) and of the direction D (tangent)
+  auto stage_tan = [&](const T xs[3], const T dxs[3], T omc, T ct, T u[3], T du[3]) {
+    LinStencilAD<T> st;
+    lin_stencil_ad(g, xs, no, st);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      u[c] = lin_apply_blend<T, T>(st.st, V.un[c], V.unp1[c], omc, ct);
+      du[c] = lin_apply_blend<T, T>(st.st, D.un[c], D.unp1[c], omc, ct);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int cq = corner(st.st, q);
+      T dwq = T(0);
+#pragma unroll
+      for (int d = 0; d < 3; d++) dwq += dweight(st.t, q, d) * st.dtdx[d] * dxs[d];
+#pragma unroll
+      for (int c = 0; c < 3; c++) du[c] += dwq * (omc * __ldg(V.un[c] + cq) + ct * __ldg(V.unp1[c] + cq));
+    }
+  };
+  if (INTEG == RK3) {
+    const T SIXTH = T(1) / T(6), TWOTHIRD = T(2) / T(3), TWO = T(2);
+    const T ct1 = T(S.ct[1]), omc1 = T(1) - ct1, ct2 = T(S.ct[2]), omc2 = T(1) - ct2;
+    T k[3], dk[3], acc[3], dacc[3], xs[3], dxs[3], u[3], du[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k[c] = dt * u1[c];
+      dk[c] = dt * du1[c];
+      acc[c] = x0[c] + SIXTH * k[c];
+      dacc[c] = SIXTH * dk[c];
+      xs[c] = x0[c] + HALF * k[c];
+      dxs[c] = HALF * dk[c];
+    }
+    stage_tan(xs, dxs, omc1, ct1, u, du);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k[c] = dt * u[c];
+      dk[c] = dt * du[c];
+      xs[c] = x0[c] + TWO * k[c];
+      dxs[c] = TWO * dk[c];
+      acc[c] = acc[c] + TWOTHIRD * k[c];
+      dacc[c] = dacc[c] + TWOTHIRD * dk[c];
+    }
+    stage_tan(xs, dxs, omc2, ct2, u, du);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k[c] = dt * u[c];
+      x[c] = acc[c] + SIXTH * k[c];
+      dx[c] = dacc[c] + SIXTH * (dt * du[c]);
+    }
+  } else if (INTEG == RK2) {
     const T ct1 = T(S.ct[1]), omc1 = T(1) - ct1;
     T xh[3], dxh[3];
 #pragma unroll
@@ -494,8 +611,8 @@ class Adjoint {
       msg = "adjoint: at least two velocity levels are needed";
       return false;
     }
-    if (pr_.integrator != EULER && pr_.integrator != TRAPEZOIDAL && pr_.integrator != RK2) {
-      msg = "adjoint: the integrator must be EULER, TRAPEZOIDAL or RK2";
+    if (pr_.integrator != EULER && pr_.integrator != TRAPEZOIDAL && pr_.integrator != RK2 && pr_.integrator != RK3) {
+      msg = "adjoint: the integrator must be EULER, TRAPEZOIDAL, RK2 or RK3";
       return false;
     }
     if (pr_.checkpoint_every < 1 || !(pr_.cfl > 0)) {
@@ -601,6 +718,7 @@ class Adjoint {
     else {
       S.ct[0] = ct(t);
       S.ct[1] = ct(t + HALF * dt);
+      if (pr_.integrator == RK3) S.ct[2] = ct(t + dt);
     }
     return S;
   }
@@ -751,14 +869,18 @@ class Adjoint {
           dfo.f[c] = dfm_[cur][c];
           dfn.f[c] = dfm_[cur ^ 1][c];
         }
-        if (pr_.integrator == RK2)
+        if (pr_.integrator == RK3)
+          k_sl_tangent<T, RK3><<<grd, blk, 0, stream_>>>(dg_, V, D, fo, dfo, dfn, S, (T)dt);
+        else if (pr_.integrator == RK2)
           k_sl_tangent<T, RK2><<<grd, blk, 0, stream_>>>(dg_, V, D, fo, dfo, dfn, S, (T)dt);
         else
           k_sl_tangent<T, EULER><<<grd, blk, 0, stream_>>>(dg_, V, D, fo, dfo, dfn, S, (T)dt);
         k_periodic_ghosts<T><<<(unsigned)((ntot_ + 255) / 256), 256, 0, stream_>>>(dg_, dfn, ntot_);
         ACK(cudaGetLastError());
       }
-      if (pr_.integrator == RK2)
+      if (pr_.integrator == RK3)
+        k_sl_subcycle<T, T, RK3_, INTERP_LINEAR, false><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, (T)dt, err);
+      else if (pr_.integrator == RK2)
         k_sl_subcycle<T, T, RK2_, INTERP_LINEAR, false><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, (T)dt, err);
       else if (pr_.integrator == TRAPEZOIDAL)
         k_sl_subcycle<T, T, TRAPEZOIDAL_, INTERP_LINEAR, false><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, (T)dt, err);
@@ -791,14 +913,16 @@ class Adjoint {
     }
     const long nb = (ntot_ + 255) / 256;
     const int nseg = (L - 2) / K + 1;
-    // per-subcycle velocity adjoints of the two stages (zero between subcycles)
-    FieldPtrsW<T> A1{}, A2{};
+    // per-subcycle velocity adjoints of the stages (zero between subcycles; a third for RK3)
+    FieldPtrsW<T> A1{}, A2{}, A3{};
     {
-      T *a[3], *b[3];
+      T *a[3], *b[3], *e[3];
       if (!field3(a, msg) || !field3(b, msg)) return false;
+      if (pr_.integrator == RK3 && !field3(e, msg)) return false;
       for (int c = 0; c < 3; c++) {
         A1.f[c] = a[c];
         A2.f[c] = b[c];
+        A3.f[c] = pr_.integrator == RK3 ? e[c] : nullptr;
       }
     }
     // flow maps before every subcycle of the largest segment
@@ -855,11 +979,18 @@ class Adjoint {
             fbo.f[c] = fbar[fb ^ 1][c];
           }
           const StageTimes S = stage_times(t0, t1, lps[q], dt);
-          if (pr_.integrator == RK2)
-            k_sl_adjoint<T, RK2><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, V, fo, fbn, fbo, A1, A2, S, (T)dt);
+          if (pr_.integrator == RK3)
+            k_sl_adjoint<T, RK3><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, V, fo, fbn, fbo, A1, A2, A3, S, (T)dt);
+          else if (pr_.integrator == RK2)
+            k_sl_adjoint<T, RK2><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, V, fo, fbn, fbo, A1, A2, A3, S, (T)dt);
           else
-            k_sl_adjoint<T, EULER><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, V, fo, fbn, fbo, A1, A2, S, (T)dt);
-          k_distribute<T><<<dim3((unsigned)nb, 3), 256, 0, stream_>>>(A1, A2, ubn, ubp, (T)S.ct[0], (T)S.ct[1], ntot_);
+            k_sl_adjoint<T, EULER><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, V, fo, fbn, fbo, A1, A2, A3, S, (T)dt);
+          if (pr_.integrator == RK3)
+            k_distribute<T, true><<<dim3((unsigned)nb, 3), 256, 0, stream_>>>(A1, A2, A3, ubn, ubp, (T)S.ct[0], (T)S.ct[1], (T)S.ct[2],
+                                                                             ntot_);
+          else
+            k_distribute<T, false><<<dim3((unsigned)nb, 3), 256, 0, stream_>>>(A1, A2, A3, ubn, ubp, (T)S.ct[0], (T)S.ct[1], T(0),
+                                                                              ntot_);
           ACK(cudaGetLastError());
           fb ^= 1;
         }

@@ -1572,18 +1572,21 @@ class Engine : public EngineBase {
   // and the forward kernel (family 1) it alternates the two variants -- launch by launch, or
   // sort interval by sort interval for the forward kernel, whose staged variant needs its own
   // sort tiles -- times each launch with the CUDA events that bracket it, and once each variant
-  // has kTuneSamples launches keeps the one with the smaller mean for the rest of the engine's
+  // has kTuneSamples launches keeps the one with the shorter launch for the rest of the engine's
   // life (per instance: the batched form tunes every instance for its own grid and options).
   // Measured on B200, ABC 256^3 FP64 per launch: staged cubic backward 3.22 against 4.63 ms,
   // staged forward 8.39 against 6.68 ms, staged LINEAR backward 0.79 against 0.90 ms.
   // CFD2LCS_B200_SL_TILE at cfd2lcs_init: 0 = gathering kernels only, 1 = tuned (default),
   // 2 = staged kernels wherever they apply.  cfd2lcs_get_tuning_c reports the choices.
-  static constexpr int kTuneSamples = 4;
+  // Each variant's first launch is dropped and the rest compared by their minimum: a launch whose
+  // events also bracket host set-up (cudaFuncSetAttribute, the first encoding of a buffer's
+  // tensor map) while the GPU idles can only read long, and such launches come first.
+  static constexpr int kTuneSamples = 6;
   int tile_mode_ = 1;
   struct Tuner {
     int choice = -1;  // -1: sampling, 0: gathering, 1: staged
-    double ms[2] = {0, 0};
-    int n[2] = {0, 0};
+    double ms[2] = {1e300, 1e300};  // smallest launch time per variant
+    int n[2] = {0, 0};              // launches seen per variant
   } tune_[2];
   long tune_idx_[2] = {0, 0};
 
@@ -1596,16 +1599,16 @@ class Engine : public EngineBase {
 
   void tune_record(int tag, double ms) {
     Tuner &t = tune_[tag / 2];
+    const int v = tag % 2;
     if (t.choice >= 0) return;
-    t.ms[tag % 2] += ms;
-    t.n[tag % 2]++;
-    if (t.n[0] >= kTuneSamples && t.n[1] >= kTuneSamples) t.choice = t.ms[1] / t.n[1] < t.ms[0] / t.n[0] ? 1 : 0;
+    if (t.n[v]++ > 0) t.ms[v] = std::min(t.ms[v], ms);
+    if (t.n[0] > kTuneSamples && t.n[1] > kTuneSamples) t.choice = t.ms[1] < t.ms[0] ? 1 : 0;
   }
 
   void tuning(int choice[2], double ms[4]) const override {
     for (int f = 0; f < 2; f++) {
       choice[f] = tune_[f].choice;
-      for (int v = 0; v < 2; v++) ms[2 * f + v] = tune_[f].n[v] ? tune_[f].ms[v] / tune_[f].n[v] : 0.0;
+      for (int v = 0; v < 2; v++) ms[2 * f + v] = tune_[f].n[v] > 1 ? tune_[f].ms[v] : 0.0;
     }
   }
 

@@ -1,6 +1,7 @@
 """The adjoint (cfd2lcs_adjoint_ftle_c): its forward objective equals the library's own FTLE
 frame for h = T, its gradient agrees with central finite differences of that objective along
-random directions, and it does not depend on the checkpoint interval."""
+random directions and with the tangent-linear model (EULER, TRAPEZOIDAL, RK2 and RK3), and it
+does not depend on the checkpoint interval."""
 import math
 
 import numpy as np
@@ -34,7 +35,7 @@ def _weight(g):
     return torch.from_numpy(np.ascontiguousarray(w.ravel(order="F"))).cuda()
 
 
-@pytest.mark.parametrize("integrator", [0, 2])
+@pytest.mark.parametrize("integrator", [0, 2, 3])
 def test_forward_objective_is_the_library_frame(integrator):
     import libcfd2lcs_b200 as L
     n, nl, dt = 12, 9, 0.05
@@ -57,7 +58,7 @@ def test_forward_objective_is_the_library_frame(integrator):
     assert abs(J - J_lib) <= 1e-12 * max(abs(J_lib), 1e-30), (J, J_lib)
 
 
-@pytest.mark.parametrize("integrator", [0, 2])
+@pytest.mark.parametrize("integrator", [0, 2, 3])
 def test_gradient_matches_finite_differences(integrator):
     import torch
 
@@ -105,7 +106,7 @@ def test_adjoint_rejects_walled_grids():
         L.adjoint_ftle(g, u, u, u, [0.0, 0.1, 0.2], torch.zeros(16 * 8, dtype=torch.float64, device="cuda"))
 
 
-@pytest.mark.parametrize("integrator", [0, 1, 2])
+@pytest.mark.parametrize("integrator", [0, 1, 2, 3])
 def test_tangent_linear_model_matches_adjoint(integrator):
     """Dot-product test: the forward-mode sweep's dJ along a direction d equals <dJ/du, d> from
     the reverse sweep to rounding (both differentiate the same discrete map with the same
