@@ -118,7 +118,7 @@ WORKLOADS = {
 
 def make_grid(w, n=None):
     """(grid, host velocity(t) -> 3 numpy arrays, steady?)"""
-    from libcfd2lcs_b200 import workloads as W
+    from tests import workloads as W
     if w["kind"] == "abc":
         g = W.abc_grid(n or w["n"])
         vel = W.abc_velocity(g)
@@ -136,7 +136,7 @@ def turbulence_on_device(n, t, dev, chunk=16):
     host form takes minutes at 512^3): FP32 field values, returned as FP64 tensors in
     i-fastest order."""
     import torch
-    from libcfd2lcs_b200 import workloads as W
+    from tests import workloads as W
     modes = W.turbulence_modes()
     L = 2.0 * math.pi
     line = (torch.arange(n, device=dev, dtype=torch.float64) + 0.5) * (L / n)
@@ -592,7 +592,7 @@ def run_b200(args, w):
     if args.precision == "mixed" and w["kind"] == "abc" and args.acc_n > 0 and rank == 0:
         # FTLE error of the mixed form against the plain FP64 path on the same flow and options
         # at a smaller grid, full T
-        from libcfd2lcs_b200 import accuracy as A
+        from tests import accuracy as A
         acc = A.compare(args.acc_n, w["T"], w["h"], w["dt"], None, w["integrator"], w["interpolator"])
         line["ftle_error"] = {"form": "mixed (FP32 velocity data, FP64 positions / flow maps / FTLE)",
                               "vs": "plain FP64 GPU path", "case": acc["config"],
@@ -642,7 +642,7 @@ def run_batch(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
     import libcfd2lcs_b200 as L
-    from libcfd2lcs_b200 import workloads as W
+    from tests import workloads as W
     dev = torch.device("cuda", local)
     b = L.Batch("dp")
     b.reset()
@@ -746,7 +746,7 @@ def run_adjoint(args):
         return
     torch.cuda.set_device(local)
     import libcfd2lcs_b200 as L
-    from libcfd2lcs_b200 import workloads as W
+    from tests import workloads as W
     n = args.n or 128
     nl, dt, K = 201, 0.05, 20
     g = W.abc_grid(n)

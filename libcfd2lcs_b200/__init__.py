@@ -15,7 +15,6 @@ import os
 
 import numpy as np
 
-from . import workloads  # noqa: F401
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
@@ -111,6 +110,8 @@ def load(precision: str = "dp") -> C.CDLL:
     lib.cfd2lcs_reconstruct_noalloc_c.restype = C.c_int
     lib.cfd2lcs_b200_grid_tables.argtypes = [P, P, P, P, P, P, P, P, P, P, C.c_char_p, C.c_size_t]
     lib.cfd2lcs_b200_grid_tables.restype = C.c_int
+    lib.cfd2lcs_b200_grid_lsq_weights.argtypes = [P, P, P, P, P, P, P, C.c_char_p, C.c_size_t]
+    lib.cfd2lcs_b200_grid_lsq_weights.restype = C.c_int
     lib.cfd2lcs_batch_add_c.argtypes = [P, P, P, P, P, C.c_int, C.c_int, R, C.c_int]
     lib.cfd2lcs_batch_add_c.restype = C.c_int
     lib.cfd2lcs_batch_diagnostic_init_c.argtypes = [C.c_int, C.c_int, R, R]
@@ -305,6 +306,23 @@ class Cfd2lcs:
             inv_delta=inv.reshape((3,) + shp).transpose(0, 3, 2, 1),
             periodic=per.astype(bool),
         )
+
+    def grid_lsq_weights(self, n, x, y, z, flag):
+        """Host-only: (curvilinear, weights) with the least-squares gradient weights of a
+        non-rectilinear grid, shape (6 face neighbours, 3 derivatives, ni+2, nj+2, nk+2)."""
+        n = np.ascontiguousarray(n, dtype=np.int32)
+        x, y, z = self._r(x), self._r(y), self._r(z)
+        f = np.asfortranarray(flag, dtype=np.int32).ravel(order="F")
+        nt = int(np.prod(np.asarray(n) + 2))
+        w = np.zeros(18 * nt, dtype=self.dtype)
+        curv = C.c_int(0)
+        msg = C.create_string_buffer(512)
+        rc = self.lib.cfd2lcs_b200_grid_lsq_weights(self._p(n), self._p(x), self._p(y), self._p(z), self._p(f), self._p(w),
+                                                    C.byref(curv), msg, 512)
+        if rc != 0:
+            raise ValueError(msg.value.decode())
+        shp = tuple(int(v) + 2 for v in n[::-1])
+        return bool(curv.value), w.reshape((6, 3) + shp).transpose(0, 1, 4, 3, 2)
 
 
 class Batch:

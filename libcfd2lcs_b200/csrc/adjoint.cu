@@ -629,6 +629,10 @@ class Adjoint {
       msg = "adjoint: " + hg_.error;
       return false;
     }
+    if (hg_.P.curv) {
+      msg = "adjoint: the grid must be an exact tensor product of coordinate lines";
+      return false;
+    }
     for (int a = 0; a < 3; a++)
       if (n[a] > 1 && !hg_.P.per[a]) {
         msg = "adjoint: every non-singleton direction must be periodic";
@@ -640,7 +644,7 @@ class Adjoint {
     }
     N_ = (long)n[0] * n[1] * n[2];
     ntot_ = hg_.ntot();
-    GridParams<T> P;
+    GridParams<T> P{};  // curv = 0 and no curvilinear tables: the adjoint runs on tensor-product grids
     const GridParams<lcsdata_t> &H = hg_.P;
     for (int a = 0; a < 3; a++) {
       P.n[a] = H.n[a];

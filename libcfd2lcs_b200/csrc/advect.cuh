@@ -171,6 +171,67 @@ __device__ __forceinline__ T tse_apply(const DevGrid<T> &g, const T x[3], const 
   return r;
 }
 
+// Coordinates of padded node (i,j,k): the full arrays of a non-rectilinear grid (CURV), else
+// the coordinate lines.
+template <typename T, bool CURV>
+__device__ __forceinline__ void node_xyz(const DevGrid<T> &g, int i, int j, int k, T x[3]) {
+  if (CURV) {
+    const int p = pidx(g.P.sx, g.P.sxy, i, j, k);
+#pragma unroll
+    for (int a = 0; a < 3; a++) x[a] = __ldg(g.X[a] + p);
+  } else {
+    x[0] = __ldg(g.lt[0] + i);
+    x[1] = __ldg(g.lt[1] + j);
+    x[2] = __ldg(g.lt[2] + k);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Taylor series on a non-rectilinear grid, interp_s2u_r1 TSE / TSE_LIMIT with grad_sr1_ls
+// (src/lp_tracking_m.f90:526-654, src/gradient_m.f90:241-295): at an interior node the
+// gradient sums, over the six face neighbours in NBR_OFFSET order (2..7), (phi(nbr) -
+// phi(no)) times the node's least-squares weights, from zero; on the ghost layer it is zero.
+// The value is phi(no) + d_x g_x + d_y g_y + d_z g_z with d = x - x(no), left to right, every
+// product and sum rounded on its own.  TSE_LIMIT clamps as tse_apply does.
+// ---------------------------------------------------------------------------------------
+template <typename T, bool LIMIT, typename F>
+__device__ __forceinline__ T tse_ls_apply(const DevGrid<T> &g, const T x[3], const int no[3], F val) {
+  const int str[3] = {1, g.P.sx, g.P.sxy};
+  const int p = pidx(g.P.sx, g.P.sxy, no[0], no[1], no[2]);
+  const T v0 = val(p);
+  const bool interior = no[0] >= 1 && no[0] <= g.P.n[0] && no[1] >= 1 && no[1] <= g.P.n[1] && no[2] >= 1 && no[2] <= g.P.n[2];
+  T gr[3] = {T(0), T(0), T(0)};
+  if (interior) {
+    const size_t plane = (size_t)g.P.sxy * (g.P.n[2] + 2);
+#pragma unroll
+    for (int nb = 0; nb < 6; nb++) {
+      const int a = nb % 3, q = nb < 3 ? p - str[a] : p + str[a];
+      const T df = val(q) - v0;
+#pragma unroll
+      for (int c = 0; c < 3; c++) gr[c] = add_rn(gr[c], mul_rn(df, __ldg(g.lsw + (size_t)(nb * 3 + c) * plane + p)));
+    }
+  }
+  T r = v0;
+#pragma unroll
+  for (int a = 0; a < 3; a++) r = add_rn(r, mul_rn(x[a] - __ldg(g.X[a] + p), gr[a]));
+  if (LIMIT) {
+    T mn = v0, mx = v0;
+    const int i0 = max(no[0] - 1, 0), i1 = min(no[0] + 1, g.P.n[0] + 1);
+    const int j0 = max(no[1] - 1, 0), j1 = min(no[1] + 1, g.P.n[1] + 1);
+    const int k0 = max(no[2] - 1, 0), k1 = min(no[2] + 1, g.P.n[2] + 1);
+    for (int k = k0; k <= k1; k++)
+      for (int j = j0; j <= j1; j++)
+        for (int i = i0; i <= i1; i++) {
+          const T v = val(pidx(g.P.sx, g.P.sxy, i, j, k));
+          mn = v < mn ? v : mn;
+          mx = v > mx ? v : mx;
+        }
+    r = r < mn ? mn : r;
+    r = r > mx ? mx : r;
+  }
+  return r;
+}
+
 // ---------------------------------------------------------------------------------------
 // Velocity sampler for one stage: NEAREST, LINEAR or B-spline, blended in time.
 // ---------------------------------------------------------------------------------------
@@ -211,6 +272,12 @@ __device__ __forceinline__ void sample_velocity(const DevGrid<T> &g, const Splin
     for (int c = 0; c < 3; c++) {
       const TV *a = V.un[c], *b = V.unp1[c];
       out[c] = tse_apply<T, INTERP == INTERP_TSE_LIMIT>(g, x, no, [&](int p) { return T(omc * __ldg(a + p) + ct * __ldg(b + p)); });
+    }
+  } else if (INTERP == INTERP_CTSE || INTERP == INTERP_CTSE_LIMIT) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const TV *a = V.un[c], *b = V.unp1[c];
+      out[c] = tse_ls_apply<T, INTERP == INTERP_CTSE_LIMIT>(g, x, no, [&](int p) { return T(omc * __ldg(a + p) + ct * __ldg(b + p)); });
     }
   } else {
     constexpr int KC = INTERP == INTERP_SPLINE4 ? 4 : 0;
@@ -256,6 +323,12 @@ __device__ __forceinline__ void sample_field(const DevGrid<T> &g, const SplineAx
     for (int c = 0; c < 3; c++) {
       const T *fc = f[c];
       out[c] = tse_apply<T, INTERP == INTERP_TSE_LIMIT>(g, x, no, [&](int p) { return __ldg(fc + p); });
+    }
+  } else if (INTERP == INTERP_CTSE || INTERP == INTERP_CTSE_LIMIT) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const T *fc = f[c];
+      out[c] = tse_ls_apply<T, INTERP == INTERP_CTSE_LIMIT>(g, x, no, [&](int p) { return __ldg(fc + p); });
     }
   } else {
     constexpr int KC = INTERP == INTERP_SPLINE4 ? 4 : 0;
@@ -368,23 +441,44 @@ __device__ __forceinline__ void integrate(const DevGrid<T> &g, const SplineAxes<
 // ---------------------------------------------------------------------------------------
 // (the singleton axis is selected by an unrolled comparison, not used as an index, so the
 // position and node arrays stay in registers)
-template <typename T>
+// On a non-rectilinear 2-D grid (CURV) the general form: the unit normal of the data plane at
+// the clamped node, the distance (x - x(node)) . n, the normal turned to make it non-negative,
+// and x - distance * n.
+template <typename T, bool CURV = false>
 __device__ __forceinline__ void project_plane(const DevGrid<T> &g, int no[3], T x[3]) {
   const int sa = g.P.single_axis;
   if (sa < 0) return;
+  if constexpr (CURV) {
+    no[0] = sa == 0 ? 1 : no[0];
+    no[1] = sa == 1 ? 1 : no[1];
+    no[2] = sa == 2 ? 1 : no[2];
+    const int p = pidx(g.P.sx, g.P.sxy, min(max(no[0], 1), g.P.n[0]), min(max(no[1], 1), g.P.n[1]), min(max(no[2], 1), g.P.n[2]));
+    T nv[3], d = T(0);
 #pragma unroll
-  for (int a = 0; a < 3; a++) {
-    if (a != sa) continue;
-    no[a] = 1;
-    const T plane = __ldg(g.lt[a] + 1);
-    T d = x[a] - plane;
-    const T dist = d < T(0) ? -d : d;
-    const T nrm = d < T(0) ? T(-1) : T(1);
-    x[a] = x[a] - dist * nrm;
+    for (int a = 0; a < 3; a++) {
+      nv[a] = __ldg(g.pnrm[a] + p);
+      const T t = mul_rn(x[a] - __ldg(g.X[a] + p), nv[a]);
+      d = a == 0 ? t : add_rn(d, t);
+    }
+    const bool flip = d < T(0);
+    d = flip ? -d : d;
+#pragma unroll
+    for (int a = 0; a < 3; a++) x[a] = x[a] - mul_rn(d, flip ? -nv[a] : nv[a]);
+  } else {
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      if (a != sa) continue;
+      no[a] = 1;
+      const T plane = __ldg(g.lt[a] + 1);
+      T d = x[a] - plane;
+      const T dist = d < T(0) ? -d : d;
+      const T nrm = d < T(0) ? T(-1) : T(1);
+      x[a] = x[a] - dist * nrm;
+    }
   }
 }
 
-template <typename T, bool HAS_FLAGS>
+template <typename T, bool HAS_FLAGS, bool CURV = false>
 __device__ __forceinline__ bool particle_bc(const DevGrid<T> &g, int no[3], T x[3], int *err) {
 #pragma unroll
   for (int a = 0; a < 3; a++) no[a] = min(max(no[a], 1), g.P.n[a]);
@@ -396,7 +490,9 @@ __device__ __forceinline__ bool particle_bc(const DevGrid<T> &g, int no[3], T x[
   if (f == LCS_MASK || f == LCS_SLIP || f == LCS_WALL) {
     if (f != LCS_MASK && interior) return false;
     T nx = __ldg(g.nrm[0] + p), ny = __ldg(g.nrm[1] + p), nz = __ldg(g.nrm[2] + p);
-    const T gx = __ldg(g.lt[0] + no[0]), gy = __ldg(g.lt[1] + no[1]), gz = __ldg(g.lt[2] + no[2]);
+    T gn[3];
+    node_xyz<T, CURV>(g, no[0], no[1], no[2], gn);
+    const T gx = gn[0], gy = gn[1], gz = gn[2];
     const T dist = (x[0] - gx) * nx + (x[1] - gy) * ny + (x[2] - gz) * nz;
     if (dist > T(0)) {
       x[0] = x[0] - nx * dist;
@@ -407,9 +503,7 @@ __device__ __forceinline__ bool particle_bc(const DevGrid<T> &g, int no[3], T x[
   }
   if (f == LCS_INFLOW || f == LCS_OUTFLOW) {
     if (interior) return false;
-    x[0] = __ldg(g.lt[0] + no[0]);
-    x[1] = __ldg(g.lt[1] + no[1]);
-    x[2] = __ldg(g.lt[2] + no[2]);
+    node_xyz<T, CURV>(g, no[0], no[1], no[2], x);
     return true;
   }
   atomicOr(err, ERR_UNKNOWN_FLAG);
@@ -431,8 +525,48 @@ __device__ __forceinline__ constexpr int nbr_offset(int nb, int a) {
 }
 
 
+// On a non-rectilinear grid (CURV) each candidate's squared distance comes from its padded
+// coordinates, (gx - x)^2 + (gy - y)^2 + (gz - z)^2 rounded term by term, the candidate index
+// clamped to the padded range.
 template <typename T>
+__device__ __forceinline__ bool track_pass_curv(const DevGrid<T> &g, const T x[3], int no[3]) {
+  const int sa = g.P.single_axis;
+  T best = T(0);
+  bool have = false;
+  int off[3] = {0, 0, 0};
+#pragma unroll
+  for (int nb = 0; nb < 27; nb++) {
+    const int o0 = nbr_offset(nb, 0), o1 = nbr_offset(nb, 1), o2 = nbr_offset(nb, 2);
+    if ((sa == 0 && o0 != 0) || (sa == 1 && o1 != 0) || (sa == 2 && o2 != 0)) continue;
+    const int q = pidx(g.P.sx, g.P.sxy, min(max(no[0] + o0, 0), g.P.n[0] + 1), min(max(no[1] + o1, 0), g.P.n[1] + 1),
+                       min(max(no[2] + o2, 0), g.P.n[2] + 1));
+    const T e0 = __ldg(g.X[0] + q) - x[0], e1 = __ldg(g.X[1] + q) - x[1], e2 = __ldg(g.X[2] + q) - x[2];
+    const T r = add_rn(add_rn(mul_rn(e0, e0), mul_rn(e1, e1)), mul_rn(e2, e2));
+    if (!have || r < T(0.99) * best) {
+      best = r;
+      have = true;
+      off[0] = o0;
+      off[1] = o1;
+      off[2] = o2;
+    }
+  }
+  no[0] += off[0];
+  no[1] += off[1];
+  no[2] += off[2];
+  return off[0] != 0 || off[1] != 0 || off[2] != 0;
+}
+
+template <typename T>
+__device__ __forceinline__ bool track_pass_lines(const DevGrid<T> &g, const T x[3], int no[3]);
+
+template <typename T, bool CURV = false>
 __device__ __forceinline__ bool track_pass(const DevGrid<T> &g, const T x[3], int no[3]) {
+  if constexpr (CURV) return track_pass_curv(g, x, no);
+  else return track_pass_lines(g, x, no);
+}
+
+template <typename T>
+__device__ __forceinline__ bool track_pass_lines(const DevGrid<T> &g, const T x[3], int no[3]) {
   // Per axis and offset o in {-1,0,1}: the squared axis distance to line no+o (clamped to
   // the padded range).  Off the interior the padded grid (sgrid%grid, src/sgrid_m.f90:
   // 182-359) holds one of two ghost coordinates: the periodic image when every out-of-range

@@ -16,10 +16,12 @@
 
 #include "adjoint.h"
 #include "engine.h"
+#include "grid.h"
 #include "writer.h"
 
 using cfd2lcs::Counters;
 using cfd2lcs::EngineBase;
+using cfd2lcs::HostGrid;
 using cfd2lcs::Options;
 
 #define CFD2LCS_EXPORT extern "C" __attribute__((visibility("default")))
@@ -456,6 +458,25 @@ CFD2LCS_EXPORT int cfd2lcs_b200_grid_tables(const int n[3], const lcsdata_t *x, 
     msg[len - 1] = 0;
   }
   return ok ? 0 : 1;
+}
+
+// Host-only: the least-squares gradient weights the library derives for a non-rectilinear
+// grid (compute_lsgw with the six face neighbours, src/gradient_m.f90:114-217), 18 padded
+// arrays [neighbour 0..5][derivative 0..2] of (n+2) points each, zero on a rectilinear grid.
+// *curv is set to 1 for a non-rectilinear grid.  Returns 0 on success.
+CFD2LCS_EXPORT int cfd2lcs_b200_grid_lsq_weights(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z,
+                                                 const int *flag, lcsdata_t *w, int *curv, char *msg, size_t len) {
+  HostGrid<lcsdata_t> g;
+  const bool ok = g.build(n, x, y, z, flag);
+  if (msg && len > 0) {
+    std::strncpy(msg, ok ? "" : g.error.c_str(), len - 1);
+    msg[len - 1] = 0;
+  }
+  if (!ok) return 1;
+  const size_t nt = (size_t)g.ntot();
+  if (curv) *curv = g.P.curv;
+  for (size_t q = 0; q < 18 * nt; q++) w[q] = g.lsw.empty() ? lcsdata_t(0) : g.lsw[q];
+  return 0;
 }
 
 // Allocation-free recomputation of a diagnostic's latest FTLE frame into caller-owned device

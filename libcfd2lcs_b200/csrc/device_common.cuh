@@ -20,10 +20,22 @@ enum : int {
 
 enum { EULER_ = 0, TRAPEZOIDAL_ = 1, RK2_ = 2, RK3_ = 3, RK4_ = 4 };
 // INTERP_SPLINE: B-spline of any order per axis; INTERP_SPLINE4: cubic on every axis (3-D grid);
-// INTERP_TSE / INTERP_TSE_LIMIT: Taylor series about the tracked node, without / with limiter
-enum { INTERP_NEAREST = 0, INTERP_LINEAR = 1, INTERP_SPLINE = 2, INTERP_SPLINE4 = 3, INTERP_TSE = 4, INTERP_TSE_LIMIT = 5 };
+// INTERP_TSE / INTERP_TSE_LIMIT: Taylor series about the tracked node, without / with limiter;
+// INTERP_CTSE / INTERP_CTSE_LIMIT: the same on a non-rectilinear grid (least-squares gradients,
+// full coordinate arrays), the only interpolators the reference runs there
+enum {
+  INTERP_NEAREST = 0,
+  INTERP_LINEAR = 1,
+  INTERP_SPLINE = 2,
+  INTERP_SPLINE4 = 3,
+  INTERP_TSE = 4,
+  INTERP_TSE_LIMIT = 5,
+  INTERP_CTSE = 6,
+  INTERP_CTSE_LIMIT = 7
+};
 
 __host__ __device__ constexpr bool interp_is_spline(int interp) { return interp == INTERP_SPLINE || interp == INTERP_SPLINE4; }
+__host__ __device__ constexpr bool interp_is_curv(int interp) { return interp == INTERP_CTSE || interp == INTERP_CTSE_LIMIT; }
 
 template <typename T>
 struct DevGrid {
@@ -33,6 +45,12 @@ struct DevGrid {
   const T *invd[3];      // inverse half spans, see HostGrid::invd
   const int8_t *flag;    // padded bcflag or nullptr
   const T *nrm[3];       // boundary normals (padded) or nullptr
+  // non-rectilinear grids (P.curv), else nullptr:
+  const T *X[3] = {nullptr, nullptr, nullptr};      // padded node coordinates
+  const T *lsw = nullptr;                           // least-squares weights: plane nb*3 + c holds face
+                                                    // neighbour nb's weight in d/dx_c
+  const T *pnrm[3] = {nullptr, nullptr, nullptr};   // 2-D grids: unit normal of the data plane per interior node
+  const T *invdp[3] = {nullptr, nullptr, nullptr};  // padded inverse half spans
 };
 
 template <typename T>

@@ -204,7 +204,9 @@ class Engine : public EngineBase {
             const int idx[3] = {i, j, k};
             for (int a = 0; a < 3; a++) {
               lcsdata_t v = 0;
-              if (inside) {
+              if (inside && g.P.curv) {
+                v = g.invdp[a][p];
+              } else if (inside) {
                 const int b = (a + 1) % 3, c = (a + 2) % 3;
                 const int cb = (idx[b] - 1 == 0 ? 1 : 0) | (idx[b] + 1 == n[b] + 1 ? 2 : 0);
                 const int cc = (idx[c] - 1 == 0 ? 1 : 0) | (idx[c] + 1 == n[c] + 1 ? 2 : 0);
@@ -239,9 +241,19 @@ class Engine : public EngineBase {
     if (const char *e = std::getenv("CFD2LCS_B200_COMPOSE_MINB")) compose_minb_ = std::atoi(e) >= 4 ? 4 : 2;
     if (const char *e = std::getenv("CFD2LCS_B200_SL_TILE")) tile_mode_ = std::max(0, std::min(2, std::atoi(e)));
     for (int a = 0; a < 3; a++) n_[a] = n[a];
-    // coordinate lines and interior flags for the output files (the grid is a tensor product)
-    for (int a = 0; a < 3; a++)
+    // coordinate lines (and, on a non-rectilinear grid, the node coordinates) and interior flags
+    // for the output files
+    for (int a = 0; a < 3; a++) {
       out_lines_[a] = std::make_shared<std::vector<double>>(hg_.lt[a].begin() + 1, hg_.lt[a].begin() + 1 + n[a]);
+      if (hg_.P.curv) {
+        auto c = std::make_shared<std::vector<double>>();
+        c->reserve((size_t)n[0] * n[1] * n[2]);
+        for (int k = 1; k <= n[2]; k++)
+          for (int j = 1; j <= n[1]; j++)
+            for (int i = 1; i <= n[0]; i++) c->push_back((double)hg_.coord(a, i, j, k));
+        out_coords_[a] = c;
+      }
+    }
     {
       auto fl = std::make_shared<std::vector<int8_t>>((size_t)n[0] * n[1] * n[2]);
       for (size_t q = 0; q < fl->size(); q++) (*fl)[q] = (int8_t)flag[q];
@@ -419,11 +431,13 @@ class Engine : public EngineBase {
       t_np1_ = time;
     }
     cur_ ^= 1;  // u_n = u_np1 (buffer swap); u_np1 is rewritten below
-    const int interp = opt_->interpolator;
-    if (interp != NEAREST_NBR && interp != LINEAR && interp != QUADRATIC && interp != CUBIC && interp != TSE && interp != TSE_LIMIT) {
+    const int raw_interp = opt_->interpolator;
+    if (raw_interp != NEAREST_NBR && raw_interp != LINEAR && raw_interp != QUADRATIC && raw_interp != CUBIC && raw_interp != TSE &&
+        raw_interp != TSE_LIMIT) {
       msg = "ERROR: Unrecognized interpolator";
       return false;
     }
+    const int interp = interpolator();
     // --- K0 ingest --------------------------------------------------------------------
     CK(cudaEventRecord(ev_[8], stream_));
     CK(cudaEventRecord(ev_[0], stream_));
@@ -488,7 +502,7 @@ class Engine : public EngineBase {
     begun_ = false;
     evnext_ = 0;
     spans_.clear();
-    const int interp = opt_->interpolator;
+    const int interp = interpolator();
     const bool spline = interp == QUADRATIC || interp == CUBIC;
     const int deg = interp == QUADRATIC ? 2 : 3;
     CK(cudaEventSynchronize(ev_[1]));
@@ -759,7 +773,7 @@ class Engine : public EngineBase {
             std::to_string(NOALLOC_MAX_SUBMAPS) + " (T/h too large)";
       return false;
     }
-    const int interp = opt_->interpolator;
+    const int interp = interpolator();
     const bool spline = interp == QUADRATIC || interp == CUBIC;
     const int deg = interp == QUADRATIC ? 2 : 3;
     const T *host_table[3 * NOALLOC_MAX_SUBMAPS];
@@ -794,14 +808,15 @@ class Engine : public EngineBase {
     else if (iv == INTERP_LINEAR) { if (F) COMPOSE_NA(INTERP_LINEAR, true); else COMPOSE_NA(INTERP_LINEAR, false); }
     else if (iv == INTERP_TSE) { if (F) COMPOSE_NA(INTERP_TSE, true); else COMPOSE_NA(INTERP_TSE, false); }
     else if (iv == INTERP_TSE_LIMIT) { if (F) COMPOSE_NA(INTERP_TSE_LIMIT, true); else COMPOSE_NA(INTERP_TSE_LIMIT, false); }
+    else if (iv == INTERP_CTSE) { if (F) COMPOSE_NA(INTERP_CTSE, true); else COMPOSE_NA(INTERP_CTSE, false); }
+    else if (iv == INTERP_CTSE_LIMIT) { if (F) COMPOSE_NA(INTERP_CTSE_LIMIT, true); else COMPOSE_NA(INTERP_CTSE_LIMIT, false); }
     else if (iv == INTERP_SPLINE4) { if (F) COMPOSE_NA(INTERP_SPLINE4, true); else COMPOSE_NA(INTERP_SPLINE4, false); }
     else { if (F) COMPOSE_NA(INTERP_SPLINE, true); else COMPOSE_NA(INTERP_SPLINE, false); }
 #undef COMPOSE_NA
     CK(cudaGetLastError());
     FieldPtrs<T> f{};
     for (int c = 0; c < 3; c++) f.f[c] = out.f[c];
-    if (F) k_ftle<T, lcsdata_t, true><<<grd, blk, 0, stream_>>>(dg_, f, d_ftle, d->T_, opt_->incompressible);
-    else k_ftle<T, lcsdata_t, false><<<grd, blk, 0, stream_>>>(dg_, f, d_ftle, d->T_, opt_->incompressible);
+    launch_ftle(dg_, f, d_ftle, d->T_, blk, grd);
     CK(cudaGetLastError());
     return sync_errors(msg);
   }
@@ -930,12 +945,12 @@ class Engine : public EngineBase {
     for (int k = 1; k <= G.P.n[2]; k++)
       for (int j = 1; j <= G.P.n[1]; j++)
         for (int i = 1; i <= G.P.n[0]; i++, q++) {
-          const lcsdata_t dx = G.lt[0][i] - X, dy = G.lt[1][j] - Y, dz = G.lt[2][k] - Z;
+          const lcsdata_t dx = G.coord(0, i, j, k) - X, dy = G.coord(1, i, j, k) - Y, dz = G.coord(2, i, j, k) - Z;
           const lcsdata_t r = std::sqrt(dx * dx + dy * dy + dz * dz);
           if (!(r <= R)) continue;
           const int nd[3] = {i, j, k};
           for (int a = 0; a < 3; a++) {
-            px[a].push_back(tmp.lg ? tpos[a][q] : (T)G.lt[a][nd[a]]);
+            px[a].push_back(tmp.lg ? tpos[a][q] : (T)G.coord(a, i, j, k));
             pn[a].push_back(tmp.lg ? tnos[a][q] : nd[a]);
           }
         }
@@ -1247,7 +1262,15 @@ class Engine : public EngineBase {
     return true;
   }
 
-  static int interp_variant(int interp, const SplineAxes<T> &sa) {
+  // The interpolator the kernels run: on a non-rectilinear grid the reference takes TSE_LIMIT
+  // unless TSE was asked for (interp_s2u_r1, src/lp_tracking_m.f90:320-327).
+  int interpolator() const {
+    const int v = opt_->interpolator;
+    return hg_.P.curv ? (v == TSE ? TSE : TSE_LIMIT) : v;
+  }
+
+  int interp_variant(int interp, const SplineAxes<T> &sa) const {
+    if (hg_.P.curv) return interp == TSE ? INTERP_CTSE : INTERP_CTSE_LIMIT;
     if (interp == NEAREST_NBR) return INTERP_NEAREST;
     if (interp == LINEAR) return INTERP_LINEAR;
     if (interp == TSE) return INTERP_TSE;
@@ -1270,6 +1293,10 @@ class Engine : public EngineBase {
   // goes through the same host set-up as the solver grid, then every lcs node is tracked to
   // the solver grid.
   bool make_lcs_grid(DiagT &d, int type, int &res, std::string &msg) {
+    if (hg_.P.curv && res != 0) {
+      msg = "diagnostic_init: resolution /= 0 on a non-rectilinear grid is not supported";
+      return false;
+    }
     for (int a = 0; a < 3; a++)
       if (n_[a] > 1 && std::abs(res) >= n_[a]) res = 0;
     if (res == 0) return true;
@@ -1356,6 +1383,10 @@ class Engine : public EngineBase {
   // product to rounding (uniform spacing around every node, as on a cube); the per-node
   // separations of each pair are kept exactly for the gradient.
   bool create_aux(int pi, std::string &msg) {
+    if (hg_.P.curv) {
+      msg = "AUX_GRID: not supported on a non-rectilinear grid";
+      return false;
+    }
     const DiagT par = diags_[pi];  // copy: diags_ grows below
     const HostGrid<lcsdata_t> &bg = par.lg ? par.lg->hg : hg_;
     const int n[3] = {bg.P.n[0], bg.P.n[1], bg.P.n[2]};
@@ -1503,7 +1534,7 @@ class Engine : public EngineBase {
   // takes the all-cubic specialisation only when both grids allow it
   bool launch_sl_refined(DiagT &d, const SplineAxes<T> &sas, const SplineAxes<T> &sal, const VelFields<TV> &V, FieldPtrs<T> fo,
                          FieldPtrsW<T> fn, StageTimes S, T dt, std::string &msg) {
-    const int interp = opt_->interpolator;
+    const int interp = interpolator();
     if (interp == NEAREST_NBR) sl_refined_flags<INTERP_NEAREST>(d, sas, sal, V, fo, fn, S, dt);
     else if (interp == LINEAR) sl_refined_flags<INTERP_LINEAR>(d, sas, sal, V, fo, fn, S, dt);
     else if (interp == TSE) sl_refined_flags<INTERP_TSE>(d, sas, sal, V, fo, fn, S, dt);
@@ -1517,7 +1548,7 @@ class Engine : public EngineBase {
 
   // Device tables of a host grid set-up (coordinate lines, spans, flags, normals, constants)
   bool make_dev_grid(const HostGrid<lcsdata_t> &hg, DevGrid<T> &dg, std::string &msg) {
-    GridParams<T> P;
+    GridParams<T> P{};
     const GridParams<lcsdata_t> &H = hg.P;
     for (int a = 0; a < 3; a++) {
       P.n[a] = H.n[a];
@@ -1534,11 +1565,26 @@ class Engine : public EngineBase {
       for (int c = 0; c < 3; c++) P.ps[d][c] = (T)H.ps[d][c];
     P.has_flags = H.has_flags;
     P.maxtrack = H.maxtrack;
+    P.curv = H.curv;
+    for (int a = 0; a < 3; a++) {
+      P.guess0[a] = H.guess0[a];
+      for (int c = 0; c < 3; c++) P.guessd[a][c] = (T)H.guessd[a][c];
+    }
     dg.P = P;
     for (int a = 0; a < 3; a++) {
       if (!(dg.lt[a] = upload(hg.lt[a], msg))) return false;
       if (!(dg.li[a] = upload(hg.li[a], msg))) return false;
       if (!(dg.invd[a] = upload(hg.invd[a], msg))) return false;
+    }
+    dg.lsw = nullptr;
+    for (int a = 0; a < 3; a++) dg.X[a] = dg.pnrm[a] = dg.invdp[a] = nullptr;
+    if (H.curv) {
+      for (int a = 0; a < 3; a++) {
+        if (!(dg.X[a] = upload(hg.X[a], msg))) return false;
+        if (!(dg.invdp[a] = upload(hg.invdp[a], msg))) return false;
+        if (!hg.pnorm[a].empty() && !(dg.pnrm[a] = upload(hg.pnorm[a], msg))) return false;
+      }
+      if (!(dg.lsw = upload(hg.lsw, msg))) return false;
     }
     dg.flag = nullptr;
     for (int a = 0; a < 3; a++) dg.nrm[a] = nullptr;
@@ -1761,6 +1807,9 @@ class Engine : public EngineBase {
     else if (iv == INTERP_LINEAR) F ? sl_integ<INTERP_LINEAR, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_LINEAR, false>(sa, V, fo, fn, S, dt);
     else if (iv == INTERP_TSE) F ? sl_integ<INTERP_TSE, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_TSE, false>(sa, V, fo, fn, S, dt);
     else if (iv == INTERP_TSE_LIMIT) F ? sl_integ<INTERP_TSE_LIMIT, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_TSE_LIMIT, false>(sa, V, fo, fn, S, dt);
+    else if (iv == INTERP_CTSE) F ? sl_integ<INTERP_CTSE, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_CTSE, false>(sa, V, fo, fn, S, dt);
+    else if (iv == INTERP_CTSE_LIMIT)
+      F ? sl_integ<INTERP_CTSE_LIMIT, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_CTSE_LIMIT, false>(sa, V, fo, fn, S, dt);
     else if (iv == INTERP_SPLINE4) F ? sl_integ<INTERP_SPLINE4, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_SPLINE4, false>(sa, V, fo, fn, S, dt);
     else F ? sl_integ<INTERP_SPLINE, true>(sa, V, fo, fn, S, dt) : sl_integ<INTERP_SPLINE, false>(sa, V, fo, fn, S, dt);
     CK(cudaGetLastError());
@@ -1790,6 +1839,9 @@ class Engine : public EngineBase {
     else if (iv == INTERP_LINEAR) F ? fwd_integ<INTERP_LINEAR, true>(sa, V, P, S, dt, n) : fwd_integ<INTERP_LINEAR, false>(sa, V, P, S, dt, n);
     else if (iv == INTERP_TSE) F ? fwd_integ<INTERP_TSE, true>(sa, V, P, S, dt, n) : fwd_integ<INTERP_TSE, false>(sa, V, P, S, dt, n);
     else if (iv == INTERP_TSE_LIMIT) F ? fwd_integ<INTERP_TSE_LIMIT, true>(sa, V, P, S, dt, n) : fwd_integ<INTERP_TSE_LIMIT, false>(sa, V, P, S, dt, n);
+    else if (iv == INTERP_CTSE) F ? fwd_integ<INTERP_CTSE, true>(sa, V, P, S, dt, n) : fwd_integ<INTERP_CTSE, false>(sa, V, P, S, dt, n);
+    else if (iv == INTERP_CTSE_LIMIT)
+      F ? fwd_integ<INTERP_CTSE_LIMIT, true>(sa, V, P, S, dt, n) : fwd_integ<INTERP_CTSE_LIMIT, false>(sa, V, P, S, dt, n);
     else if (iv == INTERP_SPLINE4) F ? fwd_integ<INTERP_SPLINE4, true>(sa, V, P, S, dt, n) : fwd_integ<INTERP_SPLINE4, false>(sa, V, P, S, dt, n);
     else F ? fwd_integ<INTERP_SPLINE, true>(sa, V, P, S, dt, n) : fwd_integ<INTERP_SPLINE, false>(sa, V, P, S, dt, n);
     CK(cudaGetLastError());
@@ -1894,6 +1946,8 @@ class Engine : public EngineBase {
       else if (iv == INTERP_LINEAR) COMPOSE_STEPS(INTERP_LINEAR);
       else if (iv == INTERP_TSE) COMPOSE_STEPS(INTERP_TSE);
       else if (iv == INTERP_TSE_LIMIT) COMPOSE_STEPS(INTERP_TSE_LIMIT);
+      else if (iv == INTERP_CTSE) COMPOSE_STEPS(INTERP_CTSE);
+      else if (iv == INTERP_CTSE_LIMIT) COMPOSE_STEPS(INTERP_CTSE_LIMIT);
       else if (iv == INTERP_SPLINE4) COMPOSE_STEPS(INTERP_SPLINE4);
       else COMPOSE_STEPS(INTERP_SPLINE);
 #undef COMPOSE_STEPS
@@ -1914,11 +1968,25 @@ class Engine : public EngineBase {
     else if (iv == INTERP_LINEAR) { if (F) COMPOSE(INTERP_LINEAR, true); else COMPOSE(INTERP_LINEAR, false); }
     else if (iv == INTERP_TSE) { if (F) COMPOSE(INTERP_TSE, true); else COMPOSE(INTERP_TSE, false); }
     else if (iv == INTERP_TSE_LIMIT) { if (F) COMPOSE(INTERP_TSE_LIMIT, true); else COMPOSE(INTERP_TSE_LIMIT, false); }
+    else if (iv == INTERP_CTSE) { if (F) COMPOSE(INTERP_CTSE, true); else COMPOSE(INTERP_CTSE, false); }
+    else if (iv == INTERP_CTSE_LIMIT) { if (F) COMPOSE(INTERP_CTSE_LIMIT, true); else COMPOSE(INTERP_CTSE_LIMIT, false); }
     else if (iv == INTERP_SPLINE4) { if (F) COMPOSE(INTERP_SPLINE4, true); else COMPOSE(INTERP_SPLINE4, false); }
     else { if (F) COMPOSE(INTERP_SPLINE, true); else COMPOSE(INTERP_SPLINE, false); }
 #undef COMPOSE
     CK(cudaGetLastError());
     return true;
+  }
+
+  // k_ftle for the grid's form: flags or not, central differences or least squares (curvilinear)
+  void launch_ftle(const DevGrid<T> &g, FieldPtrs<T> f, lcsdata_t *ftle, lcsdata_t Tint, dim3 blk, dim3 grd) {
+    const int inc = opt_->incompressible;
+    if (g.P.curv) {
+      if (g.P.has_flags) k_ftle<T, lcsdata_t, true, true><<<grd, blk, 0, stream_>>>(g, f, ftle, Tint, inc);
+      else k_ftle<T, lcsdata_t, false, true><<<grd, blk, 0, stream_>>>(g, f, ftle, Tint, inc);
+    } else {
+      if (g.P.has_flags) k_ftle<T, lcsdata_t, true><<<grd, blk, 0, stream_>>>(g, f, ftle, Tint, inc);
+      else k_ftle<T, lcsdata_t, false><<<grd, blk, 0, stream_>>>(g, f, ftle, Tint, inc);
+    }
   }
 
   bool launch_ftle(DiagT &d, std::string &msg) {
@@ -1927,10 +1995,7 @@ class Engine : public EngineBase {
     FieldPtrs<T> f{};
     for (int c = 0; c < 3; c++) f.f[c] = d.composed[c];
     counters_.kernel_launches++;
-    if (g.P.has_flags)
-      k_ftle<T, lcsdata_t, true><<<grd, blk, 0, stream_>>>(g, f, d.ftle, d.T_, opt_->incompressible);
-    else
-      k_ftle<T, lcsdata_t, false><<<grd, blk, 0, stream_>>>(g, f, d.ftle, d.T_, opt_->incompressible);
+    launch_ftle(g, f, d.ftle, d.T_, blk, grd);
     CK(cudaGetLastError());
     return true;
   }
@@ -1984,6 +2049,7 @@ class Engine : public EngineBase {
       nn[a] = d.lg ? d.lg->dg.P.n[a] : n_[a];
       job.n[a] = nn[a];
       job.lines[a] = d.lg ? d.lg->out_lines[a] : out_lines_[a];
+      if (!d.lg) job.coords[a] = out_coords_[a];
     }
     job.flags = d.lg ? d.lg->out_flags : out_flags_;
     const std::string title = d.label + "-FTLE";
@@ -2087,7 +2153,7 @@ class Engine : public EngineBase {
     }
     k_pad_snapshot<T, TV><<<(unsigned)((ntot_ + 255) / 256), 256, 0, stream_>>>(dg_, src, dst, ntot_);
     counters_.kernel_launches++;
-    const int interp = opt_->interpolator;
+    const int interp = interpolator();
     const bool spline = interp == QUADRATIC || interp == CUBIC;
     VelFields<TV> V{};
     SplineAxes<T> sa{};
@@ -2137,7 +2203,8 @@ class Engine : public EngineBase {
     for (int q = 0; q < 3; q++) o3.f[q] = d.inv[q];
     o2.f[0] = d.inv[3];
     o2.f[1] = d.inv[4];
-    k_invariants<T, TV><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, u, have ? 1 : 0, o3, o2);
+    if (dg_.P.curv) k_invariants<T, TV, true><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, u, have ? 1 : 0, o3, o2);
+    else k_invariants<T, TV><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, u, have ? 1 : 0, o3, o2);
     counters_.kernel_launches++;
     CK(cudaGetLastError());
     return true;
@@ -2195,6 +2262,7 @@ class Engine : public EngineBase {
   TV *upad_[3] = {nullptr, nullptr, nullptr}, *upcoef_[3] = {nullptr, nullptr, nullptr};  // refined lp%ugrid scratch
   std::unique_ptr<LcsWriter> writer_;  // created by the first output file
   std::shared_ptr<const std::vector<double>> out_lines_[3];
+  std::shared_ptr<const std::vector<double>> out_coords_[3];  // non-rectilinear grids only
   std::shared_ptr<const std::vector<int8_t>> out_flags_;
   HostGrid<lcsdata_t> hg_;
   DevGrid<T> dg_{};

@@ -1,11 +1,17 @@
-// Host-side grid setup of libcfd2lcs_b200: the tensor-product form of the reference's
-// init_sgrid (src/sgrid_m.f90:16-444) and compute_delta_xyz (:951-1014), one rank.
+// Host-side grid setup of libcfd2lcs_b200: the reference's init_sgrid (src/sgrid_m.f90:16-444)
+// and compute_delta_xyz (:951-1014), one rank.
 //
-// The device kernels never see full 3-D coordinate arrays.  A rectilinear grid is stored
-// as three coordinate lines plus the rules the reference's ghost construction produces:
-// mirrored "fake" ghosts, periodic images with the periodic shift (including the z shift
-// read at direction (i,k,k), src/comms_m.f90:750), and the extrusion of a singleton
-// direction (src/sgrid_m.f90:304-359).
+// A grid that is an exact tensor product of coordinate lines is stored as three lines plus
+// the rules the reference's ghost construction produces: mirrored "fake" ghosts, periodic
+// images with the periodic shift (including the z shift read at direction (i,k,k),
+// src/comms_m.f90:750), and the extrusion of a singleton direction (src/sgrid_m.f90:304-359);
+// those kernels never see full 3-D coordinate arrays.  Any other grid that the reference
+// classes as non-rectilinear (check_rectilinear, :868-949) keeps the full padded coordinate
+// arrays, built by the same ghost construction, together with what the reference's
+// non-rectilinear path needs: face-neighbour least-squares gradient weights (compute_lsgw,
+// src/gradient_m.f90:114-217), inverse half spans per node, the plane normals of a 2-D grid
+// (project_lp2plane, src/lp_m.f90:418-538) and the node-guess constants of
+// exchange_lp_alltoall (src/comms_m.f90:1625-1673).
 #pragma once
 
 #include <cstdint>
@@ -32,6 +38,12 @@ struct GridParams {
   R ps[27][3];        // periodic shift per direction, index (dk+1)*9 + (dj+1)*3 + (di+1)
   int has_flags;      // bcflag array present (some flag is not LCS_INTERNAL or 2-D)
   int maxtrack;       // 2*max(n): recursion limit of the node search
+  int curv;           // non-rectilinear grid: full coordinate arrays and least squares
+  // non-rectilinear grids, exchange_lp_alltoall's node guess per direction a:
+  // nint((imin_x + imin_y + imin_z)/3) and the index spans imax_c - imin_c of the coordinate
+  // extremes (minloc / maxloc over the padded arrays, src/comms_m.f90:1625-1673)
+  int guess0[3];
+  R guessd[3][3];     // [direction a][coordinate c]
 };
 
 template <typename R>
@@ -44,6 +56,12 @@ struct HostGrid {
   std::vector<R> invdz;   // 1/half-span for z, by (k, i class, j class): index (k*4 + ci)*4 + cj
   std::vector<int8_t> flag;  // padded bcflag (empty when has_flags == 0)
   std::vector<R> bcnorm;     // 3 x padded, only at nodes whose flag needs it (empty otherwise)
+  // non-rectilinear grids only (empty otherwise), padded layout:
+  std::vector<R> X[3];       // node coordinates (sgrid%grid)
+  std::vector<R> lsw;        // 18 planes: weight of face neighbour nb (NBR_OFFSET 2..7) for
+                             // derivative c at plane nb*3 + c, zero on the ghost layer
+  std::vector<R> invdp[3];   // inverse half spans per node (compute_delta_xyz)
+  std::vector<R> pnorm[3];   // 2-D grids: unit normal of the data plane at interior nodes
   bool rectilinear = false;
   R scaling = R(0);          // extrusion length of a singleton direction
   std::string error;         // non-empty: the grid is rejected
@@ -53,6 +71,11 @@ struct HostGrid {
 
   // Coordinate c of any node of the padded grid (the reference's sgrid%grid).
   R coord(int c, int i, int j, int k) const;
+
+  // The non-rectilinear branch of build(): padded coordinates and their tables (above).
+  bool build_curvilinear(const R *x, const R *y, const R *z);
+  // Least-squares gradient weights at an interior node over NBR_OFFSET neighbours first..last.
+  void lsq_weights(int i, int j, int k, int first, int last, R w[27][3]) const;
   long ntot() const { return (long)P.sxy * (P.n[2] + 2); }
   long pidx(int i, int j, int k) const { return (long)i + (long)P.sx * j + (long)P.sxy * k; }
 };

@@ -31,6 +31,7 @@ struct DevReduce {
 
 template <typename T>
 __device__ __forceinline__ T inv_half_span(const DevGrid<T> &g, int a, int i, int j, int k) {
+  if (g.P.curv) return __ldg(g.invdp[a] + pidx(g.P.sx, g.P.sxy, i, j, k));  // per node
   // class bits of the other two axes (b = a+1, c = a+2 mod 3), see HostGrid::invd
   const int idx[3] = {i, j, k};
   const int b = (a + 1) % 3, c = (a + 2) % 3;
@@ -148,12 +149,14 @@ __global__ void __launch_bounds__(256, sl_min_blocks<INTERP>()) k_sl_subcycle(De
   int i, j, k;
   if (!node_of_thread(g.P.n, i, j, k)) return;
   const int p = pidx(g.P.sx, g.P.sxy, i, j, k);
-  const T x0[3] = {__ldg(g.lt[0] + i), __ldg(g.lt[1] + j), __ldg(g.lt[2] + k)};
+  constexpr bool CURV = interp_is_curv(INTERP);
+  T x0[3];
+  node_xyz<T, CURV>(g, i, j, k, x0);
   int no[3] = {i, j, k};
   T x[3];
   integrate<T, TV, INTEG, INTERP, true>(g, sa, V, S, dt, x0, no, x);
-  project_plane(g, no, x);
-  const bool stick = particle_bc<T, HAS_FLAGS>(g, no, x, err);
+  project_plane<T, CURV>(g, no, x);
+  const bool stick = particle_bc<T, HAS_FLAGS, CURV>(g, no, x, err);
   if (stick) {
     x[0] = x0[0];
     x[1] = x0[1];
@@ -339,10 +342,11 @@ __global__ void __launch_bounds__(256, fwd_min_blocks<INTERP>()) k_fwd_subcycle(
   if (q >= np) return;
   T xn[3] = {P.x[0][q], P.x[1][q], P.x[2][q]};
   int no[3] = {P.no[0][q], P.no[1][q], P.no[2][q]};
+  constexpr bool CURV = interp_is_curv(INTERP);
   T x[3];
   integrate<T, TV, INTEG, INTERP>(g, sa, V, S, dt, xn, no, x);
-  project_plane(g, no, x);
-  const bool stick = particle_bc<T, HAS_FLAGS>(g, no, x, err);
+  project_plane<T, CURV>(g, no, x);
+  const bool stick = particle_bc<T, HAS_FLAGS, CURV>(g, no, x, err);
   if (stick) {
     x[0] = xn[0];
     x[1] = xn[1];
@@ -350,7 +354,7 @@ __global__ void __launch_bounds__(256, fwd_min_blocks<INTERP>()) k_fwd_subcycle(
   }
 #pragma unroll
   for (int c = 0; c < 3; c++) P.dx[c][q] = P.dx[c][q] + (x[c] - xn[c]);
-  track_pass(g, x, no);
+  track_pass<T, CURV>(g, x, no);
   wrap_particle(g, x, no);
 #pragma unroll
   for (int c = 0; c < 3; c++) {
@@ -398,7 +402,10 @@ __global__ void __launch_bounds__(256) k_snapshot(DevGrid<T> g, FieldPtrs<T> src
 // :1609-1655) and re-locate the node with the recursive search (tracking with the forward
 // wrap).  Output: the composed map (exchange_lpmap) after the interior flow-map BC.
 // ---------------------------------------------------------------------------------------
-template <typename T>
+// On a non-rectilinear grid (CURV) the node guess is comms_m.f90:1662-1673's: per direction a,
+// nint((imin_x + imin_y + imin_z)/3) + nint((s dx_a + t dy_a + u dz_a)/3) from the index
+// positions of the coordinate extremes (GridParams::guess0, guessd).
+template <typename T, bool CURV = false>
 __device__ __forceinline__ void alltoall_wrap(const DevGrid<T> &g, T x[3], int no[3]) {
   const T *bb = g.P.bb;
   bool inside = x[0] >= bb[0] && x[0] <= bb[3] && x[1] >= bb[1] && x[1] <= bb[4] && x[2] >= bb[2] && x[2] <= bb[5];
@@ -414,11 +421,24 @@ __device__ __forceinline__ void alltoall_wrap(const DevGrid<T> &g, T x[3], int n
       }
     }
   }
+  if constexpr (CURV) {
+    T st[3];
 #pragma unroll
-  for (int a = 0; a < 3; a++) {
-    const T s = clamp01((x[a] - bb[a]) / (bb[a + 3] - bb[a]));
-    const int v = (int)round(T(g.P.n[a]) * s);  // nint(real(n)*s): half away from zero
-    no[a] = min(max(v, 1), g.P.n[a]);
+    for (int a = 0; a < 3; a++) st[a] = clamp01((x[a] - bb[a]) / (bb[a + 3] - bb[a]));
+    const T third = T(1) / T(3);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const T sum = add_rn(add_rn(mul_rn(st[0], g.P.guessd[a][0]), mul_rn(st[1], g.P.guessd[a][1])), mul_rn(st[2], g.P.guessd[a][2]));
+      const int v = g.P.guess0[a] + (int)round(mul_rn(third, sum));
+      no[a] = min(max(v, 1), g.P.n[a]);
+    }
+  } else {
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const T s = clamp01((x[a] - bb[a]) / (bb[a + 3] - bb[a]));
+      const int v = (int)round(T(g.P.n[a]) * s);  // nint(real(n)*s): half away from zero
+      no[a] = min(max(v, 1), g.P.n[a]);
+    }
   }
 }
 
@@ -427,13 +447,15 @@ __global__ void __launch_bounds__(256) k_compose(DevGrid<T> g, SplineAxes<T> sa,
                                                   int *err) {
   int i, j, k;
   if (!node_of_thread(g.P.n, i, j, k)) return;
-  T x[3] = {__ldg(g.lt[0] + i), __ldg(g.lt[1] + j), __ldg(g.lt[2] + k)};
+  constexpr bool CURV = interp_is_curv(INTERP);
+  T x[3];
+  node_xyz<T, CURV>(g, i, j, k, x);
   int no[3] = {i, j, k};
   T d[3] = {T(0), T(0), T(0)};
   for (int m = 0; m < nsl; m++) {
     const T *const f[3] = {slots[3 * m], slots[3 * m + 1], slots[3 * m + 2]};
-    project_plane(g, no, x);
-    particle_bc<T, HAS_FLAGS>(g, no, x, err);
+    project_plane<T, CURV>(g, no, x);
+    particle_bc<T, HAS_FLAGS, CURV>(g, no, x, err);
     T up[3];
     sample_field<T, INTERP>(g, sa, f, x, no, up);
 #pragma unroll
@@ -441,10 +463,10 @@ __global__ void __launch_bounds__(256) k_compose(DevGrid<T> g, SplineAxes<T> sa,
       x[c] = x[c] + up[c];
       d[c] = d[c] + up[c];
     }
-    alltoall_wrap(g, x, no);
+    alltoall_wrap<T, CURV>(g, x, no);
     int passes = 0;
     while (true) {
-      const bool moved = track_pass(g, x, no);
+      const bool moved = track_pass<T, CURV>(g, x, no);
       passes++;
       if (passes > g.P.maxtrack) {
         atomicOr(err, ERR_TRACKING);
@@ -477,8 +499,9 @@ __global__ void __launch_bounds__(256, MINB) k_compose_step(DevGrid<T> g, Spline
   T x[3] = {P.x[0][q], P.x[1][q], P.x[2][q]};
   int no[3] = {P.no[0][q], P.no[1][q], P.no[2][q]};
   T d[3] = {P.dx[0][q], P.dx[1][q], P.dx[2][q]};
-  project_plane(g, no, x);
-  particle_bc<T, HAS_FLAGS>(g, no, x, err);
+  constexpr bool CURV = interp_is_curv(INTERP);
+  project_plane<T, CURV>(g, no, x);
+  particle_bc<T, HAS_FLAGS, CURV>(g, no, x, err);
   T up[3];
   sample_field<T, INTERP>(g, sa, f.f, x, no, up);
 #pragma unroll
@@ -486,10 +509,10 @@ __global__ void __launch_bounds__(256, MINB) k_compose_step(DevGrid<T> g, Spline
     x[c] = x[c] + up[c];
     d[c] = d[c] + up[c];
   }
-  alltoall_wrap(g, x, no);
+  alltoall_wrap<T, CURV>(g, x, no);
   int passes = 0;
   while (true) {
-    const bool moved = track_pass(g, x, no);
+    const bool moved = track_pass<T, CURV>(g, x, no);
     passes++;
     if (passes > g.P.maxtrack) {
       atomicOr(err, ERR_TRACKING);
@@ -545,13 +568,33 @@ __device__ __forceinline__ T fm_neighbour(const DevGrid<T> &g, const T *__restri
   return T(0);
 }
 
-template <typename T, typename R, bool HAS_FLAGS>
+// CURV: a non-rectilinear grid, gradient by grad_sr1_ls (src/lcs_m.f90:129-133): per
+// component, the face neighbours' differences (the same ghost values) times the node's
+// least-squares weights, summed in NBR_OFFSET order from zero in T.
+template <typename T, typename R, bool HAS_FLAGS, bool CURV = false>
 __global__ void __launch_bounds__(256) k_ftle(DevGrid<T> g, FieldPtrs<T> fm, R *__restrict__ ftle, R Tint, int incompressible) {
   int i, j, k;
   if (!node_of_thread(g.P.n, i, j, k)) return;
   double G[3][3];  // G[c][a] = d fm_c / d x_a
+  if (CURV) {
+    const int p = pidx(g.P.sx, g.P.sxy, i, j, k);
+    const size_t plane = (size_t)g.P.sxy * (g.P.n[2] + 2);
 #pragma unroll
-  for (int a = 0; a < 3; a++) {
+    for (int c = 0; c < 3; c++) {
+      const T f0 = __ldg(fm.f[c] + interior_index(g.P.n, i, j, k));
+      T gr[3] = {T(0), T(0), T(0)};
+#pragma unroll
+      for (int nb = 0; nb < 6; nb++) {
+        const T df = fm_neighbour<T, R, HAS_FLAGS>(g, fm.f[c], nb % 3, i, j, k, nb < 3 ? -1 : 1) - f0;
+#pragma unroll
+        for (int a = 0; a < 3; a++) gr[a] = add_rn(gr[a], mul_rn(df, __ldg(g.lsw + (size_t)(nb * 3 + a) * plane + p)));
+      }
+#pragma unroll
+      for (int a = 0; a < 3; a++) G[c][a] = (double)gr[a];
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 3 && !CURV; a++) {
     if (g.P.n[a] == 1) {
 #pragma unroll
       for (int c = 0; c < 3; c++) G[c][a] = 0.0;
@@ -677,13 +720,31 @@ __device__ __forceinline__ T ugrid_neighbour(const DevGrid<T> &g, const TU *__re
   return T(__ldg(f + interior_index(g.P.n, idx[0], idx[1], idx[2])));
 }
 
-template <typename T, typename TU>
+// CURV: a non-rectilinear grid, gradient by grad_sr1_ls (src/invariants_m.f90:38-42) over the
+// same face-neighbour values.
+template <typename T, typename TU, bool CURV = false>
 __global__ void __launch_bounds__(256) k_invariants(DevGrid<T> g, FieldPtrs<TU> u, int have, FieldPtrsW<T> out, FieldPtrsW<T> out2) {
   int i, j, k;
   if (!node_of_thread(g.P.n, i, j, k)) return;
   T G[3][3];  // G[c][a] = d u_c / d x_a
+  if (CURV) {
+    const int p = pidx(g.P.sx, g.P.sxy, i, j, k);
+    const size_t plane = (size_t)g.P.sxy * (g.P.n[2] + 2);
 #pragma unroll
-  for (int a = 0; a < 3; a++) {
+    for (int c = 0; c < 3; c++) {
+      const T f0 = have ? T(__ldg(u.f[c] + interior_index(g.P.n, i, j, k))) : T(0);
+#pragma unroll
+      for (int a = 0; a < 3; a++) G[c][a] = T(0);
+#pragma unroll
+      for (int nb = 0; nb < 6; nb++) {
+        const T df = (have ? ugrid_neighbour<T, TU>(g, u.f[c], nb % 3, i, j, k, nb < 3 ? -1 : 1) : T(0)) - f0;
+#pragma unroll
+        for (int a = 0; a < 3; a++) G[c][a] = add_rn(G[c][a], mul_rn(df, __ldg(g.lsw + (size_t)(nb * 3 + a) * plane + p)));
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 3 && !CURV; a++) {
     const int idx[3] = {i, j, k};
     const T den = __ldg(g.lt[a] + idx[a] + 1) - __ldg(g.lt[a] + idx[a] - 1);
 #pragma unroll
@@ -756,7 +817,9 @@ __global__ void k_reset_particles(DevGrid<T> g, Particles<T> P) {
   if (!node_of_thread(g.P.n, i, j, k)) return;
   const int q = interior_index(g.P.n, i, j, k);
   const int nd[3] = {i, j, k};
-  const T x[3] = {__ldg(g.lt[0] + i), __ldg(g.lt[1] + j), __ldg(g.lt[2] + k)};
+  T x[3];
+  if (g.P.curv) node_xyz<T, true>(g, i, j, k, x);
+  else node_xyz<T, false>(g, i, j, k, x);
 #pragma unroll
   for (int c = 0; c < 3; c++) {
     P.x[c][q] = x[c];

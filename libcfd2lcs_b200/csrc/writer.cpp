@@ -203,13 +203,16 @@ bool LcsWriter::write_job(const OutputJob &job, const char *staging, std::string
     const double *ly = job.lines[1] ? job.lines[1]->data() : nullptr;
     const double *lz = job.lines[2] ? job.lines[2]->data() : nullptr;
     const int8_t *fl = job.flags ? job.flags->data() : nullptr;
+    const double *cx = job.coords[0] ? job.coords[0]->data() : nullptr;
+    const double *cy = job.coords[1] ? job.coords[1]->data() : nullptr;
+    const double *cz = job.coords[2] ? job.coords[2]->data() : nullptr;
     auto get = [&](long q) -> double {
       switch (b.kind) {
         case OutputBlock::STAGED_F64: return f64[q];
         case OutputBlock::STAGED_F32: return (double)f32[q];
-        case OutputBlock::LINE_X: return lx[q % ni];
-        case OutputBlock::LINE_Y: return ly[(q / ni) % nj];
-        case OutputBlock::LINE_Z: return lz[q / (ni * nj)];
+        case OutputBlock::LINE_X: return cx ? cx[q] : lx[q % ni];
+        case OutputBlock::LINE_Y: return cy ? cy[q] : ly[(q / ni) % nj];
+        case OutputBlock::LINE_Z: return cz ? cz[q] : lz[q / (ni * nj)];
         case OutputBlock::FLAG: return fl ? (double)fl[q] : 0.0;
         default: return 0.0;
       }

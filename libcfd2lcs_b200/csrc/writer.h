@@ -43,6 +43,9 @@ struct OutputJob {
   long n[3] = {0, 0, 0};
   // grid lines (x by i, y by j, z by k) and interior flags, shared with the engine
   std::shared_ptr<const std::vector<double>> lines[3];
+  // non-rectilinear grids: the node coordinates themselves (interior, i fastest), used instead
+  // of the lines
+  std::shared_ptr<const std::vector<double>> coords[3];
   std::shared_ptr<const std::vector<int8_t>> flags;
   long points = -1;  // >= 0: POINT packing of that many particles (blocks x, y, z), one per line
   cudaEvent_t ready = nullptr;  // staged copies complete

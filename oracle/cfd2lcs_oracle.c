@@ -97,6 +97,13 @@ typedef struct sgrid_s {
     real ps[3][3][3][3]; /* periodic_shift(i,j,k,c) stored [k+1][j+1][i+1][c] */
     real bb[6];
     int scomm_flag[3][3][3]; /* max-connectivity SELF/NO comm flag per direction */
+    /* non-rectilinear grids: least-squares gradient weights of the six face neighbours
+     * (compute_lsgw with full_conn = .false., sgrid_m.f90:421-424; nbr = 2..7 of NBR_OFFSET,
+     * stored at [nbr-2][component], padded, zero on the ghost layer), and the positions of
+     * the smallest / largest coordinate (minloc / maxloc over the padded arrays, counted from
+     * 1 as Fortran returns them) for the node guess of exchange_lp_alltoall */
+    real *lsw[6][3];
+    real ijk_min[3][3], ijk_max[3][3]; /* [coordinate][direction] */
 } sgrid_t;
 
 typedef struct {
@@ -260,7 +267,7 @@ static void check_rectilinear(sgrid_t *g) {
     /* sgrid_m.f90:868-949 (including the z loop's 1:k with k = nk+1 left over) */
     const dims_t *d = &g->d;
     int ni = d->ni, nj = d->nj, nk = d->nk;
-    const real TOL = (real)1e-4;
+    const real TOL = (real)1e-4f; /* real(LCSRP),parameter:: TOL = 1e-4, a default-real literal */
     real mx[3], mn[3];
     for (int c = 0; c < 3; c++) { mx[c] = -R_HUGE; mn[c] = R_HUGE; }
     for (long p = 0; p < d->ntot; p++)
@@ -304,6 +311,37 @@ static void check_rectilinear(sgrid_t *g) {
     g->rectilinear = ortho[0] && ortho[1] && ortho[2];
 }
 
+/* compute_lsgw (gradient_m.f90:114-217) at interior node (i,j,k) for the neighbours
+ * nb = first..last of NBR_OFFSET: inverse-distance weights and the closed-form solution of
+ * the 3x3 least-squares system, w[nb][c].  Products and sums in the reference's order:
+ * sum(dx(1:3)**2) and idw*dx(a)**2 form the squares first; sdenom subtracts s*(t**2). */
+static void lsq_weights(const sgrid_t *g, int i, int j, int k, int first, int last, real w[27][3]) {
+    const dims_t *d = &g->d;
+    const real *X = g->grid.c[0], *Y = g->grid.c[1], *Z = g->grid.c[2];
+    long p = PX(d, i, j, k);
+    real sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
+    for (int nb = first; nb <= last; nb++) {
+        long q = PX(d, i + NBR[nb][0], j + NBR[nb][1], k + NBR[nb][2]);
+        real dx0 = X[q] - X[p], dx1 = Y[q] - Y[p], dx2 = Z[q] - Z[p];
+        real idw = (real)1 / (dx0 * dx0 + dx1 * dx1 + dx2 * dx2);
+        sxx = sxx + idw * (dx0 * dx0);
+        syy = syy + idw * (dx1 * dx1);
+        szz = szz + idw * (dx2 * dx2);
+        sxy = sxy + idw * dx0 * dx1;
+        sxz = sxz + idw * dx0 * dx2;
+        syz = syz + idw * dx1 * dx2;
+    }
+    real sden = (real)2 * sxy * sxz * syz + sxx * syy * szz - sxx * (syz * syz) - syy * (sxz * sxz) - szz * (sxy * sxy);
+    for (int nb = first; nb <= last; nb++) {
+        long q = PX(d, i + NBR[nb][0], j + NBR[nb][1], k + NBR[nb][2]);
+        real dx0 = X[q] - X[p], dx1 = Y[q] - Y[p], dx2 = Z[q] - Z[p];
+        real idw = (real)1 / (dx0 * dx0 + dx1 * dx1 + dx2 * dx2);
+        w[nb][0] = idw * ((syy * szz - syz * syz) * dx0 + (sxz * syz - sxy * szz) * dx1 + (sxy * syz - sxz * syy) * dx2) / sden;
+        w[nb][1] = idw * ((sxz * syz - sxy * szz) * dx0 + (sxx * szz - sxz * sxz) * dx1 + (sxy * sxz - syz * sxx) * dx2) / sden;
+        w[nb][2] = idw * ((sxy * syz - sxz * syy) * dx0 + (sxy * sxz - syz * sxx) * dx1 + (sxx * syy - sxy * sxy) * dx2) / sden;
+    }
+}
+
 static void compute_bcnorm(sgrid_t *g) {
     /* sgrid_m.f90:385-419 with compute_lsgw(full_conn) gradient_m.f90:114-217 and
      * grad_sr0_ls gradient_m.f90:297-335 */
@@ -318,36 +356,19 @@ static void compute_bcnorm(sgrid_t *g) {
             }
     exchange_self(g, &bc, 1, 1, 0);
     sr1_alloc(&g->bcnorm, d);
-    const real *X = g->grid.c[0], *Y = g->grid.c[1], *Z = g->grid.c[2];
     for (int k = 1; k <= d->nk; k++)
         for (int j = 1; j <= d->nj; j++)
             for (int i = 1; i <= d->ni; i++) {
                 long p = PX(d, i, j, k);
-                real sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
-                for (int nb = 1; nb < 27; nb++) {
-                    long q = PX(d, i + NBR[nb][0], j + NBR[nb][1], k + NBR[nb][2]);
-                    real dx0 = X[q] - X[p], dx1 = Y[q] - Y[p], dx2 = Z[q] - Z[p];
-                    real idw = (real)1 / (dx0 * dx0 + dx1 * dx1 + dx2 * dx2);
-                    sxx = sxx + idw * dx0 * dx0;
-                    syy = syy + idw * dx1 * dx1;
-                    szz = szz + idw * dx2 * dx2;
-                    sxy = sxy + idw * dx0 * dx1;
-                    sxz = sxz + idw * dx0 * dx2;
-                    syz = syz + idw * dx1 * dx2;
-                }
-                real sden = (real)2 * sxy * sxz * syz + sxx * syy * szz - sxx * syz * syz - syy * sxz * sxz - szz * sxy * sxy;
+                real w[27][3];
+                lsq_weights(g, i, j, k, 1, 26, w);
                 real gx = 0, gy = 0, gz = 0;
                 for (int nb = 1; nb < 27; nb++) {
                     long q = PX(d, i + NBR[nb][0], j + NBR[nb][1], k + NBR[nb][2]);
-                    real dx0 = X[q] - X[p], dx1 = Y[q] - Y[p], dx2 = Z[q] - Z[p];
-                    real idw = (real)1 / (dx0 * dx0 + dx1 * dx1 + dx2 * dx2);
-                    real wx = idw * ((syy * szz - syz * syz) * dx0 + (sxz * syz - sxy * szz) * dx1 + (sxy * syz - sxz * syy) * dx2) / sden;
-                    real wy = idw * ((sxz * syz - sxy * szz) * dx0 + (sxx * szz - sxz * sxz) * dx1 + (sxy * sxz - syz * sxx) * dx2) / sden;
-                    real wz = idw * ((sxy * syz - sxz * syy) * dx0 + (sxy * sxz - syz * sxx) * dx1 + (sxx * syy - sxy * sxy) * dx2) / sden;
                     real df = bc[q] - bc[p];
-                    gx = gx + df * wx;
-                    gy = gy + df * wy;
-                    gz = gz + df * wz;
+                    gx = gx + df * w[nb][0];
+                    gy = gy + df * w[nb][1];
+                    gz = gz + df * w[nb][2];
                 }
                 real mag = gx * gx + gy * gy + gz * gz;
                 if (mag <= 0) {
@@ -358,6 +379,57 @@ static void compute_bcnorm(sgrid_t *g) {
                 g->bcnorm.c[0][p] = gx; g->bcnorm.c[1][p] = gy; g->bcnorm.c[2][p] = gz;
             }
     free(bc);
+}
+
+/* Non-rectilinear grids (sgrid_m.f90:421-424): the face-neighbour least-squares weights, and
+ * minloc / maxloc of each coordinate for exchange_lp_alltoall's node guess
+ * (comms_m.f90:1625-1632). */
+static void compute_lsgw_face(sgrid_t *g) {
+    const dims_t *d = &g->d;
+    for (int nb = 0; nb < 6; nb++)
+        for (int c = 0; c < 3; c++) g->lsw[nb][c] = zalloc(d->ntot);
+    for (int k = 1; k <= d->nk; k++)
+        for (int j = 1; j <= d->nj; j++)
+            for (int i = 1; i <= d->ni; i++) {
+                real w[27][3];
+                lsq_weights(g, i, j, k, 1, 6, w);
+                long p = PX(d, i, j, k);
+                for (int nb = 1; nb <= 6; nb++)
+                    for (int c = 0; c < 3; c++) g->lsw[nb - 1][c][p] = w[nb][c];
+            }
+    for (int c = 0; c < 3; c++) {
+        /* the first position in array element order (i fastest) holding the extreme value */
+        long pmin = 0, pmax = 0;
+        for (long p = 1; p < d->ntot; p++) {
+            if (g->grid.c[c][p] < g->grid.c[c][pmin]) pmin = p;
+            if (g->grid.c[c][p] > g->grid.c[c][pmax]) pmax = p;
+        }
+        const long pp[2] = {pmin, pmax};
+        for (int e = 0; e < 2; e++) {
+            long p = pp[e];
+            real pos[3] = {(real)(p % d->sx + 1), (real)((p / d->sx) % (d->nj + 2) + 1), (real)(p / d->sy + 1)};
+            for (int a = 0; a < 3; a++) {
+                if (e == 0) g->ijk_min[c][a] = pos[a];
+                else g->ijk_max[c][a] = pos[a];
+            }
+        }
+    }
+}
+
+/* grad_sr1_ls / grad_sr0_ls (gradient_m.f90:241-335) of one component at padded node p:
+ * sum over the face neighbours of (f(nbr) - f(p)) * weight; zero on the ghost layer */
+static void grad_ls(const sgrid_t *g, const real *F, int i, int j, int k, real gr[3]) {
+    const dims_t *d = &g->d;
+    gr[0] = gr[1] = gr[2] = 0;
+    if (i < 1 || j < 1 || k < 1 || i > d->ni || j > d->nj || k > d->nk) return;
+    long p = PX(d, i, j, k);
+    for (int nb = 1; nb <= 6; nb++) {
+        long q = PX(d, i + NBR[nb][0], j + NBR[nb][1], k + NBR[nb][2]);
+        real df = F[q] - F[p];
+        gr[0] = gr[0] + df * g->lsw[nb - 1][0][p];
+        gr[1] = gr[1] + df * g->lsw[nb - 1][1][p];
+        gr[2] = gr[2] + df * g->lsw[nb - 1][2][p];
+    }
 }
 
 static int init_sgrid(sgrid_t *g, const int n[3], const real *x, const real *y, const real *z, const int *flag) {
@@ -532,6 +604,7 @@ static int init_sgrid(sgrid_t *g, const int n[3], const real *x, const real *y, 
     }
     check_rectilinear(g);
     compute_bcnorm(g);
+    if (!g->rectilinear) compute_lsgw_face(g);
     return 0;
 }
 
@@ -1007,6 +1080,8 @@ static void coord_lines(const sgrid_t *g, real **xg, real **yg, real **zg) {
 
 static void interp_r1(const sgrid_t *g, int method, int np, real *const *xp, int *const *no, const sr1_t *f, real *const *out) {
     const dims_t *d = &g->d;
+    /* non-rectilinear grids: TSE_LIMIT unless TSE was asked for (lp_tracking_m.f90:320-327) */
+    if (!g->rectilinear && method != TSE) method = TSE_LIMIT;
     switch (method) {
     case NEAREST_NBR:
 #pragma omp parallel for schedule(static)
@@ -1069,9 +1144,10 @@ static void interp_r1(const sgrid_t *g, int method, int np, real *const *xp, int
     case TSE: case TSE_LIMIT: {
         /* lp_tracking_m.f90:526-654: phi(no) + grad(phi)(no) . (x - x(no)); grad_sr1 fills
          * interior nodes only (the ghost layer of the gradient array stays zero) and zeroes
-         * the derivatives along a singleton axis.  TSE_LIMIT clamps to the 27 values around no;
-         * at a ghost node the reference reads outside its array there, and this restatement
-         * clips the window to the padded array. */
+         * the derivatives along a singleton axis; on non-rectilinear grids grad_sr1_ls
+         * (face-neighbour least squares, zero on the ghost layer) replaces it.  TSE_LIMIT
+         * clamps to the 27 values around no; at a ghost node the reference reads outside its
+         * array there, and this restatement clips the window to the padded array. */
         const int lim = method == TSE_LIMIT;
         const int nn[3] = {d->ni, d->nj, d->nk};
         const long st[3] = {PX(d, 1, 0, 0) - PX(d, 0, 0, 0), PX(d, 0, 1, 0) - PX(d, 0, 0, 0), PX(d, 0, 0, 1) - PX(d, 0, 0, 0)};
@@ -1084,9 +1160,11 @@ static void interp_r1(const sgrid_t *g, int method, int np, real *const *xp, int
             for (int c = 0; c < 3; c++) {
                 const real *F = f->c[c];
                 real gr[3] = {0, 0, 0}, dl[3];
+                if (!g->rectilinear) grad_ls(g, F, q[0], q[1], q[2], gr);
                 for (int a = 0; a < 3; a++) {
                     const real *X = g->grid.c[a];
-                    if (interior && g->gn[a] != 1) gr[a] = (F[p + st[a]] - F[p - st[a]]) / (X[p + st[a]] - X[p - st[a]]);
+                    if (g->rectilinear && interior && g->gn[a] != 1)
+                        gr[a] = (F[p + st[a]] - F[p - st[a]]) / (X[p + st[a]] - X[p - st[a]]);
                     dl[a] = xp[a][ip] - X[p];
                 }
                 real r = F[p] + dl[0] * gr[0] + dl[1] * gr[1] + dl[2] * gr[2];
@@ -1482,10 +1560,24 @@ static void alltoall_wrap(const sgrid_t *g, lp_t *lp, int ip) {
     real s = rmax(rmin((*x - bb[0]) / (bb[3] - bb[0]), (real)1.0), (real)0.0);
     real t = rmax(rmin((*y - bb[1]) / (bb[4] - bb[1]), (real)1.0), (real)0.0);
     real u = rmax(rmin((*z - bb[2]) / (bb[5] - bb[2]), (real)1.0), (real)0.0);
-    /* nint(real(ni)*s): real(ni) is a default (single precision) real */
-    lp->no[0][ip] = clampi(fnint((real)((float)d->ni) * s), 1, d->ni);
-    lp->no[1][ip] = clampi(fnint((real)((float)d->nj) * t), 1, d->nj);
-    lp->no[2][ip] = clampi(fnint((real)((float)d->nk) * u), 1, d->nk);
+    if (g->rectilinear) {
+        /* nint(real(ni)*s): real(ni) is a default (single precision) real */
+        lp->no[0][ip] = clampi(fnint((real)((float)d->ni) * s), 1, d->ni);
+        lp->no[1][ip] = clampi(fnint((real)((float)d->nj) * t), 1, d->nj);
+        lp->no[2][ip] = clampi(fnint((real)((float)d->nk) * u), 1, d->nk);
+    } else {
+        /* comms_m.f90:1662-1673: the node index guessed from the index positions of the
+         * coordinate extremes, nint(1/3 (imin_x + imin_y + imin_z)) + nint(1/3 (s (imax_x -
+         * imin_x) + t (imax_y - imin_y) + u (imax_z - imin_z))) per direction */
+        const real onethird = (real)1.0 / (real)3.0;
+        const int nn[3] = {d->ni, d->nj, d->nk};
+        for (int a = 0; a < 3; a++) {
+            int v = fnint(onethird * (g->ijk_min[0][a] + g->ijk_min[1][a] + g->ijk_min[2][a])) +
+                    fnint(onethird * (s * (g->ijk_max[0][a] - g->ijk_min[0][a]) + t * (g->ijk_max[1][a] - g->ijk_min[1][a]) +
+                                      u * (g->ijk_max[2][a] - g->ijk_min[2][a])));
+            lp->no[a][ip] = clampi(v, 1, nn[a]);
+        }
+    }
     lp->flag[ip] = LP_UNKNOWN;
 }
 
@@ -1609,6 +1701,9 @@ static void compute_ftle(lcs_t *L) {
                         for (int c = 0; c < 3; c++)
                             G[c][a] = (real)fabs((double)den) > SMALL ? (A1->lp.fm.c[c][p] - A0->lp.fm.c[c][p]) / den : (real)0;
                     }
+                } else if (!g->rectilinear) {
+                    /* grad_sr1_ls (lcs_m.f90:129-133) */
+                    for (int c = 0; c < 3; c++) grad_ls(g, fm->c[c], i, j, k, G[c]);
                 } else {
                     for (int c = 0; c < 3; c++) {
                         const real *F = fm->c[c];
@@ -1752,15 +1847,20 @@ static void compute_invariants(lcs_t *L, const sr1_t *ugp) {
                 long pyp = PX(d, i, j + 1, k), pym = PX(d, i, j - 1, k);
                 long pzp = PX(d, i, j, k + 1), pzm = PX(d, i, j, k - 1);
                 real G[3][3]; /* G[c][a] = d u_c / d x_a */
-                for (int c = 0; c < 3; c++) {
-                    const real *F = ug.c[c];
-                    G[c][0] = (F[pxp] - F[pxm]) / (X[pxp] - X[pxm]);
-                    G[c][1] = (F[pyp] - F[pym]) / (Y[pyp] - Y[pym]);
-                    G[c][2] = (F[pzp] - F[pzm]) / (Z[pzp] - Z[pzm]);
+                if (!g->rectilinear) {
+                    /* grad_sr1_ls (invariants_m.f90:38-42) */
+                    for (int c = 0; c < 3; c++) grad_ls(g, ug.c[c], i, j, k, G[c]);
+                } else {
+                    for (int c = 0; c < 3; c++) {
+                        const real *F = ug.c[c];
+                        G[c][0] = (F[pxp] - F[pxm]) / (X[pxp] - X[pxm]);
+                        G[c][1] = (F[pyp] - F[pym]) / (Y[pyp] - Y[pym]);
+                        G[c][2] = (F[pzp] - F[pzm]) / (Z[pzp] - Z[pzm]);
+                    }
+                    for (int a = 0; a < 3; a++)
+                        if (g->gn[a] == 1)
+                            for (int c = 0; c < 3; c++) G[c][a] = 0;
                 }
-                for (int a = 0; a < 3; a++)
-                    if (g->gn[a] == 1)
-                        for (int c = 0; c < 3; c++) G[c][a] = 0;
                 const real d1u1 = G[0][0], d2u1 = G[0][1], d3u1 = G[0][2];
                 const real d1u2 = G[1][0], d2u2 = G[1][1], d3u2 = G[1][2];
                 const real d1u3 = G[2][0], d2u3 = G[2][1], d3u3 = G[2][2];
@@ -1971,6 +2071,8 @@ static void free_lcs(lcs_t *L) {
     free(L->written);
     if (L->own_sg) {
         sr1_free(&L->sg->grid); sr1_free(&L->sg->bcnorm); free(L->sg->bcflag);
+        for (int nb = 0; nb < 6; nb++)
+            for (int c = 0; c < 3; c++) free(L->sg->lsw[nb][c]);
         free(L->sg);
     }
     free(L);
@@ -1983,6 +2085,8 @@ EXPORT void orc_reset(void) {
         for (int q = 0; q < MAXVSTEP; q++) free(S.vring[c][q]);
     if (S.inited) {
         sr1_free(&S.g.grid); sr1_free(&S.g.bcnorm); free(S.g.bcflag);
+        for (int nb = 0; nb < 6; nb++)
+            for (int c = 0; c < 3; c++) free(S.g.lsw[nb][c]);
         sr1_free(&S.u_n); sr1_free(&S.u_np1); sr1_free(&S.delta);
     }
     char keep[sizeof S.outdir];
@@ -2002,10 +2106,6 @@ EXPORT void orc_init(const int n[3], const int offset[3], const real *x, const r
     S.nlcs = 0;
     S.integrations_fwd = S.integrations_bkwd = 0;
     if (init_sgrid(&S.g, n, x, y, z, flag)) return;
-    if (!S.g.rectilinear) {
-        latch("init: grid is not rectilinear (the TSE/least-squares path is not restated)");
-        return;
-    }
     sr1_alloc(&S.u_n, &S.g.d);
     sr1_alloc(&S.u_np1, &S.g.d);
     compute_delta(&S.g, &S.delta);
@@ -2027,6 +2127,10 @@ static sgrid_t *new_sgrid(int *res_io) {
     const sgrid_t *g = &S.g;
     const dims_t *d = &g->d;
     int res = *res_io;
+    if (!g->rectilinear && res != 0) {
+        latch("new_sgrid_from_sgrid: resolution /= 0 on a non-rectilinear grid is not restated");
+        return NULL;
+    }
     const int n[3] = {d->ni, d->nj, d->nk};
     for (int a = 0; a < 3; a++)
         if (n[a] > 1 && abs(res) >= n[a]) res = 0;
@@ -2550,6 +2654,19 @@ EXPORT void orc_get_grid(real *xyz, int *flag, real *nrm, real *inv_delta, int *
 /* interp_s2u_r1 with `method` on the initialised solver grid for np points (pts: x block, y
  * block, z block) with their nodes (padded indices, same layout); f3 holds three padded fields
  * of orc_padded_size() values, x fastest.  out receives the three components, one block each. */
+/* compute_lsgw's face weights of a non-rectilinear grid: 18 padded arrays [nbr-2][component]
+ * (all zero on a rectilinear grid); returns sgrid%rectilinear */
+EXPORT int orc_get_lsq_weights(real *w) {
+    const dims_t *d = &S.g.d;
+    for (int nb = 0; nb < 6; nb++)
+        for (int c = 0; c < 3; c++) {
+            real *o = w + (long)(nb * 3 + c) * d->ntot;
+            if (S.g.lsw[nb][c]) memcpy(o, S.g.lsw[nb][c], sizeof(real) * (size_t)d->ntot);
+            else memset(o, 0, sizeof(real) * (size_t)d->ntot);
+        }
+    return S.g.rectilinear;
+}
+
 EXPORT int orc_interp_points(int method, const real *f3, int np, const real *pts, const int *nodes, real *out) {
     if (!S.inited) return 1;
     const long nt = S.g.d.ntot;

@@ -70,6 +70,8 @@ class Oracle:
         L.orc_counter.restype = C.c_longlong
         L.orc_padded_size.restype = C.c_long
         L.orc_get_grid.argtypes = [P, P, P, P, P]
+        L.orc_get_lsq_weights.argtypes = [P]
+        L.orc_get_lsq_weights.restype = C.c_int
         L.orc_eig3_max.argtypes = [P]
         L.orc_eig3_max.restype = C.c_double
         L.orc_bspline3.argtypes = [P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int, P, P, P, P]
@@ -198,6 +200,15 @@ class Oracle:
             inv_delta=inv.reshape((3,) + shp).transpose(0, 3, 2, 1),
             periodic=per.astype(bool),
         )
+
+    def lsq_weights(self):
+        """(rectilinear, weights): compute_lsgw's face-neighbour weights, shape
+        (6 neighbours, 3 components, ni+2, nj+2, nk+2); zeros on a rectilinear grid."""
+        nt = int(self.lib.orc_padded_size())
+        w = np.zeros(18 * nt, dtype=self.dtype)
+        rect = int(self.lib.orc_get_lsq_weights(self._p(w)))
+        shp = tuple(v + 2 for v in self.n[::-1])
+        return bool(rect), w.reshape((6, 3) + shp).transpose(0, 1, 4, 3, 2)
 
     # --- unit helpers ----------------------------------------------------------------
     def eig3_max(self, a):

@@ -1,6 +1,6 @@
 """FTLE error of the mixed-precision form against the plain FP64 form on the same inputs.
 
-    python -m libcfd2lcs_b200.accuracy --n 128 --T 10 --h 1 --updates 201
+    python -m tests.accuracy --n 128 --T 10 --h 1 --updates 201
 
 Runs the ABC workload twice through the C ABI (plain FP64, then MIXED_PRECISION), each for the
 same number of updates, and reports max / RMS differences of the FTLE fields and composed
@@ -22,7 +22,7 @@ def run(mixed: bool, n: int, T: float, h: float, dt: float, updates: int, integr
     import torch
 
     import libcfd2lcs_b200 as L
-    from libcfd2lcs_b200 import workloads as W
+    from tests import workloads as W
 
     api = L.Cfd2lcs("dp")
     api.reset()

@@ -4,7 +4,7 @@ Runs the oracle -- the plain-C restatement of libcfd2lcs's single-rank path, bui
 oracle/cfd2lcs_oracle.c -- on the benchmark configurations over their full FTLE horizon and
 stores, per diagnostic, the last frame's FTLE field (FP64, every point), the composed flow
 map on every 16th point (FP64) and the reference's work counters.  The inputs are the
-seeded synthetic flows of libcfd2lcs_b200.workloads, regenerated identically by the test.
+seeded synthetic flows of tests.workloads, regenerated identically by the test.
 
     python tests/golden/make_golden.py [dg512 abc48 turb48] [--threads N]
 
@@ -32,7 +32,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-from libcfd2lcs_b200 import workloads as W  # noqa: E402
+from tests import workloads as W  # noqa: E402
 
 FM_STRIDE = 16  # composed flow map stored on every 16th point (flat i-fastest index)
 

@@ -6,7 +6,7 @@ import math
 
 import numpy as np
 
-from libcfd2lcs_b200 import workloads as W
+from tests import workloads as W
 
 
 def rk_matrix(A: np.ndarray, dt: float, integrator: int) -> np.ndarray:

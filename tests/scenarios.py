@@ -5,7 +5,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from libcfd2lcs_b200 import workloads as W
+from tests import workloads as W
 
 FTLE_FWD, FTLE_BKWD = 0, 1
 
@@ -72,6 +72,74 @@ def make_case(name: str, n: int | None = None):
         g = W.abc_grid(n or 12)
         modes = W.turbulence_modes(nmodes=16, kmin=1, kmax=3, seed=20261203)
         return g, (lambda t: W.turbulence_velocity(g, t, modes, dtype=np.float64)), dict(T=0.2, h=0.05, dt=0.02, steps=16)
+    if name in ("curv_box", "curv_periodic", "curv_dg"):
+        g = curvilinear_grid(name, n)
+        return g, curvilinear_velocity(name, g), dict(T=0.6, h=0.2, dt=0.05, steps=16)
+    raise KeyError(name)
+
+
+def curvilinear_grid(name: str, n: int | None = None):
+    """Non-rectilinear grids (the reference's least-squares / TSE_LIMIT path): smooth
+    deformations of a box well above check_rectilinear's 1e-4 tolerance.
+      curv_box       3-D, slip walls in x and y, walls in z;
+      curv_periodic  3-D cube [0, 2 pi)^3 periodic in every direction, deformed by periodic
+                     sines (its ghost shifts follow the reference's mirror-minus-image rule);
+      curv_dg        2-D (z singleton) box [0, 2] x [0, 1] with slip walls."""
+    if name == "curv_box":
+        nx, ny, nz = (n or 12), (n or 12) - 2, (n or 12) - 4
+        a, b, c = np.meshgrid(np.linspace(0, 1, nx), np.linspace(0, 1, ny), np.linspace(0, 1, nz), indexing="ij")
+        X = a + 0.03 * np.sin(2 * np.pi * b) * np.sin(np.pi * c)
+        Y = b + 0.03 * np.sin(2 * np.pi * a) * np.sin(np.pi * c)
+        Z = c + 0.02 * np.sin(np.pi * a) * np.sin(np.pi * b)
+        flag = np.zeros(X.shape, dtype=np.int32)
+        flag[0, :, :] = flag[-1, :, :] = W.LCS_SLIP
+        flag[:, 0, :] = flag[:, -1, :] = W.LCS_SLIP
+        flag[:, :, 0] = flag[:, :, -1] = W.LCS_WALL
+    elif name == "curv_periodic":
+        m = n or 12
+        ln = (np.arange(m) + 0.5) * (2 * np.pi / m)
+        a, b, c = np.meshgrid(ln, ln, ln, indexing="ij")
+        X = a + 0.08 * np.sin(b) * np.sin(c)
+        Y = b + 0.08 * np.sin(c) * np.sin(a)
+        Z = c + 0.08 * np.sin(a) * np.sin(b)
+        flag = np.zeros(X.shape, dtype=np.int32)
+    elif name == "curv_dg":
+        nx = n or 32
+        ny = nx // 2
+        a, b, c = np.meshgrid(np.linspace(0, 2, nx), np.linspace(0, 1, ny), np.zeros(1), indexing="ij")
+        X = a + 0.03 * np.sin(np.pi * b) * np.sin(np.pi * a / 2)
+        Y = b + 0.02 * np.sin(np.pi * a)
+        Z = c
+        flag = np.zeros(X.shape, dtype=np.int32)
+        flag[0, :, :] = flag[-1, :, :] = W.LCS_SLIP
+        flag[:, 0, :] = flag[:, -1, :] = W.LCS_SLIP
+    else:
+        raise KeyError(name)
+    f = np.asfortranarray
+    return W.Grid(X.shape, f(X), f(Y), f(Z), f(flag))
+
+
+def curvilinear_velocity(name: str, g):
+    """Smooth unsteady velocity evaluated at the deformed node coordinates."""
+    if name == "curv_box":
+        def vel(t):
+            x, y, z = g.x, g.y, g.z
+            u = -0.6 * (y - 0.5) + 0.05 * np.sin(2 * np.pi * z) * np.cos(t)
+            v = 0.6 * (x - 0.5) + 0.03 * np.cos(np.pi * z + t)
+            w = 0.08 * np.sin(np.pi * x) * np.sin(np.pi * y) * np.cos(2 * t)
+            return np.asfortranarray(u), np.asfortranarray(v), np.asfortranarray(w)
+        return vel
+    if name == "curv_periodic":
+        def vel(t):
+            x, y, z = g.x, g.y, g.z
+            A, B, C = np.sqrt(3.0), np.sqrt(2.0), 1.0
+            u = A * np.sin(z) + C * np.cos(y) * (1 + 0.2 * np.sin(t))
+            v = B * np.sin(x) + A * np.cos(z)
+            w = C * np.sin(y) + B * np.cos(x)
+            return np.asfortranarray(u), np.asfortranarray(v), np.asfortranarray(w)
+        return vel
+    if name == "curv_dg":
+        return lambda t: W.double_gyre_velocity(g, t)
     raise KeyError(name)
 
 

@@ -7,6 +7,7 @@ import re
 import pytest
 
 import libcfd2lcs_b200 as L
+from tests import workloads as W
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -48,7 +49,7 @@ def test_no_cpu_fallback_without_gpu():
         pytest.skip("a GPU is present")
     api = L.Cfd2lcs("dp")
     api.reset()
-    g = L.workloads.abc_grid(4)
+    g = W.abc_grid(4)
     api.init(g.n, g.x, g.y, g.z, g.flag)
     err, msg = api.error()
     assert err == 1 and "CUDA" in msg

@@ -7,7 +7,7 @@ import math
 import numpy as np
 import pytest
 
-from libcfd2lcs_b200 import workloads as W
+from tests import workloads as W
 
 pytestmark = pytest.mark.gpu
 

@@ -4,7 +4,7 @@ inputs), for mixed grid kinds, sizes, directions and horizons advanced by one ca
 import numpy as np
 import pytest
 
-from libcfd2lcs_b200 import workloads as W
+from tests import workloads as W
 from tests import scenarios as SC
 
 pytestmark = pytest.mark.gpu

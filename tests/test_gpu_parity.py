@@ -138,7 +138,7 @@ def test_mixed_precision_form(oracle_dp, gpu_dp, case, integrator, interp):
 
 
 def _run_with_invariants(api, case, directions, integrator, interpolator):
-    from libcfd2lcs_b200 import workloads as W
+    from tests import workloads as W
     g, vel, prm = SC.make_case(case)
     api.reset()
     api.init(g.n, g.x, g.y, g.z, g.flag)

@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import libcfd2lcs_b200 as L
-from libcfd2lcs_b200 import workloads as W
+from tests import workloads as W
 
 
 def _mk(xl, yl, zl, fn=None):
@@ -78,13 +78,16 @@ def test_grid_tables_match_oracle(oracle_dp, name):
     assert np.max(np.abs(go["bcnorm"][:, sel] - gp["bcnorm"][:, sel]), initial=0.0) <= 1e-15
 
 
-def test_rejects_curvilinear_and_bad_periodicity():
+def test_grid_classes_and_bad_periodicity():
     api = L.Cfd2lcs("dp")
     n, x, y, z, f = CASES["abc_periodic"]
     x2 = x.copy()
-    x2[3, 2, 1] += 1e-3
+    x2[3, 2, 1] += 1e-3  # 1.6e-4 of the domain: non-rectilinear, the full-array (least-squares) form
+    assert api.grid_lsq_weights(n, x2, y, z, f)[0]
+    x3 = x.copy()
+    x3[3, 2, 1] += 1e-6  # within check_rectilinear's 1e-4 but not a tensor product: refused
     with pytest.raises(ValueError, match="tensor product"):
-        api.grid_tables(n, x2, y, z, f)
+        api.grid_tables(n, x3, y, z, f)
     f2 = f.copy()
     f2[0, :, :] = W.LCS_WALL  # one x face walled, the other internal
     with pytest.raises(ValueError, match="eriodicity"):

@@ -6,7 +6,7 @@ import os
 import numpy as np
 import pytest
 
-from libcfd2lcs_b200 import workloads as W
+from tests import workloads as W
 from tests import scenarios as SC
 
 LP_TRACER = 2

@@ -10,7 +10,7 @@ library against the oracle with the LINEAR parity bounds (flow map 1e-12 L, FTLE
 import numpy as np
 import pytest
 
-from libcfd2lcs_b200 import workloads as W
+from tests import workloads as W
 from tests import scenarios as SC
 
 TSE, TSE_LIMIT = 5, 6

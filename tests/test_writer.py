@@ -8,7 +8,7 @@ import os
 import numpy as np
 import pytest
 
-from libcfd2lcs_b200 import workloads as W
+from tests import workloads as W
 from tests import scenarios as SC
 
 

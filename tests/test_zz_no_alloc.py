@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 from tests import scenarios as SC
+from tests import workloads as W
 
 pytestmark = pytest.mark.gpu
 
@@ -55,7 +56,7 @@ def test_reconstruct_noalloc_rejects_without_frame():
 
     api = L.Cfd2lcs("dp")
     api.reset()
-    g = L.workloads.abc_grid(8)
+    g = W.abc_grid(8)
     api.init(g.n, g.x, g.y, g.z, g.flag)
     h = api.diagnostic_init(SC.FTLE_BKWD, 0, 1.0, 0.5)
     assert api.error()[0] == 0
@@ -69,7 +70,7 @@ def test_reconstruct_noalloc_rejects_more_submaps_than_its_table():
     """A frame of 257 sub-flow maps (T/h = 257; exact binary times so that every slot is
     written) exceeds the fixed 256-entry table: rejected with an error, nothing written."""
     import libcfd2lcs_b200 as L
-    from libcfd2lcs_b200 import workloads as W
+    from tests import workloads as W
 
     api = L.Cfd2lcs("dp")
     api.reset()
@@ -89,7 +90,7 @@ def test_reconstruct_noalloc_rejects_more_submaps_than_its_table():
 
 def test_reconstruct_noalloc_rejects_refined_grids():
     import libcfd2lcs_b200 as L
-    from libcfd2lcs_b200 import workloads as W
+    from tests import workloads as W
 
     api = L.Cfd2lcs("dp")
     api.reset()
