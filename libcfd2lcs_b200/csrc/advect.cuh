@@ -245,8 +245,9 @@ struct VelFields {  // T: velocity storage type
   const T *cs[4][3];
 };
 
-// Positions and stencils in T (the position / flow-map type); velocity data in TV.
-template <typename T, typename TV, int INTERP>
+// Positions and stencils in T (the position / flow-map type); velocity data in TV.  UNI: the
+// uniform-knot basis for the B-splines (spline.cuh).
+template <typename T, typename TV, int INTERP, bool UNI = uniform_basis<T, TV>()>
 __device__ __forceinline__ void sample_velocity(const DevGrid<T> &g, const SplineAxes<T> &sa, const VelFields<TV> &V, const T x[3],
                                                 const int no[3], T ct_, int stage, T out[3]) {
   const TV ct = TV(ct_);
@@ -281,7 +282,6 @@ __device__ __forceinline__ void sample_velocity(const DevGrid<T> &g, const Splin
     }
   } else {
     constexpr int KC = INTERP == INTERP_SPLINE4 ? 4 : 0;
-    constexpr bool UNI = !std::is_same<T, TV>::value;
     SplineStencil<T> st;
     if (!spline_stencil<T, KC, UNI>(g, sa, x, no, st)) {
       out[0] = out[1] = out[2] = T(0);
@@ -355,14 +355,14 @@ struct StageTimes {
 };
 
 // AT_NODE: xn is the coordinate of node no (first stage by sample_velocity_node)
-template <typename T, typename TV, int INTEG, int INTERP, bool AT_NODE = false>
+template <typename T, typename TV, int INTEG, int INTERP, bool AT_NODE = false, bool UNI = uniform_basis<T, TV>()>
 __device__ __forceinline__ void integrate(const DevGrid<T> &g, const SplineAxes<T> &sa, const VelFields<TV> &V, const StageTimes &S,
                                           T dt, const T xn[3], const int no[3], T x[3]) {
   const T HALF = T(1) / T(2), THIRD = T(1) / T(3), TWOTHIRD = T(2) / T(3), SIXTH = T(1) / T(6), TWO = T(2);
   T u[3];
   auto first_stage = [&](T ct) {
     if (AT_NODE) sample_velocity_node<T, TV>(g, V, no, ct, u);
-    else sample_velocity<T, TV, INTERP>(g, sa, V, xn, no, ct, 0, u);
+    else sample_velocity<T, TV, INTERP, UNI>(g, sa, V, xn, no, ct, 0, u);
   };
   if (INTEG == EULER_ || INTEG == TRAPEZOIDAL_) {
     first_stage(T(S.ct[0]));
@@ -373,7 +373,7 @@ __device__ __forceinline__ void integrate(const DevGrid<T> &g, const SplineAxes<
     T xh[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) xh[c] = xn[c] + HALF * dt * u[c];
-    sample_velocity<T, TV, INTERP>(g, sa, V, xh, no, T(S.ct[1]), 1, u);
+    sample_velocity<T, TV, INTERP, UNI>(g, sa, V, xh, no, T(S.ct[1]), 1, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) x[c] = xn[c] + dt * u[c];
   } else if (INTEG == RK3_) {
@@ -385,14 +385,14 @@ __device__ __forceinline__ void integrate(const DevGrid<T> &g, const SplineAxes<
       acc[c] = xn[c] + SIXTH * k[c];
       xs[c] = xn[c] + HALF * k[c];
     }
-    sample_velocity<T, TV, INTERP>(g, sa, V, xs, no, T(S.ct[1]), 1, u);
+    sample_velocity<T, TV, INTERP, UNI>(g, sa, V, xs, no, T(S.ct[1]), 1, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];
       xs[c] = xn[c] + TWO * k[c];
       acc[c] = acc[c] + TWOTHIRD * k[c];
     }
-    sample_velocity<T, TV, INTERP>(g, sa, V, xs, no, T(S.ct[2]), 2, u);
+    sample_velocity<T, TV, INTERP, UNI>(g, sa, V, xs, no, T(S.ct[2]), 2, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];
@@ -407,21 +407,21 @@ __device__ __forceinline__ void integrate(const DevGrid<T> &g, const SplineAxes<
       acc[c] = xn[c] + SIXTH * k[c];
       xs[c] = xn[c] + HALF * k[c];
     }
-    sample_velocity<T, TV, INTERP>(g, sa, V, xs, no, T(S.ct[1]), 1, u);
+    sample_velocity<T, TV, INTERP, UNI>(g, sa, V, xs, no, T(S.ct[1]), 1, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];
       acc[c] = acc[c] + THIRD * k[c];
       xs[c] = xn[c] + HALF * k[c];
     }
-    sample_velocity<T, TV, INTERP>(g, sa, V, xs, no, T(S.ct[2]), 2, u);
+    sample_velocity<T, TV, INTERP, UNI>(g, sa, V, xs, no, T(S.ct[2]), 2, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];
       acc[c] = acc[c] + THIRD * k[c];
       xs[c] = xn[c] + k[c];
     }
-    sample_velocity<T, TV, INTERP>(g, sa, V, xs, no, T(S.ct[3]), 3, u);
+    sample_velocity<T, TV, INTERP, UNI>(g, sa, V, xs, no, T(S.ct[3]), 3, u);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       k[c] = dt * u[c];

@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(256, sl_min_blocks<INTERP>()) k_sl_subcycle(De
   }
   T fmp[3];
   const int nod[3] = {i, j, k};
-  sample_field<T, INTERP, !std::is_same<T, TV>::value>(g, sa, fmo.f, x, nod, fmp);
+  sample_field<T, INTERP, uniform_basis<T, TV>()>(g, sa, fmo.f, x, nod, fmp);
   const int fl = HAS_FLAGS ? (int)g.flag[p] : (int)LCS_INTERNAL;
   const T mask = fl != LCS_MASK ? T(1) : T(0);
   T vpre[3], vfin[3];
@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(256) k_sl_refined(DevGrid<T> gl, DevGrid<T> gs
   no2[q] = no[2];
   T fmp[3];
   const int nod[3] = {i, j, k};
-  sample_field<T, INTERP, !std::is_same<T, TV>::value>(gl, sal, fmo.f, x, nod, fmp);
+  sample_field<T, INTERP, uniform_basis<T, TV>()>(gl, sal, fmo.f, x, nod, fmp);
   const T mask = fs != LCS_MASK ? T(1) : T(0);
   const int fl = FL ? (int)gl.flag[p] : (int)LCS_INTERNAL;
   const bool zero = FL && (fl == LCS_MASK || fl == LCS_INFLOW || fl == LCS_OUTFLOW);
@@ -344,7 +344,7 @@ __global__ void __launch_bounds__(256, fwd_min_blocks<INTERP>()) k_fwd_subcycle(
   int no[3] = {P.no[0][q], P.no[1][q], P.no[2][q]};
   constexpr bool CURV = interp_is_curv(INTERP);
   T x[3];
-  integrate<T, TV, INTEG, INTERP>(g, sa, V, S, dt, xn, no, x);
+  integrate<T, TV, INTEG, INTERP, false, particle_uniform_basis()>(g, sa, V, S, dt, xn, no, x);
   project_plane<T, CURV>(g, no, x);
   const bool stick = particle_bc<T, HAS_FLAGS, CURV>(g, no, x, err);
   if (stick) {
@@ -457,7 +457,7 @@ __global__ void __launch_bounds__(256) k_compose(DevGrid<T> g, SplineAxes<T> sa,
     project_plane<T, CURV>(g, no, x);
     particle_bc<T, HAS_FLAGS, CURV>(g, no, x, err);
     T up[3];
-    sample_field<T, INTERP>(g, sa, f, x, no, up);
+    sample_field<T, INTERP, particle_uniform_basis()>(g, sa, f, x, no, up);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       x[c] = x[c] + up[c];
@@ -503,7 +503,7 @@ __global__ void __launch_bounds__(256, MINB) k_compose_step(DevGrid<T> g, Spline
   project_plane<T, CURV>(g, no, x);
   particle_bc<T, HAS_FLAGS, CURV>(g, no, x, err);
   T up[3];
-  sample_field<T, INTERP>(g, sa, f.f, x, no, up);
+  sample_field<T, INTERP, particle_uniform_basis()>(g, sa, f.f, x, no, up);
 #pragma unroll
   for (int c = 0; c < 3; c++) {
     x[c] = x[c] + up[c];

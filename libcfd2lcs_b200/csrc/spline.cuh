@@ -14,6 +14,8 @@
 // here from the k non-zero basis values per axis (Cox-de Boor, as dbspvn :2288-2370).
 #pragma once
 
+#include <type_traits>
+
 #include "device_common.cuh"
 
 namespace cfd2lcs {
@@ -62,6 +64,21 @@ __device__ __forceinline__ int knot_interval(const T *t, T x, int lo, int hi, in
   return l;
 }
 
+// Which kernels take the uniform-knot basis below (the same values as the recurrence to
+// rounding; kernels that must give each other's bits make the same choice): the backward
+// semi-Lagrangian kernels, gathering and staged, when they gather FP32 velocity taps (the mixed
+// form); the particle kernels -- the forward subcycle, gathering and staged, and the composition
+// -- always.  Measured on B200 (ABC 256^3, RK3, cubic, FP64): the gathering forward kernel 6.63
+// -> 6.32 ms per launch with it, the staged backward kernel 3.15 -> 3.18 ms.
+template <typename T, typename TV>
+__host__ __device__ constexpr bool uniform_basis() {
+  return !std::is_same<T, TV>::value;
+}
+#ifndef CFD2LCS_PARTICLE_UNI
+#define CFD2LCS_PARTICLE_UNI 1
+#endif
+__host__ __device__ constexpr bool particle_uniform_basis() { return CFD2LCS_PARTICLE_UNI != 0; }
+
 // KC: the order when it is known at compile time for every axis (4 for cubic on a 3-D grid),
 // 0 for the general case.  UNI: take the uniform-knot form where the knots allow it.
 template <typename T, int KC, bool UNI = false>
@@ -69,9 +86,8 @@ __device__ __forceinline__ void basis_values(const SplineAxis<T> &A, int l, T x,
   const int k = KC ? KC : A.k;
   // equally spaced knots (interior intervals of a uniform grid): the uniform B-spline
   // polynomials of u = (x - t(l)) / h -- the same values as the recurrence below to rounding,
-  // from one paired table read instead of 3(k-1).  Measured on B200: faster in the kernels
-  // that gather FP32 velocity taps, slower in the all-FP64 backward kernel, so it is chosen
-  // per kernel.
+  // from one paired table read instead of 3(k-1).  Chosen per kernel (uniform_basis,
+  // particle_uniform_basis above).
   const typename Pair2<T>::type q =
       UNI ? __ldg(reinterpret_cast<const typename Pair2<T>::type *>(A.tu) + (l - 1)) : typename Pair2<T>::type{};
   const T iu = q.y;

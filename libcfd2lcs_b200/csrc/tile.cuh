@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLT_MINB)
   extern __shared__ __align__(128) unsigned char slt_smem_raw[];
   unsigned char *const slt_smem = smem_aligned128(slt_smem_raw);
   __shared__ __align__(8) uint64_t bar;
-  constexpr bool UNI = !std::is_same<T, TV>::value;
+  constexpr bool UNI = uniform_basis<T, TV>();
   constexpr int NOFF = INTEG == RK2_ ? 1 : (INTEG == RK3_ ? 2 : (INTEG == RK4_ ? 3 : 0));  // stages off the node
   const T HALF = T(1) / T(2), THIRD = T(1) / T(3), TWOTHIRD = T(2) / T(3), SIXTH = T(1) / T(6), TWO = T(2);
   const int tid = threadIdx.x + 32 * (threadIdx.y + SLT_Y * threadIdx.z);
@@ -716,7 +716,7 @@ __global__ void __launch_bounds__(FWT_THREADS, CFD2LCS_FWT_MINB)
   extern __shared__ __align__(128) unsigned char fwt_smem_raw[];
   unsigned char *const fwt_smem = smem_aligned128(fwt_smem_raw);
   __shared__ __align__(8) uint64_t bar;
-  constexpr bool UNI = !std::is_same<T, TV>::value;
+  constexpr bool UNI = particle_uniform_basis();  // as k_fwd_subcycle
   constexpr int NS = INTEG == RK2_ ? 2 : (INTEG == RK3_ ? 3 : (INTEG == RK4_ ? 4 : 1));  // samples per step
   const T HALF = T(1) / T(2), THIRD = T(1) / T(3), TWOTHIRD = T(2) / T(3), SIXTH = T(1) / T(6), TWO = T(2);
   const long ntiles = (long)st.ntx * st.nty * st.ntz;

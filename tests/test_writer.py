@@ -165,6 +165,7 @@ def _compare_files(pa, pb, rtol, bitwise_blocks, flag_blocks=(), skip_blocks=())
     ("abc_unsteady", 2, 1, {"VELOCITY_INVARIANTS": 1, "WRITE_BCFLAG": 1}),
     ("mixed_bc", 3, 3, {}),
     ("dg", 2, 1, {"WRITE_FLOWMAP": 0, "WRITE_VELOCITY": 0, "WRITE_LCS_ASYNC": 1}),
+    ("curv_box", 2, 6, {"VELOCITY_INVARIANTS": 1}),  # non-rectilinear: node coordinates, not lines
 ])
 def test_writer_matches_oracle(oracle_dp, gpu_dp, tmp_path, monkeypatch, case, integrator, interp, opts):
     """Same files, names and headers as the oracle's; grid and flag blocks identical text;
