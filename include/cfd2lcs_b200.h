@@ -189,6 +189,22 @@ int cfd2lcs_tangent_ftle_c(const int n[3], const lcsdata_t *x, const lcsdata_t *
                            const lcsdata_t *const *d_du, const lcsdata_t *const *d_dv, const lcsdata_t *const *d_dw, double *J,
                            double *dJ, char *msg, size_t len);
 
+/* The two calls above with the interpolator chosen: LINEAR or CUBIC (the not-a-knot cubic
+ * B-spline of every axis, the library's cubic path; at least 3 points per direction).  With
+ * CUBIC the reverse sweep scatters into the spline coefficients and carries that adjoint back
+ * through the transposed banded solves of each fit; the tangent model fits the direction's
+ * levels and the tangent map alongside. */
+int cfd2lcs_adjoint_ftle_interp_c(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, int integrator,
+                                  int interpolator, lcsdata_t cfl, int nlevels, const lcsdata_t *const *d_u,
+                                  const lcsdata_t *const *d_v, const lcsdata_t *const *d_w, const lcsdata_t *times,
+                                  const lcsdata_t *d_weight, int checkpoint_every, double *J, lcsdata_t *const *d_gu,
+                                  lcsdata_t *const *d_gv, lcsdata_t *const *d_gw, char *msg, size_t len);
+int cfd2lcs_tangent_ftle_interp_c(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, int integrator,
+                                  int interpolator, lcsdata_t cfl, int nlevels, const lcsdata_t *const *d_u,
+                                  const lcsdata_t *const *d_v, const lcsdata_t *const *d_w, const lcsdata_t *times,
+                                  const lcsdata_t *d_weight, const lcsdata_t *const *d_du, const lcsdata_t *const *d_dv,
+                                  const lcsdata_t *const *d_dw, double *J, double *dJ, char *msg, size_t len);
+
 
 #ifdef __cplusplus
 }

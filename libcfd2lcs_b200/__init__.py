@@ -43,7 +43,7 @@ EXPORTED_SYMBOLS = [
     "cfd2lcs_batch_get_flowmap_c", "cfd2lcs_batch_get_counters_c", "cfd2lcs_batch_size_c", "cfd2lcs_batch_error_c",
     "cfd2lcs_batch_reset_c",
     # adjoint (include/cfd2lcs_b200.h)
-    "cfd2lcs_adjoint_ftle_c", "cfd2lcs_tangent_ftle_c",
+    "cfd2lcs_adjoint_ftle_c", "cfd2lcs_tangent_ftle_c", "cfd2lcs_adjoint_ftle_interp_c", "cfd2lcs_tangent_ftle_interp_c",
     # measurement hook (include/cfd2lcs_b200.h)
 ]
 
@@ -131,6 +131,12 @@ def load(precision: str = "dp") -> C.CDLL:
     lib.cfd2lcs_adjoint_ftle_c.restype = C.c_int
     lib.cfd2lcs_tangent_ftle_c.argtypes = [P, P, P, P, C.c_int, R, C.c_int, P, P, P, P, P, P, P, P, P, P, C.c_char_p, C.c_size_t]
     lib.cfd2lcs_tangent_ftle_c.restype = C.c_int
+    lib.cfd2lcs_adjoint_ftle_interp_c.argtypes = [P, P, P, P, C.c_int, C.c_int, R, C.c_int, P, P, P, P, P, C.c_int, P, P, P, P, C.c_char_p,
+                                                  C.c_size_t]
+    lib.cfd2lcs_adjoint_ftle_interp_c.restype = C.c_int
+    lib.cfd2lcs_tangent_ftle_interp_c.argtypes = [P, P, P, P, C.c_int, C.c_int, R, C.c_int, P, P, P, P, P, P, P, P, P, P, C.c_char_p,
+                                                  C.c_size_t]
+    lib.cfd2lcs_tangent_ftle_interp_c.restype = C.c_int
     _LIBS[precision] = lib
     return lib
 
@@ -396,9 +402,10 @@ class Batch:
         return int(e), buf.value.decode(errors="replace")
 
 
-def adjoint_ftle(grid, u, v, w, times, weight, integrator=2, cfl=0.5, checkpoint_every=20, precision="dp", gradient=True):
+def adjoint_ftle(grid, u, v, w, times, weight, integrator=2, cfl=0.5, checkpoint_every=20, precision="dp", gradient=True,
+                 interpolator=1):
     """J = sum(weight * FTLE) of the backward flow map over all levels and, with gradient,
-    dJ/du of every level (cfd2lcs_adjoint_ftle_c).  u, v, w: lists of CUDA tensors, one per
+    dJ/du of every level (cfd2lcs_adjoint_ftle_interp_c; interpolator 1 LINEAR or 3 CUBIC).  u, v, w: lists of CUDA tensors, one per
     level (n[0]*n[1]*n[2] values, i fastest, the library's precision); weight: CUDA tensor.
     Returns (J, gu, gv, gw) with gu, gv, gw lists of CUDA tensors (None without gradient)."""
     import torch
@@ -416,7 +423,8 @@ def adjoint_ftle(grid, u, v, w, times, weight, integrator=2, cfl=0.5, checkpoint
         g = [[torch.empty_like(t) for t in comp] for comp in (u, v, w)]
     msg = C.create_string_buffer(512)
     p = lambda a: a.ctypes.data_as(C.c_void_p)
-    rc = lib.cfd2lcs_adjoint_ftle_c(p(n), p(xs), p(ys), p(zs), int(integrator), R(cfl), L, C.cast(ptrs(u), C.c_void_p),
+    rc = lib.cfd2lcs_adjoint_ftle_interp_c(p(n), p(xs), p(ys), p(zs), int(integrator), int(interpolator), R(cfl), L,
+                                    C.cast(ptrs(u), C.c_void_p),
                                     C.cast(ptrs(v), C.c_void_p), C.cast(ptrs(w), C.c_void_p), p(tm), C.c_void_p(weight.data_ptr()),
                                     int(checkpoint_every), C.byref(J),
                                     C.cast(ptrs(g[0]), C.c_void_p) if g else None, C.cast(ptrs(g[1]), C.c_void_p) if g else None,
@@ -428,7 +436,7 @@ def adjoint_ftle(grid, u, v, w, times, weight, integrator=2, cfl=0.5, checkpoint
     return J.value, None, None, None
 
 
-def tangent_ftle(grid, u, v, w, times, weight, du, dv, dw, integrator=2, cfl=0.5, precision="dp"):
+def tangent_ftle(grid, u, v, w, times, weight, du, dv, dw, integrator=2, cfl=0.5, precision="dp", interpolator=1):
     """J and dJ = <dJ/du, d> of the adjoint's objective for one direction d = (du, dv, dw) (lists of
     CUDA tensors, one per level, like u, v, w), by the tangent-linear sweep
     (cfd2lcs_tangent_ftle_c).  Returns (J, dJ)."""
@@ -443,7 +451,8 @@ def tangent_ftle(grid, u, v, w, times, weight, du, dv, dw, integrator=2, cfl=0.5
     J, dJ = C.c_double(0.0), C.c_double(0.0)
     msg = C.create_string_buffer(512)
     p = lambda a: a.ctypes.data_as(C.c_void_p)
-    rc = lib.cfd2lcs_tangent_ftle_c(p(n), p(xs), p(ys), p(zs), int(integrator), R(cfl), L, ptrs(u), ptrs(v), ptrs(w), p(tm),
+    rc = lib.cfd2lcs_tangent_ftle_interp_c(p(n), p(xs), p(ys), p(zs), int(integrator), int(interpolator), R(cfl), L, ptrs(u), ptrs(v),
+                                           ptrs(w), p(tm),
                                     C.c_void_p(weight.data_ptr()), ptrs(du), ptrs(dv), ptrs(dw), C.byref(J), C.byref(dJ), msg, 512)
     if rc:
         raise RuntimeError(msg.value.decode(errors="replace"))

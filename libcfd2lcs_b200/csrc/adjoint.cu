@@ -29,6 +29,7 @@
 
 #include "grid.h"
 #include "kernels.cuh"
+#include "spline_host.h"
 
 namespace cfd2lcs {
 
@@ -44,6 +45,7 @@ namespace {
   } while (0)
 
 enum { EULER = 0, TRAPEZOIDAL = 1, RK2 = 2, RK3 = 3 };
+enum { LINEAR_I = 1, CUBIC_I = 3 };
 
 // device memory of one adjoint call
 class Pool {
@@ -414,6 +416,440 @@ __global__ void __launch_bounds__(256) k_sl_tangent(DevGrid<T> g, VelFields<T> V
   for (int c = 0; c < 3; c++) dfn.f[c][p] = out[c];
 }
 
+// ---------------------------------------------------------------------------------------
+// CUBIC interpolation (the not-a-knot cubic B-spline on every axis, the library's SPLINE4
+// kernels): basis values exactly as basis_values<T, 4, false> forms them (spline.cuh, the
+// Cox-de Boor recurrence with the interval's reciprocal spans), so the recomputed stage
+// positions are the forward kernel's, and the derivative of each cubic basis function from the
+// quadratic ones of the same recurrence: B'(i,4) = 3 (B(i,3) / (t(i+3) - t(i)) - B(i+1,3) /
+// (t(i+4) - t(i+1))), whose reciprocal spans are the recurrence's third-level slots.
+// ---------------------------------------------------------------------------------------
+template <typename T>
+struct CubicStencil {
+  int p0;       // padded index of the first coefficient
+  T b[3][4];    // basis values per axis
+  T db[3][4];   // their derivatives in the coordinate
+};
+
+template <typename T>
+__device__ __forceinline__ void cubic_basis_d(const SplineAxis<T> &A, int l, T x, T *b, T *db) {
+  const T *r = A.rinv + (size_t)(l - 1) * 6;
+  T dr[4], dl[4], b3[3] = {T(0), T(0), T(0)};
+  b[0] = T(1);
+  int slot = 0;
+#pragma unroll
+  for (int j = 1; j < 4; j++) {
+    dr[j] = __ldg(A.t + l + j - 1) - x;
+    dl[j] = x - __ldg(A.t + l - j);
+    T prev = T(0);
+#pragma unroll
+    for (int m = 1; m <= 3; m++) {
+      if (m > j) break;
+      const T vm = b[m - 1] * __ldg(r + slot++);
+      b[m - 1] = vm * dr[m] + prev;
+      prev = vm * dl[j + 1 - m];
+    }
+    b[j] = prev;
+    if (j == 2) {
+      b3[0] = b[0];
+      b3[1] = b[1];
+      b3[2] = b[2];
+    }
+  }
+  const T R0 = __ldg(r + 3), R1 = __ldg(r + 4), R2 = __ldg(r + 5);
+  db[0] = T(-3) * (b3[0] * R0);
+  db[1] = T(3) * (b3[0] * R0 - b3[1] * R1);
+  db[2] = T(3) * (b3[1] * R1 - b3[2] * R2);
+  db[3] = T(3) * (b3[2] * R2);
+}
+
+// spline_stencil<T, 4, false> with the derivatives; false where db3val returns 0
+template <typename T>
+__device__ __forceinline__ bool cubic_stencil_d(const DevGrid<T> &g, const SplineAxes<T> &S, const T x[3], const int no[3], CubicStencil<T> &st) {
+  int c0[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const SplineAxis<T> &A = S.ax[a];
+    const int n = A.n, k = 4;
+    const T tfirst = __ldg(A.t), tlast = __ldg(A.t + n + k - 1);
+    if (!(x[a] >= tfirst) || x[a] > tlast) return false;
+    int l;
+    if (a == 0) {
+      l = (x[a] >= __ldg(A.t + n)) ? n : knot_interval(A.t, x[a], k, n, no[a] + k - 1);
+    } else {
+      if (x[a] >= tlast) return false;
+      l = knot_interval(A.t, x[a], k, n, no[a] + k - 1);
+    }
+    cubic_basis_d(A, l, x[a], st.b[a], st.db[a]);
+    c0[a] = l - k;
+  }
+  st.p0 = pidx(g.P.sx, g.P.sxy, c0[0], c0[1], c0[2]);
+  return true;
+}
+
+// value (spline_contract's order) and gradient of one component; tap(q) the coefficient at
+// padded index q
+template <typename T, typename Tap>
+__device__ __forceinline__ T cubic_value_grad(const DevGrid<T> &g, const CubicStencil<T> &st, Tap tap, T gr[3]) {
+  T vz = T(0), gx = T(0), gy = T(0), gz = T(0);
+#pragma unroll
+  for (int c2 = 0; c2 < 4; c2++) {
+    T vy = T(0), vyx = T(0), vyy = T(0);
+#pragma unroll
+    for (int c1 = 0; c1 < 4; c1++) {
+      T vx = T(0), dx = T(0);
+#pragma unroll
+      for (int c0 = 0; c0 < 4; c0++) {
+        const T q = tap(st.p0 + c0 + c1 * g.P.sx + c2 * g.P.sxy);
+        vx += st.b[0][c0] * q;
+        dx += st.db[0][c0] * q;
+      }
+      vy += st.b[1][c1] * vx;
+      vyx += st.b[1][c1] * dx;
+      vyy += st.db[1][c1] * vx;
+    }
+    vz += st.b[2][c2] * vy;
+    gx += st.b[2][c2] * vyx;
+    gy += st.b[2][c2] * vyy;
+    gz += st.db[2][c2] * vy;
+  }
+  gr[0] = gx;
+  gr[1] = gy;
+  gr[2] = gz;
+  return vz;
+}
+
+// adjoint of the contraction: coefficient q gets its basis product times a[c] (component c)
+template <typename T>
+__device__ __forceinline__ void cubic_scatter(const DevGrid<T> &g, const CubicStencil<T> &st, FieldPtrsW<T> C, const T a[3]) {
+#pragma unroll
+  for (int c2 = 0; c2 < 4; c2++)
+#pragma unroll
+    for (int c1 = 0; c1 < 4; c1++) {
+      const T w21 = st.b[2][c2] * st.b[1][c1];
+#pragma unroll
+      for (int c0 = 0; c0 < 4; c0++) {
+        const T w = w21 * st.b[0][c0];
+        const int q = st.p0 + c0 + c1 * g.P.sx + c2 * g.P.sxy;
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+          if (a[c] != T(0)) atomicAdd(C.f[c] + q, w * a[c]);
+      }
+    }
+}
+
+// One sampled stage of the cubic sweeps: the blended velocity (1-ct) cn + ct cp at xs (the
+// coefficients of the two levels blended tap by tap as k_blend blends them) and its gradient.
+template <typename T>
+struct CubicSample {
+  CubicStencil<T> st;
+  bool ok;
+  T u[3], gr[3][3];  // gr[c][d] = d u_c / d x_d
+};
+
+template <typename T>
+__device__ __forceinline__ void cubic_sample(const DevGrid<T> &g, const SplineAxes<T> &sa, FieldPtrs<T> cn, FieldPtrs<T> cp, T omc, T ct,
+                                             const T xs[3], const int no[3], CubicSample<T> &s) {
+  s.ok = cubic_stencil_d(g, sa, xs, no, s.st);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    if (!s.ok) {
+      s.u[c] = T(0);
+      s.gr[c][0] = s.gr[c][1] = s.gr[c][2] = T(0);
+      continue;
+    }
+    const T *a = cn.f[c], *b = cp.f[c];
+    s.u[c] = cubic_value_grad(g, s.st, [&](int q) { return omc * __ldg(a + q) + ct * __ldg(b + q); }, s.gr[c]);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Adjoint of one backward SL subcycle with CUBIC interpolation (k_sl_subcycle<..., SPLINE4>,
+// no flags): the forward stages recomputed from the coefficient levels cn, cp and the previous
+// map's coefficients cfm; the previous map's adjoint goes to cbo in coefficient space (the
+// transposed fit follows on the host side), the off-node stages' velocity adjoints to a2, a3 in
+// coefficient space, the node stage's to a1 in value space.
+// ---------------------------------------------------------------------------------------
+template <typename T, int INTEG>
+__global__ void __launch_bounds__(128) k_sl_adjoint_cubic(DevGrid<T> g, SplineAxes<T> sa, VelFields<T> V, FieldPtrs<T> cn, FieldPtrs<T> cp,
+                                                           FieldPtrs<T> cfm, FieldPtrs<T> fbn, FieldPtrsW<T> cbo, FieldPtrsW<T> a1,
+                                                           FieldPtrsW<T> a2, FieldPtrsW<T> a3, StageTimes S, T dt) {
+  int i, j, k;
+  if (!node_of_thread(g.P.n, i, j, k)) return;
+  const int p = pidx(g.P.sx, g.P.sxy, i, j, k);
+  const T a[3] = {fbn.f[0][p], fbn.f[1][p], fbn.f[2][p]};
+  if (a[0] == T(0) && a[1] == T(0) && a[2] == T(0)) return;
+  const T HALF = T(1) / T(2), SIXTH = T(1) / T(6), TWOTHIRD = T(2) / T(3), TWO = T(2);
+  const int no[3] = {i, j, k};
+  const T x0[3] = {__ldg(g.lt[0] + i), __ldg(g.lt[1] + j), __ldg(g.lt[2] + k)};
+  const T ct0 = T(S.ct[0]), omc0 = T(1) - ct0;
+  const T ct1 = T(S.ct[1]), omc1 = T(1) - ct1, ct2 = T(S.ct[2]), omc2 = T(1) - ct2;
+  T u1[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) u1[c] = omc0 * __ldg(V.un[c] + p) + ct0 * __ldg(V.unp1[c] + p);
+  // --- forward recomputation (integrate<>, first stage on the node) ---
+  CubicSample<T> s2, s3;
+  T x[3];
+  if (INTEG == RK3) {
+    T kk[3], acc[3], xs[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u1[c];
+      acc[c] = x0[c] + SIXTH * kk[c];
+      xs[c] = x0[c] + HALF * kk[c];
+    }
+    cubic_sample(g, sa, cn, cp, omc1, ct1, xs, no, s2);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * s2.u[c];
+      xs[c] = x0[c] + TWO * kk[c];
+      acc[c] = acc[c] + TWOTHIRD * kk[c];
+    }
+    cubic_sample(g, sa, cn, cp, omc2, ct2, xs, no, s3);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * s3.u[c];
+      x[c] = acc[c] + SIXTH * kk[c];
+    }
+  } else if (INTEG == RK2) {
+    T xs[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) xs[c] = x0[c] + HALF * dt * u1[c];
+    cubic_sample(g, sa, cn, cp, omc1, ct1, xs, no, s2);
+#pragma unroll
+    for (int c = 0; c < 3; c++) x[c] = x0[c] + dt * s2.u[c];
+  } else {
+#pragma unroll
+    for (int c = 0; c < 3; c++) x[c] = x0[c] + dt * u1[c];
+  }
+  // --- fm_new = fm_old(x) + (x - x0) ---
+  T xb[3] = {a[0], a[1], a[2]};
+  {
+    CubicStencil<T> sf;
+    if (cubic_stencil_d(g, sa, x, no, sf)) {
+      cubic_scatter(g, sf, cbo, a);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        T gr[3];
+        const T *f = cfm.f[c];
+        (void)cubic_value_grad(g, sf, [&](int q) { return __ldg(f + q); }, gr);
+#pragma unroll
+        for (int d = 0; d < 3; d++) xb[d] += a[c] * gr[d];
+      }
+    }
+  }
+  // --- stages: a sampled stage's velocity adjoint ub into coefficient space (as = a2 or a3),
+  // returning the adjoint of the sample position ---
+  auto stage_back = [&](const CubicSample<T> &sm, const T ub[3], FieldPtrsW<T> as, T pb[3]) {
+    pb[0] = pb[1] = pb[2] = T(0);
+    if (!sm.ok) return;
+    cubic_scatter(g, sm.st, as, ub);
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+      for (int d = 0; d < 3; d++) pb[d] += ub[c] * sm.gr[c][d];
+  };
+  T u1b[3];
+  if (INTEG == RK3) {
+    T k2b[3], k1b[3], ub[3], pb[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k2b[c] = TWOTHIRD * xb[c];
+      k1b[c] = SIXTH * xb[c];
+      ub[c] = dt * (SIXTH * xb[c]);
+    }
+    stage_back(s3, ub, a3, pb);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k2b[c] += TWO * pb[c];
+      ub[c] = dt * k2b[c];
+    }
+    stage_back(s2, ub, a2, pb);
+#pragma unroll
+    for (int c = 0; c < 3; c++) u1b[c] = dt * (k1b[c] + HALF * pb[c]);
+  } else if (INTEG == RK2) {
+    T ub[3], pb[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) ub[c] = dt * xb[c];
+    stage_back(s2, ub, a2, pb);
+#pragma unroll
+    for (int c = 0; c < 3; c++) u1b[c] = HALF * dt * pb[c];
+  } else {
+#pragma unroll
+    for (int c = 0; c < 3; c++) u1b[c] = dt * xb[c];
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) a1.f[c][p] = u1b[c];
+}
+
+// Tangent-linear form of the CUBIC subcycle: direction levels D (values, for the node stage) and
+// dcn, dcp (their coefficients), the previous map's tangent coefficients dcfm.
+template <typename T, int INTEG>
+__global__ void __launch_bounds__(128) k_sl_tangent_cubic(DevGrid<T> g, SplineAxes<T> sa, VelFields<T> V, VelFields<T> D, FieldPtrs<T> cn,
+                                                           FieldPtrs<T> cp, FieldPtrs<T> dcn, FieldPtrs<T> dcp, FieldPtrs<T> cfm,
+                                                           FieldPtrs<T> dcfm, FieldPtrsW<T> dfn, StageTimes S, T dt) {
+  int i, j, k;
+  if (!node_of_thread(g.P.n, i, j, k)) return;
+  const int p = pidx(g.P.sx, g.P.sxy, i, j, k);
+  const T HALF = T(1) / T(2), SIXTH = T(1) / T(6), TWOTHIRD = T(2) / T(3), TWO = T(2);
+  const int no[3] = {i, j, k};
+  const T x0[3] = {__ldg(g.lt[0] + i), __ldg(g.lt[1] + j), __ldg(g.lt[2] + k)};
+  const T ct0 = T(S.ct[0]), omc0 = T(1) - ct0;
+  const T ct1 = T(S.ct[1]), omc1 = T(1) - ct1, ct2 = T(S.ct[2]), omc2 = T(1) - ct2;
+  T u1[3], du1[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    u1[c] = omc0 * __ldg(V.un[c] + p) + ct0 * __ldg(V.unp1[c] + p);
+    du1[c] = omc0 * __ldg(D.un[c] + p) + ct0 * __ldg(D.unp1[c] + p);
+  }
+  // velocity at xs and its first-order change for a move dxs of the point
+  auto stage_tan = [&](const T xs[3], const T dxs[3], T omc, T ct, T u[3], T du[3]) {
+    CubicSample<T> sm;
+    cubic_sample(g, sa, cn, cp, omc, ct, xs, no, sm);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      u[c] = sm.u[c];
+      du[c] = T(0);
+      if (!sm.ok) continue;
+      T gr[3];
+      const T *a = dcn.f[c], *b = dcp.f[c];
+      du[c] = cubic_value_grad(g, sm.st, [&](int q) { return omc * __ldg(a + q) + ct * __ldg(b + q); }, gr);
+#pragma unroll
+      for (int d = 0; d < 3; d++) du[c] += sm.gr[c][d] * dxs[d];
+    }
+  };
+  T x[3], dx[3];
+  if (INTEG == RK3) {
+    T kk[3], dk[3], acc[3], dacc[3], xs[3], dxs[3], u[3], du[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u1[c];
+      dk[c] = dt * du1[c];
+      acc[c] = x0[c] + SIXTH * kk[c];
+      dacc[c] = SIXTH * dk[c];
+      xs[c] = x0[c] + HALF * kk[c];
+      dxs[c] = HALF * dk[c];
+    }
+    stage_tan(xs, dxs, omc1, ct1, u, du);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u[c];
+      dk[c] = dt * du[c];
+      xs[c] = x0[c] + TWO * kk[c];
+      dxs[c] = TWO * dk[c];
+      acc[c] = acc[c] + TWOTHIRD * kk[c];
+      dacc[c] = dacc[c] + TWOTHIRD * dk[c];
+    }
+    stage_tan(xs, dxs, omc2, ct2, u, du);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u[c];
+      x[c] = acc[c] + SIXTH * kk[c];
+      dx[c] = dacc[c] + SIXTH * (dt * du[c]);
+    }
+  } else if (INTEG == RK2) {
+    T xs[3], dxs[3], u[3], du[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      xs[c] = x0[c] + HALF * dt * u1[c];
+      dxs[c] = HALF * dt * du1[c];
+    }
+    stage_tan(xs, dxs, omc1, ct1, u, du);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      x[c] = x0[c] + dt * u[c];
+      dx[c] = dt * du[c];
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      x[c] = x0[c] + dt * u1[c];
+      dx[c] = dt * du1[c];
+    }
+  }
+  // fm_new = fm_old(x) + (x - x0)
+  T out[3] = {dx[0], dx[1], dx[2]};
+  CubicStencil<T> sf;
+  if (cubic_stencil_d(g, sa, x, no, sf)) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      T gr[3], g2[3];
+      const T *f = cfm.f[c], *df = dcfm.f[c];
+      (void)cubic_value_grad(g, sf, [&](int q) { return __ldg(f + q); }, gr);
+      out[c] += cubic_value_grad(g, sf, [&](int q) { return __ldg(df + q); }, g2);
+#pragma unroll
+      for (int d = 0; d < 3; d++) out[c] += gr[d] * dx[d];
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) dfn.f[c][p] = out[c];
+}
+
+// Adjoint of one B-spline fit pass (k_fit_xlines / k_fit_lines): the transposed banded solves of
+// spline_pull_table_transposed along every line of one axis, in place.  Line L starts at
+// (L % nfast) * ls + (L / nfast) * so, its n elements es apart.
+template <typename T>
+__global__ void __launch_bounds__(256) k_fit_transpose(const T *__restrict__ pt, int n, FieldPtrsW<T> f, int nfast, long nlines, long ls,
+                                                        long so, long es) {
+  const long L = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (L >= nlines) return;
+  T *d = f.f[blockIdx.y] + (L % nfast) * ls + (L / nfast) * so;
+  T w[3] = {T(0), T(0), T(0)};
+  for (int r = 0; r < n; r++) {
+    const T *c = pt + 8 * (size_t)r;
+    T v = d[(long)r * es];
+    v = v - w[0] * __ldg(c + 0) - w[1] * __ldg(c + 1) - w[2] * __ldg(c + 2);
+    v = v * __ldg(c + 6);
+    w[2] = w[1];
+    w[1] = w[0];
+    w[0] = v;
+    d[(long)r * es] = v;
+  }
+  w[0] = w[1] = w[2] = T(0);
+  for (int r = n - 1; r >= 0; r--) {
+    const T *c = pt + 8 * (size_t)r;
+    T v = d[(long)r * es];
+    v = v - w[0] * __ldg(c + 3) - w[1] * __ldg(c + 4) - w[2] * __ldg(c + 5);
+    w[2] = w[1];
+    w[1] = w[0];
+    w[0] = v;
+    d[(long)r * es] = v;
+  }
+}
+
+// velocity adjoint of one CUBIC subcycle onto the two levels: the node stage (a1, values) into
+// ubn / ubp with (1-ct0, ct0), the off-node stages (a2 with ct1, a3 with ct2; coefficients)
+// into cbn / cbp; the stage fields are cleared for the next subcycle
+template <typename T, bool THREE>
+__global__ void __launch_bounds__(256) k_distribute_cubic(FieldPtrsW<T> a1, FieldPtrsW<T> a2, FieldPtrsW<T> a3, FieldPtrsW<T> ubn,
+                                                           FieldPtrsW<T> ubp, FieldPtrsW<T> cbn, FieldPtrsW<T> cbp, T ct0, T ct1, T ct2,
+                                                           long ntot) {
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= ntot) return;
+  const int c = blockIdx.y;
+  const T x1 = a1.f[c][q], x2 = a2.f[c][q], x3 = THREE ? a3.f[c][q] : T(0);
+  if (x1 != T(0)) {
+    ubn.f[c][q] += (T(1) - ct0) * x1;
+    ubp.f[c][q] += ct0 * x1;
+    a1.f[c][q] = T(0);
+  }
+  if (x2 != T(0) || x3 != T(0)) {
+    cbn.f[c][q] += (T(1) - ct1) * x2 + (T(1) - ct2) * x3;
+    cbp.f[c][q] += ct1 * x2 + ct2 * x3;
+    a2.f[c][q] = T(0);
+    if (THREE) a3.f[c][q] = T(0);
+  }
+}
+
+// dst += src (three components, padded)
+template <typename T>
+__global__ void __launch_bounds__(256) k_add3(FieldPtrsW<T> dst, FieldPtrs<T> src, long ntot) {
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= ntot) return;
+  const int c = blockIdx.y;
+  dst.f[c][q] += src.f[c][q];
+}
+
 // source interior index of a padded cell along one periodic axis
 __device__ __forceinline__ int wrap_index(int v, int n) { return v < 1 ? v + n : (v > n ? v - n : v); }
 
@@ -615,6 +1051,11 @@ class Adjoint {
       msg = "adjoint: the integrator must be EULER, TRAPEZOIDAL, RK2 or RK3";
       return false;
     }
+    if (pr_.interpolator != LINEAR_I && pr_.interpolator != CUBIC_I) {
+      msg = "adjoint: the interpolator must be LINEAR or CUBIC";
+      return false;
+    }
+    cubic_ = pr_.interpolator == CUBIC_I;
     if (pr_.checkpoint_every < 1 || !(pr_.cfl > 0)) {
       msg = "adjoint: checkpoint interval and CFL must be positive";
       return false;
@@ -669,6 +1110,28 @@ class Adjoint {
       dg_.nrm[a] = nullptr;
     }
     dg_.flag = nullptr;
+    if (cubic_) {
+      // the not-a-knot cubic of every axis over its padded coordinate line (the library's
+      // ensure_spline), its pull table for the fits and the transposed one for their adjoint
+      for (int a = 0; a < 3; a++) {
+        if (n[a] < 3) {
+          msg = "adjoint: CUBIC needs at least 3 points in every direction";
+          return false;
+        }
+        SplineAxisHost<lcsdata_t> A;
+        if (!A.build(hg_.li[a], 4)) {
+          msg = "adjoint: bspline: singular collocation system or bad abscissae";
+          return false;
+        }
+        SplineAxis<T> &D = sa_.ax[a];
+        D.n = A.n;
+        D.k = A.k;
+        const std::vector<lcsdata_t> pull = spline_pull_table(A);
+        if (!(D.t = upload(A.t, msg)) || !(D.rinv = upload(A.rinv, msg)) || !(D.tu = upload(A.tu, msg)) || !(D.pull = upload(pull, msg)))
+          return false;
+        if (!(ptr_[a] = upload(spline_pull_table_transposed(pull, A.n), msg))) return false;
+      }
+    }
     ACK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     ACK(cudaMallocHost(&red_host_, sizeof(DevReduce)));
     if (!(red_dev_ = pool_.alloc<DevReduce>(1, msg))) return false;
@@ -758,6 +1221,14 @@ class Adjoint {
       nsub_[l] = (int)std::max(1L, ns);
     }
     if (!field3(fm_[0], msg) || !field3(fm_[1], msg)) return false;
+    if (cubic_) {
+      if (!slab(Cl_, (size_t)3 * L, msg)) return false;
+      for (int l = 0; l < L; l++) fit3(&U_[3 * l], &Cl_[3 * l]);
+      for (int st = 1; st < 3; st++)
+        if (!field3(blend_[st], msg)) return false;
+      if (!field3(cfm_, msg)) return false;
+      ACK(cudaGetLastError());
+    }
     if (tangent_) {
       // the direction, padded and ghost-filled like the levels (its CFL maxima are unused)
       if (!slab(DU_, (size_t)3 * L, msg)) return false;
@@ -775,6 +1246,12 @@ class Adjoint {
         return false;
       }
       if (!field3(dfm_[0], msg) || !field3(dfm_[1], msg)) return false;
+      if (cubic_) {
+        if (!slab(DC_, (size_t)3 * L, msg)) return false;
+        for (int l = 0; l < L; l++) fit3(&DU_[3 * l], &DC_[3 * l]);
+        if (!field3(dcfm_, msg)) return false;
+        ACK(cudaGetLastError());
+      }
     }
     cur_ = 0;
     const int K = pr_.checkpoint_every;
@@ -862,6 +1339,12 @@ class Adjoint {
       const SplineAxes<T> sa{};
       int *err = &red_dev_->err;
       const dim3 grd = node_grid(), blk(32, 8, 1);
+      if (cubic_) {
+        if (!advance_cubic(l, buf, cur, S, (T)dt, tangent, msg)) return false;
+        cur ^= 1;
+        lp = lp + dt;
+        continue;
+      }
       if (tangent) {
         // reads the map before the subcycle, so it runs before the forward kernel replaces it
         VelFields<T> D{};
@@ -897,9 +1380,78 @@ class Adjoint {
     return true;
   }
 
+  // one CUBIC subcycle of update l from buf[cur] into buf[cur ^ 1] (and the tangent map along)
+  bool advance_cubic(int l, T *buf[2][3], int cur, const StageTimes &S, T dt, bool tangent, std::string &msg) {
+    VelFields<T> V{};
+    FieldPtrs<T> cn{}, cp{};
+    for (int c = 0; c < 3; c++) {
+      V.un[c] = U_[3 * (l - 1) + c];
+      V.unp1[c] = U_[3 * l + c];
+      cn.f[c] = Cl_[3 * (l - 1) + c];
+      cp.f[c] = Cl_[3 * l + c];
+    }
+    // stage blends of the two levels' coefficients, as the library's k_blend forms them
+    const int nst = pr_.integrator == RK3 ? 3 : (pr_.integrator == RK2 ? 2 : 1);
+    BlendOut<T> o{};
+    int nout = 0;
+    for (int st = 1; st < nst; st++) {
+      const T ct = (T)S.ct[st];
+      for (int c = 0; c < 3; c++) {
+        o.f[nout][c] = blend_[st][c];
+        V.cs[st][c] = blend_[st][c];
+      }
+      o.omc[nout] = T(1) - ct;
+      o.ct[nout] = ct;
+      nout++;
+    }
+    if (nout > 0) {
+      const long npair = (ntot_ + 1) / 2;
+      k_blend<T><<<dim3((unsigned)((npair + 255) / 256), 3), 256, 0, stream_>>>(cn, cp, o, nout, ntot_);
+    }
+    fit3(buf[cur], cfm_);
+    FieldPtrs<T> fo{};
+    FieldPtrsW<T> fn{};
+    for (int c = 0; c < 3; c++) {
+      fo.f[c] = cfm_[c];
+      fn.f[c] = buf[cur ^ 1][c];
+    }
+    if (tangent) {
+      fit3(dfm_[cur], dcfm_);
+      VelFields<T> D{};
+      FieldPtrs<T> dcn{}, dcp{}, dcf{};
+      FieldPtrsW<T> dfn{};
+      for (int c = 0; c < 3; c++) {
+        D.un[c] = DU_[3 * (l - 1) + c];
+        D.unp1[c] = DU_[3 * l + c];
+        dcn.f[c] = DC_[3 * (l - 1) + c];
+        dcp.f[c] = DC_[3 * l + c];
+        dcf.f[c] = dcfm_[c];
+        dfn.f[c] = dfm_[cur ^ 1][c];
+      }
+      const dim3 g4 = node_grid4(), b4(32, 4, 1);
+      if (pr_.integrator == RK3) k_sl_tangent_cubic<T, RK3><<<g4, b4, 0, stream_>>>(dg_, sa_, V, D, cn, cp, dcn, dcp, fo, dcf, dfn, S, dt);
+      else if (pr_.integrator == RK2) k_sl_tangent_cubic<T, RK2><<<g4, b4, 0, stream_>>>(dg_, sa_, V, D, cn, cp, dcn, dcp, fo, dcf, dfn, S, dt);
+      else k_sl_tangent_cubic<T, EULER><<<g4, b4, 0, stream_>>>(dg_, sa_, V, D, cn, cp, dcn, dcp, fo, dcf, dfn, S, dt);
+      k_periodic_ghosts<T><<<(unsigned)((ntot_ + 255) / 256), 256, 0, stream_>>>(dg_, dfn, ntot_);
+    }
+    int *err = &red_dev_->err;
+    const dim3 grd = node_grid(), blk(32, 8, 1);
+    if (pr_.integrator == RK3)
+      k_sl_subcycle<T, T, RK3_, INTERP_SPLINE4, false><<<grd, blk, 0, stream_>>>(dg_, sa_, V, fo, fn, S, dt, err);
+    else if (pr_.integrator == RK2)
+      k_sl_subcycle<T, T, RK2_, INTERP_SPLINE4, false><<<grd, blk, 0, stream_>>>(dg_, sa_, V, fo, fn, S, dt, err);
+    else if (pr_.integrator == TRAPEZOIDAL)
+      k_sl_subcycle<T, T, TRAPEZOIDAL_, INTERP_SPLINE4, false><<<grd, blk, 0, stream_>>>(dg_, sa_, V, fo, fn, S, dt, err);
+    else
+      k_sl_subcycle<T, T, EULER_, INTERP_SPLINE4, false><<<grd, blk, 0, stream_>>>(dg_, sa_, V, fo, fn, S, dt, err);
+    ACK(cudaGetLastError());
+    return true;
+  }
+
   bool backward(std::string &msg) {
     const int L = pr_.nlevels, K = pr_.checkpoint_every;
     if (!slab(Ub_, (size_t)3 * L, msg)) return false;
+    if (cubic_ && !slab(Cb_, (size_t)3 * L, msg)) return false;
     T *fbar[2][3];
     if (!field3(fbar[0], msg) || !field3(fbar[1], msg)) return false;
     int fb = 0;
@@ -983,6 +1535,36 @@ class Adjoint {
             fbo.f[c] = fbar[fb ^ 1][c];
           }
           const StageTimes S = stage_times(t0, t1, lps[q], dt);
+          if (cubic_) {
+            fit3(&states[(size_t)3 * (first[l - l0] + q)], cfm_);
+            FieldPtrs<T> cn{}, cp{}, cf{};
+            FieldPtrsW<T> cbn{}, cbp{};
+            for (int c = 0; c < 3; c++) {
+              cn.f[c] = Cl_[3 * (l - 1) + c];
+              cp.f[c] = Cl_[3 * l + c];
+              cf.f[c] = cfm_[c];
+              cbn.f[c] = Cb_[3 * (l - 1) + c];
+              cbp.f[c] = Cb_[3 * l + c];
+            }
+            const dim3 g4 = node_grid4(), b4(32, 4, 1);
+            if (pr_.integrator == RK3)
+              k_sl_adjoint_cubic<T, RK3><<<g4, b4, 0, stream_>>>(dg_, sa_, V, cn, cp, cf, fbn, fbo, A1, A2, A3, S, (T)dt);
+            else if (pr_.integrator == RK2)
+              k_sl_adjoint_cubic<T, RK2><<<g4, b4, 0, stream_>>>(dg_, sa_, V, cn, cp, cf, fbn, fbo, A1, A2, A3, S, (T)dt);
+            else
+              k_sl_adjoint_cubic<T, EULER><<<g4, b4, 0, stream_>>>(dg_, sa_, V, cn, cp, cf, fbn, fbo, A1, A2, A3, S, (T)dt);
+            // the previous map's adjoint was scattered in coefficient space: through the fit
+            fitT3(fbar[fb ^ 1]);
+            if (pr_.integrator == RK3)
+              k_distribute_cubic<T, true><<<dim3((unsigned)nb, 3), 256, 0, stream_>>>(A1, A2, A3, ubn, ubp, cbn, cbp, (T)S.ct[0], (T)S.ct[1],
+                                                                                        (T)S.ct[2], ntot_);
+            else
+              k_distribute_cubic<T, false><<<dim3((unsigned)nb, 3), 256, 0, stream_>>>(A1, A2, A3, ubn, ubp, cbn, cbp, (T)S.ct[0],
+                                                                                         (T)S.ct[1], T(0), ntot_);
+            ACK(cudaGetLastError());
+            fb ^= 1;
+            continue;
+          }
           if (pr_.integrator == RK3)
             k_sl_adjoint<T, RK3><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, V, fo, fbn, fbo, A1, A2, A3, S, (T)dt);
           else if (pr_.integrator == RK2)
@@ -1000,13 +1582,20 @@ class Adjoint {
         }
       }
     }
-    // velocity ghosts were copies of the ingested interior: fold, then hand out
+    // velocity ghosts were copies of the ingested interior: fold, then hand out (CUBIC: the
+    // coefficient-space adjoint of each level through its fit first)
     for (int l = 0; l < L; l++) {
       FieldPtrsW<T> f{};
       FieldPtrs<T> fr{};
       for (int c = 0; c < 3; c++) {
         f.f[c] = Ub_[3 * l + c];
         fr.f[c] = Ub_[3 * l + c];
+      }
+      if (cubic_) {
+        fitT3(&Cb_[3 * l]);
+        FieldPtrs<T> cb{};
+        for (int c = 0; c < 3; c++) cb.f[c] = Cb_[3 * l + c];
+        k_add3<T><<<dim3((unsigned)nb, 3), 256, 0, stream_>>>(f, cb, ntot_);
       }
       k_fold_ghosts<T><<<(unsigned)nb, 256, 0, stream_>>>(dg_, f, ntot_);
       k_grad_out<T><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, fr, pr_.gu[l], pr_.gv[l], pr_.gw[l]);
@@ -1015,6 +1604,50 @@ class Adjoint {
     return true;
   }
 
+
+  // CUBIC: spline axes, transposed pull tables, coefficient levels (and their adjoints and
+  // tangents), the stage blends and the previous map's coefficients of one subcycle
+  bool cubic_ = false;
+  SplineAxes<T> sa_{};
+  T *ptr_[3] = {nullptr, nullptr, nullptr};
+  std::vector<T *> Cl_, Cb_, DC_;
+  T *blend_[3][3] = {};
+  T *cfm_[3] = {nullptr, nullptr, nullptr};
+  T *dcfm_[3] = {nullptr, nullptr, nullptr};
+
+  // coefficients of the padded fields src into dst (the library's fit: x, then y, then z)
+  void fit3(T *const src[3], T *const dst[3]) {
+    FieldPtrs<T> s{}, di{};
+    FieldPtrsW<T> d{};
+    for (int c = 0; c < 3; c++) {
+      s.f[c] = src[c];
+      di.f[c] = dst[c];
+      d.f[c] = dst[c];
+    }
+    const int sx = dg_.P.sx, sxy = dg_.P.sxy, ny = dg_.P.n[1] + 2, nz = dg_.P.n[2] + 2;
+    const long warps = (long)((ny + 31) / 32) * nz;
+    const size_t smem = sizeof(T) * 4 * 2 * 32 * (XFIT_W + 1);
+    k_fit_xlines<T, 4><<<dim3((unsigned)((warps + 3) / 4), 3), 128, smem, stream_>>>(sa_.ax[0], s, d, ny, nz, (long)sx, (long)sxy);
+    k_fit_lines<T, 4><<<dim3((unsigned)(((long)sx * nz + 255) / 256), 3), 256, 0, stream_>>>(sa_.ax[1], di, d, sx, (long)sx * nz,
+                                                                                             (long)sx, (long)sxy);
+    k_fit_lines<T, 4><<<dim3((unsigned)(((long)sxy + 255) / 256), 3), 256, 0, stream_>>>(sa_.ax[2], di, d, sxy, (long)sxy, (long)sxy,
+                                                                                         (long)sxy);
+  }
+
+  // adjoint of fit3, in place: the transposed passes z, then y, then x
+  void fitT3(T *const f[3]) {
+    FieldPtrsW<T> d{};
+    for (int c = 0; c < 3; c++) d.f[c] = f[c];
+    const long sx = dg_.P.sx, sxy = dg_.P.sxy;
+    const int ny = dg_.P.n[1] + 2, nz = dg_.P.n[2] + 2;
+    k_fit_transpose<T><<<dim3((unsigned)((sxy + 255) / 256), 3), 256, 0, stream_>>>(ptr_[2], sa_.ax[2].n, d, (int)sxy, sxy, 1L, sxy, sxy);
+    k_fit_transpose<T><<<dim3((unsigned)((sx * nz + 255) / 256), 3), 256, 0, stream_>>>(ptr_[1], sa_.ax[1].n, d, (int)sx, sx * nz, 1L, sxy,
+                                                                                        sx);
+    k_fit_transpose<T><<<dim3((unsigned)(((long)ny * nz + 255) / 256), 3), 256, 0, stream_>>>(ptr_[0], sa_.ax[0].n, d, ny, (long)ny * nz,
+                                                                                              sx, sxy, 1L);
+  }
+
+  dim3 node_grid4() const { return dim3((dg_.P.n[0] + 31) / 32, (dg_.P.n[1] + 3) / 4, dg_.P.n[2]); }
 
   const AdjointProblem &pr_;
   HostGrid<lcsdata_t> hg_;

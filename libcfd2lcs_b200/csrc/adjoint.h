@@ -11,7 +11,7 @@ namespace cfd2lcs {
 struct AdjointProblem {
   const int *n;                      // grid points per direction
   const lcsdata_t *x, *y, *z;        // coordinates (as cfd2lcs_init), i fastest
-  int integrator;                    // EULER, TRAPEZOIDAL or RK2
+  int integrator;                    // EULER, TRAPEZOIDAL, RK2 or RK3
   double cfl;                        // CFL number of the subcycling (cfd2lcs_set_param "CFL")
   int nlevels;                       // velocity levels, >= 2
   const lcsdata_t *const *u, *const *v, *const *w;  // device pointers, one per level, n[0]n[1]n[2] each
@@ -23,9 +23,10 @@ struct AdjointProblem {
   // a forward-mode sweep alongside the flow map
   const lcsdata_t *const *du = nullptr, *const *dv = nullptr, *const *dw = nullptr;
   double *dJ = nullptr;
+  int interpolator = 1;              // LINEAR (1) or CUBIC (3)
 };
 
-// Runs the backward flow map over all levels (LINEAR interpolation), the FTLE of the final
+// Runs the backward flow map over all levels (LINEAR or CUBIC interpolation), the FTLE of the final
 // map and J; with gradient outputs, the adjoint sweep; with a tangent direction, the tangent-
 // linear sweep in the same forward pass.  Returns false with msg on error.
 bool adjoint_ftle(const AdjointProblem &p, double *J, std::string &msg);

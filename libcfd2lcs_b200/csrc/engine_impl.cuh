@@ -1198,21 +1198,7 @@ class Engine : public EngineBase {
     return true;
   }
 
-  // coefficients of the padded fields src (3 components) into dst (db3ink, x then y then z)
-  // Band LU of one axis in the pull form the device sweeps read (pull_forward / pull_backward)
-  static std::vector<lcsdata_t> pull_table(const SplineAxisHost<lcsdata_t> &A) {
-    const int n = A.n, k = A.k, nr = 2 * k - 1, mid = k;
-    auto W = [&](int r, int c) { return A.lu[(size_t)(r - 1) + (size_t)nr * (c - 1)]; };
-    std::vector<lcsdata_t> p((size_t)8 * n, lcsdata_t(0));
-    for (int i = 1; i <= n; i++) {
-      for (int j = 1; j <= k - 1; j++) {
-        if (i - j >= 1) p[(size_t)8 * (i - 1) + j - 1] = W(mid + j, i - j);
-        if (i + j <= n) p[(size_t)8 * (i - 1) + 3 + j - 1] = W(mid - j, i + j);
-      }
-      p[(size_t)8 * (i - 1) + 6] = lcsdata_t(1) / W(mid, i);
-    }
-    return p;
-  }
+  static std::vector<lcsdata_t> pull_table(const SplineAxisHost<lcsdata_t> &A) { return spline_pull_table(A); }
 
   template <typename D, int K>
   void fit_pass(const SplineAxis<D> &A, FieldPtrs<D> s, FieldPtrsW<D> d, int axis, const DevGrid<T> &g) {

@@ -1,7 +1,7 @@
 """The adjoint (cfd2lcs_adjoint_ftle_c): its forward objective equals the library's own FTLE
 frame for h = T, its gradient agrees with central finite differences of that objective along
-random directions and with the tangent-linear model (EULER, TRAPEZOIDAL, RK2 and RK3), and it
-does not depend on the checkpoint interval."""
+random directions and with the tangent-linear model (EULER, TRAPEZOIDAL, RK2 and RK3; LINEAR and
+CUBIC interpolation), and it does not depend on the checkpoint interval."""
 import math
 
 import numpy as np
@@ -139,3 +139,79 @@ def test_tangent_requires_a_direction():
     rc = lib.cfd2lcs_tangent_ftle_c(n.ctypes.data_as(C.c_void_p), None, None, None, 2, 0.5, 2, None, None, None, None, None, None,
                                     None, None, C.byref(J), C.byref(dJ), msg, 256)
     assert rc == 1 and b"direction" in msg.value
+
+
+# --- CUBIC interpolation (the not-a-knot cubic B-spline, the ABC configuration's interpolator) --
+
+@pytest.mark.parametrize("integrator", [2, 3])
+def test_cubic_forward_objective_is_the_library_frame(integrator):
+    import libcfd2lcs_b200 as L
+    n, nl, dt = 12, 7, 0.05
+    g, lev, times = _levels(n, nl, dt)
+    wgt = _weight(g)
+    J, *_ = L.adjoint_ftle(g, *lev, times, wgt, integrator=integrator, gradient=False, interpolator=3)
+    api = L.Cfd2lcs("dp")
+    api.reset()
+    api.init(g.n, g.x, g.y, g.z, g.flag)
+    T = times[-1]
+    h = api.diagnostic_init(1, 0, T, T, "b")
+    api.set_option("INTEGRATOR", integrator)
+    api.set_option("INTERPOLATOR", 3)
+    for k in range(nl):
+        api.update_device(lev[0][k].data_ptr(), lev[1][k].data_ptr(), lev[2][k].data_ptr(), times[k])
+    assert api.error()[0] == 0, api.error()
+    ftle = api.ftle(h).ravel(order="F")
+    J_lib = float(np.dot(wgt.cpu().numpy(), ftle))
+    api.reset()
+    assert abs(J - J_lib) <= 1e-12 * max(abs(J_lib), 1e-30), (J, J_lib)
+
+
+@pytest.mark.parametrize("integrator", [0, 2, 3])
+def test_cubic_gradient_matches_finite_differences(integrator):
+    import torch
+
+    import libcfd2lcs_b200 as L
+    n, nl, dt = 10, 6, 0.05
+    g, lev, times = _levels(n, nl, dt)
+    wgt = _weight(g)
+    J, gu, gv, gw = L.adjoint_ftle(g, *lev, times, wgt, integrator=integrator, checkpoint_every=2, interpolator=3)
+    grads = (gu, gv, gw)
+    rng = np.random.default_rng(13)
+    for _ in range(3):
+        d = [[torch.from_numpy(rng.standard_normal(lev[c][k].numel())).cuda() for k in range(nl)] for c in range(3)]
+        eps = 1e-6
+        plus = [[lev[c][k] + eps * d[c][k] for k in range(nl)] for c in range(3)]
+        minus = [[lev[c][k] - eps * d[c][k] for k in range(nl)] for c in range(3)]
+        Jp, *_ = L.adjoint_ftle(g, *plus, times, wgt, integrator=integrator, gradient=False, interpolator=3)
+        Jm, *_ = L.adjoint_ftle(g, *minus, times, wgt, integrator=integrator, gradient=False, interpolator=3)
+        fd = (Jp - Jm) / (2 * eps)
+        ad = sum(float(torch.dot(grads[c][k], d[c][k])) for c in range(3) for k in range(nl))
+        assert abs(fd - ad) <= 1e-5 * max(abs(fd), abs(ad)), (fd, ad)
+
+
+@pytest.mark.parametrize("integrator", [1, 2, 3])
+def test_cubic_tangent_linear_model_matches_adjoint(integrator):
+    import torch
+
+    import libcfd2lcs_b200 as L
+    n, nl, dt = 10, 6, 0.05
+    g, lev, times = _levels(n, nl, dt)
+    wgt = _weight(g)
+    J, gu, gv, gw = L.adjoint_ftle(g, *lev, times, wgt, integrator=integrator, checkpoint_every=3, interpolator=3)
+    grads = (gu, gv, gw)
+    rng = np.random.default_rng(17)
+    for _ in range(2):
+        d = [[torch.from_numpy(rng.standard_normal(lev[c][k].numel())).cuda() for k in range(nl)] for c in range(3)]
+        Jt, dJ = L.tangent_ftle(g, *lev, times, wgt, *d, integrator=integrator, interpolator=3)
+        assert Jt == J
+        ad = sum(float(torch.dot(grads[c][k], d[c][k])) for c in range(3) for k in range(nl))
+        assert abs(dJ - ad) <= 1e-11 * max(abs(dJ), abs(ad)), (dJ, ad)
+
+
+def test_adjoint_rejects_other_interpolators():
+    import torch
+
+    import libcfd2lcs_b200 as L
+    g, lev, times = _levels(6, 3, 0.05)
+    with pytest.raises(RuntimeError, match="LINEAR or CUBIC"):
+        L.adjoint_ftle(g, *lev, times, _weight(g), interpolator=2)
