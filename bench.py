@@ -765,17 +765,17 @@ def run_adjoint(args):
     lev32 = [[t.float() for t in comp] for comp in lev64]
     w32 = w64.float()
     # FP32 gradient (timed), after one untimed call
-    L.adjoint_ftle(g, *lev32, times, w32, checkpoint_every=K, precision="sp")
+    L.adjoint_ftle(g, *lev32, times, w32, checkpoint_every=K, precision="sp", interpolator=args.adj_interp)
     runs = []
     for _ in range(max(1, args.steps)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        J32, g32u, g32v, g32w = L.adjoint_ftle(g, *lev32, times, w32, checkpoint_every=K, precision="sp")
+        J32, g32u, g32v, g32w = L.adjoint_ftle(g, *lev32, times, w32, checkpoint_every=K, precision="sp", interpolator=args.adj_interp)
         torch.cuda.synchronize()
         runs.append(time.perf_counter() - t0)
     el = min(runs)
     # FP64 gradient and finite differences
-    J64, gu, gv, gw = L.adjoint_ftle(g, *lev64, times, w64, checkpoint_every=K, precision="dp")
+    J64, gu, gv, gw = L.adjoint_ftle(g, *lev64, times, w64, checkpoint_every=K, precision="dp", interpolator=args.adj_interp)
     num = sum(float(torch.sum((a.double() - b) ** 2)) for A, B in ((g32u, gu), (g32v, gv), (g32w, gw)) for a, b in zip(A, B))
     den = sum(float(torch.sum(b ** 2)) for B in (gu, gv, gw) for b in B)
     rel32 = math.sqrt(num / den) if den > 0 else None
@@ -786,15 +786,15 @@ def run_adjoint(args):
 
     def central(d, eps):
         Jp, *_ = L.adjoint_ftle(g, *[[lev64[c][k] + eps * d[c][k] for k in range(nl)] for c in range(3)], times, w64,
-                                checkpoint_every=K, precision="dp", gradient=False)
+                                checkpoint_every=K, precision="dp", gradient=False, interpolator=args.adj_interp)
         Jm, *_ = L.adjoint_ftle(g, *[[lev64[c][k] - eps * d[c][k] for k in range(nl)] for c in range(3)], times, w64,
-                                checkpoint_every=K, precision="dp", gradient=False)
+                                checkpoint_every=K, precision="dp", gradient=False, interpolator=args.adj_interp)
         return (Jp - Jm) / (2 * eps)
 
     for q in range(nfd):
         d = [[torch.randn(lev64[c][k].numel(), generator=gen, device="cuda", dtype=torch.float64) for k in range(nl)] for c in range(3)]
         ad = sum(float(torch.dot(G[k], d[c][k])) for c, G in enumerate((gu, gv, gw)) for k in range(nl))
-        _, tl = L.tangent_ftle(g, *lev64, times, w64, *d, precision="dp")
+        _, tl = L.tangent_ftle(g, *lev64, times, w64, *d, precision="dp", interpolator=args.adj_interp)
         tl_err.append(abs(tl - ad) / max(abs(tl), abs(ad), 1e-300))
         fd = central(d, FD_EPS)
         fd_ad.append(ad)
@@ -817,7 +817,7 @@ def run_adjoint(args):
     api.init(g.n, g.x, g.y, g.z, g.flag)
     api.diagnostic_init(1, 0, times[-1], times[-1], "b")
     api.set_option("INTEGRATOR", 2)
-    api.set_option("INTERPOLATOR", 1)
+    api.set_option("INTERPOLATOR", args.adj_interp)
     for k in range(nl):
         api.update_device(lev32[0][k].data_ptr(), lev32[1][k].data_ptr(), lev32[2][k].data_ptr(), times[k])
     work = api.counters()["integrations_bkwd"]
@@ -825,6 +825,7 @@ def run_adjoint(args):
     line = {"metric": METRIC, "value": work / el, "unit": UNIT, "n_gpus": 1, "steps": len(runs), "warmup": 1,
             "ms_per_step": 1000.0 * el, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": {"workload": ADJ_DESC, "grid": [n, n, n], "levels": nl,
+                                            "interpolator": "CUBIC" if args.adj_interp == 3 else "LINEAR",
                                             "timing": "wall clock of one gradient call (forward, checkpoints, reverse sweep), best of steps",
                                             "value_counts": "grid points x subcycles of the forward map per gradient"},
             "gradient_s": el, "J_fp32": J32, "J_fp64": J64,
@@ -851,6 +852,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="abc256", choices=sorted(WORKLOADS) + ["batch64", "adj128"])
     ap.add_argument("--fd-dirs", type=int, default=16, help="adj128: finite-difference directions")
+    ap.add_argument("--adj-interp", type=int, default=1, choices=(1, 3), help="adj128: LINEAR (1, the ADJ config) or CUBIC (3)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--acc-n", type=int, default=64, help="--precision mixed: grid of its FTLE error run (0: skip)")
     ap.add_argument("--mixed", default="auto", choices=["auto", "on", "off"],
