@@ -71,6 +71,35 @@ __device__ __forceinline__ void lin_stencil(const DevGrid<T> &g, const T x[3], c
   st.w[7] = t[0] * t[1] * t[2];
 }
 
+// lin_stencil around a grid node no (1 <= no <= n on every axis) from the node's interpolation
+// lines lm, lc, lp at no-1, no, no+1: the bracket is [no, no+1] or [no-1, no], which the clamps of
+// lin_stencil leave as they are, so the stencil is the same in every bit.
+template <typename T>
+__device__ __forceinline__ void lin_stencil_node(const T lm[3], const T lc[3], const T lp[3], int sx, int sxy, const T x[3],
+                                                 const int no[3], LinStencil<T> &st) {
+  const int str[3] = {1, sx, sxy};
+  T t[3], mt[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const bool up = x[a] > lc[a];
+    const T x0 = up ? lc[a] : lm[a], x1 = up ? lp[a] : lc[a];
+    t[a] = clamp01((x[a] - x0) / (x1 - x0));
+    mt[a] = T(1) - t[a];
+    st.i0[a] = up ? no[a] : no[a] - 1;
+    st.d[a] = 1;
+    st.s[a] = str[a];
+  }
+  st.p0 = pidx(sx, sxy, st.i0[0], st.i0[1], st.i0[2]);
+  st.w[0] = mt[0] * mt[1] * mt[2];
+  st.w[1] = t[0] * mt[1] * mt[2];
+  st.w[2] = mt[0] * t[1] * mt[2];
+  st.w[3] = t[0] * t[1] * mt[2];
+  st.w[4] = mt[0] * mt[1] * t[2];
+  st.w[5] = t[0] * mt[1] * t[2];
+  st.w[6] = mt[0] * t[1] * t[2];
+  st.w[7] = t[0] * t[1] * t[2];
+}
+
 // Corner c of the stencil (bit 0: x, bit 1: y, bit 2: z upper corner) as a padded index; the
 // contractions below take the corner values through a loader, so the gathering kernels and the
 // shared-memory tile kernels run one expression (and get the same bits).

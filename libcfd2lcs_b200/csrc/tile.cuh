@@ -523,10 +523,23 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLL_MINB)
     mbar_wait_bounded(&bar, 0);  // let the copies in flight land before the block leaves
     return;
   }
-  auto vel_sample = [&](const T x[3], const int no[3], T ct_, T u[3]) {
+  // the interpolation lines at no-1, no, no+1 of both points (every bracket of a node's stages
+  // and departure point lies there), read while the box copies are in flight
+  T lm[2][3], lc[2][3], lp[2][3];
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    const int nd[3] = {min(i, g.P.n[0]), min(j, g.P.n[1]), min(kq[q], g.P.n[2])};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      lm[q][a] = __ldg(g.li[a] + nd[a] - 1);
+      lc[q][a] = __ldg(g.li[a] + nd[a]);
+      lp[q][a] = __ldg(g.li[a] + nd[a] + 1);
+    }
+  }
+  auto vel_sample = [&](const T x[3], const int no[3], T ct_, T u[3], int q) {
     const TV ct = TV(ct_), omc = TV(1) - ct;
     LinStencil<T> st;
-    lin_stencil(g, x, no, st);
+    lin_stencil_node(lm[q], lc[q], lp[q], sx, sxy, x, no, st);
     int idx[8];
 #pragma unroll
     for (int c = 0; c < 8; c++)
@@ -559,7 +572,7 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLL_MINB)
       T xh[3];
 #pragma unroll
       for (int c = 0; c < 3; c++) xh[c] = xn[q][c] + HALF * dt * u[c];
-      vel_sample(xh, no, T(S.ct[1]), u);
+      vel_sample(xh, no, T(S.ct[1]), u, q);
 #pragma unroll
       for (int c = 0; c < 3; c++) x[c] = xn[q][c] + dt * u[c];
     } else if (NOFF == 2) {
@@ -570,14 +583,14 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLL_MINB)
         acc[c] = xn[q][c] + SIXTH * kk[c];
         xs[c] = xn[q][c] + HALF * kk[c];
       }
-      vel_sample(xs, no, T(S.ct[1]), u);
+      vel_sample(xs, no, T(S.ct[1]), u, q);
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         kk[c] = dt * u[c];
         xs[c] = xn[q][c] + TWO * kk[c];
         acc[c] = acc[c] + TWOTHIRD * kk[c];
       }
-      vel_sample(xs, no, T(S.ct[2]), u);
+      vel_sample(xs, no, T(S.ct[2]), u, q);
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         kk[c] = dt * u[c];
@@ -591,21 +604,21 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLL_MINB)
         acc[c] = xn[q][c] + SIXTH * kk[c];
         xs[c] = xn[q][c] + HALF * kk[c];
       }
-      vel_sample(xs, no, T(S.ct[1]), u);
+      vel_sample(xs, no, T(S.ct[1]), u, q);
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         kk[c] = dt * u[c];
         acc[c] = acc[c] + THIRD * kk[c];
         xs[c] = xn[q][c] + HALF * kk[c];
       }
-      vel_sample(xs, no, T(S.ct[2]), u);
+      vel_sample(xs, no, T(S.ct[2]), u, q);
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         kk[c] = dt * u[c];
         acc[c] = acc[c] + THIRD * kk[c];
         xs[c] = xn[q][c] + kk[c];
       }
-      vel_sample(xs, no, T(S.ct[3]), u);
+      vel_sample(xs, no, T(S.ct[3]), u, q);
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         kk[c] = dt * u[c];
@@ -620,7 +633,7 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLL_MINB)
     }
     // previous flow map at the departure point (sample_field LINEAR around the node)
     LinStencil<T> st;
-    lin_stencil(g, x, no, st);
+    lin_stencil_node(lm[q], lc[q], lp[q], sx, sxy, x, no, st);
     int idx[8];
 #pragma unroll
     for (int c = 0; c < 8; c++)
