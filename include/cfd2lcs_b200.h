@@ -164,7 +164,7 @@ void cfd2lcs_batch_reset_c(void);
  * backward FTLE of the whole horizon (the frame the library computes with h = T, T = time of
  * the last level minus the first), with respect to the velocity at every level, by a
  * hand-written reverse sweep through the semi-Lagrangian updates (LINEAR interpolation;
- * integrator EULER, TRAPEZOIDAL, RK2 or RK3) with a flow-map checkpoint every `checkpoint_every`
+ * integrator EULER, TRAPEZOIDAL, RK2, RK3 or RK4) with a flow-map checkpoint every `checkpoint_every`
  * updates.  Grid: rectilinear, three-dimensional, every direction periodic, no boundary
  * flags.  d_u[l], d_v[l], d_w[l]: device arrays of level l (n[0]*n[1]*n[2], i fastest);
  * times: host, increasing; d_weight: device, n[0]*n[1]*n[2].  Writes *J and, when d_gu,
@@ -189,17 +189,22 @@ int cfd2lcs_tangent_ftle_c(const int n[3], const lcsdata_t *x, const lcsdata_t *
                            const lcsdata_t *const *d_du, const lcsdata_t *const *d_dv, const lcsdata_t *const *d_dw, double *J,
                            double *dJ, char *msg, size_t len);
 
-/* The two calls above with the interpolator chosen: LINEAR or CUBIC (the not-a-knot cubic
- * B-spline of every axis, the library's cubic path; at least 3 points per direction).  With
+/* The two calls above with the boundary flags and the interpolator given.  flag: n[0]*n[1]*n[2]
+ * values as cfd2lcs_init takes them, or NULL for all LCS_INTERNAL (the calls above); with LINEAR
+ * interpolation any rectilinear grid, walled, with inflow / outflow, masked or 2-D, whose
+ * particle boundary conditions and ghost rules the sweeps differentiate (projections along the
+ * boundary normal and the plane, sticks and zeroed values held as the forward took them).
+ * interpolator: LINEAR or CUBIC (the not-a-knot cubic B-spline of every axis, the library's cubic
+ * path; three-dimensional periodic grids without flags, at least 3 points per direction).  With
  * CUBIC the reverse sweep scatters into the spline coefficients and carries that adjoint back
  * through the transposed banded solves of each fit; the tangent model fits the direction's
  * levels and the tangent map alongside. */
-int cfd2lcs_adjoint_ftle_interp_c(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, int integrator,
+int cfd2lcs_adjoint_ftle_interp_c(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, const int *flag, int integrator,
                                   int interpolator, lcsdata_t cfl, int nlevels, const lcsdata_t *const *d_u,
                                   const lcsdata_t *const *d_v, const lcsdata_t *const *d_w, const lcsdata_t *times,
                                   const lcsdata_t *d_weight, int checkpoint_every, double *J, lcsdata_t *const *d_gu,
                                   lcsdata_t *const *d_gv, lcsdata_t *const *d_gw, char *msg, size_t len);
-int cfd2lcs_tangent_ftle_interp_c(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, int integrator,
+int cfd2lcs_tangent_ftle_interp_c(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, const int *flag, int integrator,
                                   int interpolator, lcsdata_t cfl, int nlevels, const lcsdata_t *const *d_u,
                                   const lcsdata_t *const *d_v, const lcsdata_t *const *d_w, const lcsdata_t *times,
                                   const lcsdata_t *d_weight, const lcsdata_t *const *d_du, const lcsdata_t *const *d_dv,

@@ -131,11 +131,11 @@ def load(precision: str = "dp") -> C.CDLL:
     lib.cfd2lcs_adjoint_ftle_c.restype = C.c_int
     lib.cfd2lcs_tangent_ftle_c.argtypes = [P, P, P, P, C.c_int, R, C.c_int, P, P, P, P, P, P, P, P, P, P, C.c_char_p, C.c_size_t]
     lib.cfd2lcs_tangent_ftle_c.restype = C.c_int
-    lib.cfd2lcs_adjoint_ftle_interp_c.argtypes = [P, P, P, P, C.c_int, C.c_int, R, C.c_int, P, P, P, P, P, C.c_int, P, P, P, P, C.c_char_p,
-                                                  C.c_size_t]
+    lib.cfd2lcs_adjoint_ftle_interp_c.argtypes = [P, P, P, P, P, C.c_int, C.c_int, R, C.c_int, P, P, P, P, P, C.c_int, P, P, P, P,
+                                                  C.c_char_p, C.c_size_t]
     lib.cfd2lcs_adjoint_ftle_interp_c.restype = C.c_int
-    lib.cfd2lcs_tangent_ftle_interp_c.argtypes = [P, P, P, P, C.c_int, C.c_int, R, C.c_int, P, P, P, P, P, P, P, P, P, P, C.c_char_p,
-                                                  C.c_size_t]
+    lib.cfd2lcs_tangent_ftle_interp_c.argtypes = [P, P, P, P, P, C.c_int, C.c_int, R, C.c_int, P, P, P, P, P, P, P, P, P, P,
+                                                  C.c_char_p, C.c_size_t]
     lib.cfd2lcs_tangent_ftle_interp_c.restype = C.c_int
     _LIBS[precision] = lib
     return lib
@@ -423,10 +423,10 @@ def adjoint_ftle(grid, u, v, w, times, weight, integrator=2, cfl=0.5, checkpoint
         g = [[torch.empty_like(t) for t in comp] for comp in (u, v, w)]
     msg = C.create_string_buffer(512)
     p = lambda a: a.ctypes.data_as(C.c_void_p)
-    rc = lib.cfd2lcs_adjoint_ftle_interp_c(p(n), p(xs), p(ys), p(zs), int(integrator), int(interpolator), R(cfl), L,
-                                    C.cast(ptrs(u), C.c_void_p),
-                                    C.cast(ptrs(v), C.c_void_p), C.cast(ptrs(w), C.c_void_p), p(tm), C.c_void_p(weight.data_ptr()),
-                                    int(checkpoint_every), C.byref(J),
+    fl = np.asfortranarray(grid.flag, dtype=np.int32).ravel(order="F")
+    rc = lib.cfd2lcs_adjoint_ftle_interp_c(p(n), p(xs), p(ys), p(zs), p(fl), int(integrator), int(interpolator), R(cfl), L,
+                                           C.cast(ptrs(u), C.c_void_p), C.cast(ptrs(v), C.c_void_p), C.cast(ptrs(w), C.c_void_p), p(tm),
+                                           C.c_void_p(weight.data_ptr()), int(checkpoint_every), C.byref(J),
                                     C.cast(ptrs(g[0]), C.c_void_p) if g else None, C.cast(ptrs(g[1]), C.c_void_p) if g else None,
                                     C.cast(ptrs(g[2]), C.c_void_p) if g else None, msg, 512)
     if rc:
@@ -451,9 +451,10 @@ def tangent_ftle(grid, u, v, w, times, weight, du, dv, dw, integrator=2, cfl=0.5
     J, dJ = C.c_double(0.0), C.c_double(0.0)
     msg = C.create_string_buffer(512)
     p = lambda a: a.ctypes.data_as(C.c_void_p)
-    rc = lib.cfd2lcs_tangent_ftle_interp_c(p(n), p(xs), p(ys), p(zs), int(integrator), int(interpolator), R(cfl), L, ptrs(u), ptrs(v),
-                                           ptrs(w), p(tm),
-                                    C.c_void_p(weight.data_ptr()), ptrs(du), ptrs(dv), ptrs(dw), C.byref(J), C.byref(dJ), msg, 512)
+    fl = np.asfortranarray(grid.flag, dtype=np.int32).ravel(order="F")
+    rc = lib.cfd2lcs_tangent_ftle_interp_c(p(n), p(xs), p(ys), p(zs), p(fl), int(integrator), int(interpolator), R(cfl), L, ptrs(u),
+                                           ptrs(v), ptrs(w), p(tm), C.c_void_p(weight.data_ptr()), ptrs(du), ptrs(dv), ptrs(dw),
+                                           C.byref(J), C.byref(dJ), msg, 512)
     if rc:
         raise RuntimeError(msg.value.decode(errors="replace"))
     return J.value, dJ.value

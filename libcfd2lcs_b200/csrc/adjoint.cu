@@ -1,8 +1,8 @@
 // Reverse-mode derivative of a backward-FTLE objective J = sum_x w(x) FTLE(x) with respect to
 // the gridded velocity at every time level.  No counterpart in the reference library; the
 // forward model is the library's own backward semi-Lagrangian path (update_flowmap_sl,
-// src/flowmap_m.f90:17-104, with LINEAR interpolation, src/lp_tracking_m.f90:342-474, and the
-// EULER / TRAPEZOIDAL / RK2 steps of integrate_lp, src/lp_motion_m.f90:129-210) over every
+// src/flowmap_m.f90:17-104, with LINEAR interpolation, src/lp_tracking_m.f90:342-474, or the
+// cubic B-spline, :476-524, and the steps of integrate_lp, src/lp_motion_m.f90:129-327) over every
 // update from the first level to the last, and compute_ftle (src/lcs_m.f90:66-193) of the
 // final flow map -- the frame the library computes when h equals the whole horizon.
 //
@@ -19,9 +19,11 @@
 // held fixed, as differentiation of the piecewise-smooth map requires.
 //
 // Scope: a rectilinear grid with every flag LCS_INTERNAL and every non-singleton direction
-// periodic (the ABC configuration); LINEAR interpolation; EULER, TRAPEZOIDAL or RK2.
+// periodic (the ABC configuration); LINEAR or CUBIC interpolation (the cubic sweeps carry the
+// adjoint through the spline fits); EULER, TRAPEZOIDAL, RK2, RK3 or RK4.
 #include "adjoint.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -44,7 +46,7 @@ namespace {
     }                                                                                            \
   } while (0)
 
-enum { EULER = 0, TRAPEZOIDAL = 1, RK2 = 2, RK3 = 3 };
+enum { EULER = 0, TRAPEZOIDAL = 1, RK2 = 2, RK3 = 3, RK4 = 4 };
 enum { LINEAR_I = 1, CUBIC_I = 3 };
 
 // device memory of one adjoint call
@@ -120,8 +122,57 @@ __device__ __forceinline__ T dweight(const T t[3], int q, int a) {
   return r;
 }
 
+// particle_bc<T, true> (advect.cuh) for the particle of interior node no, recording what it did:
+// a projection back along the boundary normal nrm (proj), or a stick to the node (returns true).
+// The same arithmetic as the forward kernel, so the positions are its positions.
+template <typename T>
+__device__ __forceinline__ bool bc_record(const DevGrid<T> &g, const int no[3], T x[3], bool &proj, T nrm[3]) {
+  proj = false;
+  const int p = pidx(g.P.sx, g.P.sxy, no[0], no[1], no[2]);
+  const int f = g.flag[p];
+  if (f == LCS_INTERNAL || f == LCS_2D) return false;
+  const bool interior = no[0] > 1 && no[1] > 1 && no[2] > 1 && no[0] < g.P.n[0] && no[1] < g.P.n[1] && no[2] < g.P.n[2];
+  if (f == LCS_MASK || f == LCS_SLIP || f == LCS_WALL) {
+    if (f != LCS_MASK && interior) return false;
+    const T nx = __ldg(g.nrm[0] + p), ny = __ldg(g.nrm[1] + p), nz = __ldg(g.nrm[2] + p);
+    const T gx = __ldg(g.lt[0] + no[0]), gy = __ldg(g.lt[1] + no[1]), gz = __ldg(g.lt[2] + no[2]);
+    const T dist = (x[0] - gx) * nx + (x[1] - gy) * ny + (x[2] - gz) * nz;
+    if (dist > T(0)) {
+      x[0] = x[0] - nx * dist;
+      x[1] = x[1] - ny * dist;
+      x[2] = x[2] - nz * dist;
+      proj = true;
+      nrm[0] = nx;
+      nrm[1] = ny;
+      nrm[2] = nz;
+    }
+    return false;
+  }
+  if (f == LCS_INFLOW || f == LCS_OUTFLOW) return !interior;
+  return false;
+}
+
+// The transpose of the plane projection and particle_bc on a position adjoint: zero after a
+// stick, (I - n n^T) after a projection, the singleton axis' component dropped on a 2-D grid.
+template <typename T>
+__device__ __forceinline__ void bc_adjoint(const DevGrid<T> &g, bool stick, bool proj, const T nrm[3], T xb[3]) {
+  if (stick) {
+    xb[0] = xb[1] = xb[2] = T(0);
+    return;
+  }
+  if (proj) {
+    const T d = xb[0] * nrm[0] + xb[1] * nrm[1] + xb[2] * nrm[2];
+#pragma unroll
+    for (int c = 0; c < 3; c++) xb[c] -= nrm[c] * d;
+  }
+  const int sa = g.P.single_axis;
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+    if (c == sa) xb[c] = T(0);
+}
+
 // ---------------------------------------------------------------------------------------
-// Adjoint of one backward SL subcycle (k_sl_subcycle with LINEAR interpolation, no flags).
+// Adjoint of one backward SL subcycle (k_sl_subcycle with LINEAR interpolation; F: boundary flags).
 // fbn: adjoint of the new flow map (interior values used); fbo: accumulated adjoint of the
 // previous map.  The velocity adjoint of the second stage goes to a2 (scattered, one blended
 // field: the time blend is distributed onto the two levels afterwards by k_distribute), that
@@ -129,7 +180,7 @@ __device__ __forceinline__ T dweight(const T t[3], int q, int a) {
 // ---------------------------------------------------------------------------------------
 // RK3 (integrate_lp, src/lp_motion_m.f90:212-263, with the third stage at xn + 2 k2): the
 // third stage's velocity adjoint goes to a3 (scattered) and k_distribute takes its ct[2].
-template <typename T, int INTEG>
+template <typename T, int INTEG, bool F = false>
 __global__ void __launch_bounds__(256) k_sl_adjoint(DevGrid<T> g, VelFields<T> V, FieldPtrs<T> fmo, FieldPtrs<T> fbn, FieldPtrsW<T> fbo,
                                                      FieldPtrsW<T> a1, FieldPtrsW<T> a2, FieldPtrsW<T> a3, StageTimes S, T dt) {
   int i, j, k;
@@ -145,12 +196,42 @@ __global__ void __launch_bounds__(256) k_sl_adjoint(DevGrid<T> g, VelFields<T> V
   T u1[3];
 #pragma unroll
   for (int c = 0; c < 3; c++) u1[c] = omc0 * __ldg(V.un[c] + p) + ct0 * __ldg(V.unp1[c] + p);
-  T x[3], xh[3], xs3[3];
-  LinStencilAD<T> s2, s2b;
+  T x[3], xh[3], xs3[3], xs4[3];
+  LinStencilAD<T> s2, s2b, s2c;
   const T ct1 = T(S.ct[1]), omc1 = T(1) - ct1;
   const T ct2 = T(S.ct[2]), omc2 = T(1) - ct2;
-  const T SIXTH = T(1) / T(6), TWOTHIRD = T(2) / T(3), TWO = T(2);
-  if (INTEG == RK3) {
+  const T ct3 = T(S.ct[3]), omc3 = T(1) - ct3;
+  const T SIXTH = T(1) / T(6), TWOTHIRD = T(2) / T(3), TWO = T(2), THIRD = T(1) / T(3);
+  if (INTEG == RK4) {
+    // integrate_lp RK4 (src/lp_motion_m.f90:265-327): stages at xn + k1/2, xn + k2/2, xn + k3
+    T k[3], acc[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k[c] = dt * u1[c];
+      acc[c] = x0[c] + SIXTH * k[c];
+      xh[c] = x0[c] + HALF * k[c];
+    }
+    lin_stencil_ad(g, xh, no, s2);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k[c] = dt * lin_apply_blend<T, T>(s2.st, V.un[c], V.unp1[c], omc1, ct1);
+      acc[c] = acc[c] + THIRD * k[c];
+      xs3[c] = x0[c] + HALF * k[c];
+    }
+    lin_stencil_ad(g, xs3, no, s2b);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k[c] = dt * lin_apply_blend<T, T>(s2b.st, V.un[c], V.unp1[c], omc2, ct2);
+      acc[c] = acc[c] + THIRD * k[c];
+      xs4[c] = x0[c] + k[c];
+    }
+    lin_stencil_ad(g, xs4, no, s2c);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k[c] = dt * lin_apply_blend<T, T>(s2c.st, V.un[c], V.unp1[c], omc3, ct3);
+      x[c] = acc[c] + SIXTH * k[c];
+    }
+  } else if (INTEG == RK3) {
     T k[3], acc[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
@@ -184,6 +265,17 @@ __global__ void __launch_bounds__(256) k_sl_adjoint(DevGrid<T> g, VelFields<T> V
 #pragma unroll
     for (int c = 0; c < 3; c++) x[c] = x0[c] + dt * u1[c];
   }
+  // --- the forward kernel's plane projection and particle boundary condition ---
+  bool stick = false, proj = false;
+  T bn[3] = {T(0), T(0), T(0)};
+  {
+    int nb[3] = {i, j, k};
+    project_plane(g, nb, x);
+    if (F) stick = bc_record(g, nb, x, proj, bn);
+    if (stick)
+#pragma unroll
+      for (int c = 0; c < 3; c++) x[c] = x0[c];
+  }
   LinStencilAD<T> s3;
   lin_stencil_ad(g, x, no, s3);
   // --- fm_new = fm_old(x) + (x - x0) ---
@@ -200,6 +292,7 @@ __global__ void __launch_bounds__(256) k_sl_adjoint(DevGrid<T> g, VelFields<T> V
       for (int d = 0; d < 3; d++) xb[d] += a[c] * dweight(s3.t, q, d) * s3.dtdx[d] * f;
     }
   }
+  bc_adjoint(g, stick, proj, bn, xb);
   // --- stages ---
   T u1b[3];
   // scatter of a sampled stage's velocity adjoint ub (weights of stencil st, blend omc/ct) into
@@ -219,7 +312,33 @@ __global__ void __launch_bounds__(256) k_sl_adjoint(DevGrid<T> g, VelFields<T> V
       }
     }
   };
-  if (INTEG == RK3) {
+  if (INTEG == RK4) {
+    // x = xn + k1/6 + k2/3 + k3/3 + k4/6; the two half-step stages share ct and go to a2, the
+    // last stage to a3 (distributed with ct[3])
+    T k3b[3], k2b[3], k1b[3], ub[3], pb[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k1b[c] = SIXTH * xb[c];
+      k2b[c] = THIRD * xb[c];
+      k3b[c] = THIRD * xb[c];
+      ub[c] = dt * (SIXTH * xb[c]);
+    }
+    stage_back(s2c, ub, a3, omc3, ct3, pb);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k3b[c] += pb[c];
+      ub[c] = dt * k3b[c];
+    }
+    stage_back(s2b, ub, a2, omc2, ct2, pb);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k2b[c] += HALF * pb[c];
+      ub[c] = dt * k2b[c];
+    }
+    stage_back(s2, ub, a2, omc1, ct1, pb);
+#pragma unroll
+    for (int c = 0; c < 3; c++) u1b[c] = dt * (k1b[c] + HALF * pb[c]);
+  } else if (INTEG == RK3) {
     // x = xn + k1/6 + 2 k2/3 + k3/6, k3 = dt u(xs3), xs3 = xn + 2 k2, k2 = dt u(xh), xh = xn + k1/2
     T k3b[3], k2b[3], k1b[3], ub[3], pb[3];
 #pragma unroll
@@ -295,9 +414,9 @@ __global__ void __launch_bounds__(256) k_distribute(FieldPtrsW<T> a1, FieldPtrsW
 // fractions as the forward kernel and k_sl_adjoint, so that for every direction d the
 // tangent's dJ equals the adjoint's <dJ/du, d> to rounding.
 // ---------------------------------------------------------------------------------------
-template <typename T, int INTEG>
+template <typename T, int INTEG, bool F = false>
 __global__ void __launch_bounds__(256) k_sl_tangent(DevGrid<T> g, VelFields<T> V, VelFields<T> D, FieldPtrs<T> fmo, FieldPtrs<T> dfo,
-                                                     FieldPtrsW<T> dfn, StageTimes S, T dt) {
+                                                     FieldPtrsW<T> dfn, StageTimes S, T dt, int *err) {
   int i, j, k;
   if (!node_of_thread(g.P.n, i, j, k)) return;
   const int p = pidx(g.P.sx, g.P.sxy, i, j, k);
@@ -331,7 +450,47 @@ __global__ void __launch_bounds__(256) k_sl_tangent(DevGrid<T> g, VelFields<T> V
       for (int c = 0; c < 3; c++) du[c] += dwq * (omc * __ldg(V.un[c] + cq) + ct * __ldg(V.unp1[c] + cq));
     }
   };
-  if (INTEG == RK3) {
+  if (INTEG == RK4) {
+    const T R4_HALF = T(1) / T(2), R4_SIXTH = T(1) / T(6), R4_THIRD = T(1) / T(3);
+    const T r1 = T(S.ct[1]), q1 = T(1) - r1, r2 = T(S.ct[2]), q2 = T(1) - r2, r3 = T(S.ct[3]), q3 = T(1) - r3;
+    T kk[3], dk[3], acc[3], dacc[3], xs[3], dxs[3], u[3], du[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u1[c];
+      dk[c] = dt * du1[c];
+      acc[c] = x0[c] + R4_SIXTH * kk[c];
+      dacc[c] = R4_SIXTH * dk[c];
+      xs[c] = x0[c] + R4_HALF * kk[c];
+      dxs[c] = R4_HALF * dk[c];
+    }
+    stage_tan(xs, dxs, q1, r1, u, du);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u[c];
+      dk[c] = dt * du[c];
+      acc[c] = acc[c] + R4_THIRD * kk[c];
+      dacc[c] = dacc[c] + R4_THIRD * dk[c];
+      xs[c] = x0[c] + R4_HALF * kk[c];
+      dxs[c] = R4_HALF * dk[c];
+    }
+    stage_tan(xs, dxs, q2, r2, u, du);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u[c];
+      dk[c] = dt * du[c];
+      acc[c] = acc[c] + R4_THIRD * kk[c];
+      dacc[c] = dacc[c] + R4_THIRD * dk[c];
+      xs[c] = x0[c] + kk[c];
+      dxs[c] = dk[c];
+    }
+    stage_tan(xs, dxs, q3, r3, u, du);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u[c];
+      x[c] = acc[c] + R4_SIXTH * kk[c];
+      dx[c] = dacc[c] + R4_SIXTH * (dt * du[c]);
+    }
+  } else if (INTEG == RK3) {
     const T SIXTH = T(1) / T(6), TWOTHIRD = T(2) / T(3), TWO = T(2);
     const T ct1 = T(S.ct[1]), omc1 = T(1) - ct1, ct2 = T(S.ct[2]), omc2 = T(1) - ct2;
     T k[3], dk[3], acc[3], dacc[3], xs[3], dxs[3], u[3], du[3];
@@ -398,6 +557,28 @@ __global__ void __launch_bounds__(256) k_sl_tangent(DevGrid<T> g, VelFields<T> V
       dx[c] = dt * du1[c];
     }
   }
+  // the forward kernel's plane projection and particle boundary condition, and their tangents
+  {
+    int nb[3] = {i, j, k};
+    project_plane(g, nb, x);
+    const int sa = g.P.single_axis;
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      if (c == sa) dx[c] = T(0);
+    bool proj = false;
+    T bn[3];
+    if (F && bc_record(g, nb, x, proj, bn)) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        x[c] = x0[c];
+        dx[c] = T(0);
+      }
+    } else if (proj) {
+      const T d = dx[0] * bn[0] + dx[1] * bn[1] + dx[2] * bn[2];
+#pragma unroll
+      for (int c = 0; c < 3; c++) dx[c] -= bn[c] * d;
+    }
+  }
   LinStencilAD<T> s3;
   lin_stencil_ad(g, x, no, s3);
   // fm_new = fm_old(x) + (x - x0)
@@ -412,8 +593,18 @@ __global__ void __launch_bounds__(256) k_sl_tangent(DevGrid<T> g, VelFields<T> V
 #pragma unroll
     for (int c = 0; c < 3; c++) out[c] += wq * __ldg(dfo.f[c] + cq) + dwq * __ldg(fmo.f[c] + cq);
   }
+  // the mask factor and the flow-map boundary rule (the forward kernel's vpre / vfin)
+  const int fl = F ? (int)g.flag[p] : (int)LCS_INTERNAL;
+  const T mask = fl != LCS_MASK ? T(1) : T(0);
+  const bool zero = F && (fl == LCS_MASK || fl == LCS_INFLOW || fl == LCS_OUTFLOW);
+  T vpre[3], vfin[3];
 #pragma unroll
-  for (int c = 0; c < 3; c++) dfn.f[c][p] = out[c];
+  for (int c = 0; c < 3; c++) {
+    vpre[c] = out[c] * mask;
+    vfin[c] = zero ? T(0) : vpre[c];
+    dfn.f[c][p] = vfin[c];
+  }
+  if (F) write_ghosts<T, true, GHOST_FM>(g, dfn.f, i, j, k, vpre, vfin, err);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -588,9 +779,38 @@ __global__ void __launch_bounds__(128) k_sl_adjoint_cubic(DevGrid<T> g, SplineAx
 #pragma unroll
   for (int c = 0; c < 3; c++) u1[c] = omc0 * __ldg(V.un[c] + p) + ct0 * __ldg(V.unp1[c] + p);
   // --- forward recomputation (integrate<>, first stage on the node) ---
-  CubicSample<T> s2, s3;
+  CubicSample<T> s2, s3, s4;
   T x[3];
-  if (INTEG == RK3) {
+  if (INTEG == RK4) {
+    const T ct3 = T(S.ct[3]), omc3 = T(1) - ct3, THIRD = T(1) / T(3);
+    T kk[3], acc[3], xs[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u1[c];
+      acc[c] = x0[c] + SIXTH * kk[c];
+      xs[c] = x0[c] + HALF * kk[c];
+    }
+    cubic_sample(g, sa, cn, cp, omc1, ct1, xs, no, s2);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * s2.u[c];
+      acc[c] = acc[c] + THIRD * kk[c];
+      xs[c] = x0[c] + HALF * kk[c];
+    }
+    cubic_sample(g, sa, cn, cp, omc2, ct2, xs, no, s3);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * s3.u[c];
+      acc[c] = acc[c] + THIRD * kk[c];
+      xs[c] = x0[c] + kk[c];
+    }
+    cubic_sample(g, sa, cn, cp, omc3, ct3, xs, no, s4);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * s4.u[c];
+      x[c] = acc[c] + SIXTH * kk[c];
+    }
+  } else if (INTEG == RK3) {
     T kk[3], acc[3], xs[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
@@ -650,7 +870,33 @@ __global__ void __launch_bounds__(128) k_sl_adjoint_cubic(DevGrid<T> g, SplineAx
       for (int d = 0; d < 3; d++) pb[d] += ub[c] * sm.gr[c][d];
   };
   T u1b[3];
-  if (INTEG == RK3) {
+  if (INTEG == RK4) {
+    // the two half-step stages share ct and go to a2, the last stage to a3 (with ct[3])
+    const T THIRD = T(1) / T(3);
+    T k3b[3], k2b[3], k1b[3], ub[3], pb[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k1b[c] = SIXTH * xb[c];
+      k2b[c] = THIRD * xb[c];
+      k3b[c] = THIRD * xb[c];
+      ub[c] = dt * (SIXTH * xb[c]);
+    }
+    stage_back(s4, ub, a3, pb);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k3b[c] += pb[c];
+      ub[c] = dt * k3b[c];
+    }
+    stage_back(s3, ub, a2, pb);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      k2b[c] += HALF * pb[c];
+      ub[c] = dt * k2b[c];
+    }
+    stage_back(s2, ub, a2, pb);
+#pragma unroll
+    for (int c = 0; c < 3; c++) u1b[c] = dt * (k1b[c] + HALF * pb[c]);
+  } else if (INTEG == RK3) {
     T k2b[3], k1b[3], ub[3], pb[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
@@ -719,7 +965,47 @@ __global__ void __launch_bounds__(128) k_sl_tangent_cubic(DevGrid<T> g, SplineAx
     }
   };
   T x[3], dx[3];
-  if (INTEG == RK3) {
+  if (INTEG == RK4) {
+    const T R4_HALF = T(1) / T(2), R4_SIXTH = T(1) / T(6), R4_THIRD = T(1) / T(3);
+    const T r1 = T(S.ct[1]), q1 = T(1) - r1, r2 = T(S.ct[2]), q2 = T(1) - r2, r3 = T(S.ct[3]), q3 = T(1) - r3;
+    T kk[3], dk[3], acc[3], dacc[3], xs[3], dxs[3], u[3], du[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u1[c];
+      dk[c] = dt * du1[c];
+      acc[c] = x0[c] + R4_SIXTH * kk[c];
+      dacc[c] = R4_SIXTH * dk[c];
+      xs[c] = x0[c] + R4_HALF * kk[c];
+      dxs[c] = R4_HALF * dk[c];
+    }
+    stage_tan(xs, dxs, q1, r1, u, du);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u[c];
+      dk[c] = dt * du[c];
+      acc[c] = acc[c] + R4_THIRD * kk[c];
+      dacc[c] = dacc[c] + R4_THIRD * dk[c];
+      xs[c] = x0[c] + R4_HALF * kk[c];
+      dxs[c] = R4_HALF * dk[c];
+    }
+    stage_tan(xs, dxs, q2, r2, u, du);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u[c];
+      dk[c] = dt * du[c];
+      acc[c] = acc[c] + R4_THIRD * kk[c];
+      dacc[c] = dacc[c] + R4_THIRD * dk[c];
+      xs[c] = x0[c] + kk[c];
+      dxs[c] = dk[c];
+    }
+    stage_tan(xs, dxs, q3, r3, u, du);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u[c];
+      x[c] = acc[c] + R4_SIXTH * kk[c];
+      dx[c] = dacc[c] + R4_SIXTH * (dt * du[c]);
+    }
+  } else if (INTEG == RK3) {
     T kk[3], dk[3], acc[3], dacc[3], xs[3], dxs[3], u[3], du[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
@@ -885,6 +1171,66 @@ __global__ void __launch_bounds__(256) k_periodic_ghosts(DevGrid<T> g, FieldPtrs
   for (int c = 0; c < 3; c++) f.f[c][p] = f.f[c][q];
 }
 
+// ---------------------------------------------------------------------------------------
+// Boundary flags (walls, slip, inflow / outflow, masks, 2-D).  The forward ghost fill
+// (write_ghosts, device_common.cuh) gives every ghost cell one rule: 0 the periodic image of a
+// node's value before the interior zeroing (vpre), 1 zero, 2 a copy of its nearest node's final
+// value (vfin); the interior zeroing is: flow map at MASK / INFLOW / OUTFLOW nodes, velocity at
+// MASK nodes, and the flow map's pre-zeroing value carries the mask factor (0 at MASK nodes).
+// Its adjoint runs in three passes over a padded adjoint field: copy ghosts into their nodes,
+// clear the nodes whose final value is zero, image ghosts into their nodes (times the mask for
+// the flow map) -- leaving at each node the adjoint of the quantity the subcycle computes before
+// any zeroing.
+// ---------------------------------------------------------------------------------------
+template <typename T, int KIND>
+__global__ void __launch_bounds__(256) k_fold_copy(DevGrid<T> g, FieldPtrsW<T> f, long ntot) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= ntot) return;
+  const int i = (int)(p % g.P.sx), j = (int)((p / g.P.sx) % (g.P.sxy / g.P.sx)), k = (int)(p / g.P.sxy);
+  if (i >= 1 && j >= 1 && k >= 1 && i <= g.P.n[0] && j <= g.P.n[1] && k <= g.P.n[2]) return;
+  const int rule = ghost_rule(KIND, (int)g.flag[p]);
+  if (rule == 0) return;
+  if (rule == 2) {
+    const int q = pidx(g.P.sx, g.P.sxy, min(max(i, 1), g.P.n[0]), min(max(j, 1), g.P.n[1]), min(max(k, 1), g.P.n[2]));
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const T v = f.f[c][p];
+      if (v != T(0)) atomicAdd(f.f[c] + q, v);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) f.f[c][p] = T(0);
+}
+
+template <typename T, int KIND>
+__global__ void __launch_bounds__(256) k_fold_zero(DevGrid<T> g, FieldPtrsW<T> f) {
+  int i, j, k;
+  if (!node_of_thread(g.P.n, i, j, k)) return;
+  const int p = pidx(g.P.sx, g.P.sxy, i, j, k);
+  const int fl = (int)g.flag[p];
+  const bool zero = KIND == GHOST_FM ? (fl == LCS_MASK || fl == LCS_INFLOW || fl == LCS_OUTFLOW) : fl == LCS_MASK;
+  if (!zero) return;
+#pragma unroll
+  for (int c = 0; c < 3; c++) f.f[c][p] = T(0);
+}
+
+template <typename T, int KIND>
+__global__ void __launch_bounds__(256) k_fold_image(DevGrid<T> g, FieldPtrsW<T> f, long ntot) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= ntot) return;
+  const int i = (int)(p % g.P.sx), j = (int)((p / g.P.sx) % (g.P.sxy / g.P.sx)), k = (int)(p / g.P.sxy);
+  if (i >= 1 && j >= 1 && k >= 1 && i <= g.P.n[0] && j <= g.P.n[1] && k <= g.P.n[2]) return;
+  if (ghost_rule(KIND, (int)g.flag[p]) != 0) return;  // cleared by k_fold_copy
+  const int q = pidx(g.P.sx, g.P.sxy, wrap_index(i, g.P.n[0]), wrap_index(j, g.P.n[1]), wrap_index(k, g.P.n[2]));
+  const T m = (KIND == GHOST_FM && g.flag[q] == LCS_MASK) ? T(0) : T(1);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const T v = f.f[c][p];
+    if (v != T(0)) atomicAdd(f.f[c] + q, m * v);
+    f.f[c][p] = T(0);
+  }
+}
+
 // interior of a padded field -> compact i-fastest arrays (the composed map of an h = T frame)
 template <typename T>
 __global__ void __launch_bounds__(256) k_interior(DevGrid<T> g, FieldPtrs<T> src, FieldPtrsW<T> dst) {
@@ -916,13 +1262,27 @@ __device__ __forceinline__ bool ftle_linearise(const DevGrid<T> &g, const FieldP
       L.qp[a] = L.qm[a] = -1;
       continue;
     }
-    int ip[3] = {i, j, k}, im[3] = {i, j, k};
-    ip[a] = wrap_index(idx[a] + 1, g.P.n[a]);
-    im[a] = wrap_index(idx[a] - 1, g.P.n[a]);
-    L.qp[a] = pidx(g.P.sx, g.P.sxy, ip[0], ip[1], ip[2]);
-    L.qm[a] = pidx(g.P.sx, g.P.sxy, im[0], im[1], im[2]);
+    // the neighbour value k_ftle's fm_neighbour reads: the node in range, its periodic image, the
+    // node itself behind a copy (rule 2) ghost, zero behind any other ghost (-1)
+    auto nbr = [&](int step) -> int {
+      int q[3] = {i, j, k};
+      q[a] = idx[a] + step;
+      if (q[a] >= 1 && q[a] <= g.P.n[a]) return pidx(g.P.sx, g.P.sxy, q[0], q[1], q[2]);
+      if (g.P.per[a]) {
+        q[a] = wrap_index(q[a], g.P.n[a]);
+        return pidx(g.P.sx, g.P.sxy, q[0], q[1], q[2]);
+      }
+      if (g.P.has_flags && ghost_rule(GHOST_FM, (int)g.flag[pidx(g.P.sx, g.P.sxy, q[0], q[1], q[2])]) == 2)
+        return pidx(g.P.sx, g.P.sxy, i, j, k);
+      return -1;
+    };
+    L.qp[a] = nbr(+1);
+    L.qm[a] = nbr(-1);
     L.den[a] = (double)(__ldg(g.lt[a] + idx[a] + 1) - __ldg(g.lt[a] + idx[a] - 1));
-    for (int c = 0; c < 3; c++) L.G[c][a] = (double)(fm.f[c][L.qp[a]] - fm.f[c][L.qm[a]]) / L.den[a];
+    for (int c = 0; c < 3; c++) {
+      const T fp = L.qp[a] >= 0 ? fm.f[c][L.qp[a]] : T(0), fq = L.qm[a] >= 0 ? fm.f[c][L.qm[a]] : T(0);
+      L.G[c][a] = (double)(fp - fq) / L.den[a];
+    }
   }
   double C[3][3];
   for (int a = 0; a < 3; a++)
@@ -970,11 +1330,11 @@ __global__ void __launch_bounds__(256) k_ftle_adjoint(DevGrid<T> g, FieldPtrs<T>
   // dJ/dG = w / (2 lam T) * 2 (G v) v^T
   const double coef = w / (L.lam * (double)Tint);
   for (int a = 0; a < 3; a++) {
-    if (L.qp[a] < 0) continue;
+    if (L.den[a] == 0.0) continue;  // singleton axis: no gradient column
     for (int c = 0; c < 3; c++) {
       const double gb = coef * L.Gv[c] * L.v[a] / L.den[a];
-      atomicAdd(fb.f[c] + L.qp[a], T(gb));
-      atomicAdd(fb.f[c] + L.qm[a], T(-gb));
+      if (L.qp[a] >= 0) atomicAdd(fb.f[c] + L.qp[a], T(gb));
+      if (L.qm[a] >= 0) atomicAdd(fb.f[c] + L.qm[a], T(-gb));
     }
   }
 }
@@ -995,8 +1355,11 @@ __global__ void __launch_bounds__(256) k_ftle_tangent(DevGrid<T> g, FieldPtrs<T>
   double dlam = 0.0;
   for (int c = 0; c < 3; c++) {
     double dGv = 0.0;
-    for (int a = 0; a < 3; a++)
-      if (L.qp[a] >= 0) dGv += (double)(dfm.f[c][L.qp[a]] - dfm.f[c][L.qm[a]]) / L.den[a] * L.v[a];
+    for (int a = 0; a < 3; a++) {
+      if (L.den[a] == 0.0) continue;
+      const T dp = L.qp[a] >= 0 ? dfm.f[c][L.qp[a]] : T(0), dq = L.qm[a] >= 0 ? dfm.f[c][L.qm[a]] : T(0);
+      dGv += (double)(dp - dq) / L.den[a] * L.v[a];
+    }
     dlam += 2.0 * L.Gv[c] * dGv;
   }
   out[q] = w * dlam / (2.0 * L.lam * (double)Tint);
@@ -1047,8 +1410,8 @@ class Adjoint {
       msg = "adjoint: at least two velocity levels are needed";
       return false;
     }
-    if (pr_.integrator != EULER && pr_.integrator != TRAPEZOIDAL && pr_.integrator != RK2 && pr_.integrator != RK3) {
-      msg = "adjoint: the integrator must be EULER, TRAPEZOIDAL, RK2 or RK3";
+    if (pr_.integrator < EULER || pr_.integrator > RK4) {
+      msg = "adjoint: the integrator must be EULER, TRAPEZOIDAL, RK2, RK3 or RK4";
       return false;
     }
     if (pr_.interpolator != LINEAR_I && pr_.interpolator != CUBIC_I) {
@@ -1066,6 +1429,7 @@ class Adjoint {
         return false;
       }
     std::vector<int> flag((size_t)n[0] * n[1] * n[2], 0);
+    if (pr_.flag) std::memcpy(flag.data(), pr_.flag, flag.size() * sizeof(int));
     if (!hg_.build(n, pr_.x, pr_.y, pr_.z, flag.data())) {
       msg = "adjoint: " + hg_.error;
       return false;
@@ -1074,15 +1438,18 @@ class Adjoint {
       msg = "adjoint: the grid must be an exact tensor product of coordinate lines";
       return false;
     }
-    for (int a = 0; a < 3; a++)
-      if (n[a] > 1 && !hg_.P.per[a]) {
-        msg = "adjoint: every non-singleton direction must be periodic";
+    if (cubic_) {
+      for (int a = 0; a < 3; a++)
+        if (n[a] > 1 && !hg_.P.per[a]) {
+          msg = "adjoint: CUBIC needs every direction periodic";
+          return false;
+        }
+      if (hg_.P.single_axis >= 0 || hg_.P.has_flags) {
+        msg = "adjoint: CUBIC needs a three-dimensional grid without boundary flags";
         return false;
       }
-    if (hg_.P.single_axis >= 0 || hg_.P.has_flags) {
-      msg = "adjoint: a three-dimensional grid without boundary flags is required";
-      return false;
     }
+    flags_ = hg_.P.has_flags != 0;
     N_ = (long)n[0] * n[1] * n[2];
     ntot_ = hg_.ntot();
     GridParams<T> P{};  // curv = 0 and no curvilinear tables: the adjoint runs on tensor-product grids
@@ -1100,7 +1467,7 @@ class Adjoint {
     for (int q = 0; q < 6; q++) P.bb[q] = (T)H.bb[q];
     for (int d = 0; d < 27; d++)
       for (int c = 0; c < 3; c++) P.ps[d][c] = (T)H.ps[d][c];
-    P.has_flags = 0;
+    P.has_flags = H.has_flags;
     P.maxtrack = H.maxtrack;
     dg_.P = P;
     for (int a = 0; a < 3; a++) {
@@ -1110,6 +1477,19 @@ class Adjoint {
       dg_.nrm[a] = nullptr;
     }
     dg_.flag = nullptr;
+    if (flags_) {
+      // the padded flags and boundary normals of the grid (the library's make_dev_grid)
+      int8_t *f = pool_.alloc<int8_t>(hg_.flag.size(), msg);
+      if (!f) return false;
+      ACK(cudaMemcpy(f, hg_.flag.data(), hg_.flag.size(), cudaMemcpyHostToDevice));
+      dg_.flag = f;
+      for (int a = 0; a < 3; a++) {
+        std::vector<lcsdata_t> comp(hg_.ntot(), lcsdata_t(0));
+        if (!hg_.bcnorm.empty())
+          std::copy(hg_.bcnorm.begin() + (size_t)a * hg_.ntot(), hg_.bcnorm.begin() + (size_t)(a + 1) * hg_.ntot(), comp.begin());
+        if (!(dg_.nrm[a] = upload(comp, msg))) return false;
+      }
+    }
     if (cubic_) {
       // the not-a-knot cubic of every axis over its padded coordinate line (the library's
       // ensure_spline), its pull table for the fits and the transposed one for their adjoint
@@ -1186,6 +1566,10 @@ class Adjoint {
       S.ct[0] = ct(t);
       S.ct[1] = ct(t + HALF * dt);
       if (pr_.integrator == RK3) S.ct[2] = ct(t + dt);
+      if (pr_.integrator == RK4) {
+        S.ct[2] = S.ct[1];
+        S.ct[3] = ct(t + dt);
+      }
     }
     return S;
   }
@@ -1202,8 +1586,12 @@ class Adjoint {
       std::memcpy(&init.cmin, &big, sizeof(double));
       *red_host_ = init;
       ACK(cudaMemcpyAsync(red_dev_, red_host_, sizeof(DevReduce), cudaMemcpyHostToDevice, stream_));
-      k_ingest<T, T, lcsdata_t, false><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, pr_.u[l], pr_.v[l], pr_.w[l], f[0], f[1], f[2],
-                                                                                  red_dev_);
+      if (flags_)
+        k_ingest<T, T, lcsdata_t, true><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, pr_.u[l], pr_.v[l], pr_.w[l], f[0], f[1], f[2],
+                                                                                   red_dev_);
+      else
+        k_ingest<T, T, lcsdata_t, false><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, pr_.u[l], pr_.v[l], pr_.w[l], f[0], f[1], f[2],
+                                                                                    red_dev_);
       ACK(cudaGetLastError());
       ACK(cudaMemcpyAsync(red_host_, red_dev_, sizeof(DevReduce), cudaMemcpyDeviceToHost, stream_));
       ACK(cudaStreamSynchronize(stream_));
@@ -1224,7 +1612,7 @@ class Adjoint {
     if (cubic_) {
       if (!slab(Cl_, (size_t)3 * L, msg)) return false;
       for (int l = 0; l < L; l++) fit3(&U_[3 * l], &Cl_[3 * l]);
-      for (int st = 1; st < 3; st++)
+      for (int st = 1; st < 4; st++)
         if (!field3(blend_[st], msg)) return false;
       if (!field3(cfm_, msg)) return false;
       ACK(cudaGetLastError());
@@ -1235,8 +1623,12 @@ class Adjoint {
       if (!(red_tan_ = pool_.alloc<DevReduce>(1, msg))) return false;
       ACK(cudaMemsetAsync(red_tan_, 0, sizeof(DevReduce), stream_));
       for (int l = 0; l < L; l++)
-        k_ingest<T, T, lcsdata_t, false><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, pr_.du[l], pr_.dv[l], pr_.dw[l], DU_[3 * l],
-                                                                                    DU_[3 * l + 1], DU_[3 * l + 2], red_tan_);
+        if (flags_)
+          k_ingest<T, T, lcsdata_t, true><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, pr_.du[l], pr_.dv[l], pr_.dw[l], DU_[3 * l],
+                                                                                     DU_[3 * l + 1], DU_[3 * l + 2], red_tan_);
+        else
+          k_ingest<T, T, lcsdata_t, false><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, pr_.du[l], pr_.dv[l], pr_.dw[l], DU_[3 * l],
+                                                                                      DU_[3 * l + 1], DU_[3 * l + 2], red_tan_);
       ACK(cudaGetLastError());
       int terr = 0;
       ACK(cudaMemcpyAsync(&terr, &red_tan_->err, sizeof(int), cudaMemcpyDeviceToHost, stream_));
@@ -1281,7 +1673,8 @@ class Adjoint {
     FieldPtrs<T> cm{};
     for (int c = 0; c < 3; c++) cm.f[c] = in[c];
     const T Tint = (T)(pr_.times[L - 1] - pr_.times[0]);
-    k_ftle<T, T, false><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, cm, ftle, Tint, 0);
+    if (flags_) k_ftle<T, T, true><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, cm, ftle, Tint, 0);
+    else k_ftle<T, T, false><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, cm, ftle, Tint, 0);
     ACK(cudaGetLastError());
     std::vector<T> hf(N_), hw(N_);
     ACK(cudaMemcpyAsync(hf.data(), ftle, N_ * sizeof(T), cudaMemcpyDeviceToHost, stream_));
@@ -1356,28 +1749,65 @@ class Adjoint {
           dfo.f[c] = dfm_[cur][c];
           dfn.f[c] = dfm_[cur ^ 1][c];
         }
-        if (pr_.integrator == RK3)
-          k_sl_tangent<T, RK3><<<grd, blk, 0, stream_>>>(dg_, V, D, fo, dfo, dfn, S, (T)dt);
-        else if (pr_.integrator == RK2)
-          k_sl_tangent<T, RK2><<<grd, blk, 0, stream_>>>(dg_, V, D, fo, dfo, dfn, S, (T)dt);
-        else
-          k_sl_tangent<T, EULER><<<grd, blk, 0, stream_>>>(dg_, V, D, fo, dfo, dfn, S, (T)dt);
-        k_periodic_ghosts<T><<<(unsigned)((ntot_ + 255) / 256), 256, 0, stream_>>>(dg_, dfn, ntot_);
+        if (flags_) tangent_linear<true>(grd, blk, V, D, fo, dfo, dfn, S, (T)dt, err);
+        else tangent_linear<false>(grd, blk, V, D, fo, dfo, dfn, S, (T)dt, err);
+        if (!flags_) k_periodic_ghosts<T><<<(unsigned)((ntot_ + 255) / 256), 256, 0, stream_>>>(dg_, dfn, ntot_);
         ACK(cudaGetLastError());
       }
-      if (pr_.integrator == RK3)
-        k_sl_subcycle<T, T, RK3_, INTERP_LINEAR, false><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, (T)dt, err);
-      else if (pr_.integrator == RK2)
-        k_sl_subcycle<T, T, RK2_, INTERP_LINEAR, false><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, (T)dt, err);
-      else if (pr_.integrator == TRAPEZOIDAL)
-        k_sl_subcycle<T, T, TRAPEZOIDAL_, INTERP_LINEAR, false><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, (T)dt, err);
-      else
-        k_sl_subcycle<T, T, EULER_, INTERP_LINEAR, false><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, (T)dt, err);
+      if (flags_) forward_linear<true>(grd, blk, sa, V, fo, fn, S, (T)dt, err);
+      else forward_linear<false>(grd, blk, sa, V, fo, fn, S, (T)dt, err);
       ACK(cudaGetLastError());
       cur ^= 1;
       lp = lp + dt;
     }
     return true;
+  }
+
+  // one LINEAR subcycle: the library's kernel, and the tangent sweep's (F: boundary flags)
+  template <bool F>
+  void forward_linear(dim3 grd, dim3 blk, const SplineAxes<T> &sa, const VelFields<T> &V, FieldPtrs<T> fo, FieldPtrsW<T> fn,
+                      const StageTimes &S, T dt, int *err) {
+    switch (pr_.integrator) {
+      case RK4: k_sl_subcycle<T, T, RK4_, INTERP_LINEAR, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
+      case RK3: k_sl_subcycle<T, T, RK3_, INTERP_LINEAR, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
+      case RK2: k_sl_subcycle<T, T, RK2_, INTERP_LINEAR, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
+      case TRAPEZOIDAL: k_sl_subcycle<T, T, TRAPEZOIDAL_, INTERP_LINEAR, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
+      default: k_sl_subcycle<T, T, EULER_, INTERP_LINEAR, F><<<grd, blk, 0, stream_>>>(dg_, sa, V, fo, fn, S, dt, err); break;
+    }
+  }
+  template <bool F>
+  void tangent_linear(dim3 grd, dim3 blk, const VelFields<T> &V, const VelFields<T> &D, FieldPtrs<T> fo, FieldPtrs<T> dfo,
+                      FieldPtrsW<T> dfn, const StageTimes &S, T dt, int *err) {
+    switch (pr_.integrator) {
+      case RK4: k_sl_tangent<T, RK4, F><<<grd, blk, 0, stream_>>>(dg_, V, D, fo, dfo, dfn, S, dt, err); break;
+      case RK3: k_sl_tangent<T, RK3, F><<<grd, blk, 0, stream_>>>(dg_, V, D, fo, dfo, dfn, S, dt, err); break;
+      case RK2: k_sl_tangent<T, RK2, F><<<grd, blk, 0, stream_>>>(dg_, V, D, fo, dfo, dfn, S, dt, err); break;
+      default: k_sl_tangent<T, EULER, F><<<grd, blk, 0, stream_>>>(dg_, V, D, fo, dfo, dfn, S, dt, err); break;
+    }
+  }
+  template <bool F>
+  void adjoint_linear(const VelFields<T> &V, FieldPtrs<T> fo, FieldPtrs<T> fbn, FieldPtrsW<T> fbo, FieldPtrsW<T> A1, FieldPtrsW<T> A2,
+                      FieldPtrsW<T> A3, const StageTimes &S, T dt) {
+    const dim3 grd = node_grid(), blk(32, 8, 1);
+    switch (pr_.integrator) {
+      case RK4: k_sl_adjoint<T, RK4, F><<<grd, blk, 0, stream_>>>(dg_, V, fo, fbn, fbo, A1, A2, A3, S, dt); break;
+      case RK3: k_sl_adjoint<T, RK3, F><<<grd, blk, 0, stream_>>>(dg_, V, fo, fbn, fbo, A1, A2, A3, S, dt); break;
+      case RK2: k_sl_adjoint<T, RK2, F><<<grd, blk, 0, stream_>>>(dg_, V, fo, fbn, fbo, A1, A2, A3, S, dt); break;
+      default: k_sl_adjoint<T, EULER, F><<<grd, blk, 0, stream_>>>(dg_, V, fo, fbn, fbo, A1, A2, A3, S, dt); break;
+    }
+  }
+  // the adjoint of a ghost fill: periodic images only, or every boundary rule (KIND: the flow map's
+  // or the velocity's)
+  template <int KIND>
+  void fold(FieldPtrsW<T> f) {
+    const unsigned nb = (unsigned)((ntot_ + 255) / 256);
+    if (!flags_) {
+      k_fold_ghosts<T><<<nb, 256, 0, stream_>>>(dg_, f, ntot_);
+      return;
+    }
+    k_fold_copy<T, KIND><<<nb, 256, 0, stream_>>>(dg_, f, ntot_);
+    k_fold_zero<T, KIND><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, f);
+    k_fold_image<T, KIND><<<nb, 256, 0, stream_>>>(dg_, f, ntot_);
   }
 
   // one CUBIC subcycle of update l from buf[cur] into buf[cur ^ 1] (and the tangent map along)
@@ -1391,10 +1821,14 @@ class Adjoint {
       cp.f[c] = Cl_[3 * l + c];
     }
     // stage blends of the two levels' coefficients, as the library's k_blend forms them
-    const int nst = pr_.integrator == RK3 ? 3 : (pr_.integrator == RK2 ? 2 : 1);
+    const int nst = pr_.integrator == RK4 ? 4 : (pr_.integrator == RK3 ? 3 : (pr_.integrator == RK2 ? 2 : 1));
     BlendOut<T> o{};
     int nout = 0;
     for (int st = 1; st < nst; st++) {
+      if (pr_.integrator == RK4 && st == 2) {  // the second half-step stage: the first's time, its blend
+        for (int c = 0; c < 3; c++) V.cs[2][c] = blend_[1][c];
+        continue;
+      }
       const T ct = (T)S.ct[st];
       for (int c = 0; c < 3; c++) {
         o.f[nout][c] = blend_[st][c];
@@ -1429,14 +1863,17 @@ class Adjoint {
         dfn.f[c] = dfm_[cur ^ 1][c];
       }
       const dim3 g4 = node_grid4(), b4(32, 4, 1);
-      if (pr_.integrator == RK3) k_sl_tangent_cubic<T, RK3><<<g4, b4, 0, stream_>>>(dg_, sa_, V, D, cn, cp, dcn, dcp, fo, dcf, dfn, S, dt);
+      if (pr_.integrator == RK4) k_sl_tangent_cubic<T, RK4><<<g4, b4, 0, stream_>>>(dg_, sa_, V, D, cn, cp, dcn, dcp, fo, dcf, dfn, S, dt);
+      else if (pr_.integrator == RK3) k_sl_tangent_cubic<T, RK3><<<g4, b4, 0, stream_>>>(dg_, sa_, V, D, cn, cp, dcn, dcp, fo, dcf, dfn, S, dt);
       else if (pr_.integrator == RK2) k_sl_tangent_cubic<T, RK2><<<g4, b4, 0, stream_>>>(dg_, sa_, V, D, cn, cp, dcn, dcp, fo, dcf, dfn, S, dt);
       else k_sl_tangent_cubic<T, EULER><<<g4, b4, 0, stream_>>>(dg_, sa_, V, D, cn, cp, dcn, dcp, fo, dcf, dfn, S, dt);
       k_periodic_ghosts<T><<<(unsigned)((ntot_ + 255) / 256), 256, 0, stream_>>>(dg_, dfn, ntot_);
     }
     int *err = &red_dev_->err;
     const dim3 grd = node_grid(), blk(32, 8, 1);
-    if (pr_.integrator == RK3)
+    if (pr_.integrator == RK4)
+      k_sl_subcycle<T, T, RK4_, INTERP_SPLINE4, false><<<grd, blk, 0, stream_>>>(dg_, sa_, V, fo, fn, S, dt, err);
+    else if (pr_.integrator == RK3)
       k_sl_subcycle<T, T, RK3_, INTERP_SPLINE4, false><<<grd, blk, 0, stream_>>>(dg_, sa_, V, fo, fn, S, dt, err);
     else if (pr_.integrator == RK2)
       k_sl_subcycle<T, T, RK2_, INTERP_SPLINE4, false><<<grd, blk, 0, stream_>>>(dg_, sa_, V, fo, fn, S, dt, err);
@@ -1474,11 +1911,12 @@ class Adjoint {
     {
       T *a[3], *b[3], *e[3];
       if (!field3(a, msg) || !field3(b, msg)) return false;
-      if (pr_.integrator == RK3 && !field3(e, msg)) return false;
+      const bool three = pr_.integrator == RK3 || pr_.integrator == RK4;
+      if (three && !field3(e, msg)) return false;
       for (int c = 0; c < 3; c++) {
         A1.f[c] = a[c];
         A2.f[c] = b[c];
-        A3.f[c] = pr_.integrator == RK3 ? e[c] : nullptr;
+        A3.f[c] = three ? e[c] : nullptr;
       }
     }
     // flow maps before every subcycle of the largest segment
@@ -1525,7 +1963,7 @@ class Adjoint {
           // the new map's ghosts were copies of its interior
           FieldPtrsW<T> fw{};
           for (int c = 0; c < 3; c++) fw.f[c] = fbar[fb][c];
-          k_fold_ghosts<T><<<(unsigned)nb, 256, 0, stream_>>>(dg_, fw, ntot_);
+          fold<GHOST_FM>(fw);
           for (int c = 0; c < 3; c++) ACK(cudaMemsetAsync(fbar[fb ^ 1][c], 0, ntot_ * sizeof(T), stream_));
           FieldPtrs<T> fo{}, fbn{};
           FieldPtrsW<T> fbo{};
@@ -1535,6 +1973,9 @@ class Adjoint {
             fbo.f[c] = fbar[fb ^ 1][c];
           }
           const StageTimes S = stage_times(t0, t1, lps[q], dt);
+          // the stage whose adjoint field a3 holds: the third (RK3) or the fourth (RK4); RK4's two
+          // half-step stages share ct[1] = ct[2] and a2
+          const int last = pr_.integrator == RK4 ? 3 : 2;
           if (cubic_) {
             fit3(&states[(size_t)3 * (first[l - l0] + q)], cfm_);
             FieldPtrs<T> cn{}, cp{}, cf{};
@@ -1547,7 +1988,9 @@ class Adjoint {
               cbp.f[c] = Cb_[3 * l + c];
             }
             const dim3 g4 = node_grid4(), b4(32, 4, 1);
-            if (pr_.integrator == RK3)
+            if (pr_.integrator == RK4)
+              k_sl_adjoint_cubic<T, RK4><<<g4, b4, 0, stream_>>>(dg_, sa_, V, cn, cp, cf, fbn, fbo, A1, A2, A3, S, (T)dt);
+            else if (pr_.integrator == RK3)
               k_sl_adjoint_cubic<T, RK3><<<g4, b4, 0, stream_>>>(dg_, sa_, V, cn, cp, cf, fbn, fbo, A1, A2, A3, S, (T)dt);
             else if (pr_.integrator == RK2)
               k_sl_adjoint_cubic<T, RK2><<<g4, b4, 0, stream_>>>(dg_, sa_, V, cn, cp, cf, fbn, fbo, A1, A2, A3, S, (T)dt);
@@ -1555,9 +1998,9 @@ class Adjoint {
               k_sl_adjoint_cubic<T, EULER><<<g4, b4, 0, stream_>>>(dg_, sa_, V, cn, cp, cf, fbn, fbo, A1, A2, A3, S, (T)dt);
             // the previous map's adjoint was scattered in coefficient space: through the fit
             fitT3(fbar[fb ^ 1]);
-            if (pr_.integrator == RK3)
+            if (pr_.integrator == RK3 || pr_.integrator == RK4)
               k_distribute_cubic<T, true><<<dim3((unsigned)nb, 3), 256, 0, stream_>>>(A1, A2, A3, ubn, ubp, cbn, cbp, (T)S.ct[0], (T)S.ct[1],
-                                                                                        (T)S.ct[2], ntot_);
+                                                                                        (T)S.ct[last], ntot_);
             else
               k_distribute_cubic<T, false><<<dim3((unsigned)nb, 3), 256, 0, stream_>>>(A1, A2, A3, ubn, ubp, cbn, cbp, (T)S.ct[0],
                                                                                          (T)S.ct[1], T(0), ntot_);
@@ -1565,14 +2008,10 @@ class Adjoint {
             fb ^= 1;
             continue;
           }
-          if (pr_.integrator == RK3)
-            k_sl_adjoint<T, RK3><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, V, fo, fbn, fbo, A1, A2, A3, S, (T)dt);
-          else if (pr_.integrator == RK2)
-            k_sl_adjoint<T, RK2><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, V, fo, fbn, fbo, A1, A2, A3, S, (T)dt);
-          else
-            k_sl_adjoint<T, EULER><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, V, fo, fbn, fbo, A1, A2, A3, S, (T)dt);
-          if (pr_.integrator == RK3)
-            k_distribute<T, true><<<dim3((unsigned)nb, 3), 256, 0, stream_>>>(A1, A2, A3, ubn, ubp, (T)S.ct[0], (T)S.ct[1], (T)S.ct[2],
+          if (flags_) adjoint_linear<true>(V, fo, fbn, fbo, A1, A2, A3, S, (T)dt);
+          else adjoint_linear<false>(V, fo, fbn, fbo, A1, A2, A3, S, (T)dt);
+          if (pr_.integrator == RK3 || pr_.integrator == RK4)
+            k_distribute<T, true><<<dim3((unsigned)nb, 3), 256, 0, stream_>>>(A1, A2, A3, ubn, ubp, (T)S.ct[0], (T)S.ct[1], (T)S.ct[last],
                                                                              ntot_);
           else
             k_distribute<T, false><<<dim3((unsigned)nb, 3), 256, 0, stream_>>>(A1, A2, A3, ubn, ubp, (T)S.ct[0], (T)S.ct[1], T(0),
@@ -1597,7 +2036,7 @@ class Adjoint {
         for (int c = 0; c < 3; c++) cb.f[c] = Cb_[3 * l + c];
         k_add3<T><<<dim3((unsigned)nb, 3), 256, 0, stream_>>>(f, cb, ntot_);
       }
-      k_fold_ghosts<T><<<(unsigned)nb, 256, 0, stream_>>>(dg_, f, ntot_);
+      fold<GHOST_VEL>(f);
       k_grad_out<T><<<node_grid(), dim3(32, 8, 1), 0, stream_>>>(dg_, fr, pr_.gu[l], pr_.gv[l], pr_.gw[l]);
       ACK(cudaGetLastError());
     }
@@ -1608,10 +2047,11 @@ class Adjoint {
   // CUBIC: spline axes, transposed pull tables, coefficient levels (and their adjoints and
   // tangents), the stage blends and the previous map's coefficients of one subcycle
   bool cubic_ = false;
+  bool flags_ = false;  // boundary flags (walls, slip, inflow / outflow, masks, 2-D)
   SplineAxes<T> sa_{};
   T *ptr_[3] = {nullptr, nullptr, nullptr};
   std::vector<T *> Cl_, Cb_, DC_;
-  T *blend_[3][3] = {};
+  T *blend_[4][3] = {};
   T *cfm_[3] = {nullptr, nullptr, nullptr};
   T *dcfm_[3] = {nullptr, nullptr, nullptr};
 

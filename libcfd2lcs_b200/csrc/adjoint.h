@@ -11,7 +11,7 @@ namespace cfd2lcs {
 struct AdjointProblem {
   const int *n;                      // grid points per direction
   const lcsdata_t *x, *y, *z;        // coordinates (as cfd2lcs_init), i fastest
-  int integrator;                    // EULER, TRAPEZOIDAL, RK2 or RK3
+  int integrator;                    // EULER, TRAPEZOIDAL, RK2, RK3 or RK4
   double cfl;                        // CFL number of the subcycling (cfd2lcs_set_param "CFL")
   int nlevels;                       // velocity levels, >= 2
   const lcsdata_t *const *u, *const *v, *const *w;  // device pointers, one per level, n[0]n[1]n[2] each
@@ -24,6 +24,7 @@ struct AdjointProblem {
   const lcsdata_t *const *du = nullptr, *const *dv = nullptr, *const *dw = nullptr;
   double *dJ = nullptr;
   int interpolator = 1;              // LINEAR (1) or CUBIC (3)
+  const int *flag = nullptr;         // boundary flags as cfd2lcs_init takes them (null: all LCS_INTERNAL)
 };
 
 // Runs the backward flow map over all levels (LINEAR or CUBIC interpolation), the FTLE of the final

@@ -646,7 +646,8 @@ CFD2LCS_EXPORT void cfd2lcs_batch_reset_c(void) {
 // ----------------------------------------------------------------------- adjoint
 // Gradient of J = sum weight * FTLE (backward FTLE of the whole horizon) with respect to the
 // velocity at every level; see include/cfd2lcs_b200.h.  Returns 0, or 1 with msg.
-CFD2LCS_EXPORT int cfd2lcs_adjoint_ftle_interp_c(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, int integrator,
+CFD2LCS_EXPORT int cfd2lcs_adjoint_ftle_interp_c(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, const int *flag,
+                                                 int integrator,
                                                  int interpolator, lcsdata_t cfl, int nlevels, const lcsdata_t *const *d_u,
                                                  const lcsdata_t *const *d_v, const lcsdata_t *const *d_w, const lcsdata_t *times,
                                                  const lcsdata_t *d_weight, int checkpoint_every, double *J, lcsdata_t *const *d_gu,
@@ -654,6 +655,7 @@ CFD2LCS_EXPORT int cfd2lcs_adjoint_ftle_interp_c(const int n[3], const lcsdata_t
   cfd2lcs::AdjointProblem p{n, x, y, z, integrator, (double)cfl, nlevels, d_u, d_v, d_w, times, d_weight, checkpoint_every,
                             d_gu, d_gv, d_gw};
   p.interpolator = interpolator;
+  p.flag = flag;
   std::string m;
   const bool ok = cfd2lcs::adjoint_ftle(p, J, m);
   if (msg && len > 0) {
@@ -669,13 +671,14 @@ CFD2LCS_EXPORT int cfd2lcs_adjoint_ftle_c(const int n[3], const lcsdata_t *x, co
                                           const lcsdata_t *const *d_w, const lcsdata_t *times, const lcsdata_t *d_weight,
                                           int checkpoint_every, double *J, lcsdata_t *const *d_gu, lcsdata_t *const *d_gv,
                                           lcsdata_t *const *d_gw, char *msg, size_t len) {
-  return cfd2lcs_adjoint_ftle_interp_c(n, x, y, z, integrator, LINEAR, cfl, nlevels, d_u, d_v, d_w, times, d_weight, checkpoint_every, J,
+  return cfd2lcs_adjoint_ftle_interp_c(n, x, y, z, nullptr, integrator, LINEAR, cfl, nlevels, d_u, d_v, d_w, times, d_weight, checkpoint_every, J,
                                        d_gu, d_gv, d_gw, msg, len);
 }
 
 // Tangent-linear check of the adjoint: J and dJ = <dJ/du, d> for one direction d, by a forward-
 // mode sweep alongside the flow map; see include/cfd2lcs_b200.h.  Returns 0, or 1 with msg.
-CFD2LCS_EXPORT int cfd2lcs_tangent_ftle_interp_c(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, int integrator,
+CFD2LCS_EXPORT int cfd2lcs_tangent_ftle_interp_c(const int n[3], const lcsdata_t *x, const lcsdata_t *y, const lcsdata_t *z, const int *flag,
+                                                 int integrator,
                                                  int interpolator, lcsdata_t cfl, int nlevels, const lcsdata_t *const *d_u,
                                                  const lcsdata_t *const *d_v, const lcsdata_t *const *d_w, const lcsdata_t *times,
                                                  const lcsdata_t *d_weight, const lcsdata_t *const *d_du, const lcsdata_t *const *d_dv,
@@ -690,6 +693,7 @@ CFD2LCS_EXPORT int cfd2lcs_tangent_ftle_interp_c(const int n[3], const lcsdata_t
     p.dw = d_dw;
     p.dJ = dJ;
     p.interpolator = interpolator;
+    p.flag = flag;
     ok = cfd2lcs::adjoint_ftle(p, J, m);
   }
   if (msg && len > 0) {
@@ -705,6 +709,6 @@ CFD2LCS_EXPORT int cfd2lcs_tangent_ftle_c(const int n[3], const lcsdata_t *x, co
                                           const lcsdata_t *const *d_w, const lcsdata_t *times, const lcsdata_t *d_weight,
                                           const lcsdata_t *const *d_du, const lcsdata_t *const *d_dv, const lcsdata_t *const *d_dw,
                                           double *J, double *dJ, char *msg, size_t len) {
-  return cfd2lcs_tangent_ftle_interp_c(n, x, y, z, integrator, LINEAR, cfl, nlevels, d_u, d_v, d_w, times, d_weight, d_du, d_dv, d_dw, J,
+  return cfd2lcs_tangent_ftle_interp_c(n, x, y, z, nullptr, integrator, LINEAR, cfl, nlevels, d_u, d_v, d_w, times, d_weight, d_du, d_dv, d_dw, J,
                                        dJ, msg, len);
 }
