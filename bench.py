@@ -476,7 +476,10 @@ def hot_kernel_rooflines(r, w, precision, hbm, fp64_peak, hbm_src=None):
     # the kernels that ran in the timed region (staged, gathering, or both while the tuner sampled)
     def kname(staged, n, st, ga):
         return st if staged == n else (ga if staged == 0 else st + "+" + ga)
-    stl = "k_sl_tile_lin" if w["interpolator"] == 1 else "k_sl_tile"
+    stl = "k_sl_tile"
+    if w["interpolator"] == 1:
+        # the staged LINEAR kernel: planes marching along z where the fields have tensor maps
+        stl = "k_sl_march_lin" if r["staged"].get("sl_march", 0) == r["staged"]["sl"] > 0 else "k_sl_tile_lin"
     if nsl > 0:
         cands.append((kname(r["staged"]["sl"], nsl, stl, "k_sl_subcycle"), k1["sl_ms"] - k0["sl_ms"], nsl,
                       sl_bytes_per_point(s_bytes, w["interpolator"], w["integrator"], v_bytes)))

@@ -93,6 +93,10 @@ void cfd2lcs_get_kernel_times_c(double t[2], long long n[2]);
  * n[1] forward particle.  The rest of those launches gathered their taps from global memory. */
 void cfd2lcs_get_staged_launches_c(long long n[2]);
 
+/* Of the staged backward launches, those of the LINEAR kernel that marches planes of the
+ * fields along z (FP64 grids whose rows are a multiple of 16 bytes), cumulative. */
+void cfd2lcs_get_march_launches_c(long long *n);
+
 /* The library times both forms of the cubic / LINEAR subcycle kernels -- taps staged in shared
  * memory or gathered from global memory, which give the same bits -- on an instance's first
  * launches and keeps the faster (environment CFD2LCS_B200_SL_TILE at cfd2lcs_init: 0 gathering

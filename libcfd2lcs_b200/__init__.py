@@ -36,7 +36,7 @@ EXPORTED_SYMBOLS = [
     # extensions (include/cfd2lcs_b200.h)
     "cfd2lcs_finalize_c", "cfd2lcs_get_error_c", "cfd2lcs_reset_c", "cfd2lcs_get_ftle_c", "cfd2lcs_get_flowmap_c",
     "cfd2lcs_update_device_c", "cfd2lcs_ftle_device_ptr_c", "cfd2lcs_get_counters_c", "cfd2lcs_get_phase_times_c",
-    "cfd2lcs_get_kernel_times_c", "cfd2lcs_get_staged_launches_c", "cfd2lcs_get_tuning_c", "cfd2lcs_reconstruct_noalloc_c", "cfd2lcs_get_invariants_c",
+    "cfd2lcs_get_kernel_times_c", "cfd2lcs_get_staged_launches_c", "cfd2lcs_get_march_launches_c", "cfd2lcs_get_tuning_c", "cfd2lcs_reconstruct_noalloc_c", "cfd2lcs_get_invariants_c",
     "cfd2lcs_tracer_count_c", "cfd2lcs_get_tracers_c", "cfd2lcs_diagnostic_size_c",
     # batched form (include/cfd2lcs_b200.h)
     "cfd2lcs_batch_add_c", "cfd2lcs_batch_diagnostic_init_c", "cfd2lcs_batch_update_device_c", "cfd2lcs_batch_get_ftle_c",
@@ -105,6 +105,7 @@ def load(precision: str = "dp") -> C.CDLL:
     lib.cfd2lcs_get_phase_times_c.argtypes = [P]
     lib.cfd2lcs_get_kernel_times_c.argtypes = [P, P]
     lib.cfd2lcs_get_staged_launches_c.argtypes = [P]
+    lib.cfd2lcs_get_march_launches_c.argtypes = [P]
     lib.cfd2lcs_get_tuning_c.argtypes = [P, P]
     lib.cfd2lcs_reconstruct_noalloc_c.argtypes = [C.c_int, P, P]
     lib.cfd2lcs_reconstruct_noalloc_c.restype = C.c_int
@@ -271,7 +272,9 @@ class Cfd2lcs:
         """Launches of the subcycle kernels that staged their spline taps in shared memory."""
         n = np.zeros(2, dtype=np.int64)
         self.lib.cfd2lcs_get_staged_launches_c(self._p(n))
-        return {"sl": int(n[0]), "fwd": int(n[1])}
+        m = np.zeros(1, dtype=np.int64)
+        self.lib.cfd2lcs_get_march_launches_c(self._p(m))
+        return {"sl": int(n[0]), "fwd": int(n[1]), "sl_march": int(m[0])}
 
     def tuning(self) -> dict:
         """The staged-versus-gathering choice of the backward and forward subcycle kernels (-1

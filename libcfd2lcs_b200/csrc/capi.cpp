@@ -425,6 +425,14 @@ CFD2LCS_EXPORT void cfd2lcs_get_staged_launches_c(long long n[2]) {
   n[1] = k.fwd_staged_launches;
 }
 
+// Of the staged backward launches, those of the LINEAR kernel that marches planes along z
+// (cumulative).
+CFD2LCS_EXPORT void cfd2lcs_get_march_launches_c(long long *n) {
+  Library &lib = L();
+  const Counters &k = lib.eng ? lib.eng->counters() : lib.zero;
+  *n = k.sl_march_launches;
+}
+
 // The engine's choice between staged and gathering subcycle kernels: choice[f] for the backward
 // (f = 0) and forward (f = 1) kernel, -1 while sampling or where staging does not apply, 0
 // gathering, 1 staged; ms[2f], ms[2f+1] the mean launch times measured for the two.

@@ -45,6 +45,8 @@ struct Counters {
   long long sl_kernel_launches = 0, fwd_kernel_launches = 0;
   // launches of the kernels that stage their spline taps in shared memory (backward, forward)
   long long sl_staged_launches = 0, fwd_staged_launches = 0;
+  // of the staged backward launches, those of the LINEAR kernel that marches planes along z
+  long long sl_march_launches = 0;
   // ingest, bkwd advect, fwd advect, snapshot, compose, ftle, whole update (event span)
   double phase_ms[7] = {0, 0, 0, 0, 0, 0, 0};
 };

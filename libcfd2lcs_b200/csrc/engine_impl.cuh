@@ -227,6 +227,7 @@ class Engine : public EngineBase {
       return false;
     }
     CK(cudaGetDevice(&dev_));  // the device this engine's stream and buffers live on
+    CK(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev_));
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     for (int e = 0; e < 10; e++) {
       cudaEvent_t ev;
@@ -240,6 +241,8 @@ class Engine : public EngineBase {
     if (const char *e = std::getenv("CFD2LCS_B200_COMPOSE_SORT_EVERY")) compose_sort_every_ = std::max(1, std::atoi(e));
     if (const char *e = std::getenv("CFD2LCS_B200_COMPOSE_MINB")) compose_minb_ = std::atoi(e) >= 4 ? 4 : 2;
     if (const char *e = std::getenv("CFD2LCS_B200_SL_TILE")) tile_mode_ = std::max(0, std::min(2, std::atoi(e)));
+    if (const char *e = std::getenv("CFD2LCS_B200_SL_MARCH")) sl_march_ = std::atoi(e) != 0;
+    if (const char *e = std::getenv("CFD2LCS_B200_SL_MARCH_KC")) sl_march_kc_ = std::max(0, std::atoi(e));
     for (int a = 0; a < 3; a++) n_[a] = n[a];
     // coordinate lines (and, on a non-rectilinear grid, the node coordinates) and interior flags
     // for the output files
@@ -1714,8 +1717,44 @@ class Engine : public EngineBase {
     return true;
   }
 
+  // The staged LINEAR backward kernel: k_sl_march_lin (planes marching along z) where every
+  // field has a tensor map and the velocity is stored in the flow map's type, else the boxes of
+  // k_sl_tile_lin.  CFD2LCS_B200_SL_MARCH=0 at cfd2lcs_init keeps the boxes;
+  // CFD2LCS_B200_SL_MARCH_KC sets the planes per column run (default: runs of 8..64 planes
+  // giving about eight waves of two blocks per SM).
+  bool sl_march_ = true;
+  int sl_march_kc_ = 0;
+  int num_sms_ = 148;
+
+  template <int IG, bool F>
+  bool launch_sl_march_lin(const VelFields<TV> &V, FieldPtrs<T> fo, FieldPtrsW<T> fn, StageTimes S, T dt) {
+    if constexpr (!std::is_same<T, TV>::value) {
+      return false;
+    } else {
+      // a box row (SLM_SX elements) must be a multiple of 16 bytes: FP64 only
+      if (!sl_march_ || (SLM_SX * sizeof(T)) % 16) return false;
+      TileMaps tm{};
+      for (int c = 0; c < 3; c++)
+        if (!tensor_map<T>(V.un[c], SLM_SX, SLM_SY, 1, tm.m[c]) || !tensor_map<T>(V.unp1[c], SLM_SX, SLM_SY, 1, tm.m[3 + c]) ||
+            !tensor_map<T>(fo.f[c], SLM_SX, SLM_SY, 1, tm.m[6 + c]))
+          return false;
+      tm.on = 1;
+      const long cols = (long)((n_[0] + SLM_X - 1) / SLM_X) * ((n_[1] + SLM_Y - 1) / SLM_Y);
+      int kc = sl_march_kc_;
+      if (kc <= 0) kc = (int)std::max(8L, std::min(64L, (long)n_[2] * cols / (8L * 2 * num_sms_)));
+      kc = std::min(kc, n_[2]);
+      const size_t smem = slm_bytes<T>() + 128;
+      cudaFuncSetAttribute(k_sl_march_lin<T, IG, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      const dim3 blk(SLM_X, SLM_Y, 1), grd((n_[0] + SLM_X - 1) / SLM_X, (n_[1] + SLM_Y - 1) / SLM_Y, (n_[2] + kc - 1) / kc);
+      k_sl_march_lin<T, IG, F><<<grd, blk, smem, stream_>>>(dg_, fn, S, dt, kc, &red_->err, tm);
+      counters_.sl_march_launches++;
+      return true;
+    }
+  }
+
   template <int IG, bool F>
   void launch_sl_tile_lin(const VelFields<TV> &V, FieldPtrs<T> fo, FieldPtrsW<T> fn, StageTimes S, T dt) {
+    if (launch_sl_march_lin<IG, F>(V, fo, fn, S, dt)) return;
     const size_t smem = sll_bytes<T, TV>() + 128;
     cudaFuncSetAttribute(k_sl_tile_lin<T, TV, IG, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const dim3 blk(32, LinGeom::TY, 2),

@@ -467,6 +467,132 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLT_MINB)
 // so the results are bitwise equal.  The gathering kernel is latency-bound (three dependent
 // gather phases per point); here the only global reads are the bulk copies.
 // ---------------------------------------------------------------------------------------
+// One node (i, j, k) of the LINEAR backward subcycle from staged taps: integrate_lp
+// (src/lp_motion_m.f90:129-360) with the stage placement of integrate<>, the first stage on the
+// node (sample_velocity_node), the trilinear samples of interp_s2u_r1 LINEAR
+// (src/lp_tracking_m.f90:342-474) around the node from its interpolation lines lm, lc, lp at
+// no-1, no, no+1, then the previous flow map at the departure point, the boundary rules and the
+// ghost writes.  iv / ifm map a padded (x, y, z) to the staged index of a velocity / flow-map
+// component; u0 / u1 / fm (c, index) read component c of u_n, u_np1 and the flow map.  Every
+// staged LINEAR kernel runs this one expression, so they are bitwise equal to each other and to
+// k_sl_subcycle.
+template <typename T, typename TV, int INTEG, bool HAS_FLAGS, typename IV, typename IF, typename U0, typename U1, typename FM>
+__device__ __forceinline__ void lin_sl_node(const DevGrid<T> &g, const StageTimes &S, T dt, int i, int j, int k, const T xn[3], const T lm[3],
+                                            const T lc[3], const T lp[3], IV iv, IF ifm, U0 u0, U1 u1, FM fm, FieldPtrsW<T> fmn,
+                                            int *err) {
+  constexpr int NOFF = INTEG == RK2_ ? 1 : (INTEG == RK3_ ? 2 : (INTEG == RK4_ ? 3 : 0));
+  const T HALF = T(1) / T(2), THIRD = T(1) / T(3), TWOTHIRD = T(2) / T(3), SIXTH = T(1) / T(6), TWO = T(2);
+  const int sx = g.P.sx, sxy = g.P.sxy;
+  const int no[3] = {i, j, k};
+  auto vel_sample = [&](const T x[3], T ct_, T u[3]) {
+    const TV ct = TV(ct_), omc = TV(1) - ct;
+    LinStencil<T> st;
+    lin_stencil_node(lm, lc, lp, sx, sxy, x, no, st);
+    int idx[8];
+#pragma unroll
+    for (int c = 0; c < 8; c++)
+      idx[c] = iv(st.i0[0] + ((c & 1) ? st.d[0] : 0), st.i0[1] + ((c & 2) ? st.d[1] : 0), st.i0[2] + ((c & 4) ? st.d[2] : 0));
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      u[c] = T(lin_blend_contract<T, TV>(st, omc, ct, [&](int e) { return u0(c, idx[e]); }, [&](int e) { return u1(c, idx[e]); }));
+  };
+  T u[3], x[3];
+  {  // first stage on the node (sample_velocity_node)
+    const TV ct = TV(T(S.ct[0])), omc = TV(1) - ct;
+    const int pv = iv(i, j, k);
+#pragma unroll
+    for (int c = 0; c < 3; c++) u[c] = T(omc * u0(c, pv) + ct * u1(c, pv));
+  }
+  if (NOFF == 0) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) x[c] = xn[c] + dt * u[c];
+  } else if (NOFF == 1) {
+    T xh[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) xh[c] = xn[c] + HALF * dt * u[c];
+    vel_sample(xh, T(S.ct[1]), u);
+#pragma unroll
+    for (int c = 0; c < 3; c++) x[c] = xn[c] + dt * u[c];
+  } else if (NOFF == 2) {
+    T kk[3], xs[3], acc[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u[c];
+      acc[c] = xn[c] + SIXTH * kk[c];
+      xs[c] = xn[c] + HALF * kk[c];
+    }
+    vel_sample(xs, T(S.ct[1]), u);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u[c];
+      xs[c] = xn[c] + TWO * kk[c];
+      acc[c] = acc[c] + TWOTHIRD * kk[c];
+    }
+    vel_sample(xs, T(S.ct[2]), u);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u[c];
+      x[c] = acc[c] + SIXTH * kk[c];
+    }
+  } else {
+    T kk[3], xs[3], acc[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u[c];
+      acc[c] = xn[c] + SIXTH * kk[c];
+      xs[c] = xn[c] + HALF * kk[c];
+    }
+    vel_sample(xs, T(S.ct[1]), u);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u[c];
+      acc[c] = acc[c] + THIRD * kk[c];
+      xs[c] = xn[c] + HALF * kk[c];
+    }
+    vel_sample(xs, T(S.ct[2]), u);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u[c];
+      acc[c] = acc[c] + THIRD * kk[c];
+      xs[c] = xn[c] + kk[c];
+    }
+    vel_sample(xs, T(S.ct[3]), u);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      kk[c] = dt * u[c];
+      x[c] = acc[c] + SIXTH * kk[c];
+    }
+  }
+  int nb[3] = {i, j, k};
+  project_plane(g, nb, x);
+  if (particle_bc<T, HAS_FLAGS>(g, nb, x, err)) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) x[c] = xn[c];
+  }
+  // previous flow map at the departure point (sample_field LINEAR around the node)
+  LinStencil<T> st;
+  lin_stencil_node(lm, lc, lp, sx, sxy, x, no, st);
+  int idx[8];
+#pragma unroll
+  for (int c = 0; c < 8; c++)
+    idx[c] = ifm(st.i0[0] + ((c & 1) ? st.d[0] : 0), st.i0[1] + ((c & 2) ? st.d[1] : 0), st.i0[2] + ((c & 4) ? st.d[2] : 0));
+  T fmp[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) fmp[c] = lin_contract<T>(st, [&](int e) { return fm(c, idx[e]); });
+  const int p = pidx(sx, sxy, i, j, k);
+  const int fl = HAS_FLAGS ? (int)g.flag[p] : (int)LCS_INTERNAL;
+  const T mask = fl != LCS_MASK ? T(1) : T(0);
+  const bool zero = HAS_FLAGS && (fl == LCS_MASK || fl == LCS_INFLOW || fl == LCS_OUTFLOW);
+  T vpre[3], vfin[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    vpre[c] = (fmp[c] + (x[c] - xn[c])) * mask;
+    vfin[c] = zero ? T(0) : vpre[c];
+    fmn.f[c][p] = vfin[c];
+  }
+  write_ghosts<T, HAS_FLAGS, GHOST_FM>(g, fmn.f, i, j, k, vpre, vfin, err);
+}
+
 using LinGeom = TileGeom<32, 4, 4, 1>;
 
 // shared memory of the LINEAR tile: u_n, u_np1 (velocity type) and the flow map (3 each)
@@ -486,8 +612,6 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLL_MINB)
   extern __shared__ __align__(128) unsigned char sll_smem_raw[];
   unsigned char *const sll_smem = smem_aligned128(sll_smem_raw);
   __shared__ __align__(8) uint64_t bar;
-  constexpr int NOFF = INTEG == RK2_ ? 1 : (INTEG == RK3_ ? 2 : (INTEG == RK4_ ? 3 : 0));
-  const T HALF = T(1) / T(2), THIRD = T(1) / T(3), TWOTHIRD = T(2) / T(3), SIXTH = T(1) / T(6), TWO = T(2);
   const int tid = threadIdx.x + 32 * (threadIdx.y + LinGeom::TY * threadIdx.z);
   const int sx = g.P.sx, sxy = g.P.sxy;
   const TileBox b = tile_box<LinGeom>(g);
@@ -536,127 +660,112 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLL_MINB)
       lp[q][a] = __ldg(g.li[a] + nd[a] + 1);
     }
   }
-  auto vel_sample = [&](const T x[3], const int no[3], T ct_, T u[3], int q) {
-    const TV ct = TV(ct_), omc = TV(1) - ct;
-    LinStencil<T> st;
-    lin_stencil_node(lm[q], lc[q], lp[q], sx, sxy, x, no, st);
-    int idx[8];
-#pragma unroll
-    for (int c = 0; c < 8; c++)
-      idx[c] = tile_index<LinGeom, TV>(b, sx, sxy, st.i0[0] + ((c & 1) ? st.d[0] : 0), st.i0[1] + ((c & 2) ? st.d[1] : 0),
-                                       st.i0[2] + ((c & 4) ? st.d[2] : 0));
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      const TV *a = su0 + (size_t)c * LinGeom::comp<TV>(), *bb = su1 + (size_t)c * LinGeom::comp<TV>();
-      u[c] = T(lin_blend_contract<T, TV>(st, omc, ct, [&](int e) { return a[idx[e]]; }, [&](int e) { return bb[idx[e]]; }));
-    }
-  };
 #pragma unroll
   for (int q = 0; q < 2; q++) {
     if (!ok[q]) continue;
-    const int k = kq[q];
-    const int no[3] = {i, j, k};
-    T u[3], x[3];
-    {  // first stage on the node (sample_velocity_node)
-      const TV ct = TV(T(S.ct[0])), omc = TV(1) - ct;
-      const int pv = tile_index<LinGeom, TV>(b, sx, sxy, i, j, k);
+    lin_sl_node<T, TV, INTEG, HAS_FLAGS>(
+        g, S, dt, i, j, kq[q], xn[q], lm[q], lc[q], lp[q],
+        [&](int x, int y, int z) { return tile_index<LinGeom, TV>(b, sx, sxy, x, y, z); },
+        [&](int x, int y, int z) { return tile_index<LinGeom, T>(b, sx, sxy, x, y, z); },
+        [&](int c, int e) { return su0[(size_t)c * LinGeom::comp<TV>() + e]; },
+        [&](int c, int e) { return su1[(size_t)c * LinGeom::comp<TV>() + e]; },
+        [&](int c, int e) { return sf[(size_t)c * LinGeom::comp<T>() + e]; }, fmn, err);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// LINEAR backward subcycle marching along z (FP64 with tensor maps).  A block owns a column of
+// 32 x 8 nodes over a run of kc planes and keeps a ring of four staged planes of all nine
+// components (u_n, u_np1, flow map; each plane 34 x 10 with its 1-node halo): while it works on
+// plane k from planes k-1, k and k+1, the copy of plane k+2 lands in the slot plane k-2 left.
+// Against the 32 x 4 x 4 boxes of k_sl_tile_lin (34 x 6 x 6 staged per 512 nodes, 2.4 staged
+// elements per node) a plane is staged once per column run, 1.33 elements per node in x and y,
+// plus two planes per run in z, and the block never waits for its copies but at the start of a
+// run.  Every copy lands on the mbarrier of its slot (one phase per plane that passes through
+// it); every wait is bounded.
+// ---------------------------------------------------------------------------------------
+constexpr int SLM_X = 32, SLM_Y = 8, SLM_SX = SLM_X + 2, SLM_SY = SLM_Y + 2, SLM_SLOTS = 4;
+constexpr int SLM_THREADS = SLM_X * SLM_Y;
+// elements of one staged component plane, padded so that every copy lands 128-byte aligned
+template <typename T>
+__host__ __device__ constexpr int slm_comp() {
+  return ((SLM_SX * SLM_SY * (int)sizeof(T) + 127) / 128) * 128 / (int)sizeof(T);
+}
+template <typename T>
+__host__ __device__ constexpr size_t slm_bytes() {
+  return (size_t)SLM_SLOTS * 9 * slm_comp<T>() * sizeof(T);
+}
+
+#ifndef CFD2LCS_SLM_MINB
+#define CFD2LCS_SLM_MINB 2
+#endif
+
+template <typename T, int INTEG, bool HAS_FLAGS>
+__global__ void __launch_bounds__(SLM_THREADS, CFD2LCS_SLM_MINB)
+    k_sl_march_lin(DevGrid<T> g, FieldPtrsW<T> fmn, StageTimes S, T dt, int kc, int *err, const __grid_constant__ TileMaps tm) {
+  extern __shared__ __align__(128) unsigned char slm_smem_raw[];
+  T *const box = reinterpret_cast<T *>(smem_aligned128(slm_smem_raw));
+  __shared__ __align__(8) uint64_t bar[SLM_SLOTS];
+  constexpr int CS = slm_comp<T>();
+  constexpr unsigned PLANE_BYTES = 9u * (unsigned)(SLM_SX * SLM_SY * sizeof(T));
+  const int tid = threadIdx.x + SLM_X * threadIdx.y;
+  const int xs = (int)blockIdx.x * SLM_X, ys = (int)blockIdx.y * SLM_Y;  // padded origin of the staged planes
+  const int K0 = 1 + (int)blockIdx.z * kc, K1 = min(K0 + kc - 1, g.P.n[2]);
+  // plane p (K0-1 <= p <= K1+1) sits in slot p & 3; its phase on that slot's barrier is the
+  // parity of its pass through the ring
+  auto parity = [&](int p) { return (unsigned)(((p - (K0 - 1)) >> 2) & 1); };
+  auto issue = [&](int p) {
+    T *const dst = box + (size_t)(p & 3) * 9 * CS;
+    mbar_arrive_expect_tx(&bar[p & 3], PLANE_BYTES);
 #pragma unroll
-      for (int c = 0; c < 3; c++)
-        u[c] = T(omc * su0[(size_t)c * LinGeom::comp<TV>() + pv] + ct * su1[(size_t)c * LinGeom::comp<TV>() + pv]);
+    for (int c = 0; c < 9; c++) tensor_copy_3d(dst + (size_t)c * CS, tm.m + c, xs, ys, p, &bar[p & 3]);
+  };
+  if (tid == 0) {
+#pragma unroll
+    for (int s = 0; s < SLM_SLOTS; s++) mbar_init(&bar[s], 1);
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int p = K0 - 1; p <= min(K0 + 1, K1 + 1); p++) issue(p);
+
+  const int i = xs + 1 + (int)threadIdx.x, j = ys + 1 + (int)threadIdx.y;
+  const bool ok = i <= g.P.n[0] && j <= g.P.n[1];
+  // x and y stay fixed along the column: the node coordinates and the interpolation lines at
+  // no-1, no, no+1 of both axes are read once
+  const int ni = min(i, g.P.n[0]), nj = min(j, g.P.n[1]);
+  T xn[3], lm[3], lc[3], lp[3];
+  xn[0] = __ldg(g.lt[0] + min(i, g.P.n[0] + 1));
+  xn[1] = __ldg(g.lt[1] + min(j, g.P.n[1] + 1));
+  lm[0] = __ldg(g.li[0] + ni - 1), lc[0] = __ldg(g.li[0] + ni), lp[0] = __ldg(g.li[0] + ni + 1);
+  lm[1] = __ldg(g.li[1] + nj - 1), lc[1] = __ldg(g.li[1] + nj), lp[1] = __ldg(g.li[1] + nj + 1);
+  T zc = __ldg(g.li[2] + K0 - 1), zp = __ldg(g.li[2] + K0);
+  auto sidx = [&](int x, int y, int z) { return (z & 3) * 9 * CS + (y - ys) * SLM_SX + (x - xs); };
+  for (int k = K0; k <= K1; k++) {
+    bool w = mbar_wait_bounded(&bar[(k + 1) & 3], parity(k + 1));
+    if (k == K0) w = mbar_wait_bounded(&bar[(k - 1) & 3], parity(k - 1)) && mbar_wait_bounded(&bar[k & 3], parity(k)) && w;
+    // the barrier also ends every thread's reads of plane k-2, whose slot the next copy fills
+    if (!__syncthreads_and(w)) {
+      if (tid == 0) atomicOr(err, ERR_ASYNC_COPY);
+      // let the copies in flight land before the block leaves
+      for (int p = max(K0 - 1, k - 1); p <= min(k + 1, K1 + 1); p++) mbar_wait_bounded(&bar[p & 3], parity(p));
+      return;
     }
-    // integrate_lp (src/lp_motion_m.f90:129-360) with the stage placement of integrate<>
-    if (NOFF == 0) {
-#pragma unroll
-      for (int c = 0; c < 3; c++) x[c] = xn[q][c] + dt * u[c];
-    } else if (NOFF == 1) {
-      T xh[3];
-#pragma unroll
-      for (int c = 0; c < 3; c++) xh[c] = xn[q][c] + HALF * dt * u[c];
-      vel_sample(xh, no, T(S.ct[1]), u, q);
-#pragma unroll
-      for (int c = 0; c < 3; c++) x[c] = xn[q][c] + dt * u[c];
-    } else if (NOFF == 2) {
-      T kk[3], xs[3], acc[3];
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        kk[c] = dt * u[c];
-        acc[c] = xn[q][c] + SIXTH * kk[c];
-        xs[c] = xn[q][c] + HALF * kk[c];
-      }
-      vel_sample(xs, no, T(S.ct[1]), u, q);
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        kk[c] = dt * u[c];
-        xs[c] = xn[q][c] + TWO * kk[c];
-        acc[c] = acc[c] + TWOTHIRD * kk[c];
-      }
-      vel_sample(xs, no, T(S.ct[2]), u, q);
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        kk[c] = dt * u[c];
-        x[c] = acc[c] + SIXTH * kk[c];
-      }
-    } else {
-      T kk[3], xs[3], acc[3];
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        kk[c] = dt * u[c];
-        acc[c] = xn[q][c] + SIXTH * kk[c];
-        xs[c] = xn[q][c] + HALF * kk[c];
-      }
-      vel_sample(xs, no, T(S.ct[1]), u, q);
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        kk[c] = dt * u[c];
-        acc[c] = acc[c] + THIRD * kk[c];
-        xs[c] = xn[q][c] + HALF * kk[c];
-      }
-      vel_sample(xs, no, T(S.ct[2]), u, q);
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        kk[c] = dt * u[c];
-        acc[c] = acc[c] + THIRD * kk[c];
-        xs[c] = xn[q][c] + kk[c];
-      }
-      vel_sample(xs, no, T(S.ct[3]), u, q);
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        kk[c] = dt * u[c];
-        x[c] = acc[c] + SIXTH * kk[c];
-      }
+    if (tid == 0 && k + 2 <= K1 + 1) {
+      fence_proxy_async_smem();
+      issue(k + 2);
     }
-    int nb[3] = {i, j, k};
-    project_plane(g, nb, x);
-    if (particle_bc<T, HAS_FLAGS>(g, nb, x, err)) {
-#pragma unroll
-      for (int c = 0; c < 3; c++) x[c] = xn[q][c];
-    }
-    // previous flow map at the departure point (sample_field LINEAR around the node)
-    LinStencil<T> st;
-    lin_stencil_node(lm[q], lc[q], lp[q], sx, sxy, x, no, st);
-    int idx[8];
-#pragma unroll
-    for (int c = 0; c < 8; c++)
-      idx[c] = tile_index<LinGeom, T>(b, sx, sxy, st.i0[0] + ((c & 1) ? st.d[0] : 0), st.i0[1] + ((c & 2) ? st.d[1] : 0),
-                                      st.i0[2] + ((c & 4) ? st.d[2] : 0));
-    T fmp[3];
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      const T *f = sf + (size_t)c * LinGeom::comp<T>();
-      fmp[c] = lin_contract<T>(st, [&](int e) { return f[idx[e]]; });
-    }
-    const int p = pidx(sx, sxy, i, j, k);
-    const int fl = HAS_FLAGS ? (int)g.flag[p] : (int)LCS_INTERNAL;
-    const T mask = fl != LCS_MASK ? T(1) : T(0);
-    const bool zero = HAS_FLAGS && (fl == LCS_MASK || fl == LCS_INFLOW || fl == LCS_OUTFLOW);
-    T vpre[3], vfin[3];
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      vpre[c] = (fmp[c] + (x[c] - xn[q][c])) * mask;
-      vfin[c] = zero ? T(0) : vpre[c];
-      fmn.f[c][p] = vfin[c];
-    }
-    write_ghosts<T, HAS_FLAGS, GHOST_FM>(g, fmn.f, i, j, k, vpre, vfin, err);
+    // z lines of this plane, rolled along the column
+    lm[2] = zc;
+    lc[2] = zp;
+    zc = zp;
+    zp = __ldg(g.li[2] + k + 1);
+    lp[2] = zp;
+    xn[2] = __ldg(g.lt[2] + k);
+    if (ok)
+      lin_sl_node<T, T, INTEG, HAS_FLAGS>(
+          g, S, dt, i, j, k, xn, lm, lc, lp, sidx, sidx, [&](int c, int e) { return box[(size_t)c * CS + e]; },
+          [&](int c, int e) { return box[(size_t)(3 + c) * CS + e]; }, [&](int c, int e) { return box[(size_t)(6 + c) * CS + e]; },
+          fmn, err);
   }
 }
 

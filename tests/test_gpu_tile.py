@@ -1,5 +1,6 @@
 """The subcycle kernels that stage their taps in shared memory -- backward cubic (k_sl_tile),
-backward LINEAR (k_sl_tile_lin) and forward cubic (k_fwd_tile, one block per 16 x 4 x 4-cell
+backward LINEAR (k_sl_march_lin, planes marching along z, where the fields have tensor maps;
+else k_sl_tile_lin) and forward cubic (k_fwd_tile, one block per 16 x 4 x 4-cell
 sort tile) -- against the gathering kernels they replace (k_sl_subcycle, k_fwd_subcycle,
 selected with CFD2LCS_B200_SL_TILE=0 at cfd2lcs_init): both contract the same taps in the same
 order, so flow maps and FTLE must be bitwise equal.  Grids of 38^3 leave partial tiles in x (38 = 32 + 6), y and z (38 = 9 x 4 + 2);
@@ -87,6 +88,34 @@ def test_staged_linear_unsteady_mixed_precision(gpu_dp):
 @pytest.mark.parametrize("case", ["mixed_bc", "turb", "channel"])
 def test_staged_linear_small_and_walled(gpu_dp, case):
     _same(gpu_dp, case, 2, interp=1)
+
+
+@pytest.mark.parametrize("kc", ["1", "3", "7", "64"])
+def test_staged_linear_march_runs(gpu_dp, kc):
+    """k_sl_march_lin with column runs of 1, 3, 7 and all planes (38 = 5 x 7 + 3 leaves a
+    partial run; a run of 1 plane issues no copy after its prologue): bitwise the gathering
+    kernel, and the marching kernel is the one that ran."""
+    env = {"CFD2LCS_B200_SL_MARCH_KC": kc}
+    _same(gpu_dp, "abc", 3, n=38, steps=10, interp=1, env=env)
+    _, _, _, sa = _run(gpu_dp, "abc", 3, True, n=38, steps=10, interp=1, env=env)
+    assert sa["sl_march"] == sa["sl"] > 0
+
+
+def test_staged_linear_boxes_without_march(gpu_dp):
+    """CFD2LCS_B200_SL_MARCH=0 keeps the 32 x 4 x 4 boxes of k_sl_tile_lin: the same bits."""
+    env = {"CFD2LCS_B200_SL_MARCH": "0"}
+    _same(gpu_dp, "abc", 2, n=38, steps=10, interp=1, env=env)
+    _, _, _, sa = _run(gpu_dp, "abc", 2, True, n=38, steps=10, interp=1, env=env)
+    assert sa["sl_march"] == 0 and sa["sl"] > 0
+
+
+def test_staged_linear_march_walled_channel(gpu_dp):
+    """A walled channel (10 x 8 x 6, rows of 12 FP64 values: tensor maps exist): the marching
+    kernel with boundary flags, runs of 4 planes."""
+    env = {"CFD2LCS_B200_SL_MARCH_KC": "4"}
+    _same(gpu_dp, "channel", 3, interp=1, env=env)
+    _, _, _, sa = _run(gpu_dp, "channel", 3, True, interp=1, env=env)
+    assert sa["sl_march"] == sa["sl"] > 0
 
 
 def test_staged_linear_single_precision(gpu_sp):
