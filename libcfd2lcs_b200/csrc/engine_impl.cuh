@@ -1609,8 +1609,9 @@ class Engine : public EngineBase {
   // sort tiles -- times each launch with the CUDA events that bracket it, and once each variant
   // has kTuneSamples launches keeps the one with the shorter launch for the rest of the engine's
   // life (per instance: the batched form tunes every instance for its own grid and options).
-  // Measured on B200, ABC 256^3 FP64 per launch: staged cubic backward 3.22 against 4.63 ms,
-  // staged forward 8.39 against 6.68 ms, staged LINEAR backward 0.79 against 0.90 ms.
+  // Measured on B200, ABC 256^3 FP64 per launch: staged cubic backward 3.14 against 4.44 ms,
+  // staged forward 5.93 against 4.88 ms (first launches), staged LINEAR backward (the z-marching
+  // kernel) 0.55 against 0.84 ms.
   // CFD2LCS_B200_SL_TILE at cfd2lcs_init: 0 = gathering kernels only, 1 = tuned (default),
   // 2 = staged kernels wherever they apply.  cfd2lcs_get_tuning_c reports the choices.
   // Each variant's first launch is dropped and the rest compared by their minimum: a launch whose
