@@ -110,6 +110,10 @@ struct Diag {
   int *pcnt = nullptr, *poffs = nullptr, *ptsum = nullptr;
   SortTiles sort_geom{};  // cell tiles of the last sort (the staged forward kernel reads one tile per block)
   int fwd_variant = 0;    // forward kernel until the next sort: 0 gathering, 1 staged
+  long since_sort = 1L << 40;  // forward subcycles since the particles were last sorted (or reset)
+  // event-timed cost of the last sort, launch time right after it, and the launch time lost
+  // since then (gathering forward kernels: the re-sort schedule of sort_due)
+  double sort_ms = 0, base_ms = -1, excess_ms = 0;
   // ring of sub-flow maps (padded) and their spline coefficients
   std::vector<T *> slot;      // 3 per slot
   std::vector<T *> slotcoef;  // 3 per slot (allocated on first spline use)
@@ -242,6 +246,7 @@ class Engine : public EngineBase {
     if (const char *e = std::getenv("CFD2LCS_B200_COMPOSE_MINB")) compose_minb_ = std::atoi(e) >= 4 ? 4 : 2;
     if (const char *e = std::getenv("CFD2LCS_B200_SL_TILE")) tile_mode_ = std::max(0, std::min(2, std::atoi(e)));
     if (const char *e = std::getenv("CFD2LCS_B200_SL_MARCH")) sl_march_ = std::atoi(e) != 0;
+    if (const char *e = std::getenv("CFD2LCS_B200_SORT_EVERY")) sort_every_ = std::max(0, std::atoi(e));
     if (const char *e = std::getenv("CFD2LCS_B200_SL_MARCH_KC")) sl_march_kc_ = std::max(0, std::atoi(e));
     for (int a = 0; a < 3; a++) n_[a] = n[a];
     // coordinate lines (and, on a non-rectilinear grid, the node coordinates) and interior flags
@@ -603,15 +608,30 @@ class Engine : public EngineBase {
         } else {
           // the variant holds from one sort to the next (the staged kernel reads the sort's tiles)
           const bool usable = fwd_tile_usable(iv, V);
-          if (sc % kSortInterval == 0) {
+          // the staged family re-sorts every kSortInterval subcycles of the update (its tiles
+          // must be the sort's); the gathering-only sets re-sort when their launches have lost
+          // more time to disorder than a sort costs (sort_due)
+          const int di = (int)(&d - diags_.data());
+          const bool resort = usable ? sc % sort_interval(interp) == 0 : sort_due(d);
+          if (resort) {
             d.fwd_variant = usable ? tile_variant(1) : 0;
+            cudaEvent_t s0, s1;
+            if (!usable && !mark(s0, msg)) return false;
             if (!sort_particles(d, msg, d.fwd_variant == 1)) return false;
+            if (!usable) {
+              if (!mark(s1, msg)) return false;
+              spans_.push_back({s0, s1, SPAN_SORT, -1, di, 0});
+            }
+            d.since_sort = 0;
+            d.excess_ms = 0;
           }
           const bool staged = usable && d.fwd_variant == 1;
           if (!mark(k0, msg)) return false;
           if (staged ? !launch_fwd_tile(d, sa, V, S, (T)dt, msg) : !launch_fwd(iv, sa, V, d.P, S, (T)dt, msg, dN(d))) return false;
           if (!mark(k1, msg)) return false;
-          spans_.push_back({k0, k1, kkind, usable && tune_[1].choice < 0 && tile_mode_ == 1 ? 2 + d.fwd_variant : -1});
+          spans_.push_back({k0, k1, kkind, usable && tune_[1].choice < 0 && tile_mode_ == 1 ? 2 + d.fwd_variant : -1, usable ? -1 : di,
+                            (int)std::min(d.since_sort, 1L << 30)});
+          d.since_sort++;
         }
         lp_time = lp_time + dt;
       }
@@ -734,6 +754,16 @@ class Engine : public EngineBase {
       } else if (sp.kind == SPAN_FWD) {
         counters_.fwd_kernel_ms += ms;
         counters_.fwd_kernel_launches++;
+        if (sp.diag >= 0 && sp.diag < (int)diags_.size()) {
+          DiagT &d = diags_[sp.diag];
+          if (sp.since == 0 || d.base_ms < 0) d.base_ms = ms;
+          else d.excess_ms += std::max(0.0, (double)ms - d.base_ms);
+        }
+      } else if (sp.kind == SPAN_SORT) {
+        if (sp.diag >= 0 && sp.diag < (int)diags_.size()) {
+          diags_[sp.diag].sort_ms = ms;
+          diags_[sp.diag].excess_ms = 0;  // launches collected before it belong to the old order
+        }
       } else {
         counters_.phase_ms[sp.kind] += ms;
       }
@@ -2239,6 +2269,9 @@ class Engine : public EngineBase {
   void launch_reset(DiagT &d) {
     const dim3 blk(32, 8, 1);
     counters_.kernel_launches++;
+    d.since_sort = 0;  // the particles are back on their nodes, in node order
+    d.base_ms = -1;
+    d.excess_ms = 0;
     if (d.lg) {
       FieldPtrs<T> pos{};
       for (int c = 0; c < 3; c++) pos.f[c] = d.lg->pos[c];
@@ -2259,6 +2292,23 @@ class Engine : public EngineBase {
 #define CFD2LCS_SORT_INTERVAL 2
 #endif
   static constexpr int kSortInterval = CFD2LCS_SORT_INTERVAL;
+  int sort_every_ = 0;  // CFD2LCS_B200_SORT_EVERY at cfd2lcs_init (0: the default below)
+  int sort_interval(int interp) const { return sort_every_ > 0 ? sort_every_ : kSortInterval; }
+  // Re-sort schedule of a set whose forward kernel gathers (not the staged family): a sort
+  // restores the coalescing the launches lose as the particles drift from the order of the
+  // last sort, so it pays once the time they have lost since that sort -- each launch's event
+  // time minus the first launch's after the sort -- reaches the sort's own event time (the
+  // rent-or-buy rule: at most twice the best fixed schedule's cost).  Launch times reach the
+  // engine when an update is collected, so the rule acts on update boundaries; until a sort
+  // has been timed the set re-sorts every kSortInterval subcycles.  Measured on B200, ABC
+  // 256^3 RK2 LINEAR: fixed intervals of 2 / 6 / 24 subcycles gave 59.2 / 52.4 / 50.0 ms per
+  // update (the launch 1.16 -> 1.20 -> 1.23 ms against 0.88 ms per sort), never re-sorting 51.2.
+  // CFD2LCS_B200_SORT_EVERY=n fixes the interval at n subcycles instead.
+  bool sort_due(const DiagT &d) const {
+    if (sort_every_ > 0) return d.since_sort >= sort_every_;
+    if (d.sort_ms <= 0) return d.since_sort >= kSortInterval;
+    return d.excess_ms >= d.sort_ms;
+  }
   // fwd_tile: the 16 x 4 x 4-cell tiles the staged forward kernel reads, else the 32 x 4 x 2
   // tiles that suit the gathering kernel
   bool sort_particles(DiagT &d, std::string &msg, bool fwd_tile = false) {
@@ -2314,11 +2364,13 @@ class Engine : public EngineBase {
   bool begun_ = false;
   Counters counters_;
   // event-timed spans of the update in flight: phase index 1..5, or one of the hot kernels
-  enum { SPAN_SL = 100, SPAN_FWD = 101 };
+  enum { SPAN_SL = 100, SPAN_FWD = 101, SPAN_SORT = 102 };
   struct Span {
     cudaEvent_t a, b;
     int kind;
-    int tune = -1;  // hot-kernel spans while the tuner samples: family * 2 + variant
+    int tune = -1;   // hot-kernel spans while the tuner samples: family * 2 + variant
+    int diag = -1;   // forward launches and sorts of a set on the sort_due schedule: its index
+    int since = 0;   // forward launches: subcycles since that set's last sort or reset
   };
   std::vector<cudaEvent_t> evpool_;
   size_t evnext_ = 0;
