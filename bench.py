@@ -99,6 +99,8 @@ WORKLOADS = {
                     desc="ABC flow 192^3 periodic, dt=0.05, FTLE bkwd T=2 h=1, RK3, cubic B-spline (profiling case)"),
     "abcproffwd": dict(kind="abc", n=192, dt=0.05, T=2.0, h=1.0, integrator=3, interpolator=3, dirs=(0,), t0=0.95,
                        desc="ABC flow 192^3 periodic, dt=0.05, FTLE fwd T=2 h=1, RK3, cubic B-spline (profiling case)"),
+    "abcproflinfwd": dict(kind="abc", n=192, dt=0.05, T=2.0, h=1.0, integrator=2, interpolator=1, dirs=(0,), t0=0.95,
+                          desc="ABC flow 192^3 periodic, dt=0.05, FTLE fwd T=2 h=1, RK2, linear (profiling case)"),
     "abcproflin": dict(kind="abc", n=192, dt=0.05, T=2.0, h=1.0, integrator=2, interpolator=1, dirs=(1,), t0=0.95,
                        desc="ABC flow 192^3 periodic, dt=0.05, FTLE bkwd T=2 h=1, RK2, linear (profiling case)"),
     # profiling case for the FTLE-field phase: frames of 10 sub-flow maps after 22 updates
