@@ -97,7 +97,7 @@ __device__ __forceinline__ void lin_stencil_ad(const DevGrid<T> &g, const T x[3]
     lo = min(max(lo, 0), g.P.n[a] + 1);
     hi = min(max(hi, 0), g.P.n[a] + 1);
     const T x0 = __ldg(L + lo), x1 = __ldg(L + hi);
-    const T raw = (x[a] - x0) / (x1 - x0);
+    const T raw = hi > lo && g.ri[a] ? lin_quotient(x[a] - x0, x1 - x0, __ldg(g.ri[a] + lo)) : (x[a] - x0) / (x1 - x0);
     s.t[a] = clamp01(raw);
     s.dtdx[a] = (raw > T(0) && raw < T(1)) ? T(1) / (x1 - x0) : T(0);
   }
@@ -1473,6 +1473,8 @@ class Adjoint {
     for (int a = 0; a < 3; a++) {
       if (!(dg_.lt[a] = upload(hg_.lt[a], msg))) return false;
       if (!(dg_.li[a] = upload(hg_.li[a], msg))) return false;
+      // the reciprocals of the spans the kernels form in T
+      if (!(dg_.ri[a] = upload(reciprocal_spans(std::vector<T>(hg_.li[a].begin(), hg_.li[a].end())), msg))) return false;
       if (!(dg_.invd[a] = upload(hg_.invd[a], msg))) return false;
       dg_.nrm[a] = nullptr;
     }

@@ -15,6 +15,22 @@ namespace cfd2lcs {
 // compiled arithmetic forms them
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
+// The interpolation fraction a / b of a LINEAR stencil from y = RN(1 / b), the bracket's
+// reciprocal span taken from a table: Markstein's correction step (P. Markstein, "Computation
+// of elementary functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990),
+// q0 = RN(a y), r = a - b q0 (exact in one FMA), q = RN(q0 + r y).  With a correctly rounded
+// reciprocal and q0 within one ulp of a / b, q is the correctly rounded quotient; it replaces
+// the IEEE division on the stencils' dependent chain.  Every LINEAR stencil of the library forms
+// its fraction this way, so the staged and gathering kernels stay bitwise equal to each other.
+template <typename T>
+__device__ __forceinline__ T lin_quotient(T a, T b, T y) {
+  const T q0 = mul_rn(a, y);
+  const T r = fma_rn(-b, q0, a);
+  return fma_rn(r, y, q0);
+}
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 
@@ -53,7 +69,8 @@ __device__ __forceinline__ void lin_stencil(const DevGrid<T> &g, const T x[3], c
     lo = min(max(lo, 0), g.P.n[a] + 1);
     hi = min(max(hi, 0), g.P.n[a] + 1);
     const T x0 = __ldg(L + lo), x1 = __ldg(L + hi);
-    t[a] = clamp01((x[a] - x0) / (x1 - x0));
+    // a bracket clamped onto one line (hi == lo) keeps the IEEE division of its 0 span
+    t[a] = clamp01(hi > lo && g.ri[a] ? lin_quotient(x[a] - x0, x1 - x0, __ldg(g.ri[a] + lo)) : (x[a] - x0) / (x1 - x0));
     mt[a] = T(1) - t[a];
     i0[a] = lo;
     st.i0[a] = lo;
@@ -72,18 +89,19 @@ __device__ __forceinline__ void lin_stencil(const DevGrid<T> &g, const T x[3], c
 }
 
 // lin_stencil around a grid node no (1 <= no <= n on every axis) from the node's interpolation
-// lines lm, lc, lp at no-1, no, no+1: the bracket is [no, no+1] or [no-1, no], which the clamps of
-// lin_stencil leave as they are, so the stencil is the same in every bit.
+// lines lm, lc, lp at no-1, no, no+1 and the reciprocal spans rm = ri[no-1], rp = ri[no]: the
+// bracket is [no, no+1] or [no-1, no], which the clamps of lin_stencil leave as they are, so the
+// stencil is the same in every bit.
 template <typename T>
-__device__ __forceinline__ void lin_stencil_node(const T lm[3], const T lc[3], const T lp[3], int sx, int sxy, const T x[3],
-                                                 const int no[3], LinStencil<T> &st) {
+__device__ __forceinline__ void lin_stencil_node(const T lm[3], const T lc[3], const T lp[3], const T rm[3], const T rp[3], int sx, int sxy,
+                                                 const T x[3], const int no[3], LinStencil<T> &st) {
   const int str[3] = {1, sx, sxy};
   T t[3], mt[3];
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     const bool up = x[a] > lc[a];
     const T x0 = up ? lc[a] : lm[a], x1 = up ? lp[a] : lc[a];
-    t[a] = clamp01((x[a] - x0) / (x1 - x0));
+    t[a] = clamp01(lin_quotient(x[a] - x0, x1 - x0, up ? rp[a] : rm[a]));
     mt[a] = T(1) - t[a];
     st.i0[a] = up ? no[a] : no[a] - 1;
     st.d[a] = 1;

@@ -42,6 +42,8 @@ struct DevGrid {
   GridParams<T> P;
   const T *lt[3];        // node coordinate lines, index 0..n+1
   const T *li[3];        // interpolation lines, index 0..n+1
+  // RN(1 / (li[a][i+1] - li[a][i])), index 0..n: the LINEAR stencils' fractions (lin_quotient)
+  const T *ri[3] = {nullptr, nullptr, nullptr};
   const T *invd[3];      // inverse half spans, see HostGrid::invd
   const int8_t *flag;    // padded bcflag or nullptr
   const T *nrm[3];       // boundary normals (padded) or nullptr

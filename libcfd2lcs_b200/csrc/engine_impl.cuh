@@ -1593,6 +1593,7 @@ class Engine : public EngineBase {
     for (int a = 0; a < 3; a++) {
       if (!(dg.lt[a] = upload(hg.lt[a], msg))) return false;
       if (!(dg.li[a] = upload(hg.li[a], msg))) return false;
+      if (!(dg.ri[a] = upload(reciprocal_spans(hg.li[a]), msg))) return false;
       if (!(dg.invd[a] = upload(hg.invd[a], msg))) return false;
     }
     dg.lsw = nullptr;
@@ -1799,7 +1800,7 @@ class Engine : public EngineBase {
 
   // LINEAR: 3-D grids whose backward set samples both levels per corner (no stage blends)
   bool sl_tile_lin_usable(const VelFields<TV> &V, FieldPtrs<T> fo) const {
-    if (!tile_mode_ || n_[2] < 4 || dg_.P.single_axis >= 0) return false;
+    if (!tile_mode_ || n_[2] < 4 || dg_.P.single_axis >= 0 || !dg_.ri[0] || !dg_.ri[1] || !dg_.ri[2]) return false;
     for (int c = 0; c < 3; c++) {
       if (V.cs[1][c] || reinterpret_cast<uintptr_t>(fo.f[c]) % 16 || reinterpret_cast<uintptr_t>(V.un[c]) % 16 ||
           reinterpret_cast<uintptr_t>(V.unp1[c]) % 16)

@@ -46,6 +46,20 @@ struct GridParams {
   R guessd[3][3];     // [direction a][coordinate c]
 };
 
+// RN(1 / (l[i+1] - l[i])) for i = 0 .. size-2 (0 where the span is 0, and at the last index):
+// the reciprocal spans of an interpolation line, the table the LINEAR stencils' quotient
+// (lin_quotient) reads.  R's own division, so the value is the correctly rounded reciprocal of
+// the span the kernels form as l[i+1] - l[i].
+template <typename R>
+inline std::vector<R> reciprocal_spans(const std::vector<R> &l) {
+  std::vector<R> r(l.size(), R(0));
+  for (size_t i = 0; i + 1 < l.size(); i++) {
+    const R b = l[i + 1] - l[i];
+    r[i] = b != R(0) ? R(1) / b : R(0);
+  }
+  return r;
+}
+
 template <typename R>
 struct HostGrid {
   GridParams<R> P{};

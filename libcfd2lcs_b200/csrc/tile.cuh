@@ -472,14 +472,15 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLT_MINB)
 // node (sample_velocity_node), the trilinear samples of interp_s2u_r1 LINEAR
 // (src/lp_tracking_m.f90:342-474) around the node from its interpolation lines lm, lc, lp at
 // no-1, no, no+1, then the previous flow map at the departure point, the boundary rules and the
-// ghost writes.  iv / ifm map a padded (x, y, z) to the staged index of a velocity / flow-map
+// ghost writes.  rm / rp are the reciprocal spans of the lines' brackets below and above the
+// node (DevGrid::ri at no-1 and no).  iv / ifm map a padded (x, y, z) to the staged index of a velocity / flow-map
 // component; u0 / u1 / fm (c, index) read component c of u_n, u_np1 and the flow map.  Every
 // staged LINEAR kernel runs this one expression, so they are bitwise equal to each other and to
 // k_sl_subcycle.
 template <typename T, typename TV, int INTEG, bool HAS_FLAGS, typename IV, typename IF, typename U0, typename U1, typename FM>
 __device__ __forceinline__ void lin_sl_node(const DevGrid<T> &g, const StageTimes &S, T dt, int i, int j, int k, const T xn[3], const T lm[3],
-                                            const T lc[3], const T lp[3], IV iv, IF ifm, U0 u0, U1 u1, FM fm, FieldPtrsW<T> fmn,
-                                            int *err) {
+                                            const T lc[3], const T lp[3], const T rm[3], const T rp[3], IV iv, IF ifm, U0 u0, U1 u1, FM fm,
+                                            FieldPtrsW<T> fmn, int *err) {
   constexpr int NOFF = INTEG == RK2_ ? 1 : (INTEG == RK3_ ? 2 : (INTEG == RK4_ ? 3 : 0));
   const T HALF = T(1) / T(2), THIRD = T(1) / T(3), TWOTHIRD = T(2) / T(3), SIXTH = T(1) / T(6), TWO = T(2);
   const int sx = g.P.sx, sxy = g.P.sxy;
@@ -487,7 +488,7 @@ __device__ __forceinline__ void lin_sl_node(const DevGrid<T> &g, const StageTime
   auto vel_sample = [&](const T x[3], T ct_, T u[3]) {
     const TV ct = TV(ct_), omc = TV(1) - ct;
     LinStencil<T> st;
-    lin_stencil_node(lm, lc, lp, sx, sxy, x, no, st);
+    lin_stencil_node(lm, lc, lp, rm, rp, sx, sxy, x, no, st);
     int idx[8];
 #pragma unroll
     for (int c = 0; c < 8; c++)
@@ -571,7 +572,7 @@ __device__ __forceinline__ void lin_sl_node(const DevGrid<T> &g, const StageTime
   }
   // previous flow map at the departure point (sample_field LINEAR around the node)
   LinStencil<T> st;
-  lin_stencil_node(lm, lc, lp, sx, sxy, x, no, st);
+  lin_stencil_node(lm, lc, lp, rm, rp, sx, sxy, x, no, st);
   int idx[8];
 #pragma unroll
   for (int c = 0; c < 8; c++)
@@ -649,7 +650,7 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLL_MINB)
   }
   // the interpolation lines at no-1, no, no+1 of both points (every bracket of a node's stages
   // and departure point lies there), read while the box copies are in flight
-  T lm[2][3], lc[2][3], lp[2][3];
+  T lm[2][3], lc[2][3], lp[2][3], rm[2][3], rp[2][3];
 #pragma unroll
   for (int q = 0; q < 2; q++) {
     const int nd[3] = {min(i, g.P.n[0]), min(j, g.P.n[1]), min(kq[q], g.P.n[2])};
@@ -658,13 +659,15 @@ __global__ void __launch_bounds__(SLT_THREADS, CFD2LCS_SLL_MINB)
       lm[q][a] = __ldg(g.li[a] + nd[a] - 1);
       lc[q][a] = __ldg(g.li[a] + nd[a]);
       lp[q][a] = __ldg(g.li[a] + nd[a] + 1);
+      rm[q][a] = __ldg(g.ri[a] + nd[a] - 1);
+      rp[q][a] = __ldg(g.ri[a] + nd[a]);
     }
   }
 #pragma unroll
   for (int q = 0; q < 2; q++) {
     if (!ok[q]) continue;
     lin_sl_node<T, TV, INTEG, HAS_FLAGS>(
-        g, S, dt, i, j, kq[q], xn[q], lm[q], lc[q], lp[q],
+        g, S, dt, i, j, kq[q], xn[q], lm[q], lc[q], lp[q], rm[q], rp[q],
         [&](int x, int y, int z) { return tile_index<LinGeom, TV>(b, sx, sxy, x, y, z); },
         [&](int x, int y, int z) { return tile_index<LinGeom, T>(b, sx, sxy, x, y, z); },
         [&](int c, int e) { return su0[(size_t)c * LinGeom::comp<TV>() + e]; },
@@ -730,8 +733,8 @@ __global__ void __launch_bounds__(SLM_THREADS, CFD2LCS_SLM_MINB)
 
   const int i = xs + 1 + (int)threadIdx.x, j = ys + 1 + (int)threadIdx.y;
   const bool ok = i <= g.P.n[0] && j <= g.P.n[1];
-  // x and y stay fixed along the column: the node coordinates and the interpolation lines at
-  // no-1, no, no+1 of both axes are read once
+  // x and y stay fixed along the column: the node coordinates, the interpolation lines at
+  // no-1, no, no+1 and the reciprocal spans of both axes are read once
   const int ni = min(i, g.P.n[0]), nj = min(j, g.P.n[1]);
   T xn[3], lm[3], lc[3], lp[3];
   xn[0] = __ldg(g.lt[0] + min(i, g.P.n[0] + 1));
@@ -739,6 +742,10 @@ __global__ void __launch_bounds__(SLM_THREADS, CFD2LCS_SLM_MINB)
   lm[0] = __ldg(g.li[0] + ni - 1), lc[0] = __ldg(g.li[0] + ni), lp[0] = __ldg(g.li[0] + ni + 1);
   lm[1] = __ldg(g.li[1] + nj - 1), lc[1] = __ldg(g.li[1] + nj), lp[1] = __ldg(g.li[1] + nj + 1);
   T zc = __ldg(g.li[2] + K0 - 1), zp = __ldg(g.li[2] + K0);
+  T rm[3], rp[3];
+  rm[0] = __ldg(g.ri[0] + ni - 1), rp[0] = __ldg(g.ri[0] + ni);
+  rm[1] = __ldg(g.ri[1] + nj - 1), rp[1] = __ldg(g.ri[1] + nj);
+  T rz = __ldg(g.ri[2] + K0 - 1);
   auto sidx = [&](int x, int y, int z) { return (z & 3) * 9 * CS + (y - ys) * SLM_SX + (x - xs); };
   for (int k = K0; k <= K1; k++) {
     bool w = mbar_wait_bounded(&bar[(k + 1) & 3], parity(k + 1));
@@ -761,9 +768,12 @@ __global__ void __launch_bounds__(SLM_THREADS, CFD2LCS_SLM_MINB)
     zp = __ldg(g.li[2] + k + 1);
     lp[2] = zp;
     xn[2] = __ldg(g.lt[2] + k);
+    rm[2] = rz;
+    rz = __ldg(g.ri[2] + k);
+    rp[2] = rz;
     if (ok)
       lin_sl_node<T, T, INTEG, HAS_FLAGS>(
-          g, S, dt, i, j, k, xn, lm, lc, lp, sidx, sidx, [&](int c, int e) { return box[(size_t)c * CS + e]; },
+          g, S, dt, i, j, k, xn, lm, lc, lp, rm, rp, sidx, sidx, [&](int c, int e) { return box[(size_t)c * CS + e]; },
           [&](int c, int e) { return box[(size_t)(3 + c) * CS + e]; }, [&](int c, int e) { return box[(size_t)(6 + c) * CS + e]; },
           fmn, err);
   }
