@@ -565,6 +565,7 @@ CFD2LCS_EXPORT int cfd2lcs_batch_add_c(const int n[3], const lcsdata_t *x, const
   bi->opt.interpolator = interpolator;
   bi->opt.cfl = (double)cfl;
   bi->opt.mixed_precision = mixed_precision ? 1 : 0;
+  bi->opt.shared_device = 1;
   for (int a = 0; a < 3; a++) bi->n[a] = n[a];
   bi->eng = cfd2lcs::make_engine(&bi->opt);
   std::string msg;

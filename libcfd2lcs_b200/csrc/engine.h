@@ -33,6 +33,9 @@ struct Options {
   // the default centre is huge(1.0), so no node is inside until the caller sets it
   double tracer_x = 1.0e300, tracer_y = 1.0e300, tracer_z = 1.0e300, tracer_r = 0.0;
   int write_lcs_async = 0;  // extension: let a frame's file complete after cfd2lcs_update returns
+  // set for the batched form's instances: their kernels overlap other instances' on the device,
+  // so their event times are not their own (the forward sets then re-sort on the fixed interval)
+  int shared_device = 0;
 };
 
 struct Counters {
