@@ -342,6 +342,8 @@ __global__ void __launch_bounds__(256, fwd_min_blocks<INTERP>()) k_fwd_subcycle(
   if (q >= np) return;
   T xn[3] = {P.x[0][q], P.x[1][q], P.x[2][q]};
   int no[3] = {P.no[0][q], P.no[1][q], P.no[2][q]};
+  // the accumulated displacement is read up front, off the integration's dependent chain
+  const T dx0[3] = {P.dx[0][q], P.dx[1][q], P.dx[2][q]};
   constexpr bool CURV = interp_is_curv(INTERP);
   T x[3];
   integrate<T, TV, INTEG, INTERP, false, particle_uniform_basis()>(g, sa, V, S, dt, xn, no, x);
@@ -353,7 +355,7 @@ __global__ void __launch_bounds__(256, fwd_min_blocks<INTERP>()) k_fwd_subcycle(
     x[2] = xn[2];
   }
 #pragma unroll
-  for (int c = 0; c < 3; c++) P.dx[c][q] = P.dx[c][q] + (x[c] - xn[c]);
+  for (int c = 0; c < 3; c++) P.dx[c][q] = dx0[c] + (x[c] - xn[c]);
   track_pass<T, CURV>(g, x, no);
   wrap_particle(g, x, no);
 #pragma unroll
