@@ -4,7 +4,8 @@ by one FMA, q = RN(q0 + r y); csrc/advect.cuh lin_quotient).  This checks that s
 IEEE quotient on the host (same IEEE-754 binary64 / binary32 arithmetic and fused multiply-add as
 the device), bit for bit: stencil-shaped cases (a point inside or just outside its bracket on
 uniform and irregular lines, spans whose significands end in long runs of ones, spans over 30
-binades) and random operands over 120 binades, in double and in float.  No GPU needed."""
+binades) and random operands over 120 binades, in double and in float; and that the table the
+kernels read holds those correctly rounded reciprocals.  No GPU needed."""
 import os
 import shutil
 import subprocess
@@ -61,3 +62,52 @@ def test_markstein_quotient_equals_ieee_division(tmp_path):
     cnt, bad, badf = int(out[0]), int(out[1]), int(out[2])
     assert cnt > 19_000_000
     assert bad == 0 and badf == 0, out
+
+
+HOST_SRC = r'''
+#include <cstdio>
+#include <vector>
+#include "grid.h"
+int main() {
+  std::vector<double> l;
+  std::vector<float> lf;
+  double x = -3.0;
+  unsigned long long s = 12345;
+  for (int i = 0; i < 2000; i++) {
+    s = s * 6364136223846793005ull + 1442695040888963407ull;
+    x += 1e-3 + (double)(s >> 11) / 9007199254740992.0;
+    l.push_back(x);
+    lf.push_back((float)x);
+  }
+  l.push_back(x);  // a repeated line: zero span
+  lf.push_back((float)x);
+  const std::vector<double> r = cfd2lcs::reciprocal_spans(l);
+  const std::vector<float> rf = cfd2lcs::reciprocal_spans(lf);
+  for (size_t i = 0; i < l.size(); i++) printf("%a %a %a %a\n", l[i], r[i], (double)lf[i], (double)rf[i]);
+  return 0;
+}
+'''
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_reciprocal_span_table_is_correctly_rounded(tmp_path):
+    """The table the kernels read (csrc/grid.h reciprocal_spans): RN(1 / (l[i+1] - l[i])) in the
+    table's own type, 0 for a zero span and at the last index."""
+    import numpy as np
+    here = os.path.dirname(os.path.abspath(__file__))
+    csrc = os.path.join(os.path.dirname(here), "libcfd2lcs_b200", "csrc")
+    c, exe = tmp_path / "rs.cpp", tmp_path / "rs"
+    c.write_text(HOST_SRC)
+    subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I", csrc, "-o", str(exe), str(c)], check=True)
+    rows = [ln.split() for ln in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines()]
+    l = np.array([float.fromhex(r[0]) for r in rows])
+    r = np.array([float.fromhex(r[1]) for r in rows])
+    lf = np.array([float.fromhex(r[2]) for r in rows], dtype=np.float32)
+    rf = np.array([float.fromhex(r[3]) for r in rows], dtype=np.float32)
+    span = l[1:] - l[:-1]
+    want = np.where(span != 0, 1.0 / np.where(span != 0, span, 1.0), 0.0)
+    assert np.array_equal(r[:-1], want) and r[-1] == 0.0
+    spanf = (lf[1:] - lf[:-1]).astype(np.float32)
+    wantf = np.where(spanf != 0, np.float32(1) / np.where(spanf != 0, spanf, np.float32(1)), np.float32(0)).astype(np.float32)
+    assert np.array_equal(rf[:-1], wantf) and rf[-1] == 0.0
+    assert r[-2] == 0.0 and rf[-2] == 0.0  # the repeated line
